@@ -1,0 +1,85 @@
+/* starplat_b200 — C ABI of the B200-native (sm_100a) static-graph kernels.
+ *
+ * Drop-in boundary: StarPlat's code generators emit one C++ entry point per DSL
+ * program, taking the CSR container `graph&` plus raw property arrays
+ * (signature emitter: src/backends/backend_omp/dsl_cpp_generator.cpp:3098-3151,
+ * type mapping :2875-3050). include/starplat_b200.hpp keeps those exact C++
+ * signatures and forwards to the plain-pointer functions below.
+ *
+ * Conventions
+ *   - Every function returns an int status: SP_OK (0) or a negative SP_ERR_*;
+ *     sp_last_error() gives a message for the calling thread. No exceptions
+ *     cross this ABI.
+ *   - Array arguments may be host or device pointers (CUDA unified addressing
+ *     decides the copy direction). Output arrays are sized num_nodes().
+ *   - A graph handle is used from one host thread at a time.
+ *   - All indices are int32, as in graph.hpp:44-57; edge counts must be < 2^31.
+ */
+#ifndef STARPLAT_B200_H
+#define STARPLAT_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  SP_OK = 0,
+  SP_ERR_INVALID = -1,     /* bad argument or malformed CSR */
+  SP_ERR_CUDA = -2,        /* CUDA runtime error */
+  SP_ERR_OOM = -3,         /* device allocation failed */
+  SP_ERR_TIMEOUT = -4,     /* a bounded device-side loop ran out of iterations */
+  SP_ERR_UNSUPPORTED = -5, /* input outside what this build handles */
+  SP_ERR_NEG_CYCLE = -6    /* SSSP: negative cycle reachable from the source */
+};
+
+typedef struct sp_graph* sp_graph_h;
+
+/* graph creation flags */
+#define SP_GRAPH_DEVICE_PTRS 0x1u  /* the CSR pointers given are device pointers */
+
+/* ---- library -------------------------------------------------------------- */
+int sp_version(void);
+const char* sp_last_error(void);
+/* Number of kernels this library has launched in this process (graph nodes count once each). */
+unsigned long long sp_launch_count(void);
+
+/* ---- device mirror of graph.hpp's CSR (uploaded once, reused by every call) ----
+ * Replaces the per-call H2D copy of the generated CUDA code
+ * (backend_cuda/dsl_cpp_generator.cpp:4104-4297, generateCSRArrays).
+ * indexofNodes[V+1], edgeList[E]: forward CSR (graph.hpp:44-50), adjacency sorted.
+ * edgeLen[E] (weights, graph.hpp:38) may be NULL.
+ * rev_indexofNodes[V+1], srcList[E] (graph.hpp:45-52) may be NULL: then the
+ * reverse CSR is built on the device. */
+int sp_graph_create(int32_t V, int64_t E, const int32_t* indexofNodes, const int32_t* edgeList,
+                    const int32_t* edgeLen, const int32_t* rev_indexofNodes, const int32_t* srcList,
+                    uint32_t flags, sp_graph_h* out);
+int sp_graph_free(sp_graph_h g);
+/* Use this CUDA stream (a cudaStream_t) for all later work on g; NULL = the library's own stream. */
+int sp_graph_set_stream(sp_graph_h g, void* cuda_stream);
+/* V, E, symmetric (1 when the forward CSR equals the reverse CSR). */
+int sp_graph_info(sp_graph_h g, int32_t* V, int64_t* E, int32_t* symmetric);
+
+/* ---- triangle counting -------------------------------------------------------
+ * Replaces generated `auto Compute_TC(graph& g)` (DSL staticDSLCodes/triangle_counting_dsl:1-13):
+ *   count = sum_v sum_{u in N(v), u<v} sum_{w in N(v), w>v} [u->w is an edge]
+ * Exact int64. Undirected graphs use a degree-ordered orientation; other graphs
+ * follow the formula literally. */
+int sp_tc(sp_graph_h g, int64_t* triangle_count);
+
+/* ---- PageRank ----------------------------------------------------------------
+ * Replaces generated `void ComputePageRank(graph& g, float beta, float delta, int maxIter,
+ * float* pageRank)` (DSL staticDSLCodes/PageRankDSLV3:1-25): Jacobi pull over the
+ * reverse CSR, pr0 = 1/V, pr' = (1-delta)/V + delta * sum pr[u]/outdeg(u), repeated
+ * while L1 diff > beta and iterations < maxIter. FP32 ranks, FP64 row sums.
+ * iterations / final_diff may be NULL. variant: SP_PR_TUNED or SP_PR_PLAIN. */
+#define SP_PR_TUNED 0
+#define SP_PR_PLAIN 1
+int sp_pagerank(sp_graph_h g, float beta, float delta, int32_t maxIter, float* pageRank,
+                int32_t* iterations, double* final_diff, int32_t variant);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* STARPLAT_B200_H */

@@ -1,0 +1,206 @@
+"""ORACLE — test infrastructure only.
+
+ctypes front end over ``oracle/libsporacle.so`` (the CPU restatement in
+sp_oracle.cpp) and, when it was built in a reference checkout,
+``oracle/_ref/libspref.so`` (the reference's own graph.hpp CSR container and
+check_if_nbr, via ref_harness.cpp). Only tests, ``__graft_entry__.smoke()`` and
+the CPU-baseline leg of ``bench.py`` import this module; the product path never
+does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+
+_OR = None
+_REF = None
+
+
+def lib():
+    global _OR
+    if _OR is None:
+        path = os.path.join(_HERE, "libsporacle.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} missing: build it with `make -C oracle`")
+        L = ctypes.CDLL(path)
+        L.or_tc.restype = ctypes.c_int64
+        L.or_tc.argtypes = [ctypes.c_int32, i32p, i32p, ctypes.c_int]
+        L.or_tc_omp.restype = ctypes.c_int64
+        L.or_tc_omp.argtypes = [ctypes.c_int32, i32p, i32p, ctypes.c_int, ctypes.c_int32, ctypes.c_int32]
+        L.or_pagerank.restype = ctypes.c_int32
+        L.or_pagerank.argtypes = [ctypes.c_int32, i32p, i32p, i32p, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_int32, ctypes.c_int32, f64p, ctypes.POINTER(ctypes.c_double),
+                                  ctypes.c_int]
+        L.or_pagerank_omp.restype = ctypes.c_int32
+        L.or_pagerank_omp.argtypes = [ctypes.c_int32, i32p, i32p, i32p, ctypes.c_float, ctypes.c_float,
+                                      ctypes.c_int32, f32p, ctypes.c_int]
+        L.or_sssp.restype = ctypes.c_int32
+        L.or_sssp.argtypes = [ctypes.c_int32, i32p, i32p, i32p, ctypes.c_int32, i32p]
+        L.or_sssp_bf.restype = ctypes.c_int32
+        L.or_sssp_bf.argtypes = [ctypes.c_int32, i32p, i32p, i32p, ctypes.c_int32, i32p]
+        L.or_sssp_omp.restype = ctypes.c_int32
+        L.or_sssp_omp.argtypes = [ctypes.c_int32, i32p, i32p, i32p, ctypes.c_int32, i32p, ctypes.c_int32,
+                                  ctypes.c_int]
+        L.or_bfs_sigma.restype = ctypes.c_int32
+        L.or_bfs_sigma.argtypes = [ctypes.c_int32, i32p, i32p, ctypes.c_int32, i32p, f64p]
+        L.or_bc.restype = None
+        L.or_bc.argtypes = [ctypes.c_int32, i32p, i32p, i32p, ctypes.c_int32, f64p, ctypes.c_int]
+        L.or_bc_omp.restype = None
+        L.or_bc_omp.argtypes = [ctypes.c_int32, i32p, i32p, i32p, ctypes.c_int32, f32p, ctypes.c_int]
+        L.or_louvain.restype = ctypes.c_double
+        L.or_louvain.argtypes = [ctypes.c_int32, i32p, i32p, ctypes.c_void_p, ctypes.c_double, i32p,
+                                 ctypes.POINTER(ctypes.c_int32)]
+        L.or_modularity.restype = ctypes.c_double
+        L.or_modularity.argtypes = [ctypes.c_int32, i32p, i32p, ctypes.c_void_p, i32p]
+        L.or_num_threads.restype = ctypes.c_int32
+        _OR = L
+    return _OR
+
+
+def ref_lib() -> Optional[ctypes.CDLL]:
+    """The reference-compiled harness, or None when it was not built."""
+    global _REF
+    if _REF is None:
+        path = os.path.join(_HERE, "_ref", "libspref.so")
+        if not os.path.exists(path):
+            return None
+        L = ctypes.CDLL(path)
+        L.ref_parse_graph.restype = ctypes.c_void_p
+        L.ref_parse_graph.argtypes = [ctypes.c_char_p]
+        L.ref_graph_sizes.restype = None
+        L.ref_graph_sizes.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]
+        L.ref_graph_copy.restype = None
+        L.ref_graph_copy.argtypes = [ctypes.c_void_p, i32p, i32p, i32p, i32p, i32p, i32p]
+        L.ref_tc.restype = ctypes.c_int64
+        L.ref_tc.argtypes = [ctypes.c_int32, i32p, i32p, ctypes.c_int, ctypes.c_int32, ctypes.c_int32]
+        _REF = L
+    return _REF
+
+
+def _c(a, dt=np.int32):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+def tc(off, adj, nthreads: int = 0) -> int:
+    return int(lib().or_tc(len(off) - 1, _c(off), _c(adj), nthreads))
+
+
+def tc_omp(off, adj, nthreads: int = 0, vfirst: int = 0, vstride: int = 1) -> int:
+    return int(lib().or_tc_omp(len(off) - 1, _c(off), _c(adj), nthreads, vfirst, vstride))
+
+
+def pagerank(off, roff, radj, beta=1e-6, delta=0.85, max_iter=100, fixed_iters=0, nthreads=0):
+    V = len(off) - 1
+    out = np.empty(V, np.float64)
+    diff = ctypes.c_double(0)
+    it = lib().or_pagerank(V, _c(off), _c(roff), _c(radj), beta, delta, max_iter, fixed_iters, out,
+                           ctypes.byref(diff), nthreads)
+    return out, int(it), float(diff.value)
+
+
+def pagerank_omp(off, roff, radj, beta=1e-6, delta=0.85, max_iter=100, nthreads=0):
+    V = len(off) - 1
+    out = np.empty(V, np.float32)
+    it = lib().or_pagerank_omp(V, _c(off), _c(roff), _c(radj), beta, delta, max_iter, out, nthreads)
+    return out, int(it)
+
+
+def sssp(off, adj, w, src: int) -> np.ndarray:
+    V = len(off) - 1
+    dist = np.empty(V, np.int32)
+    rc = lib().or_sssp(V, _c(off), _c(adj), _c(w), src, dist)
+    if rc == -2:
+        rc = lib().or_sssp_bf(V, _c(off), _c(adj), _c(w), src, dist)
+    if rc != 0:
+        raise ValueError(f"oracle sssp failed ({rc})")
+    return dist
+
+
+def sssp_omp(off, adj, w, src: int, max_rounds: int = 0, nthreads: int = 0):
+    V = len(off) - 1
+    dist = np.empty(V, np.int32)
+    rounds = lib().or_sssp_omp(V, _c(off), _c(adj), _c(w), src, dist, max_rounds, nthreads)
+    return dist, int(rounds)
+
+
+def bfs_sigma(off, adj, src: int):
+    V = len(off) - 1
+    lvl = np.empty(V, np.int32)
+    sig = np.empty(V, np.float64)
+    n = lib().or_bfs_sigma(V, _c(off), _c(adj), src, lvl, sig)
+    return lvl, sig, int(n)
+
+
+def bc(off, adj, srcs, nthreads: int = 0) -> np.ndarray:
+    V = len(off) - 1
+    out = np.empty(V, np.float64)
+    s = _c(srcs)
+    lib().or_bc(V, _c(off), _c(adj), s, s.shape[0], out, nthreads)
+    return out
+
+
+def bc_omp(off, adj, srcs, nthreads: int = 0) -> np.ndarray:
+    V = len(off) - 1
+    out = np.empty(V, np.float32)
+    s = _c(srcs)
+    lib().or_bc_omp(V, _c(off), _c(adj), s, s.shape[0], out, nthreads)
+    return out
+
+
+def louvain(off, adj, w=None, threshold: float = 1e-4):
+    V = len(off) - 1
+    comm = np.empty(V, np.int32)
+    levels = ctypes.c_int32(0)
+    wp = None
+    if w is not None:
+        w = _c(w, np.float32)
+        wp = w.ctypes.data
+    q = lib().or_louvain(V, _c(off), _c(adj), wp, threshold, comm, ctypes.byref(levels))
+    return float(q), comm, int(levels.value)
+
+
+def modularity(off, adj, comm, w=None) -> float:
+    V = len(off) - 1
+    wp = None
+    if w is not None:
+        w = _c(w, np.float32)
+        wp = w.ctypes.data
+    return float(lib().or_modularity(V, _c(off), _c(adj), wp, _c(comm)))
+
+
+def num_threads() -> int:
+    return int(lib().or_num_threads())
+
+
+# ---- reference-compiled harness ------------------------------------------------
+
+def ref_tc(off, adj, nthreads: int = 0, vfirst: int = 0, vstride: int = 1) -> int:
+    L = ref_lib()
+    if L is None:
+        raise RuntimeError("oracle/_ref/libspref.so not built (needs the reference checkout)")
+    return int(L.ref_tc(len(off) - 1, _c(off), _c(adj), nthreads, vfirst, vstride))
+
+
+def ref_parse_graph(path: str):
+    """Reference graph::parseGraph on a text edge list -> dict of CSR arrays."""
+    L = ref_lib()
+    if L is None:
+        raise RuntimeError("oracle/_ref/libspref.so not built (needs the reference checkout)")
+    h = L.ref_parse_graph(path.encode())
+    V = ctypes.c_int32(0)
+    E = ctypes.c_int32(0)
+    L.ref_graph_sizes(h, ctypes.byref(V), ctypes.byref(E))
+    V, E = V.value, E.value
+    arrs = [np.empty(V + 1, np.int32), np.empty(max(E, 1), np.int32), np.empty(max(E, 1), np.int32),
+            np.empty(V + 1, np.int32), np.empty(max(E, 1), np.int32), np.empty(max(E, 1), np.int32)]
+    L.ref_graph_copy(h, *arrs)
+    names = ["indexofNodes", "edgeList", "edgeLen", "rev_indexofNodes", "srcList", "edgeMap"]
+    return {k: (a if k in ("indexofNodes", "rev_indexofNodes") else a[:E]) for k, a in zip(names, arrs)}

@@ -1,0 +1,80 @@
+"""ctypes binding of libsp_b200.so (the C ABI in include/starplat_b200.h).
+
+The CUDA library is the only compute path: if it is missing or cannot load,
+every call raises — there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsp_b200.so")
+
+SP_OK = 0
+SP_ERR = {
+    -1: "SP_ERR_INVALID",
+    -2: "SP_ERR_CUDA",
+    -3: "SP_ERR_OOM",
+    -4: "SP_ERR_TIMEOUT",
+    -5: "SP_ERR_UNSUPPORTED",
+    -6: "SP_ERR_NEG_CYCLE",
+}
+
+SP_GRAPH_DEVICE_PTRS = 0x1
+SP_PR_TUNED = 0
+SP_PR_PLAIN = 1
+
+_L = None
+
+vp = ctypes.c_void_p
+i32 = ctypes.c_int32
+i64 = ctypes.c_int64
+f32 = ctypes.c_float
+f64 = ctypes.c_double
+P = ctypes.POINTER
+
+
+class SPError(RuntimeError):
+    def __init__(self, fn: str, status: int, msg: str):
+        super().__init__(f"{fn} failed: {SP_ERR.get(status, status)}: {msg}")
+        self.status = status
+
+
+# name -> (restype, argtypes); every symbol include/starplat_b200.h declares
+SIGNATURES = {
+    "sp_version": (ctypes.c_int, []),
+    "sp_last_error": (ctypes.c_char_p, []),
+    "sp_launch_count": (ctypes.c_ulonglong, []),
+    "sp_graph_create": (ctypes.c_int, [i32, i64, vp, vp, vp, vp, vp, ctypes.c_uint32, P(vp)]),
+    "sp_graph_free": (ctypes.c_int, [vp]),
+    "sp_graph_set_stream": (ctypes.c_int, [vp, vp]),
+    "sp_graph_info": (ctypes.c_int, [vp, P(i32), P(i64), P(i32)]),
+    "sp_tc": (ctypes.c_int, [vp, P(i64)]),
+    "sp_pagerank": (ctypes.c_int, [vp, f32, f32, i32, vp, P(i32), P(f64), i32]),
+}
+
+
+def lib() -> ctypes.CDLL:
+    global _L
+    if _L is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it (python -m starplat_b200.build); "
+                               "there is no CPU fallback")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _L = L
+    return _L
+
+
+def check(fn: str, status: int) -> None:
+    if status != SP_OK:
+        msg = lib().sp_last_error()
+        raise SPError(fn, status, msg.decode() if msg else "")
+
+
+def launch_count() -> int:
+    return int(lib().sp_launch_count())

@@ -1,0 +1,43 @@
+"""The generated StarPlat entry points, same names and argument meaning.
+
+Each takes a ``CSRGraph`` (the host container in the layout of graph.hpp) plus
+the property arrays, exactly like the C++ functions the StarPlat generator
+emits (signature emitter backend_omp/dsl_cpp_generator.cpp:3098-3151). The device
+mirror is uploaded on first use and cached on the graph object, as the C++
+wrappers in include/starplat_b200.hpp cache it per `graph*`.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .device import DeviceGraph
+from .graph import CSRGraph
+
+
+def device_graph(g: CSRGraph) -> DeviceGraph:
+    dg = getattr(g, "_device_mirror", None)
+    if dg is None:
+        dg = DeviceGraph.from_csr(g)
+        g._device_mirror = dg
+    return dg
+
+
+def invalidate(g: CSRGraph) -> None:
+    """Drop the cached device mirror (call after mutating the host CSR)."""
+    dg = getattr(g, "_device_mirror", None)
+    if dg is not None:
+        dg.free()
+        g._device_mirror = None
+
+
+def Compute_TC(g: CSRGraph) -> int:
+    """staticDSLCodes/triangle_counting_dsl: returns the int64 triangle count."""
+    return device_graph(g).tc()
+
+
+def ComputePageRank(g: CSRGraph, beta: float, delta: float, maxIter: int, pageRank: np.ndarray) -> None:
+    """staticDSLCodes/PageRankDSLV3: writes float pageRank[num_nodes()]."""
+    device_graph(g).pagerank(beta, delta, maxIter, out=pageRank)
+
+
+Compute_PR = ComputePageRank  # the V2 DSL's name, same parameters

@@ -1,0 +1,141 @@
+// Internal definitions shared by the sm_100a kernels and the C-ABI layer.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include "../../include/starplat_b200.h"
+
+namespace sp {
+
+// ----------------------------------------------------------------- errors
+void set_error(const char* fmt, ...);
+extern std::atomic<unsigned long long> g_launches;  // kernels launched by this library
+
+#define SP_CHECK_CUDA(call)                                                                  \
+  do {                                                                                       \
+    cudaError_t _e = (call);                                                                 \
+    if (_e != cudaSuccess) {                                                                 \
+      ::sp::set_error("%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(_e));     \
+      return _e == cudaErrorMemoryAllocation ? SP_ERR_OOM : SP_ERR_CUDA;                     \
+    }                                                                                        \
+  } while (0)
+
+#define SP_CHECK_LAUNCH()                                                                    \
+  do {                                                                                       \
+    ::sp::g_launches.fetch_add(1, std::memory_order_relaxed);                                \
+    cudaError_t _e = cudaGetLastError();                                                     \
+    if (_e != cudaSuccess) {                                                                 \
+      ::sp::set_error("%s:%d launch: %s", __FILE__, __LINE__, cudaGetErrorString(_e));      \
+      return SP_ERR_CUDA;                                                                    \
+    }                                                                                        \
+  } while (0)
+
+#define SP_TRY(expr)                 \
+  do {                               \
+    int _s = (expr);                 \
+    if (_s != SP_OK) return _s;      \
+  } while (0)
+
+// ----------------------------------------------------------------- device buffer
+template <class T>
+struct dbuf {
+  T* p = nullptr;
+  size_t n = 0;
+  dbuf() = default;
+  dbuf(const dbuf&) = delete;
+  dbuf& operator=(const dbuf&) = delete;
+  ~dbuf() { release(); }
+  int alloc(size_t count) {
+    if (count <= n && p) return SP_OK;
+    release();
+    size_t bytes = (count ? count : 1) * sizeof(T) + 16;  // +16: vector loads may read one int4 past the end
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      n = 0;
+      set_error("cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
+      return e == cudaErrorMemoryAllocation ? SP_ERR_OOM : SP_ERR_CUDA;
+    }
+    n = count;
+    return SP_OK;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+// ----------------------------------------------------------------- plans (per graph caches)
+struct PrPlan;
+struct TcPlan;
+struct SsspPlan;
+struct BcPlan;
+struct LvPlan;
+void free_pr_plan(PrPlan*);
+void free_tc_plan(TcPlan*);
+void free_sssp_plan(SsspPlan*);
+void free_bc_plan(BcPlan*);
+void free_lv_plan(LvPlan*);
+
+}  // namespace sp
+
+// The device-resident mirror of a reference `graph` (graph.hpp:44-57).
+struct sp_graph {
+  int device = 0;
+  int32_t V = 0;
+  int64_t E = 0;
+  sp::dbuf<int32_t> off;   // indexofNodes [V+1]
+  sp::dbuf<int32_t> adj;   // edgeList [E]
+  sp::dbuf<int32_t> w;     // edgeLen [E] (optional)
+  sp::dbuf<int32_t> roff;  // rev_indexofNodes [V+1]
+  sp::dbuf<int32_t> radj;  // srcList [E]
+  bool has_w = false;
+  bool has_rev = false;
+  int symmetric = -1;      // -1 unknown, 0/1
+  int32_t max_out_deg = -1;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  sp::PrPlan* pr = nullptr;
+  sp::TcPlan* tc = nullptr;
+  sp::SsspPlan* sssp = nullptr;
+  sp::BcPlan* bc = nullptr;
+  sp::LvPlan* lv = nullptr;
+};
+
+namespace sp {
+int ensure_reverse(sp_graph* g);      // builds roff/radj on device if missing
+int ensure_symmetry(sp_graph* g);     // fills g->symmetric
+int copy_out(void* dst, const void* src, size_t bytes, cudaStream_t s);  // host or device dst
+int num_sms();
+}  // namespace sp
+
+// ----------------------------------------------------------------- device helpers
+namespace sp {
+__device__ __forceinline__ int warp_id() { return threadIdx.x >> 5; }
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+template <class T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-wide sum with a fixed reduction tree (deterministic). All threads get the result.
+template <int THREADS, class T>
+__device__ __forceinline__ T block_sum(T v, T* s_red /* THREADS/32 */) {
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane_id() == 0) s_red[warp_id()] = v;
+  __syncthreads();
+  T r = 0;
+#pragma unroll
+  for (int i = 0; i < THREADS / 32; ++i) r += s_red[i];
+  return r;
+}
+}  // namespace sp

@@ -1,0 +1,506 @@
+// PageRank, pull form over the reverse CSR, for sm_100a.
+//
+// Semantics: DSL staticDSLCodes/PageRankDSLV3:1-25 as emitted by the CUDA generator
+// (backend_cuda/dsl_cpp_generator.cpp:1472-1480 reads d_src = srcList, count_outNbrs
+// :3113-3121): pr0 = 1/V; pr'[v] = (1-delta)/V + delta * sum_{u->v} pr[u]/outdeg(u);
+// diff = sum |pr' - pr|; repeat while diff > beta && iter < maxIter.
+//
+// Design (one kernel launch per iteration, all iterations in one CUDA graph):
+//  * Every iteration writes contrib[v] = pr[v]/outdeg(v) next to pr[v], so the next
+//    gather reads one float per in-edge (the same per-edge quotient the reference
+//    forms in float).
+//  * Work is split into row-aligned tiles of at most 2048 merged items (rows + in-edges):
+//    a CTA of 256 threads stages the tile's srcList slice and gathers contrib into
+//    shared memory with coalesced loads, then walks a merge path (8 items per thread)
+//    with a block-wide segmented scan, so row lengths never unbalance threads.
+//    Sums are accumulated in FP64 and rounded once to FP32.
+//  * Rows with more than 2047 in-edges are split into 2048-edge chunks; the CTA that
+//    finishes a row's last chunk (arrival counter) adds the chunk partials in chunk
+//    order — deterministic, no float atomics.
+//  * The L1 diff is reduced per CTA and summed in CTA order by the last CTA to
+//    finish, which also advances the iteration count and raises the done flag; later
+//    launches in the graph see the flag and return at once.
+#include <algorithm>
+#include <vector>
+
+#include "sp_internal.cuh"
+
+namespace sp {
+
+namespace pr {
+constexpr int THREADS = 256;
+constexpr int IPT = 8;                  // merged items per thread
+constexpr int CAP = THREADS * IPT;      // items per short tile
+constexpr int CHUNK = THREADS * IPT;    // edges per long-row chunk
+constexpr int LONG_DEG = CAP - 1;       // rows above this are chunked
+
+struct State {
+  int iter;
+  int done;
+  unsigned int ticket;
+  int pad;
+  double diff;
+};
+}  // namespace pr
+
+struct PrPlan {
+  int n_short = 0, n_chunks = 0, n_long = 0;
+  dbuf<int2> tiles;       // [n_short] row ranges
+  dbuf<int4> chunks;      // [n_chunks] {row, e_begin, e_end, long index}
+  dbuf<int2> longs;       // [n_long] {first chunk, chunk count}
+  dbuf<unsigned int> long_ctr;
+  dbuf<double> chunk_part;
+  dbuf<double> diff_part;
+  dbuf<float> prb[2], con[2];
+  dbuf<pr::State> state;
+  dbuf<int32_t> outdeg;   // plain variant
+  cudaGraphExec_t exec = nullptr;
+  int exec_iters = 0;
+  float exec_beta = -1, exec_delta = -1;
+  cudaStream_t exec_stream = nullptr;
+};
+
+void free_pr_plan(PrPlan* p) {
+  if (!p) return;
+  if (p->exec) cudaGraphExecDestroy(p->exec);
+  p->tiles.release();
+  p->chunks.release();
+  p->longs.release();
+  p->long_ctr.release();
+  p->chunk_part.release();
+  p->diff_part.release();
+  for (int i = 0; i < 2; ++i) {
+    p->prb[i].release();
+    p->con[i].release();
+  }
+  p->state.release();
+  p->outdeg.release();
+  delete p;
+}
+
+namespace pr {
+
+struct IterArgs {
+  const int32_t* __restrict__ roff;
+  const int32_t* __restrict__ radj;
+  const int32_t* __restrict__ off;
+  const int2* __restrict__ tiles;
+  const int4* __restrict__ chunks;
+  const int2* __restrict__ longs;
+  unsigned int* long_ctr;
+  double* chunk_part;
+  double* diff_part;
+  State* st;
+  int n_short;
+  int n_total;  // n_short + n_chunks
+  float base;   // (1 - delta) / V, in float as the DSL computes it
+  float delta;
+  double beta;
+  int max_iter;
+};
+
+__device__ __forceinline__ double finalize_row(const IterArgs& a, int r, double sum,
+                                               const float* __restrict__ pr_old, float* __restrict__ pr_new,
+                                               float* __restrict__ con_new) {
+  float s = (float)sum;
+  float np = __fadd_rn(a.base, __fmul_rn(a.delta, s));
+  float po = pr_old[r];
+  pr_new[r] = np;
+  int od = a.off[r + 1] - a.off[r];
+  con_new[r] = od > 0 ? __fdiv_rn(np, (float)od) : 0.0f;
+  return fabs((double)np - (double)po);
+}
+
+// Number of row-end items among the first `diag` merged items of a tile
+// (row-end i comes after edge s_end[i]-1 and before edge s_end[i]).
+__device__ __forceinline__ int merge_search(int diag, const int* s_end, int nrows, int nedges) {
+  int lo = max(diag - nedges, 0), hi = min(diag, nrows);
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (s_end[mid] <= diag - mid - 1)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(THREADS) k_iter(IterArgs a, const float* __restrict__ pr_old,
+                                                  const float* __restrict__ con_old, float* __restrict__ pr_new,
+                                                  float* __restrict__ con_new) {
+  __shared__ float s_val[CAP];
+  __shared__ int s_end[CAP];
+  __shared__ double s_red[THREADS / 32];
+  __shared__ double s_wv[THREADS / 32];
+  __shared__ int s_wf[THREADS / 32];
+  __shared__ int s_last;
+  if (a.st->done) return;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, wid = tid >> 5;
+  double my_diff = 0;
+
+  if ((int)blockIdx.x < a.n_short) {
+    const int2 t = a.tiles[blockIdx.x];
+    const int rb = t.x, re = t.y;
+    const int eb = a.roff[rb];
+    const int ee = a.roff[re];
+    const int nrows = re - rb, nedges = ee - eb, total = nrows + nedges;
+    for (int i = tid; i < nrows; i += THREADS) s_end[i] = a.roff[rb + i + 1] - eb;
+    {
+      int idx[IPT];
+#pragma unroll
+      for (int k = 0; k < IPT; ++k) {
+        int j = tid + k * THREADS;
+        idx[k] = j < nedges ? __ldg(a.radj + eb + j) : -1;
+      }
+      float v[IPT];
+#pragma unroll
+      for (int k = 0; k < IPT; ++k) v[k] = idx[k] >= 0 ? __ldg(con_old + idx[k]) : 0.0f;
+#pragma unroll
+      for (int k = 0; k < IPT; ++k) {
+        int j = tid + k * THREADS;
+        if (j < nedges) s_val[j] = v[k];
+      }
+    }
+    __syncthreads();
+    const int d0 = min(tid * IPT, total);
+    const int d1 = min(d0 + IPT, total);
+    const int x0 = merge_search(d0, s_end, nrows, nedges);
+    const int y0 = d0 - x0;
+    // pass 1: partial of the row left open at the end of this thread's items
+    double acc = 0;
+    int has_end = 0;
+    {
+      int x = x0, y = y0;
+      for (int d = d0; d < d1; ++d) {
+        if (y < s_end[x]) {
+          acc += (double)s_val[y];
+          ++y;
+        } else {
+          has_end = 1;
+          acc = 0;
+          ++x;
+        }
+      }
+    }
+    // block-wide exclusive segmented scan of (has_end, acc): carry into this thread
+    int f = has_end;
+    double v = acc;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int fu = __shfl_up_sync(0xffffffffu, f, o);
+      double vu = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) {
+        if (!f) v += vu;
+        f |= fu;
+      }
+    }
+    if (lane == 31) {
+      s_wf[wid] = f;
+      s_wv[wid] = v;
+    }
+    __syncthreads();
+    // exclusive prefix over warps (fixed order)
+    double pv = 0;
+    for (int w = 0; w < wid; ++w) {
+      if (s_wf[w]) {
+        pv = s_wv[w];
+      } else {
+        pv += s_wv[w];
+      }
+    }
+    int ef = __shfl_up_sync(0xffffffffu, f, 1);
+    double ev = __shfl_up_sync(0xffffffffu, v, 1);
+    double carry;
+    if (lane == 0)
+      carry = pv;
+    else
+      carry = ef ? ev : pv + ev;
+    // pass 2: finalize rows whose end item is in this thread
+    {
+      int x = x0, y = y0;
+      double s = carry;
+      for (int d = d0; d < d1; ++d) {
+        if (y < s_end[x]) {
+          s += (double)s_val[y];
+          ++y;
+        } else {
+          my_diff += finalize_row(a, rb + x, s, pr_old, pr_new, con_new);
+          s = 0;
+          ++x;
+        }
+      }
+    }
+  } else if ((int)blockIdx.x < a.n_total) {
+    const int ci = blockIdx.x - a.n_short;
+    const int4 c = a.chunks[ci];
+    double acc = 0;
+    {
+      int idx[IPT];
+#pragma unroll
+      for (int k = 0; k < IPT; ++k) {
+        int e = c.y + tid + k * THREADS;
+        idx[k] = e < c.z ? __ldg(a.radj + e) : -1;
+      }
+#pragma unroll
+      for (int k = 0; k < IPT; ++k)
+        if (idx[k] >= 0) acc += (double)__ldg(con_old + idx[k]);
+    }
+    double tot = block_sum<THREADS>(acc, s_red);
+    if (tid == 0) {
+      a.chunk_part[ci] = tot;
+      __threadfence();
+      const int2 L = a.longs[c.w];
+      unsigned int old = atomicAdd(&a.long_ctr[c.w], 1u);
+      s_last = (old == (unsigned)(L.y - 1));
+    }
+    __syncthreads();
+    if (s_last && tid == 0) {
+      __threadfence();
+      const int2 L = a.longs[c.w];
+      double sum = 0;
+      const volatile double* cp = a.chunk_part;
+      for (int k = 0; k < L.y; ++k) sum += cp[L.x + k];
+      my_diff += finalize_row(a, c.x, sum, pr_old, pr_new, con_new);
+      a.long_ctr[c.w] = 0;
+    }
+  }
+
+  // per-CTA diff partial, then the last CTA reduces them in CTA order
+  double bd = block_sum<THREADS>(my_diff, s_red);
+  if (tid == 0) {
+    a.diff_part[blockIdx.x] = bd;
+    __threadfence();
+    unsigned int t = atomicAdd(&a.st->ticket, 1u);
+    s_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    const volatile double* dp = a.diff_part;
+    double p = 0;
+    for (int i = tid; i < (int)gridDim.x; i += THREADS) p += dp[i];
+    double total = block_sum<THREADS>(p, s_red);
+    if (tid == 0) {
+      int it = a.st->iter + 1;
+      a.st->iter = it;
+      a.st->diff = total;
+      a.st->done = (total > a.beta && it < a.max_iter) ? 0 : 1;
+      a.st->ticket = 0;
+    }
+  }
+}
+
+__global__ void k_init(int V, const int32_t* __restrict__ off, float* __restrict__ pr, float* __restrict__ con,
+                       State* st) {
+  const float numNodes = (float)V;
+  const float p0 = 1.0f / numNodes;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    pr[v] = p0;
+    int od = off[v + 1] - off[v];
+    con[v] = od > 0 ? __fdiv_rn(p0, (float)od) : 0.0f;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->iter = 0;
+    st->done = 0;
+    st->ticket = 0;
+    st->diff = 0;
+  }
+}
+
+// ---- plain variant: the generated CUDA form (one thread per vertex, serial gather
+// of pr[u]/outdeg(u), atomic float diff; backend_cuda/dsl_cpp_generator.cpp:1682-1761)
+__global__ void k_plain_iter(int V, const int32_t* __restrict__ off, const int32_t* __restrict__ roff,
+                             const int32_t* __restrict__ radj, const float* __restrict__ pr,
+                             float* __restrict__ prn, float base, float delta, float* diff) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= V) return;
+  float sum = 0.0f;
+  for (int e = roff[v]; e < roff[v + 1]; ++e) {
+    int u = radj[e];
+    sum = sum + pr[u] / (float)(off[u + 1] - off[u]);
+  }
+  float np = base + delta * sum;
+  atomicAdd(diff, fabsf(np - pr[v]));
+  prn[v] = np;
+}
+
+__global__ void k_plain_init(int V, float* pr) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < V) pr[v] = 1.0f / (float)V;
+}
+
+}  // namespace pr
+
+static int build_pr_plan(sp_graph* g) {
+  if (g->pr) return SP_OK;
+  SP_TRY(ensure_reverse(g));
+  const int V = g->V;
+  std::vector<int32_t> roff(V + 1);
+  SP_CHECK_CUDA(cudaMemcpyAsync(roff.data(), g->roff.p, sizeof(int32_t) * (V + 1), cudaMemcpyDeviceToHost, g->stream));
+  SP_CHECK_CUDA(cudaStreamSynchronize(g->stream));
+  std::vector<int2> tiles;
+  std::vector<int4> chunks;
+  std::vector<int2> longs;
+  int r = 0;
+  while (r < V) {
+    int deg = roff[r + 1] - roff[r];
+    if (deg > pr::LONG_DEG) {
+      int first = (int)chunks.size();
+      for (int e = roff[r]; e < roff[r + 1]; e += pr::CHUNK)
+        chunks.push_back(make_int4(r, e, std::min(e + pr::CHUNK, roff[r + 1]), (int)longs.size()));
+      longs.push_back(make_int2(first, (int)chunks.size() - first));
+      ++r;
+      continue;
+    }
+    int start = r, items = 0;
+    while (r < V) {
+      int d = roff[r + 1] - roff[r];
+      if (d > pr::LONG_DEG || items + 1 + d > pr::CAP) break;
+      items += 1 + d;
+      ++r;
+    }
+    tiles.push_back(make_int2(start, r));
+  }
+  PrPlan* p = new PrPlan();
+  p->n_short = (int)tiles.size();
+  p->n_chunks = (int)chunks.size();
+  p->n_long = (int)longs.size();
+  int st;
+  auto fail = [&](int s) {
+    free_pr_plan(p);
+    return s;
+  };
+  if ((st = p->tiles.alloc(std::max(1, p->n_short))) || (st = p->chunks.alloc(std::max(1, p->n_chunks))) ||
+      (st = p->longs.alloc(std::max(1, p->n_long))) || (st = p->long_ctr.alloc(std::max(1, p->n_long))) ||
+      (st = p->chunk_part.alloc(std::max(1, p->n_chunks))) ||
+      (st = p->diff_part.alloc(std::max(1, p->n_short + p->n_chunks))) || (st = p->state.alloc(1)))
+    return fail(st);
+  for (int i = 0; i < 2; ++i)
+    if ((st = p->prb[i].alloc(V)) || (st = p->con[i].alloc(V))) return fail(st);
+  cudaStream_t s = g->stream;
+  if (p->n_short)
+    SP_CHECK_CUDA(cudaMemcpyAsync(p->tiles.p, tiles.data(), sizeof(int2) * p->n_short, cudaMemcpyHostToDevice, s));
+  if (p->n_chunks)
+    SP_CHECK_CUDA(cudaMemcpyAsync(p->chunks.p, chunks.data(), sizeof(int4) * p->n_chunks, cudaMemcpyHostToDevice, s));
+  if (p->n_long)
+    SP_CHECK_CUDA(cudaMemcpyAsync(p->longs.p, longs.data(), sizeof(int2) * p->n_long, cudaMemcpyHostToDevice, s));
+  SP_CHECK_CUDA(cudaMemsetAsync(p->long_ctr.p, 0, sizeof(unsigned int) * std::max(1, p->n_long), s));
+  SP_CHECK_CUDA(cudaStreamSynchronize(s));
+  g->pr = p;
+  return SP_OK;
+}
+
+static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float* out, int32_t* iters,
+                    double* fdiff) {
+  SP_TRY(build_pr_plan(g));
+  PrPlan* p = g->pr;
+  cudaStream_t s = g->stream;
+  const int V = g->V;
+  const int n_iter = std::max(1, (int)maxIter);
+  pr::IterArgs a;
+  a.roff = g->roff.p;
+  a.radj = g->radj.p;
+  a.off = g->off.p;
+  a.tiles = p->tiles.p;
+  a.chunks = p->chunks.p;
+  a.longs = p->longs.p;
+  a.long_ctr = p->long_ctr.p;
+  a.chunk_part = p->chunk_part.p;
+  a.diff_part = p->diff_part.p;
+  a.st = p->state.p;
+  a.n_short = p->n_short;
+  a.n_total = p->n_short + p->n_chunks;
+  a.delta = delta;
+  a.base = (1.0f - delta) / (float)V;
+  a.beta = (double)beta;
+  a.max_iter = n_iter;
+  const int grid = std::max(1, a.n_total);
+
+  pr::k_init<<<num_sms() * 4, 256, 0, s>>>(V, g->off.p, p->prb[0].p, p->con[0].p, p->state.p);
+  SP_CHECK_LAUNCH();
+  if (!(p->exec && p->exec_iters == n_iter && p->exec_beta == beta && p->exec_delta == delta && p->exec_stream == s)) {
+    if (p->exec) {
+      cudaGraphExecDestroy(p->exec);
+      p->exec = nullptr;
+    }
+    cudaGraph_t graph;
+    SP_CHECK_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < n_iter; ++k) {
+      int c = k & 1, n = c ^ 1;
+      pr::k_iter<<<grid, pr::THREADS, 0, s>>>(a, p->prb[c].p, p->con[c].p, p->prb[n].p, p->con[n].p);
+    }
+    cudaError_t ce = cudaStreamEndCapture(s, &graph);
+    if (ce != cudaSuccess) {
+      set_error("pagerank graph capture: %s", cudaGetErrorString(ce));
+      return SP_ERR_CUDA;
+    }
+    ce = cudaGraphInstantiate(&p->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) {
+      p->exec = nullptr;
+      set_error("pagerank graph instantiate: %s", cudaGetErrorString(ce));
+      return SP_ERR_CUDA;
+    }
+    p->exec_iters = n_iter;
+    p->exec_beta = beta;
+    p->exec_delta = delta;
+    p->exec_stream = s;
+  }
+  SP_CHECK_CUDA(cudaGraphLaunch(p->exec, s));
+  g_launches.fetch_add(n_iter);
+  pr::State hs;
+  SP_TRY(copy_out(&hs, p->state.p, sizeof(hs), s));
+  if (out) SP_TRY(copy_out(out, p->prb[hs.iter & 1].p, sizeof(float) * V, s));
+  if (iters) *iters = hs.iter;
+  if (fdiff) *fdiff = hs.diff;
+  return SP_OK;
+}
+
+static int pr_plain(sp_graph* g, float beta, float delta, int32_t maxIter, float* out, int32_t* iters,
+                    double* fdiff) {
+  SP_TRY(ensure_reverse(g));
+  SP_TRY(build_pr_plan(g));
+  PrPlan* p = g->pr;
+  cudaStream_t s = g->stream;
+  const int V = g->V;
+  dbuf<float> d_diff;
+  SP_TRY(d_diff.alloc(1));
+  const int tb = 512;  // the generator's launch shape (backend_cuda/dsl_cpp_generator.cpp:56-77)
+  const int nb = (V + tb - 1) / tb;
+  pr::k_plain_init<<<nb, tb, 0, s>>>(V, p->prb[0].p);
+  SP_CHECK_LAUNCH();
+  const float base = (1.0f - delta) / (float)V;
+  int it = 0;
+  float diff = 0;
+  int cur = 0;
+  do {
+    SP_CHECK_CUDA(cudaMemsetAsync(d_diff.p, 0, sizeof(float), s));
+    pr::k_plain_iter<<<nb, tb, 0, s>>>(V, g->off.p, g->roff.p, g->radj.p, p->prb[cur].p, p->prb[cur ^ 1].p, base,
+                                        delta, d_diff.p);
+    SP_CHECK_LAUNCH();
+    SP_TRY(copy_out(&diff, d_diff.p, sizeof(float), s));
+    cur ^= 1;
+    ++it;
+  } while (diff > beta && it < maxIter);
+  if (out) SP_TRY(copy_out(out, p->prb[cur].p, sizeof(float) * V, s));
+  if (iters) *iters = it;
+  if (fdiff) *fdiff = diff;
+  return SP_OK;
+}
+
+}  // namespace sp
+
+extern "C" int sp_pagerank(sp_graph_h g, float beta, float delta, int32_t maxIter, float* pageRank,
+                           int32_t* iterations, double* final_diff, int32_t variant) {
+  if (!g) {
+    sp::set_error("sp_pagerank: NULL graph");
+    return SP_ERR_INVALID;
+  }
+  if (variant == SP_PR_PLAIN) return sp::pr_plain(g, beta, delta, maxIter, pageRank, iterations, final_diff);
+  if (variant != SP_PR_TUNED) {
+    sp::set_error("sp_pagerank: unknown variant %d", variant);
+    return SP_ERR_INVALID;
+  }
+  return sp::pr_tuned(g, beta, delta, maxIter, pageRank, iterations, final_diff);
+}

@@ -1,0 +1,343 @@
+// Triangle counting for sm_100a.
+//
+// Semantics: DSL staticDSLCodes/triangle_counting_dsl:1-13 as emitted by the OpenMP
+// generator (backend_omp/dsl_cpp_generator.cpp:988-1015, 1277-1299, 2485-2494):
+//   count = sum_v sum_{u in N(v), u<v} sum_{w in N(v), w>v} [u->w in E]
+// The reference's GPU form tests u->w by binary search (libcuda.cuh:187-212
+// findNeighborSorted) from one thread per vertex.
+//
+// Both paths here are "anchor" loops run by one warp per anchor vertex a:
+//   S(a)  = a set staged in a shared-memory hash table (one per warp),
+//   P(a)  = probe vertices; for each p in P(a) a probe list L(p) is streamed
+//           with all 32 lanes (the (p, element) pairs are flattened across the warp
+//           with a prefix sum, so list lengths never idle lanes), and each element
+//           is looked up in S(a).
+//  * undirected graph (forward CSR == reverse CSR): degree-ordered orientation
+//    E+ = {(u,v): (deg u, u) < (deg v, v)}; a = u, S = P = N+(u), L(v) = N+(v).
+//    Each triangle is counted once, which equals the formula on a symmetric graph.
+//  * any other graph: the formula literally; a = v, S = N(v) ∩ (v, inf),
+//    P = N(v) ∩ [0, v), L(u) = N(u) ∩ (v, inf).
+// Anchors whose S does not fit the warp table are counted afterwards by whole CTAs
+// with binary search in the sorted global list.
+#include <cub/cub.cuh>
+
+#include "sp_internal.cuh"
+
+namespace sp {
+
+namespace tc {
+constexpr int THREADS = 256;
+constexpr int WARPS = THREADS / 32;
+constexpr int HCAP = 1024;          // hash slots per warp (load factor <= 1/2)
+constexpr int SMAX = HCAP / 2;      // largest S(a) handled by the warp path
+constexpr int EMPTY = -1;
+
+__device__ __forceinline__ unsigned hslot(int k) { return ((unsigned)k * 2654435761u) >> 22; }  // 10 bits
+
+struct Lists {
+  // undirected: o_off/o_adj = oriented CSR; directed: off/adj = forward CSR
+  const int32_t* __restrict__ off;
+  const int32_t* __restrict__ adj;
+  int V;
+  int directed;
+};
+
+// S and P ranges of anchor a (as index ranges into adj).
+__device__ __forceinline__ void anchor_ranges(const Lists& L, int a, int& sb, int& se, int& pb, int& pe) {
+  int b = L.off[a], e = L.off[a + 1];
+  if (!L.directed) {
+    sb = pb = b;
+    se = pe = e;
+  } else {
+    // first index with adj > a
+    int lo = b, hi = e;
+    while (lo < hi) {
+      int m = (lo + hi) >> 1;
+      if (L.adj[m] <= a) lo = m + 1; else hi = m;
+    }
+    int hi_start = lo;
+    // first index with adj >= a
+    lo = b;
+    hi = hi_start;
+    while (lo < hi) {
+      int m = (lo + hi) >> 1;
+      if (L.adj[m] < a) lo = m + 1; else hi = m;
+    }
+    pb = b;
+    pe = lo;
+    sb = hi_start;
+    se = e;
+  }
+}
+
+// Probe list of p for anchor a.
+__device__ __forceinline__ void probe_range(const Lists& L, int a, int p, int& lb, int& le) {
+  int b = L.off[p], e = L.off[p + 1];
+  if (L.directed) {
+    int lo = b, hi = e;
+    while (lo < hi) {
+      int m = (lo + hi) >> 1;
+      if (L.adj[m] <= a) lo = m + 1; else hi = m;
+    }
+    b = lo;
+  }
+  lb = b;
+  le = e;
+}
+
+__global__ void __launch_bounds__(THREADS) k_tc_warp(Lists L, unsigned int* __restrict__ next_anchor,
+                                                     int* __restrict__ heavy, unsigned int* __restrict__ n_heavy,
+                                                     unsigned long long* __restrict__ total) {
+  __shared__ int s_tab[WARPS][HCAP];
+  __shared__ short s_slot[WARPS][SMAX];
+  __shared__ int s_lb[WARPS][32];
+  __shared__ int s_excl[WARPS][32];
+  const int lane = lane_id(), w = warp_id();
+  int* tab = s_tab[w];
+  for (int i = lane; i < HCAP; i += 32) tab[i] = EMPTY;
+  __syncwarp();
+  unsigned long long cnt = 0;
+  while (true) {
+    unsigned int a = 0;
+    if (lane == 0) a = atomicAdd(next_anchor, 1u);
+    a = __shfl_sync(0xffffffffu, a, 0);
+    if (a >= (unsigned)L.V) break;
+    int sb, se, pb, pe;
+    anchor_ranges(L, (int)a, sb, se, pb, pe);
+    const int ns = se - sb, np = pe - pb;
+    if (ns == 0 || np == 0) continue;
+    if (ns > SMAX) {
+      if (lane == 0) heavy[atomicAdd(n_heavy, 1u)] = (int)a;
+      continue;
+    }
+    // insert S(a)
+    for (int i = lane; i < ns; i += 32) {
+      int k = L.adj[sb + i];
+      unsigned s = hslot(k);
+      for (int probe = 0; probe < HCAP; ++probe) {
+        int prev = atomicCAS(&tab[s], EMPTY, k);
+        if (prev == EMPTY || prev == k) break;
+        s = (s + 1) & (HCAP - 1);
+      }
+      s_slot[w][i] = (short)s;
+    }
+    __syncwarp();
+    // probe lists of P(a), 32 probe vertices at a time
+    for (int g0 = 0; g0 < np; g0 += 32) {
+      int p = g0 + lane < np ? L.adj[pb + g0 + lane] : -1;
+      int lb = 0, le = 0;
+      if (p >= 0) probe_range(L, (int)a, p, lb, le);
+      int len = le - lb;
+      int incl = len;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      int tot = __shfl_sync(0xffffffffu, incl, 31);
+      s_lb[w][lane] = lb;
+      s_excl[w][lane] = incl - len;
+      __syncwarp();
+      for (int k = lane; k < tot; k += 32) {
+        // owner: last lane whose exclusive prefix <= k
+        int lo = 0, hi = 31;
+        while (lo < hi) {
+          int m = (lo + hi + 1) >> 1;
+          if (s_excl[w][m] <= k) lo = m; else hi = m - 1;
+        }
+        int x = L.adj[s_lb[w][lo] + (k - s_excl[w][lo])];
+        unsigned s = hslot(x);
+        for (int probe = 0; probe < HCAP; ++probe) {
+          int t = tab[s];
+          if (t == x) {
+            ++cnt;
+            break;
+          }
+          if (t == EMPTY) break;
+          s = (s + 1) & (HCAP - 1);
+        }
+      }
+      __syncwarp();
+    }
+    // clear the slots S(a) used
+    for (int i = lane; i < ns; i += 32) tab[s_slot[w][i]] = EMPTY;
+    __syncwarp();
+  }
+  cnt = warp_sum(cnt);
+  if (lane == 0 && cnt) atomicAdd(total, cnt);
+}
+
+// Heavy anchors: one CTA each, lookups by binary search in the sorted S(a).
+__global__ void __launch_bounds__(THREADS) k_tc_heavy(Lists L, const int* __restrict__ heavy,
+                                                      const unsigned int* __restrict__ n_heavy,
+                                                      unsigned long long* __restrict__ total) {
+  __shared__ int s_lb[THREADS];
+  __shared__ int s_excl[THREADS];
+  __shared__ int s_tot;
+  __shared__ unsigned long long s_red[WARPS];
+  const int nh = (int)*n_heavy;
+  unsigned long long cnt = 0;
+  for (int h = blockIdx.x; h < nh; h += gridDim.x) {
+    const int a = heavy[h];
+    int sb, se, pb, pe;
+    anchor_ranges(L, a, sb, se, pb, pe);
+    for (int g0 = pb; g0 < pe; g0 += THREADS) {
+      int p = g0 + (int)threadIdx.x < pe ? L.adj[g0 + threadIdx.x] : -1;
+      int lb = 0, le = 0;
+      if (p >= 0) probe_range(L, a, p, lb, le);
+      int len = le - lb;
+      // block exclusive scan of len
+      typedef cub::BlockScan<int, THREADS> Scan;
+      __shared__ typename Scan::TempStorage ts;
+      int excl, tot;
+      Scan(ts).ExclusiveSum(len, excl, tot);
+      s_lb[threadIdx.x] = lb;
+      s_excl[threadIdx.x] = excl;
+      if (threadIdx.x == 0) s_tot = tot;
+      __syncthreads();
+      for (int k = threadIdx.x; k < s_tot; k += THREADS) {
+        int lo = 0, hi = THREADS - 1;
+        while (lo < hi) {
+          int m = (lo + hi + 1) >> 1;
+          if (s_excl[m] <= k) lo = m; else hi = m - 1;
+        }
+        int x = L.adj[s_lb[lo] + (k - s_excl[lo])];
+        int l = sb, r = se;
+        while (l < r) {
+          int m = (l + r) >> 1;
+          if (L.adj[m] < x) l = m + 1; else r = m;
+        }
+        if (l < se && L.adj[l] == x) ++cnt;
+      }
+      __syncthreads();
+    }
+  }
+  cnt = block_sum<THREADS>(cnt, s_red);
+  if (threadIdx.x == 0 && cnt) atomicAdd(total, cnt);
+}
+
+// Orientation: keep v in N+(u) iff (deg u, u) < (deg v, v).
+__device__ __forceinline__ bool before(int du, int u, int dv, int v) { return du < dv || (du == dv && u < v); }
+
+__global__ void k_orient_count(const int32_t* __restrict__ off, const int32_t* __restrict__ adj, int V,
+                               int32_t* __restrict__ cnt) {
+  const int lane = threadIdx.x & 31;
+  for (int u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < V; u += (gridDim.x * blockDim.x) >> 5) {
+    const int b = off[u], e = off[u + 1], du = e - b;
+    int c = 0;
+    for (int i = b + lane; i < e; i += 32) {
+      int v = adj[i];
+      c += before(du, u, off[v + 1] - off[v], v);
+    }
+    c = warp_sum(c);
+    if (lane == 0) cnt[u] = c;
+  }
+}
+
+__global__ void k_orient_fill(const int32_t* __restrict__ off, const int32_t* __restrict__ adj, int V,
+                              const int32_t* __restrict__ ooff, int32_t* __restrict__ oadj) {
+  const int lane = threadIdx.x & 31;
+  for (int u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < V; u += (gridDim.x * blockDim.x) >> 5) {
+    const int b = off[u], e = off[u + 1], du = e - b;
+    int pos = ooff[u];
+    for (int i0 = b; i0 < e; i0 += 32) {
+      int i = i0 + lane;
+      bool keep = false;
+      int v = 0;
+      if (i < e) {
+        v = adj[i];
+        keep = before(du, u, off[v + 1] - off[v], v);
+      }
+      unsigned m = __ballot_sync(0xffffffffu, keep);
+      if (keep) oadj[pos + __popc(m & ((1u << lane) - 1))] = v;
+      pos += __popc(m);
+    }
+  }
+}
+
+}  // namespace tc
+
+struct TcPlan {
+  dbuf<int32_t> ooff, oadj;  // oriented CSR (undirected graphs)
+  dbuf<int> heavy;
+  dbuf<unsigned int> ctr;    // [0] next anchor, [1] heavy count
+  dbuf<unsigned long long> total;
+  bool oriented = false;
+};
+
+void free_tc_plan(TcPlan* p) {
+  if (!p) return;
+  p->ooff.release();
+  p->oadj.release();
+  p->heavy.release();
+  p->ctr.release();
+  p->total.release();
+  delete p;
+}
+
+static int build_tc_plan(sp_graph* g) {
+  if (g->tc) return SP_OK;
+  SP_TRY(ensure_symmetry(g));
+  TcPlan* p = new TcPlan();
+  cudaStream_t s = g->stream;
+  auto fail = [&](int st) {
+    free_tc_plan(p);
+    return st;
+  };
+  int st;
+  if ((st = p->heavy.alloc(g->V)) || (st = p->ctr.alloc(2)) || (st = p->total.alloc(1))) return fail(st);
+  if (g->symmetric == 1) {
+    if ((st = p->ooff.alloc(g->V + 1))) return fail(st);
+    dbuf<int32_t> cnt;
+    if ((st = cnt.alloc(g->V + 1))) return fail(st);
+    cudaMemsetAsync(cnt.p + g->V, 0, sizeof(int32_t), s);
+    tc::k_orient_count<<<num_sms() * 8, 256, 0, s>>>(g->off.p, g->adj.p, g->V, cnt.p);
+    g_launches++;
+    size_t tb = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt.p, p->ooff.p, g->V + 1, s);
+    dbuf<unsigned char> tmp;
+    if ((st = tmp.alloc(tb))) return fail(st);
+    cub::DeviceScan::ExclusiveSum(tmp.p, tb, cnt.p, p->ooff.p, g->V + 1, s);
+    g_launches++;
+    int32_t eplus = 0;
+    if ((st = copy_out(&eplus, p->ooff.p + g->V, sizeof(int32_t), s))) return fail(st);
+    if ((st = p->oadj.alloc(eplus))) return fail(st);
+    tc::k_orient_fill<<<num_sms() * 8, 256, 0, s>>>(g->off.p, g->adj.p, g->V, p->ooff.p, p->oadj.p);
+    g_launches++;
+    if (cudaStreamSynchronize(s) != cudaSuccess) {
+      set_error("tc orientation: %s", cudaGetErrorString(cudaGetLastError()));
+      return fail(SP_ERR_CUDA);
+    }
+    p->oriented = true;
+  }
+  g->tc = p;
+  return SP_OK;
+}
+
+}  // namespace sp
+
+extern "C" int sp_tc(sp_graph_h g, int64_t* triangle_count) {
+  using namespace sp;
+  if (!g || !triangle_count) {
+    set_error("sp_tc: NULL argument");
+    return SP_ERR_INVALID;
+  }
+  SP_TRY(build_tc_plan(g));
+  TcPlan* p = g->tc;
+  cudaStream_t s = g->stream;
+  tc::Lists L;
+  L.V = g->V;
+  L.directed = p->oriented ? 0 : 1;
+  L.off = p->oriented ? p->ooff.p : g->off.p;
+  L.adj = p->oriented ? p->oadj.p : g->adj.p;
+  SP_CHECK_CUDA(cudaMemsetAsync(p->ctr.p, 0, sizeof(unsigned int) * 2, s));
+  SP_CHECK_CUDA(cudaMemsetAsync(p->total.p, 0, sizeof(unsigned long long), s));
+  tc::k_tc_warp<<<num_sms() * 4, tc::THREADS, 0, s>>>(L, p->ctr.p, p->heavy.p, p->ctr.p + 1, p->total.p);
+  SP_CHECK_LAUNCH();
+  tc::k_tc_heavy<<<num_sms() * 2, tc::THREADS, 0, s>>>(L, p->heavy.p, p->ctr.p + 1, p->total.p);
+  SP_CHECK_LAUNCH();
+  unsigned long long h = 0;
+  SP_TRY(copy_out(&h, p->total.p, sizeof(h), s));
+  *triangle_count = (int64_t)h;
+  return SP_OK;
+}

@@ -1,0 +1,119 @@
+"""Device mirror of a CSR graph and the algorithm entry points.
+
+``DeviceGraph`` owns an ``sp_graph_h`` from the C ABI: the forward CSR (and the
+reverse CSR / weights when given) uploaded once and reused by every algorithm
+call, replacing the per-call host-to-device copy of StarPlat's generated CUDA
+code (backend_cuda/dsl_cpp_generator.cpp:4104-4297).
+
+Arrays passed in may be numpy arrays (host) or CUDA tensors (device); outputs
+are written to caller-provided arrays of either kind.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib
+from .graph import CSRGraph
+
+
+def _ptr(a) -> Optional[int]:
+    """Data pointer of a numpy array or a torch tensor (None for None)."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("array must be C-contiguous")
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        if not a.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        return a.data_ptr()
+    raise TypeError(f"unsupported array type {type(a)}")
+
+
+def _is_device(a) -> bool:
+    return hasattr(a, "is_cuda") and bool(a.is_cuda)
+
+
+class DeviceGraph:
+    """A graph resident in GPU memory (the C ABI's sp_graph_h)."""
+
+    def __init__(self, indexofNodes, edgeList, edgeLen=None, rev_indexofNodes=None, srcList=None):
+        dev = _is_device(indexofNodes)
+        arrs = [indexofNodes, edgeList, edgeLen, rev_indexofNodes, srcList]
+        for a in arrs:
+            if a is not None and _is_device(a) != dev:
+                raise ValueError("mix of host and device arrays")
+            if a is not None:
+                dt = a.dtype
+                if str(dt) not in ("int32", "torch.int32"):
+                    raise TypeError(f"CSR arrays must be int32, got {dt}")
+        V = int(indexofNodes.shape[0]) - 1
+        E = int(edgeList.shape[0])
+        h = ctypes.c_void_p()
+        flags = _lib.SP_GRAPH_DEVICE_PTRS if dev else 0
+        check("sp_graph_create", lib().sp_graph_create(V, E, *[_ptr(a) for a in arrs], flags, ctypes.byref(h)))
+        self._h = h
+        self.V = V
+        self.E = E
+        self._keep = arrs if dev else None
+
+    @classmethod
+    def from_csr(cls, g: CSRGraph, with_reverse: bool = True, with_weights: bool = True) -> "DeviceGraph":
+        return cls(g.indexofNodes, g.edgeList, g.edgeLen if with_weights else None,
+                   g.rev_indexofNodes if with_reverse else None, g.srcList if with_reverse else None)
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise RuntimeError("graph already freed")
+        return self._h
+
+    def free(self) -> None:
+        if getattr(self, "_h", None) is not None:
+            lib().sp_graph_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.free()
+
+    def set_stream(self, stream) -> None:
+        """Run later work on this CUDA stream (torch.cuda.Stream or raw cudaStream_t int)."""
+        raw = getattr(stream, "cuda_stream", stream)
+        check("sp_graph_set_stream", lib().sp_graph_set_stream(self.handle, raw))
+
+    def info(self):
+        V = ctypes.c_int32()
+        E = ctypes.c_int64()
+        s = ctypes.c_int32()
+        check("sp_graph_info", lib().sp_graph_info(self.handle, ctypes.byref(V), ctypes.byref(E), ctypes.byref(s)))
+        return V.value, E.value, bool(s.value)
+
+    # ---------------------------------------------------------------- algorithms
+    def tc(self) -> int:
+        out = ctypes.c_int64()
+        check("sp_tc", lib().sp_tc(self.handle, ctypes.byref(out)))
+        return int(out.value)
+
+    def pagerank(self, beta: float = 1e-6, delta: float = 0.85, max_iter: int = 100, out=None,
+                 variant: int = _lib.SP_PR_TUNED):
+        if out is None:
+            out = np.empty(self.V, np.float32)
+        it = ctypes.c_int32()
+        diff = ctypes.c_double()
+        check("sp_pagerank", lib().sp_pagerank(self.handle, beta, delta, max_iter, _ptr(out), ctypes.byref(it),
+                                               ctypes.byref(diff), variant))
+        return out, int(it.value), float(diff.value)

@@ -1,0 +1,134 @@
+"""GPU parity: PageRank and triangle counting through the C ABI vs the oracle.
+
+Tolerances: triangle counts bit-exact; PageRank L1 < 1e-6 against the FP64
+oracle run for the same number of iterations (the iteration count itself must
+match the oracle's, or differ only when the FP64 diff sits within 1e-9 of beta).
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from starplat_b200 import _lib
+from starplat_b200.algorithms import ComputePageRank, Compute_TC, device_graph
+from starplat_b200.device import DeviceGraph
+from starplat_b200 import generators as G
+
+from graphs import directed_zoo, undirected_zoo
+
+pytestmark = pytest.mark.gpu
+
+
+def _pr_check(g, variant, beta=1e-6, delta=0.85, max_iter=100):
+    g.ensure_reverse()
+    dg = device_graph(g)
+    out, it, diff = dg.pagerank(beta, delta, max_iter, variant=variant)
+    ref, rit, rdiff = O.pagerank(g.indexofNodes, g.rev_indexofNodes, g.srcList, beta, delta, max_iter)
+    if it != rit:
+        # only acceptable when the convergence test is a near tie
+        _, _, d_at = O.pagerank(g.indexofNodes, g.rev_indexofNodes, g.srcList, beta, delta, max_iter,
+                                fixed_iters=min(it, rit))
+        assert abs(d_at - beta) < 1e-9, (it, rit, d_at)
+        ref, _, _ = O.pagerank(g.indexofNodes, g.rev_indexofNodes, g.srcList, beta, delta, max_iter,
+                               fixed_iters=it)
+    l1 = np.abs(out.astype(np.float64) - ref).sum()
+    assert l1 < 1e-6, (g.name, l1)
+    return it
+
+
+@pytest.mark.parametrize("gi", range(4))
+def test_pagerank_directed(gi):
+    g = directed_zoo()[gi]
+    _pr_check(g, _lib.SP_PR_TUNED)
+
+
+@pytest.mark.parametrize("gi", range(8))
+def test_pagerank_undirected(gi):
+    g = undirected_zoo()[gi]
+    _pr_check(g, _lib.SP_PR_TUNED)
+
+
+def test_pagerank_plain_variant():
+    g = directed_zoo()[1]
+    _pr_check(g, _lib.SP_PR_PLAIN)
+
+
+def test_pagerank_maxiter_and_beta():
+    g = directed_zoo()[0]
+    g.ensure_reverse()
+    dg = device_graph(g)
+    for max_iter in (1, 2, 7):
+        out, it, _ = dg.pagerank(0.0, 0.85, max_iter)
+        assert it == max_iter
+        ref, rit, _ = O.pagerank(g.indexofNodes, g.rev_indexofNodes, g.srcList, 0.0, 0.85, max_iter)
+        assert np.abs(out - ref).sum() < 1e-6
+    # maxIter <= 0 still runs the do-while body once
+    out, it, _ = dg.pagerank(1e-6, 0.85, 0)
+    assert it == 1
+    # different damping / threshold on the same mirror re-captures the graph
+    _pr_check(g, _lib.SP_PR_TUNED, beta=1e-4, delta=0.5)
+
+
+def test_pagerank_entry_point_and_device_output():
+    import torch
+
+    g = directed_zoo()[1]
+    g.ensure_reverse()
+    pr = np.zeros(g.V, np.float32)
+    ComputePageRank(g, 1e-6, 0.85, 100, pr)
+    ref, _, _ = O.pagerank(g.indexofNodes, g.rev_indexofNodes, g.srcList, 1e-6, 0.85, 100)
+    assert np.abs(pr - ref).sum() < 1e-6
+    # device-resident CSR and device output
+    t = [torch.from_numpy(a).cuda() for a in (g.indexofNodes, g.edgeList, g.rev_indexofNodes, g.srcList)]
+    with DeviceGraph(t[0], t[1], None, t[2], t[3]) as dg:
+        out = torch.empty(g.V, dtype=torch.float32, device="cuda")
+        dg.pagerank(1e-6, 0.85, 100, out=out)
+        assert np.abs(out.cpu().numpy() - ref).sum() < 1e-6
+
+
+def test_pagerank_reverse_built_on_device():
+    g = directed_zoo()[0]
+    with DeviceGraph(g.indexofNodes, g.edgeList) as dg:
+        out, it, _ = dg.pagerank(1e-6, 0.85, 100)
+    g.ensure_reverse()
+    ref, rit, _ = O.pagerank(g.indexofNodes, g.rev_indexofNodes, g.srcList, 1e-6, 0.85, 100)
+    assert it == rit and np.abs(out - ref).sum() < 1e-6
+
+
+@pytest.mark.parametrize("gi", range(8))
+def test_tc_undirected(gi):
+    g = undirected_zoo()[gi]
+    assert Compute_TC(g) == O.tc(g.indexofNodes, g.edgeList)
+
+
+@pytest.mark.parametrize("gi", range(4))
+def test_tc_directed(gi):
+    g = directed_zoo()[gi]
+    assert Compute_TC(g) == O.tc(g.indexofNodes, g.edgeList)
+
+
+def test_tc_heavy_anchor():
+    # a hub whose oriented / higher neighbour set exceeds the warp hash table
+    n = 2500
+    i, j = np.triu_indices(60, 1)
+    pairs = np.concatenate([np.stack([np.zeros(n - 1, np.int32), np.arange(1, n, dtype=np.int32)], 1),
+                            np.stack([i + 1, j + 1], 1).astype(np.int32)])
+    from graphs import from_pairs
+    for sym in (True, False):
+        g = from_pairs(n, pairs, symmetrize=sym)
+        assert Compute_TC(g) == O.tc(g.indexofNodes, g.edgeList)
+
+
+def test_tc_rmat16_config():
+    g = G.rmat(16, 16, seed=1)
+    assert Compute_TC(g) == O.tc(g.indexofNodes, g.edgeList)
+
+
+def test_invalid_csr_rejected():
+    off = np.array([0, 2, 1], np.int32)
+    adj = np.array([1, 0], np.int32)
+    with pytest.raises(_lib.SPError):
+        DeviceGraph(off, adj)
+    off = np.array([0, 2, 2], np.int32)
+    adj = np.array([1, 1], np.int32)  # duplicate
+    with pytest.raises(_lib.SPError):
+        DeviceGraph(off, adj)
