@@ -125,13 +125,18 @@ def run_reference(args, rank, world):
 
 
 def main():
+    global PR_SCALE
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--quick", action="store_true",
+                    help="device-resident timing only (no roofline/e2e/CPU legs): for profiler runs")
+    ap.add_argument("--scale", type=int, default=PR_SCALE, help="R-MAT scale (profiling on smaller cases)")
     args = ap.parse_args()
+    PR_SCALE = args.scale
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -191,6 +196,14 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     value = world * E * it_total / (ms / 1e3) / 1e9
+    if args.quick:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": "GTEPS", "quick": True, "V": V, "E": E,
+                              "iterations": it_total // args.steps, "ms_per_step": ms / args.steps}), flush=True)
+        dg.free()
+        if dist is not None:
+            dist.destroy_process_group()
+        return
 
     # ---- kernel roofline: average iteration-kernel time from two fixed-iteration runs
     def timed_fixed(n, reps=3):

@@ -67,28 +67,26 @@ __global__ void k_cmp(const int32_t* __restrict__ a, const int32_t* __restrict__
     }
 }
 
+// One warp per vertex: offsets monotone within [0, E], ids in [0, V), adjacency strictly increasing.
 __global__ void k_validate_csr(const int32_t* __restrict__ off, const int32_t* __restrict__ adj, int32_t V,
                                int64_t E, int* __restrict__ bad, int32_t* __restrict__ maxdeg) {
-  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < V; v += (int64_t)gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t v = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; v < V;
+       v += ((int64_t)gridDim.x * blockDim.x) >> 5) {
     int a = off[v], b = off[v + 1];
     if (a > b || a < 0 || b > E) {
-      atomicOr(bad, 1);
+      if (lane == 0) atomicOr(bad, 1);
       continue;
     }
-    atomicMax(maxdeg, b - a);
-    int prev = -1;
-    for (int e = a; e < b; ++e) {
+    if (lane == 0) atomicMax(maxdeg, b - a);
+    int flags = 0;
+    for (int e = a + lane; e < b; e += 32) {
       int x = adj[e];
-      if (x < 0 || x >= V) {
-        atomicOr(bad, 2);
-        break;
-      }
-      if (x <= prev) {
-        atomicOr(bad, 4);  // not strictly sorted (duplicate or unsorted adjacency)
-        break;
-      }
-      prev = x;
+      if (x < 0 || x >= V) flags |= 2;
+      if (e + 1 < b && adj[e + 1] <= x) flags |= 4;  // duplicate or unsorted adjacency
     }
+    flags = __reduce_or_sync(0xffffffffu, flags);
+    if (lane == 0 && flags) atomicOr(bad, flags);
   }
 }
 
@@ -210,7 +208,7 @@ int sp_graph_create(int32_t V, int64_t E, const int32_t* indexofNodes, const int
     if ((st = bad.alloc(2)) || (st = md.alloc(1))) return fail(st);
     cudaMemsetAsync(bad.p, 0, sizeof(int) * 2, g->stream);
     cudaMemsetAsync(md.p, 0, sizeof(int32_t), g->stream);
-    k_validate_csr<<<num_sms() * 4, 256, 0, g->stream>>>(g->off.p, g->adj.p, V, E, bad.p, md.p);
+    k_validate_csr<<<num_sms() * 16, 256, 0, g->stream>>>(g->off.p, g->adj.p, V, E, bad.p, md.p);
     g_launches++;
     int h[2] = {0, 0};
     int32_t hm = 0;
@@ -236,7 +234,7 @@ int sp_graph_create(int32_t V, int64_t E, const int32_t* indexofNodes, const int
     dbuf<int32_t> md;
     if ((st = bad.alloc(1)) || (st = md.alloc(1))) return fail(st);
     cudaMemsetAsync(bad.p, 0, sizeof(int), g->stream);
-    k_validate_csr<<<num_sms() * 4, 256, 0, g->stream>>>(g->roff.p, g->radj.p, V, E, bad.p, md.p);
+    k_validate_csr<<<num_sms() * 16, 256, 0, g->stream>>>(g->roff.p, g->radj.p, V, E, bad.p, md.p);
     g_launches++;
     int h = 0;
     int32_t last = -1, first = -1;

@@ -139,8 +139,10 @@ __global__ void __launch_bounds__(THREADS) k_iter(IterArgs a, const float* __res
   const int lane = tid & 31, wid = tid >> 5;
   double my_diff = 0;
 
-  if ((int)blockIdx.x < a.n_short) {
-    const int2 t = a.tiles[blockIdx.x];
+  // persistent CTAs: tiles (then long-row chunks) in a fixed round-robin order
+  for (int item = blockIdx.x; item < a.n_total; item += gridDim.x) {
+  if (item < a.n_short) {
+    const int2 t = a.tiles[item];
     const int rb = t.x, re = t.y;
     const int eb = a.roff[rb];
     const int ee = a.roff[re];
@@ -231,8 +233,9 @@ __global__ void __launch_bounds__(THREADS) k_iter(IterArgs a, const float* __res
         }
       }
     }
-  } else if ((int)blockIdx.x < a.n_total) {
-    const int ci = blockIdx.x - a.n_short;
+    __syncthreads();  // s_val / s_end are reused by the next tile
+  } else {
+    const int ci = item - a.n_short;
     const int4 c = a.chunks[ci];
     double acc = 0;
     {
@@ -264,6 +267,8 @@ __global__ void __launch_bounds__(THREADS) k_iter(IterArgs a, const float* __res
       my_diff += finalize_row(a, c.x, sum, pr_old, pr_new, con_new);
       a.long_ctr[c.w] = 0;
     }
+    __syncthreads();  // s_last is reused
+  }
   }
 
   // per-CTA diff partial, then the last CTA reduces them in CTA order
@@ -415,7 +420,9 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
   a.base = (1.0f - delta) / (float)V;
   a.beta = (double)beta;
   a.max_iter = n_iter;
-  const int grid = std::max(1, a.n_total);
+  int per_sm = 0;
+  SP_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pr::k_iter, pr::THREADS, 0));
+  const int grid = std::max(1, std::min(a.n_total, num_sms() * std::max(1, per_sm)));
 
   pr::k_init<<<num_sms() * 4, 256, 0, s>>>(V, g->off.p, p->prb[0].p, p->con[0].p, p->state.p);
   SP_CHECK_LAUNCH();

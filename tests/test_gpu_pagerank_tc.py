@@ -24,10 +24,19 @@ def _pr_check(g, variant, beta=1e-6, delta=0.85, max_iter=100):
     out, it, diff = dg.pagerank(beta, delta, max_iter, variant=variant)
     ref, rit, rdiff = O.pagerank(g.indexofNodes, g.rev_indexofNodes, g.srcList, beta, delta, max_iter)
     if it != rit:
-        # only acceptable when the convergence test is a near tie
-        _, _, d_at = O.pagerank(g.indexofNodes, g.rev_indexofNodes, g.srcList, beta, delta, max_iter,
-                                fixed_iters=min(it, rit))
-        assert abs(d_at - beta) < 1e-9, (it, rit, d_at)
+        # The stop test compares an L1 sum of FP32 rank changes with beta; near
+        # convergence each change is a few FP32 ulps, so that sum may sit a few
+        # percent away from the FP64 one. Accept a different stop only inside that
+        # window, then compare at the GPU's own iteration count.
+        assert abs(it - rit) <= 2, (it, rit)
+        _, _, d_gpu_stop = O.pagerank(g.indexofNodes, g.rev_indexofNodes, g.srcList, beta, delta, max_iter,
+                                      fixed_iters=it)
+        _, _, d_before = O.pagerank(g.indexofNodes, g.rev_indexofNodes, g.srcList, beta, delta, max_iter,
+                                    fixed_iters=max(1, it - 1))
+        if it < rit:
+            assert d_gpu_stop <= 1.1 * beta, (it, rit, d_gpu_stop)
+        else:
+            assert d_before >= 0.9 * beta, (it, rit, d_before)
         ref, _, _ = O.pagerank(g.indexofNodes, g.rev_indexofNodes, g.srcList, beta, delta, max_iter,
                                fixed_iters=it)
     l1 = np.abs(out.astype(np.float64) - ref).sum()
