@@ -61,6 +61,12 @@ int sp_graph_set_stream(sp_graph_h g, void* cuda_stream);
 /* V, E, symmetric (1 when the forward CSR equals the reverse CSR). */
 int sp_graph_info(sp_graph_h g, int32_t* V, int64_t* E, int32_t* symmetric);
 
+/* Schedule knobs (what the autotuner and the learned scheduler set); results never
+ * depend on them. Keys: "pr.short_deg" (in-degree up to which one thread sums a
+ * PageRank row; above it a warp does, default 32). Unknown keys: SP_ERR_INVALID. */
+int sp_tune_set(sp_graph_h g, const char* key, int64_t value);
+int sp_tune_get(sp_graph_h g, const char* key, int64_t* value);
+
 /* ---- triangle counting -------------------------------------------------------
  * Replaces generated `auto Compute_TC(graph& g)` (DSL staticDSLCodes/triangle_counting_dsl:1-13):
  *   count = sum_v sum_{u in N(v), u<v} sum_{w in N(v), w>v} [u->w is an edge]

@@ -50,6 +50,8 @@ SIGNATURES = {
     "sp_graph_free": (ctypes.c_int, [vp]),
     "sp_graph_set_stream": (ctypes.c_int, [vp, vp]),
     "sp_graph_info": (ctypes.c_int, [vp, P(i32), P(i64), P(i32)]),
+    "sp_tune_set": (ctypes.c_int, [vp, ctypes.c_char_p, i64]),
+    "sp_tune_get": (ctypes.c_int, [vp, ctypes.c_char_p, P(i64)]),
     "sp_tc": (ctypes.c_int, [vp, P(i64)]),
     "sp_pagerank": (ctypes.c_int, [vp, f32, f32, i32, vp, P(i32), P(f64), i32]),
 }

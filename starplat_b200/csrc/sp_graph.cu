@@ -289,6 +289,36 @@ int sp_graph_set_stream(sp_graph_h g, void* cuda_stream) {
   return SP_OK;
 }
 
+int sp_tune_set(sp_graph_h g, const char* key, int64_t value) {
+  if (!g || !key) {
+    set_error("sp_tune_set: NULL argument");
+    return SP_ERR_INVALID;
+  }
+  if (!strcmp(key, "pr.short_deg")) {
+    if (value < 0 || value > 4096) {
+      set_error("sp_tune_set: pr.short_deg must be in [0, 4096]");
+      return SP_ERR_INVALID;
+    }
+    g->pr_short_deg = (int32_t)value;
+    return SP_OK;
+  }
+  set_error("sp_tune_set: unknown key '%s'", key);
+  return SP_ERR_INVALID;
+}
+
+int sp_tune_get(sp_graph_h g, const char* key, int64_t* value) {
+  if (!g || !key || !value) {
+    set_error("sp_tune_get: NULL argument");
+    return SP_ERR_INVALID;
+  }
+  if (!strcmp(key, "pr.short_deg")) {
+    *value = g->pr_short_deg > 0 ? g->pr_short_deg : 32;
+    return SP_OK;
+  }
+  set_error("sp_tune_get: unknown key '%s'", key);
+  return SP_ERR_INVALID;
+}
+
 int sp_graph_info(sp_graph_h g, int32_t* V, int64_t* E, int32_t* symmetric) {
   if (!g) {
     set_error("sp_graph_info: NULL graph");

@@ -9,14 +9,12 @@
 //  * Every iteration writes contrib[v] = pr[v]/outdeg(v) next to pr[v], so the next
 //    gather reads one float per in-edge (the same per-edge quotient the reference
 //    forms in float).
-//  * Work is split into row-aligned tiles of at most 2048 merged items (rows + in-edges):
-//    a CTA of 256 threads stages the tile's srcList slice and gathers contrib into
-//    shared memory with coalesced loads, then walks a merge path (8 items per thread)
-//    with a block-wide segmented scan, so row lengths never unbalance threads.
-//    Sums are accumulated in FP64 and rounded once to FP32.
-//  * Rows with more than 2047 in-edges are split into 2048-edge chunks; the CTA that
-//    finishes a row's last chunk (arrival counter) adds the chunk partials in chunk
-//    order — deterministic, no float atomics.
+//  * Load balance by in-degree bin, decided per row inside the kernel (no bin lists,
+//    so row outputs stay coalesced): one thread per row up to short_deg in-edges,
+//    one warp per row up to 4096, and 4096-edge chunks (one CTA each) above that;
+//    the CTA that finishes a hub's last chunk adds the chunk partials in chunk order.
+//  * Row sums are FP64 and rounded once to FP32; every sum has a fixed order, so the
+//    result is deterministic (no float atomics).
 //  * The L1 diff is reduced per CTA and summed in CTA order by the last CTA to
 //    finish, which also advances the iteration count and raises the done flag; later
 //    launches in the graph see the flag and return at once.
@@ -29,10 +27,10 @@ namespace sp {
 
 namespace pr {
 constexpr int THREADS = 256;
-constexpr int IPT = 8;                  // merged items per thread
-constexpr int CAP = THREADS * IPT;      // items per short tile
-constexpr int CHUNK = THREADS * IPT;    // edges per long-row chunk
-constexpr int LONG_DEG = CAP - 1;       // rows above this are chunked
+constexpr int IPT = 8;                  // loads in flight per thread in chunk sums
+constexpr int CHUNK = 4096;             // edges per long-row chunk
+constexpr int LONG_DEG = 4096;          // rows above this are chunked
+constexpr int SHORT_DEG = 32;           // default per-lane / per-warp split
 
 struct State {
   int iter;
@@ -44,8 +42,7 @@ struct State {
 }  // namespace pr
 
 struct PrPlan {
-  int n_short = 0, n_chunks = 0, n_long = 0;
-  dbuf<int2> tiles;       // [n_short] row ranges
+  int n_chunks = 0, n_long = 0;
   dbuf<int4> chunks;      // [n_chunks] {row, e_begin, e_end, long index}
   dbuf<int2> longs;       // [n_long] {first chunk, chunk count}
   dbuf<unsigned int> long_ctr;
@@ -58,12 +55,12 @@ struct PrPlan {
   int exec_iters = 0;
   float exec_beta = -1, exec_delta = -1;
   cudaStream_t exec_stream = nullptr;
+  int exec_short = -1;
 };
 
 void free_pr_plan(PrPlan* p) {
   if (!p) return;
   if (p->exec) cudaGraphExecDestroy(p->exec);
-  p->tiles.release();
   p->chunks.release();
   p->longs.release();
   p->long_ctr.release();
@@ -84,15 +81,15 @@ struct IterArgs {
   const int32_t* __restrict__ roff;
   const int32_t* __restrict__ radj;
   const int32_t* __restrict__ off;
-  const int2* __restrict__ tiles;
   const int4* __restrict__ chunks;
   const int2* __restrict__ longs;
   unsigned int* long_ctr;
   double* chunk_part;
   double* diff_part;
   State* st;
-  int n_short;
-  int n_total;  // n_short + n_chunks
+  int V;
+  int n_chunks;
+  int short_deg;  // rows with at most this many in-edges are summed by one thread
   float base;   // (1 - delta) / V, in float as the DSL computes it
   float delta;
   double beta;
@@ -111,138 +108,32 @@ __device__ __forceinline__ double finalize_row(const IterArgs& a, int r, double 
   return fabs((double)np - (double)po);
 }
 
-// Number of row-end items among the first `diag` merged items of a tile
-// (row-end i comes after edge s_end[i]-1 and before edge s_end[i]).
-__device__ __forceinline__ int merge_search(int diag, const int* s_end, int nrows, int nedges) {
-  int lo = max(diag - nedges, 0), hi = min(diag, nrows);
-  while (lo < hi) {
-    int mid = (lo + hi) >> 1;
-    if (s_end[mid] <= diag - mid - 1)
-      lo = mid + 1;
-    else
-      hi = mid;
-  }
-  return lo;
-}
-
+// One iteration. Persistent CTAs of 256 threads:
+//  phase 1: long-row chunks (in-degree > LONG_DEG), CTA-strided; the CTA that adds
+//           the last chunk partial of a row finalizes it (arrival counter);
+//  phase 2: groups of 32 consecutive rows, one warp per group, warp-strided.
+//           Lanes whose row has <= short_deg in-edges sum it themselves (4 loads in
+//           flight per lane); rows above that are summed by the whole warp, one
+//           row at a time (coalesced srcList loads, fixed xor-tree reduction).
+// Row sums are FP64; each row's sum order is fixed, so results are deterministic.
 __global__ void __launch_bounds__(THREADS) k_iter(IterArgs a, const float* __restrict__ pr_old,
                                                   const float* __restrict__ con_old, float* __restrict__ pr_new,
                                                   float* __restrict__ con_new) {
-  __shared__ float s_val[CAP];
-  __shared__ int s_end[CAP];
   __shared__ double s_red[THREADS / 32];
-  __shared__ double s_wv[THREADS / 32];
-  __shared__ int s_wf[THREADS / 32];
   __shared__ int s_last;
   if (a.st->done) return;
   const int tid = threadIdx.x;
-  const int lane = tid & 31, wid = tid >> 5;
+  const int lane = tid & 31;
   double my_diff = 0;
 
-  // persistent CTAs: tiles (then long-row chunks) in a fixed round-robin order
-  for (int item = blockIdx.x; item < a.n_total; item += gridDim.x) {
-  if (item < a.n_short) {
-    const int2 t = a.tiles[item];
-    const int rb = t.x, re = t.y;
-    const int eb = a.roff[rb];
-    const int ee = a.roff[re];
-    const int nrows = re - rb, nedges = ee - eb, total = nrows + nedges;
-    for (int i = tid; i < nrows; i += THREADS) s_end[i] = a.roff[rb + i + 1] - eb;
-    {
-      int idx[IPT];
-#pragma unroll
-      for (int k = 0; k < IPT; ++k) {
-        int j = tid + k * THREADS;
-        idx[k] = j < nedges ? __ldg(a.radj + eb + j) : -1;
-      }
-      float v[IPT];
-#pragma unroll
-      for (int k = 0; k < IPT; ++k) v[k] = idx[k] >= 0 ? __ldg(con_old + idx[k]) : 0.0f;
-#pragma unroll
-      for (int k = 0; k < IPT; ++k) {
-        int j = tid + k * THREADS;
-        if (j < nedges) s_val[j] = v[k];
-      }
-    }
-    __syncthreads();
-    const int d0 = min(tid * IPT, total);
-    const int d1 = min(d0 + IPT, total);
-    const int x0 = merge_search(d0, s_end, nrows, nedges);
-    const int y0 = d0 - x0;
-    // pass 1: partial of the row left open at the end of this thread's items
-    double acc = 0;
-    int has_end = 0;
-    {
-      int x = x0, y = y0;
-      for (int d = d0; d < d1; ++d) {
-        if (y < s_end[x]) {
-          acc += (double)s_val[y];
-          ++y;
-        } else {
-          has_end = 1;
-          acc = 0;
-          ++x;
-        }
-      }
-    }
-    // block-wide exclusive segmented scan of (has_end, acc): carry into this thread
-    int f = has_end;
-    double v = acc;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      int fu = __shfl_up_sync(0xffffffffu, f, o);
-      double vu = __shfl_up_sync(0xffffffffu, v, o);
-      if (lane >= o) {
-        if (!f) v += vu;
-        f |= fu;
-      }
-    }
-    if (lane == 31) {
-      s_wf[wid] = f;
-      s_wv[wid] = v;
-    }
-    __syncthreads();
-    // exclusive prefix over warps (fixed order)
-    double pv = 0;
-    for (int w = 0; w < wid; ++w) {
-      if (s_wf[w]) {
-        pv = s_wv[w];
-      } else {
-        pv += s_wv[w];
-      }
-    }
-    int ef = __shfl_up_sync(0xffffffffu, f, 1);
-    double ev = __shfl_up_sync(0xffffffffu, v, 1);
-    double carry;
-    if (lane == 0)
-      carry = pv;
-    else
-      carry = ef ? ev : pv + ev;
-    // pass 2: finalize rows whose end item is in this thread
-    {
-      int x = x0, y = y0;
-      double s = carry;
-      for (int d = d0; d < d1; ++d) {
-        if (y < s_end[x]) {
-          s += (double)s_val[y];
-          ++y;
-        } else {
-          my_diff += finalize_row(a, rb + x, s, pr_old, pr_new, con_new);
-          s = 0;
-          ++x;
-        }
-      }
-    }
-    __syncthreads();  // s_val / s_end are reused by the next tile
-  } else {
-    const int ci = item - a.n_short;
+  for (int ci = blockIdx.x; ci < a.n_chunks; ci += gridDim.x) {
     const int4 c = a.chunks[ci];
     double acc = 0;
-    {
+    for (int e0 = c.y; e0 < c.z; e0 += THREADS * IPT) {
       int idx[IPT];
 #pragma unroll
       for (int k = 0; k < IPT; ++k) {
-        int e = c.y + tid + k * THREADS;
+        int e = e0 + tid + k * THREADS;
         idx[k] = e < c.z ? __ldg(a.radj + e) : -1;
       }
 #pragma unroll
@@ -267,8 +158,59 @@ __global__ void __launch_bounds__(THREADS) k_iter(IterArgs a, const float* __res
       my_diff += finalize_row(a, c.x, sum, pr_old, pr_new, con_new);
       a.long_ctr[c.w] = 0;
     }
-    __syncthreads();  // s_last is reused
+    __syncthreads();
   }
+
+  const int warps_total = gridDim.x * (THREADS / 32);
+  const int ngroups = (a.V + 31) >> 5;
+  for (int grp = blockIdx.x * (THREADS / 32) + (tid >> 5); grp < ngroups; grp += warps_total) {
+    const int r = (grp << 5) + lane;
+    int b = 0, e = 0;
+    if (r < a.V) {
+      b = a.roff[r];
+      e = a.roff[r + 1];
+    }
+    const int d = e - b;
+    const bool is_long = d > LONG_DEG;
+    const bool is_med = !is_long && d > a.short_deg;
+    double s = 0;
+    if (!is_med && !is_long) {
+      int i = b;
+      for (; i + 4 <= e; i += 4) {
+        int u0 = __ldg(a.radj + i), u1 = __ldg(a.radj + i + 1), u2 = __ldg(a.radj + i + 2),
+            u3 = __ldg(a.radj + i + 3);
+        float c0 = __ldg(con_old + u0), c1 = __ldg(con_old + u1), c2 = __ldg(con_old + u2),
+              c3 = __ldg(con_old + u3);
+        s += (double)c0;
+        s += (double)c1;
+        s += (double)c2;
+        s += (double)c3;
+      }
+      for (; i < e; ++i) s += (double)__ldg(con_old + __ldg(a.radj + i));
+    }
+    unsigned med = __ballot_sync(0xffffffffu, is_med);
+    while (med) {
+      const int l = __ffs(med) - 1;
+      med &= med - 1;
+      const int rb = __shfl_sync(0xffffffffu, b, l);
+      const int re = __shfl_sync(0xffffffffu, e, l);
+      double acc = 0;
+      int i = rb + lane;
+      for (; i + 96 < re; i += 128) {
+        int u0 = __ldg(a.radj + i), u1 = __ldg(a.radj + i + 32), u2 = __ldg(a.radj + i + 64),
+            u3 = __ldg(a.radj + i + 96);
+        float c0 = __ldg(con_old + u0), c1 = __ldg(con_old + u1), c2 = __ldg(con_old + u2),
+              c3 = __ldg(con_old + u3);
+        acc += (double)c0;
+        acc += (double)c1;
+        acc += (double)c2;
+        acc += (double)c3;
+      }
+      for (; i < re; i += 32) acc += (double)__ldg(con_old + __ldg(a.radj + i));
+      acc = warp_sum(acc);
+      if (lane == l) s = acc;
+    }
+    if (r < a.V && !is_long) my_diff += finalize_row(a, r, s, pr_old, pr_new, con_new);
   }
 
   // per-CTA diff partial, then the last CTA reduces them in CTA order
@@ -344,31 +286,18 @@ static int build_pr_plan(sp_graph* g) {
   std::vector<int32_t> roff(V + 1);
   SP_CHECK_CUDA(cudaMemcpyAsync(roff.data(), g->roff.p, sizeof(int32_t) * (V + 1), cudaMemcpyDeviceToHost, g->stream));
   SP_CHECK_CUDA(cudaStreamSynchronize(g->stream));
-  std::vector<int2> tiles;
   std::vector<int4> chunks;
   std::vector<int2> longs;
-  int r = 0;
-  while (r < V) {
+  for (int r = 0; r < V; ++r) {
     int deg = roff[r + 1] - roff[r];
     if (deg > pr::LONG_DEG) {
       int first = (int)chunks.size();
       for (int e = roff[r]; e < roff[r + 1]; e += pr::CHUNK)
         chunks.push_back(make_int4(r, e, std::min(e + pr::CHUNK, roff[r + 1]), (int)longs.size()));
       longs.push_back(make_int2(first, (int)chunks.size() - first));
-      ++r;
-      continue;
     }
-    int start = r, items = 0;
-    while (r < V) {
-      int d = roff[r + 1] - roff[r];
-      if (d > pr::LONG_DEG || items + 1 + d > pr::CAP) break;
-      items += 1 + d;
-      ++r;
-    }
-    tiles.push_back(make_int2(start, r));
   }
   PrPlan* p = new PrPlan();
-  p->n_short = (int)tiles.size();
   p->n_chunks = (int)chunks.size();
   p->n_long = (int)longs.size();
   int st;
@@ -376,16 +305,14 @@ static int build_pr_plan(sp_graph* g) {
     free_pr_plan(p);
     return s;
   };
-  if ((st = p->tiles.alloc(std::max(1, p->n_short))) || (st = p->chunks.alloc(std::max(1, p->n_chunks))) ||
-      (st = p->longs.alloc(std::max(1, p->n_long))) || (st = p->long_ctr.alloc(std::max(1, p->n_long))) ||
-      (st = p->chunk_part.alloc(std::max(1, p->n_chunks))) ||
-      (st = p->diff_part.alloc(std::max(1, p->n_short + p->n_chunks))) || (st = p->state.alloc(1)))
+  const int max_grid = num_sms() * 32;
+  if ((st = p->chunks.alloc(std::max(1, p->n_chunks))) || (st = p->longs.alloc(std::max(1, p->n_long))) ||
+      (st = p->long_ctr.alloc(std::max(1, p->n_long))) || (st = p->chunk_part.alloc(std::max(1, p->n_chunks))) ||
+      (st = p->diff_part.alloc(max_grid)) || (st = p->state.alloc(1)))
     return fail(st);
   for (int i = 0; i < 2; ++i)
     if ((st = p->prb[i].alloc(V)) || (st = p->con[i].alloc(V))) return fail(st);
   cudaStream_t s = g->stream;
-  if (p->n_short)
-    SP_CHECK_CUDA(cudaMemcpyAsync(p->tiles.p, tiles.data(), sizeof(int2) * p->n_short, cudaMemcpyHostToDevice, s));
   if (p->n_chunks)
     SP_CHECK_CUDA(cudaMemcpyAsync(p->chunks.p, chunks.data(), sizeof(int4) * p->n_chunks, cudaMemcpyHostToDevice, s));
   if (p->n_long)
@@ -407,26 +334,27 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
   a.roff = g->roff.p;
   a.radj = g->radj.p;
   a.off = g->off.p;
-  a.tiles = p->tiles.p;
   a.chunks = p->chunks.p;
   a.longs = p->longs.p;
   a.long_ctr = p->long_ctr.p;
   a.chunk_part = p->chunk_part.p;
   a.diff_part = p->diff_part.p;
   a.st = p->state.p;
-  a.n_short = p->n_short;
-  a.n_total = p->n_short + p->n_chunks;
+  a.V = V;
+  a.n_chunks = p->n_chunks;
+  a.short_deg = g->pr_short_deg > 0 ? g->pr_short_deg : pr::SHORT_DEG;
   a.delta = delta;
   a.base = (1.0f - delta) / (float)V;
   a.beta = (double)beta;
   a.max_iter = n_iter;
   int per_sm = 0;
   SP_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pr::k_iter, pr::THREADS, 0));
-  const int grid = std::max(1, std::min(a.n_total, num_sms() * std::max(1, per_sm)));
+  const int grid = std::max(1, std::min(num_sms() * 32, num_sms() * std::max(1, per_sm)));
 
   pr::k_init<<<num_sms() * 4, 256, 0, s>>>(V, g->off.p, p->prb[0].p, p->con[0].p, p->state.p);
   SP_CHECK_LAUNCH();
-  if (!(p->exec && p->exec_iters == n_iter && p->exec_beta == beta && p->exec_delta == delta && p->exec_stream == s)) {
+  if (!(p->exec && p->exec_iters == n_iter && p->exec_beta == beta && p->exec_delta == delta && p->exec_stream == s &&
+        p->exec_short == a.short_deg)) {
     if (p->exec) {
       cudaGraphExecDestroy(p->exec);
       p->exec = nullptr;
@@ -453,6 +381,7 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
     p->exec_beta = beta;
     p->exec_delta = delta;
     p->exec_stream = s;
+    p->exec_short = a.short_deg;
   }
   SP_CHECK_CUDA(cudaGraphLaunch(p->exec, s));
   g_launches.fetch_add(n_iter);

@@ -95,6 +95,14 @@ class DeviceGraph:
         raw = getattr(stream, "cuda_stream", stream)
         check("sp_graph_set_stream", lib().sp_graph_set_stream(self.handle, raw))
 
+    def tune_set(self, key: str, value: int) -> None:
+        check("sp_tune_set", lib().sp_tune_set(self.handle, key.encode(), int(value)))
+
+    def tune_get(self, key: str) -> int:
+        v = ctypes.c_int64()
+        check("sp_tune_get", lib().sp_tune_get(self.handle, key.encode(), ctypes.byref(v)))
+        return int(v.value)
+
     def info(self):
         V = ctypes.c_int32()
         E = ctypes.c_int64()
