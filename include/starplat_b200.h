@@ -62,8 +62,7 @@ int sp_graph_set_stream(sp_graph_h g, void* cuda_stream);
 int sp_graph_info(sp_graph_h g, int32_t* V, int64_t* E, int32_t* symmetric);
 
 /* Schedule knobs (what the autotuner and the learned scheduler set); results never
- * depend on them. Keys: "pr.short_deg" (in-degree up to which one thread sums a
- * PageRank row; above it a warp does, default 32). Unknown keys: SP_ERR_INVALID. */
+ * depend on them. Unknown keys: SP_ERR_INVALID. */
 int sp_tune_set(sp_graph_h g, const char* key, int64_t value);
 int sp_tune_get(sp_graph_h g, const char* key, int64_t* value);
 

@@ -294,14 +294,6 @@ int sp_tune_set(sp_graph_h g, const char* key, int64_t value) {
     set_error("sp_tune_set: NULL argument");
     return SP_ERR_INVALID;
   }
-  if (!strcmp(key, "pr.short_deg")) {
-    if (value < 0 || value > 4096) {
-      set_error("sp_tune_set: pr.short_deg must be in [0, 4096]");
-      return SP_ERR_INVALID;
-    }
-    g->pr_short_deg = (int32_t)value;
-    return SP_OK;
-  }
   set_error("sp_tune_set: unknown key '%s'", key);
   return SP_ERR_INVALID;
 }
@@ -310,10 +302,6 @@ int sp_tune_get(sp_graph_h g, const char* key, int64_t* value) {
   if (!g || !key || !value) {
     set_error("sp_tune_get: NULL argument");
     return SP_ERR_INVALID;
-  }
-  if (!strcmp(key, "pr.short_deg")) {
-    *value = g->pr_short_deg > 0 ? g->pr_short_deg : 32;
-    return SP_OK;
   }
   set_error("sp_tune_get: unknown key '%s'", key);
   return SP_ERR_INVALID;

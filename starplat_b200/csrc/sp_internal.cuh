@@ -98,7 +98,6 @@ struct sp_graph {
   bool has_rev = false;
   int symmetric = -1;      // -1 unknown, 0/1
   int32_t max_out_deg = -1;
-  int32_t pr_short_deg = 0;  // PageRank per-thread/per-warp row split (0 = default)
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   sp::PrPlan* pr = nullptr;

@@ -9,10 +9,10 @@
 //  * Every iteration writes contrib[v] = pr[v]/outdeg(v) next to pr[v], so the next
 //    gather reads one float per in-edge (the same per-edge quotient the reference
 //    forms in float).
-//  * Load balance by in-degree bin, decided per row inside the kernel (no bin lists,
-//    so row outputs stay coalesced): one thread per row up to short_deg in-edges,
-//    one warp per row up to 4096, and 4096-edge chunks (one CTA each) above that;
-//    the CTA that finishes a hub's last chunk adds the chunk partials in chunk order.
+//  * Load balance by static in-degree bins built once per graph: 1, 4, 8 or 32 lanes
+//    per row (in-degree <= 4, <= 16, <= 32, <= 2048) with every load of a row in
+//    flight at once, and 2048-edge chunks (one CTA each) above that; the CTA that
+//    finishes a hub's last chunk adds the chunk partials in chunk order.
 //  * Row sums are FP64 and rounded once to FP32; every sum has a fixed order, so the
 //    result is deterministic (no float atomics).
 //  * The L1 diff is reduced per CTA and summed in CTA order by the last CTA to
@@ -28,9 +28,10 @@ namespace sp {
 namespace pr {
 constexpr int THREADS = 256;
 constexpr int IPT = 8;                  // loads in flight per thread in chunk sums
-constexpr int CHUNK = 4096;             // edges per long-row chunk
-constexpr int LONG_DEG = 4096;          // rows above this are chunked
-constexpr int SHORT_DEG = 32;           // default per-lane / per-warp split
+constexpr int CHUNK = THREADS * IPT;    // edges per long-row chunk (one round per CTA)
+constexpr int LONG_DEG = 2048;          // rows above this are chunked
+// degree-bin upper bounds for 1, 4, 8 and 32 lanes per row
+constexpr int BIN_T1 = 4, BIN_T4 = 16, BIN_T8 = 32;
 
 struct State {
   int iter;
@@ -42,7 +43,9 @@ struct State {
 }  // namespace pr
 
 struct PrPlan {
-  int n_chunks = 0, n_long = 0;
+  int n_chunks = 0, n_long = 0, n_tasks = 0;
+  dbuf<int32_t> rows;     // row ids grouped by in-degree bin
+  dbuf<int4> tasks;       // warp tasks {W, start, count, 0}
   dbuf<int4> chunks;      // [n_chunks] {row, e_begin, e_end, long index}
   dbuf<int2> longs;       // [n_long] {first chunk, chunk count}
   dbuf<unsigned int> long_ctr;
@@ -55,13 +58,14 @@ struct PrPlan {
   int exec_iters = 0;
   float exec_beta = -1, exec_delta = -1;
   cudaStream_t exec_stream = nullptr;
-  int exec_short = -1;
 };
 
 void free_pr_plan(PrPlan* p) {
   if (!p) return;
   if (p->exec) cudaGraphExecDestroy(p->exec);
   p->chunks.release();
+  p->rows.release();
+  p->tasks.release();
   p->longs.release();
   p->long_ctr.release();
   p->chunk_part.release();
@@ -83,13 +87,15 @@ struct IterArgs {
   const int32_t* __restrict__ off;
   const int4* __restrict__ chunks;
   const int2* __restrict__ longs;
+  const int32_t* __restrict__ rows;   // binned row ids
+  const int4* __restrict__ tasks;     // warp tasks {W, start, count, 0}
   unsigned int* long_ctr;
   double* chunk_part;
   double* diff_part;
   State* st;
   int V;
   int n_chunks;
-  int short_deg;  // rows with at most this many in-edges are summed by one thread
+  int n_tasks;
   float base;   // (1 - delta) / V, in float as the DSL computes it
   float delta;
   double beta;
@@ -108,14 +114,53 @@ __device__ __forceinline__ double finalize_row(const IterArgs& a, int r, double 
   return fabs((double)np - (double)po);
 }
 
+// Sum of con[radj[i]] for i in [b, e) by a group of W lanes (sl = lane within the
+// group), U loads in flight per lane per round, reduced with a fixed xor tree.
+template <int W, int U>
+__device__ __forceinline__ double group_row_sum(int b, int e, int sl, const int32_t* __restrict__ radj,
+                                                const float* __restrict__ con) {
+  double acc = 0;
+  for (int base = b; base < e; base += W * U) {
+    int idx[U];
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+      int i = base + sl + W * k;
+      idx[k] = i < e ? __ldg(radj + i) : -1;
+    }
+    float v[U];
+#pragma unroll
+    for (int k = 0; k < U; ++k) v[k] = idx[k] >= 0 ? __ldg(con + idx[k]) : 0.0f;
+#pragma unroll
+    for (int k = 0; k < U; ++k) acc += (double)v[k];
+  }
+#pragma unroll
+  for (int o = W / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  return acc;
+}
+
+template <int W, int U>
+__device__ __forceinline__ double warp_task(const IterArgs& a, int start, int count, int lane,
+                                            const float* __restrict__ pr_old, const float* __restrict__ con_old,
+                                            float* __restrict__ pr_new, float* __restrict__ con_new) {
+  const int g = lane / W, sl = lane % W;
+  int r = -1, b = 0, e = 0;
+  if (g < count) {
+    r = a.rows[start + g];
+    b = a.roff[r];
+    e = a.roff[r + 1];
+  }
+  double sum = group_row_sum<W, U>(b, e, sl, a.radj, con_old);
+  if (r >= 0 && sl == 0) return finalize_row(a, r, sum, pr_old, pr_new, con_new);
+  return 0.0;
+}
+
 // One iteration. Persistent CTAs of 256 threads:
-//  phase 1: long-row chunks (in-degree > LONG_DEG), CTA-strided; the CTA that adds
-//           the last chunk partial of a row finalizes it (arrival counter);
-//  phase 2: groups of 32 consecutive rows, one warp per group, warp-strided.
-//           Lanes whose row has <= short_deg in-edges sum it themselves (4 loads in
-//           flight per lane); rows above that are summed by the whole warp, one
-//           row at a time (coalesced srcList loads, fixed xor-tree reduction).
-// Row sums are FP64; each row's sum order is fixed, so results are deterministic.
+//  phase 1: in-degree > 2048: 2048-edge chunks, one CTA each (CTA-strided); the CTA
+//           that adds a row's last chunk partial finalizes the row (arrival counter);
+//  phase 2: warp tasks (warp-strided), heaviest bins first: up to 32/W rows of one
+//           degree bin, W lanes per row, all of a row's loads in flight at once
+//           (W = 32 for in-degree 33..2048, 8 for 17..32, 4 for 5..16, 1 for 0..4).
+// Row sums are FP64 with a fixed order per row, so results are deterministic.
 __global__ void __launch_bounds__(THREADS) k_iter(IterArgs a, const float* __restrict__ pr_old,
                                                   const float* __restrict__ con_old, float* __restrict__ pr_new,
                                                   float* __restrict__ con_new) {
@@ -129,16 +174,18 @@ __global__ void __launch_bounds__(THREADS) k_iter(IterArgs a, const float* __res
   for (int ci = blockIdx.x; ci < a.n_chunks; ci += gridDim.x) {
     const int4 c = a.chunks[ci];
     double acc = 0;
-    for (int e0 = c.y; e0 < c.z; e0 += THREADS * IPT) {
+    {
       int idx[IPT];
 #pragma unroll
       for (int k = 0; k < IPT; ++k) {
-        int e = e0 + tid + k * THREADS;
+        int e = c.y + tid + k * THREADS;
         idx[k] = e < c.z ? __ldg(a.radj + e) : -1;
       }
+      float v[IPT];
 #pragma unroll
-      for (int k = 0; k < IPT; ++k)
-        if (idx[k] >= 0) acc += (double)__ldg(con_old + idx[k]);
+      for (int k = 0; k < IPT; ++k) v[k] = idx[k] >= 0 ? __ldg(con_old + idx[k]) : 0.0f;
+#pragma unroll
+      for (int k = 0; k < IPT; ++k) acc += (double)v[k];
     }
     double tot = block_sum<THREADS>(acc, s_red);
     if (tid == 0) {
@@ -162,55 +209,14 @@ __global__ void __launch_bounds__(THREADS) k_iter(IterArgs a, const float* __res
   }
 
   const int warps_total = gridDim.x * (THREADS / 32);
-  const int ngroups = (a.V + 31) >> 5;
-  for (int grp = blockIdx.x * (THREADS / 32) + (tid >> 5); grp < ngroups; grp += warps_total) {
-    const int r = (grp << 5) + lane;
-    int b = 0, e = 0;
-    if (r < a.V) {
-      b = a.roff[r];
-      e = a.roff[r + 1];
+  for (int t = blockIdx.x * (THREADS / 32) + (tid >> 5); t < a.n_tasks; t += warps_total) {
+    const int4 task = a.tasks[t];  // {W, start, count, -}
+    switch (task.x) {
+      case 32: my_diff += warp_task<32, 8>(a, task.y, task.z, lane, pr_old, con_old, pr_new, con_new); break;
+      case 8: my_diff += warp_task<8, 4>(a, task.y, task.z, lane, pr_old, con_old, pr_new, con_new); break;
+      case 4: my_diff += warp_task<4, 4>(a, task.y, task.z, lane, pr_old, con_old, pr_new, con_new); break;
+      default: my_diff += warp_task<1, 4>(a, task.y, task.z, lane, pr_old, con_old, pr_new, con_new); break;
     }
-    const int d = e - b;
-    const bool is_long = d > LONG_DEG;
-    const bool is_med = !is_long && d > a.short_deg;
-    double s = 0;
-    if (!is_med && !is_long) {
-      int i = b;
-      for (; i + 4 <= e; i += 4) {
-        int u0 = __ldg(a.radj + i), u1 = __ldg(a.radj + i + 1), u2 = __ldg(a.radj + i + 2),
-            u3 = __ldg(a.radj + i + 3);
-        float c0 = __ldg(con_old + u0), c1 = __ldg(con_old + u1), c2 = __ldg(con_old + u2),
-              c3 = __ldg(con_old + u3);
-        s += (double)c0;
-        s += (double)c1;
-        s += (double)c2;
-        s += (double)c3;
-      }
-      for (; i < e; ++i) s += (double)__ldg(con_old + __ldg(a.radj + i));
-    }
-    unsigned med = __ballot_sync(0xffffffffu, is_med);
-    while (med) {
-      const int l = __ffs(med) - 1;
-      med &= med - 1;
-      const int rb = __shfl_sync(0xffffffffu, b, l);
-      const int re = __shfl_sync(0xffffffffu, e, l);
-      double acc = 0;
-      int i = rb + lane;
-      for (; i + 96 < re; i += 128) {
-        int u0 = __ldg(a.radj + i), u1 = __ldg(a.radj + i + 32), u2 = __ldg(a.radj + i + 64),
-            u3 = __ldg(a.radj + i + 96);
-        float c0 = __ldg(con_old + u0), c1 = __ldg(con_old + u1), c2 = __ldg(con_old + u2),
-              c3 = __ldg(con_old + u3);
-        acc += (double)c0;
-        acc += (double)c1;
-        acc += (double)c2;
-        acc += (double)c3;
-      }
-      for (; i < re; i += 32) acc += (double)__ldg(con_old + __ldg(a.radj + i));
-      acc = warp_sum(acc);
-      if (lane == l) s = acc;
-    }
-    if (r < a.V && !is_long) my_diff += finalize_row(a, r, s, pr_old, pr_new, con_new);
   }
 
   // per-CTA diff partial, then the last CTA reduces them in CTA order
@@ -288,6 +294,7 @@ static int build_pr_plan(sp_graph* g) {
   SP_CHECK_CUDA(cudaStreamSynchronize(g->stream));
   std::vector<int4> chunks;
   std::vector<int2> longs;
+  std::vector<int32_t> bin[4];  // W = 32, 8, 4, 1
   for (int r = 0; r < V; ++r) {
     int deg = roff[r + 1] - roff[r];
     if (deg > pr::LONG_DEG) {
@@ -295,11 +302,32 @@ static int build_pr_plan(sp_graph* g) {
       for (int e = roff[r]; e < roff[r + 1]; e += pr::CHUNK)
         chunks.push_back(make_int4(r, e, std::min(e + pr::CHUNK, roff[r + 1]), (int)longs.size()));
       longs.push_back(make_int2(first, (int)chunks.size() - first));
+    } else if (deg > pr::BIN_T8) {
+      bin[0].push_back(r);
+    } else if (deg > pr::BIN_T4) {
+      bin[1].push_back(r);
+    } else if (deg > pr::BIN_T1) {
+      bin[2].push_back(r);
+    } else {
+      bin[3].push_back(r);
     }
+  }
+  // warp tasks, heaviest bin first; rows concatenated in the same order
+  const int widths[4] = {32, 8, 4, 1};
+  std::vector<int32_t> rows;
+  std::vector<int4> tasks;
+  rows.reserve(V);
+  for (int k = 0; k < 4; ++k) {
+    const int per = 32 / widths[k];
+    const int base = (int)rows.size();
+    rows.insert(rows.end(), bin[k].begin(), bin[k].end());
+    for (int i = 0; i < (int)bin[k].size(); i += per)
+      tasks.push_back(make_int4(widths[k], base + i, std::min(per, (int)bin[k].size() - i), 0));
   }
   PrPlan* p = new PrPlan();
   p->n_chunks = (int)chunks.size();
   p->n_long = (int)longs.size();
+  p->n_tasks = (int)tasks.size();
   int st;
   auto fail = [&](int s) {
     free_pr_plan(p);
@@ -308,7 +336,8 @@ static int build_pr_plan(sp_graph* g) {
   const int max_grid = num_sms() * 32;
   if ((st = p->chunks.alloc(std::max(1, p->n_chunks))) || (st = p->longs.alloc(std::max(1, p->n_long))) ||
       (st = p->long_ctr.alloc(std::max(1, p->n_long))) || (st = p->chunk_part.alloc(std::max(1, p->n_chunks))) ||
-      (st = p->diff_part.alloc(max_grid)) || (st = p->state.alloc(1)))
+      (st = p->diff_part.alloc(max_grid)) || (st = p->state.alloc(1)) ||
+      (st = p->rows.alloc(std::max<size_t>(1, rows.size()))) || (st = p->tasks.alloc(std::max(1, p->n_tasks))))
     return fail(st);
   for (int i = 0; i < 2; ++i)
     if ((st = p->prb[i].alloc(V)) || (st = p->con[i].alloc(V))) return fail(st);
@@ -317,6 +346,10 @@ static int build_pr_plan(sp_graph* g) {
     SP_CHECK_CUDA(cudaMemcpyAsync(p->chunks.p, chunks.data(), sizeof(int4) * p->n_chunks, cudaMemcpyHostToDevice, s));
   if (p->n_long)
     SP_CHECK_CUDA(cudaMemcpyAsync(p->longs.p, longs.data(), sizeof(int2) * p->n_long, cudaMemcpyHostToDevice, s));
+  if (!rows.empty())
+    SP_CHECK_CUDA(cudaMemcpyAsync(p->rows.p, rows.data(), sizeof(int32_t) * rows.size(), cudaMemcpyHostToDevice, s));
+  if (p->n_tasks)
+    SP_CHECK_CUDA(cudaMemcpyAsync(p->tasks.p, tasks.data(), sizeof(int4) * p->n_tasks, cudaMemcpyHostToDevice, s));
   SP_CHECK_CUDA(cudaMemsetAsync(p->long_ctr.p, 0, sizeof(unsigned int) * std::max(1, p->n_long), s));
   SP_CHECK_CUDA(cudaStreamSynchronize(s));
   g->pr = p;
@@ -340,9 +373,11 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
   a.chunk_part = p->chunk_part.p;
   a.diff_part = p->diff_part.p;
   a.st = p->state.p;
+  a.rows = p->rows.p;
+  a.tasks = p->tasks.p;
   a.V = V;
   a.n_chunks = p->n_chunks;
-  a.short_deg = g->pr_short_deg > 0 ? g->pr_short_deg : pr::SHORT_DEG;
+  a.n_tasks = p->n_tasks;
   a.delta = delta;
   a.base = (1.0f - delta) / (float)V;
   a.beta = (double)beta;
@@ -353,8 +388,7 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
 
   pr::k_init<<<num_sms() * 4, 256, 0, s>>>(V, g->off.p, p->prb[0].p, p->con[0].p, p->state.p);
   SP_CHECK_LAUNCH();
-  if (!(p->exec && p->exec_iters == n_iter && p->exec_beta == beta && p->exec_delta == delta && p->exec_stream == s &&
-        p->exec_short == a.short_deg)) {
+  if (!(p->exec && p->exec_iters == n_iter && p->exec_beta == beta && p->exec_delta == delta && p->exec_stream == s))  {
     if (p->exec) {
       cudaGraphExecDestroy(p->exec);
       p->exec = nullptr;
@@ -381,7 +415,6 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
     p->exec_beta = beta;
     p->exec_delta = delta;
     p->exec_stream = s;
-    p->exec_short = a.short_deg;
   }
   SP_CHECK_CUDA(cudaGraphLaunch(p->exec, s));
   g_launches.fetch_add(n_iter);
