@@ -135,6 +135,7 @@ def main():
     ap.add_argument("--quick", action="store_true",
                     help="device-resident timing only (no roofline/e2e/CPU legs): for profiler runs")
     ap.add_argument("--scale", type=int, default=PR_SCALE, help="R-MAT scale (profiling on smaller cases)")
+    ap.add_argument("--tune", action="append", default=[], help="schedule knob key=value (sp_tune_set)")
     args = ap.parse_args()
     PR_SCALE = args.scale
 
@@ -168,6 +169,9 @@ def main():
     stream = torch.cuda.current_stream()
     dg = DeviceGraph.from_csr(g, with_weights=False)
     dg.set_stream(stream)
+    for kv in args.tune:
+        k, v = kv.split("=")
+        dg.tune_set(k, int(v))
     out = torch.empty(V, dtype=torch.float32, device="cuda")
 
     for _ in range(max(3, args.warmup)):

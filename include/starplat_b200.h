@@ -62,7 +62,9 @@ int sp_graph_set_stream(sp_graph_h g, void* cuda_stream);
 int sp_graph_info(sp_graph_h g, int32_t* V, int64_t* E, int32_t* symmetric);
 
 /* Schedule knobs (what the autotuner and the learned scheduler set); results never
- * depend on them. Unknown keys: SP_ERR_INVALID. */
+ * depend on them. Unknown keys: SP_ERR_INVALID.
+ *   "pr.hot"  PageRank: number of highest-out-degree vertices whose contrib values each
+ *             CTA stages in shared memory per iteration (0..57344, default 0). */
 int sp_tune_set(sp_graph_h g, const char* key, int64_t value);
 int sp_tune_get(sp_graph_h g, const char* key, int64_t* value);
 

@@ -294,6 +294,14 @@ int sp_tune_set(sp_graph_h g, const char* key, int64_t value) {
     set_error("sp_tune_set: NULL argument");
     return SP_ERR_INVALID;
   }
+  if (!strcmp(key, "pr.hot")) {
+    if (value < 0 || value > 56 * 1024) {
+      set_error("sp_tune_set: pr.hot must be in [0, 57344]");
+      return SP_ERR_INVALID;
+    }
+    g->pr_hot = (int32_t)value;
+    return SP_OK;
+  }
   set_error("sp_tune_set: unknown key '%s'", key);
   return SP_ERR_INVALID;
 }
@@ -302,6 +310,10 @@ int sp_tune_get(sp_graph_h g, const char* key, int64_t* value) {
   if (!g || !key || !value) {
     set_error("sp_tune_get: NULL argument");
     return SP_ERR_INVALID;
+  }
+  if (!strcmp(key, "pr.hot")) {
+    *value = g->pr_hot >= 0 ? g->pr_hot : 0;
+    return SP_OK;
   }
   set_error("sp_tune_get: unknown key '%s'", key);
   return SP_ERR_INVALID;

@@ -98,6 +98,7 @@ struct sp_graph {
   bool has_rev = false;
   int symmetric = -1;      // -1 unknown, 0/1
   int32_t max_out_deg = -1;
+  int32_t pr_hot = -1;  // PageRank: contrib values staged in shared memory (-1 = default)
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   sp::PrPlan* pr = nullptr;

@@ -18,6 +18,8 @@
 //  * The L1 diff is reduced per CTA and summed in CTA order by the last CTA to
 //    finish, which also advances the iteration count and raises the done flag; later
 //    launches in the graph see the flag and return at once.
+#include <cub/cub.cuh>
+
 #include <algorithm>
 #include <vector>
 
@@ -27,9 +29,11 @@ namespace sp {
 
 namespace pr {
 constexpr int THREADS = 256;
-constexpr int IPT = 8;                  // loads in flight per thread in chunk sums
-constexpr int CHUNK = THREADS * IPT;    // edges per long-row chunk (one round per CTA)
-constexpr int LONG_DEG = 2048;          // rows above this are chunked
+constexpr int CIPT = 8;                 // loads in flight per thread in chunk sums
+constexpr int CHUNK = THREADS * CIPT;   // edges per long-row chunk (one round per CTA)
+constexpr int HOT_MAX = 56 * 1024;      // largest shared-memory contrib table
+constexpr int HOT_DEFAULT = 0;          // measured best on R-MAT 22 (L1/L2 gathers beat shared-memory ones)
+constexpr int LONG_DEG = 2048;          // rows above this are chunked (CHUNK-edge pieces)
 // degree-bin upper bounds for 1, 4, 8 and 32 lanes per row
 constexpr int BIN_T1 = 4, BIN_T4 = 16, BIN_T8 = 32;
 
@@ -44,6 +48,10 @@ struct State {
 
 struct PrPlan {
   int n_chunks = 0, n_long = 0, n_tasks = 0;
+  dbuf<int32_t> new_id;   // vertex -> rank by out-degree (descending, stable)
+  dbuf<int32_t> od;       // out-degree, in relabelled order
+  dbuf<int32_t> roffp, radjp;  // reverse CSR in relabelled ids (per-row order kept)
+  dbuf<float> outbuf;     // result in original vertex order
   dbuf<int32_t> rows;     // row ids grouped by in-degree bin
   dbuf<int4> tasks;       // warp tasks {W, start, count, 0}
   dbuf<int4> chunks;      // [n_chunks] {row, e_begin, e_end, long index}
@@ -58,6 +66,7 @@ struct PrPlan {
   int exec_iters = 0;
   float exec_beta = -1, exec_delta = -1;
   cudaStream_t exec_stream = nullptr;
+  int exec_hot = -1;
 };
 
 void free_pr_plan(PrPlan* p) {
@@ -65,6 +74,11 @@ void free_pr_plan(PrPlan* p) {
   if (p->exec) cudaGraphExecDestroy(p->exec);
   p->chunks.release();
   p->rows.release();
+  p->new_id.release();
+  p->od.release();
+  p->roffp.release();
+  p->radjp.release();
+  p->outbuf.release();
   p->tasks.release();
   p->longs.release();
   p->long_ctr.release();
@@ -84,7 +98,7 @@ namespace pr {
 struct IterArgs {
   const int32_t* __restrict__ roff;
   const int32_t* __restrict__ radj;
-  const int32_t* __restrict__ off;
+  const int32_t* __restrict__ od;    // out-degree per (relabelled) row
   const int4* __restrict__ chunks;
   const int2* __restrict__ longs;
   const int32_t* __restrict__ rows;   // binned row ids
@@ -96,6 +110,7 @@ struct IterArgs {
   int V;
   int n_chunks;
   int n_tasks;
+  int hot;       // multiple of 4, <= V: contrib[0..hot) is read from shared memory
   float base;   // (1 - delta) / V, in float as the DSL computes it
   float delta;
   double beta;
@@ -109,16 +124,22 @@ __device__ __forceinline__ double finalize_row(const IterArgs& a, int r, double 
   float np = __fadd_rn(a.base, __fmul_rn(a.delta, s));
   float po = pr_old[r];
   pr_new[r] = np;
-  int od = a.off[r + 1] - a.off[r];
+  int od = a.od[r];
   con_new[r] = od > 0 ? __fdiv_rn(np, (float)od) : 0.0f;
   return fabs((double)np - (double)po);
+}
+
+// contrib of relabelled vertex u: the first `hot` ids (highest out-degree, so the
+// most gathered) come from the shared-memory copy, the rest from global memory.
+__device__ __forceinline__ float gather(const float* __restrict__ con, const float* s_hot, int hot, int u) {
+  return u < hot ? s_hot[u] : __ldg(con + u);
 }
 
 // Sum of con[radj[i]] for i in [b, e) by a group of W lanes (sl = lane within the
 // group), U loads in flight per lane per round, reduced with a fixed xor tree.
 template <int W, int U>
 __device__ __forceinline__ double group_row_sum(int b, int e, int sl, const int32_t* __restrict__ radj,
-                                                const float* __restrict__ con) {
+                                                const float* __restrict__ con, const float* s_hot, int hot) {
   double acc = 0;
   for (int base = b; base < e; base += W * U) {
     int idx[U];
@@ -129,7 +150,7 @@ __device__ __forceinline__ double group_row_sum(int b, int e, int sl, const int3
     }
     float v[U];
 #pragma unroll
-    for (int k = 0; k < U; ++k) v[k] = idx[k] >= 0 ? __ldg(con + idx[k]) : 0.0f;
+    for (int k = 0; k < U; ++k) v[k] = idx[k] >= 0 ? gather(con, s_hot, hot, idx[k]) : 0.0f;
 #pragma unroll
     for (int k = 0; k < U; ++k) acc += (double)v[k];
   }
@@ -139,7 +160,7 @@ __device__ __forceinline__ double group_row_sum(int b, int e, int sl, const int3
 }
 
 template <int W, int U>
-__device__ __forceinline__ double warp_task(const IterArgs& a, int start, int count, int lane,
+__device__ __forceinline__ double warp_task(const IterArgs& a, int start, int count, int lane, const float* s_hot,
                                             const float* __restrict__ pr_old, const float* __restrict__ con_old,
                                             float* __restrict__ pr_new, float* __restrict__ con_new) {
   const int g = lane / W, sl = lane % W;
@@ -149,7 +170,7 @@ __device__ __forceinline__ double warp_task(const IterArgs& a, int start, int co
     b = a.roff[r];
     e = a.roff[r + 1];
   }
-  double sum = group_row_sum<W, U>(b, e, sl, a.radj, con_old);
+  double sum = group_row_sum<W, U>(b, e, sl, a.radj, con_old, s_hot, a.hot);
   if (r >= 0 && sl == 0) return finalize_row(a, r, sum, pr_old, pr_new, con_new);
   return 0.0;
 }
@@ -164,28 +185,35 @@ __device__ __forceinline__ double warp_task(const IterArgs& a, int start, int co
 __global__ void __launch_bounds__(THREADS) k_iter(IterArgs a, const float* __restrict__ pr_old,
                                                   const float* __restrict__ con_old, float* __restrict__ pr_new,
                                                   float* __restrict__ con_new) {
+  extern __shared__ float4 s_dyn[];
+  float* s_hot = reinterpret_cast<float*>(s_dyn);
   __shared__ double s_red[THREADS / 32];
   __shared__ int s_last;
   if (a.st->done) return;
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   double my_diff = 0;
+  {
+    const float4* src = reinterpret_cast<const float4*>(con_old);
+    for (int i = tid; i < a.hot / 4; i += THREADS) s_dyn[i] = __ldg(src + i);
+    __syncthreads();
+  }
 
   for (int ci = blockIdx.x; ci < a.n_chunks; ci += gridDim.x) {
     const int4 c = a.chunks[ci];
     double acc = 0;
     {
-      int idx[IPT];
+      int idx[CIPT];
 #pragma unroll
-      for (int k = 0; k < IPT; ++k) {
+      for (int k = 0; k < CIPT; ++k) {
         int e = c.y + tid + k * THREADS;
         idx[k] = e < c.z ? __ldg(a.radj + e) : -1;
       }
-      float v[IPT];
+      float v[CIPT];
 #pragma unroll
-      for (int k = 0; k < IPT; ++k) v[k] = idx[k] >= 0 ? __ldg(con_old + idx[k]) : 0.0f;
+      for (int k = 0; k < CIPT; ++k) v[k] = idx[k] >= 0 ? gather(con_old, s_hot, a.hot, idx[k]) : 0.0f;
 #pragma unroll
-      for (int k = 0; k < IPT; ++k) acc += (double)v[k];
+      for (int k = 0; k < CIPT; ++k) acc += (double)v[k];
     }
     double tot = block_sum<THREADS>(acc, s_red);
     if (tid == 0) {
@@ -212,10 +240,10 @@ __global__ void __launch_bounds__(THREADS) k_iter(IterArgs a, const float* __res
   for (int t = blockIdx.x * (THREADS / 32) + (tid >> 5); t < a.n_tasks; t += warps_total) {
     const int4 task = a.tasks[t];  // {W, start, count, -}
     switch (task.x) {
-      case 32: my_diff += warp_task<32, 8>(a, task.y, task.z, lane, pr_old, con_old, pr_new, con_new); break;
-      case 8: my_diff += warp_task<8, 4>(a, task.y, task.z, lane, pr_old, con_old, pr_new, con_new); break;
-      case 4: my_diff += warp_task<4, 4>(a, task.y, task.z, lane, pr_old, con_old, pr_new, con_new); break;
-      default: my_diff += warp_task<1, 4>(a, task.y, task.z, lane, pr_old, con_old, pr_new, con_new); break;
+      case 32: my_diff += warp_task<32, 8>(a, task.y, task.z, lane, s_hot, pr_old, con_old, pr_new, con_new); break;
+      case 8: my_diff += warp_task<8, 4>(a, task.y, task.z, lane, s_hot, pr_old, con_old, pr_new, con_new); break;
+      case 4: my_diff += warp_task<4, 4>(a, task.y, task.z, lane, s_hot, pr_old, con_old, pr_new, con_new); break;
+      default: my_diff += warp_task<1, 4>(a, task.y, task.z, lane, s_hot, pr_old, con_old, pr_new, con_new); break;
     }
   }
 
@@ -244,13 +272,49 @@ __global__ void __launch_bounds__(THREADS) k_iter(IterArgs a, const float* __res
   }
 }
 
-__global__ void k_init(int V, const int32_t* __restrict__ off, float* __restrict__ pr, float* __restrict__ con,
+// ---- relabelling by out-degree (descending): the most gathered contrib values
+// share cache lines and stay resident in L1
+__global__ void k_deg_keys(int V, const int32_t* __restrict__ off, int32_t* __restrict__ key, int32_t* __restrict__ id) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    key[v] = -(off[v + 1] - off[v]);
+    id[v] = v;
+  }
+}
+
+__global__ void k_relabel_rows(int V, const int32_t* __restrict__ inv, const int32_t* __restrict__ skey,
+                               const int32_t* __restrict__ roff, int32_t* __restrict__ new_id, int32_t* __restrict__ od,
+                               int32_t* __restrict__ indeg) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < V; k += gridDim.x * blockDim.x) {
+    int v = inv[k];
+    new_id[v] = k;
+    od[k] = -skey[k];
+    indeg[k] = roff[v + 1] - roff[v];
+  }
+}
+
+__global__ void k_relabel_adj(int V, const int32_t* __restrict__ inv, const int32_t* __restrict__ new_id,
+                              const int32_t* __restrict__ roff, const int32_t* __restrict__ radj,
+                              const int32_t* __restrict__ roffp, int32_t* __restrict__ radjp) {
+  const int lane = threadIdx.x & 31;
+  for (int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < V; k += (gridDim.x * blockDim.x) >> 5) {
+    const int v = inv[k];
+    const int b = roff[v], n = roff[v + 1] - b, d = roffp[k];
+    for (int j = lane; j < n; j += 32) radjp[d + j] = new_id[radj[b + j]];
+  }
+}
+
+__global__ void k_unpermute(int V, const int32_t* __restrict__ new_id, const float* __restrict__ src,
+                            float* __restrict__ dst) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) dst[v] = src[new_id[v]];
+}
+
+__global__ void k_init(int V, const int32_t* __restrict__ odeg, float* __restrict__ pr, float* __restrict__ con,
                        State* st) {
   const float numNodes = (float)V;
   const float p0 = 1.0f / numNodes;
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
     pr[v] = p0;
-    int od = off[v + 1] - off[v];
+    int od = odeg[v];
     con[v] = od > 0 ? __fdiv_rn(p0, (float)od) : 0.0f;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -285,12 +349,60 @@ __global__ void k_plain_init(int V, float* pr) {
 
 }  // namespace pr
 
+// Relabel vertices by out-degree on the device: new_id, od, and the reverse CSR
+// in new ids (rows in new order, each row's in-neighbours in their original order).
+static int relabel(sp_graph* g, PrPlan* p) {
+  const int V = g->V;
+  cudaStream_t s = g->stream;
+  SP_TRY(p->new_id.alloc(V));
+  SP_TRY(p->od.alloc(V));
+  SP_TRY(p->roffp.alloc(V + 1));
+  SP_TRY(p->radjp.alloc(g->E));
+  SP_TRY(p->outbuf.alloc(V));
+  dbuf<int32_t> key, id, skey, inv, indeg;
+  SP_TRY(key.alloc(V));
+  SP_TRY(id.alloc(V));
+  SP_TRY(skey.alloc(V));
+  SP_TRY(inv.alloc(V));
+  SP_TRY(indeg.alloc(V + 1));
+  const int grid = num_sms() * 8;
+  pr::k_deg_keys<<<grid, 256, 0, s>>>(V, g->off.p, key.p, id.p);
+  SP_CHECK_LAUNCH();
+  size_t tb = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tb, key.p, skey.p, id.p, inv.p, V, 0, 32, s);
+  dbuf<unsigned char> tmp;
+  SP_TRY(tmp.alloc(tb));
+  cub::DeviceRadixSort::SortPairs(tmp.p, tb, key.p, skey.p, id.p, inv.p, V, 0, 32, s);
+  SP_CHECK_LAUNCH();
+  SP_CHECK_CUDA(cudaMemsetAsync(indeg.p + V, 0, sizeof(int32_t), s));
+  pr::k_relabel_rows<<<grid, 256, 0, s>>>(V, inv.p, skey.p, g->roff.p, p->new_id.p, p->od.p, indeg.p);
+  SP_CHECK_LAUNCH();
+  size_t sb = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, sb, indeg.p, p->roffp.p, V + 1, s);
+  dbuf<unsigned char> stmp;
+  SP_TRY(stmp.alloc(sb));
+  cub::DeviceScan::ExclusiveSum(stmp.p, sb, indeg.p, p->roffp.p, V + 1, s);
+  SP_CHECK_LAUNCH();
+  pr::k_relabel_adj<<<grid, 256, 0, s>>>(V, inv.p, p->new_id.p, g->roff.p, g->radj.p, p->roffp.p, p->radjp.p);
+  SP_CHECK_LAUNCH();
+  SP_CHECK_CUDA(cudaStreamSynchronize(s));
+  return SP_OK;
+}
+
 static int build_pr_plan(sp_graph* g) {
   if (g->pr) return SP_OK;
   SP_TRY(ensure_reverse(g));
   const int V = g->V;
+  PrPlan* p = new PrPlan();
+  {
+    int st = relabel(g, p);
+    if (st) {
+      free_pr_plan(p);
+      return st;
+    }
+  }
   std::vector<int32_t> roff(V + 1);
-  SP_CHECK_CUDA(cudaMemcpyAsync(roff.data(), g->roff.p, sizeof(int32_t) * (V + 1), cudaMemcpyDeviceToHost, g->stream));
+  SP_CHECK_CUDA(cudaMemcpyAsync(roff.data(), p->roffp.p, sizeof(int32_t) * (V + 1), cudaMemcpyDeviceToHost, g->stream));
   SP_CHECK_CUDA(cudaStreamSynchronize(g->stream));
   std::vector<int4> chunks;
   std::vector<int2> longs;
@@ -324,7 +436,6 @@ static int build_pr_plan(sp_graph* g) {
     for (int i = 0; i < (int)bin[k].size(); i += per)
       tasks.push_back(make_int4(widths[k], base + i, std::min(per, (int)bin[k].size() - i), 0));
   }
-  PrPlan* p = new PrPlan();
   p->n_chunks = (int)chunks.size();
   p->n_long = (int)longs.size();
   p->n_tasks = (int)tasks.size();
@@ -364,9 +475,9 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
   const int V = g->V;
   const int n_iter = std::max(1, (int)maxIter);
   pr::IterArgs a;
-  a.roff = g->roff.p;
-  a.radj = g->radj.p;
-  a.off = g->off.p;
+  a.roff = p->roffp.p;
+  a.radj = p->radjp.p;
+  a.od = p->od.p;
   a.chunks = p->chunks.p;
   a.longs = p->longs.p;
   a.long_ctr = p->long_ctr.p;
@@ -382,13 +493,19 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
   a.base = (1.0f - delta) / (float)V;
   a.beta = (double)beta;
   a.max_iter = n_iter;
+  int hot = g->pr_hot >= 0 ? g->pr_hot : pr::HOT_DEFAULT;
+  hot = std::min(hot, V) & ~3;
+  a.hot = hot;
+  const size_t dyn = std::max<size_t>(16, sizeof(float) * (size_t)hot);
+  SP_CHECK_CUDA(cudaFuncSetAttribute(pr::k_iter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
   int per_sm = 0;
-  SP_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pr::k_iter, pr::THREADS, 0));
+  SP_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pr::k_iter, pr::THREADS, dyn));
   const int grid = std::max(1, std::min(num_sms() * 32, num_sms() * std::max(1, per_sm)));
 
-  pr::k_init<<<num_sms() * 4, 256, 0, s>>>(V, g->off.p, p->prb[0].p, p->con[0].p, p->state.p);
+  pr::k_init<<<num_sms() * 4, 256, 0, s>>>(V, p->od.p, p->prb[0].p, p->con[0].p, p->state.p);
   SP_CHECK_LAUNCH();
-  if (!(p->exec && p->exec_iters == n_iter && p->exec_beta == beta && p->exec_delta == delta && p->exec_stream == s))  {
+  if (!(p->exec && p->exec_iters == n_iter && p->exec_beta == beta && p->exec_delta == delta && p->exec_stream == s &&
+        p->exec_hot == hot)) {
     if (p->exec) {
       cudaGraphExecDestroy(p->exec);
       p->exec = nullptr;
@@ -397,7 +514,7 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
     SP_CHECK_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < n_iter; ++k) {
       int c = k & 1, n = c ^ 1;
-      pr::k_iter<<<grid, pr::THREADS, 0, s>>>(a, p->prb[c].p, p->con[c].p, p->prb[n].p, p->con[n].p);
+      pr::k_iter<<<grid, pr::THREADS, dyn, s>>>(a, p->prb[c].p, p->con[c].p, p->prb[n].p, p->con[n].p);
     }
     cudaError_t ce = cudaStreamEndCapture(s, &graph);
     if (ce != cudaSuccess) {
@@ -415,12 +532,17 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
     p->exec_beta = beta;
     p->exec_delta = delta;
     p->exec_stream = s;
+    p->exec_hot = hot;
   }
   SP_CHECK_CUDA(cudaGraphLaunch(p->exec, s));
   g_launches.fetch_add(n_iter);
   pr::State hs;
   SP_TRY(copy_out(&hs, p->state.p, sizeof(hs), s));
-  if (out) SP_TRY(copy_out(out, p->prb[hs.iter & 1].p, sizeof(float) * V, s));
+  if (out) {
+    pr::k_unpermute<<<num_sms() * 4, 256, 0, s>>>(V, p->new_id.p, p->prb[hs.iter & 1].p, p->outbuf.p);
+    SP_CHECK_LAUNCH();
+    SP_TRY(copy_out(out, p->outbuf.p, sizeof(float) * V, s));
+  }
   if (iters) *iters = hs.iter;
   if (fdiff) *fdiff = hs.diff;
   return SP_OK;

@@ -56,6 +56,21 @@ def test_pagerank_undirected(gi):
     _pr_check(g, _lib.SP_PR_TUNED)
 
 
+@pytest.mark.parametrize("hot", [0, 4, 1000, 57344])
+def test_pagerank_hot_table_knob_is_exact(hot):
+    # the knob only moves where contrib values are read from: results are bitwise equal
+    g = directed_zoo()[1]
+    g.ensure_reverse()
+    dg = device_graph(g)
+    dg.tune_set("pr.hot", 0)
+    base, it0, _ = dg.pagerank(1e-6, 0.85, 100)
+    dg.tune_set("pr.hot", hot)
+    assert dg.tune_get("pr.hot") == hot
+    out, it1, _ = dg.pagerank(1e-6, 0.85, 100)
+    dg.tune_set("pr.hot", 0)
+    assert it0 == it1 and np.array_equal(base, out)
+
+
 def test_pagerank_degree_bin_boundaries():
     from graphs import from_pairs
     # rows on every degree-bin boundary (4/5, 16/17, 32/33, 2048/2049) and multi-chunk hubs
