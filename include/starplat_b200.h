@@ -64,7 +64,9 @@ int sp_graph_info(sp_graph_h g, int32_t* V, int64_t* E, int32_t* symmetric);
 /* Schedule knobs (what the autotuner and the learned scheduler set); results never
  * depend on them. Unknown keys: SP_ERR_INVALID.
  *   "pr.hot"  PageRank: number of highest-out-degree vertices whose contrib values each
- *             CTA stages in shared memory per iteration (0..57344, default 0). */
+ *             CTA stages in shared memory per iteration (0..57344, default 0).
+ *   "sssp.delta"  SSSP bucket width used when sp_sssp gets delta <= 0 (0 = the largest
+ *             edge weight). */
 int sp_tune_set(sp_graph_h g, const char* key, int64_t value);
 int sp_tune_get(sp_graph_h g, const char* key, int64_t* value);
 
@@ -85,6 +87,20 @@ int sp_tc(sp_graph_h g, int64_t* triangle_count);
 #define SP_PR_PLAIN 1
 int sp_pagerank(sp_graph_h g, float beta, float delta, int32_t maxIter, float* pageRank,
                 int32_t* iterations, double* final_diff, int32_t variant);
+
+/* ---- single-source shortest paths --------------------------------------------
+ * Replaces generated `void Compute_SSSP(graph& g, int* dist, int* weight, int src)`
+ * (DSL staticDSLCodes/sssp_dslV3:1-26). weight[E] in forward-CSR order (the drivers
+ * fill it that way, main_functions/sssp_dslv2main.cpp:33-41); NULL = the graph's edgeLen.
+ * dist[v] = exact shortest distance, INT_MAX when unreachable. Negative weights are
+ * allowed without negative cycles (SP_ERR_NEG_CYCLE otherwise).
+ * SP_SSSP_DELTA: delta-stepping in one persistent kernel; delta <= 0 picks the tuned /
+ * default bucket width. SP_SSSP_PLAIN: the generated code's topology-driven form.
+ * rounds (may be NULL) receives the number of relaxation rounds. */
+#define SP_SSSP_DELTA 0
+#define SP_SSSP_PLAIN 1
+int sp_sssp(sp_graph_h g, const int32_t* weight, int32_t src, int32_t* dist, int64_t delta, int32_t variant,
+            int32_t* rounds);
 
 #ifdef __cplusplus
 }

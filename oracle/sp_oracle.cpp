@@ -224,7 +224,7 @@ int32_t or_sssp(int32_t V, const int32_t* off, const int32_t* adj, const int32_t
     for (int32_t e = off[v]; e < off[v + 1]; ++e) {
       int32_t u = adj[e];
       int64_t nd = dv + w[e];
-      if (nd < d[u]) {
+      if (nd < d[u] && nd < INT_MAX) {  // a sum reaching INT_MAX is never stored
         d[u] = nd;
         pq.push({nd, u});
       }
@@ -254,7 +254,7 @@ int32_t or_sssp_bf(int32_t V, const int32_t* off, const int32_t* adj, const int3
     for (int32_t e = off[v]; e < off[v + 1]; ++e) {
       int32_t u = adj[e];
       int64_t nd = (int64_t)dist[v] + w[e];
-      if (nd < dist[u]) {
+      if (nd < dist[u] && nd < INT_MAX) {
         dist[u] = (int32_t)nd;
         if (!inq[u]) {
           inq[u] = 1;

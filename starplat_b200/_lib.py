@@ -24,6 +24,8 @@ SP_ERR = {
 SP_GRAPH_DEVICE_PTRS = 0x1
 SP_PR_TUNED = 0
 SP_PR_PLAIN = 1
+SP_SSSP_DELTA = 0
+SP_SSSP_PLAIN = 1
 
 _L = None
 
@@ -54,6 +56,7 @@ SIGNATURES = {
     "sp_tune_get": (ctypes.c_int, [vp, ctypes.c_char_p, P(i64)]),
     "sp_tc": (ctypes.c_int, [vp, P(i64)]),
     "sp_pagerank": (ctypes.c_int, [vp, f32, f32, i32, vp, P(i32), P(f64), i32]),
+    "sp_sssp": (ctypes.c_int, [vp, vp, i32, vp, i64, i32, P(i32)]),
 }
 
 

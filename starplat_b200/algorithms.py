@@ -41,3 +41,9 @@ def ComputePageRank(g: CSRGraph, beta: float, delta: float, maxIter: int, pageRa
 
 
 Compute_PR = ComputePageRank  # the V2 DSL's name, same parameters
+
+
+def Compute_SSSP(g: CSRGraph, dist: np.ndarray, weight: np.ndarray, src: int) -> None:
+    """staticDSLCodes/sssp_dslV3: fills int dist[num_nodes()] (INT_MAX = unreachable);
+    weight is int[E] in forward-CSR order, as the reference drivers build it."""
+    device_graph(g).sssp(src, weight=weight, out=dist)

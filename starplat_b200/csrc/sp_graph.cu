@@ -302,6 +302,14 @@ int sp_tune_set(sp_graph_h g, const char* key, int64_t value) {
     g->pr_hot = (int32_t)value;
     return SP_OK;
   }
+  if (!strcmp(key, "sssp.delta")) {
+    if (value < 0) {
+      set_error("sp_tune_set: sssp.delta must be >= 0");
+      return SP_ERR_INVALID;
+    }
+    g->sssp_delta = value;
+    return SP_OK;
+  }
   set_error("sp_tune_set: unknown key '%s'", key);
   return SP_ERR_INVALID;
 }
@@ -313,6 +321,10 @@ int sp_tune_get(sp_graph_h g, const char* key, int64_t* value) {
   }
   if (!strcmp(key, "pr.hot")) {
     *value = g->pr_hot >= 0 ? g->pr_hot : 0;
+    return SP_OK;
+  }
+  if (!strcmp(key, "sssp.delta")) {
+    *value = g->sssp_delta;
     return SP_OK;
   }
   set_error("sp_tune_get: unknown key '%s'", key);

@@ -5,6 +5,7 @@
 #include <atomic>
 #include <cstdint>
 #include <cstdio>
+#include <algorithm>
 #include <string>
 
 #include "../../include/starplat_b200.h"
@@ -99,6 +100,7 @@ struct sp_graph {
   int symmetric = -1;      // -1 unknown, 0/1
   int32_t max_out_deg = -1;
   int32_t pr_hot = -1;  // PageRank: contrib values staged in shared memory (-1 = default)
+  int64_t sssp_delta = 0;  // SSSP bucket width (0 = max edge weight)
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   sp::PrPlan* pr = nullptr;

@@ -493,7 +493,7 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
   a.base = (1.0f - delta) / (float)V;
   a.beta = (double)beta;
   a.max_iter = n_iter;
-  int hot = g->pr_hot >= 0 ? g->pr_hot : pr::HOT_DEFAULT;
+  int hot = std::min(g->pr_hot >= 0 ? g->pr_hot : pr::HOT_DEFAULT, pr::HOT_MAX);
   hot = std::min(hot, V) & ~3;
   a.hot = hot;
   const size_t dyn = std::max<size_t>(16, sizeof(float) * (size_t)hot);

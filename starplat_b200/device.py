@@ -125,3 +125,15 @@ class DeviceGraph:
         check("sp_pagerank", lib().sp_pagerank(self.handle, beta, delta, max_iter, _ptr(out), ctypes.byref(it),
                                                ctypes.byref(diff), variant))
         return out, int(it.value), float(diff.value)
+
+    def sssp(self, src: int, weight=None, out=None, delta: int = 0, variant: int = _lib.SP_SSSP_DELTA):
+        """Exact int32 distances from src (INT_MAX = unreachable). weight: int32[E] in
+        forward-CSR order, host or device; None uses the graph's edgeLen."""
+        if out is None:
+            out = np.empty(self.V, np.int32)
+        if weight is not None and str(weight.dtype) not in ("int32", "torch.int32"):
+            raise TypeError("weights must be int32")
+        rounds = ctypes.c_int32()
+        check("sp_sssp", lib().sp_sssp(self.handle, _ptr(weight), int(src), _ptr(out), int(delta), variant,
+                                       ctypes.byref(rounds)))
+        return out, int(rounds.value)

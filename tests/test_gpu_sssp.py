@@ -1,0 +1,125 @@
+"""GPU parity: SSSP distances are bit-exact against the oracle (Dijkstra, or
+queue Bellman-Ford when weights are negative), for every schedule (delta) and
+both variants."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from starplat_b200 import _lib
+from starplat_b200 import generators as G
+from starplat_b200.algorithms import Compute_SSSP, device_graph
+from starplat_b200.device import DeviceGraph
+
+from graphs import directed_zoo, from_pairs, undirected_zoo
+
+pytestmark = pytest.mark.gpu
+INT_MAX = np.iinfo(np.int32).max
+
+
+def weighted(g, lo, hi, seed=3, symmetric=None):
+    if symmetric is None:
+        symmetric = g.is_symmetric()
+    g.edgeLen = G.hash_weights(g, seed, lo, hi, symmetric)
+    return g
+
+
+def check(g, src, **kw):
+    dg = device_graph(g)
+    out, rounds = dg.sssp(src, **kw)
+    ref = O.sssp(g.indexofNodes, g.edgeList, g.edgeLen, src)
+    assert np.array_equal(out, ref), (g.name, src, int((out != ref).sum()))
+    return rounds
+
+
+@pytest.mark.parametrize("gi", range(4))
+def test_sssp_directed(gi):
+    g = weighted(directed_zoo()[gi], 1, 100)
+    for src in G.pick_sources(g, 3, seed=gi):
+        check(g, int(src))
+
+
+@pytest.mark.parametrize("gi", range(8))
+def test_sssp_undirected(gi):
+    g = weighted(undirected_zoo()[gi], 1, 1000)
+    check(g, 0)
+    check(g, g.V - 1)
+
+
+@pytest.mark.parametrize("delta", [1, 3, 50, 1000, 10**6, 2**31 - 1])
+def test_sssp_any_delta_is_exact(delta):
+    g = weighted(G.rmat(12, 16, seed=5, directed=True), 1, 100)
+    check(g, int(G.pick_sources(g, 1, seed=1)[0]), delta=delta)
+    gg = weighted(G.grid(40, 50), 1, 1000)
+    check(gg, 0, delta=delta)
+
+
+def test_sssp_tuned_delta_knob():
+    g = weighted(G.grid(30, 30), 1, 1000)
+    dg = device_graph(g)
+    for d in (0, 17, 5000):
+        dg.tune_set("sssp.delta", d)
+        assert dg.tune_get("sssp.delta") == d
+        check(g, 5)
+    dg.tune_set("sssp.delta", 0)
+
+
+def test_sssp_plain_variant():
+    for g in (weighted(G.rmat(11, 8, seed=3, directed=True), 1, 100), weighted(G.grid(20, 20), 1, 1000)):
+        check(g, 0, variant=_lib.SP_SSSP_PLAIN)
+
+
+def test_sssp_unreachable_and_zero_weights():
+    g = from_pairs(7, [[0, 1], [1, 2], [2, 3], [4, 5]], name="chain")
+    g.edgeLen = np.zeros(g.E, np.int32)
+    out, _ = device_graph(g).sssp(0)
+    assert out.tolist() == [0, 0, 0, 0, INT_MAX, INT_MAX, INT_MAX]
+    out, _ = device_graph(g).sssp(6)  # isolated source
+    assert out.tolist() == [INT_MAX] * 6 + [0]
+
+
+def test_sssp_negative_weights_and_cycle():
+    # a DAG with negative weights: exact via the queue Bellman-Ford oracle
+    rng = np.random.default_rng(1)
+    n = 300
+    pairs = np.array([(i, j) for i in range(n) for j in rng.choice(n, 4) if i < j], np.int32)
+    g = from_pairs(n, pairs, name="dag")
+    g.edgeLen = rng.integers(-50, 100, g.E).astype(np.int32)
+    check(g, 0)
+    # a reachable negative cycle has no fixed point
+    c = from_pairs(3, [[0, 1], [1, 2], [2, 0]], name="negcycle")
+    c.edgeLen = np.array([1, -5, 1], np.int32)
+    with pytest.raises(_lib.SPError) as ei:
+        device_graph(c).sssp(0)
+    assert ei.value.status == -6
+
+
+def test_sssp_large_weights_no_overflow():
+    # 2^30 + (2^30 - 1) = INT_MAX: a sum reaching INT_MAX is never stored (the
+    # reference's `dist[nbr] > dist_new` test fails there too), so 2 and 3 stay unreachable
+    g = from_pairs(4, [[0, 1], [1, 2], [2, 3]], name="big")
+    g.edgeLen = np.array([2**30, 2**30 - 1, 2**30], np.int32)
+    out, _ = device_graph(g).sssp(0)
+    assert out.tolist() == [0, 2**30, INT_MAX, INT_MAX]
+    assert np.array_equal(out, O.sssp(g.indexofNodes, g.edgeList, g.edgeLen, 0))
+
+
+def test_sssp_entry_point_and_device_weights():
+    import torch
+
+    g = weighted(G.rmat(11, 16, seed=8, directed=True), 1, 100)
+    w = g.edgeLen.copy()
+    g.edgeLen = None  # weights passed per call, as the generated signature does
+    dist = np.zeros(g.V, np.int32)
+    Compute_SSSP(g, dist, w, 3)
+    assert np.array_equal(dist, O.sssp(g.indexofNodes, g.edgeList, w, 3))
+    t = [torch.from_numpy(a).cuda() for a in (g.indexofNodes, g.edgeList)]
+    with DeviceGraph(t[0], t[1]) as dg:
+        out = torch.empty(g.V, dtype=torch.int32, device="cuda")
+        dg.sssp(3, weight=torch.from_numpy(w).cuda(), out=out)
+        assert np.array_equal(out.cpu().numpy(), dist)
+
+
+def test_sssp_bad_source():
+    g = weighted(G.grid(5, 5), 1, 10)
+    with pytest.raises(_lib.SPError):
+        device_graph(g).sssp(25)
