@@ -66,7 +66,8 @@ int sp_graph_info(sp_graph_h g, int32_t* V, int64_t* E, int32_t* symmetric);
  *   "pr.hot"  PageRank: number of highest-out-degree vertices whose contrib values each
  *             CTA stages in shared memory per iteration (0..57344, default 0).
  *   "sssp.delta"  SSSP bucket width used when sp_sssp gets delta <= 0 (0 = the largest
- *             edge weight). */
+ *             edge weight).
+ *   "bc.batch"  BC: sources traversed together in one multi-source pass (1..64, default 64). */
 int sp_tune_set(sp_graph_h g, const char* key, int64_t value);
 int sp_tune_get(sp_graph_h g, const char* key, int64_t* value);
 
@@ -101,6 +102,35 @@ int sp_pagerank(sp_graph_h g, float beta, float delta, int32_t maxIter, float* p
 #define SP_SSSP_PLAIN 1
 int sp_sssp(sp_graph_h g, const int32_t* weight, int32_t src, int32_t* dist, int64_t delta, int32_t variant,
             int32_t* rounds);
+
+/* ---- betweenness centrality ----------------------------------------------------
+ * Replaces generated `void Compute_BC(graph& g, float* BC, std::set<int>& sourceSet)`
+ * (DSL staticDSLCodes/bc_dslV2:1-21): Brandes over the given distinct sources,
+ * BC[v] = sum over sources s != v of the dependency delta_s[v] (no halving, as the
+ * generated code). sigma is FP64 (exact below 2^53), dependencies FP32 stored /
+ * FP64 summed, BC accumulated in FP64 and written as float.
+ * SP_BC_BATCHED: multi-source traversal, 64 sources per pass, one persistent launch.
+ * SP_BC_PLAIN: one source at a time, one thread per vertex per level (the manual /
+ * generated CUDA form). */
+#define SP_BC_BATCHED 0
+#define SP_BC_PLAIN 1
+int sp_bc(sp_graph_h g, const int32_t* sources, int32_t nsrc, float* BC, int32_t variant);
+
+/* The forward half of the same multi-source pass: BFS levels (-1 = unreached) and
+ * shortest-path counts (FP64) from up to 64 distinct sources, written source-major:
+ * level[k*V + v], sigma[k*V + v]. Same level-synchronous BFS the generated code runs
+ * (backend_omp/dsl_cpp_generator.cpp:64-193) with sigma of bc_dslV2:8-11. */
+int sp_bfs_sigma(sp_graph_h g, const int32_t* sources, int32_t nsrc, int32_t* level, double* sigma);
+
+/* Many independent graphs stored as one graph whose vertex ranges
+ * [vertex_offset[k], vertex_offset[k+1]) have no edges between them; graph k's
+ * sources are sources[source_offset[k] .. source_offset[k+1]) (global ids).
+ * BC[V] gets every graph's centrality. One persistent launch, one CTA per graph
+ * (largest first), no per-graph host round trip. No counterpart in the generated
+ * code (it handles one graph per call); the per-graph result equals sp_bc on that
+ * graph alone. */
+int sp_bc_graphs(sp_graph_h g, int32_t ngraphs, const int32_t* vertex_offset, const int32_t* source_offset,
+                 const int32_t* sources, float* BC);
 
 #ifdef __cplusplus
 }

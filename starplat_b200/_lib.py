@@ -26,6 +26,8 @@ SP_PR_TUNED = 0
 SP_PR_PLAIN = 1
 SP_SSSP_DELTA = 0
 SP_SSSP_PLAIN = 1
+SP_BC_BATCHED = 0
+SP_BC_PLAIN = 1
 
 _L = None
 
@@ -57,6 +59,9 @@ SIGNATURES = {
     "sp_tc": (ctypes.c_int, [vp, P(i64)]),
     "sp_pagerank": (ctypes.c_int, [vp, f32, f32, i32, vp, P(i32), P(f64), i32]),
     "sp_sssp": (ctypes.c_int, [vp, vp, i32, vp, i64, i32, P(i32)]),
+    "sp_bc": (ctypes.c_int, [vp, vp, i32, vp, i32]),
+    "sp_bc_graphs": (ctypes.c_int, [vp, i32, vp, vp, vp, vp]),
+    "sp_bfs_sigma": (ctypes.c_int, [vp, vp, i32, vp, vp]),
 }
 
 

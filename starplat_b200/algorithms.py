@@ -47,3 +47,10 @@ def Compute_SSSP(g: CSRGraph, dist: np.ndarray, weight: np.ndarray, src: int) ->
     """staticDSLCodes/sssp_dslV3: fills int dist[num_nodes()] (INT_MAX = unreachable);
     weight is int[E] in forward-CSR order, as the reference drivers build it."""
     device_graph(g).sssp(src, weight=weight, out=dist)
+
+
+def Compute_BC(g: CSRGraph, BC: np.ndarray, sourceSet) -> None:
+    """staticDSLCodes/bc_dslV2: fills float BC[num_nodes()] over the sources in
+    sourceSet (any iterable of distinct vertex ids, like the reference's std::set<int>)."""
+    src = np.array(sorted(set(int(s) for s in sourceSet)), np.int32)
+    device_graph(g).bc(src, out=BC)

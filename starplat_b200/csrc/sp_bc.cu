@@ -1,5 +1,709 @@
+// Brandes betweenness centrality for sm_100a.
+//
+// Semantics: DSL staticDSLCodes/bc_dslV2:1-21 as emitted by the OpenMP generator
+// (BFS + reverse sweep backend_omp/dsl_cpp_generator.cpp:64-193, level guard
+// bfsDist[w]==bfsDist[v]+1 :1458-1495; bfsDist injected by
+// SymbolTableBuilder.cpp:617-633): for every source s, a level-synchronous BFS over
+// out-neighbours counts shortest paths sigma, then levels are walked backwards with
+//   delta[v] = sum_{w in N(v), level(w) = level(v)+1} sigma[v]/sigma[w] * (1 + delta[w])
+// and BC[v] += delta[v] for every reached v != s (the reverse loop stops at phase 1,
+// so the source is excluded; no halving — the manual CUDA BC bcManualv5.cu:104
+// halves, the generated code does not).
+//
+// B200 design — multi-source traversal (many sources share one pass over the edges):
+//  * up to 32*NW sources per batch; per vertex a 64-bit mask says for which sources
+//    of the batch it sits in the current frontier; sigma[v][b] (FP64, exact path
+//    counts below 2^53) and delta[v][b] (FP32) are vertex-major, so the per-source
+//    updates of one edge are coalesced across the warp's lanes;
+//  * forward level d: lanes walk a frontier vertex's edges; q = mask & ~seen[w] are
+//    the sources that reach w first at level d+1; atomicOr marks them, the first
+//    marker appends w to the level list, then lanes (one per source bit) add
+//    sigma with FP64 atomics (integer-valued, so the sum is exact in any order);
+//  * backward level d: the masks of level d+1 are scattered into a dense array; for
+//    each (v, mask) of level d the lanes pull sigma/delta of the successors in edge
+//    order — no atomics, deterministic;
+//  * BC accumulates per vertex over the batch's sources in source order (FP64).
+// One cooperative launch runs every batch of a graph (bounded grid barriers); the
+// many-small-graphs form runs one CTA per graph in a persistent launch with a
+// work queue (largest graphs first) and block-level barriers.
+#include <climits>
+#include <vector>
+
 #include "sp_internal.cuh"
+#include "sp_sync.cuh"
+
 namespace sp {
-struct BcPlan {};
+
+namespace bc {
+constexpr int GRID_THREADS = 256;
+constexpr int CTA_THREADS = 512;
+
+struct Work {
+  const int32_t* __restrict__ off;  // CSR rows of this graph (global edge indices)
+  const int32_t* __restrict__ adj;  // neighbour ids (subtract vbase for local ids)
+  int vbase;                        // first vertex id of this graph in adj
+  int V;                            // vertices of this graph
+  double* sigma;                    // [V][SW]
+  float* delta;                     // [V][SW]
+  unsigned long long* seen;         // [V]
+  unsigned long long* nxt;          // [V]
+  unsigned long long* dense;        // [V]
+  int32_t* flv;                     // [cap] level-list vertices (local ids)
+  unsigned long long* flm;          // [cap] level-list masks
+  int cap;
+  int* lo;                          // [maxd + 2] level starts in the lists
+  int maxd;
+  int* cnt;                         // append counter
+  double* bc;                       // [V] FP64 accumulator (local ids)
+  int* err;                         // 1 list overflow, 2 too deep, 3 barrier timeout
+};
+
+struct GridSync {
+  GridBar* bar;
+  __device__ __forceinline__ bool sync() { return grid_barrier(bar); }
+  __device__ __forceinline__ int tid() const { return blockIdx.x * blockDim.x + threadIdx.x; }
+  __device__ __forceinline__ int nthreads() const { return gridDim.x * blockDim.x; }
+};
+
+struct BlockSync {
+  __device__ __forceinline__ bool sync() {
+    __syncthreads();
+    return true;
+  }
+  __device__ __forceinline__ int tid() const { return threadIdx.x; }
+  __device__ __forceinline__ int nthreads() const { return blockDim.x; }
+};
+
+__device__ __forceinline__ unsigned long long shfl64(unsigned long long x, int l) {
+  unsigned lo = __shfl_sync(0xffffffffu, (unsigned)x, l);
+  unsigned hi = __shfl_sync(0xffffffffu, (unsigned)(x >> 32), l);
+  return ((unsigned long long)hi << 32) | lo;
+}
+
+template <int NW>
+__device__ void expand_entry(const Work& W, int i, int lane) {
+  constexpr int SW = 32 * NW;
+  const int v = W.flv[i];
+  const unsigned long long m = W.flm[i];
+  double sv[NW];
+#pragma unroll
+  for (int k = 0; k < NW; ++k) {
+    const int b = lane + 32 * k;
+    sv[k] = ((m >> b) & 1ull) ? W.sigma[(size_t)v * SW + b] : 0.0;
+  }
+  const int eb = W.off[v], ee = W.off[v + 1];
+  for (int c = eb; c < ee; c += 32) {
+    const int j = c + lane;
+    int w = 0;
+    unsigned long long q = 0;
+    bool isnew = false;
+    if (j < ee) {
+      w = W.adj[j] - W.vbase;
+      q = m & ~W.seen[w];
+      if (q) isnew = atomicOr(&W.nxt[w], q) == 0ull;
+    }
+    const unsigned nm = __ballot_sync(0xffffffffu, isnew);
+    if (nm) {
+      int base = 0;
+      const int leader = __ffs(nm) - 1;
+      if (lane == leader) base = atomicAdd(W.cnt, __popc(nm));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      const int pos = base + __popc(nm & ((1u << lane) - 1u));
+      if (isnew) {
+        if (pos < W.cap)
+          W.flv[pos] = w;
+        else
+          atomicExch(W.err, 1);
+      }
+    }
+    unsigned em = __ballot_sync(0xffffffffu, q != 0ull);
+    while (em) {
+      const int l = __ffs(em) - 1;
+      em &= em - 1;
+      const unsigned long long ql = shfl64(q, l);
+      const int wl = __shfl_sync(0xffffffffu, w, l);
+#pragma unroll
+      for (int k = 0; k < NW; ++k) {
+        const int b = lane + 32 * k;
+        if ((ql >> b) & 1ull) atomicAdd(&W.sigma[(size_t)wl * SW + b], sv[k]);
+      }
+    }
+  }
+}
+
+template <int NW>
+__device__ void backward_entry(const Work& W, int i, int lane) {
+  constexpr int SW = 32 * NW;
+  const int v = W.flv[i];
+  const unsigned long long m = W.flm[i];
+  double sv[NW], acc[NW];
+#pragma unroll
+  for (int k = 0; k < NW; ++k) {
+    const int b = lane + 32 * k;
+    sv[k] = ((m >> b) & 1ull) ? W.sigma[(size_t)v * SW + b] : 0.0;
+    acc[k] = 0.0;
+  }
+  const int eb = W.off[v], ee = W.off[v + 1];
+  for (int c = eb; c < ee; c += 32) {
+    const int j = c + lane;
+    int w = 0;
+    unsigned long long s = 0;
+    if (j < ee) {
+      w = W.adj[j] - W.vbase;
+      s = m & W.dense[w];
+    }
+    unsigned em = __ballot_sync(0xffffffffu, s != 0ull);
+    while (em) {
+      const int l = __ffs(em) - 1;
+      em &= em - 1;
+      const unsigned long long sl = shfl64(s, l);
+      const int wl = __shfl_sync(0xffffffffu, w, l);
+#pragma unroll
+      for (int k = 0; k < NW; ++k) {
+        const int b = lane + 32 * k;
+        if ((sl >> b) & 1ull) {
+          const size_t x = (size_t)wl * SW + b;
+          acc[k] += sv[k] / W.sigma[x] * (1.0 + (double)W.delta[x]);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < NW; ++k) {
+    const int b = lane + 32 * k;
+    if ((m >> b) & 1ull) W.delta[(size_t)v * SW + b] = (float)acc[k];
+  }
+}
+
+// One batch of nsrc (<= 32*NW) sources (local ids). Every participating thread
+// calls this with the same arguments; S provides the barrier and thread ranks.
+template <int NW, class S>
+__device__ bool run_batch(const Work& W, const int32_t* srcs, int nsrc, S& sync, int32_t* lvl_out = nullptr,
+                          double* sig_out = nullptr) {
+  constexpr int SW = 32 * NW;
+  const int gt = sync.tid(), nt = sync.nthreads();
+  const int lane = threadIdx.x & 31;
+  const int gw = gt >> 5, nw = nt >> 5;
+  for (int k = gt; k < nsrc; k += nt) {
+    const int v = srcs[k];
+    W.flv[k] = v;
+    W.flm[k] = 1ull << k;
+    W.sigma[(size_t)v * SW + k] = 1.0;
+    atomicOr(&W.seen[v], 1ull << k);
+  }
+  if (gt == 0) {
+    W.lo[0] = 0;
+    W.lo[1] = nsrc;
+    *W.cnt = nsrc;
+  }
+  if (!sync.sync()) return false;
+  int d = 0;
+  while (true) {
+    const int b = *(volatile int*)&W.lo[d], e = *(volatile int*)&W.lo[d + 1];
+    if (b == e) break;
+    if (d + 2 > W.maxd) {
+      if (gt == 0) atomicExch(W.err, 2);
+      return false;
+    }
+    for (int i = b + gw; i < e; i += nw) expand_entry<NW>(W, i, lane);
+    if (!sync.sync()) return false;
+    const int c = min(*(volatile int*)W.cnt, W.cap);
+    for (int i = e + gt; i < c; i += nt) {
+      const int w = W.flv[i];
+      const unsigned long long mk = W.nxt[w];
+      W.flm[i] = mk;
+      W.seen[w] |= mk;
+      W.nxt[w] = 0ull;
+    }
+    if (gt == 0) W.lo[d + 2] = c;
+    if (!sync.sync()) return false;
+    if (*(volatile int*)W.err) return false;
+    ++d;
+  }
+  const int D = d;  // levels 0..D-1 are non-empty
+  if (lvl_out) {
+    // forward only: BFS level and path count of every (source, vertex), source-major
+    for (int i = gt; i < W.lo[D]; i += nt) {
+      const int v = W.flv[i];
+      const unsigned long long mk = W.flm[i];
+      int lev = 0;
+      while (W.lo[lev + 1] <= i) ++lev;
+      for (int k = 0; k < nsrc; ++k)
+        if ((mk >> k) & 1ull) {
+          lvl_out[(size_t)k * W.V + v] = lev;
+          sig_out[(size_t)k * W.V + v] = W.sigma[(size_t)v * SW + k];
+        }
+    }
+    if (!sync.sync()) return false;
+  }
+  for (d = (lvl_out ? 0 : D - 1); d >= 1; --d) {
+    const int b1 = W.lo[d + 1], e1 = W.lo[d + 2];
+    for (int i = b1 + gt; i < e1; i += nt) W.dense[W.flv[i]] = W.flm[i];
+    if (!sync.sync()) return false;
+    const int b0 = W.lo[d], e0 = W.lo[d + 1];
+    for (int i = b0 + gw; i < e0; i += nw) backward_entry<NW>(W, i, lane);
+    if (!sync.sync()) return false;
+    for (int i = b1 + gt; i < e1; i += nt) W.dense[W.flv[i]] = 0ull;
+    if (!sync.sync()) return false;
+  }
+  // accumulate in source order, then reset the batch state
+  for (int v = gt; v < W.V; v += nt) {
+    double s = 0;
+    const size_t r = (size_t)v * SW;
+    for (int k = 0; k < nsrc; ++k) {
+      s += (double)W.delta[r + k];
+      W.delta[r + k] = 0.0f;
+      W.sigma[r + k] = 0.0;
+    }
+    W.bc[v] += s;
+    W.seen[v] = 0ull;
+  }
+  return sync.sync();
+}
+
+struct GridArgs {
+  Work W;
+  const int32_t* srcs;
+  int nsrc;
+  int batch;  // sources per batch (<= 32*NW)
+  GridBar* bar;
+  int32_t* lvl_out;  // forward-only mode (one batch): levels and sigma, source-major
+  double* sig_out;
+};
+
+template <int NW>
+__global__ void __launch_bounds__(GRID_THREADS) k_bc_grid(GridArgs a) {
+  GridSync gs{a.bar};
+  for (int s0 = 0; s0 < a.nsrc; s0 += a.batch) {
+    if (!run_batch<NW>(a.W, a.srcs + s0, min(a.batch, a.nsrc - s0), gs, a.lvl_out, a.sig_out)) {
+      if (threadIdx.x == 0 && a.bar->error) atomicCAS(a.W.err, 0, 3);
+      return;
+    }
+  }
+}
+
+// ---- many small graphs: one CTA per graph, persistent, work queue
+struct GraphsArgs {
+  const int32_t* off;     // union CSR rows
+  const int32_t* adj;     // union CSR neighbours (global ids)
+  const int32_t* voff;    // [G+1] vertex ranges
+  const int32_t* soff;    // [G+1] source ranges
+  const int32_t* srcs;    // global source ids
+  const int32_t* order;   // graphs, largest first
+  int G;
+  int* next;              // work-queue counter
+  // per-CTA scratch (sized for the largest graph)
+  double* sigma;
+  float* delta;
+  unsigned long long* masks;  // 3 * vmax per CTA
+  int32_t* flv;
+  unsigned long long* flm;
+  int* lo;
+  int* cnt;
+  double* bc;             // [Vtot] FP64 accumulator (global ids)
+  int vmax, cap, maxd;
+  int* err;
+};
+
+template <int NW>
+__global__ void __launch_bounds__(CTA_THREADS) k_bc_graphs(GraphsArgs a) {
+  constexpr int SW = 32 * NW;
+  __shared__ int s_g;
+  __shared__ int32_t s_src[SW];
+  BlockSync bs;
+  const int slot = blockIdx.x;
+  Work W;
+  W.sigma = a.sigma + (size_t)slot * a.vmax * SW;
+  W.delta = a.delta + (size_t)slot * a.vmax * SW;
+  W.seen = a.masks + (size_t)slot * a.vmax * 3;
+  W.nxt = W.seen + a.vmax;
+  W.dense = W.nxt + a.vmax;
+  W.flv = a.flv + (size_t)slot * a.cap;
+  W.flm = a.flm + (size_t)slot * a.cap;
+  W.cap = a.cap;
+  W.lo = a.lo + (size_t)slot * (a.maxd + 2);
+  W.maxd = a.maxd;
+  W.cnt = a.cnt + slot;
+  W.err = a.err;
+  W.off = a.off;
+  W.adj = a.adj;
+  while (true) {
+    if (threadIdx.x == 0) s_g = atomicAdd(a.next, 1);
+    __syncthreads();
+    const int k = s_g;
+    __syncthreads();
+    if (k >= a.G) break;
+    const int g = a.order[k];
+    const int vb = a.voff[g], n = a.voff[g + 1] - vb;
+    W.off = a.off + vb;
+    W.vbase = vb;
+    W.V = n;
+    W.bc = a.bc + vb;
+    const int sb = a.soff[g], ns = a.soff[g + 1] - sb;
+    for (int s0 = 0; s0 < ns; s0 += SW) {
+      const int nb = min(SW, ns - s0);
+      for (int t = threadIdx.x; t < nb; t += blockDim.x) s_src[t] = a.srcs[sb + s0 + t] - vb;
+      __syncthreads();
+      if (!run_batch<NW>(W, s_src, nb, bs)) return;
+    }
+  }
+}
+
+__global__ void k_zero(void* p, size_t words) {
+  unsigned long long* q = (unsigned long long*)p;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < words; i += (size_t)gridDim.x * blockDim.x) q[i] = 0ull;
+}
+
+__global__ void k_to_float(const double* __restrict__ a, float* __restrict__ b, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = (float)a[i];
+}
+
+// ---- plain form: the generated/manual CUDA shape (one thread per vertex per level,
+// host loop on a flag; bcManualv5.cu:55-105, backend_cuda/dsl_cpp_generator.cpp:275-437)
+__global__ void k_plain_init(int V, int src, int* level, double* sigma, float* delta) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < V) {
+    level[v] = v == src ? 0 : -1;
+    sigma[v] = v == src ? 1.0 : 0.0;
+    delta[v] = 0.0f;
+  }
+}
+
+__global__ void k_plain_fwd(int V, const int32_t* __restrict__ off, const int32_t* __restrict__ adj, int* level,
+                            double* sigma, int d, int* more) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= V || level[v] != d) return;
+  for (int e = off[v]; e < off[v + 1]; ++e) {
+    int w = adj[e];
+    int old = atomicCAS(&level[w], -1, d + 1);
+    if (old == -1) *more = 1;
+    if (old == -1 || old == d + 1) atomicAdd(&sigma[w], sigma[v]);
+  }
+}
+
+__global__ void k_plain_bwd(int V, const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
+                            const int* level, const double* sigma, float* delta, double* bc, int d) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= V || level[v] != d) return;
+  double acc = 0;
+  for (int e = off[v]; e < off[v + 1]; ++e) {
+    int w = adj[e];
+    if (level[w] == d + 1) acc += sigma[v] / sigma[w] * (1.0 + (double)delta[w]);
+  }
+  delta[v] = (float)acc;
+  bc[v] += acc;
+}
+
+}  // namespace bc
+
+struct BcPlan {
+  dbuf<double> sigma, bc;
+  dbuf<float> delta, fout;
+  dbuf<unsigned long long> masks, flm;
+  dbuf<int32_t> flv, lo, cnt, srcs, level, aux;
+  dbuf<GridBar> bar;
+  dbuf<int> err;
+};
+
 void free_bc_plan(BcPlan* p) { delete p; }
+
+static int bc_grid(sp_graph* g, const int32_t* d_srcs, int nsrc, int batch_hint, int32_t* lvl_out = nullptr,
+                   double* sig_out = nullptr) {
+  BcPlan* p = g->bc;
+  cudaStream_t s = g->stream;
+  const int V = g->V;
+  const int NW = (batch_hint > 32) ? 2 : 1;
+  const int SW = 32 * NW;
+  const int batch = std::max(1, std::min(batch_hint, SW));
+  const int maxd = 1 << 14;
+  const size_t cap = (size_t)V * std::min(batch, 16) + 1024;  // level-list entries (vertex, mask)
+  SP_TRY(p->sigma.alloc((size_t)V * SW));
+  SP_TRY(p->delta.alloc((size_t)V * SW));
+  SP_TRY(p->masks.alloc((size_t)V * 3));
+  SP_TRY(p->flv.alloc(cap));
+  SP_TRY(p->flm.alloc(cap));
+  SP_TRY(p->lo.alloc(maxd + 2));
+  SP_TRY(p->cnt.alloc(1));
+  SP_TRY(p->bc.alloc(V));
+  SP_TRY(p->bar.alloc(1));
+  SP_TRY(p->err.alloc(1));
+  const int zg = num_sms() * 8;
+  bc::k_zero<<<zg, 256, 0, s>>>(p->sigma.p, (size_t)V * SW);
+  bc::k_zero<<<zg, 256, 0, s>>>(p->delta.p, (size_t)V * SW / 2);
+  bc::k_zero<<<zg, 256, 0, s>>>(p->masks.p, (size_t)V * 3);
+  bc::k_zero<<<zg, 256, 0, s>>>(p->bc.p, (size_t)V);
+  g_launches += 4;
+  SP_CHECK_CUDA(cudaMemsetAsync(p->bar.p, 0, sizeof(GridBar), s));
+  SP_CHECK_CUDA(cudaMemsetAsync(p->err.p, 0, sizeof(int), s));
+  bc::GridArgs a;
+  bc::Work& W = a.W;
+  W.off = g->off.p;
+  W.adj = g->adj.p;
+  W.vbase = 0;
+  W.V = V;
+  W.sigma = p->sigma.p;
+  W.delta = p->delta.p;
+  W.seen = p->masks.p;
+  W.nxt = p->masks.p + V;
+  W.dense = p->masks.p + 2 * (size_t)V;
+  W.flv = p->flv.p;
+  W.flm = p->flm.p;
+  W.cap = (int)std::min<size_t>(cap, INT_MAX);
+  W.lo = p->lo.p;
+  W.maxd = maxd;
+  W.cnt = p->cnt.p;
+  W.bc = p->bc.p;
+  W.err = p->err.p;
+  a.srcs = d_srcs;
+  a.nsrc = nsrc;
+  a.batch = batch;
+  a.bar = p->bar.p;
+  a.lvl_out = lvl_out;
+  a.sig_out = sig_out;
+  void* params[] = {&a};
+  int per_sm = 0;
+  const void* fn = NW == 2 ? (const void*)bc::k_bc_grid<2> : (const void*)bc::k_bc_grid<1>;
+  SP_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, bc::GRID_THREADS, 0));
+  const int grid = num_sms() * std::max(1, std::min(per_sm, 4));
+  SP_CHECK_CUDA(cudaLaunchCooperativeKernel(fn, grid, bc::GRID_THREADS, params, 0, s));
+  g_launches++;
+  int herr = 0;
+  SP_TRY(copy_out(&herr, p->err.p, sizeof(int), s));
+  if (herr) {
+    set_error("sp_bc: device error %d (1 level lists full, 2 deeper than %d levels, 3 barrier timeout)", herr, maxd);
+    return herr == 3 ? SP_ERR_TIMEOUT : SP_ERR_UNSUPPORTED;
+  }
+  return SP_OK;
+}
+
+static int bc_plain(sp_graph* g, const int32_t* h_srcs, int nsrc) {
+  BcPlan* p = g->bc;
+  cudaStream_t s = g->stream;
+  const int V = g->V;
+  SP_TRY(p->level.alloc(V));
+  SP_TRY(p->sigma.alloc(V));
+  SP_TRY(p->delta.alloc(V));
+  SP_TRY(p->bc.alloc(V));
+  SP_TRY(p->aux.alloc(1));
+  SP_CHECK_CUDA(cudaMemsetAsync(p->bc.p, 0, sizeof(double) * V, s));
+  const int tb = 1024, nb = (V + tb - 1) / tb;  // bcManualv5.cu:198-203 launch shape
+  for (int k = 0; k < nsrc; ++k) {
+    bc::k_plain_init<<<nb, tb, 0, s>>>(V, h_srcs[k], p->level.p, p->sigma.p, p->delta.p);
+    SP_CHECK_LAUNCH();
+    int d = 0;
+    while (true) {
+      SP_CHECK_CUDA(cudaMemsetAsync(p->aux.p, 0, sizeof(int), s));
+      bc::k_plain_fwd<<<nb, tb, 0, s>>>(V, g->off.p, g->adj.p, p->level.p, p->sigma.p, d, p->aux.p);
+      SP_CHECK_LAUNCH();
+      int more = 0;
+      SP_TRY(copy_out(&more, p->aux.p, sizeof(int), s));
+      if (!more) break;
+      ++d;
+    }
+    for (; d >= 1; --d) {
+      bc::k_plain_bwd<<<nb, tb, 0, s>>>(V, g->off.p, g->adj.p, p->level.p, p->sigma.p, p->delta.p, p->bc.p, d);
+      SP_CHECK_LAUNCH();
+    }
+  }
+  return SP_OK;
+}
+
 }  // namespace sp
+
+using namespace sp;
+
+extern "C" int sp_bc(sp_graph_h g, const int32_t* sources, int32_t nsrc, float* BC, int32_t variant) {
+  if (!g || !BC || (nsrc > 0 && !sources) || nsrc < 0) {
+    set_error("sp_bc: invalid argument");
+    return SP_ERR_INVALID;
+  }
+  if (!g->bc) g->bc = new BcPlan();
+  BcPlan* p = g->bc;
+  cudaStream_t s = g->stream;
+  std::vector<int32_t> hs(nsrc);
+  if (nsrc) SP_CHECK_CUDA(cudaMemcpyAsync(hs.data(), sources, sizeof(int32_t) * nsrc, cudaMemcpyDefault, s));
+  SP_CHECK_CUDA(cudaStreamSynchronize(s));
+  {
+    // std::set<int> semantics: each source once; ids must be vertices
+    std::vector<int32_t> u = hs;
+    std::sort(u.begin(), u.end());
+    if (std::adjacent_find(u.begin(), u.end()) != u.end()) {
+      set_error("sp_bc: repeated source (the reference takes a std::set)");
+      return SP_ERR_INVALID;
+    }
+    if (nsrc && (u.front() < 0 || u.back() >= g->V)) {
+      set_error("sp_bc: source out of range");
+      return SP_ERR_INVALID;
+    }
+  }
+  SP_TRY(p->fout.alloc(g->V));
+  if (nsrc == 0) {
+    SP_CHECK_CUDA(cudaMemsetAsync(p->fout.p, 0, sizeof(float) * g->V, s));
+  } else if (variant == SP_BC_PLAIN) {
+    SP_TRY(bc_plain(g, hs.data(), nsrc));
+    bc::k_to_float<<<num_sms() * 4, 256, 0, s>>>(p->bc.p, p->fout.p, g->V);
+    SP_CHECK_LAUNCH();
+  } else if (variant == SP_BC_BATCHED) {
+    SP_TRY(p->srcs.alloc(nsrc));
+    SP_CHECK_CUDA(cudaMemcpyAsync(p->srcs.p, hs.data(), sizeof(int32_t) * nsrc, cudaMemcpyHostToDevice, s));
+    const int batch = g->bc_batch > 0 ? (int)g->bc_batch : 64;
+    int st = bc_grid(g, p->srcs.p, nsrc, batch);
+    // level lists hold at most V * min(batch, 16) entries; a deep graph can need more
+    // when many sources share a batch, so retry with 16 sources per batch (always fits)
+    if (st == SP_ERR_UNSUPPORTED && batch > 16) st = bc_grid(g, p->srcs.p, nsrc, 16);
+    SP_TRY(st);
+    bc::k_to_float<<<num_sms() * 4, 256, 0, s>>>(p->bc.p, p->fout.p, g->V);
+    SP_CHECK_LAUNCH();
+  } else {
+    set_error("sp_bc: unknown variant %d", variant);
+    return SP_ERR_INVALID;
+  }
+  return copy_out(BC, p->fout.p, sizeof(float) * g->V, s);
+}
+
+extern "C" int sp_bc_graphs(sp_graph_h g, int32_t ngraphs, const int32_t* vertex_offset, const int32_t* source_offset,
+                            const int32_t* sources, float* BC) {
+  if (!g || ngraphs <= 0 || !vertex_offset || !source_offset || !BC) {
+    set_error("sp_bc_graphs: invalid argument");
+    return SP_ERR_INVALID;
+  }
+  if (!g->bc) g->bc = new BcPlan();
+  BcPlan* p = g->bc;
+  cudaStream_t s = g->stream;
+  std::vector<int32_t> voff(ngraphs + 1), soff(ngraphs + 1);
+  SP_CHECK_CUDA(cudaMemcpyAsync(voff.data(), vertex_offset, sizeof(int32_t) * (ngraphs + 1), cudaMemcpyDefault, s));
+  SP_CHECK_CUDA(cudaMemcpyAsync(soff.data(), source_offset, sizeof(int32_t) * (ngraphs + 1), cudaMemcpyDefault, s));
+  SP_CHECK_CUDA(cudaStreamSynchronize(s));
+  if (voff[0] != 0 || voff[ngraphs] != g->V || soff[0] != 0) {
+    set_error("sp_bc_graphs: vertex_offset must run 0..V and source_offset start at 0");
+    return SP_ERR_INVALID;
+  }
+  int vmax = 0, smax = 0;
+  for (int k = 0; k < ngraphs; ++k) {
+    if (voff[k + 1] < voff[k] || soff[k + 1] < soff[k]) {
+      set_error("sp_bc_graphs: offsets must be non-decreasing");
+      return SP_ERR_INVALID;
+    }
+    vmax = std::max(vmax, voff[k + 1] - voff[k]);
+    smax = std::max(smax, soff[k + 1] - soff[k]);
+  }
+  const int nsrc = soff[ngraphs];
+  std::vector<int32_t> hs(std::max(1, nsrc));
+  if (nsrc) SP_CHECK_CUDA(cudaMemcpyAsync(hs.data(), sources, sizeof(int32_t) * nsrc, cudaMemcpyDefault, s));
+  SP_CHECK_CUDA(cudaStreamSynchronize(s));
+  for (int k = 0; k < ngraphs; ++k) {
+    std::vector<int32_t> u(hs.begin() + soff[k], hs.begin() + soff[k + 1]);
+    std::sort(u.begin(), u.end());
+    if (std::adjacent_find(u.begin(), u.end()) != u.end() || (!u.empty() && (u.front() < voff[k] || u.back() >= voff[k + 1]))) {
+      set_error("sp_bc_graphs: sources of graph %d repeat or fall outside its vertex range", k);
+      return SP_ERR_INVALID;
+    }
+  }
+  // graphs the CTAs take from the queue, largest first
+  std::vector<int32_t> order(ngraphs);
+  for (int k = 0; k < ngraphs; ++k) order[k] = k;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    return (int64_t)(voff[a + 1] - voff[a]) * (soff[a + 1] - soff[a]) > (int64_t)(voff[b + 1] - voff[b]) * (soff[b + 1] - soff[b]);
+  });
+  const int NW = smax > 32 ? 2 : 1;
+  const int SW = 32 * NW;
+  const int maxd = 4096;
+  const int cap = vmax * std::min(std::max(1, std::min(smax, SW)), 16) + 1024;
+  int per_sm = 0;
+  const void* fn = NW == 2 ? (const void*)bc::k_bc_graphs<2> : (const void*)bc::k_bc_graphs<1>;
+  SP_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, bc::CTA_THREADS, 0));
+  const int ctas = std::max(1, std::min(num_sms() * std::max(1, std::min(per_sm, 2)), ngraphs));
+  SP_TRY(p->sigma.alloc((size_t)ctas * vmax * SW));
+  SP_TRY(p->delta.alloc((size_t)ctas * vmax * SW));
+  SP_TRY(p->masks.alloc((size_t)ctas * vmax * 3));
+  SP_TRY(p->flv.alloc((size_t)ctas * cap));
+  SP_TRY(p->flm.alloc((size_t)ctas * cap));
+  SP_TRY(p->lo.alloc((size_t)ctas * (maxd + 2)));
+  SP_TRY(p->cnt.alloc(ctas + 1));
+  SP_TRY(p->bc.alloc(g->V));
+  SP_TRY(p->srcs.alloc(std::max(1, nsrc) + 2 * (ngraphs + 1) + ngraphs));
+  SP_TRY(p->err.alloc(1));
+  SP_TRY(p->fout.alloc(g->V));
+  int32_t* d_srcs = p->srcs.p;
+  int32_t* d_voff = d_srcs + std::max(1, nsrc);
+  int32_t* d_soff = d_voff + ngraphs + 1;
+  int32_t* d_order = d_soff + ngraphs + 1;
+  if (nsrc) SP_CHECK_CUDA(cudaMemcpyAsync(d_srcs, hs.data(), sizeof(int32_t) * nsrc, cudaMemcpyHostToDevice, s));
+  SP_CHECK_CUDA(cudaMemcpyAsync(d_voff, voff.data(), sizeof(int32_t) * (ngraphs + 1), cudaMemcpyHostToDevice, s));
+  SP_CHECK_CUDA(cudaMemcpyAsync(d_soff, soff.data(), sizeof(int32_t) * (ngraphs + 1), cudaMemcpyHostToDevice, s));
+  SP_CHECK_CUDA(cudaMemcpyAsync(d_order, order.data(), sizeof(int32_t) * ngraphs, cudaMemcpyHostToDevice, s));
+  const int zg = num_sms() * 8;
+  bc::k_zero<<<zg, 256, 0, s>>>(p->sigma.p, (size_t)ctas * vmax * SW);
+  bc::k_zero<<<zg, 256, 0, s>>>(p->delta.p, (size_t)ctas * vmax * SW / 2);
+  bc::k_zero<<<zg, 256, 0, s>>>(p->masks.p, (size_t)ctas * vmax * 3);
+  bc::k_zero<<<zg, 256, 0, s>>>(p->bc.p, (size_t)g->V);
+  g_launches += 4;
+  SP_CHECK_CUDA(cudaMemsetAsync(p->cnt.p, 0, sizeof(int) * (ctas + 1), s));
+  SP_CHECK_CUDA(cudaMemsetAsync(p->err.p, 0, sizeof(int), s));
+  bc::GraphsArgs a;
+  a.off = g->off.p;
+  a.adj = g->adj.p;
+  a.voff = d_voff;
+  a.soff = d_soff;
+  a.srcs = d_srcs;
+  a.order = d_order;
+  a.G = ngraphs;
+  a.next = p->cnt.p + ctas;
+  a.sigma = p->sigma.p;
+  a.delta = p->delta.p;
+  a.masks = p->masks.p;
+  a.flv = p->flv.p;
+  a.flm = p->flm.p;
+  a.lo = p->lo.p;
+  a.cnt = p->cnt.p;
+  a.bc = p->bc.p;
+  a.vmax = vmax;
+  a.cap = cap;
+  a.maxd = maxd;
+  a.err = p->err.p;
+  if (NW == 2)
+    bc::k_bc_graphs<2><<<ctas, bc::CTA_THREADS, 0, s>>>(a);
+  else
+    bc::k_bc_graphs<1><<<ctas, bc::CTA_THREADS, 0, s>>>(a);
+  SP_CHECK_LAUNCH();
+  int herr = 0;
+  SP_TRY(copy_out(&herr, p->err.p, sizeof(int), s));
+  if (herr) {
+    set_error("sp_bc_graphs: device error %d (1 level lists full, 2 deeper than %d levels)", herr, maxd);
+    return SP_ERR_UNSUPPORTED;
+  }
+  bc::k_to_float<<<num_sms() * 4, 256, 0, s>>>(p->bc.p, p->fout.p, g->V);
+  SP_CHECK_LAUNCH();
+  return copy_out(BC, p->fout.p, sizeof(float) * g->V, s);
+}
+
+extern "C" int sp_bfs_sigma(sp_graph_h g, const int32_t* sources, int32_t nsrc, int32_t* level, double* sigma) {
+  if (!g || !sources || nsrc <= 0 || nsrc > 64 || !level || !sigma) {
+    set_error("sp_bfs_sigma: invalid argument (1..64 sources)");
+    return SP_ERR_INVALID;
+  }
+  if (!g->bc) g->bc = new BcPlan();
+  BcPlan* p = g->bc;
+  cudaStream_t s = g->stream;
+  std::vector<int32_t> hs(nsrc);
+  SP_CHECK_CUDA(cudaMemcpyAsync(hs.data(), sources, sizeof(int32_t) * nsrc, cudaMemcpyDefault, s));
+  SP_CHECK_CUDA(cudaStreamSynchronize(s));
+  std::vector<int32_t> u = hs;
+  std::sort(u.begin(), u.end());
+  if (std::adjacent_find(u.begin(), u.end()) != u.end() || u.front() < 0 || u.back() >= g->V) {
+    set_error("sp_bfs_sigma: sources must be distinct vertices");
+    return SP_ERR_INVALID;
+  }
+  const size_t n = (size_t)nsrc * g->V;
+  dbuf<int32_t> dl;
+  dbuf<double> ds;
+  SP_TRY(dl.alloc(n));
+  SP_TRY(ds.alloc(n));
+  SP_CHECK_CUDA(cudaMemsetAsync(dl.p, 0xff, sizeof(int32_t) * n, s));  // -1 = unreached
+  SP_CHECK_CUDA(cudaMemsetAsync(ds.p, 0, sizeof(double) * n, s));
+  SP_TRY(p->srcs.alloc(nsrc));
+  SP_CHECK_CUDA(cudaMemcpyAsync(p->srcs.p, hs.data(), sizeof(int32_t) * nsrc, cudaMemcpyHostToDevice, s));
+  SP_TRY(bc_grid(g, p->srcs.p, nsrc, 64, dl.p, ds.p));
+  SP_TRY(copy_out(level, dl.p, sizeof(int32_t) * n, s));
+  return copy_out(sigma, ds.p, sizeof(double) * n, s);
+}

@@ -310,6 +310,14 @@ int sp_tune_set(sp_graph_h g, const char* key, int64_t value) {
     g->sssp_delta = value;
     return SP_OK;
   }
+  if (!strcmp(key, "bc.batch")) {
+    if (value < 0 || value > 64) {
+      set_error("sp_tune_set: bc.batch must be in [0, 64]");
+      return SP_ERR_INVALID;
+    }
+    g->bc_batch = (int32_t)value;
+    return SP_OK;
+  }
   set_error("sp_tune_set: unknown key '%s'", key);
   return SP_ERR_INVALID;
 }
@@ -325,6 +333,10 @@ int sp_tune_get(sp_graph_h g, const char* key, int64_t* value) {
   }
   if (!strcmp(key, "sssp.delta")) {
     *value = g->sssp_delta;
+    return SP_OK;
+  }
+  if (!strcmp(key, "bc.batch")) {
+    *value = g->bc_batch > 0 ? g->bc_batch : 64;
     return SP_OK;
   }
   set_error("sp_tune_get: unknown key '%s'", key);

@@ -137,3 +137,31 @@ class DeviceGraph:
         check("sp_sssp", lib().sp_sssp(self.handle, _ptr(weight), int(src), _ptr(out), int(delta), variant,
                                        ctypes.byref(rounds)))
         return out, int(rounds.value)
+
+    def bc(self, sources, out=None, variant: int = _lib.SP_BC_BATCHED):
+        """Brandes BC over distinct `sources` (int32, host or device); float32[V]."""
+        if out is None:
+            out = np.empty(self.V, np.float32)
+        if isinstance(sources, (list, tuple)):
+            sources = np.asarray(sources, np.int32)
+        n = int(sources.shape[0])
+        check("sp_bc", lib().sp_bc(self.handle, _ptr(sources) if n else None, n, _ptr(out), variant))
+        return out
+
+    def bc_graphs(self, vertex_offset, source_offset, sources, out=None):
+        """BC of many independent graphs stored as one disjoint union (see sp_bc_graphs)."""
+        if out is None:
+            out = np.empty(self.V, np.float32)
+        G = int(vertex_offset.shape[0]) - 1
+        check("sp_bc_graphs", lib().sp_bc_graphs(self.handle, G, _ptr(vertex_offset), _ptr(source_offset),
+                                                 _ptr(sources), _ptr(out)))
+        return out
+
+    def bfs_sigma(self, sources):
+        """BFS levels and shortest-path counts from up to 64 sources: (level[k][V], sigma[k][V])."""
+        sources = np.ascontiguousarray(sources, np.int32)
+        k = sources.shape[0]
+        lvl = np.empty((k, self.V), np.int32)
+        sig = np.empty((k, self.V), np.float64)
+        check("sp_bfs_sigma", lib().sp_bfs_sigma(self.handle, _ptr(sources), k, _ptr(lvl), _ptr(sig)))
+        return lvl, sig

@@ -1,0 +1,109 @@
+"""GPU parity: Brandes BC within 1e-5 relative of the FP64 oracle; BFS levels and
+path counts (sigma) bit-exact."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from starplat_b200 import _lib
+from starplat_b200 import generators as G
+from starplat_b200.algorithms import Compute_BC, device_graph
+from starplat_b200.device import DeviceGraph
+
+from graphs import clique, directed_zoo, from_pairs, path, star, undirected_zoo
+
+pytestmark = pytest.mark.gpu
+
+
+def assert_bc_close(out, ref, name=""):
+    out = out.astype(np.float64)
+    scale = max(1.0, float(np.abs(ref).max()))
+    err = np.abs(out - ref)
+    # relative error 1e-5 per vertex, with an absolute floor for values near zero
+    bad = err > 1e-5 * np.abs(ref) + 1e-9 * scale
+    assert not bad.any(), (name, int(bad.sum()), float((err / np.maximum(np.abs(ref), 1e-30))[bad].max()))
+
+
+@pytest.mark.parametrize("gi", range(8))
+def test_bc_undirected(gi):
+    g = undirected_zoo()[gi]
+    srcs = G.pick_sources(g, min(100, g.V), seed=gi, min_out_degree=0)
+    out = device_graph(g).bc(srcs)
+    assert_bc_close(out, O.bc(g.indexofNodes, g.edgeList, srcs), g.name)
+
+
+@pytest.mark.parametrize("gi", range(4))
+def test_bc_directed(gi):
+    g = directed_zoo()[gi]
+    srcs = G.pick_sources(g, min(70, g.V), seed=gi, min_out_degree=0)
+    out = device_graph(g).bc(srcs)
+    assert_bc_close(out, O.bc(g.indexofNodes, g.edgeList, srcs), g.name)
+
+
+@pytest.mark.parametrize("batch", [1, 7, 32, 33, 64])
+def test_bc_batch_knob(batch):
+    g = G.rmat(11, 16, seed=4)
+    srcs = G.pick_sources(g, 150, seed=2)
+    dg = device_graph(g)
+    dg.tune_set("bc.batch", batch)
+    out = dg.bc(srcs)
+    dg.tune_set("bc.batch", 0)
+    assert_bc_close(out, O.bc(g.indexofNodes, g.edgeList, srcs))
+
+
+def test_bc_all_sources_small_graphs():
+    # the reference driver passes every vertex as a source (bc_dslV2main.cpp:50-53)
+    for g in (clique(10), path(40), star(50, directed_in=False), G.grid(7, 9)):
+        srcs = np.arange(g.V, dtype=np.int32)
+        out = device_graph(g).bc(srcs)
+        assert_bc_close(out, O.bc(g.indexofNodes, g.edgeList, srcs), g.name)
+
+
+def test_bc_plain_variant():
+    g = G.rmat(10, 8, seed=3)
+    srcs = G.pick_sources(g, 20, seed=1)
+    out = device_graph(g).bc(srcs, variant=_lib.SP_BC_PLAIN)
+    assert_bc_close(out, O.bc(g.indexofNodes, g.edgeList, srcs))
+
+
+def test_bc_entry_point_and_errors():
+    g = G.rmat(10, 8, seed=9)
+    BC = np.zeros(g.V, np.float32)
+    Compute_BC(g, BC, {3, 1, 4, 15, 92})
+    assert_bc_close(BC, O.bc(g.indexofNodes, g.edgeList, np.array([1, 3, 4, 15, 92], np.int32)))
+    with pytest.raises(_lib.SPError):
+        device_graph(g).bc(np.array([1, 1], np.int32))
+    with pytest.raises(_lib.SPError):
+        device_graph(g).bc(np.array([g.V], np.int32))
+    assert not device_graph(g).bc(np.zeros(0, np.int32)).any()
+
+
+def test_bfs_levels_and_sigma_bit_exact():
+    for g in (G.rmat(12, 16, seed=6), G.rmat(11, 8, seed=2, directed=True), G.grid(12, 15)):
+        srcs = G.pick_sources(g, 64, seed=5)
+        lvl, sig = device_graph(g).bfs_sigma(srcs)
+        for k, s in enumerate(srcs):
+            rl, rs, _ = O.bfs_sigma(g.indexofNodes, g.edgeList, int(s))
+            assert np.array_equal(lvl[k], rl)
+            assert np.array_equal(sig[k], rs)  # integers below 2^53: exact
+
+
+def test_bc_many_graphs_one_launch():
+    gs = G.er_batch(12, 200, 3000, 4, 12, seed=3)
+    offs = [0]
+    src_all, soff = [], [0]
+    pairs_s, pairs_d = [], []
+    for k, g in enumerate(gs):
+        b = offs[-1]
+        u = np.repeat(np.arange(g.V, dtype=np.int32), np.diff(g.indexofNodes))
+        pairs_s.append(u + b)
+        pairs_d.append(g.edgeList + b)
+        src_all.append(G.pick_sources(g, 16, seed=k) + b)
+        soff.append(soff[-1] + src_all[-1].shape[0])
+        offs.append(b + g.V)
+    V = offs[-1]
+    union = from_pairs(V, np.stack([np.concatenate(pairs_s), np.concatenate(pairs_d)], 1), name="union")
+    with DeviceGraph.from_csr(union) as dg:
+        out = dg.bc_graphs(np.array(offs, np.int32), np.array(soff, np.int32), np.concatenate(src_all))
+    for k, g in enumerate(gs):
+        ref = O.bc(g.indexofNodes, g.edgeList, src_all[k] - offs[k])
+        assert_bc_close(out[offs[k]:offs[k + 1]], ref, f"graph{k}")
