@@ -132,6 +132,16 @@ int sp_bfs_sigma(sp_graph_h g, const int32_t* sources, int32_t nsrc, int32_t* le
 int sp_bc_graphs(sp_graph_h g, int32_t ngraphs, const int32_t* vertex_offset, const int32_t* source_offset,
                  const int32_t* sources, float* BC);
 
+/* ---- Louvain community detection -----------------------------------------------
+ * DSL staticDSLCodes/community_detection:1-211 (MPI-only in the reference; its
+ * generated entry point would be `auto Compute_CD(graph& g, int* weight)` returning
+ * the modularity). weight[E] in forward-CSR order, NULL = unit weights. Local moves
+ * and aggregation repeat while modularity improves by more than `threshold`
+ * (the DSL uses 1e-4). community (may be NULL) gets a dense community id per vertex;
+ * *modularity the final Q; levels (may be NULL) the number of levels run. */
+int sp_louvain(sp_graph_h g, const float* weight, double threshold, int32_t* community, double* modularity,
+               int32_t* levels);
+
 #ifdef __cplusplus
 }
 #endif

@@ -62,6 +62,7 @@ SIGNATURES = {
     "sp_bc": (ctypes.c_int, [vp, vp, i32, vp, i32]),
     "sp_bc_graphs": (ctypes.c_int, [vp, i32, vp, vp, vp, vp]),
     "sp_bfs_sigma": (ctypes.c_int, [vp, vp, i32, vp, vp]),
+    "sp_louvain": (ctypes.c_int, [vp, vp, f64, vp, P(f64), P(i32)]),
 }
 
 

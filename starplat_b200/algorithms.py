@@ -54,3 +54,11 @@ def Compute_BC(g: CSRGraph, BC: np.ndarray, sourceSet) -> None:
     sourceSet (any iterable of distinct vertex ids, like the reference's std::set<int>)."""
     src = np.array(sorted(set(int(s) for s in sourceSet)), np.int32)
     device_graph(g).bc(src, out=BC)
+
+
+def Compute_CD(g: CSRGraph, weight=None) -> float:
+    """staticDSLCodes/community_detection: returns the modularity of the Louvain
+    partition; weight is int[E] (or float[E]) in forward-CSR order, None = unit."""
+    w = None if weight is None else np.ascontiguousarray(weight, np.float32)
+    q, _, _ = device_graph(g).louvain(w, 1e-4)
+    return q

@@ -1,5 +1,653 @@
+// Louvain community detection (local move + aggregation) for sm_100a.
+//
+// Semantics: DSL staticDSLCodes/community_detection:1-211 (the reference's only
+// Louvain DSL; MPI-only there) and the runnable CUDA restatement
+// dynamic_louvain_community_detection/communitydetection_sequential_allocation.cu
+// (computeGraphWeight :746-778, modularity :1060-1080):
+//   W = sum of all directed edge weights; k_v = weighted degree (+ self-loop weight);
+//   gain(v -> c) = k_{v,c} - tot_c * k_v / W   (tot_c without v for v's own community,
+//   community_detection:83-107); Q = sum_c in_c / W - (tot_c / W)^2 (:40);
+//   local moves repeat while Q improves by more than `threshold`, then communities
+//   become vertices (self-loop = internal weight) and the whole repeats while a level
+//   improves Q by more than `threshold` (:34, :111, :208).
+// The sequential order of the DSL cannot be kept on a GPU, so results are compared
+// on modularity (within 1e-3 of the sequential restatement), not on labels.
+//
+// B200 design:
+//  * synchronous local moves: every vertex of a sub-sweep picks its best community
+//    from the same snapshot; two sub-sweeps per sweep (vertex hash parity) and the
+//    singleton rule (a singleton moves to another singleton only if that label is
+//    smaller) keep neighbours from swapping back and forth;
+//  * per-vertex neighbour-community weights in shared-memory hash tables by degree
+//    bin: one warp with a 128-slot table (degree <= 64), one CTA with a table of
+//    up to 16384 slots in dynamic shared memory (degree <= 8192), one CTA with a
+//    table in global scratch above that; FP64 values, shared-memory atomics;
+//  * tot_c, in_c and Q reduced with FP64 atomics (exact for integer weights);
+//  * aggregation: communities renumbered densely, external edges emitted at scan
+//    positions, sorted by (c_u, c_v) with a radix sort and merged with a reduce-by-key.
+#include <cub/cub.cuh>
+
+#include <climits>
+#include <cmath>
+#include <vector>
+
 #include "sp_internal.cuh"
+
 namespace sp {
-struct LvPlan {};
+
+namespace lv {
+constexpr int THREADS = 256;
+constexpr int WARP_DEG = 64;
+constexpr int WARP_SLOTS = 128;
+constexpr int CTA_DEG = 8192;
+constexpr int CTA_SLOTS_MAX = 16384;
+constexpr int EMPTY = -1;
+
+__device__ __forceinline__ unsigned hmix(unsigned x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+
+struct Level {
+  int n;
+  const int32_t* __restrict__ off;
+  const int32_t* __restrict__ adj;
+  const double* __restrict__ w;
+  const double* __restrict__ sl;  // self-loop weight per vertex
+};
+
+struct MoveArgs {
+  Level L;
+  const int32_t* __restrict__ comm;
+  const double* __restrict__ tot;
+  const int32_t* __restrict__ csize;
+  const double* __restrict__ kv;
+  int32_t* newcomm;
+  const int32_t* __restrict__ list;  // vertices of this bin
+  int nlist;
+  int parity;     // sub-sweep: vertices with hmix(v)&1 == parity
+  double W;
+  double* gtab_val;  // global tables (big bin)
+  int32_t* gtab_key;
+  const int64_t* gtab_off;  // per list entry: table offset (big bin)
+};
+
+// insert (key, val) into an open-addressing table; returns false if full
+__device__ __forceinline__ bool tab_add(int32_t* keys, double* vals, unsigned mask, int key, double val) {
+  unsigned s = hmix((unsigned)key) & mask;
+  for (unsigned probe = 0; probe <= mask; ++probe) {
+    int prev = atomicCAS(&keys[s], EMPTY, key);
+    if (prev == EMPTY || prev == key) {
+      atomicAdd(&vals[s], val);
+      return true;
+    }
+    s = (s + 1) & mask;
+  }
+  return false;
+}
+
+// better candidate: larger gain; on a tie the current community, then the smaller id
+__device__ __forceinline__ bool better(double g1, int c1, double g2, int c2, int cur) {
+  if (g1 != g2) return g1 > g2;
+  if (c1 == cur) return true;
+  if (c2 == cur) return false;
+  return c1 < c2;
+}
+
+__device__ __forceinline__ int decide(const MoveArgs& a, int v, int cv, double kv, double best_gain, int best_c) {
+  // baseline: the DSL starts from currcommunity.kin (always 0) - tot' * k_v / W (:88)
+  const double stay = 0.0 - (a.tot[cv] - kv) * kv / a.W;
+  if (best_c < 0 || !(best_gain > stay) || best_c == cv) return cv;
+  if (a.csize[cv] == 1 && a.csize[best_c] == 1 && best_c > cv) return cv;  // singleton rule
+  return best_c;
+}
+
+__global__ void __launch_bounds__(THREADS) k_move_warp(MoveArgs a) {
+  __shared__ int32_t s_key[THREADS / 32][WARP_SLOTS];
+  __shared__ double s_val[THREADS / 32][WARP_SLOTS];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int32_t* keys = s_key[wid];
+  double* vals = s_val[wid];
+  for (int i = lane; i < WARP_SLOTS; i += 32) {
+    keys[i] = EMPTY;
+    vals[i] = 0.0;
+  }
+  __syncwarp();
+  const int gw = (blockIdx.x * THREADS + threadIdx.x) >> 5, nw = (gridDim.x * THREADS) >> 5;
+  for (int i = gw; i < a.nlist; i += nw) {
+    const int v = a.list[i];
+    if ((int)(hmix((unsigned)v) & 1u) != a.parity) continue;
+    const int cv = a.comm[v];
+    const double kv = a.kv[v];
+    const int b = a.L.off[v], e = a.L.off[v + 1];
+    for (int j = b + lane; j < e; j += 32) tab_add(keys, vals, WARP_SLOTS - 1, a.comm[a.L.adj[j]], a.L.w[j]);
+    __syncwarp();
+    double bg = -INFINITY;
+    int bc = -1;
+    for (int s = lane; s < WARP_SLOTS; s += 32) {
+      const int c = keys[s];
+      if (c != EMPTY) {
+        const double tc = (c == cv) ? a.tot[c] - kv : a.tot[c];
+        const double gain = vals[s] - tc * kv / a.W;
+        if (bc < 0 || better(gain, c, bg, bc, cv)) {
+          bg = gain;
+          bc = c;
+        }
+        keys[s] = EMPTY;
+        vals[s] = 0.0;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double og = __shfl_xor_sync(0xffffffffu, bg, o);
+      const int oc = __shfl_xor_sync(0xffffffffu, bc, o);
+      if (oc >= 0 && (bc < 0 || better(og, oc, bg, bc, cv))) {
+        bg = og;
+        bc = oc;
+      }
+    }
+    if (lane == 0) a.newcomm[v] = decide(a, v, cv, kv, bg, bc);
+    __syncwarp();
+  }
+}
+
+// One CTA per vertex; table in dynamic shared memory (slots = power of two) or,
+// for the big bin, in global scratch at gtab_off[i].
+template <bool GLOBAL_TABLE>
+__global__ void __launch_bounds__(THREADS) k_move_cta(MoveArgs a, int slots) {
+  extern __shared__ double s_dyn[];
+  __shared__ double s_bg[THREADS / 32];
+  __shared__ int s_bc[THREADS / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int i = blockIdx.x; i < a.nlist; i += gridDim.x) {
+    const int v = a.list[i];
+    if ((int)(hmix((unsigned)v) & 1u) != a.parity) continue;
+    const int b = a.L.off[v], e = a.L.off[v + 1];
+    int nslots = slots;
+    double* vals;
+    int32_t* keys;
+    if (GLOBAL_TABLE) {
+      nslots = (int)(a.gtab_off[i + 1] - a.gtab_off[i]);
+      vals = a.gtab_val + a.gtab_off[i];
+      keys = a.gtab_key + a.gtab_off[i];
+    } else {
+      // table just large enough for this vertex (load factor <= 1/2), at most `slots`
+      int need = 64;
+      while (need < 2 * (e - b) && need < slots) need <<= 1;
+      nslots = need;
+      vals = s_dyn;
+      keys = reinterpret_cast<int32_t*>(s_dyn + slots);
+    }
+    for (int s = threadIdx.x; s < nslots; s += THREADS) {
+      keys[s] = EMPTY;
+      vals[s] = 0.0;
+    }
+    __syncthreads();
+    const int cv = a.comm[v];
+    const double kv = a.kv[v];
+    for (int j = b + threadIdx.x; j < e; j += THREADS)
+      tab_add(keys, vals, (unsigned)nslots - 1u, a.comm[a.L.adj[j]], a.L.w[j]);
+    __syncthreads();
+    double bg = -INFINITY;
+    int bc = -1;
+    for (int s = threadIdx.x; s < nslots; s += THREADS) {
+      const int c = keys[s];
+      if (c != EMPTY) {
+        const double tc = (c == cv) ? a.tot[c] - kv : a.tot[c];
+        const double gain = vals[s] - tc * kv / a.W;
+        if (bc < 0 || better(gain, c, bg, bc, cv)) {
+          bg = gain;
+          bc = c;
+        }
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double og = __shfl_xor_sync(0xffffffffu, bg, o);
+      const int oc = __shfl_xor_sync(0xffffffffu, bc, o);
+      if (oc >= 0 && (bc < 0 || better(og, oc, bg, bc, cv))) {
+        bg = og;
+        bc = oc;
+      }
+    }
+    if (lane == 0) {
+      s_bg[wid] = bg;
+      s_bc[wid] = bc;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int k = 1; k < THREADS / 32; ++k)
+        if (s_bc[k] >= 0 && (bc < 0 || better(s_bg[k], s_bc[k], bg, bc, cv))) {
+          bg = s_bg[k];
+          bc = s_bc[k];
+        }
+      a.newcomm[v] = decide(a, v, cv, kv, bg, bc);
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_kv(Level L, double* kv, double* W) {
+  const int lane = threadIdx.x & 31;
+  double acc = 0;
+  for (int v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < L.n; v += (gridDim.x * blockDim.x) >> 5) {
+    double s = 0;
+    for (int j = L.off[v] + lane; j < L.off[v + 1]; j += 32) s += L.w[j];
+    s = warp_sum(s);
+    if (lane == 0) {
+      kv[v] = s + L.sl[v];
+      acc += s + L.sl[v];
+    }
+  }
+  if (W && lane == 0 && acc != 0.0) atomicAdd(W, acc);
+}
+
+__global__ void k_init_comm(int n, int32_t* comm, int32_t* newcomm) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) comm[v] = newcomm[v] = v;
+}
+
+__global__ void k_apply(int n, int parity, int32_t* comm, const int32_t* __restrict__ newcomm, int* moved) {
+  int local = 0;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    if ((int)(hmix((unsigned)v) & 1u) != parity) continue;
+    if (comm[v] != newcomm[v]) {
+      comm[v] = newcomm[v];
+      ++local;
+    }
+  }
+  local = warp_sum(local);
+  if ((threadIdx.x & 31) == 0 && local) atomicAdd(moved, local);
+}
+
+__global__ void k_tot(int n, const int32_t* __restrict__ comm, const double* __restrict__ kv, double* tot,
+                      int32_t* csize) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    atomicAdd(&tot[comm[v]], kv[v]);
+    atomicAdd(&csize[comm[v]], 1);
+  }
+}
+
+// in_c (directed internal weight + self loops) per community, then Q
+__global__ void k_internal(Level L, const int32_t* __restrict__ comm, double* in) {
+  const int lane = threadIdx.x & 31;
+  for (int v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < L.n; v += (gridDim.x * blockDim.x) >> 5) {
+    const int cv = comm[v];
+    double s = 0;
+    for (int j = L.off[v] + lane; j < L.off[v + 1]; j += 32)
+      if (comm[L.adj[j]] == cv) s += L.w[j];
+    s = warp_sum(s);
+    if (lane == 0 && (s != 0.0 || L.sl[v] != 0.0)) atomicAdd(&in[cv], s + L.sl[v]);
+  }
+}
+
+__global__ void k_q(int n, const double* __restrict__ in, const double* __restrict__ tot, double W, double* q) {
+  __shared__ double s_red[THREADS / 32];
+  double acc = 0;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    const double t = tot[c] / W;
+    acc += in[c] / W - t * t;
+  }
+  acc = block_sum<THREADS>(acc, s_red);
+  if (threadIdx.x == 0) atomicAdd(q, acc);
+}
+
+// ---- aggregation
+__global__ void k_mark(int n, const int32_t* __restrict__ comm, int32_t* used) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) used[comm[v]] = 1;
+}
+
+__global__ void k_count_ext(Level L, const int32_t* __restrict__ comm, int32_t* cnt) {
+  const int lane = threadIdx.x & 31;
+  for (int v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < L.n; v += (gridDim.x * blockDim.x) >> 5) {
+    const int cv = comm[v];
+    int c = 0;
+    for (int j = L.off[v] + lane; j < L.off[v + 1]; j += 32) c += comm[L.adj[j]] != cv;
+    c = warp_sum(c);
+    if (lane == 0) cnt[v] = c;
+  }
+}
+
+__global__ void k_emit(Level L, const int32_t* __restrict__ comm, const int32_t* __restrict__ newid,
+                       const int32_t* __restrict__ pos, unsigned long long* keys, double* vals, double* sl_new) {
+  const int lane = threadIdx.x & 31;
+  for (int v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < L.n; v += (gridDim.x * blockDim.x) >> 5) {
+    const int cv = comm[v];
+    const unsigned long long nv = (unsigned long long)newid[cv];
+    int base = pos[v];
+    double inw = 0;
+    for (int j0 = L.off[v]; j0 < L.off[v + 1]; j0 += 32) {
+      const int j = j0 + lane;
+      bool ext = false;
+      int cu = 0;
+      if (j < L.off[v + 1]) {
+        cu = comm[L.adj[j]];
+        ext = cu != cv;
+        if (!ext) inw += L.w[j];
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, ext);
+      if (ext) {
+        const int p = base + __popc(m & ((1u << lane) - 1u));
+        keys[p] = (nv << 32) | (unsigned long long)(unsigned)newid[cu];
+        vals[p] = L.w[j];
+      }
+      base += __popc(m);
+    }
+    inw = warp_sum(inw);
+    if (lane == 0 && (inw != 0.0 || L.sl[v] != 0.0)) atomicAdd(&sl_new[nv], inw + L.sl[v]);
+  }
+}
+
+__global__ void k_build_rows(int m, const unsigned long long* __restrict__ ukeys, int32_t* adj, int32_t* rowcnt) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    adj[i] = (int32_t)(ukeys[i] & 0xffffffffull);
+    atomicAdd(&rowcnt[(int)(ukeys[i] >> 32)], 1);
+  }
+}
+
+__global__ void k_compose(int n0, int32_t* orig, const int32_t* __restrict__ comm, const int32_t* __restrict__ newid) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n0; v += gridDim.x * blockDim.x) orig[v] = newid[comm[orig[v]]];
+}
+
+__global__ void k_f2d(const float* __restrict__ a, double* b, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = a ? (double)a[i] : 1.0;
+}
+
+__global__ void k_bins(int n, const int32_t* __restrict__ off, int32_t* lists, int* counts, int cap) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const int d = off[v + 1] - off[v];
+    const int b = d <= WARP_DEG ? 0 : (d <= CTA_DEG ? 1 : 2);
+    const int p = atomicAdd(&counts[b], 1);
+    lists[(size_t)b * cap + p] = v;
+  }
+}
+
+}  // namespace lv
+
+struct LvPlan {
+  // level graphs (ping-pong)
+  dbuf<int32_t> off[2], adj[2];
+  dbuf<double> w[2], sl[2];
+  dbuf<int32_t> comm, newcomm, csize, used, newid, cnt, pos, orig, lists, rowcnt;
+  dbuf<double> kv, tot, in, scal;
+  dbuf<unsigned long long> keys, skeys, ukeys;
+  dbuf<double> vals, svals, uvals;
+  dbuf<int> icnt;
+  dbuf<unsigned char> temp;
+  dbuf<double> gval;
+  dbuf<int32_t> gkey;
+  dbuf<int64_t> goff;
+};
+
 void free_lv_plan(LvPlan* p) { delete p; }
+
+namespace {
+
+template <class T>
+int dev_scan(LvPlan* p, const T* in, T* out, int n, cudaStream_t s) {
+  size_t tb = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tb, in, out, n, s);
+  SP_TRY(p->temp.alloc(tb));
+  cub::DeviceScan::ExclusiveSum(p->temp.p, tb, in, out, n, s);
+  g_launches++;
+  return SP_OK;
+}
+
+int read_int(const int* d, int* h, cudaStream_t s) { return copy_out(h, d, sizeof(int), s); }
+
+}  // namespace
+
+static int lv_modularity(LvPlan* p, const lv::Level& L, double W, cudaStream_t s, double* q) {
+  const int n = L.n;
+  const int g = num_sms() * 8;
+  SP_CHECK_CUDA(cudaMemsetAsync(p->in.p, 0, sizeof(double) * n, s));
+  SP_CHECK_CUDA(cudaMemsetAsync(p->scal.p, 0, sizeof(double), s));
+  lv::k_internal<<<g, 256, 0, s>>>(L, p->comm.p, p->in.p);
+  SP_CHECK_LAUNCH();
+  lv::k_q<<<g, lv::THREADS, 0, s>>>(n, p->in.p, p->tot.p, W, p->scal.p);
+  SP_CHECK_LAUNCH();
+  return copy_out(q, p->scal.p, sizeof(double), s);
+}
+
+static int lv_recount(LvPlan* p, int n, cudaStream_t s) {
+  SP_CHECK_CUDA(cudaMemsetAsync(p->tot.p, 0, sizeof(double) * n, s));
+  SP_CHECK_CUDA(cudaMemsetAsync(p->csize.p, 0, sizeof(int32_t) * n, s));
+  lv::k_tot<<<num_sms() * 8, 256, 0, s>>>(n, p->comm.p, p->kv.p, p->tot.p, p->csize.p);
+  SP_CHECK_LAUNCH();
+  return SP_OK;
+}
+
+// One sub-sweep over the vertices of one parity, all degree bins.
+static int lv_subsweep(LvPlan* p, lv::MoveArgs a, const int counts[3], int cap, int parity, cudaStream_t s) {
+  a.parity = parity;
+  const int g = num_sms() * 8;
+  if (counts[0]) {
+    a.list = p->lists.p;
+    a.nlist = counts[0];
+    lv::k_move_warp<<<g, lv::THREADS, 0, s>>>(a);
+    SP_CHECK_LAUNCH();
+  }
+  if (counts[1]) {
+    a.list = p->lists.p + cap;
+    a.nlist = counts[1];
+    const int slots = lv::CTA_SLOTS_MAX;  // degree <= 8192 fits at load factor <= 1/2
+    const size_t dyn = (size_t)slots * (sizeof(double) + sizeof(int32_t));
+    SP_CHECK_CUDA(cudaFuncSetAttribute(lv::k_move_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+    lv::k_move_cta<false><<<num_sms(), lv::THREADS, dyn, s>>>(a, slots);
+    SP_CHECK_LAUNCH();
+  }
+  if (counts[2]) {
+    a.list = p->lists.p + 2 * (size_t)cap;
+    a.nlist = counts[2];
+    lv::k_move_cta<true><<<num_sms() * 2, lv::THREADS, 0, s>>>(a, 0);
+    SP_CHECK_LAUNCH();
+  }
+  return SP_OK;
+}
+
 }  // namespace sp
+
+using namespace sp;
+
+extern "C" int sp_louvain(sp_graph_h g, const float* weight, double threshold, int32_t* community, double* modularity,
+                          int32_t* levels_out) {
+  if (!g || !modularity) {
+    set_error("sp_louvain: invalid argument");
+    return SP_ERR_INVALID;
+  }
+  if (!g->lv) g->lv = new LvPlan();
+  LvPlan* p = g->lv;
+  cudaStream_t s = g->stream;
+  const int n0 = g->V;
+  const int64_t m0 = g->E;
+  const int gs = num_sms() * 8;
+  // level 0 = the input graph; weights as FP64
+  SP_TRY(p->off[0].alloc(n0 + 1));
+  SP_TRY(p->adj[0].alloc(m0));
+  SP_TRY(p->w[0].alloc(m0));
+  SP_TRY(p->sl[0].alloc(n0));
+  SP_CHECK_CUDA(cudaMemcpyAsync(p->off[0].p, g->off.p, sizeof(int32_t) * (n0 + 1), cudaMemcpyDeviceToDevice, s));
+  if (m0) SP_CHECK_CUDA(cudaMemcpyAsync(p->adj[0].p, g->adj.p, sizeof(int32_t) * m0, cudaMemcpyDeviceToDevice, s));
+  const float* dw = nullptr;
+  dbuf<float> wtmp;
+  if (weight) {
+    SP_TRY(wtmp.alloc(m0));
+    if (m0) SP_CHECK_CUDA(cudaMemcpyAsync(wtmp.p, weight, sizeof(float) * m0, cudaMemcpyDefault, s));
+    dw = wtmp.p;
+  }
+  lv::k_f2d<<<gs, 256, 0, s>>>(dw, p->w[0].p, m0);
+  SP_CHECK_LAUNCH();
+  SP_CHECK_CUDA(cudaMemsetAsync(p->sl[0].p, 0, sizeof(double) * n0, s));
+  SP_TRY(p->comm.alloc(n0));
+  SP_TRY(p->newcomm.alloc(n0));
+  SP_TRY(p->csize.alloc(n0));
+  SP_TRY(p->used.alloc(n0 + 1));
+  SP_TRY(p->newid.alloc(n0 + 1));
+  SP_TRY(p->cnt.alloc(n0 + 1));
+  SP_TRY(p->pos.alloc(n0 + 1));
+  SP_TRY(p->orig.alloc(n0));
+  SP_TRY(p->lists.alloc((size_t)3 * n0));
+  SP_TRY(p->rowcnt.alloc(n0 + 1));
+  SP_TRY(p->kv.alloc(n0));
+  SP_TRY(p->tot.alloc(n0));
+  SP_TRY(p->in.alloc(n0));
+  SP_TRY(p->scal.alloc(2));
+  SP_TRY(p->icnt.alloc(4));
+  lv::k_init_comm<<<gs, 256, 0, s>>>(n0, p->orig.p, p->newcomm.p);  // orig[v] = v
+  SP_CHECK_LAUNCH();
+
+  // total weight W (constant over levels)
+  lv::Level L{n0, p->off[0].p, p->adj[0].p, p->w[0].p, p->sl[0].p};
+  SP_CHECK_CUDA(cudaMemsetAsync(p->scal.p + 1, 0, sizeof(double), s));
+  lv::k_kv<<<gs, 256, 0, s>>>(L, p->kv.p, p->scal.p + 1);
+  SP_CHECK_LAUNCH();
+  double W = 0;
+  SP_TRY(copy_out(&W, p->scal.p + 1, sizeof(double), s));
+  if (!(W > 0)) {
+    *modularity = 0.0;
+    if (levels_out) *levels_out = 0;
+    if (community) {
+      lv::k_init_comm<<<gs, 256, 0, s>>>(n0, p->comm.p, p->newcomm.p);
+      SP_CHECK_LAUNCH();
+      SP_TRY(copy_out(community, p->comm.p, sizeof(int32_t) * n0, s));
+    }
+    return SP_OK;
+  }
+
+  int cur = 0, levels = 0;
+  double qcur = 0;
+  const int max_levels = 32, max_sweeps = 100;
+  bool first = true;
+  while (true) {
+    const int n = L.n;
+    // communities start as singletons
+    lv::k_init_comm<<<gs, 256, 0, s>>>(n, p->comm.p, p->newcomm.p);
+    SP_CHECK_LAUNCH();
+    if (!first) {
+      lv::k_kv<<<gs, 256, 0, s>>>(L, p->kv.p, nullptr);
+      SP_CHECK_LAUNCH();
+    }
+    SP_TRY(lv_recount(p, n, s));
+    double qlev0 = 0;
+    SP_TRY(lv_modularity(p, L, W, s, &qlev0));
+    if (first) qcur = qlev0;
+    first = false;
+    // degree bins
+    SP_CHECK_CUDA(cudaMemsetAsync(p->icnt.p, 0, sizeof(int) * 4, s));
+    lv::k_bins<<<gs, 256, 0, s>>>(n, L.off, p->lists.p, p->icnt.p, n0);
+    SP_CHECK_LAUNCH();
+    int counts[4];
+    SP_TRY(copy_out(counts, p->icnt.p, sizeof(int) * 4, s));
+    if (counts[2]) {
+      // global tables for the highest-degree vertices: 2 * degree slots (power of two)
+      std::vector<int32_t> big(counts[2]);
+      SP_TRY(copy_out(big.data(), p->lists.p + 2 * (size_t)n0, sizeof(int32_t) * counts[2], s));
+      std::vector<int32_t> hoff(n + 1);
+      SP_TRY(copy_out(hoff.data(), L.off, sizeof(int32_t) * (n + 1), s));
+      std::vector<int64_t> go(counts[2] + 1, 0);
+      for (int k = 0; k < counts[2]; ++k) {
+        int64_t d = hoff[big[k] + 1] - hoff[big[k]], sl = 1;
+        while (sl < 2 * d) sl <<= 1;
+        go[k + 1] = go[k] + sl;
+      }
+      SP_TRY(p->goff.alloc(counts[2] + 1));
+      SP_TRY(p->gval.alloc(go.back()));
+      SP_TRY(p->gkey.alloc(go.back()));
+      SP_CHECK_CUDA(cudaMemcpyAsync(p->goff.p, go.data(), sizeof(int64_t) * go.size(), cudaMemcpyHostToDevice, s));
+    }
+    lv::MoveArgs a;
+    a.L = L;
+    a.comm = p->comm.p;
+    a.tot = p->tot.p;
+    a.csize = p->csize.p;
+    a.kv = p->kv.p;
+    a.newcomm = p->newcomm.p;
+    a.W = W;
+    a.gtab_val = p->gval.p;
+    a.gtab_key = p->gkey.p;
+    a.gtab_off = p->goff.p;
+    double qold = qlev0, qnew = qlev0;
+    for (int sweep = 0; sweep < max_sweeps; ++sweep) {
+      for (int parity = 0; parity < 2; ++parity) {
+        SP_TRY(lv_subsweep(p, a, counts, n0, parity, s));
+        SP_CHECK_CUDA(cudaMemsetAsync(p->icnt.p + 3, 0, sizeof(int), s));
+        lv::k_apply<<<gs, 256, 0, s>>>(n, parity, p->comm.p, p->newcomm.p, p->icnt.p + 3);
+        SP_CHECK_LAUNCH();
+        SP_TRY(lv_recount(p, n, s));
+      }
+      qold = qnew;
+      SP_TRY(lv_modularity(p, L, W, s, &qnew));
+      if (!(qnew - qold > threshold)) break;
+    }
+    ++levels;
+    // renumber communities
+    SP_CHECK_CUDA(cudaMemsetAsync(p->used.p, 0, sizeof(int32_t) * (n + 1), s));
+    lv::k_mark<<<gs, 256, 0, s>>>(n, p->comm.p, p->used.p);
+    SP_CHECK_LAUNCH();
+    SP_TRY(dev_scan(p, p->used.p, p->newid.p, n + 1, s));
+    int C = 0;
+    SP_TRY(copy_out(&C, p->newid.p + n, sizeof(int32_t), s));
+    lv::k_compose<<<gs, 256, 0, s>>>(n0, p->orig.p, p->comm.p, p->newid.p);
+    SP_CHECK_LAUNCH();
+    const bool improved = qnew - qcur > threshold;
+    qcur = std::max(qcur, qnew);
+    if (!improved || C == n || levels >= max_levels) {
+      qcur = qnew;
+      break;
+    }
+    // aggregate: communities become vertices
+    const int nx = cur ^ 1;
+    lv::k_count_ext<<<gs, 256, 0, s>>>(L, p->comm.p, p->cnt.p);
+    SP_CHECK_LAUNCH();
+    SP_CHECK_CUDA(cudaMemsetAsync(p->cnt.p + n, 0, sizeof(int32_t), s));
+    SP_TRY(dev_scan(p, p->cnt.p, p->pos.p, n + 1, s));
+    int mx = 0;
+    SP_TRY(copy_out(&mx, p->pos.p + n, sizeof(int32_t), s));
+    SP_TRY(p->keys.alloc(std::max(1, mx)));
+    SP_TRY(p->vals.alloc(std::max(1, mx)));
+    SP_TRY(p->skeys.alloc(std::max(1, mx)));
+    SP_TRY(p->svals.alloc(std::max(1, mx)));
+    SP_TRY(p->ukeys.alloc(std::max(1, mx)));
+    SP_TRY(p->uvals.alloc(std::max(1, mx)));
+    SP_TRY(p->sl[nx].alloc(C));
+    SP_CHECK_CUDA(cudaMemsetAsync(p->sl[nx].p, 0, sizeof(double) * C, s));
+    lv::k_emit<<<gs, 256, 0, s>>>(L, p->comm.p, p->newid.p, p->pos.p, p->keys.p, p->vals.p, p->sl[nx].p);
+    SP_CHECK_LAUNCH();
+    int bits = 1;
+    while ((1ll << bits) < C) ++bits;
+    size_t tb = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tb, p->keys.p, p->skeys.p, p->vals.p, p->svals.p, mx, 0, 32 + bits, s);
+    SP_TRY(p->temp.alloc(tb));
+    cub::DeviceRadixSort::SortPairs(p->temp.p, tb, p->keys.p, p->skeys.p, p->vals.p, p->svals.p, mx, 0, 32 + bits, s);
+    g_launches++;
+    tb = 0;
+    cub::DeviceReduce::ReduceByKey(nullptr, tb, p->skeys.p, p->ukeys.p, p->svals.p, p->uvals.p, p->icnt.p,
+                                   cub::Sum(), mx, s);
+    SP_TRY(p->temp.alloc(tb));
+    cub::DeviceReduce::ReduceByKey(p->temp.p, tb, p->skeys.p, p->ukeys.p, p->svals.p, p->uvals.p, p->icnt.p,
+                                   cub::Sum(), mx, s);
+    g_launches++;
+    int mu = 0;
+    if (mx) SP_TRY(read_int(p->icnt.p, &mu, s));
+    SP_TRY(p->off[nx].alloc(C + 1));
+    SP_TRY(p->adj[nx].alloc(std::max(1, mu)));
+    SP_TRY(p->w[nx].alloc(std::max(1, mu)));
+    SP_CHECK_CUDA(cudaMemsetAsync(p->rowcnt.p, 0, sizeof(int32_t) * (C + 1), s));
+    if (mu) {
+      lv::k_build_rows<<<gs, 256, 0, s>>>(mu, p->ukeys.p, p->adj[nx].p, p->rowcnt.p);
+      SP_CHECK_LAUNCH();
+      SP_CHECK_CUDA(cudaMemcpyAsync(p->w[nx].p, p->uvals.p, sizeof(double) * mu, cudaMemcpyDeviceToDevice, s));
+    }
+    SP_TRY(dev_scan(p, p->rowcnt.p, p->off[nx].p, C + 1, s));
+    cur = nx;
+    L = lv::Level{C, p->off[cur].p, p->adj[cur].p, p->w[cur].p, p->sl[cur].p};
+  }
+  *modularity = qcur;
+  if (levels_out) *levels_out = levels;
+  if (community) SP_TRY(copy_out(community, p->orig.p, sizeof(int32_t) * n0, s));
+  return SP_OK;
+}

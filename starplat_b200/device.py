@@ -165,3 +165,15 @@ class DeviceGraph:
         sig = np.empty((k, self.V), np.float64)
         check("sp_bfs_sigma", lib().sp_bfs_sigma(self.handle, _ptr(sources), k, _ptr(lvl), _ptr(sig)))
         return lvl, sig
+
+    def louvain(self, weight=None, threshold: float = 1e-4, community=None):
+        """Louvain; returns (modularity, community[V] int32, levels)."""
+        if community is None:
+            community = np.empty(self.V, np.int32)
+        if weight is not None and str(weight.dtype) not in ("float32", "torch.float32"):
+            raise TypeError("Louvain weights must be float32")
+        q = ctypes.c_double()
+        lv = ctypes.c_int32()
+        check("sp_louvain", lib().sp_louvain(self.handle, _ptr(weight), threshold, _ptr(community), ctypes.byref(q),
+                                             ctypes.byref(lv)))
+        return float(q.value), community, int(lv.value)

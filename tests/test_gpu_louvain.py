@@ -1,0 +1,77 @@
+"""GPU parity: Louvain modularity within 1e-3 of the sequential restatement of the
+DSL (labels are order dependent and are not compared); the returned partition
+must have exactly the returned modularity."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from starplat_b200 import generators as G
+from starplat_b200.algorithms import Compute_CD, device_graph
+
+from graphs import clique, from_pairs
+
+pytestmark = pytest.mark.gpu
+
+
+def check(g, w=None, tol=1e-3):
+    q, comm, levels = device_graph(g).louvain(w)
+    qr, _, _ = O.louvain(g.indexofNodes, g.edgeList, w)
+    assert abs(q - qr) < tol, (g.name, q, qr)
+    # the partition really has that modularity
+    assert abs(O.modularity(g.indexofNodes, g.edgeList, comm, w) - q) < 1e-9
+    # dense community ids
+    assert comm.min() >= 0 and np.unique(comm).shape[0] == comm.max() + 1
+    return q, qr
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_louvain_sbm(seed):
+    g = G.sbm(20000, 24, exponent=2.0, avg_degree=32, p_in=0.8, seed=seed)
+    check(g)
+
+
+def test_louvain_er_and_rmat():
+    check(G.erdos_renyi(5000, 10, seed=3), tol=2e-2)
+    check(G.rmat(12, 8, seed=2), tol=2e-2)
+
+
+def test_louvain_weighted():
+    g = G.sbm(8000, 10, seed=4)
+    w = (1.0 + (G.hash_weights(g, 5, 0, 9, True) % 10)).astype(np.float32)
+    check(g, w)
+
+
+def test_louvain_known_answers():
+    # two disjoint K5: Q = 2 * (20/40 - (20/40)^2) = 0.5
+    i, j = np.triu_indices(5, 1)
+    pairs = np.concatenate([np.stack([i, j], 1), np.stack([i + 5, j + 5], 1)])
+    g = from_pairs(10, pairs, symmetrize=True, name="2K5")
+    q, comm, _ = device_graph(g).louvain()
+    assert abs(q - 0.5) < 1e-12
+    assert len(set(comm[:5])) == 1 and len(set(comm[5:])) == 1 and comm[0] != comm[5]
+    # one clique: everything in one community, Q = 0
+    q, comm, _ = device_graph(clique(8)).louvain()
+    assert abs(q) < 1e-12 and len(set(comm)) == 1
+    # no edges: Q = 0, singletons
+    g0 = from_pairs(4, np.zeros((0, 2), np.int32))
+    q, comm, lv = device_graph(g0).louvain()
+    assert q == 0.0 and sorted(comm.tolist()) == [0, 1, 2, 3]
+
+
+def test_louvain_hub_uses_cta_and_global_tables():
+    # a star with 20000 leaves plus cliques hanging off it: degrees in every bin
+    rng = np.random.default_rng(0)
+    n = 20001
+    pairs = [np.stack([np.zeros(n - 1, np.int32), np.arange(1, n, dtype=np.int32)], 1)]
+    for b in range(1, n - 200, 200):
+        i, j = np.triu_indices(100, 1)
+        pairs.append(np.stack([i + b, j + b], 1).astype(np.int32))
+    g = from_pairs(n, np.concatenate(pairs), symmetrize=True, name="hubcliques")
+    check(g, tol=2e-2)
+
+
+def test_louvain_entry_point():
+    g = G.sbm(5000, 8, seed=7)
+    q = Compute_CD(g)
+    qr, _, _ = O.louvain(g.indexofNodes, g.edgeList, None)
+    assert abs(q - qr) < 1e-3
