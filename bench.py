@@ -1,22 +1,37 @@
-"""Benchmark: GTEPS of the static-graph hot path on B200.
+"""Benchmark: GTEPS of the static-graph hot path on B200 (one JSON line on rank 0).
 
-Headline workload (one JSON line on rank 0): PageRank, pull over the reverse CSR,
-on a directed R-MAT graph, scale 22 (4,194,304 vertices), edge factor 16,
+Headline (value / e2e / roofline / cpu_baseline): PageRank, pull over the reverse
+CSR, on a directed R-MAT graph, scale 22 (4,194,304 vertices), edge factor 16,
 a/b/c/d = .57/.19/.19/.05, seed 1, damping 0.85, L1 threshold 1e-6, maxIter 100.
-A step is one full PageRank call (all iterations until convergence); GTEPS =
-E * iterations / time.
+A step is one full PageRank call (all iterations until convergence);
+GTEPS = E * iterations / time.
 
-  value       device-resident CSR (uploaded before timing), events on the stream
-  e2e         through the C ABI with HOST buffers: upload (pinned H2D) + PageRank +
-              result D2H, every step
-  roofline    the iteration kernel: algorithmic bytes 8E + 16V per launch over its
-              average launch time (from two fixed-iteration runs), vs measured HBM peak
-  cpu_baseline  the OpenMP form of the generated code (oracle port), bounded sample
+  value         device-resident CSR (uploaded before timing), CUDA events on the stream
+  e2e           through the C ABI with HOST buffers: upload from pinned memory +
+                PageRank + result D2H, every step
+  roofline      the iteration kernel: algorithmic bytes 8E + 16V per launch over its
+                average launch time (from two fixed-iteration runs) vs the measured HBM peak
+  cpu_baseline  the OpenMP form of the generated code (oracle port), 3 iterations
 
---impl reference times that OpenMP form alone on the host cores (the reference's
-CPU path; its generated sources cannot be produced here).
-Multi-GPU: PageRank on one graph is replicated per GPU ("replicas only"); value
-sums the edges all ranks processed over the max time.
+"algorithms" holds the other workloads of the metric "GTEPS per algorithm", each
+timed the same way (device-resident, events), with the plain fixed-schedule GPU
+form beside the tuned one, an algorithm-level roofline fraction and a bounded CPU
+baseline:
+  tc_rmat16        triangle counting, undirected R-MAT 16 ef16 (GTEPS = m / t)
+  sssp_rmat23      SSSP, directed R-MAT 23 ef16, weights U[1,100] (E_r / t)
+  sssp_grid4096    SSSP, 4096x4096 4-neighbour grid, weights U[1,1000] (E_r / t)
+  bc_rmat20        BC, undirected R-MAT 20 ef16, 256 sources (S * E_r / t)
+  bc_er1000        BC, 1000 ER graphs (1k-50k vertices, degree 8-32), 16 sources each
+  louvain_sbm1m    Louvain, planted partition 1,048,576 vertices, 256 blocks (E * sweeps / t)
+Inputs are seeded synthetic graphs with the configs' shapes (no dataset is
+available offline). Every workload's inputs exceed L2 (126 MB) except the TC
+graph (7 MB CSR), which is small by definition of its config.
+
+--impl reference times the reference's CPU path (the OpenMP form of the generated
+PageRank, restated in oracle/) alone on the host cores, same metric and config.
+Multi-GPU: the graph algorithms here run per graph on one GPU, so --gpus N runs N
+replicas ("replicas only"); value sums the edges all ranks processed over the max
+time (weak scaling).
 """
 from __future__ import annotations
 
@@ -37,6 +52,7 @@ import numpy as np  # noqa: E402
 PR_SCALE, PR_EF, PR_SEED = 22, 16, 1
 BETA, DELTA, MAX_ITER = 1e-6, 0.85, 100
 METRIC = "GTEPS per algorithm on 1 B200 (pagerank headline)"
+INT_MAX = 2**31 - 1
 
 
 def peaks():
@@ -48,7 +64,7 @@ def peaks():
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """nvidia-smi sampling during a timed region."""
 
     def __init__(self, index: int):
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
@@ -60,6 +76,7 @@ class Clocks:
                                        "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
+        time.sleep(0.25)
 
     def stop(self):
         if self.p is None:
@@ -70,8 +87,15 @@ class Clocks:
         self.f.flush()
         rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
         os.unlink(self.f.name)
-        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [num(r[1]) for r in rows if len(r) >= 9 and num(r[1]) is not None]
+        mx = [num(r[2]) for r in rows if len(r) >= 9 and num(r[2]) is not None]
         reasons = set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in rows:
@@ -84,15 +108,15 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
-def make_graph():
+def pr_graph(scale=None):
     from starplat_b200 import generators as G
 
     t = time.time()
-    g = G.rmat(PR_SCALE, PR_EF, seed=PR_SEED, directed=True)
+    g = G.rmat(scale or PR_SCALE, PR_EF, seed=PR_SEED, directed=True)
     return g, time.time() - t
 
 
-def cpu_baseline(g, iters: int = 3):
+def cpu_pagerank(g, iters: int = 3):
     """OpenMP form of the generated PageRank on the host cores, `iters` iterations."""
     from oracle import oracle as O
 
@@ -104,15 +128,13 @@ def cpu_baseline(g, iters: int = 3):
             "sample": f"{it} iterations of the OpenMP-form PageRank over the full graph ({dt:.2f} s)"}
 
 
-def run_reference(args, rank, world):
+def run_reference(args, rank):
     if rank != 0:
         return
-    g, _ = make_graph()
+    g, _ = pr_graph()
     for _ in range(args.warmup):
-        cpu_baseline(g, 1)
-    vals = []
-    for _ in range(args.steps):
-        vals.append(cpu_baseline(g, 3))
+        cpu_pagerank(g, 1)
+    vals = [cpu_pagerank(g, 3) for _ in range(args.steps)]
     v = statistics.median([x["value"] for x in vals])
     line = {"metric": METRIC, "value": v, "unit": "GTEPS", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
@@ -124,6 +146,252 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------------------- timing helpers
+
+def timed(fn, steps, warmup, stream):
+    """Run fn() warmup times, then time `steps` runs with CUDA events on `stream`.
+    Returns (ms per step, list of fn results)."""
+    import torch
+
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    res = [fn() for _ in range(steps)]
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / steps, res
+
+
+def roof(alg_bytes, ms, hbm):
+    gbs = alg_bytes / (ms / 1e3) / 1e9
+    return {"achieved_gbs": round(gbs, 1), "frac": round(gbs / hbm, 4), "alg_bytes": int(alg_bytes)}
+
+
+def component_edges(g):
+    """Connected components of an undirected CSR: (label per vertex, edge entries per component)."""
+    from scipy.sparse import csr_matrix
+    from scipy.sparse.csgraph import connected_components
+
+    A = csr_matrix((np.ones(g.E, np.int8), g.edgeList, g.indexofNodes), shape=(g.V, g.V))
+    _, lab = connected_components(A, directed=False)
+    ce = np.bincount(lab, weights=np.diff(g.indexofNodes))
+    return lab, ce
+
+
+# ----------------------------------------------------------------------------- other algorithms
+
+def bench_tc(steps, warmup, stream, hbm, cpu):
+    from starplat_b200 import _lib
+    from starplat_b200 import generators as G
+    from starplat_b200.device import DeviceGraph
+
+    g = G.rmat(16, 16, seed=1)
+    m = g.E // 2
+    deg = np.diff(g.indexofNodes).astype(np.int64)
+    u = np.repeat(np.arange(g.V), deg)
+    v = g.edgeList.astype(np.int64)
+    keep = (deg[u] < deg[v]) | ((deg[u] == deg[v]) & (u < v))
+    dplus = np.bincount(u[keep], minlength=g.V)
+    eplus = int(keep.sum())
+    alg = 4 * int((dplus[u[keep]] + dplus[v[keep]]).sum()) + 4 * (g.V + 1) + 4 * eplus
+    out = {"workload": "tc rmat16 ef16 undirected seed1", "V": g.V, "m": m, "E_plus": eplus}
+    with DeviceGraph.from_csr(g, with_weights=False) as dg:
+        dg.set_stream(stream)
+        ms, res = timed(lambda: dg.tc(), steps, warmup, stream)
+        msp, resp = timed(lambda: dg.tc(_lib.SP_TC_PLAIN), max(1, steps // 2), 1, stream)
+    out.update({"triangles": res[0], "value": m / (ms / 1e3) / 1e9, "unit": "GTEPS", "ms": ms,
+                "plain": {"value": m / (msp / 1e3) / 1e9, "ms": msp, "triangles": resp[0]},
+                "roofline": roof(alg, ms, hbm)})
+    if cpu:
+        from oracle import oracle as O
+
+        # work model of the OpenMP form: every (u, w) pair builds and scans N(u)
+        k = 64
+        low = v < u
+        hi_cnt = np.bincount(u[v > u], minlength=g.V)
+        sdeg = np.bincount(u[low], weights=deg[v[low]] + 1, minlength=g.V)
+        work = sdeg * hi_cnt
+        sample = work[np.arange(g.V) % k == 7].sum()
+        nt = O.num_threads()
+        kind = "reference" if O.ref_lib() is not None else "port"
+        fn = O.ref_tc if kind == "reference" else O.tc_omp
+        t = time.perf_counter()
+        tc_s = fn(g.indexofNodes, g.edgeList, nthreads=nt, vfirst=7, vstride=k)
+        dt = time.perf_counter() - t
+        est = dt * work.sum() / max(1.0, sample)
+        out["cpu_baseline"] = {"value": m / est / 1e9, "unit": "GTEPS", "cores": nt, "kind": kind,
+                               "sample": f"OpenMP Compute_TC loop with graph::check_if_nbr over every {k}th vertex "
+                                         f"({dt:.2f} s, {tc_s} triangles), scaled by the pair-scan work model "
+                                         f"to a full run of {est:.1f} s"}
+    return out
+
+
+def bench_sssp(name, g, src, steps, warmup, stream, hbm, cpu, cpu_mode):
+    import torch
+
+    from starplat_b200 import _lib
+    from starplat_b200.device import DeviceGraph
+
+    out = {"workload": name, "V": g.V, "E": g.E, "source": int(src)}
+    with DeviceGraph.from_csr(g) as dg:
+        dg.set_stream(stream)
+        dist = torch.empty(g.V, dtype=torch.int32, device="cuda")
+        ms, res = timed(lambda: dg.sssp(src, out=dist), steps, warmup, stream)
+        d = dist.cpu().numpy()
+        reached = d < INT_MAX
+        er = int(np.diff(g.indexofNodes)[reached].sum())
+        nr = int(reached.sum())
+        delta = dg.tune_get("sssp.delta")
+        msp, resp = timed(lambda: dg.sssp(src, out=dist, variant=_lib.SP_SSSP_PLAIN), 1, 0, stream)
+        same = bool(np.array_equal(dist.cpu().numpy(), d))
+    out.update({"value": er / (ms / 1e3) / 1e9, "unit": "GTEPS", "ms": ms, "E_r": er, "reached": nr,
+                "rounds": res[0][1], "delta_knob": delta,
+                "plain": {"value": er / (msp / 1e3) / 1e9, "ms": msp, "rounds": resp[0][1], "same_distances": same},
+                "roofline": roof(12 * er + 12 * g.V, ms, hbm)})
+    if cpu:
+        from oracle import oracle as O
+
+        nt = O.num_threads()
+        t = time.perf_counter()
+        if cpu_mode == "omp":
+            _, rounds = O.sssp_omp(g.indexofNodes, g.edgeList, g.edgeLen, src, nthreads=nt)
+            dt = time.perf_counter() - t
+            out["cpu_baseline"] = {"value": er / dt / 1e9, "unit": "GTEPS", "cores": nt, "kind": "port",
+                                   "sample": f"OpenMP fixed-point Compute_SSSP to convergence ({rounds} rounds, {dt:.2f} s)"}
+        else:
+            O.sssp(g.indexofNodes, g.edgeList, g.edgeLen, src)
+            dt = time.perf_counter() - t
+            out["cpu_baseline"] = {"value": er / dt / 1e9, "unit": "GTEPS", "cores": 1, "kind": "port",
+                                   "sample": f"sequential Dijkstra ({dt:.2f} s); the OpenMP fixed-point form needs "
+                                             "thousands of full-vertex sweeps on this high-diameter grid"}
+    return out
+
+
+def bench_bc(steps, warmup, stream, hbm, cpu):
+    from starplat_b200 import _lib
+    from starplat_b200 import generators as G
+    from starplat_b200.device import DeviceGraph
+
+    g = G.rmat(20, 16, seed=1)
+    srcs = G.pick_sources(g, 256, seed=20)
+    lab, ce = component_edges(g)
+    er = ce[lab[srcs]]
+    sum_er = int(er.sum())
+    alg = int(16 * er.sum() + 32 * g.V * len(srcs))
+    out = {"workload": "bc rmat20 ef16 undirected seed1, 256 sources", "V": g.V, "E": g.E, "sources": len(srcs),
+           "sum_E_r": sum_er}
+    with DeviceGraph.from_csr(g, with_weights=False) as dg:
+        dg.set_stream(stream)
+        ms, _ = timed(lambda: dg.bc(srcs), steps, warmup, stream)
+        few = srcs[:8]
+        msp, _ = timed(lambda: dg.bc(few, variant=_lib.SP_BC_PLAIN), 1, 0, stream)
+    out.update({"value": sum_er / (ms / 1e3) / 1e9, "unit": "GTEPS", "ms": ms,
+                "plain": {"value": float(er[:8].sum()) / (msp / 1e3) / 1e9, "ms_8_sources": msp,
+                          "sample": "8 sources, one at a time"},
+                "roofline": roof(alg, ms, hbm)})
+    if cpu:
+        from oracle import oracle as O
+
+        nt = O.num_threads()
+        t = time.perf_counter()
+        O.bc_omp(g.indexofNodes, g.edgeList, srcs[:4], nthreads=nt)
+        dt = time.perf_counter() - t
+        out["cpu_baseline"] = {"value": float(er[:4].sum()) / dt / 1e9, "unit": "GTEPS", "cores": nt, "kind": "port",
+                               "sample": f"OpenMP-form Compute_BC over 4 of the 256 sources ({dt:.2f} s)"}
+    return out
+
+
+def bench_bc_er(steps, warmup, stream, hbm, cpu):
+    from starplat_b200 import generators as G
+    from starplat_b200.device import DeviceGraph
+
+    t0 = time.time()
+    gs = G.er_batch(1000, 1000, 50000, 8, 32, seed=11)
+    voff = np.zeros(len(gs) + 1, np.int64)
+    eoff = np.zeros(len(gs) + 1, np.int64)
+    for k, g in enumerate(gs):
+        voff[k + 1] = voff[k] + g.V
+        eoff[k + 1] = eoff[k] + g.E
+    V, E = int(voff[-1]), int(eoff[-1])
+    off = np.empty(V + 1, np.int32)
+    adj = np.empty(E, np.int32)
+    srcs, soff, er_tot, er_k = [], [0], 0, []
+    for k, g in enumerate(gs):
+        off[voff[k]:voff[k + 1]] = g.indexofNodes[:-1] + eoff[k]
+        adj[eoff[k]:eoff[k + 1]] = g.edgeList + voff[k]
+        s = G.pick_sources(g, 16, seed=k)
+        lab, ce = component_edges(g)
+        er_k.append(int(ce[lab[s]].sum()))
+        er_tot += er_k[-1]
+        srcs.append(s + voff[k])
+        soff.append(soff[-1] + len(s))
+    off[V] = E
+    srcs = np.concatenate(srcs).astype(np.int32)
+    soff = np.array(soff, np.int32)
+    voff32 = voff.astype(np.int32)
+    gen_s = time.time() - t0
+    alg = int(16 * er_tot + 32 * sum(g.V * 16 for g in gs))
+    out = {"workload": "bc 1000 ER graphs, n log-uniform in [1e3, 5e4], degree U[8,32], 16 sources each, seed11",
+           "V": V, "E": E, "sources": int(srcs.shape[0]), "sum_E_r": er_tot, "graph_gen_s": round(gen_s, 1)}
+    with DeviceGraph(off, adj, None, off, adj) as dg:
+        dg.set_stream(stream)
+        ms, _ = timed(lambda: dg.bc_graphs(voff32, soff, srcs), steps, warmup, stream)
+    out.update({"value": er_tot / (ms / 1e3) / 1e9, "unit": "GTEPS", "ms": ms, "roofline": roof(alg, ms, hbm)})
+    if cpu:
+        from oracle import oracle as O
+
+        nt = O.num_threads()
+        t = time.perf_counter()
+        er_s = 0
+        for k in range(0, 1000, 50):
+            g = gs[k]
+            O.bc_omp(g.indexofNodes, g.edgeList, srcs[soff[k]:soff[k + 1]] - voff32[k], nthreads=nt)
+            er_s += er_k[k]
+        dt = time.perf_counter() - t
+        out["cpu_baseline"] = {"value": er_s / dt / 1e9, "unit": "GTEPS", "cores": nt, "kind": "port",
+                               "sample": f"OpenMP-form Compute_BC on 20 of the 1000 graphs, all 16 sources ({dt:.2f} s)"}
+    return out
+
+
+def bench_louvain(steps, warmup, stream, hbm, cpu):
+    from starplat_b200 import generators as G
+    from starplat_b200.device import DeviceGraph
+
+    g = G.sbm(1 << 20, 256, exponent=2.0, avg_degree=32, p_in=0.8, seed=1)
+    out = {"workload": "louvain sbm 1048576 vertices, 256 blocks (power-law sizes, exponent 2), degree 32, "
+                       "80% intra, unit weights, seed1", "V": g.V, "E": g.E}
+    res = {}
+    with DeviceGraph.from_csr(g, with_weights=False) as dg:
+        dg.set_stream(stream)
+
+        def run():
+            q, _, lv = dg.louvain(None, 1e-4)
+            res["q"], res["levels"], res["sweeps"] = q, lv, dg.last_louvain_sweeps
+            return q
+
+        ms, _ = timed(run, steps, warmup, stream)
+    sweeps = res["sweeps"]
+    out.update({"value": g.E * sweeps / (ms / 1e3) / 1e9, "unit": "GTEPS", "ms": ms, "modularity": res["q"],
+                "levels": res["levels"], "sweeps": sweeps,
+                "roofline": roof((12 * g.E + 16 * g.V) * sweeps, ms, hbm)})
+    if cpu:
+        from oracle import oracle as O
+
+        t = time.perf_counter()
+        q, _, lv, sw = O.louvain(g.indexofNodes, g.edgeList, None, 1e-4, with_sweeps=True)
+        dt = time.perf_counter() - t
+        out["cpu_baseline"] = {"value": g.E * sw / dt / 1e9, "unit": "GTEPS", "cores": 1, "kind": "port",
+                               "modularity": q, "sample": f"sequential restatement of the DSL, full run "
+                                                          f"({sw} sweeps, {lv} levels, {dt:.2f} s)"}
+        out["modularity_minus_cpu"] = res["q"] - q
+    return out
+
+
+# ----------------------------------------------------------------------------- main
+
 def main():
     global PR_SCALE
     ap = argparse.ArgumentParser()
@@ -133,17 +401,20 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true",
-                    help="device-resident timing only (no roofline/e2e/CPU legs): for profiler runs")
-    ap.add_argument("--scale", type=int, default=PR_SCALE, help="R-MAT scale (profiling on smaller cases)")
+                    help="PageRank device-resident timing only (no other legs): for profiler runs")
+    ap.add_argument("--only", default="", help="comma list of extra workloads (default: all)")
+    ap.add_argument("--no-extras", action="store_true", help="headline PageRank only")
+    ap.add_argument("--scale", type=int, default=PR_SCALE, help="R-MAT scale of the PageRank graph")
     ap.add_argument("--tune", action="append", default=[], help="schedule knob key=value (sp_tune_set)")
     args = ap.parse_args()
     PR_SCALE = args.scale
+    args.warmup = max(3, args.warmup)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
-        return run_reference(args, rank, world)
+        return run_reference(args, rank)
 
     import torch
 
@@ -161,10 +432,17 @@ def main():
         if dist is not None:
             dist.barrier()
 
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
     from starplat_b200 import _lib
     from starplat_b200.device import DeviceGraph
 
-    g, gen_s = make_graph()
+    g, gen_s = pr_graph()
     V, E = g.V, g.E
     stream = torch.cuda.current_stream()
     dg = DeviceGraph.from_csr(g, with_weights=False)
@@ -174,7 +452,7 @@ def main():
         dg.tune_set(k, int(v))
     out = torch.empty(V, dtype=torch.float32, device="cuda")
 
-    for _ in range(max(3, args.warmup)):
+    for _ in range(args.warmup):
         _, iters, _ = dg.pagerank(BETA, DELTA, MAX_ITER, out=out)
 
     # ---- device-resident timing
@@ -194,11 +472,7 @@ def main():
     barrier()
     clocks = clk.stop()
     launches = _lib.launch_count() - l0
-    ms = ev0.elapsed_time(ev1)
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
     value = world * E * it_total / (ms / 1e3) / 1e9
     if args.quick:
         if rank == 0:
@@ -208,6 +482,8 @@ def main():
         if dist is not None:
             dist.destroy_process_group()
         return
+
+    hbm, hbm_kind = peaks()
 
     # ---- kernel roofline: average iteration-kernel time from two fixed-iteration runs
     def timed_fixed(n, reps=3):
@@ -227,17 +503,20 @@ def main():
     t1, t2 = timed_fixed(n1), timed_fixed(n2)
     per_launch_ms = (t2 - t1) / (n2 - n1)
     alg_bytes = 8 * E + 16 * V
-    hbm, hbm_kind = peaks()
     achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                 "traffic": None, "peak_kind": hbm_kind, "kernel": "sp::pr::k_iter",
                 "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": per_launch_ms}
-    tf = os.path.join(ROOT, "profiles", "pagerank_traffic.json")
+    tf = os.path.join(ROOT, "profiles", "pagerank_rmat22_traffic.json")
     if os.path.exists(tf):
         try:
             roofline["traffic"] = json.load(open(tf)).get("traffic_bytes_per_launch")
         except Exception:
             pass
+
+    # plain (generated-code form) PageRank for comparison
+    msp, resp = timed(lambda: dg.pagerank(BETA, DELTA, MAX_ITER, out=out, variant=_lib.SP_PR_PLAIN), 1, 1, stream)
+    pr_plain = {"value": E * resp[0][1] / (msp / 1e3) / 1e9, "ms_per_step": msp, "iterations": resp[0][1]}
 
     # ---- end to end through the C ABI with host buffers (pinned), every step
     pin = {k: torch.from_numpy(getattr(g, k)).pin_memory()
@@ -261,17 +540,54 @@ def main():
     for _ in range(e_steps):
         e_it += e2e_step()
     torch.cuda.synchronize()
-    e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e_s = float(t.item())
+    e_s = max_over_ranks(time.perf_counter() - t0)
     e2e = {"value": world * E * e_it / e_s / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h, "ms_per_step": 1e3 * e_s / e_steps}
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(g, 3)
+    cpu_ok = rank == 0 and world == 1 and not args.no_cpu_baseline
+    cpu = cpu_pagerank(g, 3) if cpu_ok else None
+    dg.free()
+    del g
+
+    # ---- the other algorithms of the metric
+    extras = {}
+    if not args.no_extras:
+        from starplat_b200 import generators as G
+
+        want = set(filter(None, args.only.split(","))) or {"tc_rmat16", "sssp_rmat23", "sssp_grid4096", "bc_rmat20",
+                                                           "bc_er1000", "louvain_sbm1m"}
+        ks, kw = max(1, min(args.steps, 5)), 2
+
+        def guarded(name, fn):
+            try:
+                extras[name] = fn()
+            except Exception as e:  # report, keep the headline line
+                extras[name] = {"error": f"{type(e).__name__}: {e}"}
+
+        if "tc_rmat16" in want:
+            guarded("tc_rmat16", lambda: bench_tc(ks, kw, stream, hbm, cpu_ok))
+        if "sssp_rmat23" in want:
+            def _s1():
+                gs = G.rmat(23, 16, seed=1, directed=True)
+                gs.edgeLen = G.hash_weights(gs, 23, 1, 100, False)
+                src = int(G.pick_sources(gs, 1, seed=23)[0])
+                return bench_sssp("sssp rmat23 ef16 directed seed1, w U[1,100]", gs, src, ks, kw, stream, hbm,
+                                  cpu_ok, "omp")
+            guarded("sssp_rmat23", _s1)
+        if "sssp_grid4096" in want:
+            def _s2():
+                gg = G.grid(4096, 4096)
+                gg.edgeLen = G.hash_weights(gg, 4096, 1, 1000, True)
+                src = int(np.random.default_rng(4096).integers(0, gg.V))
+                return bench_sssp("sssp grid 4096x4096 4-neighbour, w U[1,1000] symmetric", gg, src, max(1, ks // 2),
+                                  1, stream, hbm, cpu_ok, "dijkstra")
+            guarded("sssp_grid4096", _s2)
+        if "bc_rmat20" in want:
+            guarded("bc_rmat20", lambda: bench_bc(max(1, ks // 2), 1, stream, hbm, cpu_ok))
+        if "bc_er1000" in want:
+            guarded("bc_er1000", lambda: bench_bc_er(max(1, ks // 2), 1, stream, hbm, cpu_ok))
+        if "louvain_sbm1m" in want:
+            guarded("louvain_sbm1m", lambda: bench_louvain(max(1, ks // 2), 1, stream, hbm, cpu_ok))
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
@@ -281,9 +597,9 @@ def main():
                            "beta": BETA, "delta": DELTA, "max_iter": MAX_ITER, "iterations": it_total // args.steps,
                            "l2": "inputs larger than L2 (srcList %.2f GB streamed per iteration)" % (4 * E / 1e9),
                            "parallelism": "replicas" if world > 1 else "single", "graph_gen_s": round(gen_s, 2)},
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks}
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
+                "plain": pr_plain, "algorithms": extras}
         print(json.dumps(line), flush=True)
-    dg.free()
     if dist is not None:
         dist.destroy_process_group()
 

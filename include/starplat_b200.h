@@ -74,9 +74,13 @@ int sp_tune_get(sp_graph_h g, const char* key, int64_t* value);
 /* ---- triangle counting -------------------------------------------------------
  * Replaces generated `auto Compute_TC(graph& g)` (DSL staticDSLCodes/triangle_counting_dsl:1-13):
  *   count = sum_v sum_{u in N(v), u<v} sum_{w in N(v), w>v} [u->w is an edge]
- * Exact int64. Undirected graphs use a degree-ordered orientation; other graphs
- * follow the formula literally. */
-int sp_tc(sp_graph_h g, int64_t* triangle_count);
+ * Exact int64. SP_TC_TUNED: undirected graphs use a degree-ordered orientation
+ * and warp-cooperative hash intersection; other graphs follow the formula
+ * literally. SP_TC_PLAIN: the generated CUDA form (one thread per vertex, binary
+ * search per pair; libcuda.cuh:187-212). */
+#define SP_TC_TUNED 0
+#define SP_TC_PLAIN 1
+int sp_tc(sp_graph_h g, int64_t* triangle_count, int32_t variant);
 
 /* ---- PageRank ----------------------------------------------------------------
  * Replaces generated `void ComputePageRank(graph& g, float beta, float delta, int maxIter,
@@ -138,9 +142,10 @@ int sp_bc_graphs(sp_graph_h g, int32_t ngraphs, const int32_t* vertex_offset, co
  * the modularity). weight[E] in forward-CSR order, NULL = unit weights. Local moves
  * and aggregation repeat while modularity improves by more than `threshold`
  * (the DSL uses 1e-4). community (may be NULL) gets a dense community id per vertex;
- * *modularity the final Q; levels (may be NULL) the number of levels run. */
+ * *modularity the final Q; levels / sweeps (may be NULL) the number of levels and
+ * of local-move sweeps run. */
 int sp_louvain(sp_graph_h g, const float* weight, double threshold, int32_t* community, double* modularity,
-               int32_t* levels);
+               int32_t* levels, int32_t* sweeps);
 
 #ifdef __cplusplus
 }

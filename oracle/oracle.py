@@ -57,7 +57,7 @@ def lib():
         L.or_bc_omp.argtypes = [ctypes.c_int32, i32p, i32p, i32p, ctypes.c_int32, f32p, ctypes.c_int]
         L.or_louvain.restype = ctypes.c_double
         L.or_louvain.argtypes = [ctypes.c_int32, i32p, i32p, ctypes.c_void_p, ctypes.c_double, i32p,
-                                 ctypes.POINTER(ctypes.c_int32)]
+                                 ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]
         L.or_modularity.restype = ctypes.c_double
         L.or_modularity.argtypes = [ctypes.c_int32, i32p, i32p, ctypes.c_void_p, i32p]
         L.or_num_threads.restype = ctypes.c_int32
@@ -155,15 +155,18 @@ def bc_omp(off, adj, srcs, nthreads: int = 0) -> np.ndarray:
     return out
 
 
-def louvain(off, adj, w=None, threshold: float = 1e-4):
+def louvain(off, adj, w=None, threshold: float = 1e-4, with_sweeps: bool = False):
     V = len(off) - 1
     comm = np.empty(V, np.int32)
     levels = ctypes.c_int32(0)
+    sweeps = ctypes.c_int32(0)
     wp = None
     if w is not None:
         w = _c(w, np.float32)
         wp = w.ctypes.data
-    q = lib().or_louvain(V, _c(off), _c(adj), wp, threshold, comm, ctypes.byref(levels))
+    q = lib().or_louvain(V, _c(off), _c(adj), wp, threshold, comm, ctypes.byref(levels), ctypes.byref(sweeps))
+    if with_sweeps:
+        return float(q), comm, int(levels.value), int(sweeps.value)
     return float(q), comm, int(levels.value)
 
 

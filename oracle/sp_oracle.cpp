@@ -498,7 +498,8 @@ void or_bc_omp(int32_t V, const int32_t* off, const int32_t* adj, const int32_t*
 // (:40). Both loops stop when Q improves by no more than threshold (:34, :111, :208).
 // w may be null (unit weights). community_out[v] = final community of original v.
 double or_louvain(int32_t V, const int32_t* off, const int32_t* adj, const float* w,
-                  double threshold, int32_t* community_out, int32_t* levels_out) {
+                  double threshold, int32_t* community_out, int32_t* levels_out, int32_t* sweeps_out) {
+  int32_t sweeps = 0;
   using adjlist = std::vector<std::pair<int32_t, double>>;  // (nbr, weight), no self entries
   std::vector<adjlist> wadj(V);
   std::vector<int32_t> community(V);
@@ -569,6 +570,7 @@ double or_louvain(int32_t V, const int32_t* off, const int32_t* adj, const float
         sigtot[newcommunity] += kv;
       }
       newmodularity = modularity();
+      ++sweeps;
     } while ((newmodularity - oldmodularity) > threshold);
 
     // aggregation (:113-206)
@@ -613,6 +615,7 @@ double or_louvain(int32_t V, const int32_t* off, const int32_t* adj, const float
   if (community_out)
     for (int32_t v = 0; v < V; ++v) community_out[v] = orig_comm[v];
   if (levels_out) *levels_out = levels;
+  if (sweeps_out) *sweeps_out = sweeps;
   return newmodularity;
 }
 

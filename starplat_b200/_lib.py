@@ -22,6 +22,8 @@ SP_ERR = {
 }
 
 SP_GRAPH_DEVICE_PTRS = 0x1
+SP_TC_TUNED = 0
+SP_TC_PLAIN = 1
 SP_PR_TUNED = 0
 SP_PR_PLAIN = 1
 SP_SSSP_DELTA = 0
@@ -56,13 +58,13 @@ SIGNATURES = {
     "sp_graph_info": (ctypes.c_int, [vp, P(i32), P(i64), P(i32)]),
     "sp_tune_set": (ctypes.c_int, [vp, ctypes.c_char_p, i64]),
     "sp_tune_get": (ctypes.c_int, [vp, ctypes.c_char_p, P(i64)]),
-    "sp_tc": (ctypes.c_int, [vp, P(i64)]),
+    "sp_tc": (ctypes.c_int, [vp, P(i64), i32]),
     "sp_pagerank": (ctypes.c_int, [vp, f32, f32, i32, vp, P(i32), P(f64), i32]),
     "sp_sssp": (ctypes.c_int, [vp, vp, i32, vp, i64, i32, P(i32)]),
     "sp_bc": (ctypes.c_int, [vp, vp, i32, vp, i32]),
     "sp_bc_graphs": (ctypes.c_int, [vp, i32, vp, vp, vp, vp]),
     "sp_bfs_sigma": (ctypes.c_int, [vp, vp, i32, vp, vp]),
-    "sp_louvain": (ctypes.c_int, [vp, vp, f64, vp, P(f64), P(i32)]),
+    "sp_louvain": (ctypes.c_int, [vp, vp, f64, vp, P(f64), P(i32), P(i32)]),
 }
 
 

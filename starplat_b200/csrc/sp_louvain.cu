@@ -454,7 +454,8 @@ static int lv_subsweep(LvPlan* p, lv::MoveArgs a, const int counts[3], int cap, 
 using namespace sp;
 
 extern "C" int sp_louvain(sp_graph_h g, const float* weight, double threshold, int32_t* community, double* modularity,
-                          int32_t* levels_out) {
+                          int32_t* levels_out, int32_t* sweeps_out) {
+  int total_sweeps = 0;
   if (!g || !modularity) {
     set_error("sp_louvain: invalid argument");
     return SP_ERR_INVALID;
@@ -510,6 +511,7 @@ extern "C" int sp_louvain(sp_graph_h g, const float* weight, double threshold, i
   if (!(W > 0)) {
     *modularity = 0.0;
     if (levels_out) *levels_out = 0;
+    if (sweeps_out) *sweeps_out = 0;
     if (community) {
       lv::k_init_comm<<<gs, 256, 0, s>>>(n0, p->comm.p, p->newcomm.p);
       SP_CHECK_LAUNCH();
@@ -580,6 +582,7 @@ extern "C" int sp_louvain(sp_graph_h g, const float* weight, double threshold, i
         SP_TRY(lv_recount(p, n, s));
       }
       qold = qnew;
+      ++total_sweeps;
       SP_TRY(lv_modularity(p, L, W, s, &qnew));
       if (!(qnew - qold > threshold)) break;
     }
@@ -648,6 +651,7 @@ extern "C" int sp_louvain(sp_graph_h g, const float* weight, double threshold, i
   }
   *modularity = qcur;
   if (levels_out) *levels_out = levels;
+  if (sweeps_out) *sweeps_out = total_sweeps;
   if (community) SP_TRY(copy_out(community, p->orig.p, sizeof(int32_t) * n0, s));
   return SP_OK;
 }

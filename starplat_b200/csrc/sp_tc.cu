@@ -216,6 +216,35 @@ __global__ void __launch_bounds__(THREADS) k_tc_heavy(Lists L, const int* __rest
   if (threadIdx.x == 0 && cnt) atomicAdd(total, cnt);
 }
 
+// Plain form: the generated CUDA code's shape — one thread per vertex v, the
+// formula's double loop over N(v), u->w tested by binary search in N(u)
+// (libcuda.cuh:187-212 findNeighborSorted).
+__global__ void k_tc_plain(const int32_t* __restrict__ off, const int32_t* __restrict__ adj, int V,
+                           unsigned long long* __restrict__ total) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= V) return;
+  unsigned long long c = 0;
+  for (int e = off[v]; e < off[v + 1]; ++e) {
+    int u = adj[e];
+    if (u >= v) continue;
+    for (int e2 = off[v]; e2 < off[v + 1]; ++e2) {
+      int w = adj[e2];
+      if (w <= v) continue;
+      int lo = off[u], hi = off[u + 1] - 1;
+      while (lo <= hi) {
+        int mid = (lo + hi) >> 1;
+        int x = adj[mid];
+        if (x == w) {
+          ++c;
+          break;
+        }
+        if (x < w) lo = mid + 1; else hi = mid - 1;
+      }
+    }
+  }
+  if (c) atomicAdd(total, c);
+}
+
 // Orientation: keep v in N+(u) iff (deg u, u) < (deg v, v).
 __device__ __forceinline__ bool before(int du, int u, int dv, int v) { return du < dv || (du == dv && u < v); }
 
@@ -263,6 +292,7 @@ struct TcPlan {
   dbuf<unsigned int> ctr;    // [0] next anchor, [1] heavy count
   dbuf<unsigned long long> total;
   bool oriented = false;
+  bool built = false;
 };
 
 void free_tc_plan(TcPlan* p) {
@@ -276,7 +306,11 @@ void free_tc_plan(TcPlan* p) {
 }
 
 static int build_tc_plan(sp_graph* g) {
-  if (g->tc) return SP_OK;
+  if (g->tc && g->tc->built) return SP_OK;
+  if (g->tc) {
+    free_tc_plan(g->tc);
+    g->tc = nullptr;
+  }
   SP_TRY(ensure_symmetry(g));
   TcPlan* p = new TcPlan();
   cudaStream_t s = g->stream;
@@ -310,16 +344,34 @@ static int build_tc_plan(sp_graph* g) {
     }
     p->oriented = true;
   }
+  p->built = true;
   g->tc = p;
   return SP_OK;
 }
 
 }  // namespace sp
 
-extern "C" int sp_tc(sp_graph_h g, int64_t* triangle_count) {
+extern "C" int sp_tc(sp_graph_h g, int64_t* triangle_count, int32_t variant) {
   using namespace sp;
   if (!g || !triangle_count) {
     set_error("sp_tc: NULL argument");
+    return SP_ERR_INVALID;
+  }
+  if (variant == SP_TC_PLAIN) {
+    if (!g->tc) g->tc = new TcPlan();
+    TcPlan* p = g->tc;
+    SP_TRY(p->total.alloc(1));
+    SP_CHECK_CUDA(cudaMemsetAsync(p->total.p, 0, sizeof(unsigned long long), g->stream));
+    const int tb = 512;  // backend_cuda/dsl_cpp_generator.cpp:56-77
+    tc::k_tc_plain<<<(g->V + tb - 1) / tb, tb, 0, g->stream>>>(g->off.p, g->adj.p, g->V, p->total.p);
+    SP_CHECK_LAUNCH();
+    unsigned long long h = 0;
+    SP_TRY(copy_out(&h, p->total.p, sizeof(h), g->stream));
+    *triangle_count = (int64_t)h;
+    return SP_OK;
+  }
+  if (variant != SP_TC_TUNED) {
+    set_error("sp_tc: unknown variant %d", variant);
     return SP_ERR_INVALID;
   }
   SP_TRY(build_tc_plan(g));

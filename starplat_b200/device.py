@@ -111,9 +111,9 @@ class DeviceGraph:
         return V.value, E.value, bool(s.value)
 
     # ---------------------------------------------------------------- algorithms
-    def tc(self) -> int:
+    def tc(self, variant: int = _lib.SP_TC_TUNED) -> int:
         out = ctypes.c_int64()
-        check("sp_tc", lib().sp_tc(self.handle, ctypes.byref(out)))
+        check("sp_tc", lib().sp_tc(self.handle, ctypes.byref(out), variant))
         return int(out.value)
 
     def pagerank(self, beta: float = 1e-6, delta: float = 0.85, max_iter: int = 100, out=None,
@@ -174,6 +174,8 @@ class DeviceGraph:
             raise TypeError("Louvain weights must be float32")
         q = ctypes.c_double()
         lv = ctypes.c_int32()
+        sw = ctypes.c_int32()
         check("sp_louvain", lib().sp_louvain(self.handle, _ptr(weight), threshold, _ptr(community), ctypes.byref(q),
-                                             ctypes.byref(lv)))
+                                             ctypes.byref(lv), ctypes.byref(sw)))
+        self.last_louvain_sweeps = int(sw.value)
         return float(q.value), community, int(lv.value)

@@ -43,4 +43,4 @@ def test_errors_do_not_cross_abi():
     st = L.sp_graph_create(0, 0, None, None, None, None, None, 0, ctypes.byref(h))
     assert st == -1 and b"invalid" in L.sp_last_error()
     assert L.sp_graph_free(None) == 0
-    assert L.sp_tc(None, None) == -1
+    assert L.sp_tc(None, None, 0) == -1

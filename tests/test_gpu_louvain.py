@@ -1,6 +1,12 @@
-"""GPU parity: Louvain modularity within 1e-3 of the sequential restatement of the
-DSL (labels are order dependent and are not compared); the returned partition
-must have exactly the returned modularity."""
+"""GPU parity for Louvain.
+
+Louvain is a greedy heuristic whose result depends on the vertex visiting order:
+the DSL visits a hash set sequentially, a GPU moves vertices in parallel, and the
+two stop in different local optima. Labels are therefore not compared; the bar is
+on modularity, one-sided: the GPU partition must be no worse than the sequential
+restatement of the DSL by more than 1e-3 (on the planted-partition graphs it
+finds the planted blocks, which score higher than the sequential order). The
+returned partition must have exactly the returned modularity."""
 import numpy as np
 import pytest
 
@@ -16,7 +22,7 @@ pytestmark = pytest.mark.gpu
 def check(g, w=None, tol=1e-3):
     q, comm, levels = device_graph(g).louvain(w)
     qr, _, _ = O.louvain(g.indexofNodes, g.edgeList, w)
-    assert abs(q - qr) < tol, (g.name, q, qr)
+    assert q > qr - tol, (g.name, q, qr)
     # the partition really has that modularity
     assert abs(O.modularity(g.indexofNodes, g.edgeList, comm, w) - q) < 1e-9
     # dense community ids
@@ -27,7 +33,10 @@ def check(g, w=None, tol=1e-3):
 @pytest.mark.parametrize("seed", [1, 2])
 def test_louvain_sbm(seed):
     g = G.sbm(20000, 24, exponent=2.0, avg_degree=32, p_in=0.8, seed=seed)
-    check(g)
+    q, _ = check(g)
+    bs = g.meta["block_start"]
+    planted = (np.searchsorted(bs, np.arange(g.V), side="right") - 1).astype(np.int32)
+    assert q > O.modularity(g.indexofNodes, g.edgeList, planted) - 1e-3
 
 
 def test_louvain_er_and_rmat():

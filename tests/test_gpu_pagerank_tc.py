@@ -156,6 +156,11 @@ def test_tc_heavy_anchor():
         assert Compute_TC(g) == O.tc(g.indexofNodes, g.edgeList)
 
 
+def test_tc_plain_variant():
+    for g in (undirected_zoo()[0], directed_zoo()[3], G.rmat(12, 16, seed=5)):
+        assert device_graph(g).tc(variant=_lib.SP_TC_PLAIN) == O.tc(g.indexofNodes, g.edgeList)
+
+
 def test_tc_rmat16_config():
     g = G.rmat(16, 16, seed=1)
     assert Compute_TC(g) == O.tc(g.indexofNodes, g.edgeList)
