@@ -217,7 +217,6 @@ __device__ bool run_batch(const Work& W, const int32_t* srcs, int nsrc, S& sync,
     }
     if (gt == 0) W.lo[d + 2] = c;
     if (!sync.sync()) return false;
-    if (*(volatile int*)W.err) return false;
     ++d;
   }
   const int D = d;  // levels 0..D-1 are non-empty
@@ -258,7 +257,10 @@ __device__ bool run_batch(const Work& W, const int32_t* srcs, int nsrc, S& sync,
     W.bc[v] += s;
     W.seen[v] = 0ull;
   }
-  return sync.sync();
+  // a full level list (err 1) truncated this batch: every CTA reads the flag after
+  // the last barrier (nothing writes it after that), so all leave together
+  if (!sync.sync()) return false;
+  return *(volatile int*)W.err == 0;
 }
 
 struct GridArgs {

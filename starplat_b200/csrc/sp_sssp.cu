@@ -163,12 +163,15 @@ __global__ void __launch_bounds__(THREADS) k_delta(Args a) {
       const long long thr_old = thr;
       thr = (a.delta >= (long long)INT_MAX) ? (long long)INT_MAX + 1 : (fm / a.delta + 1) * a.delta;
       if (thr <= thr_old) thr = thr_old + a.delta;
+      // The split fills the queue of the NEXT round (its own counter slot): every
+      // phase decision reads qcount[round % 3], and no phase may write the slot its
+      // own decision read while slower CTAs may still be reading it.
       const int32_t* F = a.f[epoch & 1];
       int32_t* FN = a.f[(epoch + 1) & 1];
       int* fnext = &c->fcount[(epoch + 1) % 3];
       int* fminn = &c->fmin[(epoch + 1) % 3];
-      int32_t* Q = a.q[round & 1];
-      int* qcnt = &c->qcount[round % 3];
+      int32_t* Q = a.q[(round + 1) & 1];
+      int* qcnt = &c->qcount[(round + 1) % 3];
       for (int base = gw * 32; base < fn; base += nw * 32) {
         const int i = base + lane;
         bool toq = false, tof = false;
@@ -178,7 +181,7 @@ __global__ void __launch_bounds__(THREADS) k_delta(Args a) {
           const int du = __ldcg(a.dist + u);
           if ((long long)du >= thr_old) {  // below thr_old: already settled through the queue
             if ((long long)du < thr) {
-              toq = atomicExch(a.qstamp + u, round) != round;
+              toq = atomicExch(a.qstamp + u, round + 1) != round + 1;
             } else {
               tof = atomicExch(a.fstamp + u, epoch + 1) != epoch + 1;
               if (tof) atomicMin(fminn, du);
@@ -191,13 +194,15 @@ __global__ void __launch_bounds__(THREADS) k_delta(Args a) {
       if (blockIdx.x == 0 && threadIdx.x == 0) {
         c->fcount[(epoch + 2) % 3] = 0;
         c->fmin[(epoch + 2) % 3] = INT_MAX;
+        c->qcount[(round + 2) % 3] = 0;  // read two phases ago
       }
       if (!grid_barrier(&c->bar)) break;
       ++epoch;
+      ++round;
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    c->rounds = round;
+    c->rounds = round - epoch;  // relax rounds (each split also consumed a round number)
     c->epochs = epoch;
     if (c->bar.error) c->status = 1;
   }

@@ -107,3 +107,10 @@ def test_bc_many_graphs_one_launch():
     for k, g in enumerate(gs):
         ref = O.bc(g.indexofNodes, g.edgeList, src_all[k] - offs[k])
         assert_bc_close(out[offs[k]:offs[k + 1]], ref, f"graph{k}")
+
+
+def test_bc_at_scale():
+    g = G.rmat(17, 16, seed=1)
+    srcs = G.pick_sources(g, 96, seed=20)
+    out = device_graph(g).bc(srcs)
+    assert_bc_close(out, O.bc(g.indexofNodes, g.edgeList, srcs), "rmat17")

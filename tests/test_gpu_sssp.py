@@ -123,3 +123,17 @@ def test_sssp_bad_source():
     g = weighted(G.grid(5, 5), 1, 10)
     with pytest.raises(_lib.SPError):
         device_graph(g).sssp(25)
+
+
+@pytest.mark.parametrize("case", ["rmat17", "rmat20", "grid1024"])
+def test_sssp_at_scale(case):
+    # sizes where phases of different CTAs overlap in time (the small graphs above
+    # finish each phase before a second CTA starts)
+    if case.startswith("rmat"):
+        g = weighted(G.rmat(int(case[4:]), 16, seed=1, directed=True), 1, 100, seed=23)
+        src = int(G.pick_sources(g, 1, seed=23)[0])
+    else:
+        g = weighted(G.grid(1024, 1024), 1, 1000, seed=4096)
+        src = 123457
+    check(g, src)
+    check(g, src, variant=_lib.SP_SSSP_PLAIN)
