@@ -22,6 +22,9 @@
 //  * backward level d: the masks of level d+1 are scattered into a dense array; for
 //    each (v, mask) of level d the lanes pull sigma/delta of the successors in edge
 //    order — no atomics, deterministic;
+//  * level-list entries of vertices with more than 4096 edges (R-MAT hubs) are cut
+//    into 256-edge pieces that all warps share (one extra barrier per level);
+//    their backward partials meet in an FP64 scratch through atomics;
 //  * BC accumulates per vertex over the batch's sources in source order (FP64).
 // One cooperative launch runs every batch of a graph (bounded grid barriers); the
 // many-small-graphs form runs one CTA per graph in a persistent launch with a
@@ -37,6 +40,8 @@ namespace sp {
 namespace bc {
 constexpr int GRID_THREADS = 256;
 constexpr int CTA_THREADS = 512;
+constexpr int HUB_DEG = 4096;   // level-list entries of vertices above this degree are split
+constexpr int HUB_CHUNK = 256;  // edges per hub piece
 
 struct Work {
   const int32_t* __restrict__ off;  // CSR rows of this graph (global edge indices)
@@ -56,6 +61,12 @@ struct Work {
   int* cnt;                         // append counter
   double* bc;                       // [V] FP64 accumulator (local ids)
   int* err;                         // 1 list overflow, 2 too deep, 3 barrier timeout
+  // hub pieces (grid form only; hub_cap = 0 disables splitting)
+  int32_t* hub_ent;                 // [hub_cap] level-list entry index
+  int32_t* hub_base;                // [hub_cap] first piece index (increasing)
+  unsigned long long* hub_cnt;      // (entries << 32) | pieces
+  int hub_cap;
+  double* dacc;                     // [V][SW] FP64 partial dependencies of hub entries
 };
 
 struct GridSync {
@@ -80,8 +91,42 @@ __device__ __forceinline__ unsigned long long shfl64(unsigned long long x, int l
   return ((unsigned long long)hi << 32) | lo;
 }
 
+// Entry i of a level list: a hub (more than HUB_DEG edges) when splitting is on.
+// Returns true if it was queued as pieces instead of being processed here.
+__device__ __forceinline__ bool queue_hub(const Work& W, int i, int lane) {
+  if (W.hub_cap == 0) return false;
+  const int v = W.flv[i];
+  const int d = W.off[v + 1] - W.off[v];
+  if (d <= HUB_DEG) return false;
+  if (lane == 0) {
+    const int np = (d + HUB_CHUNK - 1) / HUB_CHUNK;
+    const unsigned long long old = atomicAdd(W.hub_cnt, (1ull << 32) | (unsigned long long)np);
+    const int k = (int)(old >> 32);
+    if (k < W.hub_cap) {
+      W.hub_ent[k] = i;
+      W.hub_base[k] = (int)(old & 0xffffffffull);
+    } else {
+      atomicExch(W.err, 1);
+    }
+  }
+  return true;
+}
+
+// Piece p of the queued hubs -> (entry, edge range).
+__device__ __forceinline__ void hub_piece(const Work& W, int nh, int p, int& i, int& eb, int& ee) {
+  int lo = 0, hi = nh - 1;
+  while (lo < hi) {
+    const int m = (lo + hi + 1) >> 1;
+    if (W.hub_base[m] <= p) lo = m; else hi = m - 1;
+  }
+  i = W.hub_ent[lo];
+  const int v = W.flv[i];
+  eb = W.off[v] + (p - W.hub_base[lo]) * HUB_CHUNK;
+  ee = min(eb + HUB_CHUNK, W.off[v + 1]);
+}
+
 template <int NW>
-__device__ void expand_entry(const Work& W, int i, int lane) {
+__device__ void expand_entry(const Work& W, int i, int lane, int eb, int ee) {
   constexpr int SW = 32 * NW;
   const int v = W.flv[i];
   const unsigned long long m = W.flm[i];
@@ -91,7 +136,6 @@ __device__ void expand_entry(const Work& W, int i, int lane) {
     const int b = lane + 32 * k;
     sv[k] = ((m >> b) & 1ull) ? W.sigma[(size_t)v * SW + b] : 0.0;
   }
-  const int eb = W.off[v], ee = W.off[v + 1];
   for (int c = eb; c < ee; c += 32) {
     const int j = c + lane;
     int w = 0;
@@ -131,8 +175,10 @@ __device__ void expand_entry(const Work& W, int i, int lane) {
   }
 }
 
+// piece = false: the whole entry, dependencies written to delta; piece = true: an
+// edge range of a hub entry, partial dependencies added to dacc (FP64 atomics).
 template <int NW>
-__device__ void backward_entry(const Work& W, int i, int lane) {
+__device__ void backward_entry(const Work& W, int i, int lane, int eb, int ee, bool piece) {
   constexpr int SW = 32 * NW;
   const int v = W.flv[i];
   const unsigned long long m = W.flm[i];
@@ -143,7 +189,6 @@ __device__ void backward_entry(const Work& W, int i, int lane) {
     sv[k] = ((m >> b) & 1ull) ? W.sigma[(size_t)v * SW + b] : 0.0;
     acc[k] = 0.0;
   }
-  const int eb = W.off[v], ee = W.off[v + 1];
   for (int c = eb; c < ee; c += 32) {
     const int j = c + lane;
     int w = 0;
@@ -171,7 +216,13 @@ __device__ void backward_entry(const Work& W, int i, int lane) {
 #pragma unroll
   for (int k = 0; k < NW; ++k) {
     const int b = lane + 32 * k;
-    if ((m >> b) & 1ull) W.delta[(size_t)v * SW + b] = (float)acc[k];
+    if ((m >> b) & 1ull) {
+      if (piece) {
+        if (acc[k] != 0.0) atomicAdd(&W.dacc[(size_t)v * SW + b], acc[k]);
+      } else {
+        W.delta[(size_t)v * SW + b] = (float)acc[k];
+      }
+    }
   }
 }
 
@@ -205,9 +256,23 @@ __device__ bool run_batch(const Work& W, const int32_t* srcs, int nsrc, S& sync,
       if (gt == 0) atomicExch(W.err, 2);
       return false;
     }
-    for (int i = b + gw; i < e; i += nw) expand_entry<NW>(W, i, lane);
+    for (int i = b + gw; i < e; i += nw)
+      if (!queue_hub(W, i, lane)) expand_entry<NW>(W, i, lane, W.off[W.flv[i]], W.off[W.flv[i] + 1]);
     if (!sync.sync()) return false;
+    if (W.hub_cap) {
+      const unsigned long long hc = *(volatile unsigned long long*)W.hub_cnt;
+      const int nh = min((int)(hc >> 32), W.hub_cap), np = (int)(hc & 0xffffffffull);
+      if (nh > 0) {
+        for (int p = gw; p < np; p += nw) {
+          int i, eb, ee;
+          hub_piece(W, nh, p, i, eb, ee);
+          expand_entry<NW>(W, i, lane, eb, ee);
+        }
+        if (!sync.sync()) return false;
+      }
+    }
     const int c = min(*(volatile int*)W.cnt, W.cap);
+    if (W.hub_cap && gt == 0) *W.hub_cnt = 0ull;  // read by every CTA before the barrier above
     for (int i = e + gt; i < c; i += nt) {
       const int w = W.flv[i];
       const unsigned long long mk = W.nxt[w];
@@ -240,8 +305,38 @@ __device__ bool run_batch(const Work& W, const int32_t* srcs, int nsrc, S& sync,
     for (int i = b1 + gt; i < e1; i += nt) W.dense[W.flv[i]] = W.flm[i];
     if (!sync.sync()) return false;
     const int b0 = W.lo[d], e0 = W.lo[d + 1];
-    for (int i = b0 + gw; i < e0; i += nw) backward_entry<NW>(W, i, lane);
+    for (int i = b0 + gw; i < e0; i += nw)
+      if (!queue_hub(W, i, lane)) backward_entry<NW>(W, i, lane, W.off[W.flv[i]], W.off[W.flv[i] + 1], false);
     if (!sync.sync()) return false;
+    if (W.hub_cap) {
+      const unsigned long long hc = *(volatile unsigned long long*)W.hub_cnt;
+      const int nh = min((int)(hc >> 32), W.hub_cap), np = (int)(hc & 0xffffffffull);
+      if (nh > 0) {
+        for (int p = gw; p < np; p += nw) {
+          int i, eb, ee;
+          hub_piece(W, nh, p, i, eb, ee);
+          backward_entry<NW>(W, i, lane, eb, ee, true);
+        }
+        if (!sync.sync()) return false;
+        // hub dependencies: FP64 partials -> delta, scratch back to zero
+        for (int k = gw; k < nh; k += nw) {
+          const int i = W.hub_ent[k];
+          const int v = W.flv[i];
+          const unsigned long long m = W.flm[i];
+#pragma unroll
+          for (int q = 0; q < NW; ++q) {
+            const int bb = lane + 32 * q;
+            if ((m >> bb) & 1ull) {
+              const size_t x = (size_t)v * SW + bb;
+              W.delta[x] = (float)W.dacc[x];
+              W.dacc[x] = 0.0;
+            }
+          }
+        }
+        if (!sync.sync()) return false;
+      }
+      if (gt == 0) *W.hub_cnt = 0ull;  // every CTA read it before the barrier above
+    }
     for (int i = b1 + gt; i < e1; i += nt) W.dense[W.flv[i]] = 0ull;
     if (!sync.sync()) return false;
   }
@@ -329,6 +424,10 @@ __global__ void __launch_bounds__(CTA_THREADS) k_bc_graphs(GraphsArgs a) {
   W.err = a.err;
   W.off = a.off;
   W.adj = a.adj;
+  W.hub_cap = 0;
+  W.hub_ent = W.hub_base = nullptr;
+  W.hub_cnt = nullptr;
+  W.dacc = nullptr;
   while (true) {
     if (threadIdx.x == 0) s_g = atomicAdd(a.next, 1);
     __syncthreads();
@@ -399,7 +498,9 @@ __global__ void k_plain_bwd(int V, const int32_t* __restrict__ off, const int32_
 }  // namespace bc
 
 struct BcPlan {
-  dbuf<double> sigma, bc;
+  dbuf<double> sigma, bc, dacc;
+  dbuf<int32_t> hub_ent, hub_base;
+  dbuf<unsigned long long> hub_cnt;
   dbuf<float> delta, fout;
   dbuf<unsigned long long> masks, flm;
   dbuf<int32_t> flv, lo, cnt, srcs, level, aux;
@@ -429,7 +530,15 @@ static int bc_grid(sp_graph* g, const int32_t* d_srcs, int nsrc, int batch_hint,
   SP_TRY(p->bc.alloc(V));
   SP_TRY(p->bar.alloc(1));
   SP_TRY(p->err.alloc(1));
+  const int hub_cap = V;
+  SP_TRY(p->hub_ent.alloc(hub_cap));
+  SP_TRY(p->hub_base.alloc(hub_cap));
+  SP_TRY(p->hub_cnt.alloc(1));
+  SP_TRY(p->dacc.alloc((size_t)V * SW));
+  SP_CHECK_CUDA(cudaMemsetAsync(p->hub_cnt.p, 0, sizeof(unsigned long long), s));
   const int zg = num_sms() * 8;
+  bc::k_zero<<<zg, 256, 0, s>>>(p->dacc.p, (size_t)V * SW);
+  g_launches++;
   bc::k_zero<<<zg, 256, 0, s>>>(p->sigma.p, (size_t)V * SW);
   bc::k_zero<<<zg, 256, 0, s>>>(p->delta.p, (size_t)V * SW / 2);
   bc::k_zero<<<zg, 256, 0, s>>>(p->masks.p, (size_t)V * 3);
@@ -456,6 +565,11 @@ static int bc_grid(sp_graph* g, const int32_t* d_srcs, int nsrc, int batch_hint,
   W.cnt = p->cnt.p;
   W.bc = p->bc.p;
   W.err = p->err.p;
+  W.hub_ent = p->hub_ent.p;
+  W.hub_base = p->hub_base.p;
+  W.hub_cnt = p->hub_cnt.p;
+  W.hub_cap = hub_cap;
+  W.dacc = p->dacc.p;
   a.srcs = d_srcs;
   a.nsrc = nsrc;
   a.batch = batch;

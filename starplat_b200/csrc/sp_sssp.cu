@@ -11,9 +11,11 @@
 //   * near queue Q (ping-pong) holds vertices whose distance dropped below the
 //     current bucket threshold; far pile F holds the rest;
 //   * relax rounds: every frontier vertex pushes along its out-edges with
-//     atomicMin; a lane sums its own edges for low degree, the whole warp
-//     cooperates on high-degree vertices; queue appends are warp-aggregated and
-//     de-duplicated with per-round / per-epoch stamps;
+//     atomicMin; a lane walks its own edges for low degree, the whole warp
+//     cooperates on medium degree, and vertices above 2048 out-edges (R-MAT hubs)
+//     are queued in a hub list whose 256-edge chunks all warps share in the next
+//     round; queue appends are warp-aggregated and de-duplicated with per-round /
+//     per-epoch stamps;
 //   * when Q empties, the threshold jumps to the bucket of the smallest far
 //     distance and F is split into Q and the next far pile.
 //   Negative weights switch to delta = infinity (queue-based Bellman-Ford), bounded
@@ -30,11 +32,14 @@ namespace sp {
 
 namespace ss {
 constexpr int THREADS = 256;
-constexpr int LANE_DEG = 16;  // frontier vertices up to this out-degree are walked by one lane
+constexpr int LANE_DEG = 16;   // frontier vertices up to this out-degree are walked by one lane
+constexpr int HUB_DEG = 2048;  // above this a vertex is relaxed in HUB_CHUNK pieces by many warps
+constexpr int HUB_CHUNK = 256;
 
 struct Ctl {
   GridBar bar;
   int qcount[3];   // per round (mod 3): entries appended to the queue read next round
+  unsigned long long hcount[3];  // per round (mod 3): (hub entries << 32) | hub chunks
   int fcount[3];   // per epoch (mod 3)
   int fmin[3];     // per epoch: smallest distance pushed to the far pile
   int rounds;      // relax rounds executed
@@ -50,6 +55,8 @@ struct Args {
   int32_t* dist;
   int32_t* q[2];
   int32_t* f[2];
+  int32_t* hv[2];      // hub vertices per round (ping-pong)
+  int32_t* hbase[2];   // first chunk index of each hub entry (increasing)
   int32_t* qstamp;
   int32_t* fstamp;
   Ctl* ctl;
@@ -68,6 +75,28 @@ __device__ __forceinline__ void warp_push(bool want, int val, int32_t* buf, int*
   if (lane == leader) base = atomicAdd(counter, __popc(m));
   base = __shfl_sync(0xffffffffu, base, leader);
   if (want) buf[base + __popc(m & ((1u << lane) - 1u))] = val;
+}
+
+// Queue u for the next round: hubs go to the hub list (with their chunk count),
+// everything else to the near queue (warp-aggregated).
+__device__ __forceinline__ void queue_push(const Args& a, bool want, int u, int32_t* QN, int* qnext, int32_t* HV,
+                                           int32_t* HB, unsigned long long* hcnt) {
+  bool hub = false;
+  int nch = 0;
+  if (want) {
+    const int d = a.off[u + 1] - a.off[u];
+    if (d > HUB_DEG) {
+      hub = true;
+      nch = (d + HUB_CHUNK - 1) / HUB_CHUNK;
+    }
+  }
+  if (hub) {
+    const unsigned long long old = atomicAdd(hcnt, (1ull << 32) | (unsigned long long)nch);
+    const int idx = (int)(old >> 32);
+    HV[idx] = u;
+    HB[idx] = (int)(old & 0xffffffffull);
+  }
+  warp_push(want && !hub, u, QN, qnext);
 }
 
 // Relax one edge (dv + wt to u); returns queue (1), far (2) or nothing (0).
@@ -95,17 +124,23 @@ __global__ void __launch_bounds__(THREADS) k_delta(Args a) {
   int round = 0, epoch = 0;
   long long thr = a.delta;  // bucket 0 = [0, delta)
   while (true) {
-    const int qn = *(volatile int*)&c->qcount[round % 3];
+    const int qv = *(volatile int*)&c->qcount[round % 3];
+    const unsigned long long hc = *(volatile unsigned long long*)&c->hcount[round % 3];
+    const int hn = (int)(hc >> 32), hchunks = (int)(hc & 0xffffffffull);
+    const int qn = qv;
     const int fn = *(volatile int*)&c->fcount[epoch % 3];
-    if (qn == 0 && fn == 0) break;
+    if (qv == 0 && hn == 0 && fn == 0) break;
     if ((long long)round >= a.max_rounds) {
       if (blockIdx.x == 0 && threadIdx.x == 0) c->status = 1;
       break;
     }
-    if (qn > 0) {
+    if (qv > 0 || hn > 0) {
       const int32_t* Q = a.q[round & 1];
       int32_t* QN = a.q[(round + 1) & 1];
       int* qnext = &c->qcount[(round + 1) % 3];
+      int32_t* HV = a.hv[(round + 1) & 1];
+      int32_t* HB = a.hbase[(round + 1) & 1];
+      unsigned long long* hnext = &c->hcount[(round + 1) % 3];
       int32_t* F = a.f[epoch & 1];
       int* fcnt = &c->fcount[epoch % 3];
       int* fmin = &c->fmin[epoch % 3];
@@ -131,7 +166,7 @@ __global__ void __launch_bounds__(THREADS) k_delta(Args a) {
             u = a.adj[b + j];
             res = relax(a, u, dv + a.w[b + j], thr, round, epoch, fmin);
           }
-          warp_push(res == 1, u, QN, qnext);
+          queue_push(a, res == 1, u, QN, qnext, HV, HB, hnext);
           warp_push(res == 2, u, F, fcnt);
         }
         // high-degree vertices: whole warp, one vertex at a time
@@ -149,12 +184,41 @@ __global__ void __launch_bounds__(THREADS) k_delta(Args a) {
               u = a.adj[k];
               res = relax(a, u, vd + a.w[k], thr, round, epoch, fmin);
             }
-            warp_push(res == 1, u, QN, qnext);
+            queue_push(a, res == 1, u, QN, qnext, HV, HB, hnext);
             warp_push(res == 2, u, F, fcnt);
           }
         }
       }
-      if (blockIdx.x == 0 && threadIdx.x == 0) c->qcount[(round + 2) % 3] = 0;  // read two rounds ago
+      // hub pieces of this round: HUB_CHUNK edges per warp, all warps
+      {
+        const int32_t* HVc = a.hv[round & 1];
+        const int32_t* HBc = a.hbase[round & 1];
+        for (int ch = gw; ch < hchunks; ch += nw) {
+          int lo = 0, hi = hn - 1;  // last entry whose first chunk <= ch
+          while (lo < hi) {
+            const int m = (lo + hi + 1) >> 1;
+            if (HBc[m] <= ch) lo = m; else hi = m - 1;
+          }
+          const int v = HVc[lo];
+          const long long vd = __ldcg(a.dist + v);
+          const int vb = a.off[v] + (ch - HBc[lo]) * HUB_CHUNK;
+          const int ve = min(vb + HUB_CHUNK, a.off[v + 1]);
+          for (int k0 = vb; k0 < ve; k0 += 32) {
+            const int k = k0 + lane;
+            int res = 0, u = 0;
+            if (k < ve) {
+              u = a.adj[k];
+              res = relax(a, u, vd + a.w[k], thr, round, epoch, fmin);
+            }
+            queue_push(a, res == 1, u, QN, qnext, HV, HB, hnext);
+            warp_push(res == 2, u, F, fcnt);
+          }
+        }
+      }
+      if (blockIdx.x == 0 && threadIdx.x == 0) {
+        c->qcount[(round + 2) % 3] = 0;  // read two rounds ago
+        c->hcount[(round + 2) % 3] = 0ull;
+      }
       if (!grid_barrier(&c->bar)) break;
       ++round;
     } else {
@@ -172,6 +236,9 @@ __global__ void __launch_bounds__(THREADS) k_delta(Args a) {
       int* fminn = &c->fmin[(epoch + 1) % 3];
       int32_t* Q = a.q[(round + 1) & 1];
       int* qcnt = &c->qcount[(round + 1) % 3];
+      int32_t* HV = a.hv[(round + 1) & 1];
+      int32_t* HB = a.hbase[(round + 1) & 1];
+      unsigned long long* hnext = &c->hcount[(round + 1) % 3];
       for (int base = gw * 32; base < fn; base += nw * 32) {
         const int i = base + lane;
         bool toq = false, tof = false;
@@ -188,13 +255,14 @@ __global__ void __launch_bounds__(THREADS) k_delta(Args a) {
             }
           }
         }
-        warp_push(toq, u, Q, qcnt);
+        queue_push(a, toq, u, Q, qcnt, HV, HB, hnext);
         warp_push(tof, u, FN, fnext);
       }
       if (blockIdx.x == 0 && threadIdx.x == 0) {
         c->fcount[(epoch + 2) % 3] = 0;
         c->fmin[(epoch + 2) % 3] = INT_MAX;
         c->qcount[(round + 2) % 3] = 0;  // read two phases ago
+        c->hcount[(round + 2) % 3] = 0ull;
       }
       if (!grid_barrier(&c->bar)) break;
       ++epoch;
@@ -208,19 +276,30 @@ __global__ void __launch_bounds__(THREADS) k_delta(Args a) {
   }
 }
 
-__global__ void k_init(int V, int src, int32_t* dist, int32_t* qstamp, int32_t* fstamp, int32_t* q0, Ctl* c) {
+__global__ void k_init(int V, int src, int32_t* dist, int32_t* qstamp, int32_t* fstamp, int32_t* q0, int32_t* hv0,
+                       int32_t* hb0, const int32_t* __restrict__ off, Ctl* c) {
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
     dist[v] = v == src ? 0 : INT_MAX;
     qstamp[v] = -1;
     fstamp[v] = -1;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    q0[0] = src;
     qstamp[src] = 0;
     c->bar.arrived = 0;
     c->bar.error = 0;
-    c->qcount[0] = 1;
-    c->qcount[1] = c->qcount[2] = 0;
+    for (int k = 0; k < 3; ++k) {
+      c->qcount[k] = 0;
+      c->hcount[k] = 0ull;
+    }
+    const int d = off[src + 1] - off[src];
+    if (d > HUB_DEG) {
+      hv0[0] = src;
+      hb0[0] = 0;
+      c->hcount[0] = (1ull << 32) | (unsigned long long)((d + HUB_CHUNK - 1) / HUB_CHUNK);
+    } else {
+      q0[0] = src;
+      c->qcount[0] = 1;
+    }
     for (int k = 0; k < 3; ++k) {
       c->fcount[k] = 0;
       c->fmin[k] = INT_MAX;
@@ -276,7 +355,7 @@ __global__ void k_minmax_w(const int32_t* __restrict__ w, int64_t E, int* mn, in
 }  // namespace ss
 
 struct SsspPlan {
-  dbuf<int32_t> dist, q0, q1, f0, f1, qstamp, fstamp, wbuf;
+  dbuf<int32_t> dist, q0, q1, f0, f1, qstamp, fstamp, wbuf, h0, h1, hb0, hb1;
   dbuf<char> m0, m1;
   dbuf<ss::Ctl> ctl;
   dbuf<int> tmp;
@@ -328,6 +407,10 @@ static int sssp_delta(sp_graph* g, const int32_t* w, int32_t src, int32_t* dist_
   SP_TRY(p->f1.alloc(V));
   SP_TRY(p->qstamp.alloc(V));
   SP_TRY(p->fstamp.alloc(V));
+  SP_TRY(p->h0.alloc(V));
+  SP_TRY(p->h1.alloc(V));
+  SP_TRY(p->hb0.alloc(V));
+  SP_TRY(p->hb1.alloc(V));
   SP_TRY(p->ctl.alloc(1));
   const bool negative = p->w_min < 0;
   if (negative || delta <= 0) delta = negative ? (int64_t)INT_MAX : std::max<int64_t>(1, delta);
@@ -340,6 +423,10 @@ static int sssp_delta(sp_graph* g, const int32_t* w, int32_t src, int32_t* dist_
   a.q[1] = p->q1.p;
   a.f[0] = p->f0.p;
   a.f[1] = p->f1.p;
+  a.hv[0] = p->h0.p;
+  a.hv[1] = p->h1.p;
+  a.hbase[0] = p->hb0.p;
+  a.hbase[1] = p->hb1.p;
   a.qstamp = p->qstamp.p;
   a.fstamp = p->fstamp.p;
   a.ctl = p->ctl.p;
@@ -348,7 +435,8 @@ static int sssp_delta(sp_graph* g, const int32_t* w, int32_t src, int32_t* dist_
   // Bellman-Ford needs at most V-1 rounds of improvement per vertex chain; far more
   // rounds than V * 4 + 64 can only come from a negative cycle.
   a.max_rounds = (long long)V * 4 + 64;
-  ss::k_init<<<num_sms() * 4, 256, 0, s>>>(V, src, p->dist.p, p->qstamp.p, p->fstamp.p, p->q0.p, p->ctl.p);
+  ss::k_init<<<num_sms() * 4, 256, 0, s>>>(V, src, p->dist.p, p->qstamp.p, p->fstamp.p, p->q0.p, p->h0.p, p->hb0.p,
+                                            g->off.p, p->ctl.p);
   SP_CHECK_LAUNCH();
   int per_sm = 0;
   SP_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ss::k_delta, ss::THREADS, 0));

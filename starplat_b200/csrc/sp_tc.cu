@@ -31,6 +31,7 @@ constexpr int WARPS = THREADS / 32;
 constexpr int HCAP = 1024;          // hash slots per warp (load factor <= 1/2)
 constexpr int SMAX = HCAP / 2;      // largest S(a) handled by the warp path
 constexpr int EMPTY = -1;
+constexpr int ANCHOR_BATCH = 16;
 
 __device__ __forceinline__ unsigned hslot(int k) { return ((unsigned)k * 2654435761u) >> 22; }  // 10 bits
 
@@ -97,11 +98,18 @@ __global__ void __launch_bounds__(THREADS) k_tc_warp(Lists L, unsigned int* __re
   for (int i = lane; i < HCAP; i += 32) tab[i] = EMPTY;
   __syncwarp();
   unsigned long long cnt = 0;
+  // anchors are taken ANCHOR_BATCH at a time (one atomic per batch, not per anchor)
+  unsigned int a_next = 0, a_end = 0;
   while (true) {
-    unsigned int a = 0;
-    if (lane == 0) a = atomicAdd(next_anchor, 1u);
-    a = __shfl_sync(0xffffffffu, a, 0);
-    if (a >= (unsigned)L.V) break;
+    if (a_next == a_end) {
+      unsigned int a0 = 0;
+      if (lane == 0) a0 = atomicAdd(next_anchor, (unsigned)ANCHOR_BATCH);
+      a0 = __shfl_sync(0xffffffffu, a0, 0);
+      if (a0 >= (unsigned)L.V) break;
+      a_next = a0;
+      a_end = min(a0 + (unsigned)ANCHOR_BATCH, (unsigned)L.V);
+    }
+    const unsigned int a = a_next++;
     int sb, se, pb, pe;
     anchor_ranges(L, (int)a, sb, se, pb, pe);
     const int ns = se - sb, np = pe - pb;
