@@ -67,6 +67,8 @@ int sp_graph_info(sp_graph_h g, int32_t* V, int64_t* E, int32_t* symmetric);
  *             CTA stages in shared memory per iteration (0..57344, default 0).
  *   "sssp.delta"  SSSP bucket width used when sp_sssp gets delta <= 0 (0 = the largest
  *             edge weight).
+ *   "sssp.ctas_per_sm"  SSSP: persistent CTAs per SM of the delta-stepping kernel (1..8,
+ *             default 4; fewer CTAs make each grid barrier cheaper on high-diameter graphs).
  *   "bc.batch"  BC: sources traversed together in one multi-source pass (1..64, default 64). */
 int sp_tune_set(sp_graph_h g, const char* key, int64_t value);
 int sp_tune_get(sp_graph_h g, const char* key, int64_t* value);

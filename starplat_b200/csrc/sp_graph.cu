@@ -310,6 +310,14 @@ int sp_tune_set(sp_graph_h g, const char* key, int64_t value) {
     g->sssp_delta = value;
     return SP_OK;
   }
+  if (!strcmp(key, "sssp.ctas_per_sm")) {
+    if (value < 0 || value > 8) {
+      set_error("sp_tune_set: sssp.ctas_per_sm must be in [0, 8]");
+      return SP_ERR_INVALID;
+    }
+    g->sssp_ctas_per_sm = (int32_t)value;
+    return SP_OK;
+  }
   if (!strcmp(key, "bc.batch")) {
     if (value < 0 || value > 64) {
       set_error("sp_tune_set: bc.batch must be in [0, 64]");
@@ -333,6 +341,10 @@ int sp_tune_get(sp_graph_h g, const char* key, int64_t* value) {
   }
   if (!strcmp(key, "sssp.delta")) {
     *value = g->sssp_delta;
+    return SP_OK;
+  }
+  if (!strcmp(key, "sssp.ctas_per_sm")) {
+    *value = g->sssp_ctas_per_sm > 0 ? g->sssp_ctas_per_sm : 4;
     return SP_OK;
   }
   if (!strcmp(key, "bc.batch")) {

@@ -440,7 +440,8 @@ static int sssp_delta(sp_graph* g, const int32_t* w, int32_t src, int32_t* dist_
   SP_CHECK_LAUNCH();
   int per_sm = 0;
   SP_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ss::k_delta, ss::THREADS, 0));
-  const int grid = num_sms() * std::max(1, std::min(per_sm, 4));
+  const int want = g->sssp_ctas_per_sm > 0 ? g->sssp_ctas_per_sm : 4;
+  const int grid = num_sms() * std::max(1, std::min(per_sm, want));
   void* params[] = {&a};
   SP_CHECK_CUDA(cudaLaunchCooperativeKernel((void*)ss::k_delta, grid, ss::THREADS, params, 0, s));
   g_launches++;

@@ -31,7 +31,6 @@ constexpr int WARPS = THREADS / 32;
 constexpr int HCAP = 1024;          // hash slots per warp (load factor <= 1/2)
 constexpr int SMAX = HCAP / 2;      // largest S(a) handled by the warp path
 constexpr int EMPTY = -1;
-constexpr int ANCHOR_BATCH = 16;
 
 __device__ __forceinline__ unsigned hslot(int k) { return ((unsigned)k * 2654435761u) >> 22; }  // 10 bits
 
@@ -86,7 +85,7 @@ __device__ __forceinline__ void probe_range(const Lists& L, int a, int p, int& l
   le = e;
 }
 
-__global__ void __launch_bounds__(THREADS) k_tc_warp(Lists L, unsigned int* __restrict__ next_anchor,
+__global__ void __launch_bounds__(THREADS) k_tc_warp(Lists L, const int32_t* __restrict__ order,
                                                      int* __restrict__ heavy, unsigned int* __restrict__ n_heavy,
                                                      unsigned long long* __restrict__ total) {
   __shared__ int s_tab[WARPS][HCAP];
@@ -98,18 +97,10 @@ __global__ void __launch_bounds__(THREADS) k_tc_warp(Lists L, unsigned int* __re
   for (int i = lane; i < HCAP; i += 32) tab[i] = EMPTY;
   __syncwarp();
   unsigned long long cnt = 0;
-  // anchors are taken ANCHOR_BATCH at a time (one atomic per batch, not per anchor)
-  unsigned int a_next = 0, a_end = 0;
-  while (true) {
-    if (a_next == a_end) {
-      unsigned int a0 = 0;
-      if (lane == 0) a0 = atomicAdd(next_anchor, (unsigned)ANCHOR_BATCH);
-      a0 = __shfl_sync(0xffffffffu, a0, 0);
-      if (a0 >= (unsigned)L.V) break;
-      a_next = a0;
-      a_end = min(a0 + (unsigned)ANCHOR_BATCH, (unsigned)L.V);
-    }
-    const unsigned int a = a_next++;
+  // anchors in decreasing estimated work, dealt round-robin to the warps (no atomics)
+  const int gwarp = (blockIdx.x * THREADS + threadIdx.x) >> 5, nwarps = (gridDim.x * THREADS) >> 5;
+  for (int ai = gwarp; ai < L.V; ai += nwarps) {
+    const int a = order[ai];
     int sb, se, pb, pe;
     anchor_ranges(L, (int)a, sb, se, pb, pe);
     const int ns = se - sb, np = pe - pb;
@@ -253,6 +244,26 @@ __global__ void k_tc_plain(const int32_t* __restrict__ off, const int32_t* __res
   if (c) atomicAdd(total, c);
 }
 
+// Estimated work of anchor a: the probe-list lengths it streams (sum over P(a)),
+// as a sort key (negated, so an ascending sort puts the heaviest first).
+__global__ void k_tc_work(Lists L, int32_t* __restrict__ key, int32_t* __restrict__ id) {
+  const int lane = threadIdx.x & 31;
+  for (int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; a < L.V; a += (gridDim.x * blockDim.x) >> 5) {
+    int sb, se, pb, pe;
+    anchor_ranges(L, a, sb, se, pb, pe);
+    long long w = 0;
+    for (int i = pb + lane; i < pe; i += 32) {
+      const int p = L.adj[i];
+      w += L.off[p + 1] - L.off[p];
+    }
+    w = warp_sum(w);
+    if (lane == 0) {
+      key[a] = (int32_t)(-min(w * (long long)(se - sb > 0), (long long)INT32_MAX));
+      id[a] = a;
+    }
+  }
+}
+
 // Orientation: keep v in N+(u) iff (deg u, u) < (deg v, v).
 __device__ __forceinline__ bool before(int du, int u, int dv, int v) { return du < dv || (du == dv && u < v); }
 
@@ -296,6 +307,7 @@ __global__ void k_orient_fill(const int32_t* __restrict__ off, const int32_t* __
 
 struct TcPlan {
   dbuf<int32_t> ooff, oadj;  // oriented CSR (undirected graphs)
+  dbuf<int32_t> order;       // anchors, heaviest first
   dbuf<int> heavy;
   dbuf<unsigned int> ctr;    // [0] next anchor, [1] heavy count
   dbuf<unsigned long long> total;
@@ -307,6 +319,7 @@ void free_tc_plan(TcPlan* p) {
   if (!p) return;
   p->ooff.release();
   p->oadj.release();
+  p->order.release();
   p->heavy.release();
   p->ctr.release();
   p->total.release();
@@ -352,6 +365,28 @@ static int build_tc_plan(sp_graph* g) {
     }
     p->oriented = true;
   }
+  {
+    tc::Lists L;
+    L.V = g->V;
+    L.directed = p->oriented ? 0 : 1;
+    L.off = p->oriented ? p->ooff.p : g->off.p;
+    L.adj = p->oriented ? p->oadj.p : g->adj.p;
+    dbuf<int32_t> key, id, skey;
+    if ((st = key.alloc(g->V)) || (st = id.alloc(g->V)) || (st = skey.alloc(g->V)) || (st = p->order.alloc(g->V)))
+      return fail(st);
+    tc::k_tc_work<<<num_sms() * 8, 256, 0, s>>>(L, key.p, id.p);
+    g_launches++;
+    size_t tb = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tb, key.p, skey.p, id.p, p->order.p, g->V, 0, 32, s);
+    dbuf<unsigned char> tmp;
+    if ((st = tmp.alloc(tb))) return fail(st);
+    cub::DeviceRadixSort::SortPairs(tmp.p, tb, key.p, skey.p, id.p, p->order.p, g->V, 0, 32, s);
+    g_launches++;
+    if (cudaStreamSynchronize(s) != cudaSuccess) {
+      set_error("tc anchor order: %s", cudaGetErrorString(cudaGetLastError()));
+      return fail(SP_ERR_CUDA);
+    }
+  }
   p->built = true;
   g->tc = p;
   return SP_OK;
@@ -392,7 +427,7 @@ extern "C" int sp_tc(sp_graph_h g, int64_t* triangle_count, int32_t variant) {
   L.adj = p->oriented ? p->oadj.p : g->adj.p;
   SP_CHECK_CUDA(cudaMemsetAsync(p->ctr.p, 0, sizeof(unsigned int) * 2, s));
   SP_CHECK_CUDA(cudaMemsetAsync(p->total.p, 0, sizeof(unsigned long long), s));
-  tc::k_tc_warp<<<num_sms() * 4, tc::THREADS, 0, s>>>(L, p->ctr.p, p->heavy.p, p->ctr.p + 1, p->total.p);
+  tc::k_tc_warp<<<num_sms() * 4, tc::THREADS, 0, s>>>(L, p->order.p, p->heavy.p, p->ctr.p + 1, p->total.p);
   SP_CHECK_LAUNCH();
   tc::k_tc_heavy<<<num_sms() * 2, tc::THREADS, 0, s>>>(L, p->heavy.p, p->ctr.p + 1, p->total.p);
   SP_CHECK_LAUNCH();
