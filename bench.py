@@ -53,6 +53,7 @@ PR_SCALE, PR_EF, PR_SEED = 22, 16, 1
 BETA, DELTA, MAX_ITER = 1e-6, 0.85, 100
 METRIC = "GTEPS per algorithm on 1 B200 (pagerank headline)"
 INT_MAX = 2**31 - 1
+TUNE = []  # (key, value) schedule knobs from --tune, applied to every device graph
 
 
 def peaks():
@@ -165,6 +166,15 @@ def timed(fn, steps, warmup, stream):
     return a.elapsed_time(b) / steps, res
 
 
+def tuned(dg):
+    for k, v in TUNE:
+        try:
+            dg.tune_set(k, v)
+        except Exception:
+            pass
+    return dg
+
+
 def roof(alg_bytes, ms, hbm):
     gbs = alg_bytes / (ms / 1e3) / 1e9
     return {"achieved_gbs": round(gbs, 1), "frac": round(gbs / hbm, 4), "alg_bytes": int(alg_bytes)}
@@ -200,6 +210,7 @@ def bench_tc(steps, warmup, stream, hbm, cpu):
     out = {"workload": "tc rmat16 ef16 undirected seed1", "V": g.V, "m": m, "E_plus": eplus}
     with DeviceGraph.from_csr(g, with_weights=False) as dg:
         dg.set_stream(stream)
+        tuned(dg)
         ms, res = timed(lambda: dg.tc(), steps, warmup, stream)
         msp, resp = timed(lambda: dg.tc(_lib.SP_TC_PLAIN), max(1, steps // 2), 1, stream)
     out.update({"triangles": res[0], "value": m / (ms / 1e3) / 1e9, "unit": "GTEPS", "ms": ms,
@@ -238,6 +249,7 @@ def bench_sssp(name, g, src, steps, warmup, stream, hbm, cpu, cpu_mode):
     out = {"workload": name, "V": g.V, "E": g.E, "source": int(src)}
     with DeviceGraph.from_csr(g) as dg:
         dg.set_stream(stream)
+        tuned(dg)
         dist = torch.empty(g.V, dtype=torch.int32, device="cuda")
         ms, res = timed(lambda: dg.sssp(src, out=dist), steps, warmup, stream)
         d = dist.cpu().numpy()
@@ -285,6 +297,7 @@ def bench_bc(steps, warmup, stream, hbm, cpu):
            "sum_E_r": sum_er}
     with DeviceGraph.from_csr(g, with_weights=False) as dg:
         dg.set_stream(stream)
+        tuned(dg)
         ms, _ = timed(lambda: dg.bc(srcs), steps, warmup, stream)
         few = srcs[:8]
         msp, _ = timed(lambda: dg.bc(few, variant=_lib.SP_BC_PLAIN), 1, 0, stream)
@@ -449,7 +462,8 @@ def main():
     dg.set_stream(stream)
     for kv in args.tune:
         k, v = kv.split("=")
-        dg.tune_set(k, int(v))
+        TUNE.append((k, int(v)))
+    tuned(dg)
     out = torch.empty(V, dtype=torch.float32, device="cuda")
 
     for _ in range(args.warmup):

@@ -17,8 +17,10 @@
 //    Each triangle is counted once, which equals the formula on a symmetric graph.
 //  * any other graph: the formula literally; a = v, S = N(v) ∩ (v, inf),
 //    P = N(v) ∩ [0, v), L(u) = N(u) ∩ (v, inf).
-// Anchors whose S does not fit the warp table are counted afterwards by whole CTAs
-// with binary search in the sorted global list.
+// Graphs up to 65536 vertices keep S(a) as a per-warp bitmap; larger graphs use a
+// per-warp hash table, and anchors whose S does not fit it are counted afterwards
+// by whole CTAs with binary search in the sorted global list. Anchors are visited
+// heaviest first (estimated probe work) and dealt round-robin to the warps.
 #include <cub/cub.cuh>
 
 #include "sp_internal.cuh"
@@ -160,6 +162,84 @@ __global__ void __launch_bounds__(THREADS) k_tc_warp(Lists L, const int32_t* __r
     }
     // clear the slots S(a) used
     for (int i = lane; i < ns; i += 32) tab[s_slot[w][i]] = EMPTY;
+    __syncwarp();
+  }
+  cnt = warp_sum(cnt);
+  if (lane == 0 && cnt) atomicAdd(total, cnt);
+}
+
+// Small graphs (V <= 65536): the same anchor loop with S(a) as a V-bit bitmap per
+// warp (8 KB) — a lookup is one shared-memory load and a bit test, any |S(a)|
+// fits, and each lane keeps BM_UNROLL probe loads in flight.
+constexpr int BM_WARPS = 4;
+constexpr int BM_THREADS = 32 * BM_WARPS;
+constexpr int BM_WORDS = 65536 / 32;
+constexpr int BM_UNROLL = 4;
+
+__device__ __forceinline__ int owner_of(const int* excl, int k) {
+  int lo = 0, hi = 31;
+  while (lo < hi) {
+    int m = (lo + hi + 1) >> 1;
+    if (excl[m] <= k) lo = m; else hi = m - 1;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(BM_THREADS) k_tc_bitmap(Lists L, const int32_t* __restrict__ order,
+                                                          unsigned long long* __restrict__ total) {
+  __shared__ unsigned s_bm[BM_WARPS][BM_WORDS];
+  __shared__ int s_lb[BM_WARPS][32];
+  __shared__ int s_excl[BM_WARPS][32];
+  const int lane = lane_id(), w = warp_id();
+  unsigned* bm = s_bm[w];
+  for (int i = lane; i < BM_WORDS; i += 32) bm[i] = 0u;
+  __syncwarp();
+  unsigned long long cnt = 0;
+  const int gwarp = (blockIdx.x * BM_THREADS + threadIdx.x) >> 5, nwarps = (gridDim.x * BM_THREADS) >> 5;
+  for (int ai = gwarp; ai < L.V; ai += nwarps) {
+    const int a = order[ai];
+    int sb, se, pb, pe;
+    anchor_ranges(L, a, sb, se, pb, pe);
+    const int ns = se - sb, np = pe - pb;
+    if (ns == 0 || np == 0) continue;
+    for (int i = lane; i < ns; i += 32) {
+      const int k = L.adj[sb + i];
+      atomicOr(&bm[k >> 5], 1u << (k & 31));
+    }
+    __syncwarp();
+    for (int g0 = 0; g0 < np; g0 += 32) {
+      const int p = g0 + lane < np ? L.adj[pb + g0 + lane] : -1;
+      int lb = 0, le = 0;
+      if (p >= 0) probe_range(L, a, p, lb, le);
+      const int len = le - lb;
+      int incl = len;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      const int tot = __shfl_sync(0xffffffffu, incl, 31);
+      s_lb[w][lane] = lb;
+      s_excl[w][lane] = incl - len;
+      __syncwarp();
+      for (int k0 = lane; k0 < tot; k0 += 32 * BM_UNROLL) {
+        int x[BM_UNROLL];
+#pragma unroll
+        for (int u = 0; u < BM_UNROLL; ++u) {
+          const int k = k0 + 32 * u;
+          x[u] = -1;
+          if (k < tot) {
+            const int o = owner_of(s_excl[w], k);
+            x[u] = L.adj[s_lb[w][o] + (k - s_excl[w][o])];
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < BM_UNROLL; ++u)
+          if (x[u] >= 0) cnt += (bm[x[u] >> 5] >> (x[u] & 31)) & 1u;
+      }
+      __syncwarp();
+    }
+    for (int i = lane; i < ns; i += 32) bm[L.adj[sb + i] >> 5] = 0u;
     __syncwarp();
   }
   cnt = warp_sum(cnt);
@@ -427,10 +507,17 @@ extern "C" int sp_tc(sp_graph_h g, int64_t* triangle_count, int32_t variant) {
   L.adj = p->oriented ? p->oadj.p : g->adj.p;
   SP_CHECK_CUDA(cudaMemsetAsync(p->ctr.p, 0, sizeof(unsigned int) * 2, s));
   SP_CHECK_CUDA(cudaMemsetAsync(p->total.p, 0, sizeof(unsigned long long), s));
-  tc::k_tc_warp<<<num_sms() * 4, tc::THREADS, 0, s>>>(L, p->order.p, p->heavy.p, p->ctr.p + 1, p->total.p);
-  SP_CHECK_LAUNCH();
-  tc::k_tc_heavy<<<num_sms() * 2, tc::THREADS, 0, s>>>(L, p->heavy.p, p->ctr.p + 1, p->total.p);
-  SP_CHECK_LAUNCH();
+  if (g->V <= 65536) {
+    int per_sm = 0;
+    SP_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tc::k_tc_bitmap, tc::BM_THREADS, 0));
+    tc::k_tc_bitmap<<<num_sms() * std::max(1, per_sm), tc::BM_THREADS, 0, s>>>(L, p->order.p, p->total.p);
+    SP_CHECK_LAUNCH();
+  } else {
+    tc::k_tc_warp<<<num_sms() * 4, tc::THREADS, 0, s>>>(L, p->order.p, p->heavy.p, p->ctr.p + 1, p->total.p);
+    SP_CHECK_LAUNCH();
+    tc::k_tc_heavy<<<num_sms() * 2, tc::THREADS, 0, s>>>(L, p->heavy.p, p->ctr.p + 1, p->total.p);
+    SP_CHECK_LAUNCH();
+  }
   unsigned long long h = 0;
   SP_TRY(copy_out(&h, p->total.p, sizeof(h), s));
   *triangle_count = (int64_t)h;

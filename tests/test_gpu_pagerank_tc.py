@@ -175,3 +175,11 @@ def test_invalid_csr_rejected():
     adj = np.array([1, 1], np.int32)  # duplicate
     with pytest.raises(_lib.SPError):
         DeviceGraph(off, adj)
+
+
+def test_tc_large_graph_hash_path():
+    # above 65536 vertices the anchor sets live in per-warp hash tables (+ the heavy-anchor kernel)
+    g = G.rmat(17, 16, seed=3)
+    assert Compute_TC(g) == O.tc(g.indexofNodes, g.edgeList)
+    gd = G.rmat(17, 8, seed=4, directed=True)
+    assert Compute_TC(gd) == O.tc(gd.indexofNodes, gd.edgeList)
