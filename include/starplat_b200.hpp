@@ -1,0 +1,133 @@
+// starplat_b200.hpp — drop-in replacements for the entry points StarPlat's code
+// generators emit for the static-graph programs, with their exact C++ signatures
+// (signature emitter src/backends/backend_omp/dsl_cpp_generator.cpp:3098-3151,
+// type mapping :2875-3050: Graph -> graph&, propNode<T>/propEdge<T> -> T*,
+// node -> int, SetN<g> -> std::set<int>&, a returning DSL function -> auto).
+//
+// Include this header AFTER the reference's graphcode/graph.hpp (it needs the
+// `graph` class and its public CSR fields) in place of the generated .cc file, and
+// link libsp_b200.so. The CSR of each `graph` object is uploaded to the GPU once
+// (first call) and reused by later calls; call starplat_b200::invalidate(g) after
+// changing the graph. Errors throw std::runtime_error (define
+// STARPLAT_B200_ABORT_ON_ERROR to print and abort instead).
+//
+// Replaces:
+//   auto Compute_TC(graph& g)                                        triangle_counting_dsl
+//   void ComputePageRank(graph& g, float beta, float delta, int maxIter, float* pageRank)
+//                                                                     PageRankDSLV3
+//   void Compute_PR(graph& g, float beta, float delta, int maxIter, float* pageRank)
+//                                                                     PageRankDSLV2 (same body)
+//   void Compute_SSSP(graph& g, int* dist, int* weight, int src)      sssp_dslV3
+//   void Compute_BC(graph& g, float* BC, std::set<int>& sourceSet)    bc_dslV2
+//   auto Compute_CD(graph& g, int* weight)                            community_detection
+#ifndef STARPLAT_B200_HPP
+#define STARPLAT_B200_HPP
+
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <set>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "starplat_b200.h"
+
+namespace starplat_b200 {
+
+inline void check(int status, const char* fn) {
+  if (status == SP_OK) return;
+  std::string msg = std::string(fn) + " failed (" + std::to_string(status) + "): " + sp_last_error();
+#ifdef STARPLAT_B200_ABORT_ON_ERROR
+  std::fprintf(stderr, "%s\n", msg.c_str());
+  std::abort();
+#else
+  throw std::runtime_error(msg);
+#endif
+}
+
+struct MirrorCache {
+  std::mutex mu;
+  std::map<const void*, sp_graph_h> by_graph;
+  ~MirrorCache() {
+    for (auto& kv : by_graph) sp_graph_free(kv.second);
+  }
+};
+
+inline MirrorCache& cache() {
+  static MirrorCache c;
+  return c;
+}
+
+// The device mirror of g (uploaded on first use).
+template <class Graph>
+inline sp_graph_h mirror(Graph& g) {
+  MirrorCache& c = cache();
+  std::lock_guard<std::mutex> lock(c.mu);
+  auto it = c.by_graph.find(&g);
+  if (it != c.by_graph.end()) return it->second;
+  const int V = g.num_nodes();
+  const long long E = g.num_edges();
+  sp_graph_h h = nullptr;
+  check(sp_graph_create(V, E, g.indexofNodes, g.edgeList, g.getEdgeLen(), g.rev_indexofNodes, g.srcList, 0, &h),
+        "sp_graph_create");
+  c.by_graph[&g] = h;
+  return h;
+}
+
+// Drop the cached mirror of g (after the host CSR changed, or before g is destroyed).
+template <class Graph>
+inline void invalidate(Graph& g) {
+  MirrorCache& c = cache();
+  std::lock_guard<std::mutex> lock(c.mu);
+  auto it = c.by_graph.find(&g);
+  if (it == c.by_graph.end()) return;
+  sp_graph_free(it->second);
+  c.by_graph.erase(it);
+}
+
+}  // namespace starplat_b200
+
+// ---- the generated entry points ------------------------------------------------
+
+inline auto Compute_TC(graph& g) {
+  int64_t count = 0;
+  starplat_b200::check(sp_tc(starplat_b200::mirror(g), &count, SP_TC_TUNED), "Compute_TC");
+  return (long)count;
+}
+
+inline void ComputePageRank(graph& g, float beta, float delta, int maxIter, float* pageRank) {
+  starplat_b200::check(sp_pagerank(starplat_b200::mirror(g), beta, delta, maxIter, pageRank, nullptr, nullptr,
+                                   SP_PR_TUNED),
+                       "ComputePageRank");
+}
+
+inline void Compute_PR(graph& g, float beta, float delta, int maxIter, float* pageRank) {
+  ComputePageRank(g, beta, delta, maxIter, pageRank);
+}
+
+inline void Compute_SSSP(graph& g, int* dist, int* weight, int src) {
+  starplat_b200::check(sp_sssp(starplat_b200::mirror(g), weight, src, dist, 0, SP_SSSP_DELTA, nullptr), "Compute_SSSP");
+}
+
+inline void Compute_BC(graph& g, float* BC, std::set<int>& sourceSet) {
+  std::vector<int32_t> src(sourceSet.begin(), sourceSet.end());
+  starplat_b200::check(sp_bc(starplat_b200::mirror(g), src.data(), (int32_t)src.size(), BC, SP_BC_BATCHED),
+                       "Compute_BC");
+}
+
+// community_detection takes propEdge<int> weight and returns the modularity.
+inline auto Compute_CD(graph& g, int* weight) {
+  std::vector<float> w;
+  const float* wp = nullptr;
+  if (weight) {
+    w.assign(weight, weight + g.num_edges());
+    wp = w.data();
+  }
+  double q = 0;
+  starplat_b200::check(sp_louvain(starplat_b200::mirror(g), wp, 1e-4, nullptr, &q, nullptr, nullptr), "Compute_CD");
+  return q;
+}
+
+#endif  // STARPLAT_B200_HPP

@@ -1,0 +1,46 @@
+// Driver in the shape of the reference's main_functions/*main.cpp: builds a graph,
+// calls the generated entry points (now from starplat_b200.hpp) and prints results.
+#include <cstdio>
+#include <set>
+#include <vector>
+
+#include GRAPH_HEADER
+#include "starplat_b200.hpp"
+
+int main(int argc, char** argv) {
+  if (argc < 3) return 2;
+#ifdef PARSE_TEXT
+  graph g(argv[1]);
+#else
+  graph g;
+#endif
+#ifdef PARSE_TEXT
+  g.parseGraph();
+#else
+  if (!g.load(argv[1])) return 3;
+#endif
+  const int V = g.num_nodes();
+  std::printf("V %d E %d\n", V, g.num_edges());
+  long tc = Compute_TC(g);
+  std::printf("TC %ld\n", tc);
+  std::vector<float> pr(V);
+  ComputePageRank(g, 1e-6f, 0.85f, 100, pr.data());
+  std::printf("PR");
+  for (int v = 0; v < V; ++v) std::printf(" %.9g", pr[v]);
+  std::printf("\n");
+  std::vector<int> dist(V), w(g.getEdgeLen(), g.getEdgeLen() + g.num_edges());
+  Compute_SSSP(g, dist.data(), w.data(), atoi(argv[2]));
+  std::printf("SSSP");
+  for (int v = 0; v < V; ++v) std::printf(" %d", dist[v]);
+  std::printf("\n");
+  std::set<int> sources;
+  for (int v = 0; v < V; v += 3) sources.insert(v);
+  std::vector<float> bc(V);
+  Compute_BC(g, bc.data(), sources);
+  std::printf("BC");
+  for (int v = 0; v < V; ++v) std::printf(" %.9g", bc[v]);
+  std::printf("\n");
+  std::printf("CD %.12f\n", Compute_CD(g, nullptr));
+  starplat_b200::invalidate(g);
+  return 0;
+}

@@ -1,0 +1,95 @@
+"""The C++ drop-in header (include/starplat_b200.hpp): the generated entry points'
+exact signatures, compiled into a driver shaped like the reference's
+main_functions/*main.cpp. CPU: it compiles. GPU: its outputs match the oracle,
+with a test stand-in `graph` and — when built in a reference checkout — with the
+reference's own graph.hpp and parseGraph (oracle/_ref/ref_driver)."""
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from starplat_b200 import generators as G
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIBDIR = os.path.join(ROOT, "starplat_b200")
+
+
+def build_driver(outdir):
+    exe = os.path.join(outdir, "drop_in")
+    cmd = ["g++", "-O2", "-std=c++17", '-DGRAPH_HEADER="mini_graph.hpp"', "-I", os.path.join(ROOT, "tests", "cpp"),
+           "-I", os.path.join(ROOT, "include"), os.path.join(ROOT, "tests", "cpp", "drop_in_main.cpp"),
+           "-L", LIBDIR, "-lsp_b200", f"-Wl,-rpath,{LIBDIR}", "-o", exe]
+    subprocess.check_call(cmd)
+    return exe
+
+
+def test_dropin_header_compiles():
+    with tempfile.TemporaryDirectory() as d:
+        assert os.path.exists(build_driver(d))
+
+
+def write_bin(g, path):
+    with open(path, "wb") as f:
+        np.array([g.V, g.E], np.int32).tofile(f)
+        for a in (g.indexofNodes, g.edgeList, g.edgeLen, g.rev_indexofNodes, g.srcList):
+            np.ascontiguousarray(a, np.int32).tofile(f)
+
+
+def parse(out):
+    res = {}
+    for line in out.splitlines():
+        k, *vals = line.split()
+        res[k] = vals
+    return res
+
+
+def check_outputs(res, g, src):
+    assert int(res["TC"][0]) == O.tc(g.indexofNodes, g.edgeList)
+    pr = np.array(res["PR"], np.float64)
+    ref, _, _ = O.pagerank(g.indexofNodes, g.rev_indexofNodes, g.srcList, 1e-6, 0.85, 100)
+    assert np.abs(pr - ref).sum() < 1e-6
+    assert np.array_equal(np.array(res["SSSP"], np.int64), O.sssp(g.indexofNodes, g.edgeList, g.edgeLen, src))
+    srcs = np.arange(0, g.V, 3, dtype=np.int32)
+    bc = np.array(res["BC"], np.float64)
+    rb = O.bc(g.indexofNodes, g.edgeList, srcs)
+    assert np.all(np.abs(bc - rb) <= 1e-5 * np.abs(rb) + 1e-6)
+    q, _, _ = O.louvain(g.indexofNodes, g.edgeList)
+    assert float(res["CD"][0]) > q - 1e-3
+
+
+def small_graph():
+    g = G.rmat(10, 8, seed=12)
+    g.edgeLen = G.hash_weights(g, 5, 1, 50, True)
+    # every vertex id up to V-1 must appear for parseGraph's num_nodes() = max id + 1
+    assert g.indexofNodes[-1] > g.indexofNodes[-2]
+    return g
+
+
+@pytest.mark.gpu
+def test_dropin_driver_matches_oracle():
+    g = small_graph()
+    with tempfile.TemporaryDirectory() as d:
+        exe = build_driver(d)
+        path = os.path.join(d, "g.bin")
+        write_bin(g, path)
+        out = subprocess.run([exe, path, "5"], check=True, capture_output=True, text=True).stdout
+    check_outputs(parse(out), g, 5)
+
+
+@pytest.mark.gpu
+def test_dropin_with_reference_graph_hpp():
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+    if not os.path.exists(exe):
+        pytest.skip("oracle/_ref/ref_driver not built (needs the reference checkout)")
+    g = small_graph()
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "g.txt")
+        u = np.repeat(np.arange(g.V), np.diff(g.indexofNodes))
+        np.savetxt(path, np.stack([u, g.edgeList, g.edgeLen], 1), fmt="%d")
+        out = subprocess.run([exe, path, "5"], check=True, capture_output=True, text=True).stdout
+    res = parse(out)
+    assert int(res["V"][0]) == g.V and int(res["V"][2]) == g.E  # parseGraph built the same CSR
+    check_outputs(res, g, 5)
