@@ -61,9 +61,15 @@ def check_outputs(res, g, src):
 
 
 def small_graph():
-    g = G.rmat(10, 8, seed=12)
+    from starplat_b200.graph import CSRGraph
+
+    r = G.rmat(10, 8, seed=12)
+    u = np.repeat(np.arange(r.V, dtype=np.int32), np.diff(r.indexofNodes))
+    # an edge at the last id, so parseGraph's num_nodes() (max id + 1) is V
+    src = np.concatenate([u, [r.V - 1]]).astype(np.int32)
+    dst = np.concatenate([r.edgeList, [0]]).astype(np.int32)
+    g = CSRGraph.from_edges(r.V, src, dst, symmetrize=True, name="dropin")
     g.edgeLen = G.hash_weights(g, 5, 1, 50, True)
-    # every vertex id up to V-1 must appear for parseGraph's num_nodes() = max id + 1
     assert g.indexofNodes[-1] > g.indexofNodes[-2]
     return g
 
