@@ -149,6 +149,24 @@ int sp_bc_graphs(sp_graph_h g, int32_t ngraphs, const int32_t* vertex_offset, co
 int sp_louvain(sp_graph_h g, const float* weight, double threshold, int32_t* community, double* modularity,
                int32_t* levels, int32_t* sweeps);
 
+/* ---- PageRank without device allocation -------------------------------------------
+ * No counterpart in the reference: an addition for callers that cannot call
+ * cudaMalloc (an engine that owns all device memory through its own pool and hands
+ * in its buffers, a process under a hard memory cap, a caller that cannot accept the
+ * device-wide synchronisation an allocation may cause). Same semantics and tolerance
+ * as sp_pagerank. All pointers are DEVICE pointers owned by the caller:
+ * indexofNodes[V+1] (for out-degrees), rev_indexofNodes[V+1], srcList[E], pageRank[V].
+ * Scratch is a fixed array inside the library (about 12.6 MB, held on every GPU that
+ * loads the library until exit), so V is limited to SP_NOALLOC_MAX_V; larger graphs
+ * get SP_ERR_INVALID. The first call on a device looks up that array's address
+ * (cudaGetSymbolAddress) with the device current; make it before any stream capture.
+ * Calls share the array: calls that overlap on the GPU race and must be serialised.
+ * cuda_stream may be NULL (default stream); iterations may be NULL. */
+#define SP_NOALLOC_MAX_V (1 << 20)
+int sp_pagerank_noalloc(const int32_t* indexofNodes, const int32_t* rev_indexofNodes, const int32_t* srcList,
+                        int32_t V, int64_t E, float beta, float delta, int32_t maxIter, float* pageRank,
+                        int32_t* iterations, void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -21,6 +21,7 @@ SP_ERR = {
     -6: "SP_ERR_NEG_CYCLE",
 }
 
+SP_ERR_INVALID_CODE = -1
 SP_GRAPH_DEVICE_PTRS = 0x1
 SP_TC_TUNED = 0
 SP_TC_PLAIN = 1
@@ -65,6 +66,7 @@ SIGNATURES = {
     "sp_bc_graphs": (ctypes.c_int, [vp, i32, vp, vp, vp, vp]),
     "sp_bfs_sigma": (ctypes.c_int, [vp, vp, i32, vp, vp]),
     "sp_louvain": (ctypes.c_int, [vp, vp, f64, vp, P(f64), P(i32), P(i32)]),
+    "sp_pagerank_noalloc": (ctypes.c_int, [vp, vp, vp, i32, i64, f32, f32, i32, vp, P(i32), vp]),
 }
 
 
