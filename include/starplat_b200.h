@@ -69,6 +69,7 @@ int sp_graph_info(sp_graph_h g, int32_t* V, int64_t* E, int32_t* symmetric);
  *             edge weight).
  *   "sssp.ctas_per_sm"  SSSP: persistent CTAs per SM of the delta-stepping kernel (1..8,
  *             default 4; fewer CTAs make each grid barrier cheaper on high-diameter graphs).
+ *   "sssp.last_delta", "sssp.last_ctas" (read only): the schedule the last SSSP call ran.
  *   "bc.batch"  BC: sources traversed together in one multi-source pass (1..64, default 64). */
 int sp_tune_set(sp_graph_h g, const char* key, int64_t value);
 int sp_tune_get(sp_graph_h g, const char* key, int64_t* value);
@@ -148,6 +149,28 @@ int sp_bc_graphs(sp_graph_h g, int32_t ngraphs, const int32_t* vertex_offset, co
  * of local-move sweeps run. */
 int sp_louvain(sp_graph_h g, const float* weight, double threshold, int32_t* community, double* modularity,
                int32_t* levels, int32_t* sweeps);
+
+/* ---- learned scheduler ----------------------------------------------------------
+ * No counterpart in the reference. A small MLP scores candidate schedules (for SSSP:
+ * bucket width and CTAs per SM) from graph features and predicts their log run time;
+ * sp_sssp with delta <= 0 and no "sssp.delta" knob runs the best-scored candidate when
+ * a model is loaded, else the fixed heuristic. Schedules never change results.
+ * Network: x[SP_MLP_IN] -> tanh(H) -> tanh(H) -> 1, H = SP_MLP_HIDDEN, parameters
+ * W1(H x IN) b1 W2(H x H) b2 w3 b3 in that order (SP_MLP_PARAMS floats). Host or device
+ * pointers. sp_mlp_grad: gradient of the mean squared error (for checking against a
+ * CPU reference); sp_mlp_train: full-batch Adam, all steps in one fused launch. */
+#define SP_MLP_IN 12
+#define SP_MLP_HIDDEN 32
+#define SP_MLP_PARAMS (SP_MLP_HIDDEN * SP_MLP_IN + SP_MLP_HIDDEN * SP_MLP_HIDDEN + 3 * SP_MLP_HIDDEN + 1)
+int sp_mlp_forward(const float* params, const float* X, int32_t N, float* y);
+int sp_mlp_grad(const float* params, const float* X, const float* T, int32_t N, float* grad, float* loss);
+int sp_mlp_train(float* params, const float* X, const float* T, int32_t N, int32_t steps, float lr, float* final_loss);
+/* Load (params != NULL) or unload (params == NULL) the process-wide scheduling model;
+ * feat_mean/feat_scale normalise inputs: x' = (x - mean) * scale. */
+int sp_sched_load(const float* params, const float* feat_mean, const float* feat_scale);
+/* The SP_MLP_IN inputs the scheduler builds for SSSP on g with a candidate schedule
+ * (delta multiple of the largest weight, CTAs per SM); weight NULL = edgeLen. */
+int sp_sssp_features(sp_graph_h g, const int32_t* weight, double delta_mult, int32_t ctas_per_sm, float* x);
 
 /* ---- PageRank without device allocation -------------------------------------------
  * No counterpart in the reference: an addition for callers that cannot call

@@ -344,7 +344,15 @@ int sp_tune_get(sp_graph_h g, const char* key, int64_t* value) {
     return SP_OK;
   }
   if (!strcmp(key, "sssp.ctas_per_sm")) {
-    *value = g->sssp_ctas_per_sm > 0 ? g->sssp_ctas_per_sm : 4;
+    *value = g->sssp_ctas_per_sm;
+    return SP_OK;
+  }
+  if (!strcmp(key, "sssp.last_delta")) {
+    *value = g->sssp_last_delta;
+    return SP_OK;
+  }
+  if (!strcmp(key, "sssp.last_ctas")) {
+    *value = g->sssp_last_ctas;
     return SP_OK;
   }
   if (!strcmp(key, "bc.batch")) {

@@ -101,7 +101,9 @@ struct sp_graph {
   int32_t max_out_deg = -1;
   int32_t pr_hot = -1;  // PageRank: contrib values staged in shared memory (-1 = default)
   int64_t sssp_delta = 0;  // SSSP bucket width (0 = max edge weight)
-  int32_t sssp_ctas_per_sm = 0;  // SSSP persistent CTAs per SM (0 = 4)
+  int32_t sssp_ctas_per_sm = 0;  // SSSP persistent CTAs per SM (0 = learned / 4)
+  int64_t sssp_last_delta = 0;   // schedule of the last SSSP call (reporting)
+  int32_t sssp_last_ctas = 0;
   int32_t bc_batch = 0;    // BC sources per multi-source batch (0 = 64)
   cudaStream_t stream = nullptr;
   bool own_stream = false;

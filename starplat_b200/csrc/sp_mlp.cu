@@ -1,0 +1,296 @@
+// The learned scheduler's network: a small MLP, with hand-written CUDA kernels
+// for batched inference, the loss gradient, and fully fused training (one launch
+// runs every Adam step, parameters and moments held in shared memory).
+//
+// Architecture (fixed): x[SP_MLP_IN] -> tanh(W1 x + b1)[H] -> tanh(W2 h1 + b2)[H]
+// -> y = w3 . h2 + b3, H = SP_MLP_HIDDEN. Loss: mean squared error over the batch.
+// Parameter vector layout: W1 (H x IN, row-major), b1 (H), W2 (H x H), b2 (H),
+// w3 (H), b3 (1). FP32 throughout.
+//
+// It never affects results: it only scores candidate schedules (see sp_sssp), and
+// the scheduler falls back to the fixed heuristic when no model is loaded.
+#include <cmath>
+#include <mutex>
+#include <vector>
+
+#include "sp_internal.cuh"
+
+namespace sp {
+namespace mlp {
+
+constexpr int IN = SP_MLP_IN;
+constexpr int H = SP_MLP_HIDDEN;
+constexpr int OFF_W1 = 0;
+constexpr int OFF_B1 = OFF_W1 + H * IN;
+constexpr int OFF_W2 = OFF_B1 + H;
+constexpr int OFF_B2 = OFF_W2 + H * H;
+constexpr int OFF_W3 = OFF_B2 + H;
+constexpr int OFF_B3 = OFF_W3 + H;
+constexpr int P = OFF_B3 + 1;
+static_assert(P == SP_MLP_PARAMS, "parameter count");
+
+// forward for one sample; keeps the activations for the backward pass
+__device__ __forceinline__ float forward(const float* __restrict__ p, const float* x, float* h1, float* h2) {
+#pragma unroll 4
+  for (int j = 0; j < H; ++j) {
+    float z = p[OFF_B1 + j];
+#pragma unroll
+    for (int i = 0; i < IN; ++i) z = fmaf(p[OFF_W1 + j * IN + i], x[i], z);
+    h1[j] = tanhf(z);
+  }
+#pragma unroll 4
+  for (int j = 0; j < H; ++j) {
+    float z = p[OFF_B2 + j];
+#pragma unroll 8
+    for (int i = 0; i < H; ++i) z = fmaf(p[OFF_W2 + j * H + i], h1[i], z);
+    h2[j] = tanhf(z);
+  }
+  float y = p[OFF_B3];
+#pragma unroll 8
+  for (int j = 0; j < H; ++j) y = fmaf(p[OFF_W3 + j], h2[j], y);
+  return y;
+}
+
+// Add one sample's gradient (scaled by gy = dL/dy) into g, summed over the warp
+// first (shuffles), then one shared/global atomic per parameter per warp.
+__device__ __forceinline__ void warp_add(float* g, int idx, float v, bool lane0) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if (lane0 && v != 0.0f) atomicAdd(&g[idx], v);
+}
+
+__device__ void backward(const float* __restrict__ p, const float* x, const float* h1, const float* h2, float gy,
+                         float* g, bool lane0) {
+  float dz2[H];
+#pragma unroll 4
+  for (int j = 0; j < H; ++j) {
+    warp_add(g, OFF_W3 + j, gy * h2[j], lane0);
+    dz2[j] = gy * p[OFF_W3 + j] * (1.0f - h2[j] * h2[j]);
+    warp_add(g, OFF_B2 + j, dz2[j], lane0);
+  }
+  warp_add(g, OFF_B3, gy, lane0);
+#pragma unroll 2
+  for (int j = 0; j < H; ++j)
+#pragma unroll 8
+    for (int i = 0; i < H; ++i) warp_add(g, OFF_W2 + j * H + i, dz2[j] * h1[i], lane0);
+#pragma unroll 2
+  for (int i = 0; i < H; ++i) {
+    float dh1 = 0.0f;
+#pragma unroll 8
+    for (int j = 0; j < H; ++j) dh1 = fmaf(p[OFF_W2 + j * H + i], dz2[j], dh1);
+    const float dz1 = dh1 * (1.0f - h1[i] * h1[i]);
+    warp_add(g, OFF_B1 + i, dz1, lane0);
+#pragma unroll
+    for (int k = 0; k < IN; ++k) warp_add(g, OFF_W1 + i * IN + k, dz1 * x[k], lane0);
+  }
+}
+
+__global__ void k_forward(const float* __restrict__ params, const float* __restrict__ X, int N, float* __restrict__ y) {
+  __shared__ float sp_[P];
+  for (int i = threadIdx.x; i < P; i += blockDim.x) sp_[i] = params[i];
+  __syncthreads();
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < N; n += gridDim.x * blockDim.x) {
+    float x[IN], h1[H], h2[H];
+#pragma unroll
+    for (int i = 0; i < IN; ++i) x[i] = X[(size_t)n * IN + i];
+    y[n] = forward(sp_, x, h1, h2);
+  }
+}
+
+// dL/dparams of L = mean (y - t)^2 into grad (zeroed by the caller) and L into loss.
+__global__ void k_grad(const float* __restrict__ params, const float* __restrict__ X, const float* __restrict__ T,
+                       int N, float* grad, float* loss) {
+  __shared__ float sp_[P];
+  __shared__ float sg[P];
+  for (int i = threadIdx.x; i < P; i += blockDim.x) {
+    sp_[i] = params[i];
+    sg[i] = 0.0f;
+  }
+  __syncthreads();
+  float lsum = 0.0f;
+  const int lane = threadIdx.x & 31;
+  // whole warps step through the samples together (shuffles need every lane)
+  const int base0 = (blockIdx.x * blockDim.x + (threadIdx.x & ~31));
+  for (int b = base0; b < N; b += gridDim.x * blockDim.x) {
+    const int n = b + lane;
+    const bool valid = n < N;
+    float x[IN], h1[H], h2[H];
+#pragma unroll
+    for (int i = 0; i < IN; ++i) x[i] = valid ? X[(size_t)n * IN + i] : 0.0f;
+    const float y = forward(sp_, x, h1, h2);
+    const float r = valid ? (y - T[n]) : 0.0f;
+    lsum += r * r;
+    backward(sp_, x, h1, h2, 2.0f * r / (float)N, sg, lane == 0);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < P; i += blockDim.x)
+    if (sg[i] != 0.0f) atomicAdd(&grad[i], sg[i]);
+  lsum = warp_sum(lsum);
+  if (lane == 0 && lsum != 0.0f) atomicAdd(loss, lsum / (float)N);
+}
+
+// Fused training: ONE CTA runs `steps` full-batch Adam steps; parameters,
+// gradients and both moments live in shared memory for the whole run.
+__global__ void __launch_bounds__(256) k_train(float* params, const float* __restrict__ X,
+                                                const float* __restrict__ T, int N, int steps, float lr,
+                                                float* loss_out) {
+  __shared__ float sp_[P];
+  __shared__ float sg[P];
+  __shared__ float sm[P];
+  __shared__ float sv[P];
+  __shared__ float s_loss;
+  for (int i = threadIdx.x; i < P; i += blockDim.x) {
+    sp_[i] = params[i];
+    sm[i] = 0.0f;
+    sv[i] = 0.0f;
+  }
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  const int lane = threadIdx.x & 31;
+  float b1t = 1.0f, b2t = 1.0f;
+  for (int t = 0; t < steps; ++t) {
+    for (int i = threadIdx.x; i < P; i += blockDim.x) sg[i] = 0.0f;
+    if (threadIdx.x == 0) s_loss = 0.0f;
+    __syncthreads();
+    float lsum = 0.0f;
+    for (int b = (threadIdx.x & ~31); b < N; b += blockDim.x) {
+      const int n = b + lane;
+      const bool valid = n < N;
+      float x[IN], h1[H], h2[H];
+#pragma unroll
+      for (int i = 0; i < IN; ++i) x[i] = valid ? X[(size_t)n * IN + i] : 0.0f;
+      const float y = forward(sp_, x, h1, h2);
+      const float r = valid ? (y - T[n]) : 0.0f;
+      lsum += r * r;
+      backward(sp_, x, h1, h2, 2.0f * r / (float)N, sg, lane == 0);
+    }
+    lsum = warp_sum(lsum);
+    if (lane == 0) atomicAdd(&s_loss, lsum / (float)N);
+    __syncthreads();
+    b1t *= b1;
+    b2t *= b2;
+    const float a = lr * sqrtf(1.0f - b2t) / (1.0f - b1t);
+    for (int i = threadIdx.x; i < P; i += blockDim.x) {
+      const float g = sg[i];
+      sm[i] = b1 * sm[i] + (1.0f - b1) * g;
+      sv[i] = b2 * sv[i] + (1.0f - b2) * g * g;
+      sp_[i] -= a * sm[i] / (sqrtf(sv[i]) + eps);
+    }
+    if (threadIdx.x == 0 && t == steps - 1) *loss_out = s_loss;
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < P; i += blockDim.x) params[i] = sp_[i];
+}
+
+// ---- the loaded scheduling model (process-wide)
+std::mutex g_mu;
+std::vector<float> g_params;   // empty = no model: fixed heuristic
+std::vector<float> g_mean, g_scale;
+
+}  // namespace mlp
+
+// Score candidate rows X[n][IN] with the loaded model (host in, host out).
+// Returns SP_ERR_UNSUPPORTED when no model is loaded.
+int mlp_score(const std::vector<float>& X, std::vector<float>& y, cudaStream_t s) {
+  std::vector<float> params, mean, scale;
+  {
+    std::lock_guard<std::mutex> lock(mlp::g_mu);
+    if (mlp::g_params.empty()) return SP_ERR_UNSUPPORTED;
+    params = mlp::g_params;
+    mean = mlp::g_mean;
+    scale = mlp::g_scale;
+  }
+  const int N = (int)(X.size() / mlp::IN);
+  std::vector<float> Xn(X.size());
+  for (int n = 0; n < N; ++n)
+    for (int i = 0; i < mlp::IN; ++i) Xn[(size_t)n * mlp::IN + i] = (X[(size_t)n * mlp::IN + i] - mean[i]) * scale[i];
+  dbuf<float> dp, dx, dy;
+  SP_TRY(dp.alloc(mlp::P));
+  SP_TRY(dx.alloc(Xn.size()));
+  SP_TRY(dy.alloc(N));
+  SP_CHECK_CUDA(cudaMemcpyAsync(dp.p, params.data(), sizeof(float) * mlp::P, cudaMemcpyHostToDevice, s));
+  SP_CHECK_CUDA(cudaMemcpyAsync(dx.p, Xn.data(), sizeof(float) * Xn.size(), cudaMemcpyHostToDevice, s));
+  mlp::k_forward<<<std::max(1, (N + 127) / 128), 128, 0, s>>>(dp.p, dx.p, N, dy.p);
+  SP_CHECK_LAUNCH();
+  y.resize(N);
+  return copy_out(y.data(), dy.p, sizeof(float) * N, s);
+}
+
+}  // namespace sp
+
+using namespace sp;
+
+namespace {
+int stage(const float* src, size_t n, dbuf<float>& buf, cudaStream_t s) {
+  SP_TRY(buf.alloc(n));
+  if (n) SP_CHECK_CUDA(cudaMemcpyAsync(buf.p, src, sizeof(float) * n, cudaMemcpyDefault, s));
+  return SP_OK;
+}
+}  // namespace
+
+extern "C" int sp_mlp_forward(const float* params, const float* X, int32_t N, float* y) {
+  if (!params || !X || !y || N <= 0) {
+    set_error("sp_mlp_forward: invalid argument");
+    return SP_ERR_INVALID;
+  }
+  cudaStream_t s = 0;
+  dbuf<float> dp, dx, dy;
+  SP_TRY(stage(params, mlp::P, dp, s));
+  SP_TRY(stage(X, (size_t)N * mlp::IN, dx, s));
+  SP_TRY(dy.alloc(N));
+  mlp::k_forward<<<std::max(1, (N + 127) / 128), 128, 0, s>>>(dp.p, dx.p, N, dy.p);
+  SP_CHECK_LAUNCH();
+  return copy_out(y, dy.p, sizeof(float) * N, s);
+}
+
+extern "C" int sp_mlp_grad(const float* params, const float* X, const float* T, int32_t N, float* grad, float* loss) {
+  if (!params || !X || !T || !grad || !loss || N <= 0) {
+    set_error("sp_mlp_grad: invalid argument");
+    return SP_ERR_INVALID;
+  }
+  cudaStream_t s = 0;
+  dbuf<float> dp, dx, dt, dg;
+  SP_TRY(stage(params, mlp::P, dp, s));
+  SP_TRY(stage(X, (size_t)N * mlp::IN, dx, s));
+  SP_TRY(stage(T, N, dt, s));
+  SP_TRY(dg.alloc(mlp::P + 1));
+  SP_CHECK_CUDA(cudaMemsetAsync(dg.p, 0, sizeof(float) * (mlp::P + 1), s));
+  mlp::k_grad<<<std::max(1, std::min(64, (N + 255) / 256)), 256, 0, s>>>(dp.p, dx.p, dt.p, N, dg.p, dg.p + mlp::P);
+  SP_CHECK_LAUNCH();
+  SP_TRY(copy_out(grad, dg.p, sizeof(float) * mlp::P, s));
+  return copy_out(loss, dg.p + mlp::P, sizeof(float), s);
+}
+
+extern "C" int sp_mlp_train(float* params, const float* X, const float* T, int32_t N, int32_t steps, float lr,
+                            float* final_loss) {
+  if (!params || !X || !T || N <= 0 || steps <= 0 || !(lr > 0)) {
+    set_error("sp_mlp_train: invalid argument");
+    return SP_ERR_INVALID;
+  }
+  cudaStream_t s = 0;
+  dbuf<float> dp, dx, dt, dl;
+  SP_TRY(stage(params, mlp::P, dp, s));
+  SP_TRY(stage(X, (size_t)N * mlp::IN, dx, s));
+  SP_TRY(stage(T, N, dt, s));
+  SP_TRY(dl.alloc(1));
+  mlp::k_train<<<1, 256, 0, s>>>(dp.p, dx.p, dt.p, N, steps, lr, dl.p);
+  SP_CHECK_LAUNCH();
+  SP_TRY(copy_out(params, dp.p, sizeof(float) * mlp::P, s));
+  if (final_loss) SP_TRY(copy_out(final_loss, dl.p, sizeof(float), s));
+  return SP_OK;
+}
+
+extern "C" int sp_sched_load(const float* params, const float* feat_mean, const float* feat_scale) {
+  std::lock_guard<std::mutex> lock(mlp::g_mu);
+  if (!params) {
+    mlp::g_params.clear();
+    return SP_OK;
+  }
+  if (!feat_mean || !feat_scale) {
+    set_error("sp_sched_load: feature normalisation required");
+    return SP_ERR_INVALID;
+  }
+  mlp::g_params.assign(params, params + mlp::P);
+  mlp::g_mean.assign(feat_mean, feat_mean + mlp::IN);
+  mlp::g_scale.assign(feat_scale, feat_scale + mlp::IN);
+  return SP_OK;
+}

@@ -23,6 +23,7 @@
 // SP_SSSP_PLAIN: the generated CUDA form — one thread per vertex over all V each
 // iteration, modified flags, atomicMin, host loop on a finished flag.
 #include <climits>
+#include <cmath>
 #include <vector>
 
 #include "sp_internal.cuh"
@@ -395,7 +396,30 @@ static int sssp_prepare(sp_graph* g, const int32_t* weight, const int32_t** wdev
   return SP_OK;
 }
 
-static int sssp_delta(sp_graph* g, const int32_t* w, int32_t src, int32_t* dist_out, int64_t delta,
+int mlp_score(const std::vector<float>& X, std::vector<float>& y, cudaStream_t s);
+
+// Scheduler inputs (SP_MLP_IN): graph shape and weight range, then the candidate
+// schedule (log2 of the delta multiple of the largest weight, CTAs per SM).
+static int sssp_features(sp_graph* g, double mult, int ctas, float* x) {
+  SP_TRY(ensure_symmetry(g));
+  const double V = g->V, E = (double)g->E, avg = E / V;
+  const double mx = g->max_out_deg, wmax = std::max(1, g->sssp->w_max), wmin = g->sssp->w_min;
+  x[0] = (float)std::log2(V);
+  x[1] = (float)std::log2(E + 1.0);
+  x[2] = (float)avg;
+  x[3] = (float)std::log2(mx + 1.0);
+  x[4] = (float)std::log2((mx + 1.0) / (avg + 1.0));
+  x[5] = (float)g->symmetric;
+  x[6] = (float)std::log2(wmax + 1.0);
+  x[7] = (float)std::log2(std::max(1.0, wmax - wmin + 1.0));
+  x[8] = (float)std::log2(mult);
+  x[9] = (float)ctas;
+  x[10] = (float)(std::log2(mult) * std::log2(V));  // interaction: bucket width vs size
+  x[11] = (float)(ctas * avg);
+  return SP_OK;
+}
+
+static int sssp_delta(sp_graph* g, const int32_t* w, int32_t src, int32_t* dist_out, int64_t delta, int ctas,
                       int32_t* rounds_out) {
   SsspPlan* p = g->sssp;
   cudaStream_t s = g->stream;
@@ -440,8 +464,7 @@ static int sssp_delta(sp_graph* g, const int32_t* w, int32_t src, int32_t* dist_
   SP_CHECK_LAUNCH();
   int per_sm = 0;
   SP_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ss::k_delta, ss::THREADS, 0));
-  const int want = g->sssp_ctas_per_sm > 0 ? g->sssp_ctas_per_sm : 4;
-  const int grid = num_sms() * std::max(1, std::min(per_sm, want));
+  const int grid = num_sms() * std::max(1, std::min(per_sm, ctas));
   void* params[] = {&a};
   SP_CHECK_CUDA(cudaLaunchCooperativeKernel((void*)ss::k_delta, grid, ss::THREADS, params, 0, s));
   g_launches++;
@@ -516,6 +539,45 @@ extern "C" int sp_sssp(sp_graph_h g, const int32_t* weight, int32_t src, int32_t
     set_error("sp_sssp: unknown variant %d", variant);
     return SP_ERR_INVALID;
   }
-  if (delta <= 0) delta = g->sssp_delta > 0 ? g->sssp_delta : std::max<int64_t>(1, (int64_t)g->sssp->w_max);
-  return sssp_delta(g, w, src, dist, delta, rounds);
+  int ctas = g->sssp_ctas_per_sm > 0 ? g->sssp_ctas_per_sm : 4;
+  const int64_t wmax = std::max<int64_t>(1, (int64_t)g->sssp->w_max);
+  if (delta <= 0 && g->sssp_delta > 0) delta = g->sssp_delta;
+  if (delta <= 0 && g->sssp_ctas_per_sm == 0) {
+    // learned schedule: score every candidate, run the best (fixed heuristic if no model)
+    static const double mults[] = {1, 2, 4, 8, 16, 32, 64};
+    static const int cts[] = {1, 2, 4};
+    std::vector<float> X;
+    std::vector<std::pair<double, int>> cand;
+    for (double m : mults)
+      for (int c : cts) {
+        float x[SP_MLP_IN];
+        SP_TRY(sssp_features(g, m, c, x));
+        X.insert(X.end(), x, x + SP_MLP_IN);
+        cand.push_back({m, c});
+      }
+    std::vector<float> score;
+    if (mlp_score(X, score, g->stream) == SP_OK) {
+      int best = 0;
+      for (int k = 1; k < (int)score.size(); ++k)
+        if (score[k] < score[best]) best = k;
+      delta = (int64_t)std::llround(cand[best].first * (double)wmax);
+      ctas = cand[best].second;
+    }
+  }
+  if (delta <= 0) delta = wmax;
+  g->sssp_last_delta = delta;
+  g->sssp_last_ctas = ctas;
+  return sssp_delta(g, w, src, dist, delta, ctas, rounds);
+}
+
+extern "C" int sp_sssp_features(sp_graph_h g, const int32_t* weight, double delta_mult, int32_t ctas_per_sm,
+                                float* x) {
+  using namespace sp;
+  if (!g || !x || !(delta_mult > 0) || ctas_per_sm <= 0) {
+    set_error("sp_sssp_features: invalid argument");
+    return SP_ERR_INVALID;
+  }
+  const int32_t* w = nullptr;
+  SP_TRY(sssp_prepare(g, weight, &w));
+  return sssp_features(g, delta_mult, ctas_per_sm, x);
 }

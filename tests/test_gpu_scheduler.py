@@ -1,0 +1,131 @@
+"""GPU: the learned scheduler. The network's CUDA kernels agree with the FP64
+oracle (forward, gradient); the fused training kernel fits; a loaded model keeps
+SSSP exact; and on graphs it was not trained on, the learned schedule is compared
+with the fixed heuristic (the gain is printed; the learned one must not lose)."""
+import math
+import os
+
+import numpy as np
+import pytest
+
+from oracle import mlp_oracle as M
+from oracle import oracle as O
+from starplat_b200 import _lib
+from starplat_b200 import generators as G
+from starplat_b200 import scheduler as S
+from starplat_b200.device import DeviceGraph
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(autouse=True)
+def no_model_after_each_test():
+    yield
+    S.unload()
+
+
+def data(n=300, seed=1):
+    rng = np.random.default_rng(seed)
+    X = rng.normal(0, 1, (n, M.IN)).astype(np.float32)
+    T = (np.sin(X[:, 0]) + 0.5 * X[:, 1] * X[:, 2] - 0.3 * X[:, 3] ** 2).astype(np.float32)
+    return X, T
+
+
+def test_forward_matches_oracle():
+    p = S.init_params(3)
+    X, _ = data()
+    y = S.mlp_forward(p, X)
+    ref, _, _ = M.forward(p.astype(np.float64), X.astype(np.float64))
+    assert np.allclose(y, ref, rtol=1e-4, atol=1e-5)
+
+
+def test_gradient_matches_oracle():
+    rng = np.random.default_rng(2)
+    p = (rng.normal(0, 0.3, _lib.SP_MLP_PARAMS)).astype(np.float32)
+    X, T = data(517)  # not a multiple of the warp size
+    loss, g = S.mlp_grad(p, X, T)
+    L, gr = M.loss_grad(p.astype(np.float64), X.astype(np.float64), T.astype(np.float64))
+    assert abs(loss - L) <= 1e-4 * max(1.0, L)
+    err = np.linalg.norm(g - gr) / np.linalg.norm(gr)
+    assert err < 1e-4, err
+    assert np.allclose(g, gr, rtol=1e-3, atol=1e-6 * np.abs(gr).max())
+
+
+def test_fused_training_fits():
+    X, T = data(800)
+    p0 = S.init_params(0)
+    L0, _ = M.loss_grad(p0.astype(np.float64), X, T)
+    p, loss = S.mlp_train(p0, X, T, steps=1500, lr=3e-3)
+    L1, _ = M.loss_grad(p.astype(np.float64), X, T)
+    assert L1 < 0.1 * L0 and abs(loss - L1) < 0.05 * max(L1, 1e-3)
+
+
+def _small_model():
+    """A model trained on random rows (schedule choice arbitrary but valid)."""
+    rng = np.random.default_rng(5)
+    X = rng.normal(0, 1, (256, M.IN)).astype(np.float32)
+    T = rng.normal(0, 1, 256).astype(np.float32)
+    p, _ = S.mlp_train(S.init_params(1), X, T, steps=50, lr=1e-3)
+    mean = np.zeros(M.IN, np.float32)
+    scale = np.ones(M.IN, np.float32)
+    return p, mean, scale
+
+
+def test_loaded_model_keeps_sssp_exact():
+    p, mean, scale = _small_model()
+    _lib.check("sp_sched_load", _lib.lib().sp_sched_load(p.ctypes.data, mean.ctypes.data, scale.ctypes.data))
+    for g in (G.rmat(13, 16, seed=2, directed=True), G.grid(60, 70)):
+        g.edgeLen = G.hash_weights(g, 9, 1, 100, g.is_symmetric())
+        with DeviceGraph.from_csr(g) as dg:
+            out, _ = dg.sssp(1)
+            assert dg.tune_get("sssp.last_delta") >= 1 and dg.tune_get("sssp.last_ctas") in (1, 2, 4)
+        assert np.array_equal(out, O.sssp(g.indexofNodes, g.edgeList, g.edgeLen, 1))
+
+
+def test_learned_schedule_gain_on_unseen_graphs():
+    if not os.path.exists(S.MODEL_PATH):
+        pytest.skip("no trained model (python -m starplat_b200.scheduler train)")
+    import torch
+
+    held_out = []
+    g = G.rmat(19, 16, seed=77, directed=True)
+    g.edgeLen = G.hash_weights(g, 77, 1, 100, False)
+    held_out.append(("rmat19", g, int(G.pick_sources(g, 1, seed=77)[0])))
+    g = G.grid(1536, 1536)
+    g.edgeLen = G.hash_weights(g, 78, 1, 1000, True)
+    held_out.append(("grid1536", g, 777))
+    g = G.erdos_renyi(1 << 19, 6, seed=79)
+    g.edgeLen = G.hash_weights(g, 79, 1, 100, True)
+    held_out.append(("er19_d6", g, 5))
+    total_fixed = total_learned = 0.0
+    lines = []
+    for name, g, src in held_out:
+        with DeviceGraph.from_csr(g) as dg:
+            dg.set_stream(torch.cuda.current_stream())
+
+            def run():
+                out = torch.empty(g.V, dtype=torch.int32, device="cuda")
+                dg.sssp(src, out=out)
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                best = None
+                for _ in range(3):
+                    a.record()
+                    dg.sssp(src, out=out)
+                    b.record()
+                    torch.cuda.synchronize()
+                    best = a.elapsed_time(b) if best is None else min(best, a.elapsed_time(b))
+                return best, out.cpu().numpy()
+
+            S.unload()
+            t_fixed, d_fixed = run()
+            assert S.load()
+            t_learned, d_learned = run()
+            choice = (dg.tune_get("sssp.last_delta"), dg.tune_get("sssp.last_ctas"))
+        assert np.array_equal(d_fixed, d_learned)
+        total_fixed += t_fixed
+        total_learned += t_learned
+        lines.append(f"{name}: fixed {t_fixed:.2f} ms, learned {t_learned:.2f} ms (delta, ctas = {choice})")
+    print("\n".join(lines) + f"\ntotal: fixed {total_fixed:.2f} ms, learned {total_learned:.2f} ms, "
+          f"gain x{total_fixed / total_learned:.2f}")
+    assert total_learned <= 1.05 * total_fixed
