@@ -246,22 +246,34 @@ def bench_sssp(name, g, src, steps, warmup, stream, hbm, cpu, cpu_mode):
     from starplat_b200 import _lib
     from starplat_b200.device import DeviceGraph
 
+    from starplat_b200 import scheduler as S
+
     out = {"workload": name, "V": g.V, "E": g.E, "source": int(src)}
     with DeviceGraph.from_csr(g) as dg:
         dg.set_stream(stream)
         tuned(dg)
         dist = torch.empty(g.V, dtype=torch.int32, device="cuda")
+        # fixed heuristic schedule (no model), then the learned schedule (model loaded)
+        S.unload()
+        msf, resf = timed(lambda: dg.sssp(src, out=dist), max(1, steps // 2), 1, stream)
+        fixed = {"ms": msf, "rounds": resf[0][1], "delta": dg.tune_get("sssp.last_delta"),
+                 "ctas_per_sm": dg.tune_get("sssp.last_ctas")}
+        d_fixed = dist.cpu().numpy()
+        learned = S.load()
         ms, res = timed(lambda: dg.sssp(src, out=dist), steps, warmup, stream)
         d = dist.cpu().numpy()
         reached = d < INT_MAX
         er = int(np.diff(g.indexofNodes)[reached].sum())
         nr = int(reached.sum())
-        delta = dg.tune_get("sssp.delta")
+        sched = {"learned": learned, "delta": dg.tune_get("sssp.last_delta"),
+                 "ctas_per_sm": dg.tune_get("sssp.last_ctas")}
         msp, resp = timed(lambda: dg.sssp(src, out=dist, variant=_lib.SP_SSSP_PLAIN), 1, 0, stream)
-        same = bool(np.array_equal(dist.cpu().numpy(), d))
+        same = bool(np.array_equal(dist.cpu().numpy(), d) and np.array_equal(d_fixed, d))
+    fixed["value"] = er / (msf / 1e3) / 1e9
     out.update({"value": er / (ms / 1e3) / 1e9, "unit": "GTEPS", "ms": ms, "E_r": er, "reached": nr,
-                "rounds": res[0][1], "delta_knob": delta,
-                "plain": {"value": er / (msp / 1e3) / 1e9, "ms": msp, "rounds": resp[0][1], "same_distances": same},
+                "rounds": res[0][1], "schedule": sched, "fixed_schedule": fixed,
+                "plain": {"value": er / (msp / 1e3) / 1e9, "ms": msp, "rounds": resp[0][1]},
+                "same_distances_all_forms": same,
                 "roofline": roof(12 * er + 12 * g.V, ms, hbm)})
     if cpu:
         from oracle import oracle as O

@@ -39,6 +39,19 @@ def _is_device(a) -> bool:
     return hasattr(a, "is_cuda") and bool(a.is_cuda)
 
 
+_SCHED_TRIED = False
+
+
+def _ensure_scheduler():
+    """Load the trained scheduling model once per process, if it ships with the package."""
+    global _SCHED_TRIED
+    if not _SCHED_TRIED:
+        _SCHED_TRIED = True
+        from . import scheduler
+
+        scheduler.load()
+
+
 class DeviceGraph:
     """A graph resident in GPU memory (the C ABI's sp_graph_h)."""
 
@@ -128,7 +141,9 @@ class DeviceGraph:
 
     def sssp(self, src: int, weight=None, out=None, delta: int = 0, variant: int = _lib.SP_SSSP_DELTA):
         """Exact int32 distances from src (INT_MAX = unreachable). weight: int32[E] in
-        forward-CSR order, host or device; None uses the graph's edgeLen."""
+        forward-CSR order, host or device; None uses the graph's edgeLen. delta <= 0
+        lets the learned scheduler pick the schedule (fixed heuristic without a model)."""
+        _ensure_scheduler()
         if out is None:
             out = np.empty(self.V, np.int32)
         if weight is not None and str(weight.dtype) not in ("int32", "torch.int32"):
