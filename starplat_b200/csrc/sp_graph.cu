@@ -295,8 +295,8 @@ int sp_tune_set(sp_graph_h g, const char* key, int64_t value) {
     return SP_ERR_INVALID;
   }
   if (!strcmp(key, "pr.hot")) {
-    if (value < 0 || value > 56 * 1024) {
-      set_error("sp_tune_set: pr.hot must be in [0, 57344]");
+    if (value < 0 || value > (1 << 22)) {
+      set_error("sp_tune_set: pr.hot must be in [0, 4194304]");
       return SP_ERR_INVALID;
     }
     g->pr_hot = (int32_t)value;
@@ -336,7 +336,7 @@ int sp_tune_get(sp_graph_h g, const char* key, int64_t* value) {
     return SP_ERR_INVALID;
   }
   if (!strcmp(key, "pr.hot")) {
-    *value = g->pr_hot >= 0 ? g->pr_hot : 0;
+    *value = g->pr_hot >= 0 ? g->pr_hot : 40960;
     return SP_OK;
   }
   if (!strcmp(key, "sssp.delta")) {
