@@ -64,8 +64,8 @@ int sp_graph_info(sp_graph_h g, int32_t* V, int64_t* E, int32_t* symmetric);
 /* Schedule knobs (what the autotuner and the learned scheduler set); results never
  * depend on them. Unknown keys: SP_ERR_INVALID.
  *   "pr.hot"  PageRank: source ids (after relabelling by out-degree) gathered in the
- *             L1-resident hot phase of each iteration (0..2^22, default 40960; 0 = one
- *             phase for all sources).
+ *             L1-resident hot phase of each iteration (0..2^22, default 0 = one phase
+ *             for all sources).
  *   "sssp.delta"  SSSP bucket width used when sp_sssp gets delta <= 0 (0 = the largest
  *             edge weight).
  *   "sssp.ctas_per_sm"  SSSP: persistent CTAs per SM of the delta-stepping kernel (1..8,

@@ -336,7 +336,7 @@ int sp_tune_get(sp_graph_h g, const char* key, int64_t* value) {
     return SP_ERR_INVALID;
   }
   if (!strcmp(key, "pr.hot")) {
-    *value = g->pr_hot >= 0 ? g->pr_hot : 40960;
+    *value = g->pr_hot >= 0 ? g->pr_hot : 0;
     return SP_OK;
   }
   if (!strcmp(key, "sssp.delta")) {

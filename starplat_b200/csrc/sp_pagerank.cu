@@ -11,10 +11,11 @@
 //  * Vertices are relabelled by out-degree (descending) once per graph and each
 //    row's in-neighbours are sorted by the new ids, so the sources gathered most
 //    often share cache lines and form a prefix of every row.
-//  * Each iteration runs in two launches split by source id: the HOT phase gathers
-//    only from the first `hot` ids (a block of contrib small enough to stay in L1;
-//    srcList is streamed past L1), the COLD phase gathers the rest and finalises
-//    rows. A row's hot partial sum passes between the phases in FP64.
+//  * Optionally (knob "pr.hot", off by default: measured slower on R-MAT 22) each
+//    iteration runs in two launches split by source id: a HOT phase gathering only
+//    from the first `hot` ids (a block of contrib small enough to stay in L1,
+//    srcList streamed past L1) and a COLD phase gathering the rest and finalising
+//    rows; a row's hot partial sum passes between the phases in FP64.
 //  * Load balance by static bins built once per graph, per phase: 1, 4, 8 or 32
 //    lanes per row segment (<= 4, <= 16, <= 32, <= 2048 edges) with all of a
 //    segment's loads in flight at once; rows above 2048 in-edges are cut into
@@ -41,7 +42,7 @@ constexpr int THREADS = 256;
 constexpr int CIPT = 8;                 // loads in flight per thread in chunk sums
 constexpr int CHUNK = THREADS * CIPT;   // edges per long-row chunk (one round per CTA)
 constexpr int LONG_DEG = 2048;          // rows with more in-edges are processed as chunks
-constexpr int HOT_DEFAULT = 40960;      // source ids of the hot phase (160 KB of contrib)
+constexpr int HOT_DEFAULT = 0;          // one phase: measured fastest on R-MAT 22 (12.0 vs 13.0-13.5 ms)
 constexpr int HOT_MAX = 1 << 22;
 // degree-bin upper bounds for 1, 4, 8 and 32 lanes per row segment
 constexpr int BIN_T1 = 4, BIN_T4 = 16, BIN_T8 = 32;
@@ -638,7 +639,8 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
       const int c = k & 1, n = c ^ 1;
       if (k < 2 && p->n_zero)
         pr::k_zero_rows<<<num_sms() * 2, 256, 0, s>>>(a, p->zrows.p, p->n_zero, p->prb[c].p, p->prb[n].p, p->con[n].p);
-      pr::k_phase<0><<<grid, pr::THREADS, 0, s>>>(a, p->prb[c].p, p->con[c].p, p->prb[n].p, p->con[n].p);
+      if (p->n_tasks[0] || p->n_chunks[0])
+        pr::k_phase<0><<<grid, pr::THREADS, 0, s>>>(a, p->prb[c].p, p->con[c].p, p->prb[n].p, p->con[n].p);
       pr::k_phase<1><<<grid, pr::THREADS, 0, s>>>(a, p->prb[c].p, p->con[c].p, p->prb[n].p, p->con[n].p);
     }
     cudaError_t ce = cudaStreamEndCapture(s, &graph);
@@ -659,7 +661,8 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
     p->exec_stream = s;
   }
   SP_CHECK_CUDA(cudaGraphLaunch(p->exec, s));
-  g_launches.fetch_add((unsigned long long)n_iter * 2 + (p->n_zero ? std::min(2, n_iter) : 0));
+  g_launches.fetch_add((unsigned long long)n_iter * ((p->n_tasks[0] || p->n_chunks[0]) ? 2 : 1) +
+                       (p->n_zero ? std::min(2, n_iter) : 0));
   pr::State hs;
   SP_TRY(copy_out(&hs, p->state.p, sizeof(hs), s));
   if (out) {
