@@ -415,6 +415,48 @@ def bench_louvain(steps, warmup, stream, hbm, cpu):
     return out
 
 
+EXTRAS = ("tc_rmat16", "sssp_rmat23", "sssp_grid4096", "bc_rmat20", "bc_er1000", "louvain_sbm1m")
+
+
+def run_extras(want, args, stream, hbm, cpu_ok):
+    from starplat_b200 import generators as G
+
+    extras = {}
+    ks, kw = max(1, min(args.steps, 5)), 2
+
+    def guarded(name, fn):
+        try:
+            extras[name] = fn()
+        except Exception as e:  # report, keep the headline line
+            extras[name] = {"error": f"{type(e).__name__}: {e}"}
+
+    if "tc_rmat16" in want:
+        guarded("tc_rmat16", lambda: bench_tc(ks, kw, stream, hbm, cpu_ok))
+    if "sssp_rmat23" in want:
+        def _s1():
+            gs = G.rmat(23, 16, seed=1, directed=True)
+            gs.edgeLen = G.hash_weights(gs, 23, 1, 100, False)
+            src = int(G.pick_sources(gs, 1, seed=23)[0])
+            return bench_sssp("sssp rmat23 ef16 directed seed1, w U[1,100]", gs, src, ks, kw, stream, hbm,
+                              cpu_ok, "omp")
+        guarded("sssp_rmat23", _s1)
+    if "sssp_grid4096" in want:
+        def _s2():
+            gg = G.grid(4096, 4096)
+            gg.edgeLen = G.hash_weights(gg, 4096, 1, 1000, True)
+            src = int(np.random.default_rng(4096).integers(0, gg.V))
+            return bench_sssp("sssp grid 4096x4096 4-neighbour, w U[1,1000] symmetric", gg, src, max(1, ks // 2),
+                              1, stream, hbm, cpu_ok, "dijkstra")
+        guarded("sssp_grid4096", _s2)
+    if "bc_rmat20" in want:
+        guarded("bc_rmat20", lambda: bench_bc(max(1, ks // 2), 1, stream, hbm, cpu_ok))
+    if "bc_er1000" in want:
+        guarded("bc_er1000", lambda: bench_bc_er(max(1, ks // 2), 1, stream, hbm, cpu_ok))
+    if "louvain_sbm1m" in want:
+        guarded("louvain_sbm1m", lambda: bench_louvain(max(1, ks // 2), 1, stream, hbm, cpu_ok))
+    return extras
+
+
 # ----------------------------------------------------------------------------- main
 
 def main():
@@ -431,6 +473,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="headline PageRank only")
     ap.add_argument("--scale", type=int, default=PR_SCALE, help="R-MAT scale of the PageRank graph")
     ap.add_argument("--tune", action="append", default=[], help="schedule knob key=value (sp_tune_set)")
+    ap.add_argument("--algo-only", default="", help="run only these extra workloads (comma list), no headline: "
+                                                     "for profiler runs")
     args = ap.parse_args()
     PR_SCALE = args.scale
     args.warmup = max(3, args.warmup)
@@ -466,6 +510,15 @@ def main():
 
     from starplat_b200 import _lib
     from starplat_b200.device import DeviceGraph
+
+    if args.algo_only:
+        for kv in args.tune:
+            k, v = kv.split("=")
+            TUNE.append((k, int(v)))
+        res = run_extras(set(args.algo_only.split(",")), args, torch.cuda.current_stream(), peaks()[0], False)
+        if rank == 0:
+            print(json.dumps({"algo_only": True, "algorithms": res}), flush=True)
+        return
 
     g, gen_s = pr_graph()
     V, E = g.V, g.E
@@ -578,42 +631,8 @@ def main():
     # ---- the other algorithms of the metric
     extras = {}
     if not args.no_extras:
-        from starplat_b200 import generators as G
-
-        want = set(filter(None, args.only.split(","))) or {"tc_rmat16", "sssp_rmat23", "sssp_grid4096", "bc_rmat20",
-                                                           "bc_er1000", "louvain_sbm1m"}
-        ks, kw = max(1, min(args.steps, 5)), 2
-
-        def guarded(name, fn):
-            try:
-                extras[name] = fn()
-            except Exception as e:  # report, keep the headline line
-                extras[name] = {"error": f"{type(e).__name__}: {e}"}
-
-        if "tc_rmat16" in want:
-            guarded("tc_rmat16", lambda: bench_tc(ks, kw, stream, hbm, cpu_ok))
-        if "sssp_rmat23" in want:
-            def _s1():
-                gs = G.rmat(23, 16, seed=1, directed=True)
-                gs.edgeLen = G.hash_weights(gs, 23, 1, 100, False)
-                src = int(G.pick_sources(gs, 1, seed=23)[0])
-                return bench_sssp("sssp rmat23 ef16 directed seed1, w U[1,100]", gs, src, ks, kw, stream, hbm,
-                                  cpu_ok, "omp")
-            guarded("sssp_rmat23", _s1)
-        if "sssp_grid4096" in want:
-            def _s2():
-                gg = G.grid(4096, 4096)
-                gg.edgeLen = G.hash_weights(gg, 4096, 1, 1000, True)
-                src = int(np.random.default_rng(4096).integers(0, gg.V))
-                return bench_sssp("sssp grid 4096x4096 4-neighbour, w U[1,1000] symmetric", gg, src, max(1, ks // 2),
-                                  1, stream, hbm, cpu_ok, "dijkstra")
-            guarded("sssp_grid4096", _s2)
-        if "bc_rmat20" in want:
-            guarded("bc_rmat20", lambda: bench_bc(max(1, ks // 2), 1, stream, hbm, cpu_ok))
-        if "bc_er1000" in want:
-            guarded("bc_er1000", lambda: bench_bc_er(max(1, ks // 2), 1, stream, hbm, cpu_ok))
-        if "louvain_sbm1m" in want:
-            guarded("louvain_sbm1m", lambda: bench_louvain(max(1, ks // 2), 1, stream, hbm, cpu_ok))
+        want = set(filter(None, args.only.split(","))) or set(EXTRAS)
+        extras = run_extras(want, args, stream, hbm, cpu_ok)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
