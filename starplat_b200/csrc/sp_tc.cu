@@ -169,27 +169,17 @@ __global__ void __launch_bounds__(THREADS) k_tc_warp(Lists L, const int32_t* __r
 }
 
 // Small graphs (V <= 65536): the same anchor loop with S(a) as a V-bit bitmap per
-// warp (8 KB) — a lookup is one shared-memory load and a bit test, any |S(a)|
-// fits, and each lane keeps BM_UNROLL probe loads in flight.
+// warp (8 KB) — a lookup is one shared-memory load and a bit test and any |S(a)|
+// fits. Probe lists are long here (about 100 entries on R-MAT 16), so the warp
+// streams them one at a time, coalesced, BM_UNROLL loads in flight per lane.
 constexpr int BM_WARPS = 4;
 constexpr int BM_THREADS = 32 * BM_WARPS;
 constexpr int BM_WORDS = 65536 / 32;
 constexpr int BM_UNROLL = 4;
 
-__device__ __forceinline__ int owner_of(const int* excl, int k) {
-  int lo = 0, hi = 31;
-  while (lo < hi) {
-    int m = (lo + hi + 1) >> 1;
-    if (excl[m] <= k) lo = m; else hi = m - 1;
-  }
-  return lo;
-}
-
 __global__ void __launch_bounds__(BM_THREADS) k_tc_bitmap(Lists L, const int32_t* __restrict__ order,
                                                           unsigned long long* __restrict__ total) {
   __shared__ unsigned s_bm[BM_WARPS][BM_WORDS];
-  __shared__ int s_lb[BM_WARPS][32];
-  __shared__ int s_excl[BM_WARPS][32];
   const int lane = lane_id(), w = warp_id();
   unsigned* bm = s_bm[w];
   for (int i = lane; i < BM_WORDS; i += 32) bm[i] = 0u;
@@ -207,38 +197,30 @@ __global__ void __launch_bounds__(BM_THREADS) k_tc_bitmap(Lists L, const int32_t
       atomicOr(&bm[k >> 5], 1u << (k & 31));
     }
     __syncwarp();
+    // probe lists: bounds of 32 probe vertices per lane load, then the whole warp
+    // streams one list at a time (coalesced, BM_UNROLL loads in flight per lane)
     for (int g0 = 0; g0 < np; g0 += 32) {
       const int p = g0 + lane < np ? L.adj[pb + g0 + lane] : -1;
       int lb = 0, le = 0;
       if (p >= 0) probe_range(L, a, p, lb, le);
-      const int len = le - lb;
-      int incl = len;
+      const int nl = min(32, np - g0);
+      for (int l = 0; l < nl; ++l) {
+        const int b = __shfl_sync(0xffffffffu, lb, l);
+        const int e = __shfl_sync(0xffffffffu, le, l);
+        for (int k0 = b + lane; k0 < e; k0 += 32 * BM_UNROLL) {
+          int x[BM_UNROLL];
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        int t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += t;
-      }
-      const int tot = __shfl_sync(0xffffffffu, incl, 31);
-      s_lb[w][lane] = lb;
-      s_excl[w][lane] = incl - len;
-      __syncwarp();
-      for (int k0 = lane; k0 < tot; k0 += 32 * BM_UNROLL) {
-        int x[BM_UNROLL];
-#pragma unroll
-        for (int u = 0; u < BM_UNROLL; ++u) {
-          const int k = k0 + 32 * u;
-          x[u] = -1;
-          if (k < tot) {
-            const int o = owner_of(s_excl[w], k);
-            x[u] = L.adj[s_lb[w][o] + (k - s_excl[w][o])];
+          for (int u = 0; u < BM_UNROLL; ++u) {
+            const int k = k0 + 32 * u;
+            x[u] = k < e ? __ldg(L.adj + k) : -1;
           }
-        }
 #pragma unroll
-        for (int u = 0; u < BM_UNROLL; ++u)
-          if (x[u] >= 0) cnt += (bm[x[u] >> 5] >> (x[u] & 31)) & 1u;
+          for (int u = 0; u < BM_UNROLL; ++u)
+            if (x[u] >= 0) cnt += (bm[x[u] >> 5] >> (x[u] & 31)) & 1u;
+        }
       }
-      __syncwarp();
     }
+    __syncwarp();
     for (int i = lane; i < ns; i += 32) bm[L.adj[sb + i] >> 5] = 0u;
     __syncwarp();
   }
