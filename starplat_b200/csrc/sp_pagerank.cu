@@ -107,6 +107,7 @@ struct IterArgs {
   double* part;                      // hot-phase partial sums (FP64)
   double* diff_part;                 // [2 * grid] per-CTA diff partials of both phases
   State* st;
+  int two_phase;                     // phase 0 runs; else only diff_part[grid, 2*grid) is written
   Phase ph[2];
   float base;   // (1 - delta) / V, in float as the DSL computes it
   float delta;
@@ -272,7 +273,7 @@ __global__ void __launch_bounds__(THREADS) k_phase(IterArgs a, const float* __re
     __threadfence();
     const volatile double* dp = a.diff_part;
     double p = 0;
-    for (int i = tid; i < 2 * (int)gridDim.x; i += THREADS) p += dp[i];
+    for (int i = (a.two_phase ? 0 : (int)gridDim.x) + tid; i < 2 * (int)gridDim.x; i += THREADS) p += dp[i];
     const double total = block_sum<THREADS>(p, s_red);
     if (tid == 0) {
       const double all = total + *(volatile double*)&a.st->extra;
@@ -622,6 +623,7 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
   a.base = (1.0f - delta) / (float)V;
   a.beta = (double)beta;
   a.max_iter = n_iter;
+  a.two_phase = (p->n_tasks[0] || p->n_chunks[0]) ? 1 : 0;
   int per_sm = 0;
   SP_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pr::k_phase<1>, pr::THREADS, 0));
   const int grid = std::max(1, std::min(num_sms() * 32, num_sms() * std::max(1, per_sm)));
@@ -639,7 +641,7 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
       const int c = k & 1, n = c ^ 1;
       if (k < 2 && p->n_zero)
         pr::k_zero_rows<<<num_sms() * 2, 256, 0, s>>>(a, p->zrows.p, p->n_zero, p->prb[c].p, p->prb[n].p, p->con[n].p);
-      if (p->n_tasks[0] || p->n_chunks[0])
+      if (a.two_phase)
         pr::k_phase<0><<<grid, pr::THREADS, 0, s>>>(a, p->prb[c].p, p->con[c].p, p->prb[n].p, p->con[n].p);
       pr::k_phase<1><<<grid, pr::THREADS, 0, s>>>(a, p->prb[c].p, p->con[c].p, p->prb[n].p, p->con[n].p);
     }
