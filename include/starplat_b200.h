@@ -44,6 +44,14 @@ int sp_version(void);
 const char* sp_last_error(void);
 /* Number of kernels this library has launched in this process (graph nodes count once each). */
 unsigned long long sp_launch_count(void);
+/* Device memory released by this library (graph handles, plans, scratch) is kept in a
+ * per-device cache, at most 1/8 of the device's memory, and reused by later
+ * allocations of a similar size. sp_cache_bytes: bytes held for the current device.
+ * sp_cache_trim: returns every cached block to the driver (like
+ * torch.cuda.empty_cache); an allocation that runs out of memory does the same for
+ * its device before failing. bytes_freed may be NULL. */
+int sp_cache_bytes(int64_t* bytes);
+int sp_cache_trim(int64_t* bytes_freed);
 
 /* ---- device mirror of graph.hpp's CSR (uploaded once, reused by every call) ----
  * Replaces the per-call H2D copy of the generated CUDA code

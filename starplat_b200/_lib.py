@@ -56,6 +56,8 @@ SIGNATURES = {
     "sp_version": (ctypes.c_int, []),
     "sp_last_error": (ctypes.c_char_p, []),
     "sp_launch_count": (ctypes.c_ulonglong, []),
+    "sp_cache_bytes": (ctypes.c_int, [P(i64)]),
+    "sp_cache_trim": (ctypes.c_int, [P(i64)]),
     "sp_graph_create": (ctypes.c_int, [i32, i64, vp, vp, vp, vp, vp, ctypes.c_uint32, P(vp)]),
     "sp_graph_free": (ctypes.c_int, [vp]),
     "sp_graph_set_stream": (ctypes.c_int, [vp, vp]),

@@ -38,6 +38,118 @@ int copy_out(void* dst, const void* src, size_t bytes, cudaStream_t s) {
   return SP_OK;
 }
 
+// ---------------------------------------------------------------- device block cache
+namespace {
+struct Block {
+  void* p;
+  size_t bytes;
+  int device;
+};
+struct BlockCache {
+  std::mutex mu;
+  std::vector<Block> blocks;
+  size_t cached[64] = {};  // bytes held per device
+  size_t cap[64] = {};     // at most 1/8 of the device's memory is held
+};
+// Never destroyed: buffers in static objects may be released during exit.
+BlockCache& cache() {
+  static BlockCache* c = new BlockCache();
+  return *c;
+}
+
+// Frees the cached blocks of one device (all devices when dev < 0); returns the bytes.
+size_t drain(int dev) {
+  BlockCache& c = cache();
+  std::lock_guard<std::mutex> lk(c.mu);
+  int cur = 0;
+  cudaGetDevice(&cur);
+  size_t freed = 0;
+  for (size_t i = 0; i < c.blocks.size();) {
+    const Block b = c.blocks[i];
+    if (dev >= 0 && b.device != dev) {
+      ++i;
+      continue;
+    }
+    if (b.device != cur) cudaSetDevice(b.device);
+    cudaFree(b.p);
+    if (b.device != cur) cudaSetDevice(cur);
+    c.cached[b.device] -= b.bytes;
+    freed += b.bytes;
+    c.blocks[i] = c.blocks.back();
+    c.blocks.pop_back();
+  }
+  return freed;
+}
+}  // namespace
+
+int dev_alloc(void** p, size_t bytes, size_t* got, int* dev) {
+  int d = 0;
+  cudaGetDevice(&d);
+  BlockCache& c = cache();
+  {
+    // best fit among this device's blocks no larger than twice the request (+1 MiB)
+    std::lock_guard<std::mutex> lk(c.mu);
+    int best = -1;
+    for (int i = 0; i < (int)c.blocks.size(); ++i) {
+      const Block& b = c.blocks[i];
+      if (b.device == d && b.bytes >= bytes && b.bytes <= 2 * bytes + (1u << 20) &&
+          (best < 0 || b.bytes < c.blocks[best].bytes))
+        best = i;
+    }
+    if (best >= 0) {
+      const Block b = c.blocks[best];
+      c.blocks[best] = c.blocks.back();
+      c.blocks.pop_back();
+      c.cached[d] -= b.bytes;
+      *p = b.p;
+      *got = b.bytes;
+      *dev = d;
+      return SP_OK;
+    }
+  }
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    drain(d);
+    e = cudaMalloc(p, bytes);
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    set_error("cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? SP_ERR_OOM : SP_ERR_CUDA;
+  }
+  *got = bytes;
+  *dev = d;
+  return SP_OK;
+}
+
+void dev_free(void* p, size_t bytes, int dev) {
+  int cur = 0;
+  cudaGetDevice(&cur);
+  BlockCache& c = cache();
+  if (dev != cur || dev < 0 || dev >= 64) {
+    cudaFree(p);
+    return;
+  }
+  // the same ordering cudaFree gives: work still using the block finishes first
+  if (cudaDeviceSynchronize() != cudaSuccess) {
+    cudaFree(p);
+    return;
+  }
+  std::lock_guard<std::mutex> lk(c.mu);
+  if (!c.cap[dev]) {
+    size_t fr = 0, tot = 0;
+    c.cap[dev] = cudaMemGetInfo(&fr, &tot) == cudaSuccess ? tot / 8 : 0;
+  }
+  if (c.cached[dev] + bytes > c.cap[dev]) {
+    cudaFree(p);
+    return;
+  }
+  c.blocks.push_back({p, bytes, dev});
+  c.cached[dev] += bytes;
+}
+
 // ---------------------------------------------------------------- reverse CSR on device
 __global__ void k_count_in(const int32_t* __restrict__ adj, int64_t E, int32_t* __restrict__ cnt) {
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x)
@@ -67,27 +179,59 @@ __global__ void k_cmp(const int32_t* __restrict__ a, const int32_t* __restrict__
     }
 }
 
-// One warp per vertex: offsets monotone within [0, E], ids in [0, V), adjacency strictly increasing.
-__global__ void k_validate_csr(const int32_t* __restrict__ off, const int32_t* __restrict__ adj, int32_t V,
-                               int64_t E, int* __restrict__ bad, int32_t* __restrict__ maxdeg) {
-  const int lane = threadIdx.x & 31;
-  for (int64_t v = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; v < V;
-       v += ((int64_t)gridDim.x * blockDim.x) >> 5) {
-    int a = off[v], b = off[v + 1];
+// CSR check in two coalesced passes (no warp ever walks a hub row alone).
+// res[0] = flags: 1 offsets not monotone within [0, E] (or off[0] != 0, off[V] != E),
+// 2 an id outside [0, V), 4 a row not strictly increasing (unsorted or duplicate);
+// res[1] = maximum row length.
+// Row pass: offsets, row lengths, and a bit at the first edge of every non-empty row.
+__global__ void k_val_rows(const int32_t* __restrict__ off, int32_t V, int64_t E, uint32_t* __restrict__ starts,
+                           int* __restrict__ res) {
+  int flags = 0, md = 0;
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < V; v += (int64_t)gridDim.x * blockDim.x) {
+    const int a = off[v], b = off[v + 1];
     if (a > b || a < 0 || b > E) {
-      if (lane == 0) atomicOr(bad, 1);
+      flags |= 1;
       continue;
     }
-    if (lane == 0) atomicMax(maxdeg, b - a);
-    int flags = 0;
-    for (int e = a + lane; e < b; e += 32) {
-      int x = adj[e];
-      if (x < 0 || x >= V) flags |= 2;
-      if (e + 1 < b && adj[e + 1] <= x) flags |= 4;  // duplicate or unsorted adjacency
-    }
-    flags = __reduce_or_sync(0xffffffffu, flags);
-    if (lane == 0 && flags) atomicOr(bad, flags);
+    md = max(md, b - a);
+    if (a < b) atomicOr(&starts[a >> 5], 1u << (a & 31));
   }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && (off[0] != 0 || off[V] != E)) flags |= 1;
+  flags = __reduce_or_sync(0xffffffffu, flags);
+  md = __reduce_max_sync(0xffffffffu, md);
+  if ((threadIdx.x & 31) == 0) {
+    if (flags) atomicOr(&res[0], flags);
+    atomicMax(&res[1], md);
+  }
+}
+
+// Edge pass: ids in range; a step down (adj[e+1] <= adj[e]) is allowed only where
+// e+1 starts a row.
+__global__ void k_val_edges(const int32_t* __restrict__ adj, int32_t V, int64_t E,
+                            const uint32_t* __restrict__ starts, int* __restrict__ res) {
+  int flags = 0;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
+    const int x = adj[e];
+    if (x < 0 || x >= V) flags |= 2;
+    if (e + 1 < E && adj[e + 1] <= x && !((starts[(e + 1) >> 5] >> ((e + 1) & 31)) & 1u)) flags |= 4;
+  }
+  flags = __reduce_or_sync(0xffffffffu, flags);
+  if ((threadIdx.x & 31) == 0 && flags) atomicOr(&res[0], flags);
+}
+
+// Checks a CSR on the device; res (2 ints, device) receives the flags and the maximum
+// row length. starts must hold (E + 31) / 32 words.
+static int validate_csr(const int32_t* off, const int32_t* adj, int32_t V, int64_t E, uint32_t* starts, int* res,
+                        cudaStream_t s) {
+  SP_CHECK_CUDA(cudaMemsetAsync(starts, 0, sizeof(uint32_t) * (size_t)((E + 31) / 32 + 1), s));
+  SP_CHECK_CUDA(cudaMemsetAsync(res, 0, 2 * sizeof(int), s));
+  k_val_rows<<<num_sms() * 8, 256, 0, s>>>(off, V, E, starts, res);
+  SP_CHECK_LAUNCH();
+  if (E > 0) {
+    k_val_edges<<<num_sms() * 8, 256, 0, s>>>(adj, V, E, starts, res);
+    SP_CHECK_LAUNCH();
+  }
+  return SP_OK;
 }
 
 int ensure_reverse(sp_graph* g) {
@@ -155,6 +299,25 @@ const char* sp_last_error(void) { return t_err; }
 
 unsigned long long sp_launch_count(void) { return g_launches.load(); }
 
+int sp_cache_bytes(int64_t* bytes) {
+  if (!bytes) {
+    set_error("sp_cache_bytes: NULL output");
+    return SP_ERR_INVALID;
+  }
+  int d = 0;
+  cudaGetDevice(&d);
+  BlockCache& c = cache();
+  std::lock_guard<std::mutex> lk(c.mu);
+  *bytes = (d >= 0 && d < 64) ? (int64_t)c.cached[d] : 0;
+  return SP_OK;
+}
+
+int sp_cache_trim(int64_t* bytes_freed) {
+  const size_t f = drain(-1);
+  if (bytes_freed) *bytes_freed = (int64_t)f;
+  return SP_OK;
+}
+
 int sp_graph_create(int32_t V, int64_t E, const int32_t* indexofNodes, const int32_t* edgeList,
                     const int32_t* edgeLen, const int32_t* rev_indexofNodes, const int32_t* srcList,
                     uint32_t flags, sp_graph_h* out) {
@@ -201,28 +364,6 @@ int sp_graph_create(int32_t V, int64_t E, const int32_t* indexofNodes, const int
     }
     g->has_w = true;
   }
-  // validate: offsets monotone within [0,E], ids in range, adjacency strictly sorted
-  {
-    dbuf<int> bad;
-    dbuf<int32_t> md;
-    if ((st = bad.alloc(2)) || (st = md.alloc(1))) return fail(st);
-    cudaMemsetAsync(bad.p, 0, sizeof(int) * 2, g->stream);
-    cudaMemsetAsync(md.p, 0, sizeof(int32_t), g->stream);
-    k_validate_csr<<<num_sms() * 16, 256, 0, g->stream>>>(g->off.p, g->adj.p, V, E, bad.p, md.p);
-    g_launches++;
-    int h[2] = {0, 0};
-    int32_t hm = 0;
-    if (copy_out(h, bad.p, sizeof(int), g->stream) || copy_out(&hm, md.p, sizeof(int32_t), g->stream)) return fail(SP_ERR_CUDA);
-    int32_t last = 0, first = -1;
-    cudaMemcpy(&last, g->off.p + V, sizeof(int32_t), cudaMemcpyDeviceToHost);
-    cudaMemcpy(&first, g->off.p, sizeof(int32_t), cudaMemcpyDeviceToHost);
-    if (h[0] || last != E || first != 0) {
-      set_error("sp_graph_create: malformed CSR (flags=%d, indexofNodes[0]=%d, indexofNodes[V]=%d, E=%lld)", h[0],
-                first, last, (long long)E);
-      return fail(SP_ERR_INVALID);
-    }
-    g->max_out_deg = hm;
-  }
   if (rev_indexofNodes) {
     if ((st = g->roff.alloc(V + 1)) || (st = g->radj.alloc(E))) return fail(st);
     if (cudaMemcpyAsync(g->roff.p, rev_indexofNodes, sizeof(int32_t) * (V + 1), kind, g->stream) != cudaSuccess ||
@@ -230,22 +371,29 @@ int sp_graph_create(int32_t V, int64_t E, const int32_t* indexofNodes, const int
       set_error("sp_graph_create: copy of reverse CSR failed");
       return fail(SP_ERR_CUDA);
     }
-    dbuf<int> bad;
-    dbuf<int32_t> md;
-    if ((st = bad.alloc(1)) || (st = md.alloc(1))) return fail(st);
-    cudaMemsetAsync(bad.p, 0, sizeof(int), g->stream);
-    k_validate_csr<<<num_sms() * 16, 256, 0, g->stream>>>(g->roff.p, g->radj.p, V, E, bad.p, md.p);
-    g_launches++;
-    int h = 0;
-    int32_t last = -1, first = -1;
-    if (copy_out(&h, bad.p, sizeof(int), g->stream)) return fail(SP_ERR_CUDA);
-    cudaMemcpy(&last, g->roff.p + V, sizeof(int32_t), cudaMemcpyDeviceToHost);
-    cudaMemcpy(&first, g->roff.p, sizeof(int32_t), cudaMemcpyDeviceToHost);
-    if (h || last != E || first != 0) {
-      set_error("sp_graph_create: malformed reverse CSR (flags=%d)", h);
+  }
+  // validate both CSRs: offsets monotone from 0 to E, ids in range, rows strictly increasing
+  {
+    const size_t nw = (size_t)((E + 31) / 32) + 1;
+    dbuf<uint32_t> scratch;
+    if ((st = scratch.alloc(nw + 4))) return fail(st);
+    int* res = (int*)(scratch.p + nw);  // forward {flags, max degree}, reverse {flags, max degree}
+    if ((st = validate_csr(g->off.p, g->adj.p, V, E, scratch.p, res, g->stream))) return fail(st);
+    if (rev_indexofNodes && (st = validate_csr(g->roff.p, g->radj.p, V, E, scratch.p, res + 2, g->stream)))
+      return fail(st);
+    int h[4] = {0, 0, 0, 0};
+    if (copy_out(h, res, sizeof(h), g->stream)) return fail(SP_ERR_CUDA);
+    if (h[0]) {
+      set_error("sp_graph_create: malformed CSR (flags=%d: 1 offsets, 2 ids, 4 unsorted or duplicate row)", h[0]);
       return fail(SP_ERR_INVALID);
     }
-    g->has_rev = true;
+    if (rev_indexofNodes && h[2]) {
+      set_error("sp_graph_create: malformed reverse CSR (flags=%d: 1 offsets, 2 ids, 4 unsorted or duplicate row)",
+                h[2]);
+      return fail(SP_ERR_INVALID);
+    }
+    g->max_out_deg = h[1];
+    g->has_rev = rev_indexofNodes != nullptr;
   }
   if (cudaStreamSynchronize(g->stream) != cudaSuccess) {
     set_error("sp_graph_create: %s", cudaGetErrorString(cudaGetLastError()));

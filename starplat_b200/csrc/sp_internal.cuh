@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <algorithm>
 #include <string>
+#include <vector>
 
 #include "../../include/starplat_b200.h"
 
@@ -42,10 +43,21 @@ extern std::atomic<unsigned long long> g_launches;  // kernels launched by this 
   } while (0)
 
 // ----------------------------------------------------------------- device buffer
+// Device blocks come from a per-process, per-device cache (sp_graph.cu): a released
+// block is kept after a device-wide synchronize (the ordering cudaFree gives) and
+// handed to a later request of similar size, since cudaMalloc of a large block maps
+// fresh pages and cudaFree waits for the device (each 0.2-2 ms of host time).
+// dev_alloc: SP_OK, SP_ERR_OOM or SP_ERR_CUDA (message set); *got = the block's size
+// (at least bytes), *dev = its device.
+int dev_alloc(void** p, size_t bytes, size_t* got, int* dev);
+void dev_free(void* p, size_t bytes, int dev);
+
 template <class T>
 struct dbuf {
   T* p = nullptr;
   size_t n = 0;
+  size_t bytes = 0;
+  int dev = 0;
   dbuf() = default;
   dbuf(const dbuf&) = delete;
   dbuf& operator=(const dbuf&) = delete;
@@ -53,21 +65,59 @@ struct dbuf {
   int alloc(size_t count) {
     if (count <= n && p) return SP_OK;
     release();
-    size_t bytes = (count ? count : 1) * sizeof(T) + 16;  // +16: vector loads may read one int4 past the end
-    cudaError_t e = cudaMalloc(&p, bytes);
-    if (e != cudaSuccess) {
-      p = nullptr;
-      n = 0;
-      set_error("cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
-      return e == cudaErrorMemoryAllocation ? SP_ERR_OOM : SP_ERR_CUDA;
-    }
+    const size_t b = (count ? count : 1) * sizeof(T) + 16;  // +16: vector loads may read one int4 past the end
+    void* q = nullptr;
+    const int st = dev_alloc(&q, b, &bytes, &dev);
+    if (st != SP_OK) return st;
+    p = (T*)q;
     n = count;
     return SP_OK;
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) dev_free(p, bytes, dev);
     p = nullptr;
     n = 0;
+    bytes = 0;
+  }
+};
+
+// A view of device memory owned elsewhere (an Arena).
+template <class T>
+struct dspan {
+  T* p = nullptr;
+  size_t n = 0;
+};
+
+// Many buffers carved from one cudaMalloc. A cudaMalloc/cudaFree pair costs 0.2-0.5 ms
+// of host time for large sizes (cudaFree also waits for the device), so a plan made of
+// dozens of buffers asks for them with want(), then takes them all with one commit().
+// Pieces start on 256-byte boundaries and carry 16 spare bytes (vector loads may read
+// one int4 past the end). A later layout reuses the allocation when it fits.
+struct Arena {
+  dbuf<unsigned char> mem;
+  size_t size = 0;
+  struct Req {
+    void** slot;
+    size_t* n;
+    size_t count, off;
+  };
+  std::vector<Req> reqs;
+  template <class T>
+  void want(dspan<T>& s, size_t count) {
+    const size_t off = (size + 255) & ~(size_t)255;
+    reqs.push_back({(void**)&s.p, &s.n, count, off});
+    size = off + (count ? count : 1) * sizeof(T) + 16;
+  }
+  int commit() {
+    const int st = mem.alloc(size);
+    if (st != SP_OK) return st;
+    for (const Req& r : reqs) {
+      *r.slot = mem.p + r.off;
+      *r.n = r.count;
+    }
+    reqs.clear();
+    size = 0;
+    return SP_OK;
   }
 };
 

@@ -56,32 +56,45 @@ struct State {
   double extra;  // diff terms of rows without in-edges (added by the last CTA)
 };
 
+// Row classes of one phase: bins 0-3 (32, 8, 4, 1 lanes per row segment), 4 = no
+// segment in this phase, 5 = long row (chunks), 6 = no in-edges. Phase 0 puts long
+// and empty rows in class 4.
+constexpr int N_CLASS = 7;
+constexpr int BIN_W[4] = {32, 8, 4, 1};
+
+// A phase's warp tasks are implicit: bin k holds rows[row_base[k], row_base[k+1]) and
+// task t of bin k covers 32 / W_k consecutive rows from row_base[k] + (t - task_base[k]) * (32 / W_k).
 struct Phase {
-  const int32_t* __restrict__ rows;   // binned row ids
-  const int4* __restrict__ tasks;     // warp tasks {W, start, count, 0}
+  const int32_t* __restrict__ rows;   // row ids grouped by class, ascending within a class
   const int4* __restrict__ chunks;    // {row, e_begin, e_end, slot}
   const int32_t* __restrict__ chunk_long;  // long-row index of each chunk
-  int n_tasks;
+  int row_base[5];
+  int task_base[5];                   // task_base[4] = number of warp tasks
   int n_chunks;
 };
 }  // namespace pr
 
 struct PrPlan {
-  dbuf<int32_t> new_id;   // vertex -> rank by out-degree (descending, stable)
-  dbuf<int32_t> od;       // out-degree, in relabelled order
-  dbuf<int32_t> roffp, radjp;  // reverse CSR in relabelled ids, rows sorted
-  dbuf<int32_t> hot_end;  // per row: first edge whose source id >= hot
-  dbuf<float> outbuf;     // result in original vertex order
-  dbuf<int32_t> rows[2], chunk_long[2], zrows;
-  dbuf<int4> tasks[2], chunks[2];
-  int n_tasks[2] = {0, 0}, n_chunks[2] = {0, 0}, n_zero = 0, n_long = 0;
-  dbuf<int2> longs;       // [n_long] {first slot, slot count}
-  dbuf<unsigned int> long_ctr;
-  dbuf<double> chunk_part, part;
-  dbuf<double> diff_part;
-  dbuf<float> prb[2], con[2];
-  dbuf<pr::State> state;
+  Arena graph_mem;        // per graph: relabelled CSR and iteration buffers
+  Arena bin_mem;          // per hot setting: row classes and long-row chunks
+  dspan<int32_t> new_id;  // vertex -> rank by out-degree (descending, stable)
+  dspan<int32_t> od;      // out-degree, in relabelled order
+  dspan<int32_t> roffp, radjp;  // reverse CSR in relabelled ids, rows sorted
+  dspan<int32_t> hot_end; // per row: first edge whose source id >= hot
+  dspan<float> outbuf;    // result in original vertex order
+  dspan<int32_t> rows[2], chunk_long[2];
+  dspan<int4> chunks[2];
+  int row_base[2][5] = {}, task_base[2][5] = {};
+  int n_chunks[2] = {0, 0}, n_zero = 0, n_long = 0;
+  const int32_t* zrows = nullptr;  // rows without in-edges (class 6 of rows[1])
+  dspan<int2> longs;      // [n_long] {first slot, slot count}
+  dspan<unsigned int> long_ctr;
+  dspan<double> chunk_part, part;
+  dspan<double> diff_part;
+  dspan<float> prb[2], con[2];
+  dspan<pr::State> state;
   int hot = -1;           // hot id count the plan was built for
+  bool two_phase() const { return task_base[0][4] > 0 || n_chunks[0] > 0; }
   cudaGraphExec_t exec = nullptr;
   int exec_iters = 0;
   float exec_beta = -1, exec_delta = -1;
@@ -246,13 +259,16 @@ __global__ void __launch_bounds__(THREADS) k_phase(IterArgs a, const float* __re
   }
 
   const int warps_total = gridDim.x * (THREADS / 32);
-  for (int t = blockIdx.x * (THREADS / 32) + (tid >> 5); t < P.n_tasks; t += warps_total) {
-    const int4 task = P.tasks[t];  // {W, start, count, -}
-    switch (task.x) {
-      case 32: my_diff += warp_task<PH, 32, 8>(a, task.y, task.z, lane, pr_old, con_old, pr_new, con_new); break;
-      case 8: my_diff += warp_task<PH, 8, 4>(a, task.y, task.z, lane, pr_old, con_old, pr_new, con_new); break;
-      case 4: my_diff += warp_task<PH, 4, 4>(a, task.y, task.z, lane, pr_old, con_old, pr_new, con_new); break;
-      default: my_diff += warp_task<PH, 1, 4>(a, task.y, task.z, lane, pr_old, con_old, pr_new, con_new); break;
+  for (int t = blockIdx.x * (THREADS / 32) + (tid >> 5); t < P.task_base[4]; t += warps_total) {
+    const int k = (t >= P.task_base[1]) + (t >= P.task_base[2]) + (t >= P.task_base[3]);
+    const int per = 32 >> (k == 0 ? 5 : k == 1 ? 3 : k == 2 ? 2 : 0);  // rows per task: 32 / W
+    const int start = P.row_base[k] + (t - P.task_base[k]) * per;
+    const int count = min(per, P.row_base[k + 1] - start);
+    switch (k) {
+      case 0: my_diff += warp_task<PH, 32, 8>(a, start, count, lane, pr_old, con_old, pr_new, con_new); break;
+      case 1: my_diff += warp_task<PH, 8, 4>(a, start, count, lane, pr_old, con_old, pr_new, con_new); break;
+      case 2: my_diff += warp_task<PH, 4, 4>(a, start, count, lane, pr_old, con_old, pr_new, con_new); break;
+      default: my_diff += warp_task<PH, 1, 4>(a, start, count, lane, pr_old, con_old, pr_new, con_new); break;
     }
   }
 
@@ -325,32 +341,123 @@ __global__ void k_relabel_rows(int V, const int32_t* __restrict__ inv, const int
   }
 }
 
-// new row k <- old row inv[k], ids mapped; rows above 1024 in-edges are left to
-// k_relabel_adj_big (a whole CTA per row) so one warp never walks a hub alone.
-__global__ void k_relabel_adj(int V, const int32_t* __restrict__ inv, const int32_t* __restrict__ new_id,
-                              const int32_t* __restrict__ roff, const int32_t* __restrict__ radj,
-                              const int32_t* __restrict__ roffp, int32_t* __restrict__ radjp, int32_t* big,
-                              int* nbig) {
+// Stable transpose, step 1: the (new dst, new src) pair of every edge, written in
+// ascending new source order (source k is old vertex inv[k]; its pairs start at
+// offp[k]). Sources of more than 1024 out-edges come first (descending out-degree)
+// and are left to k_fwd_pairs_big, a CTA per row, so one warp never walks a hub.
+__global__ void k_fwd_pairs(int V, const int32_t* __restrict__ inv, const int32_t* __restrict__ new_id,
+                            const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
+                            const int32_t* __restrict__ offp, const int32_t* __restrict__ od,
+                            int32_t* __restrict__ dst, int32_t* __restrict__ src) {
   const int lane = threadIdx.x & 31;
   for (int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < V; k += (gridDim.x * blockDim.x) >> 5) {
-    const int v = inv[k];
-    const int b = roff[v], n = roff[v + 1] - b, d = roffp[k];
-    if (n > 1024) {
-      if (lane == 0) big[atomicAdd(nbig, 1)] = k;
-      continue;
+    const int n = od[k];
+    if (n > 1024) continue;
+    const int b = off[inv[k]], d = offp[k];
+    for (int j = lane; j < n; j += 32) {
+      dst[d + j] = new_id[adj[b + j]];
+      src[d + j] = k;
     }
-    for (int j = lane; j < n; j += 32) radjp[d + j] = new_id[radj[b + j]];
   }
 }
 
-__global__ void k_relabel_adj_big(const int32_t* __restrict__ inv, const int32_t* __restrict__ new_id,
-                                  const int32_t* __restrict__ roff, const int32_t* __restrict__ radj,
-                                  const int32_t* __restrict__ roffp, int32_t* __restrict__ radjp,
-                                  const int32_t* __restrict__ big, const int* __restrict__ nbig) {
-  for (int i = blockIdx.x; i < *nbig; i += gridDim.x) {
-    const int k = big[i], v = inv[k];
-    const int b = roff[v], n = roff[v + 1] - b, d = roffp[k];
-    for (int j = threadIdx.x; j < n; j += blockDim.x) radjp[d + j] = new_id[radj[b + j]];
+__global__ void k_fwd_pairs_big(int V, const int32_t* __restrict__ inv, const int32_t* __restrict__ new_id,
+                                const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
+                                const int32_t* __restrict__ offp, const int32_t* __restrict__ od,
+                                int32_t* __restrict__ dst, int32_t* __restrict__ src) {
+  for (int k = blockIdx.x; k < V && od[k] > 1024; k += gridDim.x) {
+    const int n = od[k], b = off[inv[k]], d = offp[k];
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+      dst[d + j] = new_id[adj[b + j]];
+      src[d + j] = k;
+    }
+  }
+}
+
+__device__ __forceinline__ int bin_of(int d) { return d > BIN_T8 ? 0 : d > BIN_T4 ? 1 : d > BIN_T1 ? 2 : 3; }
+
+// Row class per phase (see N_CLASS) and the class sizes; iota[r] = r is the value
+// array of the stable sort that groups rows by class.
+__global__ void k_row_classes(int V, const int32_t* __restrict__ roffp, const int32_t* __restrict__ hot_end,
+                              uint8_t* __restrict__ key0, uint8_t* __restrict__ key1, int32_t* __restrict__ iota,
+                              int* __restrict__ counts /* [2 * N_CLASS] */) {
+  int c0[N_CLASS], c1[N_CLASS];
+#pragma unroll
+  for (int j = 0; j < N_CLASS; ++j) c0[j] = c1[j] = 0;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < V; r += gridDim.x * blockDim.x) {
+    const int b = roffp[r], e = roffp[r + 1], h = hot_end[r];
+    int k0 = 4, k1;
+    if (e == b) {
+      k1 = 6;
+    } else if (e - b > LONG_DEG) {
+      k1 = 5;
+    } else {
+      k0 = h > b ? bin_of(h - b) : 4;
+      k1 = e > h ? bin_of(e - h) : 4;
+    }
+    key0[r] = (uint8_t)k0;
+    key1[r] = (uint8_t)k1;
+    iota[r] = r;
+#pragma unroll
+    for (int j = 0; j < N_CLASS; ++j) {
+      c0[j] += k0 == j;
+      c1[j] += k1 == j;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < N_CLASS; ++j) {
+    const int a = __reduce_add_sync(0xffffffffu, c0[j]), b = __reduce_add_sync(0xffffffffu, c1[j]);
+    if ((threadIdx.x & 31) == 0) {
+      if (a) atomicAdd(&counts[j], a);
+      if (b) atomicAdd(&counts[N_CLASS + j], b);
+    }
+  }
+}
+
+// Chunk counts of each long row's two segments packed as n0 | n1 << 32, so that one
+// exclusive scan gives both phases' chunk offsets (and their sum, the row's first
+// slot). Entry n_long is 0: its prefix is the total.
+__global__ void k_long_counts(int n_long, const int32_t* __restrict__ lrows, const int32_t* __restrict__ roffp,
+                              const int32_t* __restrict__ hot_end, unsigned long long* __restrict__ packed) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= n_long; i += gridDim.x * blockDim.x) {
+    unsigned long long v = 0;
+    if (i < n_long) {
+      const int r = lrows[i];
+      const int b = roffp[r], h = hot_end[r], e = roffp[r + 1];
+      const unsigned long long n0 = (unsigned)(h - b + CHUNK - 1) / CHUNK;
+      const unsigned long long n1 = (unsigned)(e - h + CHUNK - 1) / CHUNK;
+      v = n0 | (n1 << 32);
+    }
+    packed[i] = v;
+  }
+}
+
+// One warp per long row: its chunks in both phases; the row's slots (chunk partial
+// sums, added in slot order when the row is finalised) are its phase-0 chunks, then
+// its phase-1 chunks.
+__global__ void k_long_chunks(int n_long, const int32_t* __restrict__ lrows, const int32_t* __restrict__ roffp,
+                              const int32_t* __restrict__ hot_end, const unsigned long long* __restrict__ pre,
+                              int4* __restrict__ ch0, int32_t* __restrict__ cl0, int4* __restrict__ ch1,
+                              int32_t* __restrict__ cl1, int2* __restrict__ longs) {
+  const int lane = threadIdx.x & 31;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n_long; i += (gridDim.x * blockDim.x) >> 5) {
+    const int r = lrows[i];
+    const int s0 = roffp[r], s1 = hot_end[r], s2 = roffp[r + 1];
+    const unsigned long long p = pre[i], q = pre[i + 1];
+    const int c0 = (int)(p & 0xffffffffull), c1 = (int)(p >> 32);
+    const int n0 = (int)(q & 0xffffffffull) - c0, n1 = (int)(q >> 32) - c1;
+    const int first = c0 + c1;
+    if (lane == 0) longs[i] = make_int2(first, n0 + n1);
+    for (int j = lane; j < n0; j += 32) {
+      const int e = s0 + j * CHUNK;
+      ch0[c0 + j] = make_int4(r, e, min(e + CHUNK, s1), first + j);
+      cl0[c0 + j] = i;
+    }
+    for (int j = lane; j < n1; j += 32) {
+      const int e = s1 + j * CHUNK;
+      ch1[c1 + j] = make_int4(r, e, min(e + CHUNK, s2), first + n0 + j);
+      cl1[c1 + j] = i;
+    }
   }
 }
 
@@ -413,84 +520,86 @@ __global__ void k_plain_init(int V, float* pr) {
 
 }  // namespace pr
 
-// Relabel vertices by out-degree on the device: new_id, od, and the reverse CSR in
-// new ids with every row sorted.
+// Relabel vertices by out-degree (descending, stable) and build the reverse CSR in the
+// new ids with every row ascending, all on the device. The rows come from a stable
+// transpose: the (new dst, new src) pair of every edge, written in ascending source
+// order from the forward CSR and radix-sorted by dst (LSD radix sort keeps equal keys
+// in input order, so each row's sources stay ascending). Also lays out the per-graph
+// iteration buffers.
 static int relabel(sp_graph* g, PrPlan* p) {
   const int V = g->V;
+  const int E = (int)g->E;
   cudaStream_t s = g->stream;
-  SP_TRY(p->new_id.alloc(V));
-  SP_TRY(p->od.alloc(V));
-  SP_TRY(p->roffp.alloc(V + 1));
-  SP_TRY(p->radjp.alloc(g->E));
-  SP_TRY(p->outbuf.alloc(V));
-  dbuf<int32_t> key, id, skey, inv, indeg, big, tmp;
-  dbuf<int> nbig;
-  SP_TRY(key.alloc(V));
-  SP_TRY(id.alloc(V));
-  SP_TRY(skey.alloc(V));
-  SP_TRY(inv.alloc(V));
-  SP_TRY(indeg.alloc(V + 1));
-  SP_TRY(big.alloc(V));
-  SP_TRY(nbig.alloc(1));
+  Arena& A = p->graph_mem;
+  A.want(p->new_id, V);
+  A.want(p->od, V);
+  A.want(p->roffp, (size_t)V + 1);
+  A.want(p->radjp, (size_t)E);
+  A.want(p->outbuf, V);
+  A.want(p->hot_end, V);
+  A.want(p->part, V);
+  A.want(p->diff_part, 2 * (size_t)num_sms() * 32);
+  A.want(p->state, 1);
+  for (int i = 0; i < 2; ++i) {
+    A.want(p->prb[i], V);
+    A.want(p->con[i], V);
+  }
+  SP_TRY(A.commit());
+
+  int bits = 1;
+  while (bits < 31 && (1 << bits) < V) ++bits;
+  size_t t_vsort = 0, t_scan = 0, t_esort = 0;
+  cub::DoubleBuffer<int32_t> nk(nullptr, nullptr), nv(nullptr, nullptr);
+  cub::DeviceRadixSort::SortPairs(nullptr, t_vsort, (const int32_t*)nullptr, (int32_t*)nullptr,
+                                  (const int32_t*)nullptr, (int32_t*)nullptr, V, 0, 32, s);
+  cub::DeviceScan::ExclusiveSum(nullptr, t_scan, (const int32_t*)nullptr, (int32_t*)nullptr, V + 1, s);
+  cub::DeviceRadixSort::SortPairs(nullptr, t_esort, nk, nv, E, 0, bits, s);
+  Arena T;
+  dspan<int32_t> key, id, skey, inv, indeg, offp, dst, dst_alt, src;
+  dspan<unsigned char> temp;
+  T.want(key, V);
+  T.want(id, V);
+  T.want(skey, V);
+  T.want(inv, V);
+  T.want(indeg, (size_t)V + 1);
+  T.want(offp, V);
+  T.want(dst, E);
+  T.want(dst_alt, E);
+  T.want(src, E);
+  T.want(temp, std::max(t_vsort, std::max(t_scan, t_esort)));
+  SP_TRY(T.commit());
+  const size_t tb = temp.n;
+
   const int grid = num_sms() * 8;
   pr::k_deg_keys<<<grid, 256, 0, s>>>(V, g->off.p, key.p, id.p);
   SP_CHECK_LAUNCH();
-  size_t tb = 0;
-  cub::DeviceRadixSort::SortPairs(nullptr, tb, key.p, skey.p, id.p, inv.p, V, 0, 32, s);
-  dbuf<unsigned char> temp;
-  SP_TRY(temp.alloc(tb));
-  cub::DeviceRadixSort::SortPairs(temp.p, tb, key.p, skey.p, id.p, inv.p, V, 0, 32, s);
-  SP_CHECK_LAUNCH();
+  size_t t = tb;
+  SP_CHECK_CUDA(cub::DeviceRadixSort::SortPairs(temp.p, t, key.p, skey.p, id.p, inv.p, V, 0, 32, s));
   SP_CHECK_CUDA(cudaMemsetAsync(indeg.p + V, 0, sizeof(int32_t), s));
   pr::k_relabel_rows<<<grid, 256, 0, s>>>(V, inv.p, skey.p, g->roff.p, p->new_id.p, p->od.p, indeg.p);
   SP_CHECK_LAUNCH();
-  size_t sb = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, sb, indeg.p, p->roffp.p, V + 1, s);
-  SP_TRY(temp.alloc(sb));
-  cub::DeviceScan::ExclusiveSum(temp.p, sb, indeg.p, p->roffp.p, V + 1, s);
+  t = tb;
+  SP_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, t, indeg.p, p->roffp.p, V + 1, s));
+  t = tb;
+  SP_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, t, p->od.p, offp.p, V, s));
+  pr::k_fwd_pairs<<<grid, 256, 0, s>>>(V, inv.p, p->new_id.p, g->off.p, g->adj.p, offp.p, p->od.p, dst.p, src.p);
   SP_CHECK_LAUNCH();
-  SP_CHECK_CUDA(cudaMemsetAsync(nbig.p, 0, sizeof(int), s));
-  SP_TRY(tmp.alloc(g->E));
-  pr::k_relabel_adj<<<grid, 256, 0, s>>>(V, inv.p, p->new_id.p, g->roff.p, g->radj.p, p->roffp.p, tmp.p, big.p, nbig.p);
+  pr::k_fwd_pairs_big<<<num_sms() * 2, 256, 0, s>>>(V, inv.p, p->new_id.p, g->off.p, g->adj.p, offp.p, p->od.p,
+                                                     dst.p, src.p);
   SP_CHECK_LAUNCH();
-  pr::k_relabel_adj_big<<<num_sms() * 2, 256, 0, s>>>(inv.p, p->new_id.p, g->roff.p, g->radj.p, p->roffp.p, tmp.p,
-                                                       big.p, nbig.p);
-  SP_CHECK_LAUNCH();
-  size_t xb = 0;
-  cub::DeviceSegmentedSort::SortKeys(nullptr, xb, tmp.p, p->radjp.p, (int)g->E, V, p->roffp.p, p->roffp.p + 1, s);
-  SP_TRY(temp.alloc(xb));
-  cub::DeviceSegmentedSort::SortKeys(temp.p, xb, tmp.p, p->radjp.p, (int)g->E, V, p->roffp.p, p->roffp.p + 1, s);
-  SP_CHECK_LAUNCH();
+  cub::DoubleBuffer<int32_t> keys(dst.p, dst_alt.p), vals(src.p, p->radjp.p);
+  t = tb;
+  SP_CHECK_CUDA(cub::DeviceRadixSort::SortPairs(temp.p, t, keys, vals, E, 0, bits, s));
+  if (E > 0 && vals.Current() != p->radjp.p)
+    SP_CHECK_CUDA(cudaMemcpyAsync(p->radjp.p, vals.Current(), sizeof(int32_t) * E, cudaMemcpyDeviceToDevice, s));
   SP_CHECK_CUDA(cudaStreamSynchronize(s));
   return SP_OK;
 }
 
-// Bins of one phase: rows whose segment in this phase is non-empty, by its length.
-static void bin_phase(const std::vector<int32_t>& seg_b, const std::vector<int32_t>& seg_e,
-                      const std::vector<char>& is_long, std::vector<int32_t>& rows, std::vector<int4>& tasks) {
-  const int V = (int)seg_b.size();
-  std::vector<int32_t> bin[4];  // W = 32, 8, 4, 1
-  for (int r = 0; r < V; ++r) {
-    if (is_long[r]) continue;
-    const int d = seg_e[r] - seg_b[r];
-    if (d <= 0) continue;
-    if (d > pr::BIN_T8) bin[0].push_back(r);
-    else if (d > pr::BIN_T4) bin[1].push_back(r);
-    else if (d > pr::BIN_T1) bin[2].push_back(r);
-    else bin[3].push_back(r);
-  }
-  const int widths[4] = {32, 8, 4, 1};
-  rows.clear();
-  tasks.clear();
-  for (int k = 0; k < 4; ++k) {
-    const int per = 32 / widths[k];
-    const int base = (int)rows.size();
-    rows.insert(rows.end(), bin[k].begin(), bin[k].end());
-    for (int i = 0; i < (int)bin[k].size(); i += per)
-      tasks.push_back(make_int4(widths[k], base + i, std::min(per, (int)bin[k].size() - i), 0));
-  }
-}
-
+// Row classes and long-row chunks for one hot setting, built on the device: a stable
+// 3-bit radix sort groups each phase's rows by class (ascending ids within a class),
+// and one scan over the long rows places their chunks and chunk-partial slots. The
+// host reads back only the class sizes and the chunk totals.
 static int build_pr_plan(sp_graph* g, int hot) {
   if (g->pr && g->pr->hot == hot) return SP_OK;
   SP_TRY(ensure_reverse(g));
@@ -506,88 +615,103 @@ static int build_pr_plan(sp_graph* g, int hot) {
     g->pr = p;
   }
   cudaStream_t s = g->stream;
-  SP_TRY(p->hot_end.alloc(V));
-  pr::k_hot_end<<<num_sms() * 8, 256, 0, s>>>(V, p->roffp.p, p->radjp.p, hot, p->hot_end.p);
-  SP_CHECK_LAUNCH();
-  std::vector<int32_t> roff(V + 1), hend(V);
-  SP_CHECK_CUDA(cudaMemcpyAsync(roff.data(), p->roffp.p, sizeof(int32_t) * (V + 1), cudaMemcpyDeviceToHost, s));
-  SP_CHECK_CUDA(cudaMemcpyAsync(hend.data(), p->hot_end.p, sizeof(int32_t) * V, cudaMemcpyDeviceToHost, s));
-  SP_CHECK_CUDA(cudaStreamSynchronize(s));
-  // long rows: chunks in both phases, slots contiguous per row
-  std::vector<char> is_long(V, 0);
-  std::vector<int4> chunks[2];
-  std::vector<int32_t> clong[2];
-  std::vector<int2> longs;
-  std::vector<int32_t> zrows;
-  int slots = 0;
-  for (int r = 0; r < V; ++r) {
-    const int d = roff[r + 1] - roff[r];
-    if (d == 0) {
-      zrows.push_back(r);
-      continue;
-    }
-    if (d <= pr::LONG_DEG) continue;
-    is_long[r] = 1;
-    const int first = slots, li = (int)longs.size();
-    const int seg[3] = {roff[r], hend[r], roff[r + 1]};
-    for (int ph = 0; ph < 2; ++ph)
-      for (int e = seg[ph]; e < seg[ph + 1]; e += pr::CHUNK) {
-        chunks[ph].push_back(make_int4(r, e, std::min(e + pr::CHUNK, seg[ph + 1]), slots++));
-        clong[ph].push_back(li);
-      }
-    longs.push_back(make_int2(first, slots - first));
-  }
-  std::vector<int32_t> rows[2];
-  std::vector<int4> tasks[2];
-  {
-    std::vector<int32_t> b0(V), e0(V), b1(V), e1(V);
-    for (int r = 0; r < V; ++r) {
-      b0[r] = roff[r];
-      e0[r] = hend[r];
-      b1[r] = hend[r];
-      e1[r] = roff[r + 1];
-    }
-    bin_phase(b0, e0, is_long, rows[0], tasks[0]);
-    bin_phase(b1, e1, is_long, rows[1], tasks[1]);
-  }
-  const int max_grid = num_sms() * 32;
-  for (int ph = 0; ph < 2; ++ph) {
-    p->n_tasks[ph] = (int)tasks[ph].size();
-    p->n_chunks[ph] = (int)chunks[ph].size();
-    SP_TRY(p->rows[ph].alloc(std::max<size_t>(1, rows[ph].size())));
-    SP_TRY(p->tasks[ph].alloc(std::max(1, p->n_tasks[ph])));
-    SP_TRY(p->chunks[ph].alloc(std::max(1, p->n_chunks[ph])));
-    SP_TRY(p->chunk_long[ph].alloc(std::max(1, p->n_chunks[ph])));
-    if (!rows[ph].empty())
-      SP_CHECK_CUDA(cudaMemcpyAsync(p->rows[ph].p, rows[ph].data(), 4 * rows[ph].size(), cudaMemcpyHostToDevice, s));
-    if (p->n_tasks[ph])
-      SP_CHECK_CUDA(cudaMemcpyAsync(p->tasks[ph].p, tasks[ph].data(), sizeof(int4) * p->n_tasks[ph], cudaMemcpyHostToDevice, s));
-    if (p->n_chunks[ph]) {
-      SP_CHECK_CUDA(cudaMemcpyAsync(p->chunks[ph].p, chunks[ph].data(), sizeof(int4) * p->n_chunks[ph], cudaMemcpyHostToDevice, s));
-      SP_CHECK_CUDA(cudaMemcpyAsync(p->chunk_long[ph].p, clong[ph].data(), 4 * p->n_chunks[ph], cudaMemcpyHostToDevice, s));
-    }
-  }
-  p->n_long = (int)longs.size();
-  p->n_zero = (int)zrows.size();
-  SP_TRY(p->longs.alloc(std::max(1, p->n_long)));
-  SP_TRY(p->long_ctr.alloc(std::max(1, p->n_long)));
-  SP_TRY(p->chunk_part.alloc(std::max(1, slots)));
-  SP_TRY(p->zrows.alloc(std::max(1, p->n_zero)));
-  SP_TRY(p->part.alloc(V));
-  SP_TRY(p->diff_part.alloc(2 * max_grid));
-  SP_TRY(p->state.alloc(1));
-  for (int i = 0; i < 2; ++i) SP_TRY(p->prb[i].alloc(V));
-  for (int i = 0; i < 2; ++i) SP_TRY(p->con[i].alloc(V));
-  if (p->n_long)
-    SP_CHECK_CUDA(cudaMemcpyAsync(p->longs.p, longs.data(), sizeof(int2) * p->n_long, cudaMemcpyHostToDevice, s));
-  if (p->n_zero)
-    SP_CHECK_CUDA(cudaMemcpyAsync(p->zrows.p, zrows.data(), 4 * p->n_zero, cudaMemcpyHostToDevice, s));
-  SP_CHECK_CUDA(cudaMemsetAsync(p->long_ctr.p, 0, sizeof(unsigned int) * std::max(1, p->n_long), s));
-  SP_CHECK_CUDA(cudaStreamSynchronize(s));
-  if (p->exec) {
+  if (p->exec) {  // it refers to the buffers rebuilt below
     cudaGraphExecDestroy(p->exec);
     p->exec = nullptr;
   }
+  p->hot = -1;  // incomplete until the end
+  const int32_t* hend = p->roffp.p;  // hot = 0: every row is all cold
+  if (hot > 0) {
+    pr::k_hot_end<<<num_sms() * 8, 256, 0, s>>>(V, p->roffp.p, p->radjp.p, hot, p->hot_end.p);
+    SP_CHECK_LAUNCH();
+    hend = p->hot_end.p;
+  }
+
+  size_t t_sort = 0, t_scan = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, t_sort, (const uint8_t*)nullptr, (uint8_t*)nullptr,
+                                  (const int32_t*)nullptr, (int32_t*)nullptr, V, 0, 3, s);
+  cub::DeviceScan::ExclusiveSum(nullptr, t_scan, (const unsigned long long*)nullptr, (unsigned long long*)nullptr,
+                                V + 1, s);
+  Arena T;
+  dspan<uint8_t> key0, key1, skey;
+  dspan<int32_t> iota;
+  dspan<int> counts;
+  dspan<unsigned long long> packed, pre;
+  dspan<unsigned char> temp;
+  T.want(key0, V);
+  T.want(key1, V);
+  T.want(skey, V);
+  T.want(iota, V);
+  T.want(counts, 2 * pr::N_CLASS);
+  T.want(packed, (size_t)V + 1);
+  T.want(pre, (size_t)V + 1);
+  T.want(temp, std::max(t_sort, t_scan));
+  SP_TRY(T.commit());
+  const size_t tb = temp.n;
+
+  SP_CHECK_CUDA(cudaMemsetAsync(counts.p, 0, sizeof(int) * 2 * pr::N_CLASS, s));
+  pr::k_row_classes<<<num_sms() * 8, 256, 0, s>>>(V, p->roffp.p, hend, key0.p, key1.p, iota.p, counts.p);
+  SP_CHECK_LAUNCH();
+  int hc[2 * pr::N_CLASS];
+  SP_TRY(copy_out(hc, counts.p, sizeof(hc), s));
+  int n_rows[2] = {0, 0};
+  for (int ph = 0; ph < 2; ++ph) {
+    const int* c = hc + ph * pr::N_CLASS;
+    p->row_base[ph][0] = p->task_base[ph][0] = 0;
+    for (int k = 0; k < 4; ++k) {
+      const int per = 32 / pr::BIN_W[k];
+      p->row_base[ph][k + 1] = p->row_base[ph][k] + c[k];
+      p->task_base[ph][k + 1] = p->task_base[ph][k] + (c[k] + per - 1) / per;
+    }
+    n_rows[ph] = p->row_base[ph][4];
+  }
+  p->n_long = hc[pr::N_CLASS + 5];
+  p->n_zero = hc[pr::N_CLASS + 6];
+  const int long_at = V - p->n_long - p->n_zero;  // classes 5 and 6 sort last
+  // a segment of h edges has at most h / CHUNK + 1 chunks
+  const size_t max_chunks = (size_t)(g->E / pr::CHUNK) + (size_t)p->n_long + 1;
+
+  Arena& B = p->bin_mem;
+  B.want(p->rows[0], n_rows[0] ? V : 1);
+  B.want(p->rows[1], V);
+  for (int ph = 0; ph < 2; ++ph) {
+    B.want(p->chunks[ph], p->n_long ? max_chunks : 1);
+    B.want(p->chunk_long[ph], p->n_long ? max_chunks : 1);
+  }
+  B.want(p->longs, std::max(1, p->n_long));
+  B.want(p->long_ctr, std::max(1, p->n_long));
+  B.want(p->chunk_part, p->n_long ? 2 * max_chunks : 1);
+  SP_TRY(B.commit());
+
+  size_t t = tb;
+  SP_CHECK_CUDA(cub::DeviceRadixSort::SortPairs(temp.p, t, key1.p, skey.p, iota.p, p->rows[1].p, V, 0, 3, s));
+  if (n_rows[0]) {
+    t = tb;
+    SP_CHECK_CUDA(cub::DeviceRadixSort::SortPairs(temp.p, t, key0.p, skey.p, iota.p, p->rows[0].p, V, 0, 3, s));
+  }
+  p->n_chunks[0] = p->n_chunks[1] = 0;
+  if (p->n_long) {
+    const int32_t* lrows = p->rows[1].p + long_at;
+    pr::k_long_counts<<<num_sms() * 2, 256, 0, s>>>(p->n_long, lrows, p->roffp.p, hend, packed.p);
+    SP_CHECK_LAUNCH();
+    t = tb;
+    SP_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, t, packed.p, pre.p, p->n_long + 1, s));
+    unsigned long long tot = 0;
+    SP_TRY(copy_out(&tot, pre.p + p->n_long, sizeof(tot), s));
+    p->n_chunks[0] = (int)(tot & 0xffffffffull);
+    p->n_chunks[1] = (int)(tot >> 32);
+    if ((size_t)p->n_chunks[0] > max_chunks || (size_t)p->n_chunks[1] > max_chunks) {
+      set_error("pagerank plan: %d/%d chunks above the bound %zu", p->n_chunks[0], p->n_chunks[1], max_chunks);
+      return SP_ERR_UNSUPPORTED;
+    }
+    pr::k_long_chunks<<<num_sms() * 2, 256, 0, s>>>(p->n_long, lrows, p->roffp.p, hend, pre.p, p->chunks[0].p,
+                                                     p->chunk_long[0].p, p->chunks[1].p, p->chunk_long[1].p,
+                                                     p->longs.p);
+    SP_CHECK_LAUNCH();
+  }
+  SP_CHECK_CUDA(cudaMemsetAsync(p->long_ctr.p, 0, sizeof(unsigned int) * std::max(1, p->n_long), s));
+  p->zrows = p->rows[1].p + long_at + p->n_long;
+  SP_CHECK_CUDA(cudaStreamSynchronize(s));
   p->hot = hot;
   return SP_OK;
 }
@@ -603,7 +727,7 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
   pr::IterArgs a;
   a.roff = p->roffp.p;
   a.radj = p->radjp.p;
-  a.hot_end = p->hot_end.p;
+  a.hot_end = p->hot > 0 ? p->hot_end.p : p->roffp.p;  // hot = 0: each row's split is its start
   a.od = p->od.p;
   a.longs = p->longs.p;
   a.long_ctr = p->long_ctr.p;
@@ -613,17 +737,19 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
   a.st = p->state.p;
   for (int ph = 0; ph < 2; ++ph) {
     a.ph[ph].rows = p->rows[ph].p;
-    a.ph[ph].tasks = p->tasks[ph].p;
     a.ph[ph].chunks = p->chunks[ph].p;
     a.ph[ph].chunk_long = p->chunk_long[ph].p;
-    a.ph[ph].n_tasks = p->n_tasks[ph];
+    for (int k = 0; k < 5; ++k) {
+      a.ph[ph].row_base[k] = p->row_base[ph][k];
+      a.ph[ph].task_base[k] = p->task_base[ph][k];
+    }
     a.ph[ph].n_chunks = p->n_chunks[ph];
   }
   a.delta = delta;
   a.base = (1.0f - delta) / (float)V;
   a.beta = (double)beta;
   a.max_iter = n_iter;
-  a.two_phase = (p->n_tasks[0] || p->n_chunks[0]) ? 1 : 0;
+  a.two_phase = p->two_phase() ? 1 : 0;
   int per_sm = 0;
   SP_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pr::k_phase<1>, pr::THREADS, 0));
   const int grid = std::max(1, std::min(num_sms() * 32, num_sms() * std::max(1, per_sm)));
@@ -640,7 +766,7 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
     for (int k = 0; k < n_iter; ++k) {
       const int c = k & 1, n = c ^ 1;
       if (k < 2 && p->n_zero)
-        pr::k_zero_rows<<<num_sms() * 2, 256, 0, s>>>(a, p->zrows.p, p->n_zero, p->prb[c].p, p->prb[n].p, p->con[n].p);
+        pr::k_zero_rows<<<num_sms() * 2, 256, 0, s>>>(a, p->zrows, p->n_zero, p->prb[c].p, p->prb[n].p, p->con[n].p);
       if (a.two_phase)
         pr::k_phase<0><<<grid, pr::THREADS, 0, s>>>(a, p->prb[c].p, p->con[c].p, p->prb[n].p, p->con[n].p);
       pr::k_phase<1><<<grid, pr::THREADS, 0, s>>>(a, p->prb[c].p, p->con[c].p, p->prb[n].p, p->con[n].p);
@@ -663,7 +789,7 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
     p->exec_stream = s;
   }
   SP_CHECK_CUDA(cudaGraphLaunch(p->exec, s));
-  g_launches.fetch_add((unsigned long long)n_iter * ((p->n_tasks[0] || p->n_chunks[0]) ? 2 : 1) +
+  g_launches.fetch_add((unsigned long long)n_iter * (p->two_phase() ? 2 : 1) +
                        (p->n_zero ? std::min(2, n_iter) : 0));
   pr::State hs;
   SP_TRY(copy_out(&hs, p->state.p, sizeof(hs), s));

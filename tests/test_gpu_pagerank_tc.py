@@ -178,6 +178,30 @@ def test_invalid_csr_rejected():
     adj = np.array([1, 1], np.int32)  # duplicate
     with pytest.raises(_lib.SPError):
         DeviceGraph(off, adj)
+    bad = [
+        ([0, 3, 3], [0, 1, 0]),  # step down inside a row, next row empty at the same offset
+        ([0, 1, 1], [5]),  # id out of range
+        ([0, 1, 1], [-1]),
+        ([0, 1, 1], [0, 1]),  # indexofNodes[V] != E
+        ([1, 1, 2], [0, 1]),  # indexofNodes[0] != 0
+    ]
+    for o, a in bad:
+        with pytest.raises(_lib.SPError):
+            DeviceGraph(np.array(o, np.int32), np.array(a, np.int32))
+    # steps down only where a row starts (after an empty row too) are fine
+    off = np.array([0, 2, 2, 4], np.int32)
+    adj = np.array([1, 2, 0, 1], np.int32)
+    with DeviceGraph(off, adj) as dg:
+        assert dg.V == 3
+    # a malformed reverse CSR is rejected as well
+    roff = np.array([0, 1, 1, 4], np.int32)
+    radj = np.array([2, 2, 0, 0], np.int32)
+    with pytest.raises(_lib.SPError):
+        DeviceGraph(off, adj, None, roff, radj)
+    roff = np.array([0, 1, 3, 4], np.int32)
+    radj = np.array([2, 0, 2, 0], np.int32)
+    with DeviceGraph(off, adj, None, roff, radj) as dg:
+        assert dg.V == 3
 
 
 def test_tc_large_graph_hash_path():
