@@ -584,7 +584,7 @@ def main():
     alg_bytes = 8 * E + 16 * V
     achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                "traffic": None, "peak_kind": hbm_kind, "kernel": "sp::pr::k_iter",
+                "traffic": None, "peak_kind": hbm_kind, "kernel": "sp::pr::k_phase<1>",
                 "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": per_launch_ms}
     tf = os.path.join(ROOT, "profiles", "pagerank_rmat22_traffic.json")
     if os.path.exists(tf):

@@ -450,6 +450,14 @@ int sp_tune_set(sp_graph_h g, const char* key, int64_t value) {
     g->pr_hot = (int32_t)value;
     return SP_OK;
   }
+  if (!strcmp(key, "pr.order")) {
+    if (value != 0 && value != 1) {
+      set_error("sp_tune_set: pr.order must be 0 or 1");
+      return SP_ERR_INVALID;
+    }
+    g->pr_order = (int32_t)value;
+    return SP_OK;
+  }
   if (!strcmp(key, "sssp.delta")) {
     if (value < 0) {
       set_error("sp_tune_set: sssp.delta must be >= 0");
@@ -485,6 +493,10 @@ int sp_tune_get(sp_graph_h g, const char* key, int64_t* value) {
   }
   if (!strcmp(key, "pr.hot")) {
     *value = g->pr_hot >= 0 ? g->pr_hot : 0;
+    return SP_OK;
+  }
+  if (!strcmp(key, "pr.order")) {
+    *value = g->pr_order >= 0 ? g->pr_order : pr_order_default();
     return SP_OK;
   }
   if (!strcmp(key, "sssp.delta")) {

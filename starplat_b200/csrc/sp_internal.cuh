@@ -149,7 +149,8 @@ struct sp_graph {
   bool has_rev = false;
   int symmetric = -1;      // -1 unknown, 0/1
   int32_t max_out_deg = -1;
-  int32_t pr_hot = -1;  // PageRank: contrib values staged in shared memory (-1 = default)
+  int32_t pr_hot = -1;  // PageRank: source ids of the L1 hot phase (-1 = default)
+  int32_t pr_order = -1;  // PageRank: vertex order of the plan (-1 = default)
   int64_t sssp_delta = 0;  // SSSP bucket width (0 = max edge weight)
   int32_t sssp_ctas_per_sm = 0;  // SSSP persistent CTAs per SM (0 = learned / 4)
   int64_t sssp_last_delta = 0;   // schedule of the last SSSP call (reporting)
@@ -166,6 +167,7 @@ struct sp_graph {
 
 namespace sp {
 int ensure_reverse(sp_graph* g);      // builds roff/radj on device if missing
+int pr_order_default();               // PageRank vertex order default (sp_pagerank.cu)
 int ensure_symmetry(sp_graph* g);     // fills g->symmetric
 int copy_out(void* dst, const void* src, size_t bytes, cudaStream_t s);  // host or device dst
 int num_sms();

@@ -44,6 +44,7 @@ constexpr int CHUNK = THREADS * CIPT;   // edges per long-row chunk (one round p
 constexpr int LONG_DEG = 2048;          // rows with more in-edges are processed as chunks
 constexpr int HOT_DEFAULT = 0;          // one phase: measured fastest on R-MAT 22 (12.0 vs 13.0-13.5 ms)
 constexpr int HOT_MAX = 1 << 22;
+constexpr int ORDER_DEFAULT = 0;        // vertex order: 0 out-degree, 1 in-degree class then out-degree
 // degree-bin upper bounds for 1, 4, 8 and 32 lanes per row segment
 constexpr int BIN_T1 = 4, BIN_T4 = 16, BIN_T8 = 32;
 
@@ -94,12 +95,15 @@ struct PrPlan {
   dspan<float> prb[2], con[2];
   dspan<pr::State> state;
   int hot = -1;           // hot id count the plan was built for
+  int order = 0;          // vertex order (k_deg_keys)
   bool two_phase() const { return task_base[0][4] > 0 || n_chunks[0] > 0; }
   cudaGraphExec_t exec = nullptr;
   int exec_iters = 0;
   float exec_beta = -1, exec_delta = -1;
   cudaStream_t exec_stream = nullptr;
 };
+
+int pr_order_default() { return pr::ORDER_DEFAULT; }
 
 void free_pr_plan(PrPlan* p) {
   if (!p) return;
@@ -152,11 +156,19 @@ __device__ __forceinline__ int ld_src(const int32_t* p) {
   return __ldg(p);
 }
 
+// Where a gather of contrib[u] reads from. Only global memory (through L1) is used:
+// staging the hottest sources in shared memory measured 20-180% slower on R-MAT 22
+// (the carve-out shrinks L1, where those sources already hit, and large tables halve
+// the resident CTAs).
+struct GatherGlobal {
+  const float* __restrict__ con;
+  __device__ __forceinline__ float operator()(int u) const { return __ldg(con + u); }
+};
 // Sum of con[radj[i]] for i in [b, e) by a group of W lanes (sl = lane within the
 // group), U loads in flight per lane per round, reduced with a fixed xor tree.
-template <int PH, int W, int U>
+template <int PH, int W, int U, class G>
 __device__ __forceinline__ double group_row_sum(int b, int e, int sl, const int32_t* __restrict__ radj,
-                                                const float* __restrict__ con) {
+                                                const G& gather) {
   double acc = 0;
   for (int base = b; base < e; base += W * U) {
     int idx[U];
@@ -167,7 +179,7 @@ __device__ __forceinline__ double group_row_sum(int b, int e, int sl, const int3
     }
     float v[U];
 #pragma unroll
-    for (int k = 0; k < U; ++k) v[k] = idx[k] >= 0 ? __ldg(con + idx[k]) : 0.0f;
+    for (int k = 0; k < U; ++k) v[k] = idx[k] >= 0 ? gather(idx[k]) : 0.0f;
 #pragma unroll
     for (int k = 0; k < U; ++k) acc += (double)v[k];
   }
@@ -177,9 +189,9 @@ __device__ __forceinline__ double group_row_sum(int b, int e, int sl, const int3
 }
 
 // One warp task: up to 32/W rows of one bin, W lanes per row segment.
-template <int PH, int W, int U>
+template <int PH, int W, int U, class G>
 __device__ __forceinline__ double warp_task(const IterArgs& a, int start, int count, int lane,
-                                            const float* __restrict__ pr_old, const float* __restrict__ con_old,
+                                            const float* __restrict__ pr_old, const G& gather,
                                             float* __restrict__ pr_new, float* __restrict__ con_new) {
   const int g = lane / W, sl = lane % W;
   int r = -1, b = 0, e = 0, other = 0;
@@ -192,7 +204,7 @@ __device__ __forceinline__ double warp_task(const IterArgs& a, int start, int co
       b = h, e = r1, other = h - r0;  // other > 0: a hot partial is waiting
     }
   }
-  double sum = group_row_sum<PH, W, U>(b, e, sl, a.radj, con_old);
+  double sum = group_row_sum<PH, W, U>(b, e, sl, a.radj, gather);
   if (r < 0 || sl != 0) return 0.0;
   if (PH == 0) {
     if (other > 0) {
@@ -205,15 +217,15 @@ __device__ __forceinline__ double warp_task(const IterArgs& a, int start, int co
   return finalize_row(a, r, sum, pr_old, pr_new, con_new);
 }
 
-// One phase of one iteration. Persistent CTAs of 256 threads: long-row chunks
-// first (CTA each), then the warp tasks, heaviest bins first.
-template <int PH>
-__global__ void __launch_bounds__(THREADS) k_phase(IterArgs a, const float* __restrict__ pr_old,
-                                                   const float* __restrict__ con_old, float* __restrict__ pr_new,
-                                                   float* __restrict__ con_new) {
-  __shared__ double s_red[THREADS / 32];
-  __shared__ int s_last;
-  if (a.st->done) return;
+// One phase of one iteration by persistent CTAs of NT threads: long-row chunks
+// first (a CTA each, CHUNK / NT loads per thread), then the warp tasks, heaviest
+// bins first; then the diff partials (the last CTA of the cold phase sums them).
+template <int PH, int NT, class G>
+__device__ __forceinline__ void phase_body(const IterArgs& a, const G& gather, const float* __restrict__ pr_old,
+                                           float* __restrict__ pr_new, float* __restrict__ con_new, double* s_red,
+                                           int& s_last) {
+  constexpr int CI = CHUNK / NT;
+  static_assert(CI * NT == CHUNK, "chunk must be a multiple of the CTA size");
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const Phase& P = a.ph[PH];
@@ -223,19 +235,19 @@ __global__ void __launch_bounds__(THREADS) k_phase(IterArgs a, const float* __re
     const int4 c = P.chunks[ci];
     double acc = 0;
     {
-      int idx[CIPT];
+      int idx[CI];
 #pragma unroll
-      for (int k = 0; k < CIPT; ++k) {
-        const int e = c.y + tid + k * THREADS;
+      for (int k = 0; k < CI; ++k) {
+        const int e = c.y + tid + k * NT;
         idx[k] = e < c.z ? ld_src<PH>(a.radj + e) : -1;
       }
-      float v[CIPT];
+      float v[CI];
 #pragma unroll
-      for (int k = 0; k < CIPT; ++k) v[k] = idx[k] >= 0 ? __ldg(con_old + idx[k]) : 0.0f;
+      for (int k = 0; k < CI; ++k) v[k] = idx[k] >= 0 ? gather(idx[k]) : 0.0f;
 #pragma unroll
-      for (int k = 0; k < CIPT; ++k) acc += (double)v[k];
+      for (int k = 0; k < CI; ++k) acc += (double)v[k];
     }
-    const double tot = block_sum<THREADS>(acc, s_red);
+    const double tot = block_sum<NT>(acc, s_red);
     if (tid == 0) {
       a.chunk_part[c.w] = tot;
       __threadfence();
@@ -258,21 +270,21 @@ __global__ void __launch_bounds__(THREADS) k_phase(IterArgs a, const float* __re
     __syncthreads();
   }
 
-  const int warps_total = gridDim.x * (THREADS / 32);
-  for (int t = blockIdx.x * (THREADS / 32) + (tid >> 5); t < P.task_base[4]; t += warps_total) {
+  const int warps_total = gridDim.x * (NT / 32);
+  for (int t = blockIdx.x * (NT / 32) + (tid >> 5); t < P.task_base[4]; t += warps_total) {
     const int k = (t >= P.task_base[1]) + (t >= P.task_base[2]) + (t >= P.task_base[3]);
     const int per = 32 >> (k == 0 ? 5 : k == 1 ? 3 : k == 2 ? 2 : 0);  // rows per task: 32 / W
     const int start = P.row_base[k] + (t - P.task_base[k]) * per;
     const int count = min(per, P.row_base[k + 1] - start);
     switch (k) {
-      case 0: my_diff += warp_task<PH, 32, 8>(a, start, count, lane, pr_old, con_old, pr_new, con_new); break;
-      case 1: my_diff += warp_task<PH, 8, 4>(a, start, count, lane, pr_old, con_old, pr_new, con_new); break;
-      case 2: my_diff += warp_task<PH, 4, 4>(a, start, count, lane, pr_old, con_old, pr_new, con_new); break;
-      default: my_diff += warp_task<PH, 1, 4>(a, start, count, lane, pr_old, con_old, pr_new, con_new); break;
+      case 0: my_diff += warp_task<PH, 32, 8>(a, start, count, lane, pr_old, gather, pr_new, con_new); break;
+      case 1: my_diff += warp_task<PH, 8, 4>(a, start, count, lane, pr_old, gather, pr_new, con_new); break;
+      case 2: my_diff += warp_task<PH, 4, 4>(a, start, count, lane, pr_old, gather, pr_new, con_new); break;
+      default: my_diff += warp_task<PH, 1, 4>(a, start, count, lane, pr_old, gather, pr_new, con_new); break;
     }
   }
 
-  const double bd = block_sum<THREADS>(my_diff, s_red);
+  const double bd = block_sum<NT>(my_diff, s_red);
   if (PH == 0) {
     if (tid == 0) a.diff_part[blockIdx.x] = bd;
     return;
@@ -289,8 +301,8 @@ __global__ void __launch_bounds__(THREADS) k_phase(IterArgs a, const float* __re
     __threadfence();
     const volatile double* dp = a.diff_part;
     double p = 0;
-    for (int i = (a.two_phase ? 0 : (int)gridDim.x) + tid; i < 2 * (int)gridDim.x; i += THREADS) p += dp[i];
-    const double total = block_sum<THREADS>(p, s_red);
+    for (int i = (a.two_phase ? 0 : (int)gridDim.x) + tid; i < 2 * (int)gridDim.x; i += NT) p += dp[i];
+    const double total = block_sum<NT>(p, s_red);
     if (tid == 0) {
       const double all = total + *(volatile double*)&a.st->extra;
       const int it = a.st->iter + 1;
@@ -301,6 +313,17 @@ __global__ void __launch_bounds__(THREADS) k_phase(IterArgs a, const float* __re
       a.st->extra = 0.0;
     }
   }
+}
+
+// One phase of one iteration, every gather from global memory (256-thread CTAs).
+template <int PH>
+__global__ void __launch_bounds__(THREADS) k_phase(IterArgs a, const float* __restrict__ pr_old,
+                                                   const float* __restrict__ con_old, float* __restrict__ pr_new,
+                                                   float* __restrict__ con_new) {
+  __shared__ double s_red[THREADS / 32];
+  __shared__ int s_last;
+  if (a.st->done) return;
+  phase_body<PH, THREADS>(a, GatherGlobal{con_old}, pr_old, pr_new, con_new, s_red, s_last);
 }
 
 // Rows without in-edges, iterations 0 and 1 only: pr' = (1-delta)/V. Their diff
@@ -323,36 +346,50 @@ __global__ void k_zero_rows(IterArgs a, const int32_t* __restrict__ zrows, int n
 }
 
 // ---- relabelling by out-degree (descending)
-__global__ void k_deg_keys(int V, const int32_t* __restrict__ off, int32_t* __restrict__ key, int32_t* __restrict__ id) {
+// Relabelling sort keys. Order 0: out-degree, descending. Order 1: in-degree class
+// first (rows of more than LONG_DEG in-edges, then the 32-, 8-, 4- and 1-lane bins,
+// then rows without in-edges), out-degree descending within a class, so that each
+// bin of the single-phase iteration is one contiguous id range.
+__device__ __forceinline__ int indeg_class(int d) {
+  return d > LONG_DEG ? 0 : d > BIN_T8 ? 1 : d > BIN_T4 ? 2 : d > BIN_T1 ? 3 : d > 0 ? 4 : 5;
+}
+
+__global__ void k_deg_keys(int V, int order, const int32_t* __restrict__ off, const int32_t* __restrict__ roff,
+                           int32_t* __restrict__ key, int32_t* __restrict__ id) {
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
-    key[v] = -(off[v + 1] - off[v]);
+    const int od = off[v + 1] - off[v];
+    key[v] = order == 0 ? -od : (indeg_class(roff[v + 1] - roff[v]) << 28) | (0x0fffffff - min(od, 0x0fffffff));
     id[v] = v;
   }
 }
 
-__global__ void k_relabel_rows(int V, const int32_t* __restrict__ inv, const int32_t* __restrict__ skey,
+__global__ void k_relabel_rows(int V, const int32_t* __restrict__ inv, const int32_t* __restrict__ off,
                                const int32_t* __restrict__ roff, int32_t* __restrict__ new_id, int32_t* __restrict__ od,
                                int32_t* __restrict__ indeg) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < V; k += gridDim.x * blockDim.x) {
     const int v = inv[k];
     new_id[v] = k;
-    od[k] = -skey[k];
+    od[k] = off[v + 1] - off[v];
     indeg[k] = roff[v + 1] - roff[v];
   }
 }
 
 // Stable transpose, step 1: the (new dst, new src) pair of every edge, written in
 // ascending new source order (source k is old vertex inv[k]; its pairs start at
-// offp[k]). Sources of more than 1024 out-edges come first (descending out-degree)
-// and are left to k_fwd_pairs_big, a CTA per row, so one warp never walks a hub.
+// offp[k]). Sources of more than 1024 out-edges are listed for k_fwd_pairs_big, a
+// CTA per row, so one warp never walks a hub.
 __global__ void k_fwd_pairs(int V, const int32_t* __restrict__ inv, const int32_t* __restrict__ new_id,
                             const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
                             const int32_t* __restrict__ offp, const int32_t* __restrict__ od,
-                            int32_t* __restrict__ dst, int32_t* __restrict__ src) {
+                            int32_t* __restrict__ dst, int32_t* __restrict__ src, int32_t* __restrict__ big,
+                            int* __restrict__ nbig) {
   const int lane = threadIdx.x & 31;
   for (int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < V; k += (gridDim.x * blockDim.x) >> 5) {
     const int n = od[k];
-    if (n > 1024) continue;
+    if (n > 1024) {
+      if (lane == 0) big[atomicAdd(nbig, 1)] = k;
+      continue;
+    }
     const int b = off[inv[k]], d = offp[k];
     for (int j = lane; j < n; j += 32) {
       dst[d + j] = new_id[adj[b + j]];
@@ -361,11 +398,13 @@ __global__ void k_fwd_pairs(int V, const int32_t* __restrict__ inv, const int32_
   }
 }
 
-__global__ void k_fwd_pairs_big(int V, const int32_t* __restrict__ inv, const int32_t* __restrict__ new_id,
+__global__ void k_fwd_pairs_big(const int32_t* __restrict__ inv, const int32_t* __restrict__ new_id,
                                 const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
                                 const int32_t* __restrict__ offp, const int32_t* __restrict__ od,
-                                int32_t* __restrict__ dst, int32_t* __restrict__ src) {
-  for (int k = blockIdx.x; k < V && od[k] > 1024; k += gridDim.x) {
+                                int32_t* __restrict__ dst, int32_t* __restrict__ src,
+                                const int32_t* __restrict__ big, const int* __restrict__ nbig) {
+  for (int i = blockIdx.x; i < *nbig; i += gridDim.x) {
+    const int k = big[i];
     const int n = od[k], b = off[inv[k]], d = offp[k];
     for (int j = threadIdx.x; j < n; j += blockDim.x) {
       dst[d + j] = new_id[adj[b + j]];
@@ -555,7 +594,8 @@ static int relabel(sp_graph* g, PrPlan* p) {
   cub::DeviceScan::ExclusiveSum(nullptr, t_scan, (const int32_t*)nullptr, (int32_t*)nullptr, V + 1, s);
   cub::DeviceRadixSort::SortPairs(nullptr, t_esort, nk, nv, E, 0, bits, s);
   Arena T;
-  dspan<int32_t> key, id, skey, inv, indeg, offp, dst, dst_alt, src;
+  dspan<int32_t> key, id, skey, inv, indeg, offp, dst, dst_alt, src, big;
+  dspan<int> nbig;
   dspan<unsigned char> temp;
   T.want(key, V);
   T.want(id, V);
@@ -566,26 +606,30 @@ static int relabel(sp_graph* g, PrPlan* p) {
   T.want(dst, E);
   T.want(dst_alt, E);
   T.want(src, E);
+  T.want(big, V);
+  T.want(nbig, 1);
   T.want(temp, std::max(t_vsort, std::max(t_scan, t_esort)));
   SP_TRY(T.commit());
   const size_t tb = temp.n;
 
   const int grid = num_sms() * 8;
-  pr::k_deg_keys<<<grid, 256, 0, s>>>(V, g->off.p, key.p, id.p);
+  pr::k_deg_keys<<<grid, 256, 0, s>>>(V, p->order, g->off.p, g->roff.p, key.p, id.p);
   SP_CHECK_LAUNCH();
   size_t t = tb;
   SP_CHECK_CUDA(cub::DeviceRadixSort::SortPairs(temp.p, t, key.p, skey.p, id.p, inv.p, V, 0, 32, s));
   SP_CHECK_CUDA(cudaMemsetAsync(indeg.p + V, 0, sizeof(int32_t), s));
-  pr::k_relabel_rows<<<grid, 256, 0, s>>>(V, inv.p, skey.p, g->roff.p, p->new_id.p, p->od.p, indeg.p);
+  pr::k_relabel_rows<<<grid, 256, 0, s>>>(V, inv.p, g->off.p, g->roff.p, p->new_id.p, p->od.p, indeg.p);
   SP_CHECK_LAUNCH();
   t = tb;
   SP_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, t, indeg.p, p->roffp.p, V + 1, s));
   t = tb;
   SP_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, t, p->od.p, offp.p, V, s));
-  pr::k_fwd_pairs<<<grid, 256, 0, s>>>(V, inv.p, p->new_id.p, g->off.p, g->adj.p, offp.p, p->od.p, dst.p, src.p);
+  SP_CHECK_CUDA(cudaMemsetAsync(nbig.p, 0, sizeof(int), s));
+  pr::k_fwd_pairs<<<grid, 256, 0, s>>>(V, inv.p, p->new_id.p, g->off.p, g->adj.p, offp.p, p->od.p, dst.p, src.p,
+                                       big.p, nbig.p);
   SP_CHECK_LAUNCH();
-  pr::k_fwd_pairs_big<<<num_sms() * 2, 256, 0, s>>>(V, inv.p, p->new_id.p, g->off.p, g->adj.p, offp.p, p->od.p,
-                                                     dst.p, src.p);
+  pr::k_fwd_pairs_big<<<num_sms() * 2, 256, 0, s>>>(inv.p, p->new_id.p, g->off.p, g->adj.p, offp.p, p->od.p, dst.p,
+                                                     src.p, big.p, nbig.p);
   SP_CHECK_LAUNCH();
   cub::DoubleBuffer<int32_t> keys(dst.p, dst_alt.p), vals(src.p, p->radjp.p);
   t = tb;
@@ -600,13 +644,18 @@ static int relabel(sp_graph* g, PrPlan* p) {
 // 3-bit radix sort groups each phase's rows by class (ascending ids within a class),
 // and one scan over the long rows places their chunks and chunk-partial slots. The
 // host reads back only the class sizes and the chunk totals.
-static int build_pr_plan(sp_graph* g, int hot) {
-  if (g->pr && g->pr->hot == hot) return SP_OK;
+static int build_pr_plan(sp_graph* g, int hot, int order) {
+  if (g->pr && g->pr->hot == hot && g->pr->order == order) return SP_OK;
   SP_TRY(ensure_reverse(g));
   const int V = g->V;
+  if (g->pr && g->pr->order != order) {  // a new vertex order: a new plan
+    free_pr_plan(g->pr);
+    g->pr = nullptr;
+  }
   PrPlan* p = g->pr;
   if (!p) {
     p = new PrPlan();
+    p->order = order;
     int st = relabel(g, p);
     if (st) {
       free_pr_plan(p);
@@ -719,7 +768,8 @@ static int build_pr_plan(sp_graph* g, int hot) {
 static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float* out, int32_t* iters,
                     double* fdiff) {
   const int hot = std::max(0, std::min(g->pr_hot >= 0 ? g->pr_hot : pr::HOT_DEFAULT, pr::HOT_MAX));
-  SP_TRY(build_pr_plan(g, hot));
+  const int order = g->pr_order >= 0 ? g->pr_order : pr::ORDER_DEFAULT;
+  SP_TRY(build_pr_plan(g, hot, order));
   PrPlan* p = g->pr;
   cudaStream_t s = g->stream;
   const int V = g->V;
@@ -753,7 +803,6 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
   int per_sm = 0;
   SP_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pr::k_phase<1>, pr::THREADS, 0));
   const int grid = std::max(1, std::min(num_sms() * 32, num_sms() * std::max(1, per_sm)));
-
   pr::k_init<<<num_sms() * 4, 256, 0, s>>>(V, p->od.p, p->prb[0].p, p->con[0].p, p->state.p);
   SP_CHECK_LAUNCH();
   if (!(p->exec && p->exec_iters == n_iter && p->exec_beta == beta && p->exec_delta == delta && p->exec_stream == s)) {
@@ -791,15 +840,15 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
   SP_CHECK_CUDA(cudaGraphLaunch(p->exec, s));
   g_launches.fetch_add((unsigned long long)n_iter * (p->two_phase() ? 2 : 1) +
                        (p->n_zero ? std::min(2, n_iter) : 0));
-  pr::State hs;
-  SP_TRY(copy_out(&hs, p->state.p, sizeof(hs), s));
+  pr::State st;
+  SP_TRY(copy_out(&st, p->state.p, sizeof(st), s));
   if (out) {
-    pr::k_unpermute<<<num_sms() * 4, 256, 0, s>>>(V, p->new_id.p, p->prb[hs.iter & 1].p, p->outbuf.p);
+    pr::k_unpermute<<<num_sms() * 4, 256, 0, s>>>(V, p->new_id.p, p->prb[st.iter & 1].p, p->outbuf.p);
     SP_CHECK_LAUNCH();
     SP_TRY(copy_out(out, p->outbuf.p, sizeof(float) * V, s));
   }
-  if (iters) *iters = hs.iter;
-  if (fdiff) *fdiff = hs.diff;
+  if (iters) *iters = st.iter;
+  if (fdiff) *fdiff = st.diff;
   return SP_OK;
 }
 

@@ -74,7 +74,7 @@ def test_pagerank_hot_phase_knob(hot):
     _pr_check(g, _lib.SP_PR_TUNED)
 
 
-def test_pagerank_degree_bin_boundaries():
+def _bins_graph():
     from graphs import from_pairs
     # rows on every degree-bin boundary (4/5, 16/17, 32/33, 2048/2049) and multi-chunk hubs
     pairs = []
@@ -84,8 +84,27 @@ def test_pagerank_degree_bin_boundaries():
         pairs.append(np.stack([src, np.full(d, r, np.int32)], 1))
         base += d
     pairs = np.concatenate(pairs + [np.array([[0, 1], [1, 2], [2, 0], [3, 4]], np.int32)])
-    g = from_pairs(base + 5, pairs, name="bins")
-    _pr_check(g, _lib.SP_PR_TUNED)
+    return from_pairs(base + 5, pairs, name="bins")
+
+
+def test_pagerank_degree_bin_boundaries():
+    _pr_check(_bins_graph(), _lib.SP_PR_TUNED)
+
+
+@pytest.mark.parametrize("order", [0, 1])
+def test_pagerank_vertex_order_knob(order):
+    # the vertex order of the plan changes the order of each row's sum, so results
+    # agree with the oracle to the usual tolerance under either order
+    for g in directed_zoo() + undirected_zoo()[:3] + [_bins_graph()]:
+        g.ensure_reverse()
+        dg = device_graph(g)
+        dg.tune_set("pr.order", order)
+        assert dg.tune_get("pr.order") == order
+        _pr_check(g, _lib.SP_PR_TUNED)
+        dg.tune_set("pr.hot", 4096)  # the two-phase split on top of either order
+        _pr_check(g, _lib.SP_PR_TUNED)
+        dg.tune_set("pr.hot", 0)
+        dg.tune_set("pr.order", 0)
 
 
 def test_pagerank_plain_variant():
