@@ -474,6 +474,14 @@ int sp_tune_set(sp_graph_h g, const char* key, int64_t value) {
     g->sssp_ctas_per_sm = (int32_t)value;
     return SP_OK;
   }
+  if (!strcmp(key, "tc.cta_warps")) {
+    if (value != 0 && value != 2 && value != 4 && value != 8 && value != 16) {
+      set_error("sp_tune_set: tc.cta_warps must be 0, 2, 4, 8 or 16");
+      return SP_ERR_INVALID;
+    }
+    g->tc_cta_warps = (int32_t)value;
+    return SP_OK;
+  }
   if (!strcmp(key, "bc.batch")) {
     if (value < 0 || value > 64) {
       set_error("sp_tune_set: bc.batch must be in [0, 64]");
@@ -513,6 +521,10 @@ int sp_tune_get(sp_graph_h g, const char* key, int64_t* value) {
   }
   if (!strcmp(key, "sssp.last_ctas")) {
     *value = g->sssp_last_ctas;
+    return SP_OK;
+  }
+  if (!strcmp(key, "tc.cta_warps")) {
+    *value = g->tc_cta_warps >= 0 ? g->tc_cta_warps : tc_cta_warps_default();
     return SP_OK;
   }
   if (!strcmp(key, "bc.batch")) {

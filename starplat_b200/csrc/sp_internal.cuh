@@ -155,6 +155,7 @@ struct sp_graph {
   int32_t sssp_ctas_per_sm = 0;  // SSSP persistent CTAs per SM (0 = learned / 4)
   int64_t sssp_last_delta = 0;   // schedule of the last SSSP call (reporting)
   int32_t sssp_last_ctas = 0;
+  int32_t tc_cta_warps = -1;  // TC: warps per CTA of the shared-bitmap kernel (-1 = default, 0 = off)
   int32_t bc_batch = 0;    // BC sources per multi-source batch (0 = 64)
   cudaStream_t stream = nullptr;
   bool own_stream = false;
@@ -168,6 +169,7 @@ struct sp_graph {
 namespace sp {
 int ensure_reverse(sp_graph* g);      // builds roff/radj on device if missing
 int pr_order_default();               // PageRank vertex order default (sp_pagerank.cu)
+int tc_cta_warps_default();           // TC kernel choice default (sp_tc.cu)
 int ensure_symmetry(sp_graph* g);     // fills g->symmetric
 int copy_out(void* dst, const void* src, size_t bytes, cudaStream_t s);  // host or device dst
 int num_sms();

@@ -183,6 +183,18 @@ def test_tc_plain_variant():
         assert device_graph(g).tc(variant=_lib.SP_TC_PLAIN) == O.tc(g.indexofNodes, g.edgeList)
 
 
+@pytest.mark.parametrize("cta_warps", [0, 2, 4, 8, 16])
+def test_tc_bitmap_kernel_knob(cta_warps):
+    # per-warp or per-CTA bitmaps: the same exact count
+    graphs = undirected_zoo() + directed_zoo() + [G.rmat(13, 16, seed=7), G.rmat(12, 8, seed=8, directed=True)]
+    for g in graphs:
+        dg = device_graph(g)
+        dg.tune_set("tc.cta_warps", cta_warps)
+        assert dg.tune_get("tc.cta_warps") == cta_warps
+        assert dg.tc() == O.tc(g.indexofNodes, g.edgeList), g.name
+        dg.tune_set("tc.cta_warps", 0)
+
+
 def test_tc_rmat16_config():
     g = G.rmat(16, 16, seed=1)
     assert Compute_TC(g) == O.tc(g.indexofNodes, g.edgeList)
