@@ -160,9 +160,16 @@ int sp_bc_graphs(sp_graph_h g, int32_t ngraphs, const int32_t* vertex_offset, co
  * and aggregation repeat while modularity improves by more than `threshold`
  * (the DSL uses 1e-4). community (may be NULL) gets a dense community id per vertex;
  * *modularity the final Q; levels / sweeps (may be NULL) the number of levels and
- * of local-move sweeps run. */
+ * of local-move sweeps run.
+ * SP_LV_TUNED: degree-binned warp / CTA kernels with shared-memory hash tables.
+ * SP_LV_PLAIN: one thread per vertex, each candidate community's weight found by
+ * rescanning the neighbour list (the O(deg^2) shape of the reference's runnable CUDA
+ * Louvain, communitydetection_sequential_allocation.cu moveNodesKernel). Both use the
+ * same gains and tie-breaks: with integer weights they return the same partition. */
+#define SP_LV_TUNED 0
+#define SP_LV_PLAIN 1
 int sp_louvain(sp_graph_h g, const float* weight, double threshold, int32_t* community, double* modularity,
-               int32_t* levels, int32_t* sweeps);
+               int32_t* levels, int32_t* sweeps, int32_t variant);
 
 /* ---- learned scheduler ----------------------------------------------------------
  * No counterpart in the reference. A small MLP scores candidate schedules (for SSSP:

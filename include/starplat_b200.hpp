@@ -126,7 +126,7 @@ inline auto Compute_CD(graph& g, int* weight) {
     wp = w.data();
   }
   double q = 0;
-  starplat_b200::check(sp_louvain(starplat_b200::mirror(g), wp, 1e-4, nullptr, &q, nullptr, nullptr), "Compute_CD");
+  starplat_b200::check(sp_louvain(starplat_b200::mirror(g), wp, 1e-4, nullptr, &q, nullptr, nullptr, SP_LV_TUNED), "Compute_CD");
   return q;
 }
 

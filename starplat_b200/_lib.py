@@ -31,6 +31,8 @@ SP_SSSP_DELTA = 0
 SP_SSSP_PLAIN = 1
 SP_BC_BATCHED = 0
 SP_BC_PLAIN = 1
+SP_LV_TUNED = 0
+SP_LV_PLAIN = 1
 SP_MLP_IN = 12
 SP_MLP_HIDDEN = 32
 SP_MLP_PARAMS = SP_MLP_HIDDEN * SP_MLP_IN + SP_MLP_HIDDEN * SP_MLP_HIDDEN + 3 * SP_MLP_HIDDEN + 1
@@ -70,7 +72,7 @@ SIGNATURES = {
     "sp_bc": (ctypes.c_int, [vp, vp, i32, vp, i32]),
     "sp_bc_graphs": (ctypes.c_int, [vp, i32, vp, vp, vp, vp]),
     "sp_bfs_sigma": (ctypes.c_int, [vp, vp, i32, vp, vp]),
-    "sp_louvain": (ctypes.c_int, [vp, vp, f64, vp, P(f64), P(i32), P(i32)]),
+    "sp_louvain": (ctypes.c_int, [vp, vp, f64, vp, P(f64), P(i32), P(i32), i32]),
     "sp_mlp_forward": (ctypes.c_int, [vp, vp, i32, vp]),
     "sp_mlp_grad": (ctypes.c_int, [vp, vp, vp, i32, vp, vp]),
     "sp_mlp_train": (ctypes.c_int, [vp, vp, vp, i32, i32, f32, vp]),

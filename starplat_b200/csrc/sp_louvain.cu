@@ -155,6 +155,39 @@ __global__ void __launch_bounds__(THREADS) k_move_warp(MoveArgs a) {
   }
 }
 
+// Plain form (SP_LV_PLAIN): one thread per vertex of the sub-sweep's parity and no
+// tables. Each neighbour community is scored once, at the first neighbour carrying it,
+// and its weight k_{v,c} is found by rescanning the neighbour list: O(deg^2) work per
+// vertex, the shape of the reference's runnable CUDA local move
+// (communitydetection_sequential_allocation.cu, moveNodesKernel). Gains, tie-breaks and
+// the singleton rule are the tuned kernels' own, so with integer weights both forms
+// make the same moves.
+__global__ void k_move_plain(MoveArgs a) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= a.L.n || (int)(hmix((unsigned)v) & 1u) != a.parity) return;
+  const int cv = a.comm[v];
+  const double kv = a.kv[v];
+  const int b = a.L.off[v], e = a.L.off[v + 1];
+  double bg = -INFINITY;
+  int bc = -1;
+  for (int j = b; j < e; ++j) {
+    const int c = a.comm[a.L.adj[j]];
+    bool seen = false;
+    for (int i = b; i < j && !seen; ++i) seen = a.comm[a.L.adj[i]] == c;
+    if (seen) continue;
+    double kc = 0.0;
+    for (int i = b; i < e; ++i)
+      if (a.comm[a.L.adj[i]] == c) kc += a.L.w[i];
+    const double tc = (c == cv) ? a.tot[c] - kv : a.tot[c];
+    const double gain = kc - tc * kv / a.W;
+    if (bc < 0 || better(gain, c, bg, bc, cv)) {
+      bg = gain;
+      bc = c;
+    }
+  }
+  a.newcomm[v] = decide(a, v, cv, kv, bg, bc);
+}
+
 // One CTA per vertex; table in dynamic shared memory (slots = power of two) or,
 // for the big bin, in global scratch at gtab_off[i].
 template <bool GLOBAL_TABLE>
@@ -422,8 +455,15 @@ static int lv_recount(LvPlan* p, int n, cudaStream_t s) {
 }
 
 // One sub-sweep over the vertices of one parity, all degree bins.
-static int lv_subsweep(LvPlan* p, lv::MoveArgs a, const int counts[3], int cap, int parity, cudaStream_t s) {
+static int lv_subsweep(LvPlan* p, lv::MoveArgs a, const int counts[3], int cap, int parity, bool plain,
+                       cudaStream_t s) {
   a.parity = parity;
+  if (plain) {
+    const int tb = 512;  // the generated code's launch shape (backend_cuda/dsl_cpp_generator.cpp:56-77)
+    lv::k_move_plain<<<(a.L.n + tb - 1) / tb, tb, 0, s>>>(a);
+    SP_CHECK_LAUNCH();
+    return SP_OK;
+  }
   const int g = num_sms() * 8;
   if (counts[0]) {
     a.list = p->lists.p;
@@ -454,12 +494,17 @@ static int lv_subsweep(LvPlan* p, lv::MoveArgs a, const int counts[3], int cap, 
 using namespace sp;
 
 extern "C" int sp_louvain(sp_graph_h g, const float* weight, double threshold, int32_t* community, double* modularity,
-                          int32_t* levels_out, int32_t* sweeps_out) {
+                          int32_t* levels_out, int32_t* sweeps_out, int32_t variant) {
   int total_sweeps = 0;
   if (!g || !modularity) {
     set_error("sp_louvain: invalid argument");
     return SP_ERR_INVALID;
   }
+  if (variant != SP_LV_TUNED && variant != SP_LV_PLAIN) {
+    set_error("sp_louvain: unknown variant %d", variant);
+    return SP_ERR_INVALID;
+  }
+  const bool plain = variant == SP_LV_PLAIN;
   if (!g->lv) g->lv = new LvPlan();
   LvPlan* p = g->lv;
   cudaStream_t s = g->stream;
@@ -544,7 +589,7 @@ extern "C" int sp_louvain(sp_graph_h g, const float* weight, double threshold, i
     SP_CHECK_LAUNCH();
     int counts[4];
     SP_TRY(copy_out(counts, p->icnt.p, sizeof(int) * 4, s));
-    if (counts[2]) {
+    if (counts[2] && !plain) {
       // global tables for the highest-degree vertices: 2 * degree slots (power of two)
       std::vector<int32_t> big(counts[2]);
       SP_TRY(copy_out(big.data(), p->lists.p + 2 * (size_t)n0, sizeof(int32_t) * counts[2], s));
@@ -575,7 +620,7 @@ extern "C" int sp_louvain(sp_graph_h g, const float* weight, double threshold, i
     double qold = qlev0, qnew = qlev0;
     for (int sweep = 0; sweep < max_sweeps; ++sweep) {
       for (int parity = 0; parity < 2; ++parity) {
-        SP_TRY(lv_subsweep(p, a, counts, n0, parity, s));
+        SP_TRY(lv_subsweep(p, a, counts, n0, parity, plain, s));
         SP_CHECK_CUDA(cudaMemsetAsync(p->icnt.p + 3, 0, sizeof(int), s));
         lv::k_apply<<<gs, 256, 0, s>>>(n, parity, p->comm.p, p->newcomm.p, p->icnt.p + 3);
         SP_CHECK_LAUNCH();

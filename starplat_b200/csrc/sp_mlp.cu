@@ -184,12 +184,18 @@ __global__ void __launch_bounds__(256) k_train(float* params, const float* __res
 // ---- the loaded scheduling model (process-wide)
 std::mutex g_mu;
 std::vector<float> g_params;   // empty = no model: fixed heuristic
+unsigned g_generation = 0;     // bumped by every sp_sched_load
 std::vector<float> g_mean, g_scale;
 
 }  // namespace mlp
 
 // Score candidate rows X[n][IN] with the loaded model (host in, host out).
 // Returns SP_ERR_UNSUPPORTED when no model is loaded.
+unsigned mlp_generation() {
+  std::lock_guard<std::mutex> lock(mlp::g_mu);
+  return mlp::g_params.empty() ? 0u : mlp::g_generation;
+}
+
 int mlp_score(const std::vector<float>& X, std::vector<float>& y, cudaStream_t s) {
   std::vector<float> params, mean, scale;
   {
@@ -281,6 +287,7 @@ extern "C" int sp_mlp_train(float* params, const float* X, const float* T, int32
 
 extern "C" int sp_sched_load(const float* params, const float* feat_mean, const float* feat_scale) {
   std::lock_guard<std::mutex> lock(mlp::g_mu);
+  ++mlp::g_generation;
   if (!params) {
     mlp::g_params.clear();
     return SP_OK;

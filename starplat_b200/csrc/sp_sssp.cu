@@ -362,6 +362,11 @@ struct SsspPlan {
   dbuf<int> tmp;
   const void* w_src = nullptr;  // weights cached in wbuf came from this pointer
   int w_min = 0, w_max = 0;
+  // the learned choice of the last call: its inputs are the graph and the weight range
+  // only, so it is reused while the range and the loaded model stay the same
+  unsigned sel_gen = 0;
+  int sel_wmin = 0, sel_wmax = 0, sel_ctas = 0;
+  int64_t sel_delta = 0;
 };
 
 void free_sssp_plan(SsspPlan* p) { delete p; }
@@ -397,6 +402,7 @@ static int sssp_prepare(sp_graph* g, const int32_t* weight, const int32_t** wdev
 }
 
 int mlp_score(const std::vector<float>& X, std::vector<float>& y, cudaStream_t s);
+unsigned mlp_generation();  // 0 = no model loaded
 
 // Scheduler inputs (SP_MLP_IN): graph shape and weight range, then the candidate
 // schedule (log2 of the delta multiple of the largest weight, CTAs per SM).
@@ -542,7 +548,14 @@ extern "C" int sp_sssp(sp_graph_h g, const int32_t* weight, int32_t src, int32_t
   int ctas = g->sssp_ctas_per_sm > 0 ? g->sssp_ctas_per_sm : 4;
   const int64_t wmax = std::max<int64_t>(1, (int64_t)g->sssp->w_max);
   if (delta <= 0 && g->sssp_delta > 0) delta = g->sssp_delta;
-  if (delta <= 0 && g->sssp_ctas_per_sm == 0) {
+  SsspPlan* sp_ = g->sssp;
+  const unsigned gen = mlp_generation();
+  if (delta <= 0 && g->sssp_ctas_per_sm == 0 && gen != 0 && sp_->sel_gen == gen && sp_->sel_wmin == sp_->w_min &&
+      sp_->sel_wmax == sp_->w_max) {
+    delta = sp_->sel_delta;  // same inputs as the last scored call
+    ctas = sp_->sel_ctas;
+  }
+  if (delta <= 0 && g->sssp_ctas_per_sm == 0 && gen != 0) {
     // learned schedule: score every candidate, run the best (fixed heuristic if no model)
     static const double mults[] = {1, 2, 4, 8, 16, 32, 64};
     static const int cts[] = {1, 2, 4};
@@ -562,6 +575,11 @@ extern "C" int sp_sssp(sp_graph_h g, const int32_t* weight, int32_t src, int32_t
         if (score[k] < score[best]) best = k;
       delta = (int64_t)std::llround(cand[best].first * (double)wmax);
       ctas = cand[best].second;
+      sp_->sel_gen = gen;
+      sp_->sel_wmin = sp_->w_min;
+      sp_->sel_wmax = sp_->w_max;
+      sp_->sel_delta = delta;
+      sp_->sel_ctas = ctas;
     }
   }
   if (delta <= 0) delta = wmax;

@@ -181,7 +181,7 @@ class DeviceGraph:
         check("sp_bfs_sigma", lib().sp_bfs_sigma(self.handle, _ptr(sources), k, _ptr(lvl), _ptr(sig)))
         return lvl, sig
 
-    def louvain(self, weight=None, threshold: float = 1e-4, community=None):
+    def louvain(self, weight=None, threshold: float = 1e-4, community=None, variant: int = _lib.SP_LV_TUNED):
         """Louvain; returns (modularity, community[V] int32, levels)."""
         if community is None:
             community = np.empty(self.V, np.int32)
@@ -191,6 +191,6 @@ class DeviceGraph:
         lv = ctypes.c_int32()
         sw = ctypes.c_int32()
         check("sp_louvain", lib().sp_louvain(self.handle, _ptr(weight), threshold, _ptr(community), ctypes.byref(q),
-                                             ctypes.byref(lv), ctypes.byref(sw)))
+                                             ctypes.byref(lv), ctypes.byref(sw), variant))
         self.last_louvain_sweeps = int(sw.value)
         return float(q.value), community, int(lv.value)

@@ -94,8 +94,17 @@ def features(dg, mult: float, ctas: int, weight=None) -> np.ndarray:
 
 # ----------------------------------------------------------------------------- model file
 
+def _settle_auto_load() -> None:
+    """An explicit load() or unload() decides: the first DeviceGraph.sssp of the process
+    must not load the shipped model over it afterwards."""
+    from . import device
+
+    device._SCHED_TRIED = True
+
+
 def load(path: str = MODEL_PATH) -> bool:
     """Load the model into the library; False (fixed heuristic stays) if absent."""
+    _settle_auto_load()
     if not os.path.exists(path):
         return False
     d = json.load(open(path))
@@ -109,6 +118,8 @@ def load(path: str = MODEL_PATH) -> bool:
 
 
 def unload() -> None:
+    """Back to the fixed heuristic, also for later calls in this process."""
+    _settle_auto_load()
     check("sp_sched_load", lib().sp_sched_load(None, None, None))
 
 

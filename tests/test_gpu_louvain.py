@@ -85,3 +85,32 @@ def test_louvain_entry_point():
     q = Compute_CD(g)
     qr, _, _ = O.louvain(g.indexofNodes, g.edgeList, None)
     assert abs(q - qr) < 1e-3
+
+
+def _hub_graph():
+    # a star of 9000 leaves over an SBM: the centre reaches the global-table bin
+    # (degree > 8192) and some SBM vertices the CTA bin (degree > 64)
+    g = G.sbm(12000, 12, exponent=2.0, avg_degree=40, p_in=0.8, seed=9)
+    src = np.repeat(np.arange(g.V, dtype=np.int32), np.diff(g.indexofNodes))
+    pairs = np.concatenate([np.stack([src, g.edgeList], 1),
+                            np.stack([np.zeros(9000, np.int32), np.arange(1, 9001, dtype=np.int32)], 1)])
+    return from_pairs(g.V, pairs, symmetrize=True, name="sbm+star")
+
+
+def test_louvain_plain_variant_makes_the_same_moves():
+    # same gains and tie-breaks: with integer weights both forms return one partition
+    from starplat_b200 import _lib
+    for g in (G.sbm(20000, 24, exponent=2.0, avg_degree=32, p_in=0.8, seed=1), G.rmat(12, 8, seed=2),
+              _hub_graph()):
+        dg = device_graph(g)
+        q1, c1, l1 = dg.louvain()
+        q2, c2, l2 = dg.louvain(variant=_lib.SP_LV_PLAIN)
+        assert (q1, l1) == (q2, l2), g.name
+        assert np.array_equal(c1, c2), g.name
+    # float weights: sums in another order, the same bar against the oracle
+    g = G.sbm(8000, 10, seed=4)
+    w = (0.5 + (G.hash_weights(g, 5, 0, 9, True) % 10) * 0.37).astype(np.float32)
+    q, comm, _ = device_graph(g).louvain(w, variant=_lib.SP_LV_PLAIN)
+    qr, _, _ = O.louvain(g.indexofNodes, g.edgeList, w)
+    assert q > qr - 1e-3
+    assert abs(O.modularity(g.indexofNodes, g.edgeList, comm, w) - q) < 1e-9

@@ -74,6 +74,7 @@ def _small_model():
 
 def test_loaded_model_keeps_sssp_exact():
     p, mean, scale = _small_model()
+    S.unload()  # settles the shipped model's lazy load, which would replace this one
     _lib.check("sp_sched_load", _lib.lib().sp_sched_load(p.ctypes.data, mean.ctypes.data, scale.ctypes.data))
     for g in (G.rmat(13, 16, seed=2, directed=True), G.grid(60, 70)):
         g.edgeLen = G.hash_weights(g, 9, 1, 100, g.is_symmetric())
@@ -81,6 +82,63 @@ def test_loaded_model_keeps_sssp_exact():
             out, _ = dg.sssp(1)
             assert dg.tune_get("sssp.last_delta") >= 1 and dg.tune_get("sssp.last_ctas") in (1, 2, 4)
         assert np.array_equal(out, O.sssp(g.indexofNodes, g.edgeList, g.edgeLen, 1))
+
+
+def test_learned_choice_is_reused_only_for_the_same_inputs():
+    # the network's inputs are the graph and the weight range: a second call with the
+    # same range reuses the choice, a new range or a new model scores again, and
+    # without a model the fixed heuristic runs; distances stay exact throughout
+    g = G.rmat(13, 8, seed=4, directed=True)
+    w = G.hash_weights(g, 4, 1, 100, False)
+    ref = O.sssp(g.indexofNodes, g.edgeList, w, 0)
+    p, mean, scale = _small_model()
+    with DeviceGraph.from_csr(g) as dg:
+        S.unload()  # settles the shipped model's lazy load, which would replace this one
+        _lib.check("sp_sched_load", _lib.lib().sp_sched_load(p.ctypes.data, mean.ctypes.data, scale.ctypes.data))
+
+        def run(weights):
+            out, _ = dg.sssp(0, weight=weights)
+            return out, (dg.tune_get("sssp.last_delta"), dg.tune_get("sssp.last_ctas"))
+
+        out1, c1 = run(w)
+        out2, c2 = run(w)
+        assert c1 == c2 and np.array_equal(out1, ref) and np.array_equal(out2, ref)
+        assert c1[0] % int(w.max()) == 0
+        w10 = (w * 10).astype(np.int32)
+        out3, c3 = run(w10)
+        assert c3[0] % int(w10.max()) == 0  # scored again: a multiple of the new largest weight
+        assert np.array_equal(out3, O.sssp(g.indexofNodes, g.edgeList, w10, 0))
+        # another model (negated scores reverse the ranking) must not reuse the old choice
+        q = p.copy()
+        q[-1 - _lib.SP_MLP_HIDDEN:] *= -1
+        _lib.check("sp_sched_load", _lib.lib().sp_sched_load(q.ctypes.data, mean.ctypes.data, scale.ctypes.data))
+        out4, c4 = run(w)
+        assert np.array_equal(out4, ref)
+        S.unload()
+        out5, c5 = run(w)
+        assert c5 == (int(w.max()), 4) and np.array_equal(out5, ref)
+
+
+def test_unload_is_not_undone_by_the_lazy_model_load():
+    # in a fresh process the first sssp call loads the shipped model, unless the caller
+    # already chose: after an explicit unload the fixed heuristic must run
+    import subprocess
+    import sys
+
+    code = (
+        "from starplat_b200 import generators as G, scheduler as S\n"
+        "from starplat_b200.device import DeviceGraph\n"
+        "g = G.rmat(12, 8, seed=3, directed=True)\n"
+        "w = G.hash_weights(g, 3, 1, 100, False)\n"
+        "S.unload()\n"
+        "with DeviceGraph.from_csr(g) as dg:\n"
+        "    dg.sssp(0, weight=w)\n"
+        "    print(dg.tune_get('sssp.last_delta'), dg.tune_get('sssp.last_ctas'), int(w.max()))\n")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    delta, ctas, wmax = map(int, out.stdout.split())
+    assert (delta, ctas) == (wmax, 4)
 
 
 def test_learned_schedule_gain_on_unseen_graphs():
