@@ -527,26 +527,11 @@ def main():
 
     import torch
 
+    from starplat_b200.replicas import Replicas
+
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    rep = Replicas("nccl" if world > 1 else None)
+    barrier, max_over_ranks = rep.barrier, rep.max
 
     from starplat_b200 import _lib
     from starplat_b200.device import DeviceGraph
@@ -558,6 +543,7 @@ def main():
         res = run_extras(set(args.algo_only.split(",")), args, torch.cuda.current_stream(), peaks()[0], False)
         if rank == 0:
             print(json.dumps({"algo_only": True, "algorithms": res}), flush=True)
+        rep.close()
         return
 
     g, gen_s = pr_graph()
@@ -592,14 +578,13 @@ def main():
     clocks = clk.stop()
     launches = _lib.launch_count() - l0
     ms = max_over_ranks(ev0.elapsed_time(ev1))
-    value = world * E * it_total / (ms / 1e3) / 1e9
+    value = rep.sum(E * it_total) / (ms / 1e3) / 1e9  # every rank's edges over the slowest rank's time
     if args.quick:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": "GTEPS", "quick": True, "V": V, "E": E,
                               "iterations": it_total // args.steps, "ms_per_step": ms / args.steps}), flush=True)
         dg.free()
-        if dist is not None:
-            dist.destroy_process_group()
+        rep.close()
         return
 
     hbm, hbm_kind = peaks()
@@ -660,7 +645,7 @@ def main():
         e_it += e2e_step()
     torch.cuda.synchronize()
     e_s = max_over_ranks(time.perf_counter() - t0)
-    e2e = {"value": world * E * e_it / e_s / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": h2d,
+    e2e = {"value": rep.sum(E * e_it) / e_s / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h, "ms_per_step": 1e3 * e_s / e_steps}
 
     cpu_ok = rank == 0 and world == 1 and not args.no_cpu_baseline
@@ -685,8 +670,7 @@ def main():
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
                 "plain": pr_plain, "algorithms": extras}
         print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.destroy_process_group()
+    rep.close()
 
 
 if __name__ == "__main__":
