@@ -64,6 +64,24 @@ int sp_graph_create(int32_t V, int64_t E, const int32_t* indexofNodes, const int
                     const int32_t* edgeLen, const int32_t* rev_indexofNodes, const int32_t* srcList,
                     uint32_t flags, sp_graph_h* out);
 int sp_graph_free(sp_graph_h g);
+/* Builds the device mirror straight from a text edge list, in place of
+ * graph::parseGraph (graph.hpp:464-512 parseEdges, :720-865 parseEdgesContent): one
+ * edge per line "src dst weight"; lines that are empty or do not start with a digit
+ * are skipped; fields are read as std::stringstream reads integers (sign, digits up
+ * to the first other character; a malformed weight reads 0); V = largest id + 1;
+ * duplicate pairs become one edge with the summed weight; self-loops are kept. Where
+ * the reference is undefined: a line without a weight gets weight 1, and a missing,
+ * malformed, negative or out-of-range id is SP_ERR_INVALID naming the line.
+ * Host threads tokenise (nthreads <= 0: all cores); sorting, merging and both CSRs
+ * are built on the device. */
+int sp_graph_load_text(const char* path, int32_t nthreads, sp_graph_h* out);
+/* Copies the mirror's CSR to host buffers, each optional (NULL skips it), sized like
+ * the reference's fields: indexofNodes[V+1], edgeList[E], edgeLen[E],
+ * rev_indexofNodes[V+1], srcList[E], edgeMap[E] (edgeMap[i] = forward index of
+ * reverse entry i, graph.hpp:836-846; built on the first request). V and E come
+ * from sp_graph_info. */
+int sp_graph_export(sp_graph_h g, int32_t* indexofNodes, int32_t* edgeList, int32_t* edgeLen,
+                    int32_t* rev_indexofNodes, int32_t* srcList, int32_t* edgeMap);
 /* Use this CUDA stream (a cudaStream_t) for all later work on g; NULL = the library's own stream. */
 int sp_graph_set_stream(sp_graph_h g, void* cuda_stream);
 /* V, E, symmetric (1 when the forward CSR equals the reverse CSR). */

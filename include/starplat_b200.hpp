@@ -4,9 +4,10 @@
 // type mapping :2875-3050: Graph -> graph&, propNode<T>/propEdge<T> -> T*,
 // node -> int, SetN<g> -> std::set<int>&, a returning DSL function -> auto).
 //
-// Include this header AFTER the reference's graphcode/graph.hpp (it needs the
-// `graph` class and its public CSR fields) in place of the generated .cc file, and
-// link libsp_b200.so. The CSR of each `graph` object is uploaded to the GPU once
+// Include this header in place of the generated .cc file and link libsp_b200.so. The
+// entry points take the reference's `graph` (graphcode/graph.hpp, its public CSR
+// fields) or starplat_b200::Graph (below, read from the text file by the library).
+// The CSR of each `graph` object is uploaded to the GPU once
 // (first call) and reused by later calls; call starplat_b200::invalidate(g) after
 // changing the graph. Errors throw std::runtime_error (define
 // STARPLAT_B200_ABORT_ON_ERROR to print and abort instead).
@@ -87,38 +88,111 @@ inline void invalidate(Graph& g) {
   c.by_graph.erase(it);
 }
 
+// A graph read from a text edge list by the library, in place of the reference's
+// graph + parseGraph (graph.hpp:464-865), whose std::map insertion per line and
+// O(indeg^2) edgeMap loop dominate a driver's run time at scale. Drivers keep their
+// shape: construct with the file path, call parseGraph(), pass the object to the
+// entry points. The device mirror is built during parseGraph() (file format and the
+// few cases the reference leaves undefined: sp_graph_load_text in starplat_b200.h);
+// the public CSR fields are host copies laid out like graph's.
+class Graph {
+ public:
+  int32_t* indexofNodes = nullptr;      // [V + 1]
+  int32_t* edgeList = nullptr;          // [E]
+  int32_t* rev_indexofNodes = nullptr;  // [V + 1]
+  int32_t* srcList = nullptr;           // [E]
+  int32_t* edgeMap = nullptr;           // [E]: forward index of each reverse entry
+
+  explicit Graph(const char* file, int nthreads = 0) : path_(file ? file : ""), nthreads_(nthreads) {}
+  Graph(const Graph&) = delete;
+  Graph& operator=(const Graph&) = delete;
+  ~Graph() { release(); }
+
+  void parseGraph() {
+    release();
+    check(sp_graph_load_text(path_.c_str(), nthreads_, &h_), "parseGraph");
+    int32_t V = 0;
+    int64_t E = 0;
+    check(sp_graph_info(h_, &V, &E, nullptr), "parseGraph");
+    V_ = V;
+    E_ = (int32_t)E;
+    const size_t e = E > 0 ? (size_t)E : 1;
+    indexofNodes = new int32_t[(size_t)V + 1];
+    rev_indexofNodes = new int32_t[(size_t)V + 1];
+    edgeList = new int32_t[e];
+    srcList = new int32_t[e];
+    edgeMap = new int32_t[e];
+    edgeLen_ = new int32_t[e];
+    check(sp_graph_export(h_, indexofNodes, edgeList, edgeLen_, rev_indexofNodes, srcList, edgeMap), "parseGraph");
+  }
+
+  int num_nodes() const { return V_; }
+  int num_edges() const { return E_; }
+  int32_t* getEdgeLen() { return edgeLen_; }
+  sp_graph_h handle() const { return h_; }
+
+ private:
+  void release() {
+    if (h_) sp_graph_free(h_);
+    h_ = nullptr;
+    for (int32_t** a : {&indexofNodes, &edgeList, &rev_indexofNodes, &srcList, &edgeMap, &edgeLen_}) {
+      delete[] * a;
+      *a = nullptr;
+    }
+    V_ = E_ = 0;
+  }
+  std::string path_;
+  int nthreads_ = 0;
+  sp_graph_h h_ = nullptr;
+  int32_t* edgeLen_ = nullptr;
+  int32_t V_ = 0, E_ = 0;
+};
+
+// A Graph carries its own mirror.
+inline sp_graph_h mirror(Graph& g) {
+  if (!g.handle()) check(SP_ERR_INVALID, "starplat_b200::Graph used before parseGraph()");
+  return g.handle();
+}
+inline void invalidate(Graph&) {}
+
 }  // namespace starplat_b200
 
 // ---- the generated entry points ------------------------------------------------
 
-inline auto Compute_TC(graph& g) {
+template <class GraphT>
+inline auto Compute_TC(GraphT& g) {
   int64_t count = 0;
   starplat_b200::check(sp_tc(starplat_b200::mirror(g), &count, SP_TC_TUNED), "Compute_TC");
   return (long)count;
 }
 
-inline void ComputePageRank(graph& g, float beta, float delta, int maxIter, float* pageRank) {
+template <class GraphT>
+inline void ComputePageRank(GraphT& g, float beta, float delta, int maxIter, float* pageRank) {
   starplat_b200::check(sp_pagerank(starplat_b200::mirror(g), beta, delta, maxIter, pageRank, nullptr, nullptr,
                                    SP_PR_TUNED),
                        "ComputePageRank");
 }
 
-inline void Compute_PR(graph& g, float beta, float delta, int maxIter, float* pageRank) {
+template <class GraphT>
+inline void Compute_PR(GraphT& g, float beta, float delta, int maxIter, float* pageRank) {
   ComputePageRank(g, beta, delta, maxIter, pageRank);
 }
 
-inline void Compute_SSSP(graph& g, int* dist, int* weight, int src) {
+template <class GraphT>
+inline void Compute_SSSP(GraphT& g, int* dist, int* weight, int src) {
   starplat_b200::check(sp_sssp(starplat_b200::mirror(g), weight, src, dist, 0, SP_SSSP_DELTA, nullptr), "Compute_SSSP");
 }
 
-inline void Compute_BC(graph& g, float* BC, std::set<int>& sourceSet) {
+template <class GraphT>
+inline void Compute_BC(GraphT& g, float* BC, std::set<int>& sourceSet) {
   std::vector<int32_t> src(sourceSet.begin(), sourceSet.end());
   starplat_b200::check(sp_bc(starplat_b200::mirror(g), src.data(), (int32_t)src.size(), BC, SP_BC_BATCHED),
                        "Compute_BC");
 }
 
 // community_detection takes propEdge<int> weight and returns the modularity.
-inline auto Compute_CD(graph& g, int* weight) {
+template <class GraphT>
+inline auto Compute_CD(GraphT& g, int* weight) {
   std::vector<float> w;
   const float* wp = nullptr;
   if (weight) {

@@ -207,3 +207,81 @@ def ref_parse_graph(path: str):
     L.ref_graph_copy(h, *arrs)
     names = ["indexofNodes", "edgeList", "edgeLen", "rev_indexofNodes", "srcList", "edgeMap"]
     return {k: (a if k in ("indexofNodes", "rev_indexofNodes") else a[:E]) for k, a in zip(names, arrs)}
+
+
+# ----------------------------------------------------------------------------- text edge lists
+
+_WS = " \t\r\v\f"
+
+
+def _read_int(line: str, i: int):
+    """std::stringstream >> int32 at line[i:]: optional sign, digits up to the first other
+    character. Returns (value, next index, status): status 0 ok, 1 no digits, 2 out of
+    range (value saturated)."""
+    j = i
+    neg = False
+    if j < len(line) and line[j] in "+-":
+        neg = line[j] == "-"
+        j += 1
+    k = j
+    while k < len(line) and "0" <= line[k] <= "9":
+        k += 1
+    if k == j:
+        return 0, k, 1
+    x = int(line[j:k])
+    x = -x if neg else x
+    if x > 2**31 - 1 or x < -2**31:
+        return (-2**31 if neg else 2**31 - 1), k, 2
+    return x, k, 0
+
+
+def parse_edgelist(path: str):
+    """graph::parseGraph (graph.hpp:464-512, :720-865) restated for small files: skip lines
+    that are empty or do not start with a digit; "src dst weight" read as stringstream
+    reads int32; V = largest id + 1; duplicate pairs summed (int32 wrap); self-loops kept;
+    rows sorted; edgeMap[i] = forward index of reverse entry i. A line without a weight
+    gets 1 (the reference leaves it uninitialised); an id that is missing, malformed,
+    negative or out of range raises ValueError."""
+    pairs = {}
+    max_id = 0
+    with open(path, "rb") as f:
+        data = f.read().decode("latin-1")
+    for ln, line in enumerate(data.split("\n"), 1):
+        if not line or not ("0" <= line[0] <= "9"):
+            continue
+        s, i, st = _read_int(line, 0)
+        if st:
+            raise ValueError(f"line {ln}: source out of range")
+        while i < len(line) and line[i] in _WS:
+            i += 1
+        d, i, st = _read_int(line, i)
+        if st or d < 0:
+            raise ValueError(f"line {ln}: bad destination")
+        while i < len(line) and line[i] in _WS:
+            i += 1
+        w = 1
+        if i < len(line):
+            w, i, st = _read_int(line, i)
+            if st == 1:
+                w = 0
+        if s == 2**31 - 1 or d == 2**31 - 1:
+            raise ValueError(f"line {ln}: id too large")
+        key = (s, d)
+        pairs[key] = ((pairs.get(key, 0) + w + 2**31) % 2**32) - 2**31
+        max_id = max(max_id, s, d)
+    V = max_id + 1
+    keys = sorted(pairs)
+    E = len(keys)
+    src = np.array([k[0] for k in keys], np.int64).reshape(-1)
+    dst = np.array([k[1] for k in keys], np.int32).reshape(-1)
+    w = np.array([pairs[k] for k in keys], np.int32).reshape(-1)
+    off = np.zeros(V + 1, np.int32)
+    np.add.at(off, src + 1, 1)
+    off = np.cumsum(off).astype(np.int32)
+    order = np.lexsort((src, dst))  # by dst, then src
+    rev_src = src[order].astype(np.int32)
+    roff = np.zeros(V + 1, np.int32)
+    np.add.at(roff, dst.astype(np.int64) + 1, 1)
+    roff = np.cumsum(roff).astype(np.int32)
+    return {"indexofNodes": off, "edgeList": dst, "edgeLen": w, "rev_indexofNodes": roff, "srcList": rev_src,
+            "edgeMap": order.astype(np.int32)}

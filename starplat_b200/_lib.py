@@ -62,6 +62,8 @@ SIGNATURES = {
     "sp_cache_trim": (ctypes.c_int, [P(i64)]),
     "sp_graph_create": (ctypes.c_int, [i32, i64, vp, vp, vp, vp, vp, ctypes.c_uint32, P(vp)]),
     "sp_graph_free": (ctypes.c_int, [vp]),
+    "sp_graph_load_text": (ctypes.c_int, [ctypes.c_char_p, i32, P(vp)]),
+    "sp_graph_export": (ctypes.c_int, [vp, vp, vp, vp, vp, vp, vp]),
     "sp_graph_set_stream": (ctypes.c_int, [vp, vp]),
     "sp_graph_info": (ctypes.c_int, [vp, P(i32), P(i64), P(i32)]),
     "sp_tune_set": (ctypes.c_int, [vp, ctypes.c_char_p, i64]),

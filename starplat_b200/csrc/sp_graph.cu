@@ -151,22 +151,49 @@ void dev_free(void* p, size_t bytes, int dev) {
 }
 
 // ---------------------------------------------------------------- reverse CSR on device
-__global__ void k_count_in(const int32_t* __restrict__ adj, int64_t E, int32_t* __restrict__ cnt) {
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x)
-    atomicAdd(&cnt[adj[e]], 1);
+// Row of every CSR entry: each thread takes 32 consecutive entries, finds the row of
+// the first by binary search over the offsets and walks forward (empty rows and hub
+// rows cost nothing extra).
+__global__ void k_row_of(int32_t V, int64_t E, const int32_t* __restrict__ off, int32_t* __restrict__ row) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x * 32;
+  for (int64_t e0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) * 32; e0 < E; e0 += stride) {
+    int lo = 0, hi = V;  // last v with off[v] <= e0
+    while (lo < hi) {
+      const int m = (lo + hi + 1) >> 1;
+      if (off[m] <= e0) lo = m; else hi = m - 1;
+    }
+    int r = lo;
+    const int64_t e1 = e0 + 32 < E ? e0 + 32 : E;
+    for (int64_t e = e0; e < e1; ++e) {
+      while (off[r + 1] <= e) ++r;
+      row[e] = r;
+    }
+  }
 }
 
-__global__ void k_scatter_rev(const int32_t* __restrict__ off, const int32_t* __restrict__ adj, int32_t V,
-                              int32_t* __restrict__ cursor, int32_t* __restrict__ radj) {
-  // one warp per source vertex
-  int lane = threadIdx.x & 31;
-  for (int64_t u = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; u < V;
-       u += ((int64_t)gridDim.x * blockDim.x) >> 5) {
-    for (int e = off[u] + lane; e < off[u + 1]; e += 32) {
-      int v = adj[e];
-      int p = atomicAdd(&cursor[v], 1);
-      radj[p] = (int32_t)u;
+// off[v] = first index whose sorted key is >= v, for v = 0..V.
+__global__ void k_offsets_of_sorted(int32_t V, int64_t E, const int32_t* __restrict__ keys, int32_t* __restrict__ off) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v <= V; v += (int64_t)gridDim.x * blockDim.x) {
+    int64_t lo = 0, hi = E;
+    while (lo < hi) {
+      const int64_t m = (lo + hi) >> 1;
+      if (keys[m] < v) lo = m + 1; else hi = m;
     }
+    off[v] = (int32_t)lo;
+  }
+}
+
+// edgeMap: reverse entry i (row r, source u) -> index of r in u's forward row.
+__global__ void k_emap(int32_t V, int64_t E, const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
+                       const int32_t* __restrict__ rrow, const int32_t* __restrict__ radj, int32_t* __restrict__ emap) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < E; i += (int64_t)gridDim.x * blockDim.x) {
+    const int r = rrow[i], u = radj[i];
+    int lo = off[u], hi = off[u + 1];
+    while (lo < hi) {
+      const int m = (lo + hi) >> 1;
+      if (adj[m] < r) lo = m + 1; else hi = m;
+    }
+    emap[i] = lo;
   }
 }
 
@@ -234,38 +261,64 @@ static int validate_csr(const int32_t* off, const int32_t* adj, int32_t V, int64
   return SP_OK;
 }
 
+// Reverse CSR by a stable transpose: (dst, src) of every forward entry, in forward
+// order (ascending src), radix-sorted by dst; a stable sort keeps each row's sources
+// ascending, as graph.hpp:825-832 sorts srcList per vertex.
 int ensure_reverse(sp_graph* g) {
   if (g->has_rev) return SP_OK;
   cudaStream_t s = g->stream;
-  SP_TRY(g->roff.alloc(g->V + 1));
-  SP_TRY(g->radj.alloc(g->E));
-  dbuf<int32_t> cnt, cursor, tmp;
-  SP_TRY(cnt.alloc(g->V + 1));
-  SP_TRY(cursor.alloc(g->V + 1));
-  SP_CHECK_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int32_t) * (g->V + 1), s));
-  int grid = num_sms() * 8;
-  k_count_in<<<grid, 256, 0, s>>>(g->adj.p, g->E, cnt.p);
-  SP_CHECK_LAUNCH();
-  size_t tb = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt.p, g->roff.p, g->V + 1, s);
-  dbuf<unsigned char> temp;
-  SP_TRY(temp.alloc(tb));
-  cub::DeviceScan::ExclusiveSum(temp.p, tb, cnt.p, g->roff.p, g->V + 1, s);
-  SP_CHECK_LAUNCH();
-  SP_CHECK_CUDA(cudaMemcpyAsync(cursor.p, g->roff.p, sizeof(int32_t) * g->V, cudaMemcpyDeviceToDevice, s));
-  k_scatter_rev<<<grid, 256, 0, s>>>(g->off.p, g->adj.p, g->V, cursor.p, g->radj.p);
-  SP_CHECK_LAUNCH();
-  // sort each reverse segment (graph.hpp:825-832 sorts srcList per vertex)
-  SP_TRY(tmp.alloc(g->E));
-  size_t sb = 0;
-  cub::DeviceSegmentedSort::SortKeys(nullptr, sb, g->radj.p, tmp.p, (int)g->E, g->V, g->roff.p, g->roff.p + 1, s);
-  dbuf<unsigned char> stemp;
-  SP_TRY(stemp.alloc(sb));
-  cub::DeviceSegmentedSort::SortKeys(stemp.p, sb, g->radj.p, tmp.p, (int)g->E, g->V, g->roff.p, g->roff.p + 1, s);
-  SP_CHECK_LAUNCH();
-  SP_CHECK_CUDA(cudaMemcpyAsync(g->radj.p, tmp.p, sizeof(int32_t) * g->E, cudaMemcpyDeviceToDevice, s));
+  const int V = g->V;
+  const int64_t E = g->E;
+  SP_TRY(g->roff.alloc((size_t)V + 1));
+  SP_TRY(g->radj.alloc(E));
+  int bits = 1;
+  while (bits < 31 && (1 << bits) < V) ++bits;
+  size_t t_sort = 0;
+  cub::DoubleBuffer<int32_t> kb(nullptr, nullptr), vb(nullptr, nullptr);
+  cub::DeviceRadixSort::SortPairs(nullptr, t_sort, kb, vb, (int)E, 0, bits, s);
+  Arena T;
+  dspan<int32_t> keys, keys_alt, src, src_alt;
+  dspan<unsigned char> temp;
+  T.want(keys, E);
+  T.want(keys_alt, E);
+  T.want(src, E);
+  T.want(src_alt, E);
+  T.want(temp, t_sort);
+  SP_TRY(T.commit());
+  if (E > 0) {
+    SP_CHECK_CUDA(cudaMemcpyAsync(keys.p, g->adj.p, 4 * (size_t)E, cudaMemcpyDeviceToDevice, s));
+    k_row_of<<<num_sms() * 8, 256, 0, s>>>(V, E, g->off.p, src.p);
+    SP_CHECK_LAUNCH();
+    cub::DoubleBuffer<int32_t> kd(keys.p, keys_alt.p), vd(src.p, src_alt.p);
+    size_t t = temp.n;
+    SP_CHECK_CUDA(cub::DeviceRadixSort::SortPairs(temp.p, t, kd, vd, (int)E, 0, bits, s));
+    g_launches++;
+    SP_CHECK_CUDA(cudaMemcpyAsync(g->radj.p, vd.Current(), 4 * (size_t)E, cudaMemcpyDeviceToDevice, s));
+    k_offsets_of_sorted<<<num_sms() * 8, 256, 0, s>>>(V, E, kd.Current(), g->roff.p);
+    SP_CHECK_LAUNCH();
+  } else {
+    SP_CHECK_CUDA(cudaMemsetAsync(g->roff.p, 0, sizeof(int32_t) * ((size_t)V + 1), s));
+  }
   SP_CHECK_CUDA(cudaStreamSynchronize(s));
   g->has_rev = true;
+  return SP_OK;
+}
+
+int ensure_emap(sp_graph* g) {
+  if (g->emap.p && g->emap.n >= (size_t)g->E) return SP_OK;
+  SP_TRY(ensure_reverse(g));
+  cudaStream_t s = g->stream;
+  const int64_t E = g->E;
+  SP_TRY(g->emap.alloc(E));
+  if (E > 0) {
+    dbuf<int32_t> rrow;
+    SP_TRY(rrow.alloc(E));
+    k_row_of<<<num_sms() * 8, 256, 0, s>>>(g->V, E, g->roff.p, rrow.p);
+    SP_CHECK_LAUNCH();
+    k_emap<<<num_sms() * 8, 256, 0, s>>>(g->V, E, g->off.p, g->adj.p, rrow.p, g->radj.p, g->emap.p);
+    SP_CHECK_LAUNCH();
+    SP_CHECK_CUDA(cudaStreamSynchronize(s));
+  }
   return SP_OK;
 }
 
@@ -284,6 +337,26 @@ int ensure_symmetry(sp_graph* g) {
   int h = 0;
   SP_TRY(copy_out(&h, bad.p, sizeof(int), s));
   g->symmetric = h ? 0 : 1;
+  return SP_OK;
+}
+
+// Checks a CSR built inside the library (both directions when present) and records
+// the largest out-degree, as sp_graph_create does for a caller's arrays.
+int finish_graph(sp_graph* g) {
+  const int64_t E = g->E;
+  const size_t nw = (size_t)((E + 31) / 32) + 1;
+  dbuf<uint32_t> scratch;
+  SP_TRY(scratch.alloc(nw + 4));
+  int* res = (int*)(scratch.p + nw);
+  SP_TRY(validate_csr(g->off.p, g->adj.p, g->V, E, scratch.p, res, g->stream));
+  if (g->has_rev) SP_TRY(validate_csr(g->roff.p, g->radj.p, g->V, E, scratch.p, res + 2, g->stream));
+  int h[4] = {0, 0, 0, 0};
+  SP_TRY(copy_out(h, res, sizeof(h), g->stream));
+  if (h[0] || (g->has_rev && h[2])) {
+    set_error("internal CSR check failed (flags %d / %d)", h[0], h[2]);
+    return SP_ERR_INVALID;
+  }
+  g->max_out_deg = h[1];
   return SP_OK;
 }
 
@@ -416,6 +489,7 @@ int sp_graph_free(sp_graph_h g) {
   g->w.release();
   g->roff.release();
   g->radj.release();
+  g->emap.release();
   if (g->own_stream && g->stream) cudaStreamDestroy(g->stream);
   delete g;
   return SP_OK;

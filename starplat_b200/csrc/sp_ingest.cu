@@ -1,0 +1,330 @@
+// Text edge-list ingestion: the reference's graph::parseGraph (graph.hpp:464-512
+// parseEdges, :720-865 parseEdgesContent) rebuilt for a GPU host.
+//
+// Reference semantics kept:
+//  * one edge per line "src dst weight"; a line that is empty or does not start with
+//    a digit is skipped (comments, headers, blank lines) (:471-474);
+//  * fields are whitespace separated integers as std::stringstream reads them: an
+//    optional sign, digits up to the first other character ("3.7" reads 3); a
+//    malformed weight reads 0; one out of int32 range saturates (:478-490);
+//  * the vertex count is the largest id + 1 (nodesTotal starts at 0) (:483-487, :139);
+//  * duplicate (src, dst) pairs become one edge whose weight is the sum (:493-506);
+//    self-loops are kept;
+//  * forward rows sorted by destination, reverse rows sorted by source, and
+//    edgeMap[i] = forward index of reverse entry i (:725-859).
+// Where the reference is undefined this build decides: a line without a weight field
+// gets weight 1 (the reference leaves it uninitialised), and a missing, malformed,
+// negative or out-of-range source / destination is an error naming the line (the
+// reference stores 0 or a negative id and indexes out of its arrays).
+//
+// B200 design: host threads tokenise disjoint byte ranges of the file (the only
+// per-byte work), the triples go to the device once, and everything else runs
+// there: a radix sort of (src << 32 | dst) keys with their weights, a
+// reduce-by-key for the duplicate sums, the forward offsets by binary search, and
+// the reverse CSR and edgeMap by a stable transpose (ensure_reverse). The reference
+// spends its time in a std::map insertion per line and an O(indeg^2) edgeMap loop.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <climits>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "sp_internal.cuh"
+
+namespace sp {
+
+namespace ingest {
+
+struct Part {
+  std::vector<int32_t> s, d, w;
+  int64_t lines = 0;      // lines that start in this part
+  int32_t max_id = 0;
+  int64_t err_line = -1;  // line index within the part
+  const char* err = nullptr;
+};
+
+inline bool is_space(char c) { return c == ' ' || c == '\t' || c == '\r' || c == '\v' || c == '\f'; }
+
+// An integer as stringstream's operator>> reads it: optional sign, then digits up to
+// the first non-digit. 0 = ok, 1 = no digits, 2 = out of int32 range (v saturated).
+inline int read_int(const char*& p, const char* end, int32_t& v) {
+  bool neg = false;
+  if (p < end && (*p == '+' || *p == '-')) {
+    neg = *p == '-';
+    ++p;
+  }
+  if (p >= end || *p < '0' || *p > '9') return 1;
+  long long x = 0;
+  bool over = false;
+  for (; p < end && *p >= '0' && *p <= '9'; ++p) {
+    if (!over) {
+      x = x * 10 + (*p - '0');
+      if (x > (long long)INT_MAX + 1) over = true;
+    }
+  }
+  if (neg) x = -x;
+  if (over || x > INT_MAX || x < INT_MIN) {
+    v = neg ? INT_MIN : INT_MAX;
+    return 2;
+  }
+  v = (int32_t)x;
+  return 0;
+}
+
+// Parses the lines that start in [lo, hi) of buf[0, n).
+void parse_part(const char* buf, size_t n, size_t lo, size_t hi, Part& out) {
+  size_t pos = lo;
+  if (lo > 0) {  // the line containing lo belongs to the previous part
+    while (pos < n && buf[pos - 1] != '\n') ++pos;
+  }
+  out.s.reserve((hi - lo) / 12 + 16);
+  out.d.reserve((hi - lo) / 12 + 16);
+  out.w.reserve((hi - lo) / 12 + 16);
+  while (pos < hi && pos < n) {
+    const char* a = buf + pos;
+    const char* nl = (const char*)memchr(a, '\n', n - pos);
+    const char* b = nl ? nl : buf + n;
+    pos = (size_t)(b - buf) + 1;
+    const int64_t line = out.lines++;
+    if (a == b || *a < '0' || *a > '9') continue;
+    const char* p = a;
+    int32_t src = 0, dst = 0, w = 1;
+    if (read_int(p, b, src) != 0) {
+      out.err_line = line;
+      out.err = "source id out of int32 range";
+      return;
+    }
+    while (p < b && is_space(*p)) ++p;
+    const int rd = read_int(p, b, dst);
+    if (rd != 0 || dst < 0) {
+      out.err_line = line;
+      out.err = rd == 1 ? "missing or malformed destination" : "destination id negative or out of int32 range";
+      return;
+    }
+    while (p < b && is_space(*p)) ++p;
+    if (p < b) {
+      const int rw = read_int(p, b, w);
+      if (rw == 1) w = 0;  // a malformed field reads as 0
+    }
+    if (src == INT_MAX || dst == INT_MAX) {
+      out.err_line = line;
+      out.err = "vertex id too large (the vertex count would exceed int32)";
+      return;
+    }
+    out.s.push_back(src);
+    out.d.push_back(dst);
+    out.w.push_back(w);
+    out.max_id = std::max(out.max_id, std::max(src, dst));
+  }
+}
+
+__global__ void k_pack(int64_t n, const int32_t* __restrict__ s, const int32_t* __restrict__ d,
+                       unsigned long long* __restrict__ keys) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    keys[i] = ((unsigned long long)(uint32_t)s[i] << 32) | (uint32_t)d[i];
+}
+
+// Forward CSR from the sorted unique keys: adj = low halves; off[v] = first key whose
+// source is >= v (binary search, one thread per vertex, v = 0..V).
+__global__ void k_forward(int32_t V, int64_t E, const unsigned long long* __restrict__ ukeys,
+                          int32_t* __restrict__ off, int32_t* __restrict__ adj) {
+  const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t e = tid; e < E; e += stride) adj[e] = (int32_t)(uint32_t)(ukeys[e] & 0xffffffffull);
+  for (int64_t v = tid; v <= V; v += stride) {
+    int64_t lo = 0, hi = E;
+    while (lo < hi) {
+      const int64_t m = (lo + hi) >> 1;
+      if ((int64_t)(ukeys[m] >> 32) < v) lo = m + 1; else hi = m;
+    }
+    off[v] = (int32_t)lo;
+  }
+}
+
+}  // namespace ingest
+
+static int load_text(const char* path, int nthreads, sp_graph_h* out) {
+  FILE* f = fopen(path, "rb");
+  if (!f) {
+    set_error("sp_graph_load_text: cannot open %s", path);
+    return SP_ERR_INVALID;
+  }
+  std::vector<char> buf;
+  if (fseek(f, 0, SEEK_END) == 0) {
+    const long sz = ftell(f);
+    if (sz > 0) buf.resize((size_t)sz);
+    fseek(f, 0, SEEK_SET);
+  }
+  const size_t got = buf.empty() ? 0 : fread(buf.data(), 1, buf.size(), f);
+  fclose(f);
+  buf.resize(got);
+  const size_t n = buf.size();
+
+  int T = nthreads > 0 ? nthreads : (int)std::thread::hardware_concurrency();
+  T = std::max(1, std::min(T, 64));
+  if (n < ((size_t)1 << 20)) T = 1;
+  std::vector<ingest::Part> parts(T);
+  {
+    std::vector<std::thread> th;
+    for (int t = 0; t < T; ++t)
+      th.emplace_back(ingest::parse_part, buf.data(), n, n * t / T, n * (t + 1) / T, std::ref(parts[t]));
+    for (auto& x : th) x.join();
+  }
+  int64_t line0 = 0, m = 0;
+  int32_t max_id = 0;
+  for (int t = 0; t < T; ++t) {
+    if (parts[t].err) {
+      set_error("sp_graph_load_text: %s:%lld: %s", path, (long long)(line0 + parts[t].err_line + 1), parts[t].err);
+      return SP_ERR_INVALID;
+    }
+    line0 += parts[t].lines;
+    m += (int64_t)parts[t].s.size();
+    max_id = std::max(max_id, parts[t].max_id);
+  }
+  if (m > INT_MAX) {
+    set_error("sp_graph_load_text: %lld edge lines (int32 edge indices)", (long long)m);
+    return SP_ERR_UNSUPPORTED;
+  }
+  std::vector<int32_t> hs((size_t)m), hd((size_t)m), hw((size_t)m);
+  {
+    std::vector<int64_t> at(T + 1, 0);
+    for (int t = 0; t < T; ++t) at[t + 1] = at[t] + (int64_t)parts[t].s.size();
+    std::vector<std::thread> th;
+    for (int t = 0; t < T; ++t)
+      th.emplace_back([&, t] {
+        const size_t k = parts[t].s.size();
+        if (!k) return;
+        std::memcpy(hs.data() + at[t], parts[t].s.data(), 4 * k);
+        std::memcpy(hd.data() + at[t], parts[t].d.data(), 4 * k);
+        std::memcpy(hw.data() + at[t], parts[t].w.data(), 4 * k);
+        std::vector<int32_t>().swap(parts[t].s);
+        std::vector<int32_t>().swap(parts[t].d);
+        std::vector<int32_t>().swap(parts[t].w);
+      });
+    for (auto& x : th) x.join();
+  }
+  std::vector<char>().swap(buf);
+
+  const int32_t V = max_id + 1;
+  sp_graph* g = new sp_graph();
+  auto fail = [&](int st) {
+    sp_graph_free(g);
+    return st;
+  };
+  cudaGetDevice(&g->device);
+  g->V = V;
+  if (cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete g;
+    set_error("sp_graph_load_text: cudaStreamCreate failed");
+    return SP_ERR_CUDA;
+  }
+  g->own_stream = true;
+  cudaStream_t s = g->stream;
+  int st;
+  {
+    Arena T0;
+    dspan<int32_t> ds, dd, dw, dw_alt, uw;
+    dspan<unsigned long long> keys, keys_alt, ukeys;
+    dspan<int> nrun;
+    dspan<unsigned char> temp;
+    int bits = 1;
+    while (bits < 31 && (1 << bits) < V) ++bits;
+    size_t t_sort = 0, t_red = 0;
+    cub::DoubleBuffer<unsigned long long> kb(nullptr, nullptr);
+    cub::DoubleBuffer<int32_t> vb(nullptr, nullptr);
+    cub::DeviceRadixSort::SortPairs(nullptr, t_sort, kb, vb, (int)m, 0, 32 + bits, s);
+    cub::DeviceReduce::ReduceByKey(nullptr, t_red, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
+                                   (int32_t*)nullptr, (int32_t*)nullptr, (int*)nullptr, cub::Sum(), (int)m, s);
+    T0.want(ds, m);
+    T0.want(dd, m);
+    T0.want(dw, m);
+    T0.want(dw_alt, m);
+    T0.want(uw, m);
+    T0.want(keys, m);
+    T0.want(keys_alt, m);
+    T0.want(ukeys, m);
+    T0.want(nrun, 1);
+    T0.want(temp, std::max(t_sort, t_red));
+    if ((st = T0.commit())) return fail(st);
+    const size_t tb = temp.n;
+    if (m > 0) {
+      if (cudaMemcpyAsync(ds.p, hs.data(), 4 * (size_t)m, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+          cudaMemcpyAsync(dd.p, hd.data(), 4 * (size_t)m, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+          cudaMemcpyAsync(dw.p, hw.data(), 4 * (size_t)m, cudaMemcpyHostToDevice, s) != cudaSuccess) {
+        set_error("sp_graph_load_text: copy to the device failed");
+        return fail(SP_ERR_CUDA);
+      }
+      ingest::k_pack<<<num_sms() * 8, 256, 0, s>>>(m, ds.p, dd.p, keys.p);
+      g_launches++;
+      cub::DoubleBuffer<unsigned long long> kd(keys.p, keys_alt.p);
+      cub::DoubleBuffer<int32_t> vd(dw.p, dw_alt.p);
+      size_t t = tb;
+      if (cub::DeviceRadixSort::SortPairs(temp.p, t, kd, vd, (int)m, 0, 32 + bits, s) != cudaSuccess) return fail(SP_ERR_CUDA);
+      t = tb;
+      if (cub::DeviceReduce::ReduceByKey(temp.p, t, kd.Current(), ukeys.p, vd.Current(), uw.p, nrun.p, cub::Sum(),
+                                         (int)m, s) != cudaSuccess)
+        return fail(SP_ERR_CUDA);
+      g_launches += 2;
+    }
+    int E = 0;
+    if (m > 0 && (st = copy_out(&E, nrun.p, sizeof(int), s))) return fail(st);
+    g->E = E;
+    if ((st = g->off.alloc((size_t)V + 1)) || (st = g->adj.alloc(E)) || (st = g->w.alloc(E))) return fail(st);
+    if (E > 0) {
+      ingest::k_forward<<<num_sms() * 8, 256, 0, s>>>(V, E, ukeys.p, g->off.p, g->adj.p);
+      g_launches++;
+      if (cudaMemcpyAsync(g->w.p, uw.p, 4 * (size_t)E, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+        return fail(SP_ERR_CUDA);
+    } else if (cudaMemsetAsync(g->off.p, 0, sizeof(int32_t) * ((size_t)V + 1), s) != cudaSuccess) {
+      return fail(SP_ERR_CUDA);
+    }
+    if (cudaStreamSynchronize(s) != cudaSuccess) {
+      set_error("sp_graph_load_text: %s", cudaGetErrorString(cudaGetLastError()));
+      return fail(SP_ERR_CUDA);
+    }
+  }
+  g->has_w = true;
+  if ((st = ensure_reverse(g))) return fail(st);
+  if ((st = finish_graph(g))) return fail(st);
+  *out = g;
+  return SP_OK;
+}
+
+}  // namespace sp
+
+using namespace sp;
+
+extern "C" int sp_graph_load_text(const char* path, int32_t nthreads, sp_graph_h* out) {
+  if (!path || !out) {
+    set_error("sp_graph_load_text: NULL argument");
+    return SP_ERR_INVALID;
+  }
+  *out = nullptr;
+  return load_text(path, nthreads, out);
+}
+
+extern "C" int sp_graph_export(sp_graph_h g, int32_t* indexofNodes, int32_t* edgeList, int32_t* edgeLen,
+                               int32_t* rev_indexofNodes, int32_t* srcList, int32_t* edgeMap) {
+  if (!g) {
+    set_error("sp_graph_export: NULL graph");
+    return SP_ERR_INVALID;
+  }
+  if (edgeLen && !g->has_w) {
+    set_error("sp_graph_export: the graph has no edgeLen");
+    return SP_ERR_INVALID;
+  }
+  if (rev_indexofNodes || srcList) SP_TRY(ensure_reverse(g));
+  if (edgeMap) SP_TRY(ensure_emap(g));
+  const size_t V1 = (size_t)g->V + 1, E = (size_t)g->E;
+  cudaStream_t s = g->stream;
+  if (indexofNodes) SP_TRY(copy_out(indexofNodes, g->off.p, 4 * V1, s));
+  if (edgeList) SP_TRY(copy_out(edgeList, g->adj.p, 4 * E, s));
+  if (edgeLen) SP_TRY(copy_out(edgeLen, g->w.p, 4 * E, s));
+  if (rev_indexofNodes) SP_TRY(copy_out(rev_indexofNodes, g->roff.p, 4 * V1, s));
+  if (srcList) SP_TRY(copy_out(srcList, g->radj.p, 4 * E, s));
+  if (edgeMap) SP_TRY(copy_out(edgeMap, g->emap.p, 4 * E, s));
+  return SP_OK;
+}

@@ -145,6 +145,7 @@ struct sp_graph {
   sp::dbuf<int32_t> w;     // edgeLen [E] (optional)
   sp::dbuf<int32_t> roff;  // rev_indexofNodes [V+1]
   sp::dbuf<int32_t> radj;  // srcList [E]
+  sp::dbuf<int32_t> emap;  // edgeMap [E]: forward index of each reverse entry (built on demand)
   bool has_w = false;
   bool has_rev = false;
   int symmetric = -1;      // -1 unknown, 0/1
@@ -168,6 +169,8 @@ struct sp_graph {
 
 namespace sp {
 int ensure_reverse(sp_graph* g);      // builds roff/radj on device if missing
+int ensure_emap(sp_graph* g);         // builds emap (edgeMap) on device if missing
+int finish_graph(sp_graph* g);        // checks a library-built CSR, sets max_out_deg
 int pr_order_default();               // PageRank vertex order default (sp_pagerank.cu)
 int tc_cta_warps_default();           // TC kernel choice default (sp_tc.cu)
 int ensure_symmetry(sp_graph* g);     // fills g->symmetric

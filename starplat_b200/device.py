@@ -11,6 +11,7 @@ are written to caller-provided arrays of either kind.
 from __future__ import annotations
 
 import ctypes
+import os
 from typing import Optional
 
 import numpy as np
@@ -74,6 +75,36 @@ class DeviceGraph:
         self.V = V
         self.E = E
         self._keep = arrs if dev else None
+
+    @classmethod
+    def load_text(cls, path: str, nthreads: int = 0) -> "DeviceGraph":
+        """Read a text edge list (the reference's graph::parseGraph format) straight into
+        GPU memory: tokenised on the host, sorted, merged and turned into both CSRs on the
+        device."""
+        h = ctypes.c_void_p()
+        check("sp_graph_load_text", lib().sp_graph_load_text(os.fsencode(path), int(nthreads), ctypes.byref(h)))
+        self = cls.__new__(cls)
+        self._h = h
+        self._keep = None
+        V = ctypes.c_int32()
+        E = ctypes.c_int64()
+        check("sp_graph_info", lib().sp_graph_info(h, ctypes.byref(V), ctypes.byref(E), None))
+        self.V, self.E = int(V.value), int(E.value)
+        return self
+
+    def export(self) -> dict:
+        """The mirror's CSR as host arrays named like graph.hpp's fields."""
+        V, E = self.V, self.E
+        out = {"indexofNodes": np.empty(V + 1, np.int32), "edgeList": np.empty(E, np.int32),
+               "edgeLen": np.empty(E, np.int32), "rev_indexofNodes": np.empty(V + 1, np.int32),
+               "srcList": np.empty(E, np.int32), "edgeMap": np.empty(E, np.int32)}
+        names = ("indexofNodes", "edgeList", "edgeLen", "rev_indexofNodes", "srcList", "edgeMap")
+        try:
+            check("sp_graph_export", lib().sp_graph_export(self.handle, *[_ptr(out[k]) for k in names]))
+        except _lib.SPError:  # a graph created without weights has no edgeLen
+            del out["edgeLen"]
+            check("sp_graph_export", lib().sp_graph_export(self.handle, *[_ptr(out.get(k)) for k in names]))
+        return out
 
     @classmethod
     def from_csr(cls, g: CSRGraph, with_reverse: bool = True, with_weights: bool = True) -> "DeviceGraph":

@@ -4,19 +4,21 @@
 #include <set>
 #include <vector>
 
+#ifdef GRAPH_HEADER
 #include GRAPH_HEADER
+#endif
 #include "starplat_b200.hpp"
 
 int main(int argc, char** argv) {
   if (argc < 3) return 2;
-#ifdef PARSE_TEXT
+#if defined(LIBRARY_PARSE)  // the library reads the text file (starplat_b200::Graph)
+  starplat_b200::Graph g(argv[1]);
+  g.parseGraph();
+#elif defined(PARSE_TEXT)  // the reference's graph::parseGraph
   graph g(argv[1]);
-#else
-  graph g;
-#endif
-#ifdef PARSE_TEXT
   g.parseGraph();
 #else
+  graph g;
   if (!g.load(argv[1])) return 3;
 #endif
   const int V = g.num_nodes();

@@ -17,9 +17,10 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIBDIR = os.path.join(ROOT, "starplat_b200")
 
 
-def build_driver(outdir):
+def build_driver(outdir, library_parse=False):
     exe = os.path.join(outdir, "drop_in")
-    cmd = ["g++", "-O2", "-std=c++17", '-DGRAPH_HEADER="mini_graph.hpp"', "-I", os.path.join(ROOT, "tests", "cpp"),
+    mode = "-DLIBRARY_PARSE" if library_parse else '-DGRAPH_HEADER="mini_graph.hpp"'
+    cmd = ["g++", "-O2", "-std=c++17", mode, "-I", os.path.join(ROOT, "tests", "cpp"),
            "-I", os.path.join(ROOT, "include"), os.path.join(ROOT, "tests", "cpp", "drop_in_main.cpp"),
            "-L", LIBDIR, "-lsp_b200", f"-Wl,-rpath,{LIBDIR}", "-o", exe]
     subprocess.check_call(cmd)
@@ -29,6 +30,7 @@ def build_driver(outdir):
 def test_dropin_header_compiles():
     with tempfile.TemporaryDirectory() as d:
         assert os.path.exists(build_driver(d))
+        assert os.path.exists(build_driver(d, library_parse=True))
 
 
 def write_bin(g, path):
@@ -100,4 +102,20 @@ def test_dropin_with_reference_graph_hpp():
         out = subprocess.run([exe, path, "5"], check=True, capture_output=True, text=True).stdout
     res = parse(out)
     assert int(res["V"][0]) == g.V and int(res["V"][2]) == g.E  # parseGraph built the same CSR
+    check_outputs(res, g, 5)
+
+
+@pytest.mark.gpu
+def test_dropin_with_library_parse_of_the_text_file():
+    # the driver's `graph g(path); g.parseGraph();` becomes starplat_b200::Graph: the
+    # library reads the same text file the reference's parseGraph reads
+    g = small_graph()
+    with tempfile.TemporaryDirectory() as d:
+        exe = build_driver(d, library_parse=True)
+        path = os.path.join(d, "g.txt")
+        u = np.repeat(np.arange(g.V), np.diff(g.indexofNodes))
+        np.savetxt(path, np.stack([u, g.edgeList, g.edgeLen], 1), fmt="%d")
+        out = subprocess.run([exe, path, "5"], check=True, capture_output=True, text=True).stdout
+    res = parse(out)
+    assert int(res["V"][0]) == g.V and int(res["V"][2]) == g.E
     check_outputs(res, g, 5)
