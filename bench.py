@@ -23,6 +23,8 @@ baseline:
   bc_rmat20        BC, undirected R-MAT 20 ef16, 256 sources (S * E_r / t)
   bc_er1000        BC, 1000 ER graphs (1k-50k vertices, degree 8-32), 16 sources each
   louvain_sbm1m    Louvain, planted partition 1,048,576 vertices, 256 blocks (E * sweeps / t)
+  ingest_rmat20    text edge list -> device mirror (sp_graph_load_text), directed R-MAT 20
+                   ef16 with weights (M edge lines / s; not a GTEPS figure)
 Inputs are seeded synthetic graphs with the configs' shapes (no dataset is
 available offline). Every workload's inputs exceed L2 (126 MB) except the TC
 graph (7 MB CSR), which is small by definition of its config.
@@ -455,7 +457,60 @@ def bench_louvain(steps, warmup, stream, hbm, cpu):
     return out
 
 
-EXTRAS = ("tc_rmat16", "sssp_rmat23", "sssp_grid4096", "bc_rmat20", "bc_er1000", "louvain_sbm1m")
+def bench_ingest(steps, warmup, cpu):
+    """Text edge list -> device mirror through sp_graph_load_text, wall time of the call
+    (file read from the page cache, host tokenising, copy, device sort / merge / both
+    CSRs / check). The CPU figure is the reference's own graph::parseGraph (compiled
+    from graph.hpp) on an R-MAT 16 file of the same shape, when that build is present."""
+    import shutil
+    import tempfile
+
+    import torch
+
+    from starplat_b200 import generators as G
+    from starplat_b200.device import DeviceGraph
+
+    d = tempfile.mkdtemp(prefix="sp_ingest_")
+    try:
+        g = G.rmat(20, 16, seed=20, directed=True)
+        w = G.hash_weights(g, 20, 1, 100, False)
+        path = os.path.join(d, "rmat20.txt")
+        nbytes = G.write_edgelist(g, path, w)
+        times, E = [], 0
+        for i in range(warmup + steps):
+            t = time.perf_counter()
+            dg = DeviceGraph.load_text(path)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t
+            E = dg.E
+            dg.free()
+            if i >= warmup:
+                times.append(dt)
+        ms = 1e3 * statistics.median(times)
+        out = {"workload": "text edge list of directed R-MAT 20 ef16 (seed 20), weights U[1,100], "
+                           "one 'src dst weight' line per edge", "lines": int(g.E), "bytes": int(nbytes),
+               "V": int(g.V), "E": int(E), "value": g.E / (ms / 1e3) / 1e6, "unit": "M edge lines/s", "ms": ms,
+               "text_gb_per_s": nbytes / (ms / 1e3) / 1e9}
+        if cpu:
+            from oracle import oracle as O
+
+            if O.ref_lib() is not None:
+                g16 = G.rmat(16, 16, seed=20, directed=True)
+                p16 = os.path.join(d, "rmat16.txt")
+                G.write_edgelist(g16, p16, G.hash_weights(g16, 20, 1, 100, False))
+                t = time.perf_counter()
+                O.ref_parse_graph(p16)
+                dt = time.perf_counter() - t
+                out["cpu_baseline"] = {"value": g16.E / dt / 1e6, "unit": "M edge lines/s",
+                                       "cores": O.num_threads(), "kind": "reference",
+                                       "sample": f"graph::parseGraph on the R-MAT 16 file ({g16.E} lines, {dt:.2f} s; "
+                                                 "its line reading is sequential, its sorts use OpenMP)"}
+        return out
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
+EXTRAS = ("tc_rmat16", "sssp_rmat23", "sssp_grid4096", "bc_rmat20", "bc_er1000", "louvain_sbm1m", "ingest_rmat20")
 
 
 def run_extras(want, args, stream, hbm, cpu_ok):
@@ -494,6 +549,8 @@ def run_extras(want, args, stream, hbm, cpu_ok):
         guarded("bc_er1000", lambda: bench_bc_er(max(1, ks // 2), 1, stream, hbm, cpu_ok))
     if "louvain_sbm1m" in want:
         guarded("louvain_sbm1m", lambda: bench_louvain(max(1, ks // 2), 1, stream, hbm, cpu_ok))
+    if "ingest_rmat20" in want:
+        guarded("ingest_rmat20", lambda: bench_ingest(max(1, ks // 2), 1, cpu_ok))
     return extras
 
 

@@ -25,6 +25,11 @@
 // spends its time in a std::map insertion per line and an O(indeg^2) edgeMap loop.
 #include <cub/cub.cuh>
 
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include <algorithm>
 #include <climits>
 #include <cstdio>
@@ -146,22 +151,44 @@ __global__ void k_forward(int32_t V, int64_t E, const unsigned long long* __rest
 
 }  // namespace ingest
 
+// The file mapped read-only (no copy of its bytes), unmapped on scope exit.
+struct Mapped {
+  const char* p = nullptr;
+  size_t n = 0;
+  ~Mapped() {
+    if (p) munmap((void*)p, n);
+  }
+};
+
 static int load_text(const char* path, int nthreads, sp_graph_h* out) {
-  FILE* f = fopen(path, "rb");
-  if (!f) {
-    set_error("sp_graph_load_text: cannot open %s", path);
-    return SP_ERR_INVALID;
+  Mapped file;
+  {
+    const int fd = open(path, O_RDONLY);
+    if (fd < 0) {
+      set_error("sp_graph_load_text: cannot open %s", path);
+      return SP_ERR_INVALID;
+    }
+    struct stat sb;
+    if (fstat(fd, &sb) != 0) {
+      close(fd);
+      set_error("sp_graph_load_text: cannot stat %s", path);
+      return SP_ERR_INVALID;
+    }
+    if (sb.st_size > 0) {
+      void* m = mmap(nullptr, (size_t)sb.st_size, PROT_READ, MAP_PRIVATE, fd, 0);
+      if (m == MAP_FAILED) {
+        close(fd);
+        set_error("sp_graph_load_text: cannot map %s", path);
+        return SP_ERR_INVALID;
+      }
+      madvise(m, (size_t)sb.st_size, MADV_SEQUENTIAL);
+      file.p = (const char*)m;
+      file.n = (size_t)sb.st_size;
+    }
+    close(fd);
   }
-  std::vector<char> buf;
-  if (fseek(f, 0, SEEK_END) == 0) {
-    const long sz = ftell(f);
-    if (sz > 0) buf.resize((size_t)sz);
-    fseek(f, 0, SEEK_SET);
-  }
-  const size_t got = buf.empty() ? 0 : fread(buf.data(), 1, buf.size(), f);
-  fclose(f);
-  buf.resize(got);
-  const size_t n = buf.size();
+  const char* buf = file.p;
+  const size_t n = file.n;
 
   int T = nthreads > 0 ? nthreads : (int)std::thread::hardware_concurrency();
   T = std::max(1, std::min(T, 64));
@@ -170,7 +197,7 @@ static int load_text(const char* path, int nthreads, sp_graph_h* out) {
   {
     std::vector<std::thread> th;
     for (int t = 0; t < T; ++t)
-      th.emplace_back(ingest::parse_part, buf.data(), n, n * t / T, n * (t + 1) / T, std::ref(parts[t]));
+      th.emplace_back(ingest::parse_part, buf, n, n * t / T, n * (t + 1) / T, std::ref(parts[t]));
     for (auto& x : th) x.join();
   }
   int64_t line0 = 0, m = 0;
@@ -188,26 +215,6 @@ static int load_text(const char* path, int nthreads, sp_graph_h* out) {
     set_error("sp_graph_load_text: %lld edge lines (int32 edge indices)", (long long)m);
     return SP_ERR_UNSUPPORTED;
   }
-  std::vector<int32_t> hs((size_t)m), hd((size_t)m), hw((size_t)m);
-  {
-    std::vector<int64_t> at(T + 1, 0);
-    for (int t = 0; t < T; ++t) at[t + 1] = at[t] + (int64_t)parts[t].s.size();
-    std::vector<std::thread> th;
-    for (int t = 0; t < T; ++t)
-      th.emplace_back([&, t] {
-        const size_t k = parts[t].s.size();
-        if (!k) return;
-        std::memcpy(hs.data() + at[t], parts[t].s.data(), 4 * k);
-        std::memcpy(hd.data() + at[t], parts[t].d.data(), 4 * k);
-        std::memcpy(hw.data() + at[t], parts[t].w.data(), 4 * k);
-        std::vector<int32_t>().swap(parts[t].s);
-        std::vector<int32_t>().swap(parts[t].d);
-        std::vector<int32_t>().swap(parts[t].w);
-      });
-    for (auto& x : th) x.join();
-  }
-  std::vector<char>().swap(buf);
-
   const int32_t V = max_id + 1;
   sp_graph* g = new sp_graph();
   auto fail = [&](int st) {
@@ -251,11 +258,18 @@ static int load_text(const char* path, int nthreads, sp_graph_h* out) {
     if ((st = T0.commit())) return fail(st);
     const size_t tb = temp.n;
     if (m > 0) {
-      if (cudaMemcpyAsync(ds.p, hs.data(), 4 * (size_t)m, cudaMemcpyHostToDevice, s) != cudaSuccess ||
-          cudaMemcpyAsync(dd.p, hd.data(), 4 * (size_t)m, cudaMemcpyHostToDevice, s) != cudaSuccess ||
-          cudaMemcpyAsync(dw.p, hw.data(), 4 * (size_t)m, cudaMemcpyHostToDevice, s) != cudaSuccess) {
-        set_error("sp_graph_load_text: copy to the device failed");
-        return fail(SP_ERR_CUDA);
+      // each thread's triples go to their place in the device arrays
+      int64_t at = 0;
+      for (int t = 0; t < T; ++t) {
+        const size_t k = parts[t].s.size();
+        if (!k) continue;
+        if (cudaMemcpyAsync(ds.p + at, parts[t].s.data(), 4 * k, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+            cudaMemcpyAsync(dd.p + at, parts[t].d.data(), 4 * k, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+            cudaMemcpyAsync(dw.p + at, parts[t].w.data(), 4 * k, cudaMemcpyHostToDevice, s) != cudaSuccess) {
+          set_error("sp_graph_load_text: copy to the device failed");
+          return fail(SP_ERR_CUDA);
+        }
+        at += (int64_t)k;
       }
       ingest::k_pack<<<num_sms() * 8, 256, 0, s>>>(m, ds.p, dd.p, keys.p);
       g_launches++;

@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <string>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -309,6 +310,51 @@ int64_t spg_grid(int32_t rows, int32_t cols, int32_t* off, int32_t* adj) {
     if (r + 1 < rows) adj[p++] = (int32_t)(v + cols);
   }
   return s;
+}
+
+// Writes a CSR as a text edge list, one "src dst weight" line per edge in CSR order
+// (the format graph::parseGraph reads). Lines are formatted in parallel blocks and
+// written in order. Returns the bytes written, or -1 if the file cannot be written.
+int64_t spg_write_edgelist(const char* path, int32_t V, const int32_t* off, const int32_t* adj, const int32_t* w) {
+  FILE* f = fopen(path, "wb");
+  if (!f) return -1;
+  const int64_t E = off[V];
+  const int64_t B = 1 << 20;  // edges per block
+  const int64_t nb = (E + B - 1) / B;
+  int64_t total = 0;
+  std::vector<std::string> out(16);
+  for (int64_t b0 = 0; b0 < nb; b0 += 16) {
+    const int64_t b1 = std::min(nb, b0 + 16);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t b = b0; b < b1; ++b) {
+      std::string& s = out[b - b0];
+      s.clear();
+      const int64_t e0 = b * B, e1 = std::min(E, e0 + B);
+      // the source of e0: last v with off[v] <= e0
+      int64_t lo = 0, hi = V;
+      while (lo < hi) {
+        const int64_t m = (lo + hi + 1) / 2;
+        if (off[m] <= e0) lo = m; else hi = m - 1;
+      }
+      int32_t u = (int32_t)lo;
+      char tmp[48];
+      for (int64_t e = e0; e < e1; ++e) {
+        while (off[u + 1] <= e) ++u;
+        const int n = snprintf(tmp, sizeof(tmp), "%d %d %d\n", u, adj[e], w ? w[e] : 1);
+        s.append(tmp, n);
+      }
+    }
+    for (int64_t b = b0; b < b1; ++b) {
+      const std::string& s = out[b - b0];
+      if (fwrite(s.data(), 1, s.size(), f) != s.size()) {
+        fclose(f);
+        return -1;
+      }
+      total += (int64_t)s.size();
+    }
+  }
+  fclose(f);
+  return total;
 }
 
 // Is the forward CSR equal to its reverse (an undirected graph)?

@@ -11,6 +11,8 @@ import ctypes
 import math
 import os
 
+from typing import Optional
+
 import numpy as np
 
 from .graph import CSRGraph
@@ -50,6 +52,8 @@ def _lib():
         L.spg_grid.restype = ctypes.c_int64
         L.spg_grid.argtypes = [ctypes.c_int32, ctypes.c_int32, i32p, i32p]
         L.spg_num_threads.restype = ctypes.c_int32
+        L.spg_write_edgelist.restype = ctypes.c_int64
+        L.spg_write_edgelist.argtypes = [ctypes.c_char_p, ctypes.c_int32, i32p, i32p, ctypes.c_void_p]
         _LIB = L
     return _LIB
 
@@ -177,3 +181,14 @@ def pick_sources(g: CSRGraph, count: int, seed: int, min_out_degree: int = 1) ->
 
 def num_threads() -> int:
     return int(_lib().spg_num_threads())
+
+
+def write_edgelist(g: CSRGraph, path: str, weights: Optional[np.ndarray] = None) -> int:
+    """Writes g as a text edge list ("src dst weight" per line, CSR order), the format
+    graph::parseGraph reads; weight 1 where no weights are given. Returns the bytes."""
+    w = None if weights is None else np.ascontiguousarray(weights, np.int32)
+    n = _lib().spg_write_edgelist(os.fsencode(path), g.V, g.indexofNodes, g.edgeList,
+                                  None if w is None else w.ctypes.data)
+    if n < 0:
+        raise OSError(f"cannot write {path}")
+    return int(n)
