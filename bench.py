@@ -311,18 +311,19 @@ def bench_sssp(name, g, src, steps, warmup, stream, hbm, cpu, cpu_mode):
     return out
 
 
-def bench_bc(steps, warmup, stream, hbm, cpu):
+def bench_bc(steps, warmup, stream, hbm, cpu, nsrc=256):
     from starplat_b200 import _lib
     from starplat_b200 import generators as G
     from starplat_b200.device import DeviceGraph
 
     g = G.rmat(20, 16, seed=1)
-    srcs = G.pick_sources(g, 256, seed=20)
+    srcs = G.pick_sources(g, 256, seed=20)[:nsrc]
     lab, ce = component_edges(g)
     er = ce[lab[srcs]]
     sum_er = int(er.sum())
     alg = int(16 * er.sum() + 32 * g.V * len(srcs))
-    out = {"workload": "bc rmat20 ef16 undirected seed1, 256 sources", "V": g.V, "E": g.E, "sources": len(srcs),
+    out = {"workload": f"bc rmat20 ef16 undirected seed1, {len(srcs)} sources", "V": g.V, "E": g.E,
+           "sources": len(srcs),
            "sum_E_r": sum_er}
     with DeviceGraph.from_csr(g, with_weights=False) as dg:
         dg.set_stream(stream)
@@ -544,7 +545,7 @@ def run_extras(want, args, stream, hbm, cpu_ok):
                               1, stream, hbm, cpu_ok, "dijkstra")
         guarded("sssp_grid4096", _s2)
     if "bc_rmat20" in want:
-        guarded("bc_rmat20", lambda: bench_bc(max(1, ks // 2), 1, stream, hbm, cpu_ok))
+        guarded("bc_rmat20", lambda: bench_bc(max(1, ks // 2), 1, stream, hbm, cpu_ok, args.sources))
     if "bc_er1000" in want:
         guarded("bc_er1000", lambda: bench_bc_er(max(1, ks // 2), 1, stream, hbm, cpu_ok))
     if "louvain_sbm1m" in want:
@@ -570,6 +571,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="headline PageRank only")
     ap.add_argument("--scale", type=int, default=PR_SCALE, help="R-MAT scale of the PageRank graph")
     ap.add_argument("--tune", action="append", default=[], help="schedule knob key=value (sp_tune_set)")
+    ap.add_argument("--sources", type=int, default=256,
+                    help="BC sources of the bc_rmat20 workload (256 = the config; fewer for profiler runs)")
     ap.add_argument("--algo-only", default="", help="run only these extra workloads (comma list), no headline: "
                                                      "for profiler runs")
     args = ap.parse_args()

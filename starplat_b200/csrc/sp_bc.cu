@@ -40,8 +40,12 @@ namespace sp {
 namespace bc {
 constexpr int GRID_THREADS = 256;
 constexpr int CTA_THREADS = 512;
-constexpr int HUB_DEG = 4096;   // level-list entries of vertices above this degree are split
-constexpr int HUB_CHUNK = 256;  // edges per hub piece
+// Level-list entries of vertices above HUB_DEG edges are cut into HUB_CHUNK-edge
+// pieces that every warp shares. Small values balance the warps between the grid
+// barriers: R-MAT 20, 256 sources: 257 ms at (4096, 256), 138 at (1024, 256),
+// 121 at (128, 256), 110 at (64, 64).
+constexpr int HUB_DEG = 64;
+constexpr int HUB_CHUNK = 64;
 
 struct Work {
   const int32_t* __restrict__ off;  // CSR rows of this graph (global edge indices)
@@ -66,6 +70,8 @@ struct Work {
   int32_t* hub_base;                // [hub_cap] first piece index (increasing)
   unsigned long long* hub_cnt;      // (entries << 32) | pieces
   int hub_cap;
+  int hub_deg;                      // entries of vertices with more edges are split
+  int hub_chunk;                    // edges per piece
   double* dacc;                     // [V][SW] FP64 partial dependencies of hub entries
 };
 
@@ -91,15 +97,15 @@ __device__ __forceinline__ unsigned long long shfl64(unsigned long long x, int l
   return ((unsigned long long)hi << 32) | lo;
 }
 
-// Entry i of a level list: a hub (more than HUB_DEG edges) when splitting is on.
+// Entry i of a level list: a hub (more than W.hub_deg edges) when splitting is on.
 // Returns true if it was queued as pieces instead of being processed here.
 __device__ __forceinline__ bool queue_hub(const Work& W, int i, int lane) {
   if (W.hub_cap == 0) return false;
   const int v = W.flv[i];
   const int d = W.off[v + 1] - W.off[v];
-  if (d <= HUB_DEG) return false;
+  if (d <= W.hub_deg) return false;
   if (lane == 0) {
-    const int np = (d + HUB_CHUNK - 1) / HUB_CHUNK;
+    const int np = (d + W.hub_chunk - 1) / W.hub_chunk;
     const unsigned long long old = atomicAdd(W.hub_cnt, (1ull << 32) | (unsigned long long)np);
     const int k = (int)(old >> 32);
     if (k < W.hub_cap) {
@@ -121,8 +127,8 @@ __device__ __forceinline__ void hub_piece(const Work& W, int nh, int p, int& i, 
   }
   i = W.hub_ent[lo];
   const int v = W.flv[i];
-  eb = W.off[v] + (p - W.hub_base[lo]) * HUB_CHUNK;
-  ee = min(eb + HUB_CHUNK, W.off[v + 1]);
+  eb = W.off[v] + (p - W.hub_base[lo]) * W.hub_chunk;
+  ee = min(eb + W.hub_chunk, W.off[v + 1]);
 }
 
 template <int NW>
@@ -425,6 +431,8 @@ __global__ void __launch_bounds__(CTA_THREADS) k_bc_graphs(GraphsArgs a) {
   W.off = a.off;
   W.adj = a.adj;
   W.hub_cap = 0;
+  W.hub_deg = bc::HUB_DEG;
+  W.hub_chunk = bc::HUB_CHUNK;
   W.hub_ent = W.hub_base = nullptr;
   W.hub_cnt = nullptr;
   W.dacc = nullptr;
@@ -508,6 +516,9 @@ struct BcPlan {
   dbuf<int> err;
 };
 
+int bc_hub_deg_default() { return bc::HUB_DEG; }
+int bc_hub_chunk_default() { return bc::HUB_CHUNK; }
+
 void free_bc_plan(BcPlan* p) { delete p; }
 
 static int bc_grid(sp_graph* g, const int32_t* d_srcs, int nsrc, int batch_hint, int32_t* lvl_out = nullptr,
@@ -569,6 +580,8 @@ static int bc_grid(sp_graph* g, const int32_t* d_srcs, int nsrc, int batch_hint,
   W.hub_base = p->hub_base.p;
   W.hub_cnt = p->hub_cnt.p;
   W.hub_cap = hub_cap;
+  W.hub_deg = g->bc_hub_deg > 0 ? g->bc_hub_deg : bc::HUB_DEG;
+  W.hub_chunk = g->bc_hub_chunk > 0 ? g->bc_hub_chunk : bc::HUB_CHUNK;
   W.dacc = p->dacc.p;
   a.srcs = d_srcs;
   a.nsrc = nsrc;

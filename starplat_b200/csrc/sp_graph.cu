@@ -548,6 +548,22 @@ int sp_tune_set(sp_graph_h g, const char* key, int64_t value) {
     g->sssp_ctas_per_sm = (int32_t)value;
     return SP_OK;
   }
+  if (!strcmp(key, "bc.hub_deg")) {
+    if (value < 0 || value > (1 << 30)) {
+      set_error("sp_tune_set: bc.hub_deg must be in [0, 2^30]");
+      return SP_ERR_INVALID;
+    }
+    g->bc_hub_deg = (int32_t)value;
+    return SP_OK;
+  }
+  if (!strcmp(key, "bc.hub_chunk")) {
+    if (value < 0 || value > (1 << 20)) {
+      set_error("sp_tune_set: bc.hub_chunk must be in [0, 2^20]");
+      return SP_ERR_INVALID;
+    }
+    g->bc_hub_chunk = (int32_t)value;
+    return SP_OK;
+  }
   if (!strcmp(key, "tc.cta_warps")) {
     if (value != 0 && value != 2 && value != 4 && value != 8 && value != 16) {
       set_error("sp_tune_set: tc.cta_warps must be 0, 2, 4, 8 or 16");
@@ -595,6 +611,14 @@ int sp_tune_get(sp_graph_h g, const char* key, int64_t* value) {
   }
   if (!strcmp(key, "sssp.last_ctas")) {
     *value = g->sssp_last_ctas;
+    return SP_OK;
+  }
+  if (!strcmp(key, "bc.hub_deg")) {
+    *value = g->bc_hub_deg > 0 ? g->bc_hub_deg : bc_hub_deg_default();
+    return SP_OK;
+  }
+  if (!strcmp(key, "bc.hub_chunk")) {
+    *value = g->bc_hub_chunk > 0 ? g->bc_hub_chunk : bc_hub_chunk_default();
     return SP_OK;
   }
   if (!strcmp(key, "tc.cta_warps")) {

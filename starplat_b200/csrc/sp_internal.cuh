@@ -157,7 +157,9 @@ struct sp_graph {
   int64_t sssp_last_delta = 0;   // schedule of the last SSSP call (reporting)
   int32_t sssp_last_ctas = 0;
   int32_t tc_cta_warps = -1;  // TC: warps per CTA of the shared-bitmap kernel (-1 = default, 0 = off)
-  int32_t bc_batch = 0;    // BC sources per multi-source batch (0 = 64)
+  int32_t bc_batch = 0;
+  int32_t bc_hub_deg = 0;  // BC: split level-list entries above this degree (0 = default)
+  int32_t bc_hub_chunk = 0;  // BC: edges per piece of a split entry (0 = default)    // BC sources per multi-source batch (0 = 64)
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   sp::PrPlan* pr = nullptr;
@@ -173,6 +175,8 @@ int ensure_emap(sp_graph* g);         // builds emap (edgeMap) on device if miss
 int finish_graph(sp_graph* g);        // checks a library-built CSR, sets max_out_deg
 int pr_order_default();               // PageRank vertex order default (sp_pagerank.cu)
 int tc_cta_warps_default();           // TC kernel choice default (sp_tc.cu)
+int bc_hub_deg_default();             // BC entry-splitting defaults (sp_bc.cu)
+int bc_hub_chunk_default();
 int ensure_symmetry(sp_graph* g);     // fills g->symmetric
 int copy_out(void* dst, const void* src, size_t bytes, cudaStream_t s);  // host or device dst
 int num_sms();

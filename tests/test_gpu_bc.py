@@ -50,6 +50,26 @@ def test_bc_batch_knob(batch):
     assert_bc_close(out, O.bc(g.indexofNodes, g.edgeList, srcs))
 
 
+@pytest.mark.parametrize("hub_deg,chunk", [(4096, 256), (64, 64), (1, 1), (1, 7), (16, 1000)])
+def test_bc_entry_splitting_knobs(hub_deg, chunk):
+    # how level-list entries are cut into shared pieces changes the work split, not the
+    # result: BC within the tolerance, BFS levels and sigma exact
+    for g in (G.rmat(12, 16, seed=4), star(300, directed_in=False), G.grid(9, 11)):
+        srcs = G.pick_sources(g, 70, seed=1, min_out_degree=0)
+        dg = device_graph(g)
+        dg.tune_set("bc.hub_deg", hub_deg)
+        dg.tune_set("bc.hub_chunk", chunk)
+        assert (dg.tune_get("bc.hub_deg"), dg.tune_get("bc.hub_chunk")) == (hub_deg, chunk)
+        out = dg.bc(srcs)
+        lvl, sig = dg.bfs_sigma(srcs[:64])
+        dg.tune_set("bc.hub_deg", 0)
+        dg.tune_set("bc.hub_chunk", 0)
+        assert_bc_close(out, O.bc(g.indexofNodes, g.edgeList, srcs), g.name)
+        for k, s in enumerate(srcs[:64]):
+            rl, rs, _ = O.bfs_sigma(g.indexofNodes, g.edgeList, int(s))
+            assert np.array_equal(lvl[k], rl) and np.array_equal(sig[k], rs)
+
+
 def test_bc_all_sources_small_graphs():
     # the reference driver passes every vertex as a source (bc_dslV2main.cpp:50-53)
     for g in (clique(10), path(40), star(50, directed_in=False), G.grid(7, 9)):
