@@ -102,6 +102,9 @@ int sp_graph_info(sp_graph_h g, int32_t* V, int64_t* E, int32_t* symmetric);
  *   "sssp.last_delta", "sssp.last_ctas" (read only): the schedule the last SSSP call ran.
  *   "tc.cta_warps"  TC on graphs of up to 65536 vertices: 0 = a bitmap per warp;
  *             2, 4, 8 or 16 = one bitmap per CTA of that many warps sharing each anchor.
+ *   "sssp.hub_deg", "sssp.hub_chunk"  SSSP: queued vertices with more out-edges than
+ *             hub_deg are relaxed in hub_chunk-edge pieces shared by all warps
+ *             (defaults 128 and 64).
  *   "bc.hub_deg", "bc.hub_chunk"  BC: level-list entries of vertices with more than
  *             hub_deg edges are cut into hub_chunk-edge pieces shared by all warps
  *             (defaults 64 and 64).

@@ -548,6 +548,17 @@ int sp_tune_set(sp_graph_h g, const char* key, int64_t value) {
     g->sssp_ctas_per_sm = (int32_t)value;
     return SP_OK;
   }
+  if (!strcmp(key, "sssp.hub_deg") || !strcmp(key, "sssp.hub_chunk")) {
+    if (value < 0 || value > (1 << 30)) {
+      set_error("sp_tune_set: %s must be in [0, 2^30]", key);
+      return SP_ERR_INVALID;
+    }
+    if (!strcmp(key, "sssp.hub_deg"))
+      g->sssp_hub_deg = (int32_t)value;
+    else
+      g->sssp_hub_chunk = (int32_t)value;
+    return SP_OK;
+  }
   if (!strcmp(key, "bc.hub_deg")) {
     if (value < 0 || value > (1 << 30)) {
       set_error("sp_tune_set: bc.hub_deg must be in [0, 2^30]");
@@ -611,6 +622,14 @@ int sp_tune_get(sp_graph_h g, const char* key, int64_t* value) {
   }
   if (!strcmp(key, "sssp.last_ctas")) {
     *value = g->sssp_last_ctas;
+    return SP_OK;
+  }
+  if (!strcmp(key, "sssp.hub_deg")) {
+    *value = g->sssp_hub_deg > 0 ? g->sssp_hub_deg : sssp_hub_deg_default();
+    return SP_OK;
+  }
+  if (!strcmp(key, "sssp.hub_chunk")) {
+    *value = g->sssp_hub_chunk > 0 ? g->sssp_hub_chunk : sssp_hub_chunk_default();
     return SP_OK;
   }
   if (!strcmp(key, "bc.hub_deg")) {

@@ -34,8 +34,12 @@ namespace sp {
 namespace ss {
 constexpr int THREADS = 256;
 constexpr int LANE_DEG = 16;   // frontier vertices up to this out-degree are walked by one lane
-constexpr int HUB_DEG = 2048;  // above this a vertex is relaxed in HUB_CHUNK pieces by many warps
-constexpr int HUB_CHUNK = 256;
+// Queued vertices above HUB_DEG out-edges are relaxed in HUB_CHUNK-edge pieces that
+// every warp shares, so no warp walks a long row alone while the others wait at the
+// round's barrier. R-MAT 23 (learned schedule): 12.6 ms at (2048, 256), 11.5 at
+// (512, 128), 11.2 at (128, 64), 12.0 at (32, 32).
+constexpr int HUB_DEG = 128;
+constexpr int HUB_CHUNK = 64;
 
 struct Ctl {
   GridBar bar;
@@ -64,6 +68,8 @@ struct Args {
   int V;
   long long delta;      // bucket width; >= INT_MAX means a single bucket
   long long max_rounds;
+  int hub_deg;          // vertices with more out-edges are relaxed in pieces by all warps
+  int hub_chunk;        // edges per piece
 };
 
 // Warp-aggregated append of `want` lanes into buf via counter.
@@ -86,9 +92,9 @@ __device__ __forceinline__ void queue_push(const Args& a, bool want, int u, int3
   int nch = 0;
   if (want) {
     const int d = a.off[u + 1] - a.off[u];
-    if (d > HUB_DEG) {
+    if (d > a.hub_deg) {
       hub = true;
-      nch = (d + HUB_CHUNK - 1) / HUB_CHUNK;
+      nch = (d + a.hub_chunk - 1) / a.hub_chunk;
     }
   }
   if (hub) {
@@ -190,7 +196,7 @@ __global__ void __launch_bounds__(THREADS) k_delta(Args a) {
           }
         }
       }
-      // hub pieces of this round: HUB_CHUNK edges per warp, all warps
+      // hub pieces of this round: hub_chunk edges per warp, all warps
       {
         const int32_t* HVc = a.hv[round & 1];
         const int32_t* HBc = a.hbase[round & 1];
@@ -202,8 +208,8 @@ __global__ void __launch_bounds__(THREADS) k_delta(Args a) {
           }
           const int v = HVc[lo];
           const long long vd = __ldcg(a.dist + v);
-          const int vb = a.off[v] + (ch - HBc[lo]) * HUB_CHUNK;
-          const int ve = min(vb + HUB_CHUNK, a.off[v + 1]);
+          const int vb = a.off[v] + (ch - HBc[lo]) * a.hub_chunk;
+          const int ve = min(vb + a.hub_chunk, a.off[v + 1]);
           for (int k0 = vb; k0 < ve; k0 += 32) {
             const int k = k0 + lane;
             int res = 0, u = 0;
@@ -278,7 +284,7 @@ __global__ void __launch_bounds__(THREADS) k_delta(Args a) {
 }
 
 __global__ void k_init(int V, int src, int32_t* dist, int32_t* qstamp, int32_t* fstamp, int32_t* q0, int32_t* hv0,
-                       int32_t* hb0, const int32_t* __restrict__ off, Ctl* c) {
+                       int32_t* hb0, const int32_t* __restrict__ off, Ctl* c, int hub_deg, int hub_chunk) {
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
     dist[v] = v == src ? 0 : INT_MAX;
     qstamp[v] = -1;
@@ -293,10 +299,10 @@ __global__ void k_init(int V, int src, int32_t* dist, int32_t* qstamp, int32_t* 
       c->hcount[k] = 0ull;
     }
     const int d = off[src + 1] - off[src];
-    if (d > HUB_DEG) {
+    if (d > hub_deg) {
       hv0[0] = src;
       hb0[0] = 0;
-      c->hcount[0] = (1ull << 32) | (unsigned long long)((d + HUB_CHUNK - 1) / HUB_CHUNK);
+      c->hcount[0] = (1ull << 32) | (unsigned long long)((d + hub_chunk - 1) / hub_chunk);
     } else {
       q0[0] = src;
       c->qcount[0] = 1;
@@ -370,6 +376,8 @@ struct SsspPlan {
 };
 
 void free_sssp_plan(SsspPlan* p) { delete p; }
+int sssp_hub_deg_default() { return ss::HUB_DEG; }
+int sssp_hub_chunk_default() { return ss::HUB_CHUNK; }
 
 static int sssp_prepare(sp_graph* g, const int32_t* weight, const int32_t** wdev) {
   if (!g->sssp) g->sssp = new SsspPlan();
@@ -465,8 +473,10 @@ static int sssp_delta(sp_graph* g, const int32_t* w, int32_t src, int32_t* dist_
   // Bellman-Ford needs at most V-1 rounds of improvement per vertex chain; far more
   // rounds than V * 4 + 64 can only come from a negative cycle.
   a.max_rounds = (long long)V * 4 + 64;
+  a.hub_deg = g->sssp_hub_deg > 0 ? g->sssp_hub_deg : ss::HUB_DEG;
+  a.hub_chunk = g->sssp_hub_chunk > 0 ? g->sssp_hub_chunk : ss::HUB_CHUNK;
   ss::k_init<<<num_sms() * 4, 256, 0, s>>>(V, src, p->dist.p, p->qstamp.p, p->fstamp.p, p->q0.p, p->h0.p, p->hb0.p,
-                                            g->off.p, p->ctl.p);
+                                            g->off.p, p->ctl.p, a.hub_deg, a.hub_chunk);
   SP_CHECK_LAUNCH();
   int per_sm = 0;
   SP_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ss::k_delta, ss::THREADS, 0));

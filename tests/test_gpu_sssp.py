@@ -53,6 +53,21 @@ def test_sssp_any_delta_is_exact(delta):
     check(gg, 0, delta=delta)
 
 
+@pytest.mark.parametrize("hub_deg,chunk", [(2048, 256), (128, 64), (1, 1), (3, 1000), (0, 0)])
+def test_sssp_hub_splitting_knobs_keep_distances_exact(hub_deg, chunk):
+    from graphs import star
+
+    for g in (weighted(G.rmat(13, 16, seed=8, directed=True), 1, 100), weighted(star(5000, directed_in=False), 1, 9),
+              weighted(G.grid(40, 50), 1, 1000)):
+        dg = device_graph(g)
+        dg.tune_set("sssp.hub_deg", hub_deg)
+        dg.tune_set("sssp.hub_chunk", chunk)
+        for src in (0, g.V // 2):
+            check(g, src)
+        dg.tune_set("sssp.hub_deg", 0)
+        dg.tune_set("sssp.hub_chunk", 0)
+
+
 def test_sssp_tuned_delta_knob():
     g = weighted(G.grid(30, 30), 1, 1000)
     dg = device_graph(g)
