@@ -22,7 +22,11 @@
 //    bin: one warp with a 128-slot table (degree <= 64), one CTA with a table of
 //    up to 16384 slots in dynamic shared memory (degree <= 8192), one CTA with a
 //    table in global scratch above that; FP64 values, shared-memory atomics;
-//  * tot_c, in_c and Q reduced with FP64 atomics (exact for integer weights);
+//  * vertices binned by degree class and by sub-sweep parity, so a sub-sweep's
+//    kernels read only the vertices that may move in it;
+//  * tot_c with FP64 atomics aggregated per warp over lanes of one community (exact
+//    for integer weights); Q from the total internal weight (a CTA reduction) and
+//    the tot_c;
 //  * aggregation: communities renumbered densely, external edges emitted at scan
 //    positions, sorted by (c_u, c_v) with a radix sort and merged with a reduce-by-key.
 #include <cub/cub.cuh>
@@ -120,7 +124,6 @@ __global__ void __launch_bounds__(THREADS) k_move_warp(MoveArgs a) {
   const int gw = (blockIdx.x * THREADS + threadIdx.x) >> 5, nw = (gridDim.x * THREADS) >> 5;
   for (int i = gw; i < a.nlist; i += nw) {
     const int v = a.list[i];
-    if ((int)(hmix((unsigned)v) & 1u) != a.parity) continue;
     const int cv = a.comm[v];
     const double kv = a.kv[v];
     const int b = a.L.off[v], e = a.L.off[v + 1];
@@ -198,7 +201,6 @@ __global__ void __launch_bounds__(THREADS) k_move_cta(MoveArgs a, int slots) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for (int i = blockIdx.x; i < a.nlist; i += gridDim.x) {
     const int v = a.list[i];
-    if ((int)(hmix((unsigned)v) & 1u) != a.parity) continue;
     const int b = a.L.off[v], e = a.L.off[v + 1];
     int nslots = slots;
     double* vals;
@@ -296,36 +298,57 @@ __global__ void k_apply(int n, int parity, int32_t* comm, const int32_t* __restr
   if ((threadIdx.x & 31) == 0 && local) atomicAdd(moved, local);
 }
 
+// tot_c = sum of k_v and csize_c = members, per community. Lanes of a warp that hold
+// the same community add up first (members of a community are mostly neighbours in
+// the vertex order), so the hot communities see one atomic per group, not per vertex.
 __global__ void k_tot(int n, const int32_t* __restrict__ comm, const double* __restrict__ kv, double* tot,
                       int32_t* csize) {
-  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-    atomicAdd(&tot[comm[v]], kv[v]);
-    atomicAdd(&csize[comm[v]], 1);
+  const int lane = threadIdx.x & 31;
+  const int n32 = (n + 31) & ~31;  // every lane of a warp runs the same iterations
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n32; v += gridDim.x * blockDim.x) {
+    const bool on = v < n;
+    const int c = on ? comm[v] : -1 - lane;  // idle lanes: keys no real community has
+    const double k = on ? kv[v] : 0.0;
+    const unsigned grp = __match_any_sync(0xffffffffu, c);
+    double sum = 0.0;
+    for (unsigned m = grp; m; m &= m - 1) sum += __shfl_sync(grp, k, __ffs(m) - 1);
+    if (on && lane == __ffs(grp) - 1) {
+      atomicAdd(&tot[c], sum);
+      atomicAdd(&csize[c], __popc(grp));
+    }
   }
 }
 
-// in_c (directed internal weight + self loops) per community, then Q
-__global__ void k_internal(Level L, const int32_t* __restrict__ comm, double* in) {
+// Q = sum_c in_c / W - (tot_c / W)^2 needs only the total internal weight
+// sum_c in_c = sum_v (weight of v's edges inside its community + its self-loop):
+// one partial per CTA, no per-community atomics; the host adds the partials of both
+// kernels in CTA order, so Q is the same on every run.
+__global__ void __launch_bounds__(THREADS) k_internal(Level L, const int32_t* __restrict__ comm, double W,
+                                                      double* q) {
+  __shared__ double s_red[THREADS / 32];
   const int lane = threadIdx.x & 31;
+  double acc = 0;
   for (int v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < L.n; v += (gridDim.x * blockDim.x) >> 5) {
     const int cv = comm[v];
     double s = 0;
     for (int j = L.off[v] + lane; j < L.off[v + 1]; j += 32)
       if (comm[L.adj[j]] == cv) s += L.w[j];
     s = warp_sum(s);
-    if (lane == 0 && (s != 0.0 || L.sl[v] != 0.0)) atomicAdd(&in[cv], s + L.sl[v]);
+    if (lane == 0) acc += s + L.sl[v];
   }
+  acc = block_sum<THREADS>(acc, s_red);
+  if (threadIdx.x == 0) q[blockIdx.x] = acc / W;
 }
 
-__global__ void k_q(int n, const double* __restrict__ in, const double* __restrict__ tot, double W, double* q) {
+__global__ void k_q(int n, const double* __restrict__ tot, double W, double* q) {
   __shared__ double s_red[THREADS / 32];
   double acc = 0;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
     const double t = tot[c] / W;
-    acc += in[c] / W - t * t;
+    acc -= t * t;
   }
   acc = block_sum<THREADS>(acc, s_red);
-  if (threadIdx.x == 0) atomicAdd(q, acc);
+  if (threadIdx.x == 0) q[blockIdx.x] = acc;
 }
 
 // ---- aggregation
@@ -390,12 +413,15 @@ __global__ void k_f2d(const float* __restrict__ a, double* b, int64_t n) {
     b[i] = a ? (double)a[i] : 1.0;
 }
 
+// Vertex lists per (degree class, sub-sweep parity): list 2 * b + parity, b = 0 warp,
+// 1 CTA, 2 CTA with a global table; each list holds at most cap entries.
 __global__ void k_bins(int n, const int32_t* __restrict__ off, int32_t* lists, int* counts, int cap) {
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
     const int d = off[v + 1] - off[v];
     const int b = d <= WARP_DEG ? 0 : (d <= CTA_DEG ? 1 : 2);
-    const int p = atomicAdd(&counts[b], 1);
-    lists[(size_t)b * cap + p] = v;
+    const int k = 2 * b + (int)(hmix((unsigned)v) & 1u);
+    const int p = atomicAdd(&counts[k], 1);
+    lists[(size_t)k * cap + p] = v;
   }
 }
 
@@ -406,7 +432,7 @@ struct LvPlan {
   dbuf<int32_t> off[2], adj[2];
   dbuf<double> w[2], sl[2];
   dbuf<int32_t> comm, newcomm, csize, used, newid, cnt, pos, orig, lists, rowcnt;
-  dbuf<double> kv, tot, in, scal;
+  dbuf<double> kv, tot, scal, qpart;
   dbuf<unsigned long long> keys, skeys, ukeys;
   dbuf<double> vals, svals, uvals;
   dbuf<int> icnt;
@@ -437,13 +463,18 @@ int read_int(const int* d, int* h, cudaStream_t s) { return copy_out(h, d, sizeo
 static int lv_modularity(LvPlan* p, const lv::Level& L, double W, cudaStream_t s, double* q) {
   const int n = L.n;
   const int g = num_sms() * 8;
-  SP_CHECK_CUDA(cudaMemsetAsync(p->in.p, 0, sizeof(double) * n, s));
-  SP_CHECK_CUDA(cudaMemsetAsync(p->scal.p, 0, sizeof(double), s));
-  lv::k_internal<<<g, 256, 0, s>>>(L, p->comm.p, p->in.p);
+  SP_TRY(p->qpart.alloc(2 * (size_t)g));
+  lv::k_internal<<<g, lv::THREADS, 0, s>>>(L, p->comm.p, W, p->qpart.p);
   SP_CHECK_LAUNCH();
-  lv::k_q<<<g, lv::THREADS, 0, s>>>(n, p->in.p, p->tot.p, W, p->scal.p);
+  lv::k_q<<<g, lv::THREADS, 0, s>>>(n, p->tot.p, W, p->qpart.p + g);
   SP_CHECK_LAUNCH();
-  return copy_out(q, p->scal.p, sizeof(double), s);
+  std::vector<double> part(2 * (size_t)g);
+  SP_TRY(copy_out(part.data(), p->qpart.p, sizeof(double) * part.size(), s));
+  double in = 0, sq = 0;
+  for (int i = 0; i < g; ++i) in += part[i];
+  for (int i = 0; i < g; ++i) sq += part[g + i];
+  *q = in + sq;
+  return SP_OK;
 }
 
 static int lv_recount(LvPlan* p, int n, cudaStream_t s) {
@@ -454,8 +485,10 @@ static int lv_recount(LvPlan* p, int n, cudaStream_t s) {
   return SP_OK;
 }
 
-// One sub-sweep over the vertices of one parity, all degree bins.
-static int lv_subsweep(LvPlan* p, lv::MoveArgs a, const int counts[3], int cap, int parity, bool plain,
+// One sub-sweep over the vertices of one parity, all degree bins. counts[2 * b + parity]
+// = entries of list (b, parity); the global tables of parity 1's big list follow
+// parity 0's in gtab_off.
+static int lv_subsweep(LvPlan* p, lv::MoveArgs a, const int counts[6], int cap, int parity, bool plain,
                        cudaStream_t s) {
   a.parity = parity;
   if (plain) {
@@ -465,24 +498,26 @@ static int lv_subsweep(LvPlan* p, lv::MoveArgs a, const int counts[3], int cap, 
     return SP_OK;
   }
   const int g = num_sms() * 8;
-  if (counts[0]) {
-    a.list = p->lists.p;
-    a.nlist = counts[0];
+  auto list = [&](int b) { return p->lists.p + (size_t)(2 * b + parity) * cap; };
+  if (counts[0 + parity]) {
+    a.list = list(0);
+    a.nlist = counts[0 + parity];
     lv::k_move_warp<<<g, lv::THREADS, 0, s>>>(a);
     SP_CHECK_LAUNCH();
   }
-  if (counts[1]) {
-    a.list = p->lists.p + cap;
-    a.nlist = counts[1];
+  if (counts[2 + parity]) {
+    a.list = list(1);
+    a.nlist = counts[2 + parity];
     const int slots = lv::CTA_SLOTS_MAX;  // degree <= 8192 fits at load factor <= 1/2
     const size_t dyn = (size_t)slots * (sizeof(double) + sizeof(int32_t));
     SP_CHECK_CUDA(cudaFuncSetAttribute(lv::k_move_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
     lv::k_move_cta<false><<<num_sms(), lv::THREADS, dyn, s>>>(a, slots);
     SP_CHECK_LAUNCH();
   }
-  if (counts[2]) {
-    a.list = p->lists.p + 2 * (size_t)cap;
-    a.nlist = counts[2];
+  if (counts[4 + parity]) {
+    a.list = list(2);
+    a.nlist = counts[4 + parity];
+    a.gtab_off = p->goff.p + (parity ? counts[4] : 0);
     lv::k_move_cta<true><<<num_sms() * 2, lv::THREADS, 0, s>>>(a, 0);
     SP_CHECK_LAUNCH();
   }
@@ -536,13 +571,12 @@ extern "C" int sp_louvain(sp_graph_h g, const float* weight, double threshold, i
   SP_TRY(p->cnt.alloc(n0 + 1));
   SP_TRY(p->pos.alloc(n0 + 1));
   SP_TRY(p->orig.alloc(n0));
-  SP_TRY(p->lists.alloc((size_t)3 * n0));
+  SP_TRY(p->lists.alloc((size_t)6 * n0));
   SP_TRY(p->rowcnt.alloc(n0 + 1));
   SP_TRY(p->kv.alloc(n0));
   SP_TRY(p->tot.alloc(n0));
-  SP_TRY(p->in.alloc(n0));
   SP_TRY(p->scal.alloc(2));
-  SP_TRY(p->icnt.alloc(4));
+  SP_TRY(p->icnt.alloc(8));
   lv::k_init_comm<<<gs, 256, 0, s>>>(n0, p->orig.p, p->newcomm.p);  // orig[v] = v
   SP_CHECK_LAUNCH();
 
@@ -584,24 +618,28 @@ extern "C" int sp_louvain(sp_graph_h g, const float* weight, double threshold, i
     if (first) qcur = qlev0;
     first = false;
     // degree bins
-    SP_CHECK_CUDA(cudaMemsetAsync(p->icnt.p, 0, sizeof(int) * 4, s));
+    SP_CHECK_CUDA(cudaMemsetAsync(p->icnt.p, 0, sizeof(int) * 6, s));
     lv::k_bins<<<gs, 256, 0, s>>>(n, L.off, p->lists.p, p->icnt.p, n0);
     SP_CHECK_LAUNCH();
-    int counts[4];
-    SP_TRY(copy_out(counts, p->icnt.p, sizeof(int) * 4, s));
-    if (counts[2] && !plain) {
-      // global tables for the highest-degree vertices: 2 * degree slots (power of two)
-      std::vector<int32_t> big(counts[2]);
-      SP_TRY(copy_out(big.data(), p->lists.p + 2 * (size_t)n0, sizeof(int32_t) * counts[2], s));
+    int counts[6];
+    SP_TRY(copy_out(counts, p->icnt.p, sizeof(int) * 6, s));
+    const int nbig = counts[4] + counts[5];
+    if (nbig && !plain) {
+      // global tables for the highest-degree vertices (both parities' lists, in that
+      // order): 2 * degree slots, a power of two
+      std::vector<int32_t> big(nbig);
+      if (counts[4]) SP_TRY(copy_out(big.data(), p->lists.p + 4 * (size_t)n0, sizeof(int32_t) * counts[4], s));
+      if (counts[5])
+        SP_TRY(copy_out(big.data() + counts[4], p->lists.p + 5 * (size_t)n0, sizeof(int32_t) * counts[5], s));
       std::vector<int32_t> hoff(n + 1);
       SP_TRY(copy_out(hoff.data(), L.off, sizeof(int32_t) * (n + 1), s));
-      std::vector<int64_t> go(counts[2] + 1, 0);
-      for (int k = 0; k < counts[2]; ++k) {
+      std::vector<int64_t> go(nbig + 1, 0);
+      for (int k = 0; k < nbig; ++k) {
         int64_t d = hoff[big[k] + 1] - hoff[big[k]], sl = 1;
         while (sl < 2 * d) sl <<= 1;
         go[k + 1] = go[k] + sl;
       }
-      SP_TRY(p->goff.alloc(counts[2] + 1));
+      SP_TRY(p->goff.alloc(nbig + 1));
       SP_TRY(p->gval.alloc(go.back()));
       SP_TRY(p->gkey.alloc(go.back()));
       SP_CHECK_CUDA(cudaMemcpyAsync(p->goff.p, go.data(), sizeof(int64_t) * go.size(), cudaMemcpyHostToDevice, s));
@@ -621,8 +659,8 @@ extern "C" int sp_louvain(sp_graph_h g, const float* weight, double threshold, i
     for (int sweep = 0; sweep < max_sweeps; ++sweep) {
       for (int parity = 0; parity < 2; ++parity) {
         SP_TRY(lv_subsweep(p, a, counts, n0, parity, plain, s));
-        SP_CHECK_CUDA(cudaMemsetAsync(p->icnt.p + 3, 0, sizeof(int), s));
-        lv::k_apply<<<gs, 256, 0, s>>>(n, parity, p->comm.p, p->newcomm.p, p->icnt.p + 3);
+        SP_CHECK_CUDA(cudaMemsetAsync(p->icnt.p + 6, 0, sizeof(int), s));
+        lv::k_apply<<<gs, 256, 0, s>>>(n, parity, p->comm.p, p->newcomm.p, p->icnt.p + 6);
         SP_CHECK_LAUNCH();
         SP_TRY(lv_recount(p, n, s));
       }
