@@ -18,10 +18,11 @@
 //    from the same snapshot; two sub-sweeps per sweep (vertex hash parity) and the
 //    singleton rule (a singleton moves to another singleton only if that label is
 //    smaller) keep neighbours from swapping back and forth;
-//  * per-vertex neighbour-community weights in shared-memory hash tables by degree
-//    bin: one warp with a 128-slot table (degree <= 64), one CTA with a table of
-//    up to 16384 slots in dynamic shared memory (degree <= 8192), one CTA with a
-//    table in global scratch above that; FP64 values, shared-memory atomics;
+//  * per-vertex neighbour-community weights by degree bin: up to 64 edges, one warp
+//    with no table (lanes holding one community found by __match_any_sync and summed
+//    by shuffles); up to 8192, one CTA with a hash table of up to 16384 slots in
+//    dynamic shared memory; above that, one CTA with a table in global scratch; FP64
+//    values, shared-memory atomics in the tables;
 //  * vertices binned by degree class and by sub-sweep parity, so a sub-sweep's
 //    kernels read only the vertices that may move in it;
 //  * tot_c with FP64 atomics aggregated per warp over lanes of one community (exact
@@ -42,7 +43,6 @@ namespace sp {
 namespace lv {
 constexpr int THREADS = 256;
 constexpr int WARP_DEG = 64;
-constexpr int WARP_SLOTS = 128;
 constexpr int CTA_DEG = 8192;
 constexpr int CTA_SLOTS_MAX = 16384;
 constexpr int EMPTY = -1;
@@ -110,38 +110,67 @@ __device__ __forceinline__ int decide(const MoveArgs& a, int v, int cv, double k
   return best_c;
 }
 
+// Weight of the community c, summed over the lanes of grp (the lanes holding c) in
+// lane order; every lane of grp gets the sum.
+__device__ __forceinline__ double group_sum(unsigned grp, double w) {
+  double s = 0.0;
+  for (unsigned m = grp; m; m &= m - 1) s += __shfl_sync(grp, w, __ffs(m) - 1);
+  return s;
+}
+
+// One warp per vertex of degree <= 64 (= WARP_DEG), no tables: a lane holds one
+// neighbour per 32-edge round; __match_any_sync groups the lanes holding the same
+// community and the group sums its weights in lane order; a round-1 group adds into
+// the round-0 group of the same community, or stands as a candidate of its own. Every
+// distinct neighbour community is scored once, with the tables' gain and tie-break.
 __global__ void __launch_bounds__(THREADS) k_move_warp(MoveArgs a) {
-  __shared__ int32_t s_key[THREADS / 32][WARP_SLOTS];
-  __shared__ double s_val[THREADS / 32][WARP_SLOTS];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  int32_t* keys = s_key[wid];
-  double* vals = s_val[wid];
-  for (int i = lane; i < WARP_SLOTS; i += 32) {
-    keys[i] = EMPTY;
-    vals[i] = 0.0;
-  }
-  __syncwarp();
+  const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * THREADS + threadIdx.x) >> 5, nw = (gridDim.x * THREADS) >> 5;
   for (int i = gw; i < a.nlist; i += nw) {
     const int v = a.list[i];
     const int cv = a.comm[v];
     const double kv = a.kv[v];
     const int b = a.L.off[v], e = a.L.off[v + 1];
-    for (int j = b + lane; j < e; j += 32) tab_add(keys, vals, WARP_SLOTS - 1, a.comm[a.L.adj[j]], a.L.w[j]);
-    __syncwarp();
+    const int j0 = b + lane, j1 = b + 32 + lane;
+    const bool on0 = j0 < e, on1 = j1 < e;
+    const int c0 = on0 ? a.comm[a.L.adj[j0]] : -1 - lane;  // idle lanes: keys no community has
+    const double w0 = on0 ? a.L.w[j0] : 0.0;
+    const unsigned g0 = __match_any_sync(0xffffffffu, c0);
+    double s0 = group_sum(g0, w0);
+    const bool lead0 = on0 && lane == __ffs(g0) - 1;
+    bool cand1 = false;
+    int c1 = -1;
+    double s1 = 0.0;
+    if (e - b > 32) {  // the same for the whole warp
+      c1 = on1 ? a.comm[a.L.adj[j1]] : -33 - lane;
+      const double w1 = on1 ? a.L.w[j1] : 0.0;
+      const unsigned g1 = __match_any_sync(0xffffffffu, c1);
+      s1 = group_sum(g1, w1);
+      cand1 = on1 && lane == __ffs(g1) - 1;
+      unsigned leads = __ballot_sync(0xffffffffu, cand1);
+      while (leads) {
+        const int l = __ffs(leads) - 1;
+        leads &= leads - 1;
+        const int cl = __shfl_sync(0xffffffffu, c1, l);
+        const double sl = __shfl_sync(0xffffffffu, s1, l);
+        const bool hit = lead0 && c0 == cl;
+        if (hit) s0 += sl;
+        if (__any_sync(0xffffffffu, hit) && lane == l) cand1 = false;
+      }
+    }
     double bg = -INFINITY;
     int bc = -1;
-    for (int s = lane; s < WARP_SLOTS; s += 32) {
-      const int c = keys[s];
-      if (c != EMPTY) {
-        const double tc = (c == cv) ? a.tot[c] - kv : a.tot[c];
-        const double gain = vals[s] - tc * kv / a.W;
-        if (bc < 0 || better(gain, c, bg, bc, cv)) {
-          bg = gain;
-          bc = c;
-        }
-        keys[s] = EMPTY;
-        vals[s] = 0.0;
+    if (lead0) {
+      const double tc = (c0 == cv) ? a.tot[c0] - kv : a.tot[c0];
+      bg = s0 - tc * kv / a.W;
+      bc = c0;
+    }
+    if (cand1) {
+      const double tc = (c1 == cv) ? a.tot[c1] - kv : a.tot[c1];
+      const double gain = s1 - tc * kv / a.W;
+      if (bc < 0 || better(gain, c1, bg, bc, cv)) {
+        bg = gain;
+        bc = c1;
       }
     }
 #pragma unroll
@@ -154,7 +183,6 @@ __global__ void __launch_bounds__(THREADS) k_move_warp(MoveArgs a) {
       }
     }
     if (lane == 0) a.newcomm[v] = decide(a, v, cv, kv, bg, bc);
-    __syncwarp();
   }
 }
 
