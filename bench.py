@@ -347,12 +347,12 @@ def bench_bc(steps, warmup, stream, hbm, cpu, nsrc=256):
     return out
 
 
-def bench_bc_er(steps, warmup, stream, hbm, cpu):
+def bench_bc_er(steps, warmup, stream, hbm, cpu, ngraphs=1000):
     from starplat_b200 import generators as G
     from starplat_b200.device import DeviceGraph
 
     t0 = time.time()
-    gs = G.er_batch(1000, 1000, 50000, 8, 32, seed=11)
+    gs = G.er_batch(1000, 1000, 50000, 8, 32, seed=11)[:ngraphs]
     voff = np.zeros(len(gs) + 1, np.int64)
     eoff = np.zeros(len(gs) + 1, np.int64)
     for k, g in enumerate(gs):
@@ -377,7 +377,7 @@ def bench_bc_er(steps, warmup, stream, hbm, cpu):
     voff32 = voff.astype(np.int32)
     gen_s = time.time() - t0
     alg = int(16 * er_tot + 32 * sum(g.V * 16 for g in gs))
-    out = {"workload": "bc 1000 ER graphs, n log-uniform in [1e3, 5e4], degree U[8,32], 16 sources each, seed11",
+    out = {"workload": f"bc {len(gs)} ER graphs, n log-uniform in [1e3, 5e4], degree U[8,32], 16 sources each, seed11",
            "V": V, "E": E, "sources": int(srcs.shape[0]), "sum_E_r": er_tot, "graph_gen_s": round(gen_s, 1)}
     with DeviceGraph(off, adj, None, off, adj) as dg:
         dg.set_stream(stream)
@@ -387,7 +387,7 @@ def bench_bc_er(steps, warmup, stream, hbm, cpu):
     from starplat_b200 import _lib
 
     ms_plain, er_plain = 0.0, 0
-    for k in range(0, 1000, 50):
+    for k in range(0, len(gs), 50):
         with DeviceGraph.from_csr(gs[k], with_weights=False) as dgk:
             dgk.set_stream(stream)
             s_k = (srcs[soff[k]:soff[k + 1]] - voff32[k]).astype(np.int32)
@@ -403,7 +403,7 @@ def bench_bc_er(steps, warmup, stream, hbm, cpu):
         nt = O.num_threads()
         t = time.perf_counter()
         er_s = 0
-        for k in range(0, 1000, 50):
+        for k in range(0, len(gs), 50):
             g = gs[k]
             O.bc_omp(g.indexofNodes, g.edgeList, srcs[soff[k]:soff[k + 1]] - voff32[k], nthreads=nt)
             er_s += er_k[k]
@@ -547,7 +547,7 @@ def run_extras(want, args, stream, hbm, cpu_ok):
     if "bc_rmat20" in want:
         guarded("bc_rmat20", lambda: bench_bc(max(1, ks // 2), 1, stream, hbm, cpu_ok, args.sources))
     if "bc_er1000" in want:
-        guarded("bc_er1000", lambda: bench_bc_er(max(1, ks // 2), 1, stream, hbm, cpu_ok))
+        guarded("bc_er1000", lambda: bench_bc_er(max(1, ks // 2), 1, stream, hbm, cpu_ok, args.graphs))
     if "louvain_sbm1m" in want:
         guarded("louvain_sbm1m", lambda: bench_louvain(max(1, ks // 2), 1, stream, hbm, cpu_ok))
     if "ingest_rmat20" in want:
@@ -571,6 +571,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="headline PageRank only")
     ap.add_argument("--scale", type=int, default=PR_SCALE, help="R-MAT scale of the PageRank graph")
     ap.add_argument("--tune", action="append", default=[], help="schedule knob key=value (sp_tune_set)")
+    ap.add_argument("--graphs", type=int, default=1000,
+                    help="ER graphs of the bc_er1000 workload (1000 = the config; fewer for profiler runs)")
     ap.add_argument("--sources", type=int, default=256,
                     help="BC sources of the bc_rmat20 workload (256 = the config; fewer for profiler runs)")
     ap.add_argument("--algo-only", default="", help="run only these extra workloads (comma list), no headline: "

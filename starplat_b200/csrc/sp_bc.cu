@@ -29,6 +29,8 @@
 // One cooperative launch runs every batch of a graph (bounded grid barriers); the
 // many-small-graphs form runs one CTA per graph in a persistent launch with a
 // work queue (largest graphs first) and block-level barriers.
+#include <cooperative_groups.h>
+
 #include <climits>
 #include <vector>
 
@@ -36,6 +38,8 @@
 #include "sp_sync.cuh"
 
 namespace sp {
+
+namespace cg = cooperative_groups;
 
 namespace bc {
 constexpr int GRID_THREADS = 256;
@@ -46,6 +50,7 @@ constexpr int CTA_THREADS = 512;
 // 121 at (128, 256), 110 at (64, 64).
 constexpr int HUB_DEG = 64;
 constexpr int HUB_CHUNK = 64;
+constexpr int CLUSTER_DEFAULT = 1;  // CTAs per graph in the many-graphs form (bc.cluster)
 
 struct Work {
   const int32_t* __restrict__ off;  // CSR rows of this graph (global edge indices)
@@ -91,6 +96,17 @@ struct BlockSync {
   __device__ __forceinline__ int nthreads() const { return blockDim.x; }
 };
 
+// A thread-block cluster as one team: the hardware cluster barrier (release /
+// acquire at cluster scope, so global-memory writes before it are seen after it).
+struct ClusterSync {
+  __device__ __forceinline__ bool sync() {
+    cg::this_cluster().sync();
+    return true;
+  }
+  __device__ __forceinline__ int tid() const { return (int)cg::this_cluster().thread_rank(); }
+  __device__ __forceinline__ int nthreads() const { return (int)cg::this_cluster().num_threads(); }
+};
+
 __device__ __forceinline__ unsigned long long shfl64(unsigned long long x, int l) {
   unsigned lo = __shfl_sync(0xffffffffu, (unsigned)x, l);
   unsigned hi = __shfl_sync(0xffffffffu, (unsigned)(x >> 32), l);
@@ -131,8 +147,27 @@ __device__ __forceinline__ void hub_piece(const Work& W, int nh, int p, int& i, 
   ee = min(eb + W.hub_chunk, W.off[v + 1]);
 }
 
-template <int NW>
+// The next two edges with new (or successor) sources of a 32-edge chunk, for the
+// half-warp form (GS = 16): lanes 0-15 take the first, lanes 16-31 the second.
+__device__ __forceinline__ int half_pick(unsigned& em, int lane, int& from) {
+  const int l0 = __ffs(em) - 1;
+  em &= em - 1;
+  int l1 = -1;
+  if (em) {
+    l1 = __ffs(em) - 1;
+    em &= em - 1;
+  }
+  const int ml = lane < 16 ? l0 : l1;
+  from = ml >= 0 ? ml : l0;
+  return ml;
+}
+
+// GS = lanes per edge step: 32 (one lane per source bit, up to 32 * NW sources), or
+// 16 when the batch has at most 16 sources, so that the two half-warps take two
+// edges per step instead of leaving lanes 16-31 idle.
+template <int NW, int GS>
 __device__ void expand_entry(const Work& W, int i, int lane, int eb, int ee) {
+  static_assert(GS == 32 || (GS == 16 && NW == 1), "half-warp steps hold up to 16 sources");
   constexpr int SW = 32 * NW;
   const int v = W.flv[i];
   const unsigned long long m = W.flm[i];
@@ -142,6 +177,7 @@ __device__ void expand_entry(const Work& W, int i, int lane, int eb, int ee) {
     const int b = lane + 32 * k;
     sv[k] = ((m >> b) & 1ull) ? W.sigma[(size_t)v * SW + b] : 0.0;
   }
+  const double svg = GS == 16 ? __shfl_sync(0xffffffffu, sv[0], lane & 15) : 0.0;
   for (int c = eb; c < ee; c += 32) {
     const int j = c + lane;
     int w = 0;
@@ -168,6 +204,15 @@ __device__ void expand_entry(const Work& W, int i, int lane, int eb, int ee) {
     }
     unsigned em = __ballot_sync(0xffffffffu, q != 0ull);
     while (em) {
+      if (GS == 16) {
+        int from;
+        const int ml = half_pick(em, lane, from);
+        const unsigned long long qm = shfl64(q, from);
+        const int wm = __shfl_sync(0xffffffffu, w, from);
+        const int b = lane & 15;
+        if (ml >= 0 && ((qm >> b) & 1ull)) atomicAdd(&W.sigma[(size_t)wm * SW + b], svg);
+        continue;
+      }
       const int l = __ffs(em) - 1;
       em &= em - 1;
       const unsigned long long ql = shfl64(q, l);
@@ -183,8 +228,9 @@ __device__ void expand_entry(const Work& W, int i, int lane, int eb, int ee) {
 
 // piece = false: the whole entry, dependencies written to delta; piece = true: an
 // edge range of a hub entry, partial dependencies added to dacc (FP64 atomics).
-template <int NW>
+template <int NW, int GS>
 __device__ void backward_entry(const Work& W, int i, int lane, int eb, int ee, bool piece) {
+  static_assert(GS == 32 || (GS == 16 && NW == 1), "half-warp steps hold up to 16 sources");
   constexpr int SW = 32 * NW;
   const int v = W.flv[i];
   const unsigned long long m = W.flm[i];
@@ -195,6 +241,8 @@ __device__ void backward_entry(const Work& W, int i, int lane, int eb, int ee, b
     sv[k] = ((m >> b) & 1ull) ? W.sigma[(size_t)v * SW + b] : 0.0;
     acc[k] = 0.0;
   }
+  const double svg = GS == 16 ? __shfl_sync(0xffffffffu, sv[0], lane & 15) : 0.0;
+  double accg = 0.0;  // GS = 16: this half-warp's share for source bit (lane & 15)
   for (int c = eb; c < ee; c += 32) {
     const int j = c + lane;
     int w = 0;
@@ -205,6 +253,18 @@ __device__ void backward_entry(const Work& W, int i, int lane, int eb, int ee, b
     }
     unsigned em = __ballot_sync(0xffffffffu, s != 0ull);
     while (em) {
+      if (GS == 16) {
+        int from;
+        const int ml = half_pick(em, lane, from);
+        const unsigned long long sm = shfl64(s, from);
+        const int wm = __shfl_sync(0xffffffffu, w, from);
+        const int b = lane & 15;
+        if (ml >= 0 && ((sm >> b) & 1ull)) {
+          const size_t x = (size_t)wm * SW + b;
+          accg += svg / W.sigma[x] * (1.0 + (double)W.delta[x]);
+        }
+        continue;
+      }
       const int l = __ffs(em) - 1;
       em &= em - 1;
       const unsigned long long sl = shfl64(s, l);
@@ -219,6 +279,7 @@ __device__ void backward_entry(const Work& W, int i, int lane, int eb, int ee, b
       }
     }
   }
+  if (GS == 16) acc[0] = accg + __shfl_down_sync(0xffffffffu, accg, 16);  // first half, then second
 #pragma unroll
   for (int k = 0; k < NW; ++k) {
     const int b = lane + 32 * k;
@@ -234,7 +295,7 @@ __device__ void backward_entry(const Work& W, int i, int lane, int eb, int ee, b
 
 // One batch of nsrc (<= 32*NW) sources (local ids). Every participating thread
 // calls this with the same arguments; S provides the barrier and thread ranks.
-template <int NW, class S>
+template <int NW, int GS, class S>
 __device__ bool run_batch(const Work& W, const int32_t* srcs, int nsrc, S& sync, int32_t* lvl_out = nullptr,
                           double* sig_out = nullptr) {
   constexpr int SW = 32 * NW;
@@ -263,7 +324,7 @@ __device__ bool run_batch(const Work& W, const int32_t* srcs, int nsrc, S& sync,
       return false;
     }
     for (int i = b + gw; i < e; i += nw)
-      if (!queue_hub(W, i, lane)) expand_entry<NW>(W, i, lane, W.off[W.flv[i]], W.off[W.flv[i] + 1]);
+      if (!queue_hub(W, i, lane)) expand_entry<NW, GS>(W, i, lane, W.off[W.flv[i]], W.off[W.flv[i] + 1]);
     if (!sync.sync()) return false;
     if (W.hub_cap) {
       const unsigned long long hc = *(volatile unsigned long long*)W.hub_cnt;
@@ -272,7 +333,7 @@ __device__ bool run_batch(const Work& W, const int32_t* srcs, int nsrc, S& sync,
         for (int p = gw; p < np; p += nw) {
           int i, eb, ee;
           hub_piece(W, nh, p, i, eb, ee);
-          expand_entry<NW>(W, i, lane, eb, ee);
+          expand_entry<NW, GS>(W, i, lane, eb, ee);
         }
         if (!sync.sync()) return false;
       }
@@ -312,7 +373,7 @@ __device__ bool run_batch(const Work& W, const int32_t* srcs, int nsrc, S& sync,
     if (!sync.sync()) return false;
     const int b0 = W.lo[d], e0 = W.lo[d + 1];
     for (int i = b0 + gw; i < e0; i += nw)
-      if (!queue_hub(W, i, lane)) backward_entry<NW>(W, i, lane, W.off[W.flv[i]], W.off[W.flv[i] + 1], false);
+      if (!queue_hub(W, i, lane)) backward_entry<NW, GS>(W, i, lane, W.off[W.flv[i]], W.off[W.flv[i] + 1], false);
     if (!sync.sync()) return false;
     if (W.hub_cap) {
       const unsigned long long hc = *(volatile unsigned long long*)W.hub_cnt;
@@ -321,7 +382,7 @@ __device__ bool run_batch(const Work& W, const int32_t* srcs, int nsrc, S& sync,
         for (int p = gw; p < np; p += nw) {
           int i, eb, ee;
           hub_piece(W, nh, p, i, eb, ee);
-          backward_entry<NW>(W, i, lane, eb, ee, true);
+          backward_entry<NW, GS>(W, i, lane, eb, ee, true);
         }
         if (!sync.sync()) return false;
         // hub dependencies: FP64 partials -> delta, scratch back to zero
@@ -364,6 +425,17 @@ __device__ bool run_batch(const Work& W, const int32_t* srcs, int nsrc, S& sync,
   return *(volatile int*)W.err == 0;
 }
 
+// run_batch with the half-warp step when the batch has at most 16 sources (every
+// thread of the team sees the same nsrc, so all take the same branch).
+template <int NW, class S>
+__device__ bool run_batch_any(const Work& W, const int32_t* srcs, int nsrc, S& sync, int32_t* lvl_out = nullptr,
+                              double* sig_out = nullptr) {
+  if constexpr (NW == 1) {
+    if (nsrc <= 16) return run_batch<1, 16>(W, srcs, nsrc, sync, lvl_out, sig_out);
+  }
+  return run_batch<NW, 32>(W, srcs, nsrc, sync, lvl_out, sig_out);
+}
+
 struct GridArgs {
   Work W;
   const int32_t* srcs;
@@ -378,7 +450,7 @@ template <int NW>
 __global__ void __launch_bounds__(GRID_THREADS) k_bc_grid(GridArgs a) {
   GridSync gs{a.bar};
   for (int s0 = 0; s0 < a.nsrc; s0 += a.batch) {
-    if (!run_batch<NW>(a.W, a.srcs + s0, min(a.batch, a.nsrc - s0), gs, a.lvl_out, a.sig_out)) {
+    if (!run_batch_any<NW>(a.W, a.srcs + s0, min(a.batch, a.nsrc - s0), gs, a.lvl_out, a.sig_out)) {
       if (threadIdx.x == 0 && a.bar->error) atomicCAS(a.W.err, 0, 3);
       return;
     }
@@ -453,7 +525,63 @@ __global__ void __launch_bounds__(CTA_THREADS) k_bc_graphs(GraphsArgs a) {
       const int nb = min(SW, ns - s0);
       for (int t = threadIdx.x; t < nb; t += blockDim.x) s_src[t] = a.srcs[sb + s0 + t] - vb;
       __syncthreads();
-      if (!run_batch<NW>(W, s_src, nb, bs)) return;
+      if (!run_batch_any<NW>(W, s_src, nb, bs)) return;
+    }
+  }
+}
+
+// The many-graphs form with a cluster of C CTAs per graph (C > 1): the work queue hands
+// graphs to clusters, largest first, and each graph's batches run with cluster barriers,
+// so a large graph gets C SMs' worth of warps instead of one CTA's.
+template <int NW, int C>
+__global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(CTA_THREADS) k_bc_clusters(GraphsArgs a) {
+  constexpr int SW = 32 * NW;
+  __shared__ int s_g;
+  __shared__ int32_t s_src[SW];
+  cg::cluster_group cl = cg::this_cluster();
+  ClusterSync cs;
+  const int slot = blockIdx.x / C;
+  const bool leader = cl.block_rank() == 0;
+  Work W;
+  W.sigma = a.sigma + (size_t)slot * a.vmax * SW;
+  W.delta = a.delta + (size_t)slot * a.vmax * SW;
+  W.seen = a.masks + (size_t)slot * a.vmax * 3;
+  W.nxt = W.seen + a.vmax;
+  W.dense = W.nxt + a.vmax;
+  W.flv = a.flv + (size_t)slot * a.cap;
+  W.flm = a.flm + (size_t)slot * a.cap;
+  W.cap = a.cap;
+  W.lo = a.lo + (size_t)slot * (a.maxd + 2);
+  W.maxd = a.maxd;
+  W.cnt = a.cnt + slot;
+  W.err = a.err;
+  W.off = a.off;
+  W.adj = a.adj;
+  W.hub_cap = 0;
+  W.hub_deg = HUB_DEG;
+  W.hub_chunk = HUB_CHUNK;
+  W.hub_ent = W.hub_base = nullptr;
+  W.hub_cnt = nullptr;
+  W.dacc = nullptr;
+  while (true) {
+    if (leader && threadIdx.x == 0) s_g = atomicAdd(a.next, 1);
+    cl.sync();
+    const int k = *cl.map_shared_rank(&s_g, 0);
+    cl.sync();  // every CTA has read the leader's s_g before it is overwritten
+    if (k >= a.G) break;
+    const int g = a.order[k];
+    const int vb = a.voff[g], n = a.voff[g + 1] - vb;
+    W.off = a.off + vb;
+    W.vbase = vb;
+    W.V = n;
+    W.bc = a.bc + vb;
+    const int sb = a.soff[g], ns = a.soff[g + 1] - sb;
+    for (int s0 = 0; s0 < ns; s0 += SW) {
+      const int nb = min(SW, ns - s0);
+      // every CTA keeps its own copy: run_batch reads srcs from the caller's CTA
+      for (int t = threadIdx.x; t < nb; t += blockDim.x) s_src[t] = a.srcs[sb + s0 + t] - vb;
+      __syncthreads();
+      if (!run_batch_any<NW>(W, s_src, nb, cs)) return;
     }
   }
 }
@@ -517,6 +645,7 @@ struct BcPlan {
 };
 
 int bc_hub_deg_default() { return bc::HUB_DEG; }
+int bc_cluster_default() { return bc::CLUSTER_DEFAULT; }
 int bc_hub_chunk_default() { return bc::HUB_CHUNK; }
 
 void free_bc_plan(BcPlan* p) { delete p; }
@@ -741,7 +870,10 @@ extern "C" int sp_bc_graphs(sp_graph_h g, int32_t ngraphs, const int32_t* vertex
   int per_sm = 0;
   const void* fn = NW == 2 ? (const void*)bc::k_bc_graphs<2> : (const void*)bc::k_bc_graphs<1>;
   SP_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, bc::CTA_THREADS, 0));
-  const int ctas = std::max(1, std::min(num_sms() * std::max(1, std::min(per_sm, 2)), ngraphs));
+  const int C = g->bc_cluster > 0 ? g->bc_cluster : bc::CLUSTER_DEFAULT;
+  // one scratch slot per team (a CTA, or a cluster of C CTAs)
+  const int teams = std::max(1, std::min(num_sms() * std::max(1, std::min(per_sm, 2)) / C, ngraphs));
+  const int ctas = teams;
   SP_TRY(p->sigma.alloc((size_t)ctas * vmax * SW));
   SP_TRY(p->delta.alloc((size_t)ctas * vmax * SW));
   SP_TRY(p->masks.alloc((size_t)ctas * vmax * 3));
@@ -790,10 +922,27 @@ extern "C" int sp_bc_graphs(sp_graph_h g, int32_t ngraphs, const int32_t* vertex
   a.cap = cap;
   a.maxd = maxd;
   a.err = p->err.p;
-  if (NW == 2)
-    bc::k_bc_graphs<2><<<ctas, bc::CTA_THREADS, 0, s>>>(a);
-  else
-    bc::k_bc_graphs<1><<<ctas, bc::CTA_THREADS, 0, s>>>(a);
+  if (C == 1) {
+    if (NW == 2)
+      bc::k_bc_graphs<2><<<teams, bc::CTA_THREADS, 0, s>>>(a);
+    else
+      bc::k_bc_graphs<1><<<teams, bc::CTA_THREADS, 0, s>>>(a);
+  } else {
+    const int grid = teams * C;
+#define SP_BC_CLUSTERS(CC)                                                          \
+  if (NW == 2)                                                                     \
+    bc::k_bc_clusters<2, CC><<<grid, bc::CTA_THREADS, 0, s>>>(a);                  \
+  else                                                                             \
+    bc::k_bc_clusters<1, CC><<<grid, bc::CTA_THREADS, 0, s>>>(a);
+    if (C == 2) {
+      SP_BC_CLUSTERS(2)
+    } else if (C == 4) {
+      SP_BC_CLUSTERS(4)
+    } else {
+      SP_BC_CLUSTERS(8)
+    }
+#undef SP_BC_CLUSTERS
+  }
   SP_CHECK_LAUNCH();
   int herr = 0;
   SP_TRY(copy_out(&herr, p->err.p, sizeof(int), s));

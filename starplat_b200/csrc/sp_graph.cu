@@ -559,6 +559,14 @@ int sp_tune_set(sp_graph_h g, const char* key, int64_t value) {
       g->sssp_hub_chunk = (int32_t)value;
     return SP_OK;
   }
+  if (!strcmp(key, "bc.cluster")) {
+    if (value != 0 && value != 1 && value != 2 && value != 4 && value != 8) {
+      set_error("sp_tune_set: bc.cluster must be 0, 1, 2, 4 or 8");
+      return SP_ERR_INVALID;
+    }
+    g->bc_cluster = (int32_t)value;
+    return SP_OK;
+  }
   if (!strcmp(key, "bc.hub_deg")) {
     if (value < 0 || value > (1 << 30)) {
       set_error("sp_tune_set: bc.hub_deg must be in [0, 2^30]");
@@ -630,6 +638,10 @@ int sp_tune_get(sp_graph_h g, const char* key, int64_t* value) {
   }
   if (!strcmp(key, "sssp.hub_chunk")) {
     *value = g->sssp_hub_chunk > 0 ? g->sssp_hub_chunk : sssp_hub_chunk_default();
+    return SP_OK;
+  }
+  if (!strcmp(key, "bc.cluster")) {
+    *value = g->bc_cluster > 0 ? g->bc_cluster : bc_cluster_default();
     return SP_OK;
   }
   if (!strcmp(key, "bc.hub_deg")) {

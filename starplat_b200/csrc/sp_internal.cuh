@@ -161,7 +161,8 @@ struct sp_graph {
   int32_t tc_cta_warps = -1;  // TC: warps per CTA of the shared-bitmap kernel (-1 = default, 0 = off)
   int32_t bc_batch = 0;
   int32_t bc_hub_deg = 0;  // BC: split level-list entries above this degree (0 = default)
-  int32_t bc_hub_chunk = 0;  // BC: edges per piece of a split entry (0 = default)    // BC sources per multi-source batch (0 = 64)
+  int32_t bc_hub_chunk = 0;  // BC: edges per piece of a split entry (0 = default)
+  int32_t bc_cluster = 0;    // BC many-graphs form: CTAs per graph (0 = default)    // BC sources per multi-source batch (0 = 64)
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   sp::PrPlan* pr = nullptr;
@@ -181,6 +182,7 @@ int bc_hub_deg_default();             // BC entry-splitting defaults (sp_bc.cu)
 int sssp_hub_deg_default();           // SSSP hub-splitting defaults (sp_sssp.cu)
 int sssp_hub_chunk_default();
 int bc_hub_chunk_default();
+int bc_cluster_default();
 int ensure_symmetry(sp_graph* g);     // fills g->symmetric
 int copy_out(void* dst, const void* src, size_t bytes, cudaStream_t s);  // host or device dst
 int num_sms();

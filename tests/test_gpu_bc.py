@@ -107,7 +107,9 @@ def test_bfs_levels_and_sigma_bit_exact():
             assert np.array_equal(sig[k], rs)  # integers below 2^53: exact
 
 
-def test_bc_many_graphs_one_launch():
+@pytest.mark.parametrize("cluster", [1, 2, 4, 8])
+def test_bc_many_graphs_one_launch(cluster):
+    # each graph taken by one CTA or by a cluster of CTAs with cluster barriers
     gs = G.er_batch(12, 200, 3000, 4, 12, seed=3)
     offs = [0]
     src_all, soff = [], [0]
@@ -123,6 +125,8 @@ def test_bc_many_graphs_one_launch():
     V = offs[-1]
     union = from_pairs(V, np.stack([np.concatenate(pairs_s), np.concatenate(pairs_d)], 1), name="union")
     with DeviceGraph.from_csr(union) as dg:
+        dg.tune_set("bc.cluster", cluster)
+        assert dg.tune_get("bc.cluster") == cluster
         out = dg.bc_graphs(np.array(offs, np.int32), np.array(soff, np.int32), np.concatenate(src_all))
     for k, g in enumerate(gs):
         ref = O.bc(g.indexofNodes, g.edgeList, src_all[k] - offs[k])
