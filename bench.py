@@ -56,6 +56,7 @@ BETA, DELTA, MAX_ITER = 1e-6, 0.85, 100
 METRIC = "GTEPS per algorithm on 1 B200 (pagerank headline)"
 INT_MAX = 2**31 - 1
 TUNE = []  # (key, value) schedule knobs from --tune, applied to every device graph
+REP = None  # the replica group of a multi-GPU run (set in main)
 
 
 def peaks():
@@ -328,7 +329,16 @@ def bench_bc(steps, warmup, stream, hbm, cpu, nsrc=256):
     with DeviceGraph.from_csr(g, with_weights=False) as dg:
         dg.set_stream(stream)
         tuned(dg)
-        ms, _ = timed(lambda: dg.bc(srcs), steps, warmup, stream)
+        if REP is not None and REP.world > 1:
+            # the sources split over the GPUs, one all-reduce of BC[V] (strong scaling)
+            from starplat_b200.distributed import bc_on_gpus
+
+            REP.barrier()
+            ms, _ = timed(lambda: bc_on_gpus(dg, srcs, REP), steps, warmup, stream)
+            ms = REP.max(ms)
+            out["parallelism"] = f"sources split over {REP.world} GPUs, one all-reduce of BC[V]"
+        else:
+            ms, _ = timed(lambda: dg.bc(srcs), steps, warmup, stream)
         few = srcs[:8]
         msp, _ = timed(lambda: dg.bc(few, variant=_lib.SP_BC_PLAIN), 1, 0, stream)
     out.update({"value": sum_er / (ms / 1e3) / 1e9, "unit": "GTEPS", "ms": ms,
@@ -558,7 +568,7 @@ def run_extras(want, args, stream, hbm, cpu_ok):
 # ----------------------------------------------------------------------------- main
 
 def main():
-    global PR_SCALE
+    global PR_SCALE, REP
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
@@ -593,6 +603,7 @@ def main():
 
     torch.cuda.set_device(local)
     rep = Replicas("nccl" if world > 1 else None)
+    REP = rep
     barrier, max_over_ranks = rep.barrier, rep.max
 
     from starplat_b200 import _lib

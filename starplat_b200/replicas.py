@@ -58,6 +58,18 @@ class Replicas:
         """x summed over all ranks (the units the whole job processed)."""
         return float(x) if self._dist is None else self._reduce(x, self._dist.ReduceOp.SUM)
 
+    def all_reduce_sum(self, a):
+        """Element-wise sum of a float32 numpy array over all ranks (every rank gets it)."""
+        if self._dist is None:
+            return a
+        import numpy as np
+        import torch
+
+        dev = "cuda" if self.backend == "nccl" else "cpu"
+        t = torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+        self._dist.all_reduce(t, op=self._dist.ReduceOp.SUM)
+        return t.cpu().numpy()
+
     def whole_job_rate(self, units: float, seconds: float) -> float:
         """Units all ranks processed per second of the slowest rank."""
         total, slowest = self.sum(units), self.max(seconds)

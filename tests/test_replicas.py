@@ -73,3 +73,43 @@ def test_reference_arm_under_torchrun_prints_once_from_rank_zero():
     line = lines[0]
     assert line["impl"] == "reference" and line["n_gpus"] == 2 and line["value"] > 0
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["cpu_baseline"]["kind"] in ("port", "reference")
+
+
+def _bc_rank_main(rank, world, port, out_dir):
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port), "RANK": str(rank),
+                       "WORLD_SIZE": str(world), "LOCAL_RANK": str(rank)})
+    sys.path.insert(0, ROOT)
+    import numpy as np
+
+    from oracle import oracle as O
+    from starplat_b200 import generators as G
+    from starplat_b200.distributed import bc_sharded, split_sources
+    from starplat_b200.replicas import Replicas
+
+    g = G.rmat(9, 8, seed=4)
+    srcs = G.pick_sources(g, 37, seed=1)
+    rep = Replicas(backend="gloo", timeout_s=60)
+    mine = split_sources(srcs, world, rank)
+    out = bc_sharded(g.V, srcs, rep, lambda s: O.bc(g.indexofNodes, g.edgeList, s).astype(np.float32))
+    rep.close()
+    np.save(os.path.join(out_dir, f"bc{rank}.npy"), out)
+    np.save(os.path.join(out_dir, f"src{rank}.npy"), mine)
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_bc_split_over_ranks_sums_to_the_whole(tmp_path, world):
+    import numpy as np
+
+    from oracle import oracle as O
+    from starplat_b200 import generators as G
+
+    mp.start_processes(_bc_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    g = G.rmat(9, 8, seed=4)
+    srcs = G.pick_sources(g, 37, seed=1)
+    ref = O.bc(g.indexofNodes, g.edgeList, srcs)
+    slices = [np.load(tmp_path / f"src{r}.npy") for r in range(world)]
+    assert np.array_equal(np.concatenate(slices), srcs)  # a partition, in order
+    for r in range(world):
+        out = np.load(tmp_path / f"bc{r}.npy").astype(np.float64)
+        assert np.all(np.abs(out - ref) <= 1e-5 * np.abs(ref) + 1e-6)
