@@ -92,6 +92,8 @@ int sp_graph_info(sp_graph_h g, int32_t* V, int64_t* E, int32_t* symmetric);
  *   "pr.hot"  PageRank: source ids (after relabelling by out-degree) gathered in the
  *             L1-resident hot phase of each iteration (0..2^22, default 0 = one phase
  *             for all sources).
+ *   "pr.src_hint"  PageRank: L1 policy of the srcList loads, read once per iteration
+ *             (0 cached, 1 not allocated, 2 evicted first = default).
  *   "pr.order"  PageRank vertex order, fixed when the plan is built (a change rebuilds
  *             it): 0 = out-degree descending; 1 = in-degree class first (the row bins
  *             of the iteration kernel), out-degree descending within a class.

@@ -3,7 +3,8 @@
 Each algorithm's kernels take thresholds that change only how work is split:
   tc        tc.cta_warps: a bitmap per warp (0) or per CTA of 2 / 4 / 8 warps
   pagerank  pr.order: vertex order by out-degree (0) or in-degree class first (1);
-            pr.hot: sources of the L1-resident hot phase (0 = one phase)
+            pr.src_hint: L1 policy of the srcList loads; pr.hot: sources of the
+            L1-resident hot phase (0 = one phase)
   sssp      sssp.hub_deg / sssp.hub_chunk: queued vertices above hub_deg out-edges are
             relaxed in hub_chunk-edge pieces shared by all warps
   bc        bc.hub_deg / bc.hub_chunk: the same for level-list entries
@@ -23,7 +24,7 @@ import numpy as np
 
 KNOBS: Dict[str, Dict[str, Sequence[int]]] = {
     "tc": {"tc.cta_warps": (0, 2, 4, 8)},
-    "pagerank": {"pr.order": (0, 1), "pr.hot": (0, 4096, 65536)},
+    "pagerank": {"pr.order": (0, 1), "pr.src_hint": (0, 2), "pr.hot": (0, 4096)},
     "sssp": {"sssp.hub_deg": (64, 128, 512, 2048), "sssp.hub_chunk": (32, 64, 256)},
     "bc": {"bc.hub_deg": (32, 64, 256, 4096), "bc.hub_chunk": (64, 128, 256)},
 }

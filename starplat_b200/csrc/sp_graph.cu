@@ -524,6 +524,14 @@ int sp_tune_set(sp_graph_h g, const char* key, int64_t value) {
     g->pr_hot = (int32_t)value;
     return SP_OK;
   }
+  if (!strcmp(key, "pr.src_hint")) {
+    if (value < 0 || value > 2) {
+      set_error("sp_tune_set: pr.src_hint must be 0, 1 or 2");
+      return SP_ERR_INVALID;
+    }
+    g->pr_src_hint = (int32_t)value;
+    return SP_OK;
+  }
   if (!strcmp(key, "pr.order")) {
     if (value != 0 && value != 1) {
       set_error("sp_tune_set: pr.order must be 0 or 1");
@@ -610,6 +618,10 @@ int sp_tune_get(sp_graph_h g, const char* key, int64_t* value) {
   }
   if (!strcmp(key, "pr.hot")) {
     *value = g->pr_hot >= 0 ? g->pr_hot : 0;
+    return SP_OK;
+  }
+  if (!strcmp(key, "pr.src_hint")) {
+    *value = g->pr_src_hint >= 0 ? g->pr_src_hint : pr_src_hint_default();
     return SP_OK;
   }
   if (!strcmp(key, "pr.order")) {

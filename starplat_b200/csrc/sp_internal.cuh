@@ -152,6 +152,7 @@ struct sp_graph {
   int32_t max_out_deg = -1;
   int32_t pr_hot = -1;  // PageRank: source ids of the L1 hot phase (-1 = default)
   int32_t pr_order = -1;  // PageRank: vertex order of the plan (-1 = default)
+  int32_t pr_src_hint = -1;  // PageRank: L1 policy of srcList loads (-1 = default)
   int64_t sssp_delta = 0;  // SSSP bucket width (0 = max edge weight)
   int32_t sssp_ctas_per_sm = 0;  // SSSP persistent CTAs per SM (0 = learned / 4)
   int64_t sssp_last_delta = 0;   // schedule of the last SSSP call (reporting)
@@ -177,6 +178,7 @@ int ensure_reverse(sp_graph* g);      // builds roff/radj on device if missing
 int ensure_emap(sp_graph* g);         // builds emap (edgeMap) on device if missing
 int finish_graph(sp_graph* g);        // checks a library-built CSR, sets max_out_deg
 int pr_order_default();               // PageRank vertex order default (sp_pagerank.cu)
+int pr_src_hint_default();
 int tc_cta_warps_default();           // TC kernel choice default (sp_tc.cu)
 int bc_hub_deg_default();             // BC entry-splitting defaults (sp_bc.cu)
 int sssp_hub_deg_default();           // SSSP hub-splitting defaults (sp_sssp.cu)

@@ -44,6 +44,7 @@ constexpr int CHUNK = THREADS * CIPT;   // edges per long-row chunk (one round p
 constexpr int LONG_DEG = 2048;          // rows with more in-edges are processed as chunks
 constexpr int HOT_DEFAULT = 0;          // one phase: measured fastest on R-MAT 22 (12.0 vs 13.0-13.5 ms)
 constexpr int HOT_MAX = 1 << 22;
+constexpr int SRC_HINT_DEFAULT = 2;     // srcList loads: 0 __ldg, 1 L1::no_allocate, 2 L1::evict_first
 constexpr int ORDER_DEFAULT = 0;        // vertex order: 0 out-degree, 1 in-degree class then out-degree
 // degree-bin upper bounds for 1, 4, 8 and 32 lanes per row segment
 constexpr int BIN_T1 = 4, BIN_T4 = 16, BIN_T8 = 32;
@@ -100,10 +101,12 @@ struct PrPlan {
   cudaGraphExec_t exec = nullptr;
   int exec_iters = 0;
   float exec_beta = -1, exec_delta = -1;
+  int exec_sh = -1;
   cudaStream_t exec_stream = nullptr;
 };
 
 int pr_order_default() { return pr::ORDER_DEFAULT; }
+int pr_src_hint_default() { return pr::SRC_HINT_DEFAULT; }
 
 void free_pr_plan(PrPlan* p) {
   if (!p) return;
@@ -144,13 +147,20 @@ __device__ __forceinline__ double finalize_row(const IterArgs& a, int r, double 
   return fabs((double)np - (double)po);
 }
 
-// srcList is read once per iteration: in the hot phase keep it out of L1 so the
-// hot block of contrib stays resident.
-template <int PH>
+// srcList is read once per iteration. SH picks how its loads treat L1: 0 cached
+// (__ldg), 1 not allocated in L1, 2 allocated but evicted first, so that streaming it
+// does not push out the contrib lines that the gathers reuse. R-MAT 22: 11.72 ms per
+// run with 0, 11.68 with 1, 11.57 with 2 (contrib gathers marked evict-last on top:
+// 12.0). The hot phase (PH 0) always keeps it out of L1.
+template <int PH, int SH>
 __device__ __forceinline__ int ld_src(const int32_t* p) {
-  if (PH == 0) {
-    int v;
+  int v;
+  if (PH == 0 || SH == 1) {
     asm("ld.global.nc.L1::no_allocate.b32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+  }
+  if (SH == 2) {
+    asm("ld.global.nc.L1::evict_first.b32 %0, [%1];" : "=r"(v) : "l"(p));
     return v;
   }
   return __ldg(p);
@@ -160,7 +170,9 @@ __device__ __forceinline__ int ld_src(const int32_t* p) {
 // staging the hottest sources in shared memory measured 20-180% slower on R-MAT 22
 // (the carve-out shrinks L1, where those sources already hit, and large tables halve
 // the resident CTAs).
+template <int SH>
 struct GatherGlobal {
+  static constexpr int kSrcHint = SH;
   const float* __restrict__ con;
   __device__ __forceinline__ float operator()(int u) const { return __ldg(con + u); }
 };
@@ -175,7 +187,7 @@ __device__ __forceinline__ double group_row_sum(int b, int e, int sl, const int3
 #pragma unroll
     for (int k = 0; k < U; ++k) {
       const int i = base + sl + W * k;
-      idx[k] = i < e ? ld_src<PH>(radj + i) : -1;
+      idx[k] = i < e ? ld_src<PH, G::kSrcHint>(radj + i) : -1;
     }
     float v[U];
 #pragma unroll
@@ -239,7 +251,7 @@ __device__ __forceinline__ void phase_body(const IterArgs& a, const G& gather, c
 #pragma unroll
       for (int k = 0; k < CI; ++k) {
         const int e = c.y + tid + k * NT;
-        idx[k] = e < c.z ? ld_src<PH>(a.radj + e) : -1;
+        idx[k] = e < c.z ? ld_src<PH, G::kSrcHint>(a.radj + e) : -1;
       }
       float v[CI];
 #pragma unroll
@@ -316,14 +328,14 @@ __device__ __forceinline__ void phase_body(const IterArgs& a, const G& gather, c
 }
 
 // One phase of one iteration, every gather from global memory (256-thread CTAs).
-template <int PH>
+template <int PH, int SH>
 __global__ void __launch_bounds__(THREADS) k_phase(IterArgs a, const float* __restrict__ pr_old,
                                                    const float* __restrict__ con_old, float* __restrict__ pr_new,
                                                    float* __restrict__ con_new) {
   __shared__ double s_red[THREADS / 32];
   __shared__ int s_last;
   if (a.st->done) return;
-  phase_body<PH, THREADS>(a, GatherGlobal{con_old}, pr_old, pr_new, con_new, s_red, s_last);
+  phase_body<PH, THREADS>(a, GatherGlobal<SH>{con_old}, pr_old, pr_new, con_new, s_red, s_last);
 }
 
 // Rows without in-edges, iterations 0 and 1 only: pr' = (1-delta)/V. Their diff
@@ -801,11 +813,15 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
   a.max_iter = n_iter;
   a.two_phase = p->two_phase() ? 1 : 0;
   int per_sm = 0;
-  SP_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pr::k_phase<1>, pr::THREADS, 0));
+  const int sh = g->pr_src_hint >= 0 ? g->pr_src_hint : pr::SRC_HINT_DEFAULT;
+  using PhaseFn = void (*)(pr::IterArgs, const float*, const float*, float*, float*);
+  const PhaseFn ph1 = sh == 1 ? pr::k_phase<1, 1> : sh == 2 ? pr::k_phase<1, 2> : pr::k_phase<1, 0>;
+  SP_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ph1, pr::THREADS, 0));
   const int grid = std::max(1, std::min(num_sms() * 32, num_sms() * std::max(1, per_sm)));
   pr::k_init<<<num_sms() * 4, 256, 0, s>>>(V, p->od.p, p->prb[0].p, p->con[0].p, p->state.p);
   SP_CHECK_LAUNCH();
-  if (!(p->exec && p->exec_iters == n_iter && p->exec_beta == beta && p->exec_delta == delta && p->exec_stream == s)) {
+  if (!(p->exec && p->exec_iters == n_iter && p->exec_beta == beta && p->exec_delta == delta && p->exec_stream == s &&
+        p->exec_sh == sh)) {
     if (p->exec) {
       cudaGraphExecDestroy(p->exec);
       p->exec = nullptr;
@@ -817,8 +833,8 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
       if (k < 2 && p->n_zero)
         pr::k_zero_rows<<<num_sms() * 2, 256, 0, s>>>(a, p->zrows, p->n_zero, p->prb[c].p, p->prb[n].p, p->con[n].p);
       if (a.two_phase)
-        pr::k_phase<0><<<grid, pr::THREADS, 0, s>>>(a, p->prb[c].p, p->con[c].p, p->prb[n].p, p->con[n].p);
-      pr::k_phase<1><<<grid, pr::THREADS, 0, s>>>(a, p->prb[c].p, p->con[c].p, p->prb[n].p, p->con[n].p);
+        pr::k_phase<0, 1><<<grid, pr::THREADS, 0, s>>>(a, p->prb[c].p, p->con[c].p, p->prb[n].p, p->con[n].p);
+      ph1<<<grid, pr::THREADS, 0, s>>>(a, p->prb[c].p, p->con[c].p, p->prb[n].p, p->con[n].p);
     }
     cudaError_t ce = cudaStreamEndCapture(s, &graph);
     if (ce != cudaSuccess) {
@@ -836,6 +852,7 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
     p->exec_beta = beta;
     p->exec_delta = delta;
     p->exec_stream = s;
+    p->exec_sh = sh;
   }
   SP_CHECK_CUDA(cudaGraphLaunch(p->exec, s));
   g_launches.fetch_add((unsigned long long)n_iter * (p->two_phase() ? 2 : 1) +

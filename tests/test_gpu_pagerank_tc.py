@@ -91,6 +91,21 @@ def test_pagerank_degree_bin_boundaries():
     _pr_check(_bins_graph(), _lib.SP_PR_TUNED)
 
 
+@pytest.mark.parametrize("hint", [0, 1, 2])
+def test_pagerank_src_hint_knob(hint):
+    # a cache policy of the srcList loads: identical results
+    for g in directed_zoo()[:2] + [_bins_graph()]:
+        g.ensure_reverse()
+        dg = device_graph(g)
+        dg.tune_set("pr.src_hint", 0)
+        base, it0, _ = dg.pagerank(1e-6, 0.85, 100)
+        dg.tune_set("pr.src_hint", hint)
+        assert dg.tune_get("pr.src_hint") == hint
+        out, it1, _ = dg.pagerank(1e-6, 0.85, 100)
+        dg.tune_set("pr.src_hint", 2)
+        assert it0 == it1 and np.array_equal(out, base)
+
+
 @pytest.mark.parametrize("order", [0, 1])
 def test_pagerank_vertex_order_knob(order):
     # the vertex order of the plan changes the order of each row's sum, so results
