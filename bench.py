@@ -696,15 +696,15 @@ def main():
     pr_plain = {"value": E * resp[0][1] / (msp / 1e3) / 1e9, "ms_per_step": msp, "iterations": resp[0][1]}
 
     # ---- end to end through the C ABI with host buffers (pinned), every step
-    pin = {k: torch.from_numpy(getattr(g, k)).pin_memory()
-           for k in ("indexofNodes", "edgeList", "rev_indexofNodes", "srcList")}
+    # what the drop-in header uploads: the forward CSR (PageRank builds its relabelled
+    # reverse rows on the device)
+    pin = {k: torch.from_numpy(getattr(g, k)).pin_memory() for k in ("indexofNodes", "edgeList")}
     host_out = torch.empty(V, dtype=torch.float32).pin_memory()
     h2d = sum(t.numel() * 4 for t in pin.values())
     d2h = V * 4
 
     def e2e_step():
-        with DeviceGraph(pin["indexofNodes"].numpy(), pin["edgeList"].numpy(), None,
-                         pin["rev_indexofNodes"].numpy(), pin["srcList"].numpy()) as hg:
+        with DeviceGraph(pin["indexofNodes"].numpy(), pin["edgeList"].numpy()) as hg:
             _, n, _ = hg.pagerank(BETA, DELTA, MAX_ITER, out=host_out.numpy())
         return n
 

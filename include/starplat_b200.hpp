@@ -61,7 +61,9 @@ inline MirrorCache& cache() {
   return c;
 }
 
-// The device mirror of g (uploaded on first use).
+// The device mirror of g (uploaded on first use): the forward CSR and edgeLen. The
+// reverse CSR is not copied over PCIe; an algorithm that needs it builds it on the
+// device (a stable transpose, rows ascending: what graph.hpp:825-832 makes srcList).
 template <class Graph>
 inline sp_graph_h mirror(Graph& g) {
   MirrorCache& c = cache();
@@ -71,7 +73,7 @@ inline sp_graph_h mirror(Graph& g) {
   const int V = g.num_nodes();
   const long long E = g.num_edges();
   sp_graph_h h = nullptr;
-  check(sp_graph_create(V, E, g.indexofNodes, g.edgeList, g.getEdgeLen(), g.rev_indexofNodes, g.srcList, 0, &h),
+  check(sp_graph_create(V, E, g.indexofNodes, g.edgeList, g.getEdgeLen(), nullptr, nullptr, 0, &h),
         "sp_graph_create");
   c.by_graph[&g] = h;
   return h;

@@ -304,6 +304,16 @@ int ensure_reverse(sp_graph* g) {
   return SP_OK;
 }
 
+int offsets_of_sorted(int32_t V, int64_t E, const int32_t* keys, int32_t* off, cudaStream_t s) {
+  if (E > 0) {
+    k_offsets_of_sorted<<<num_sms() * 8, 256, 0, s>>>(V, E, keys, off);
+    SP_CHECK_LAUNCH();
+  } else {
+    SP_CHECK_CUDA(cudaMemsetAsync(off, 0, sizeof(int32_t) * ((size_t)V + 1), s));
+  }
+  return SP_OK;
+}
+
 int ensure_emap(sp_graph* g) {
   if (g->emap.p && g->emap.n >= (size_t)g->E) return SP_OK;
   SP_TRY(ensure_reverse(g));

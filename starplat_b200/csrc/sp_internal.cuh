@@ -176,6 +176,8 @@ struct sp_graph {
 namespace sp {
 int ensure_reverse(sp_graph* g);      // builds roff/radj on device if missing
 int ensure_emap(sp_graph* g);         // builds emap (edgeMap) on device if missing
+// off[v] = first index of keys (ascending, E of them) that is >= v, for v = 0..V
+int offsets_of_sorted(int32_t V, int64_t E, const int32_t* keys, int32_t* off, cudaStream_t s);
 int finish_graph(sp_graph* g);        // checks a library-built CSR, sets max_out_deg
 int pr_order_default();               // PageRank vertex order default (sp_pagerank.cu)
 int pr_src_hint_default();

@@ -376,13 +376,11 @@ __global__ void k_deg_keys(int V, int order, const int32_t* __restrict__ off, co
 }
 
 __global__ void k_relabel_rows(int V, const int32_t* __restrict__ inv, const int32_t* __restrict__ off,
-                               const int32_t* __restrict__ roff, int32_t* __restrict__ new_id, int32_t* __restrict__ od,
-                               int32_t* __restrict__ indeg) {
+                               int32_t* __restrict__ new_id, int32_t* __restrict__ od) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < V; k += gridDim.x * blockDim.x) {
     const int v = inv[k];
     new_id[v] = k;
     od[k] = off[v + 1] - off[v];
-    indeg[k] = roff[v + 1] - roff[v];
   }
 }
 
@@ -606,14 +604,13 @@ static int relabel(sp_graph* g, PrPlan* p) {
   cub::DeviceScan::ExclusiveSum(nullptr, t_scan, (const int32_t*)nullptr, (int32_t*)nullptr, V + 1, s);
   cub::DeviceRadixSort::SortPairs(nullptr, t_esort, nk, nv, E, 0, bits, s);
   Arena T;
-  dspan<int32_t> key, id, skey, inv, indeg, offp, dst, dst_alt, src, big;
+  dspan<int32_t> key, id, skey, inv, offp, dst, dst_alt, src, big;
   dspan<int> nbig;
   dspan<unsigned char> temp;
   T.want(key, V);
   T.want(id, V);
   T.want(skey, V);
   T.want(inv, V);
-  T.want(indeg, (size_t)V + 1);
   T.want(offp, V);
   T.want(dst, E);
   T.want(dst_alt, E);
@@ -629,11 +626,8 @@ static int relabel(sp_graph* g, PrPlan* p) {
   SP_CHECK_LAUNCH();
   size_t t = tb;
   SP_CHECK_CUDA(cub::DeviceRadixSort::SortPairs(temp.p, t, key.p, skey.p, id.p, inv.p, V, 0, 32, s));
-  SP_CHECK_CUDA(cudaMemsetAsync(indeg.p + V, 0, sizeof(int32_t), s));
-  pr::k_relabel_rows<<<grid, 256, 0, s>>>(V, inv.p, g->off.p, g->roff.p, p->new_id.p, p->od.p, indeg.p);
+  pr::k_relabel_rows<<<grid, 256, 0, s>>>(V, inv.p, g->off.p, p->new_id.p, p->od.p);
   SP_CHECK_LAUNCH();
-  t = tb;
-  SP_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, t, indeg.p, p->roffp.p, V + 1, s));
   t = tb;
   SP_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, t, p->od.p, offp.p, V, s));
   SP_CHECK_CUDA(cudaMemsetAsync(nbig.p, 0, sizeof(int), s));
@@ -648,6 +642,9 @@ static int relabel(sp_graph* g, PrPlan* p) {
   SP_CHECK_CUDA(cub::DeviceRadixSort::SortPairs(temp.p, t, keys, vals, E, 0, bits, s));
   if (E > 0 && vals.Current() != p->radjp.p)
     SP_CHECK_CUDA(cudaMemcpyAsync(p->radjp.p, vals.Current(), sizeof(int32_t) * E, cudaMemcpyDeviceToDevice, s));
+  // row offsets of the relabelled reverse CSR straight from the sorted destinations
+  // (no reverse CSR of the caller's graph is needed)
+  SP_TRY(offsets_of_sorted(V, E, keys.Current(), p->roffp.p, s));
   SP_CHECK_CUDA(cudaStreamSynchronize(s));
   return SP_OK;
 }
@@ -658,7 +655,7 @@ static int relabel(sp_graph* g, PrPlan* p) {
 // host reads back only the class sizes and the chunk totals.
 static int build_pr_plan(sp_graph* g, int hot, int order) {
   if (g->pr && g->pr->hot == hot && g->pr->order == order) return SP_OK;
-  SP_TRY(ensure_reverse(g));
+  if (order != 0) SP_TRY(ensure_reverse(g));  // in-degree classes read the caller's reverse offsets
   const int V = g->V;
   if (g->pr && g->pr->order != order) {  // a new vertex order: a new plan
     free_pr_plan(g->pr);
