@@ -45,7 +45,7 @@ const char* sp_last_error(void);
 /* Number of kernels this library has launched in this process (graph nodes count once each). */
 unsigned long long sp_launch_count(void);
 /* Device memory released by this library (graph handles, plans, scratch) is kept in a
- * per-device cache, at most 1/8 of the device's memory, and reused by later
+ * per-device cache, at most 1/8 of the device's memory or 4 GiB, and reused by later
  * allocations of a similar size. sp_cache_bytes: bytes held for the current device.
  * sp_cache_trim: returns every cached block to the driver (like
  * torch.cuda.empty_cache); an allocation that runs out of memory does the same for

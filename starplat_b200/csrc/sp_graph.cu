@@ -49,7 +49,7 @@ struct BlockCache {
   std::mutex mu;
   std::vector<Block> blocks;
   size_t cached[64] = {};  // bytes held per device
-  size_t cap[64] = {};     // at most 1/8 of the device's memory is held
+  size_t cap[64] = {};     // at most min(1/8 of the device's memory, 4 GiB) is held
 };
 // Never destroyed: buffers in static objects may be released during exit.
 BlockCache& cache() {
@@ -140,7 +140,8 @@ void dev_free(void* p, size_t bytes, int dev) {
   std::lock_guard<std::mutex> lk(c.mu);
   if (!c.cap[dev]) {
     size_t fr = 0, tot = 0;
-    c.cap[dev] = cudaMemGetInfo(&fr, &tot) == cudaSuccess ? tot / 8 : 0;
+    // other allocators in the process (torch's) cannot reclaim what this cache holds
+    c.cap[dev] = cudaMemGetInfo(&fr, &tot) == cudaSuccess ? std::min(tot / 8, (size_t)4 << 30) : 0;
   }
   if (c.cached[dev] + bytes > c.cap[dev]) {
     cudaFree(p);
