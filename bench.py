@@ -260,7 +260,8 @@ def bench_sssp(name, g, src, steps, warmup, stream, hbm, cpu, cpu_mode):
         # warm both, then alternate single timed runs and take each one's median
         S.unload()  # also keeps the first sssp call from loading the shipped model
         timed(lambda: dg.sssp(src, out=dist), 1, max(1, warmup), stream)
-        fixed = {"delta": dg.tune_get("sssp.last_delta"), "ctas_per_sm": dg.tune_get("sssp.last_ctas")}
+        fixed = {"delta": dg.tune_get("sssp.last_delta"), "ctas_per_sm": dg.tune_get("sssp.last_ctas"),
+                 "local": dg.tune_get("sssp.last_local")}
         d_fixed = dist.cpu().numpy()
         learned = S.load()
         timed(lambda: dg.sssp(src, out=dist), 1, max(1, warmup), stream)
@@ -276,6 +277,7 @@ def bench_sssp(name, g, src, steps, warmup, stream, hbm, cpu, cpu_mode):
             dg.tune_set("sssp.ctas_per_sm", 0)
             ms1, res = timed(lambda: dg.sssp(src, out=dist), 1, 0, stream)
             t_learned.append(ms1)
+            relaxed = dg.tune_get("sssp.last_relaxed")
         tuned(dg)
         msf, ms = statistics.median(t_fixed), statistics.median(t_learned)
         fixed.update({"ms": msf, "rounds": resf[0][1]})
@@ -284,12 +286,13 @@ def bench_sssp(name, g, src, steps, warmup, stream, hbm, cpu, cpu_mode):
         er = int(np.diff(g.indexofNodes)[reached].sum())
         nr = int(reached.sum())
         sched = {"learned": learned, "delta": dg.tune_get("sssp.last_delta"),
-                 "ctas_per_sm": dg.tune_get("sssp.last_ctas")}
+                 "ctas_per_sm": dg.tune_get("sssp.last_ctas"), "local": dg.tune_get("sssp.last_local")}
         msp, resp = timed(lambda: dg.sssp(src, out=dist, variant=_lib.SP_SSSP_PLAIN), 1, 0, stream)
         same = bool(np.array_equal(dist.cpu().numpy(), d) and np.array_equal(d_fixed, d))
     fixed["value"] = er / (msf / 1e3) / 1e9
     out.update({"value": er / (ms / 1e3) / 1e9, "unit": "GTEPS", "ms": ms, "E_r": er, "reached": nr,
-                "rounds": res[0][1], "schedule": sched, "fixed_schedule": fixed,
+                "rounds": res[0][1], "relaxed_per_edge": round(relaxed / max(1, er), 3), "schedule": sched,
+                "fixed_schedule": fixed,
                 "plain": {"value": er / (msp / 1e3) / 1e9, "ms": msp, "rounds": resp[0][1]},
                 "same_distances_all_forms": same,
                 "roofline": roof(12 * er + 12 * g.V, ms, hbm)})

@@ -101,12 +101,18 @@ int sp_graph_info(sp_graph_h g, int32_t* V, int64_t* E, int32_t* symmetric);
  *             edge weight).
  *   "sssp.ctas_per_sm"  SSSP: persistent CTAs per SM of the delta-stepping kernel (1..8,
  *             default 4; fewer CTAs make each grid barrier cheaper on high-diameter graphs).
- *   "sssp.last_delta", "sssp.last_ctas" (read only): the schedule the last SSSP call ran.
+ *   "sssp.last_delta", "sssp.last_ctas", "sssp.last_local" (read only): the schedule the
+ *             last SSSP call ran; "sssp.last_relaxed": the edges it relaxed (each
+ *             out-edge of a vertex once per time the vertex was expanded).
  *   "tc.cta_warps"  TC on graphs of up to 65536 vertices: 0 = a bitmap per warp;
  *             2, 4, 8 or 16 = one bitmap per CTA of that many warps sharing each anchor.
  *   "sssp.hub_deg", "sssp.hub_chunk"  SSSP: queued vertices with more out-edges than
  *             hub_deg are relaxed in hub_chunk-edge pieces shared by all warps
  *             (defaults 128 and 64).
+ *   "sssp.local"  SSSP: in rounds whose frontier is at most 32 vertices per warp, a warp
+ *             keeps relaxing the vertices it improved below the bucket threshold, up to
+ *             this many 32-edge steps per round, before the grid barrier (0 = off,
+ *             default 64). Unset, the learned scheduler chooses between 0 and 64.
  *   "bc.hub_deg", "bc.hub_chunk"  BC: level-list entries of vertices with more than
  *             hub_deg edges are cut into hub_chunk-edge pieces shared by all warps
  *             (defaults 64 and 64).
@@ -199,14 +205,15 @@ int sp_louvain(sp_graph_h g, const float* weight, double threshold, int32_t* com
 
 /* ---- learned scheduler ----------------------------------------------------------
  * No counterpart in the reference. A small MLP scores candidate schedules (for SSSP:
- * bucket width and CTAs per SM) from graph features and predicts their log run time;
+ * bucket width, CTAs per SM and warp cascades on or off) from graph features and
+ * predicts their log run time;
  * sp_sssp with delta <= 0 and no "sssp.delta" knob runs the best-scored candidate when
  * a model is loaded, else the fixed heuristic. Schedules never change results.
  * Network: x[SP_MLP_IN] -> tanh(H) -> tanh(H) -> 1, H = SP_MLP_HIDDEN, parameters
  * W1(H x IN) b1 W2(H x H) b2 w3 b3 in that order (SP_MLP_PARAMS floats). Host or device
  * pointers. sp_mlp_grad: gradient of the mean squared error (for checking against a
  * CPU reference); sp_mlp_train: full-batch Adam, all steps in one fused launch. */
-#define SP_MLP_IN 12
+#define SP_MLP_IN 13
 #define SP_MLP_HIDDEN 32
 #define SP_MLP_PARAMS (SP_MLP_HIDDEN * SP_MLP_IN + SP_MLP_HIDDEN * SP_MLP_HIDDEN + 3 * SP_MLP_HIDDEN + 1)
 int sp_mlp_forward(const float* params, const float* X, int32_t N, float* y);
@@ -216,8 +223,10 @@ int sp_mlp_train(float* params, const float* X, const float* T, int32_t N, int32
  * feat_mean/feat_scale normalise inputs: x' = (x - mean) * scale. */
 int sp_sched_load(const float* params, const float* feat_mean, const float* feat_scale);
 /* The SP_MLP_IN inputs the scheduler builds for SSSP on g with a candidate schedule
- * (delta multiple of the largest weight, CTAs per SM); weight NULL = edgeLen. */
-int sp_sssp_features(sp_graph_h g, const int32_t* weight, double delta_mult, int32_t ctas_per_sm, float* x);
+ * (delta multiple of the largest weight, CTAs per SM, cascade budget as for
+ * "sssp.local"); weight NULL = edgeLen. */
+int sp_sssp_features(sp_graph_h g, const int32_t* weight, double delta_mult, int32_t ctas_per_sm,
+                     int32_t local_steps, float* x);
 
 /* ---- PageRank without device allocation -------------------------------------------
  * No counterpart in the reference: an addition for callers that cannot call

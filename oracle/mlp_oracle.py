@@ -3,7 +3,7 @@
 starplat_b200/csrc/sp_mlp.cu. Parameter layout: W1 (H x IN), b1, W2 (H x H), b2, w3, b3."""
 import numpy as np
 
-IN, H = 12, 32
+IN, H = 13, 32
 
 
 def unpack(p):

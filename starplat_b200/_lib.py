@@ -33,7 +33,7 @@ SP_BC_BATCHED = 0
 SP_BC_PLAIN = 1
 SP_LV_TUNED = 0
 SP_LV_PLAIN = 1
-SP_MLP_IN = 12
+SP_MLP_IN = 13
 SP_MLP_HIDDEN = 32
 SP_MLP_PARAMS = SP_MLP_HIDDEN * SP_MLP_IN + SP_MLP_HIDDEN * SP_MLP_HIDDEN + 3 * SP_MLP_HIDDEN + 1
 
@@ -79,7 +79,7 @@ SIGNATURES = {
     "sp_mlp_grad": (ctypes.c_int, [vp, vp, vp, i32, vp, vp]),
     "sp_mlp_train": (ctypes.c_int, [vp, vp, vp, i32, i32, f32, vp]),
     "sp_sched_load": (ctypes.c_int, [vp, vp, vp]),
-    "sp_sssp_features": (ctypes.c_int, [vp, vp, f64, i32, vp]),
+    "sp_sssp_features": (ctypes.c_int, [vp, vp, f64, i32, i32, vp]),
     "sp_pagerank_noalloc": (ctypes.c_int, [vp, vp, vp, i32, i64, f32, f32, i32, vp, P(i32), vp]),
 }
 

@@ -6,7 +6,8 @@ Each algorithm's kernels take thresholds that change only how work is split:
             pr.src_hint: L1 policy of the srcList loads; pr.hot: sources of the
             L1-resident hot phase (0 = one phase)
   sssp      sssp.hub_deg / sssp.hub_chunk: queued vertices above hub_deg out-edges are
-            relaxed in hub_chunk-edge pieces shared by all warps
+            relaxed in hub_chunk-edge pieces shared by all warps; sssp.local: warp
+            cascade budget per round (0 = off)
   bc        bc.hub_deg / bc.hub_chunk: the same for level-list entries
 tune() times every candidate on the caller's graph with CUDA events on the graph's
 stream (median of `reps` runs after one untimed run), keeps the fastest, leaves it set
@@ -25,7 +26,7 @@ import numpy as np
 KNOBS: Dict[str, Dict[str, Sequence[int]]] = {
     "tc": {"tc.cta_warps": (0, 2, 4, 8)},
     "pagerank": {"pr.order": (0, 1), "pr.src_hint": (0, 2), "pr.hot": (0, 4096)},
-    "sssp": {"sssp.hub_deg": (64, 128, 512, 2048), "sssp.hub_chunk": (32, 64, 256)},
+    "sssp": {"sssp.hub_deg": (64, 128, 512, 2048), "sssp.hub_chunk": (32, 64, 256), "sssp.local": (0, 16, 64)},
     "bc": {"bc.hub_deg": (32, 64, 256, 4096), "bc.hub_chunk": (64, 128, 256)},
 }
 

@@ -578,6 +578,14 @@ int sp_tune_set(sp_graph_h g, const char* key, int64_t value) {
       g->sssp_hub_chunk = (int32_t)value;
     return SP_OK;
   }
+  if (!strcmp(key, "sssp.local")) {
+    if (value < 0 || value > (1 << 16)) {
+      set_error("sp_tune_set: sssp.local must be in [0, 65536]");
+      return SP_ERR_INVALID;
+    }
+    g->sssp_local = (int32_t)value;
+    return SP_OK;
+  }
   if (!strcmp(key, "bc.cluster")) {
     if (value != 0 && value != 1 && value != 2 && value != 4 && value != 8) {
       set_error("sp_tune_set: bc.cluster must be 0, 1, 2, 4 or 8");
@@ -655,12 +663,24 @@ int sp_tune_get(sp_graph_h g, const char* key, int64_t* value) {
     *value = g->sssp_last_ctas;
     return SP_OK;
   }
+  if (!strcmp(key, "sssp.last_local")) {
+    *value = g->sssp_last_local;
+    return SP_OK;
+  }
+  if (!strcmp(key, "sssp.last_relaxed")) {
+    *value = g->sssp_last_relaxed;
+    return SP_OK;
+  }
   if (!strcmp(key, "sssp.hub_deg")) {
     *value = g->sssp_hub_deg > 0 ? g->sssp_hub_deg : sssp_hub_deg_default();
     return SP_OK;
   }
   if (!strcmp(key, "sssp.hub_chunk")) {
     *value = g->sssp_hub_chunk > 0 ? g->sssp_hub_chunk : sssp_hub_chunk_default();
+    return SP_OK;
+  }
+  if (!strcmp(key, "sssp.local")) {
+    *value = g->sssp_local >= 0 ? g->sssp_local : sssp_local_default();
     return SP_OK;
   }
   if (!strcmp(key, "bc.cluster")) {

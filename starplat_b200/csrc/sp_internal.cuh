@@ -157,8 +157,11 @@ struct sp_graph {
   int32_t sssp_ctas_per_sm = 0;  // SSSP persistent CTAs per SM (0 = learned / 4)
   int64_t sssp_last_delta = 0;   // schedule of the last SSSP call (reporting)
   int32_t sssp_last_ctas = 0;
+  int32_t sssp_last_local = 0;
+  int64_t sssp_last_relaxed = 0;  // edges the last delta-stepping run relaxed
   int32_t sssp_hub_deg = 0;    // SSSP: vertices above this out-degree go to shared pieces (0 = default)
   int32_t sssp_hub_chunk = 0;  // SSSP: edges per piece (0 = default)
+  int32_t sssp_local = -1;     // SSSP: warp cascade budget in 32-edge steps per round (-1 = default, 0 = off)
   int32_t tc_cta_warps = -1;  // TC: warps per CTA of the shared-bitmap kernel (-1 = default, 0 = off)
   int32_t bc_batch = 0;
   int32_t bc_hub_deg = 0;  // BC: split level-list entries above this degree (0 = default)
@@ -185,6 +188,7 @@ int tc_cta_warps_default();           // TC kernel choice default (sp_tc.cu)
 int bc_hub_deg_default();             // BC entry-splitting defaults (sp_bc.cu)
 int sssp_hub_deg_default();           // SSSP hub-splitting defaults (sp_sssp.cu)
 int sssp_hub_chunk_default();
+int sssp_local_default();
 int bc_hub_chunk_default();
 int bc_cluster_default();
 int ensure_symmetry(sp_graph* g);     // fills g->symmetric

@@ -11,11 +11,22 @@
 //   * near queue Q (ping-pong) holds vertices whose distance dropped below the
 //     current bucket threshold; far pile F holds the rest;
 //   * relax rounds: every frontier vertex pushes along its out-edges with
-//     atomicMin; a lane walks its own edges for low degree, the whole warp
-//     cooperates on medium degree, and vertices above 2048 out-edges (R-MAT hubs)
-//     are queued in a hub list whose 256-edge chunks all warps share in the next
-//     round; queue appends are warp-aggregated and de-duplicated with per-round /
-//     per-epoch stamps;
+//     atomicMin. A warp holds up to 32 frontier vertices, one per lane, and their
+//     edges are flattened over its lanes (an exclusive scan of the degrees), 32
+//     edges per step, so a 4-neighbour grid vertex costs one step, not four; a
+//     small frontier is spread over all warps. Vertices above hub_deg out-edges
+//     (R-MAT hubs) are queued in a hub list whose chunks all warps share in the
+//     next round; queue appends are warp-aggregated and de-duplicated with
+//     per-round / per-epoch stamps;
+//   * warp-local cascades (rounds whose frontier is at most 32 vertices per warp):
+//     a vertex a warp improves below the bucket threshold goes to the warp's ring
+//     in shared memory instead of the next round's queue, and the warp relaxes its
+//     ring until it is empty or its edge budget (sssp.local warp steps) is spent,
+//     then moves what is left to the queue. On a high-diameter graph one round then
+//     covers many hops of the same bucket, where each hop used to cost a grid
+//     barrier. Ring entries carry no stamp: every improvement puts its vertex in
+//     the ring (or, when full, in the stamped queue), so the last improvement of a
+//     vertex is always relaxed after it;
 //   * when Q empties, the threshold jumps to the bucket of the smallest far
 //     distance and F is split into Q and the next far pile.
 //   Negative weights switch to delta = infinity (queue-based Bellman-Ford), bounded
@@ -33,13 +44,16 @@ namespace sp {
 
 namespace ss {
 constexpr int THREADS = 256;
-constexpr int LANE_DEG = 16;   // frontier vertices up to this out-degree are walked by one lane
 // Queued vertices above HUB_DEG out-edges are relaxed in HUB_CHUNK-edge pieces that
 // every warp shares, so no warp walks a long row alone while the others wait at the
 // round's barrier. R-MAT 23 (learned schedule): 12.6 ms at (2048, 256), 11.5 at
 // (512, 128), 11.2 at (128, 64), 12.0 at (32, 32).
 constexpr int HUB_DEG = 128;
 constexpr int HUB_CHUNK = 64;
+constexpr int HUB_DEG_MAX = 1 << 25;  // 32 entries of at most this degree sum below 2^31
+constexpr int RING = 256;             // entries of a warp's cascade ring (power of two)
+constexpr int LOCAL_STEPS = 64;       // default cascade budget: 32-edge warp steps per round
+constexpr unsigned FULL = 0xffffffffu;
 
 struct Ctl {
   GridBar bar;
@@ -51,6 +65,7 @@ struct Ctl {
   int epochs;
   int status;      // 0 ok, 1 timeout / round cap, 2 negative cycle suspected
   int pad;
+  unsigned long long relaxed;  // edges relaxed over the run (work inflation = relaxed / E_r)
 };
 
 struct Args {
@@ -70,6 +85,27 @@ struct Args {
   long long max_rounds;
   int hub_deg;          // vertices with more out-edges are relaxed in pieces by all warps
   int hub_chunk;        // edges per piece
+  int local_edges;      // cascade budget of a warp per round, in edges (0 = no cascades)
+};
+
+// Where a round's relaxations go: the next round's queue and hub list, this
+// epoch's far pile.
+struct Out {
+  int32_t* QN;
+  int* qnext;
+  int32_t* HV;
+  int32_t* HB;
+  unsigned long long* hnext;
+  int32_t* F;
+  int* fcnt;
+  int* fmin;
+};
+
+// A warp's cascade ring in shared memory; head and cnt are warp-uniform.
+struct Ring {
+  int32_t* s;
+  int head;
+  int cnt;
 };
 
 // Warp-aggregated append of `want` lanes into buf via counter.
@@ -106,7 +142,10 @@ __device__ __forceinline__ void queue_push(const Args& a, bool want, int u, int3
   warp_push(want && !hub, u, QN, qnext);
 }
 
-// Relax one edge (dv + wt to u); returns queue (1), far (2) or nothing (0).
+// Relax one edge (dv + wt to u); returns queue (1), far (2) or nothing (0). With
+// STAMP, a below-threshold improvement returns 1 only for the first of this round
+// (the vertex is then queued once); without, every improvement returns 1.
+template <bool STAMP>
 __device__ __forceinline__ int relax(const Args& a, int u, long long nd, long long thr, int round, int epoch,
                                      int* fmin_slot) {
   if (nd >= (long long)INT_MAX) return 0;
@@ -115,7 +154,7 @@ __device__ __forceinline__ int relax(const Args& a, int u, long long nd, long lo
   const int old = atomicMin(a.dist + u, ndi);
   if (ndi >= old) return 0;
   if (nd < thr) {
-    if (atomicExch(a.qstamp + u, round + 1) != round + 1) return 1;
+    if (!STAMP || atomicExch(a.qstamp + u, round + 1) != round + 1) return 1;
     return 0;
   }
   atomicMin(fmin_slot, ndi);
@@ -123,7 +162,131 @@ __device__ __forceinline__ int relax(const Args& a, int u, long long nd, long lo
   return 0;
 }
 
-__global__ void __launch_bounds__(THREADS) k_delta(Args a) {
+// Below-threshold improvements of this step (want lanes). LOCAL: into the warp's
+// ring while it has room, the rest stamped into the next round's queue. Otherwise
+// the caller's relax already stamped them: straight into the queue.
+template <bool LOCAL>
+__device__ __forceinline__ void push_near(const Args& a, bool want, int u, int round, const Out& o, Ring& r) {
+  if (LOCAL) {
+    const unsigned m = __ballot_sync(FULL, want);
+    if (!m) return;
+    const int lane = threadIdx.x & 31;
+    const int room = RING - r.cnt;
+    const int rank = __popc(m & ((1u << lane) - 1u));
+    const bool mine = want && rank < room;
+    if (mine) r.s[(r.head + r.cnt + rank) & (RING - 1)] = u;
+    r.cnt += min(__popc(m), room);
+    want = want && !mine && atomicExch(a.qstamp + u, round + 1) != round + 1;
+  }
+  queue_push(a, want, u, o.QN, o.qnext, o.HV, o.HB, o.hnext);
+}
+
+// Relax the out-edges of the warp's batch: lane i holds frontier vertex v (or -1).
+// Lane i's edges take positions [excl_i, excl_i + d_i) of the flattened batch; in a
+// step, lane t relaxes position t0 + t, owned by the last lane j with excl_j <= t0 + t
+// (a lane of degree 0 is never that last lane). LOCAL also sends vertices above
+// hub_deg (which only the ring can hold) to the next round's hub list. `work` counts
+// the edges relaxed.
+template <bool LOCAL>
+__device__ __forceinline__ void relax_batch(const Args& a, int v, long long thr, int round, int epoch, const Out& o,
+                                            Ring& r, int& work) {
+  const int lane = threadIdx.x & 31;
+  int b = 0, d = 0;
+  long long dv = 0;
+  bool hub = false;
+  if (v >= 0) {
+    b = a.off[v];
+    d = a.off[v + 1] - b;
+    if (LOCAL && d > a.hub_deg) {
+      hub = true;
+      d = 0;
+    } else {
+      dv = __ldcg(a.dist + v);
+    }
+  }
+  if (LOCAL) queue_push(a, hub && atomicExch(a.qstamp + v, round + 1) != round + 1, v, o.QN, o.qnext, o.HV, o.HB,
+                        o.hnext);
+  int inc = d;
+#pragma unroll
+  for (int k = 1; k < 32; k <<= 1) {
+    const int t = __shfl_up_sync(FULL, inc, k);
+    if (lane >= k) inc += t;
+  }
+  const int total = __shfl_sync(FULL, inc, 31);
+  const int excl = inc - d;
+  work += total;
+  for (int t0 = 0; t0 < total; t0 += 32) {
+    const int t = t0 + lane;
+    int j = 0;
+#pragma unroll
+    for (int k = 16; k > 0; k >>= 1)
+      if (__shfl_sync(FULL, excl, j + k) <= t) j += k;
+    const int jb = __shfl_sync(FULL, b, j);
+    const int je = __shfl_sync(FULL, excl, j);
+    const long long jd = __shfl_sync(FULL, dv, j);
+    int res = 0, u = 0;
+    if (t < total) {
+      const int k = jb + (t - je);
+      u = a.adj[k];
+      res = relax<!LOCAL>(a, u, jd + a.w[k], thr, round, epoch, o.fmin);
+    }
+    push_near<LOCAL>(a, res == 1, u, round, o, r);
+    warp_push(res == 2, u, o.F, o.fcnt);
+  }
+}
+
+// Edges [vb, ve) of one vertex at distance vd, 32 per step (a hub piece).
+template <bool LOCAL>
+__device__ __forceinline__ void relax_range(const Args& a, int vb, int ve, long long vd, long long thr, int round,
+                                            int epoch, const Out& o, Ring& r) {
+  const int lane = threadIdx.x & 31;
+  for (int k0 = vb; k0 < ve; k0 += 32) {
+    const int k = k0 + lane;
+    int res = 0, u = 0;
+    if (k < ve) {
+      u = a.adj[k];
+      res = relax<!LOCAL>(a, u, vd + a.w[k], thr, round, epoch, o.fmin);
+    }
+    push_near<LOCAL>(a, res == 1, u, round, o, r);
+    warp_push(res == 2, u, o.F, o.fcnt);
+  }
+}
+
+// Warp-local cascade: relax the ring, 32 entries at a time, until it is empty or the
+// warp has relaxed a.local_edges edges; what is left goes to the next round's queue.
+// Each pass either relaxes edges (work grows) or only pops, so the loop ends.
+__device__ __forceinline__ void cascade(const Args& a, long long thr, int round, int epoch, const Out& o, Ring& r,
+                                        int& relaxed) {
+  const int lane = threadIdx.x & 31;
+  int work = 0;
+  while (r.cnt > 0 && work < a.local_edges) {
+    __syncwarp();
+    const int take = min(r.cnt, 32);
+    const int v = lane < take ? r.s[(r.head + lane) & (RING - 1)] : -1;
+    __syncwarp();
+    r.head = (r.head + take) & (RING - 1);
+    r.cnt -= take;
+    relax_batch<true>(a, v, thr, round, epoch, o, r, work);
+  }
+  relaxed += work;
+  __syncwarp();
+  for (int i0 = 0; i0 < r.cnt; i0 += 32) {
+    const int i = i0 + lane;
+    int u = 0;
+    bool want = false;
+    if (i < r.cnt) {
+      u = r.s[(r.head + i) & (RING - 1)];
+      want = atomicExch(a.qstamp + u, round + 1) != round + 1;
+    }
+    queue_push(a, want, u, o.QN, o.qnext, o.HV, o.HB, o.hnext);
+  }
+  __syncwarp();
+  r.head = 0;
+  r.cnt = 0;
+}
+
+__global__ void __launch_bounds__(THREADS, 4) k_delta(Args a) {
+  __shared__ int32_t ring[(THREADS / 32) * RING];
   Ctl* c = a.ctl;
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * THREADS + threadIdx.x) >> 5;
@@ -143,58 +306,20 @@ __global__ void __launch_bounds__(THREADS) k_delta(Args a) {
     }
     if (qv > 0 || hn > 0) {
       const int32_t* Q = a.q[round & 1];
-      int32_t* QN = a.q[(round + 1) & 1];
-      int* qnext = &c->qcount[(round + 1) % 3];
-      int32_t* HV = a.hv[(round + 1) & 1];
-      int32_t* HB = a.hbase[(round + 1) & 1];
-      unsigned long long* hnext = &c->hcount[(round + 1) % 3];
-      int32_t* F = a.f[epoch & 1];
-      int* fcnt = &c->fcount[epoch % 3];
-      int* fmin = &c->fmin[epoch % 3];
-      for (int base = gw * 32; base < qn; base += nw * 32) {
-        const int i = base + lane;
-        int v = -1, b = 0, e = 0;
-        long long dv = 0;
-        if (i < qn) {
-          v = Q[i];
-          b = a.off[v];
-          e = a.off[v + 1];
-          dv = __ldcg(a.dist + v);
-        }
-        const int d = e - b;
-        const bool big = d > LANE_DEG;
-        // lanes with small out-degree walk their own edges, converged step by step
-        int steps = big ? 0 : d;
-#pragma unroll 1
-        for (int o = 16; o > 0; o >>= 1) steps = max(steps, __shfl_xor_sync(0xffffffffu, steps, o));
-        for (int j = 0; j < steps; ++j) {
-          int res = 0, u = 0;
-          if (!big && j < d) {
-            u = a.adj[b + j];
-            res = relax(a, u, dv + a.w[b + j], thr, round, epoch, fmin);
-          }
-          queue_push(a, res == 1, u, QN, qnext, HV, HB, hnext);
-          warp_push(res == 2, u, F, fcnt);
-        }
-        // high-degree vertices: whole warp, one vertex at a time
-        unsigned bigm = __ballot_sync(0xffffffffu, big);
-        while (bigm) {
-          const int l = __ffs(bigm) - 1;
-          bigm &= bigm - 1;
-          const int vb = __shfl_sync(0xffffffffu, b, l);
-          const int ve = __shfl_sync(0xffffffffu, e, l);
-          const long long vd = __shfl_sync(0xffffffffu, dv, l);
-          for (int k0 = vb; k0 < ve; k0 += 32) {
-            const int k = k0 + lane;
-            int res = 0, u = 0;
-            if (k < ve) {
-              u = a.adj[k];
-              res = relax(a, u, vd + a.w[k], thr, round, epoch, fmin);
-            }
-            queue_push(a, res == 1, u, QN, qnext, HV, HB, hnext);
-            warp_push(res == 2, u, F, fcnt);
-          }
-        }
+      const Out o = {a.q[(round + 1) & 1], &c->qcount[(round + 1) % 3], a.hv[(round + 1) & 1],
+                     a.hbase[(round + 1) & 1], &c->hcount[(round + 1) % 3], a.f[epoch & 1], &c->fcount[epoch % 3],
+                     &c->fmin[epoch % 3]};
+      Ring r = {ring + (threadIdx.x >> 5) * RING, 0, 0};
+      // a small frontier is spread over all warps (fewer entries per warp, fewer steps)
+      const int per = min(32, max(1, (qn + nw - 1) / nw));
+      const bool local = a.local_edges > 0 && qn <= nw * 32;
+      int work = 0;
+      for (int base = gw * per; base < qn; base += nw * per) {
+        const int v = (lane < per && base + lane < qn) ? Q[base + lane] : -1;
+        if (local)
+          relax_batch<true>(a, v, thr, round, epoch, o, r, work);
+        else
+          relax_batch<false>(a, v, thr, round, epoch, o, r, work);
       }
       // hub pieces of this round: hub_chunk edges per warp, all warps
       {
@@ -210,18 +335,15 @@ __global__ void __launch_bounds__(THREADS) k_delta(Args a) {
           const long long vd = __ldcg(a.dist + v);
           const int vb = a.off[v] + (ch - HBc[lo]) * a.hub_chunk;
           const int ve = min(vb + a.hub_chunk, a.off[v + 1]);
-          for (int k0 = vb; k0 < ve; k0 += 32) {
-            const int k = k0 + lane;
-            int res = 0, u = 0;
-            if (k < ve) {
-              u = a.adj[k];
-              res = relax(a, u, vd + a.w[k], thr, round, epoch, fmin);
-            }
-            queue_push(a, res == 1, u, QN, qnext, HV, HB, hnext);
-            warp_push(res == 2, u, F, fcnt);
-          }
+          work += max(0, ve - vb);
+          if (local)
+            relax_range<true>(a, vb, ve, vd, thr, round, epoch, o, r);
+          else
+            relax_range<false>(a, vb, ve, vd, thr, round, epoch, o, r);
         }
       }
+      if (local) cascade(a, thr, round, epoch, o, r, work);
+      if (lane == 0 && work > 0) atomicAdd(&c->relaxed, (unsigned long long)work);
       if (blockIdx.x == 0 && threadIdx.x == 0) {
         c->qcount[(round + 2) % 3] = 0;  // read two rounds ago
         c->hcount[(round + 2) % 3] = 0ull;
@@ -312,6 +434,7 @@ __global__ void k_init(int V, int src, int32_t* dist, int32_t* qstamp, int32_t* 
       c->fmin[k] = INT_MAX;
     }
     c->rounds = c->epochs = c->status = 0;
+    c->relaxed = 0ull;
   }
 }
 
@@ -371,13 +494,14 @@ struct SsspPlan {
   // the learned choice of the last call: its inputs are the graph and the weight range
   // only, so it is reused while the range and the loaded model stay the same
   unsigned sel_gen = 0;
-  int sel_wmin = 0, sel_wmax = 0, sel_ctas = 0;
+  int sel_wmin = 0, sel_wmax = 0, sel_ctas = 0, sel_local = 0, sel_local_knob = -1;
   int64_t sel_delta = 0;
 };
 
 void free_sssp_plan(SsspPlan* p) { delete p; }
 int sssp_hub_deg_default() { return ss::HUB_DEG; }
 int sssp_hub_chunk_default() { return ss::HUB_CHUNK; }
+int sssp_local_default() { return ss::LOCAL_STEPS; }
 
 static int sssp_prepare(sp_graph* g, const int32_t* weight, const int32_t** wdev) {
   if (!g->sssp) g->sssp = new SsspPlan();
@@ -413,8 +537,9 @@ int mlp_score(const std::vector<float>& X, std::vector<float>& y, cudaStream_t s
 unsigned mlp_generation();  // 0 = no model loaded
 
 // Scheduler inputs (SP_MLP_IN): graph shape and weight range, then the candidate
-// schedule (log2 of the delta multiple of the largest weight, CTAs per SM).
-static int sssp_features(sp_graph* g, double mult, int ctas, float* x) {
+// schedule (log2 of the delta multiple of the largest weight, CTAs per SM, warp
+// cascade budget).
+static int sssp_features(sp_graph* g, double mult, int ctas, int local, float* x) {
   SP_TRY(ensure_symmetry(g));
   const double V = g->V, E = (double)g->E, avg = E / V;
   const double mx = g->max_out_deg, wmax = std::max(1, g->sssp->w_max), wmin = g->sssp->w_min;
@@ -430,11 +555,12 @@ static int sssp_features(sp_graph* g, double mult, int ctas, float* x) {
   x[9] = (float)ctas;
   x[10] = (float)(std::log2(mult) * std::log2(V));  // interaction: bucket width vs size
   x[11] = (float)(ctas * avg);
+  x[12] = (float)std::log2(1.0 + local);
   return SP_OK;
 }
 
 static int sssp_delta(sp_graph* g, const int32_t* w, int32_t src, int32_t* dist_out, int64_t delta, int ctas,
-                      int32_t* rounds_out) {
+                      int local, int32_t* rounds_out) {
   SsspPlan* p = g->sssp;
   cudaStream_t s = g->stream;
   const int V = g->V;
@@ -473,8 +599,9 @@ static int sssp_delta(sp_graph* g, const int32_t* w, int32_t src, int32_t* dist_
   // Bellman-Ford needs at most V-1 rounds of improvement per vertex chain; far more
   // rounds than V * 4 + 64 can only come from a negative cycle.
   a.max_rounds = (long long)V * 4 + 64;
-  a.hub_deg = g->sssp_hub_deg > 0 ? g->sssp_hub_deg : ss::HUB_DEG;
+  a.hub_deg = std::min(g->sssp_hub_deg > 0 ? g->sssp_hub_deg : ss::HUB_DEG, ss::HUB_DEG_MAX);
   a.hub_chunk = g->sssp_hub_chunk > 0 ? g->sssp_hub_chunk : ss::HUB_CHUNK;
+  a.local_edges = 32 * local;
   ss::k_init<<<num_sms() * 4, 256, 0, s>>>(V, src, p->dist.p, p->qstamp.p, p->fstamp.p, p->q0.p, p->h0.p, p->hb0.p,
                                             g->off.p, p->ctl.p, a.hub_deg, a.hub_chunk);
   SP_CHECK_LAUNCH();
@@ -487,6 +614,7 @@ static int sssp_delta(sp_graph* g, const int32_t* w, int32_t src, int32_t* dist_
   ss::Ctl hc;
   SP_TRY(copy_out(&hc, p->ctl.p, sizeof(hc), s));
   if (rounds_out) *rounds_out = hc.rounds;
+  g->sssp_last_relaxed = (int64_t)hc.relaxed;
   if (hc.status != 0 || hc.bar.error) {
     if (negative && !hc.bar.error) {
       set_error("sp_sssp: no fixed point after %d rounds (negative cycle)", hc.rounds);
@@ -556,56 +684,71 @@ extern "C" int sp_sssp(sp_graph_h g, const int32_t* weight, int32_t src, int32_t
     return SP_ERR_INVALID;
   }
   int ctas = g->sssp_ctas_per_sm > 0 ? g->sssp_ctas_per_sm : 4;
+  int local = g->sssp_local >= 0 ? g->sssp_local : ss::LOCAL_STEPS;
   const int64_t wmax = std::max<int64_t>(1, (int64_t)g->sssp->w_max);
   if (delta <= 0 && g->sssp_delta > 0) delta = g->sssp_delta;
   SsspPlan* sp_ = g->sssp;
   const unsigned gen = mlp_generation();
   if (delta <= 0 && g->sssp_ctas_per_sm == 0 && gen != 0 && sp_->sel_gen == gen && sp_->sel_wmin == sp_->w_min &&
-      sp_->sel_wmax == sp_->w_max) {
+      sp_->sel_wmax == sp_->w_max && sp_->sel_local_knob == g->sssp_local) {
     delta = sp_->sel_delta;  // same inputs as the last scored call
     ctas = sp_->sel_ctas;
+    local = sp_->sel_local;
   }
   if (delta <= 0 && g->sssp_ctas_per_sm == 0 && gen != 0) {
-    // learned schedule: score every candidate, run the best (fixed heuristic if no model)
+    // learned schedule: score every candidate, run the best (fixed heuristic if no
+    // model). The cascade budget is a candidate too unless the sssp.local knob is set.
     static const double mults[] = {1, 2, 4, 8, 16, 32, 64};
     static const int cts[] = {1, 2, 4};
+    const int locs[2] = {0, ss::LOCAL_STEPS};
+    const int nloc = g->sssp_local >= 0 ? 1 : 2;
     std::vector<float> X;
-    std::vector<std::pair<double, int>> cand;
+    struct Cand {
+      double mult;
+      int ctas, local;
+    };
+    std::vector<Cand> cand;
     for (double m : mults)
-      for (int c : cts) {
-        float x[SP_MLP_IN];
-        SP_TRY(sssp_features(g, m, c, x));
-        X.insert(X.end(), x, x + SP_MLP_IN);
-        cand.push_back({m, c});
-      }
+      for (int c : cts)
+        for (int l = 0; l < nloc; ++l) {
+          const int lv = g->sssp_local >= 0 ? g->sssp_local : locs[l];
+          float x[SP_MLP_IN];
+          SP_TRY(sssp_features(g, m, c, lv, x));
+          X.insert(X.end(), x, x + SP_MLP_IN);
+          cand.push_back({m, c, lv});
+        }
     std::vector<float> score;
     if (mlp_score(X, score, g->stream) == SP_OK) {
       int best = 0;
       for (int k = 1; k < (int)score.size(); ++k)
         if (score[k] < score[best]) best = k;
-      delta = (int64_t)std::llround(cand[best].first * (double)wmax);
-      ctas = cand[best].second;
+      delta = (int64_t)std::llround(cand[best].mult * (double)wmax);
+      ctas = cand[best].ctas;
+      local = cand[best].local;
       sp_->sel_gen = gen;
       sp_->sel_wmin = sp_->w_min;
       sp_->sel_wmax = sp_->w_max;
       sp_->sel_delta = delta;
       sp_->sel_ctas = ctas;
+      sp_->sel_local = local;
+      sp_->sel_local_knob = g->sssp_local;
     }
   }
   if (delta <= 0) delta = wmax;
   g->sssp_last_delta = delta;
   g->sssp_last_ctas = ctas;
-  return sssp_delta(g, w, src, dist, delta, ctas, rounds);
+  g->sssp_last_local = local;
+  return sssp_delta(g, w, src, dist, delta, ctas, local, rounds);
 }
 
 extern "C" int sp_sssp_features(sp_graph_h g, const int32_t* weight, double delta_mult, int32_t ctas_per_sm,
-                                float* x) {
+                                int32_t local_steps, float* x) {
   using namespace sp;
-  if (!g || !x || !(delta_mult > 0) || ctas_per_sm <= 0) {
+  if (!g || !x || !(delta_mult > 0) || ctas_per_sm <= 0 || local_steps < 0) {
     set_error("sp_sssp_features: invalid argument");
     return SP_ERR_INVALID;
   }
   const int32_t* w = nullptr;
   SP_TRY(sssp_prepare(g, weight, &w));
-  return sssp_features(g, delta_mult, ctas_per_sm, x);
+  return sssp_features(g, delta_mult, ctas_per_sm, local_steps, x);
 }

@@ -1,14 +1,16 @@
-"""Learned schedule selection for SSSP (bucket width and CTAs per SM).
+"""Learned schedule selection for SSSP (bucket width, CTAs per SM, warp cascades).
 
 The network (csrc/sp_mlp.cu) predicts the log run time of SSSP on a graph under a
-candidate schedule from 12 inputs the library builds itself (sp_sssp_features:
+candidate schedule from 13 inputs the library builds itself (sp_sssp_features:
 graph size, degree skew, symmetry, weight range, the candidate). It is trained on
 timings this method generates (``collect`` times every candidate on a set of
 training graphs with CUDA events) by the project's own fused training kernel
 (``sp_mlp_train``), and loaded with ``sp_sched_load``; from then on sp_sssp with no
-explicit delta scores all 21 candidates on the GPU and runs the best one. Without a
-model the fixed heuristic (delta = largest weight, 4 CTAs per SM) runs. Schedules
-change speed only: distances are exact either way.
+explicit delta scores all 42 candidates on the GPU and runs the best one. Warp
+cascades (the sssp.local knob) pay on thin, high-diameter frontiers and cost on
+skewed ones, so they are part of the choice. Without a model the fixed heuristic
+(delta = largest weight, 4 CTAs per SM, cascades of 64 steps) runs. Schedules change
+speed only: distances are exact either way.
 
     python -m starplat_b200.scheduler train     # collect, train, write sched_model.json
 """
@@ -30,7 +32,8 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 MODEL_PATH = os.path.join(_HERE, "sched_model.json")
 MULTS = (1, 2, 4, 8, 16, 32, 64)
 CTAS = (1, 2, 4)
-CANDIDATES = [(m, c) for m in MULTS for c in CTAS]
+LOCALS = (0, 64)  # warp cascade budget per round (sssp.local), off or the default
+CANDIDATES = [(m, c, l) for m in MULTS for c in CTAS for l in LOCALS]
 IN, P = _lib.SP_MLP_IN, _lib.SP_MLP_PARAMS
 
 f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
@@ -84,11 +87,12 @@ def mlp_train(params, X, T, steps: int, lr: float):
     return p, float(loss[0])
 
 
-def features(dg, mult: float, ctas: int, weight=None) -> np.ndarray:
+def features(dg, mult: float, ctas: int, local: int = 64, weight=None) -> np.ndarray:
     from .device import _ptr
 
     x = np.empty(IN, np.float32)
-    check("sp_sssp_features", lib().sp_sssp_features(dg.handle, _ptr(weight), float(mult), int(ctas), x.ctypes.data))
+    check("sp_sssp_features", lib().sp_sssp_features(dg.handle, _ptr(weight), float(mult), int(ctas), int(local),
+                                                     x.ctypes.data))
     return x
 
 
@@ -137,12 +141,12 @@ def training_graphs():
         src = int(G.pick_sources(g, 1, seed=seed)[0])
         out.append((name, g, src))
 
-    for sc in (14, 16, 18):
+    for sc in (14, 16, 18, 20):
         add(f"rmat{sc}d_w100", G.rmat(sc, 16, seed=sc, directed=True), 1, 100, False, sc)
     add("rmat17d_ef8_w1000", G.rmat(17, 8, seed=5, directed=True), 1, 1000, False, 5)
     for sc in (15, 17):
         add(f"rmat{sc}u_w100", G.rmat(sc, 16, seed=sc + 100), 1, 100, True, sc)
-    for n in (128, 256, 512, 1024, 2048):
+    for n in (128, 256, 512, 1024, 2048, 3072):
         add(f"grid{n}_w1000", G.grid(n, n), 1, 1000, True, n)
     add("grid512_w100", G.grid(512, 512), 1, 100, True, 7)
     add("er16_d4", G.erdos_renyi(1 << 16, 4, seed=3), 1, 100, True, 3)
@@ -151,11 +155,12 @@ def training_graphs():
     return out
 
 
-def time_sssp(dg, src, mult, ctas, wmax, reps=3):
+def time_sssp(dg, src, mult, ctas, wmax, reps=3, local=64):
     import torch
 
     dg.tune_set("sssp.delta", max(1, int(round(mult * wmax))))
     dg.tune_set("sssp.ctas_per_sm", ctas)
+    dg.tune_set("sssp.local", local)
     out = torch.empty(dg.V, dtype=torch.int32, device="cuda")
     dg.sssp(src, out=out)  # warm-up
     best = None
@@ -170,6 +175,7 @@ def time_sssp(dg, src, mult, ctas, wmax, reps=3):
         best = t if best is None else min(best, t)
     dg.tune_set("sssp.delta", 0)
     dg.tune_set("sssp.ctas_per_sm", 0)
+    dg.tune_set("sssp.local", 64)
     return best
 
 
@@ -183,13 +189,13 @@ def collect(graphs, reps: int = 3, log=print):
         wmax = int(g.edgeLen.max()) if g.E else 1
         with DeviceGraph.from_csr(g) as dg:
             dg.set_stream(torch.cuda.current_stream())
-            for m, c in CANDIDATES:
-                ms = time_sssp(dg, src, m, c, wmax, reps)
-                rows.append(features(dg, m, c))
+            for m, c, l in CANDIDATES:
+                ms = time_sssp(dg, src, m, c, wmax, reps, l)
+                rows.append(features(dg, m, c, l))
                 targets.append(math.log(ms))
-                meta.append((name, m, c, ms))
-        best = min((x for x in meta if x[0] == name), key=lambda x: x[3])
-        log(f"  {name}: best delta={best[1]}x ctas={best[2]} {best[3]:.3f} ms")
+                meta.append((name, m, c, l, ms))
+        best = min((x for x in meta if x[0] == name), key=lambda x: x[4])
+        log(f"  {name}: best delta={best[1]}x ctas={best[2]} local={best[3]} {best[4]:.3f} ms")
     return np.array(rows, np.float32), np.array(targets, np.float32), meta
 
 
@@ -240,7 +246,7 @@ def main(argv=None):
     d = {"params": params.tolist(), "feat_mean": mean.tolist(), "feat_scale": scale.tolist(),
          "candidates": CANDIDATES, "train_loss": loss, "samples": int(X.shape[0]),
          "leave_one_graph_out_regret": loo, "train_regret": regret(params, mean, scale, X, T, meta),
-         "timings_ms": [[m[0], m[1], m[2], round(m[3], 4)] for m in meta],
+         "timings_ms": [[m[0], m[1], m[2], m[3], round(m[4], 4)] for m in meta],
          "gpu": torch.cuda.get_device_name(0), "collect_and_train_s": round(time.time() - t0, 1)}
     with open(out, "w") as f:
         json.dump(d, f, indent=1)

@@ -68,6 +68,47 @@ def test_sssp_hub_splitting_knobs_keep_distances_exact(hub_deg, chunk):
         dg.tune_set("sssp.hub_chunk", 0)
 
 
+@pytest.mark.parametrize("local", [0, 1, 2, 64, 65536])
+def test_sssp_warp_cascade_budget_keeps_distances_exact(local):
+    # the cascade ring (256 entries per warp) overflows into the stamped queue on the
+    # star and R-MAT; the grid cascades for many hops; budget 1 stops after one step
+    from graphs import star
+
+    cases = [(weighted(G.rmat(13, 16, seed=8, directed=True), 1, 100), None),
+             (weighted(star(5000, directed_in=False), 1, 9), None),
+             (weighted(G.grid(64, 80), 1, 1000), None), (weighted(G.grid(64, 80), 1, 1000), 2**31 - 1),
+             (weighted(G.grid(64, 80), 1, 1000), 1)]
+    for g, delta in cases:
+        dg = device_graph(g)
+        dg.tune_set("sssp.local", local)
+        assert dg.tune_get("sssp.local") == local
+        for src in (0, g.V // 2):
+            check(g, src, **({} if delta is None else {"delta": delta}))
+        dg.tune_set("sssp.hub_deg", 3)  # hubs popped from a ring go to the hub list
+        check(g, g.V - 1, **({} if delta is None else {"delta": delta}))
+        dg.tune_set("sssp.hub_deg", 0)
+        dg.tune_set("sssp.local", 64)
+
+
+def test_sssp_cascade_with_negative_weights():
+    rng = np.random.default_rng(2)
+    n = 400
+    pairs = np.array([(i, j) for i in range(n) for j in rng.choice(n, 5) if i < j], np.int32)
+    g = from_pairs(n, pairs, name="dag2")
+    g.edgeLen = rng.integers(-50, 100, g.E).astype(np.int32)
+    dg = device_graph(g)
+    for local in (0, 4, 1000):
+        dg.tune_set("sssp.local", local)
+        check(g, 0)
+    c = from_pairs(3, [[0, 1], [1, 2], [2, 0]], name="negcycle2")
+    c.edgeLen = np.array([1, -5, 1], np.int32)
+    dc = device_graph(c)
+    dc.tune_set("sssp.local", 1000)
+    with pytest.raises(_lib.SPError) as ei:
+        dc.sssp(0)
+    assert ei.value.status == -6
+
+
 def test_sssp_tuned_delta_knob():
     g = weighted(G.grid(30, 30), 1, 1000)
     dg = device_graph(g)
