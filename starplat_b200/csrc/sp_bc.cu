@@ -21,10 +21,11 @@
 //    sigma with FP64 atomics (integer-valued, so the sum is exact in any order);
 //  * backward level d: the masks of level d+1 are scattered into a dense array; for
 //    each (v, mask) of level d the lanes pull sigma/delta of the successors in edge
-//    order — no atomics, deterministic;
-//  * level-list entries of vertices with more than 4096 edges (R-MAT hubs) are cut
-//    into 256-edge pieces that all warps share (one extra barrier per level);
-//    their backward partials meet in an FP64 scratch through atomics;
+//    order, the loads of BU successors in flight together — no atomics,
+//    deterministic;
+//  * level-list entries of vertices with more than hub_deg edges (default 64) are cut
+//    into hub_chunk-edge pieces (default 64) that all warps share (one extra barrier
+//    per level); their backward partials meet in an FP64 scratch through atomics;
 //  * BC accumulates per vertex over the batch's sources in source order (FP64).
 // One cooperative launch runs every batch of a graph (bounded grid barriers); the
 // many-small-graphs form runs one CTA per graph in a persistent launch with a
@@ -51,6 +52,12 @@ constexpr int CTA_THREADS = 512;
 constexpr int HUB_DEG = 64;
 constexpr int HUB_CHUNK = 64;
 constexpr int CLUSTER_DEFAULT = 1;  // CTAs per graph in the many-graphs form (bc.cluster)
+// Successors whose sigma / delta loads are in flight together in the backward sweep,
+// with the grid kernel held to 64 registers (4 CTAs per SM). R-MAT 20, 256 sources:
+// 110 ms with one at a time, 87 ms with 2 at 64 registers, 97 ms with 2 at 78
+// registers (3 CTAs per SM), 121 ms with 4 at 128 registers; 1000 ER graphs: 135 ->
+// 104 ms.
+constexpr int BU = 2;
 
 struct Work {
   const int32_t* __restrict__ off;  // CSR rows of this graph (global edge indices)
@@ -251,32 +258,68 @@ __device__ void backward_entry(const Work& W, int i, int lane, int eb, int ee, b
       w = W.adj[j] - W.vbase;
       s = m & W.dense[w];
     }
+    // Successors are taken BU at a time: all their sigma / delta loads are issued
+    // before any is summed (one memory latency per BU successors instead of per
+    // successor), and the sums still run in edge order.
     unsigned em = __ballot_sync(0xffffffffu, s != 0ull);
     while (em) {
       if (GS == 16) {
-        int from;
-        const int ml = half_pick(em, lane, from);
-        const unsigned long long sm = shfl64(s, from);
-        const int wm = __shfl_sync(0xffffffffu, w, from);
         const int b = lane & 15;
-        if (ml >= 0 && ((sm >> b) & 1ull)) {
-          const size_t x = (size_t)wm * SW + b;
-          accg += svg / W.sigma[x] * (1.0 + (double)W.delta[x]);
+        int wm[BU];
+        bool on[BU];
+#pragma unroll
+        for (int u = 0; u < BU; ++u) {
+          int from;
+          const int ml = half_pick(em, lane, from);  // -1 once em is empty
+          from = max(from, 0);
+          const unsigned long long sm = shfl64(s, from);
+          wm[u] = __shfl_sync(0xffffffffu, w, from);
+          on[u] = ml >= 0 && ((sm >> b) & 1ull);
         }
+        double sg[BU];
+        float dl[BU];
+#pragma unroll
+        for (int u = 0; u < BU; ++u) {
+          if (on[u]) {
+            const size_t x = (size_t)wm[u] * SW + b;
+            sg[u] = W.sigma[x];
+            dl[u] = W.delta[x];
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < BU; ++u)
+          if (on[u]) accg += svg / sg[u] * (1.0 + (double)dl[u]);
         continue;
       }
-      const int l = __ffs(em) - 1;
-      em &= em - 1;
-      const unsigned long long sl = shfl64(s, l);
-      const int wl = __shfl_sync(0xffffffffu, w, l);
+      int wl[BU];
+      unsigned pm = 0;  // bit u * NW + k: successor u has source bit lane + 32 k
 #pragma unroll
-      for (int k = 0; k < NW; ++k) {
-        const int b = lane + 32 * k;
-        if ((sl >> b) & 1ull) {
-          const size_t x = (size_t)wl * SW + b;
-          acc[k] += sv[k] / W.sigma[x] * (1.0 + (double)W.delta[x]);
-        }
+      for (int u = 0; u < BU; ++u) {
+        const bool have = em != 0u;
+        const int l = have ? __ffs(em) - 1 : 0;
+        em &= em - 1;
+        const unsigned long long sl = shfl64(s, l);
+        wl[u] = __shfl_sync(0xffffffffu, w, l);
+#pragma unroll
+        for (int k = 0; k < NW; ++k)
+          if (have && ((sl >> (lane + 32 * k)) & 1ull)) pm |= 1u << (u * NW + k);
       }
+      double sg[BU][NW];
+      float dl[BU][NW];
+#pragma unroll
+      for (int u = 0; u < BU; ++u)
+#pragma unroll
+        for (int k = 0; k < NW; ++k)
+          if ((pm >> (u * NW + k)) & 1u) {
+            const size_t x = (size_t)wl[u] * SW + lane + 32 * k;
+            sg[u][k] = W.sigma[x];
+            dl[u][k] = W.delta[x];
+          }
+#pragma unroll
+      for (int u = 0; u < BU; ++u)
+#pragma unroll
+        for (int k = 0; k < NW; ++k)
+          if ((pm >> (u * NW + k)) & 1u) acc[k] += sv[k] / sg[u][k] * (1.0 + (double)dl[u][k]);
     }
   }
   if (GS == 16) acc[0] = accg + __shfl_down_sync(0xffffffffu, accg, 16);  // first half, then second
@@ -447,7 +490,7 @@ struct GridArgs {
 };
 
 template <int NW>
-__global__ void __launch_bounds__(GRID_THREADS) k_bc_grid(GridArgs a) {
+__global__ void __launch_bounds__(GRID_THREADS, 4) k_bc_grid(GridArgs a) {
   GridSync gs{a.bar};
   for (int s0 = 0; s0 < a.nsrc; s0 += a.batch) {
     if (!run_batch_any<NW>(a.W, a.srcs + s0, min(a.batch, a.nsrc - s0), gs, a.lvl_out, a.sig_out)) {
