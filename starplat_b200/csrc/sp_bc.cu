@@ -58,6 +58,9 @@ constexpr int CLUSTER_DEFAULT = 1;  // CTAs per graph in the many-graphs form (b
 // registers (3 CTAs per SM), 121 ms with 4 at 128 registers; 1000 ER graphs: 135 ->
 // 104 ms.
 constexpr int BU = 2;
+// 32-edge chunks of one entry whose loads and atomics are in flight together in the
+// forward sweep.
+constexpr int FU = 2;
 
 struct Work {
   const int32_t* __restrict__ off;  // CSR rows of this graph (global edge indices)
@@ -185,49 +188,68 @@ __device__ void expand_entry(const Work& W, int i, int lane, int eb, int ee) {
     sv[k] = ((m >> b) & 1ull) ? W.sigma[(size_t)v * SW + b] : 0.0;
   }
   const double svg = GS == 16 ? __shfl_sync(0xffffffffu, sv[0], lane & 15) : 0.0;
-  for (int c = eb; c < ee; c += 32) {
-    const int j = c + lane;
-    int w = 0;
-    unsigned long long q = 0;
-    bool isnew = false;
-    if (j < ee) {
-      w = W.adj[j] - W.vbase;
-      q = m & ~W.seen[w];
-      if (q) isnew = atomicOr(&W.nxt[w], q) == 0ull;
-    }
-    const unsigned nm = __ballot_sync(0xffffffffu, isnew);
-    if (nm) {
-      int base = 0;
-      const int leader = __ffs(nm) - 1;
-      if (lane == leader) base = atomicAdd(W.cnt, __popc(nm));
-      base = __shfl_sync(0xffffffffu, base, leader);
-      const int pos = base + __popc(nm & ((1u << lane) - 1u));
-      if (isnew) {
-        if (pos < W.cap)
-          W.flv[pos] = w;
-        else
-          atomicExch(W.err, 1);
-      }
-    }
-    unsigned em = __ballot_sync(0xffffffffu, q != 0ull);
-    while (em) {
-      if (GS == 16) {
-        int from;
-        const int ml = half_pick(em, lane, from);
-        const unsigned long long qm = shfl64(q, from);
-        const int wm = __shfl_sync(0xffffffffu, w, from);
-        const int b = lane & 15;
-        if (ml >= 0 && ((qm >> b) & 1ull)) atomicAdd(&W.sigma[(size_t)wm * SW + b], svg);
-        continue;
-      }
-      const int l = __ffs(em) - 1;
-      em &= em - 1;
-      const unsigned long long ql = shfl64(q, l);
-      const int wl = __shfl_sync(0xffffffffu, w, l);
+  // FU 32-edge chunks go together: their adj, seen and nxt accesses are each issued
+  // for all chunks before any result is waited for, and their level-list appends
+  // share one counter atomic.
+  for (int c = eb; c < ee; c += 32 * FU) {
+    int w[FU];
+    unsigned long long q[FU];
+    bool isnew[FU];
 #pragma unroll
-      for (int k = 0; k < NW; ++k) {
-        const int b = lane + 32 * k;
-        if ((ql >> b) & 1ull) atomicAdd(&W.sigma[(size_t)wl * SW + b], sv[k]);
+    for (int f = 0; f < FU; ++f) {
+      const int j = c + 32 * f + lane;
+      w[f] = j < ee ? W.adj[j] - W.vbase : -1;
+    }
+#pragma unroll
+    for (int f = 0; f < FU; ++f) q[f] = w[f] >= 0 ? m & ~W.seen[w[f]] : 0ull;
+#pragma unroll
+    for (int f = 0; f < FU; ++f) isnew[f] = q[f] ? atomicOr(&W.nxt[w[f]], q[f]) == 0ull : false;
+    unsigned nm[FU];
+    int n = 0;
+#pragma unroll
+    for (int f = 0; f < FU; ++f) {
+      nm[f] = __ballot_sync(0xffffffffu, isnew[f]);
+      n += __popc(nm[f]);
+    }
+    if (n) {
+      int base = 0;
+      if (lane == 0) base = atomicAdd(W.cnt, n);
+      base = __shfl_sync(0xffffffffu, base, 0);
+#pragma unroll
+      for (int f = 0; f < FU; ++f) {
+        if (isnew[f]) {
+          const int pos = base + __popc(nm[f] & ((1u << lane) - 1u));
+          if (pos < W.cap)
+            W.flv[pos] = w[f];
+          else
+            atomicExch(W.err, 1);
+        }
+        base += __popc(nm[f]);
+      }
+    }
+#pragma unroll
+    for (int f = 0; f < FU; ++f) {
+      unsigned em = __ballot_sync(0xffffffffu, q[f] != 0ull);
+      while (em) {
+        if (GS == 16) {
+          int from;
+          const int ml = half_pick(em, lane, from);
+          from = max(from, 0);
+          const unsigned long long qm = shfl64(q[f], from);
+          const int wm = __shfl_sync(0xffffffffu, w[f], from);
+          const int b = lane & 15;
+          if (ml >= 0 && ((qm >> b) & 1ull)) atomicAdd(&W.sigma[(size_t)wm * SW + b], svg);
+          continue;
+        }
+        const int l = __ffs(em) - 1;
+        em &= em - 1;
+        const unsigned long long ql = shfl64(q[f], l);
+        const int wl = __shfl_sync(0xffffffffu, w[f], l);
+#pragma unroll
+        for (int k = 0; k < NW; ++k) {
+          const int b = lane + 32 * k;
+          if ((ql >> b) & 1ull) atomicAdd(&W.sigma[(size_t)wl * SW + b], sv[k]);
+        }
       }
     }
   }

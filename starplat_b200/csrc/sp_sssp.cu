@@ -14,7 +14,9 @@
 //     atomicMin. A warp holds up to 32 frontier vertices, one per lane, and their
 //     edges are flattened over its lanes (an exclusive scan of the degrees), 32
 //     edges per step, so a 4-neighbour grid vertex costs one step, not four; a
-//     small frontier is spread over all warps. Vertices above hub_deg out-edges
+//     small frontier is spread over all warps. SU steps go together: their dist
+//     loads, atomicMins and stamp exchanges are all issued before any is waited
+//     for, and their queue appends share one counter atomic. Vertices above hub_deg out-edges
 //     (R-MAT hubs) are queued in a hub list whose chunks all warps share in the
 //     next round; queue appends are warp-aggregated and de-duplicated with
 //     per-round / per-epoch stamps;
@@ -53,6 +55,7 @@ constexpr int HUB_CHUNK = 64;
 constexpr int HUB_DEG_MAX = 1 << 25;  // 32 entries of at most this degree sum below 2^31
 constexpr int RING = 256;             // entries of a warp's cascade ring (power of two)
 constexpr int LOCAL_STEPS = 64;       // default cascade budget: 32-edge warp steps per round
+constexpr int SU = 4;                 // 32-edge steps whose loads and atomics are in flight together
 constexpr unsigned FULL = 0xffffffffu;
 
 struct Ctl {
@@ -142,26 +145,6 @@ __device__ __forceinline__ void queue_push(const Args& a, bool want, int u, int3
   warp_push(want && !hub, u, QN, qnext);
 }
 
-// Relax one edge (dv + wt to u); returns queue (1), far (2) or nothing (0). With
-// STAMP, a below-threshold improvement returns 1 only for the first of this round
-// (the vertex is then queued once); without, every improvement returns 1.
-template <bool STAMP>
-__device__ __forceinline__ int relax(const Args& a, int u, long long nd, long long thr, int round, int epoch,
-                                     int* fmin_slot) {
-  if (nd >= (long long)INT_MAX) return 0;
-  const int ndi = (int)nd;
-  if (ndi >= __ldcg(a.dist + u)) return 0;
-  const int old = atomicMin(a.dist + u, ndi);
-  if (ndi >= old) return 0;
-  if (nd < thr) {
-    if (!STAMP || atomicExch(a.qstamp + u, round + 1) != round + 1) return 1;
-    return 0;
-  }
-  atomicMin(fmin_slot, ndi);
-  if (atomicExch(a.fstamp + u, epoch) != epoch) return 2;
-  return 0;
-}
-
 // Below-threshold improvements of this step (want lanes). LOCAL: into the warp's
 // ring while it has room, the rest stamped into the next round's queue. Otherwise
 // the caller's relax already stamped them: straight into the queue.
@@ -179,6 +162,110 @@ __device__ __forceinline__ void push_near(const Args& a, bool want, int u, int r
     want = want && !mine && atomicExch(a.qstamp + u, round + 1) != round + 1;
   }
   queue_push(a, want, u, o.QN, o.qnext, o.HV, o.HB, o.hnext);
+}
+
+// Relax N edges per lane (nd = dist + weight for target u; nd >= INT_MAX: no edge):
+// every dist load is issued, then every atomicMin, then every stamp exchange, before
+// any result is waited for. res: 1 = improved below the bucket threshold (with
+// STAMP, only the first such improvement of u this round), 2 = improved above it
+// and first in the far pile this epoch, 0 = nothing to queue. When two edges of a
+// group hit the same vertex, the atomics decide; the loads only filter.
+template <bool STAMP, int N>
+__device__ __forceinline__ void relax_group(const Args& a, const int (&u)[N], const long long (&nd)[N],
+                                            long long thr, int round, int epoch, int* fmin_slot, int (&res)[N]) {
+  int cur[N], old[N];
+#pragma unroll
+  for (int q = 0; q < N; ++q) cur[q] = nd[q] < (long long)INT_MAX ? __ldcg(a.dist + u[q]) : INT_MIN;
+#pragma unroll
+  for (int q = 0; q < N; ++q) {
+    old[q] = INT_MIN;
+    if ((int)nd[q] < cur[q]) old[q] = atomicMin(a.dist + u[q], (int)nd[q]);
+  }
+#pragma unroll
+  for (int q = 0; q < N; ++q) {
+    res[q] = 0;
+    const int ndi = (int)nd[q];
+    if (ndi < old[q]) {
+      if (nd[q] < thr) {
+        res[q] = (!STAMP || atomicExch(a.qstamp + u[q], round + 1) != round + 1) ? 1 : 0;
+      } else {
+        atomicMin(fmin_slot, ndi);
+        res[q] = atomicExch(a.fstamp + u[q], epoch) != epoch ? 2 : 0;
+      }
+    }
+  }
+}
+
+// Appends the flagged values of N steps to buf with one counter atomic per warp.
+template <int N>
+__device__ __forceinline__ void warp_push_many(const bool (&want)[N], const int (&val)[N], int32_t* buf,
+                                               int* counter) {
+  unsigned m[N];
+  int n = 0;
+#pragma unroll
+  for (int q = 0; q < N; ++q) {
+    m[q] = __ballot_sync(FULL, want[q]);
+    n += __popc(m[q]);
+  }
+  if (n == 0) return;
+  const int lane = threadIdx.x & 31;
+  int base = 0;
+  if (lane == 0) base = atomicAdd(counter, n);
+  base = __shfl_sync(FULL, base, 0);
+  const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+  for (int q = 0; q < N; ++q) {
+    if (want[q]) buf[base + __popc(m[q] & lt)] = val[q];
+    base += __popc(m[q]);
+  }
+}
+
+// Next round's queue for N steps: vertices above hub_deg out-edges go to the hub list
+// (their degree loads all issued first), the rest with one counter atomic.
+template <int N>
+__device__ __forceinline__ void queue_push_many(const Args& a, const bool (&want)[N], const int (&u)[N],
+                                                const Out& o) {
+  int nch[N];
+#pragma unroll
+  for (int q = 0; q < N; ++q) {
+    nch[q] = 0;
+    if (want[q]) {
+      const int d = a.off[u[q] + 1] - a.off[u[q]];
+      if (d > a.hub_deg) nch[q] = (d + a.hub_chunk - 1) / a.hub_chunk;
+    }
+  }
+  bool nr[N];
+#pragma unroll
+  for (int q = 0; q < N; ++q) {
+    if (nch[q]) {
+      const unsigned long long old = atomicAdd(o.hnext, (1ull << 32) | (unsigned long long)nch[q]);
+      const int idx = (int)(old >> 32);
+      o.HV[idx] = u[q];
+      o.HB[idx] = (int)(old & 0xffffffffull);
+    }
+    nr[q] = want[q] && nch[q] == 0;
+  }
+  warp_push_many<N>(nr, u, o.QN, o.qnext);
+}
+
+// Pushes of one group: below-threshold improvements to the ring (LOCAL) or the next
+// round's queue, far ones to the far pile.
+template <bool LOCAL, int N>
+__device__ __forceinline__ void push_group(const Args& a, const int (&res)[N], const int (&u)[N], int round,
+                                           const Out& o, Ring& r) {
+  bool nr[N], fr[N];
+#pragma unroll
+  for (int q = 0; q < N; ++q) {
+    nr[q] = res[q] == 1;
+    fr[q] = res[q] == 2;
+  }
+  if (LOCAL) {
+#pragma unroll
+    for (int q = 0; q < N; ++q) push_near<true>(a, nr[q], u[q], round, o, r);
+  } else {
+    queue_push_many<N>(a, nr, u, o);
+  }
+  warp_push_many<N>(fr, u, o.F, o.fcnt);
 }
 
 // Relax the out-edges of the warp's batch: lane i holds frontier vertex v (or -1).
@@ -215,23 +302,29 @@ __device__ __forceinline__ void relax_batch(const Args& a, int v, long long thr,
   const int total = __shfl_sync(FULL, inc, 31);
   const int excl = inc - d;
   work += total;
-  for (int t0 = 0; t0 < total; t0 += 32) {
-    const int t = t0 + lane;
-    int j = 0;
+  for (int t0 = 0; t0 < total; t0 += 32 * SU) {
+    int u[SU], res[SU];
+    long long nd[SU];
 #pragma unroll
-    for (int k = 16; k > 0; k >>= 1)
-      if (__shfl_sync(FULL, excl, j + k) <= t) j += k;
-    const int jb = __shfl_sync(FULL, b, j);
-    const int je = __shfl_sync(FULL, excl, j);
-    const long long jd = __shfl_sync(FULL, dv, j);
-    int res = 0, u = 0;
-    if (t < total) {
-      const int k = jb + (t - je);
-      u = a.adj[k];
-      res = relax<!LOCAL>(a, u, jd + a.w[k], thr, round, epoch, o.fmin);
+    for (int q = 0; q < SU; ++q) {
+      const int t = t0 + 32 * q + lane;
+      int j = 0;
+#pragma unroll
+      for (int k = 16; k > 0; k >>= 1)
+        if (__shfl_sync(FULL, excl, j + k) <= t) j += k;
+      const int jb = __shfl_sync(FULL, b, j);
+      const int je = __shfl_sync(FULL, excl, j);
+      const long long jd = __shfl_sync(FULL, dv, j);
+      u[q] = 0;
+      nd[q] = INT_MAX;
+      if (t < total) {
+        const int k = jb + (t - je);
+        u[q] = a.adj[k];
+        nd[q] = jd + a.w[k];
+      }
     }
-    push_near<LOCAL>(a, res == 1, u, round, o, r);
-    warp_push(res == 2, u, o.F, o.fcnt);
+    relax_group<!LOCAL, SU>(a, u, nd, thr, round, epoch, o.fmin, res);
+    push_group<LOCAL, SU>(a, res, u, round, o, r);
   }
 }
 
@@ -240,15 +333,21 @@ template <bool LOCAL>
 __device__ __forceinline__ void relax_range(const Args& a, int vb, int ve, long long vd, long long thr, int round,
                                             int epoch, const Out& o, Ring& r) {
   const int lane = threadIdx.x & 31;
-  for (int k0 = vb; k0 < ve; k0 += 32) {
-    const int k = k0 + lane;
-    int res = 0, u = 0;
-    if (k < ve) {
-      u = a.adj[k];
-      res = relax<!LOCAL>(a, u, vd + a.w[k], thr, round, epoch, o.fmin);
+  for (int k0 = vb; k0 < ve; k0 += 32 * SU) {
+    int u[SU], res[SU];
+    long long nd[SU];
+#pragma unroll
+    for (int q = 0; q < SU; ++q) {
+      const int k = k0 + 32 * q + lane;
+      u[q] = 0;
+      nd[q] = INT_MAX;
+      if (k < ve) {
+        u[q] = a.adj[k];
+        nd[q] = vd + a.w[k];
+      }
     }
-    push_near<LOCAL>(a, res == 1, u, round, o, r);
-    warp_push(res == 2, u, o.F, o.fcnt);
+    relax_group<!LOCAL, SU>(a, u, nd, thr, round, epoch, o.fmin, res);
+    push_group<LOCAL, SU>(a, res, u, round, o, r);
   }
 }
 

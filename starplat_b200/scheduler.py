@@ -141,7 +141,7 @@ def training_graphs():
         src = int(G.pick_sources(g, 1, seed=seed)[0])
         out.append((name, g, src))
 
-    for sc in (14, 16, 18, 20):
+    for sc in (14, 16, 18, 20, 21, 22):
         add(f"rmat{sc}d_w100", G.rmat(sc, 16, seed=sc, directed=True), 1, 100, False, sc)
     add("rmat17d_ef8_w1000", G.rmat(17, 8, seed=5, directed=True), 1, 1000, False, 5)
     for sc in (15, 17):
