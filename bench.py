@@ -25,6 +25,9 @@ baseline:
   louvain_sbm1m    Louvain, planted partition 1,048,576 vertices, 256 blocks (E * sweeps / t)
   ingest_rmat20    text edge list -> device mirror (sp_graph_load_text), directed R-MAT 20
                    ef16 with weights (M edge lines / s; not a GTEPS figure)
+  centrality       per-vertex triangle counts on the TC graph (m / t), and closeness on
+                   the BC graph: unweighted over its 256 sources, weighted (U[1,100])
+                   over 16 of them (sum of E_r / t)
 Inputs are seeded synthetic graphs with the configs' shapes (no dataset is
 available offline). Every workload's inputs exceed L2 (126 MB) except the TC
 graph (7 MB CSR), which is small by definition of its config.
@@ -524,7 +527,75 @@ def bench_ingest(steps, warmup, cpu):
         shutil.rmtree(d, ignore_errors=True)
 
 
-EXTRAS = ("tc_rmat16", "sssp_rmat23", "sssp_grid4096", "bc_rmat20", "bc_er1000", "louvain_sbm1m", "ingest_rmat20")
+EXTRAS = ("tc_rmat16", "sssp_rmat23", "sssp_grid4096", "bc_rmat20", "bc_er1000", "louvain_sbm1m", "ingest_rmat20",
+          "centrality")
+
+
+def bench_centrality(steps, warmup, stream, hbm, cpu):
+    """Algorithms on the same kernels: per-vertex triangle counts (staticClusteringCoeff)
+    on the TC graph, and closeness (Compute_CC_Unweighted over BC's graph and sources,
+    Compute_CC weighted over 16 of them)."""
+    from starplat_b200 import _lib
+    from starplat_b200 import generators as G
+    from starplat_b200.device import DeviceGraph
+
+    out = {}
+    g = G.rmat(16, 16, seed=1)
+    m = g.E // 2
+    with DeviceGraph.from_csr(g, with_weights=False) as dg:
+        dg.set_stream(stream)
+        tuned(dg)
+        ms, res = timed(lambda: dg.clustering_coeff(), steps, warmup, stream)
+        msp, _ = timed(lambda: dg.clustering_coeff(variant=_lib.SP_TC_PLAIN), 1, 1, stream)
+        cf = res[0]
+    lcc = {"workload": "clustering_coeff rmat16 ef16 undirected seed1", "value": m / (ms / 1e3) / 1e9,
+           "unit": "GTEPS", "ms": ms, "triangle_incidences": int(cf.astype(np.int64).sum()),
+           "plain": {"value": m / (msp / 1e3) / 1e9, "ms": msp}}
+    if cpu:
+        from oracle import oracle as O
+
+        nt = O.num_threads()
+        t = time.perf_counter()
+        ref = O.lcc(g.indexofNodes, g.edgeList, nthreads=nt)
+        dt = time.perf_counter() - t
+        lcc["same_as_oracle"] = bool(np.array_equal(ref, cf))
+        lcc["cpu_baseline"] = {"value": m / dt / 1e9, "unit": "GTEPS", "cores": nt, "kind": "port",
+                               "sample": f"OpenMP clustering_coeff loop, binary-search form, full graph ({dt:.2f} s)"}
+    out["clustering_coeff_rmat16"] = lcc
+
+    g = G.rmat(20, 16, seed=1)
+    g.edgeLen = G.hash_weights(g, 20, 1, 100, True)
+    srcs = np.sort(G.pick_sources(g, 256, seed=20)).astype(np.int32)
+    lab, ce = component_edges(g)
+    er = ce[lab[srcs]].astype(np.int64)
+    with DeviceGraph.from_csr(g) as dg:
+        dg.set_stream(stream)
+        tuned(dg)
+        msu, resu = timed(lambda: dg.closeness_unweighted(srcs), max(1, steps // 2), 1, stream)
+        w16 = srcs[:16]
+        msw, resw = timed(lambda: dg.closeness(w16), max(1, steps // 2), 1, stream)
+    cu = {"workload": "closeness unweighted rmat20 ef16 undirected seed1, 256 sources",
+          "value": int(er.sum()) / (msu / 1e3) / 1e9, "unit": "GTEPS", "ms": msu}
+    cw = {"workload": "closeness weighted rmat20 ef16 undirected seed1, w U[1,100], 16 sources",
+          "value": int(er[:16].sum()) / (msw / 1e3) / 1e9, "unit": "GTEPS", "ms": msw}
+    if cpu:
+        from oracle import oracle as O
+
+        t = time.perf_counter()
+        refw = O.closeness(g.indexofNodes, g.edgeList, g.edgeLen, w16[:4])
+        dt = time.perf_counter() - t
+        cw["same_as_oracle_on_sample"] = bool(np.array_equal(refw[w16[:4]], resw[0][w16[:4]]))
+        cw["cpu_baseline"] = {"value": int(er[:4].sum()) / dt / 1e9, "unit": "GTEPS", "cores": 1, "kind": "port",
+                              "sample": f"sequential Dijkstra from 4 of the 16 sources ({dt:.2f} s)"}
+        t = time.perf_counter()
+        refu = O.closeness_unweighted(g.indexofNodes, g.edgeList, srcs[:8])
+        dt = time.perf_counter() - t
+        cu["same_as_oracle_on_sample"] = bool(np.array_equal(refu[srcs[:8]], resu[0][srcs[:8]]))
+        cu["cpu_baseline"] = {"value": int(er[:8].sum()) / dt / 1e9, "unit": "GTEPS", "cores": 1, "kind": "port",
+                              "sample": f"sequential BFS from 8 of the 256 sources ({dt:.2f} s)"}
+    out["closeness_unweighted_rmat20"] = cu
+    out["closeness_rmat20"] = cw
+    return out
 
 
 def run_extras(want, args, stream, hbm, cpu_ok):
@@ -565,6 +636,8 @@ def run_extras(want, args, stream, hbm, cpu_ok):
         guarded("louvain_sbm1m", lambda: bench_louvain(max(1, ks // 2), 1, stream, hbm, cpu_ok))
     if "ingest_rmat20" in want:
         guarded("ingest_rmat20", lambda: bench_ingest(max(1, ks // 2), 1, cpu_ok))
+    if "centrality" in want:
+        guarded("centrality", lambda: bench_centrality(ks, kw, stream, hbm, cpu_ok))
     return extras
 
 

@@ -131,6 +131,32 @@ int sp_tune_get(sp_graph_h g, const char* key, int64_t* value);
 #define SP_TC_PLAIN 1
 int sp_tc(sp_graph_h g, int64_t* triangle_count, int32_t variant);
 
+/* ---- clustering coefficient ---------------------------------------------------
+ * Replaces generated `void staticClusteringCoeff(graph& g, int* cf)` (DSL
+ * staticDSLCodes/clustering_coeff:1-14): the Compute_TC loop, where every triangle
+ * (v, u, w) it finds adds one to cf of all three vertices. On a symmetric graph cf[v]
+ * is the number of triangles through v. cf[V] (int32, host or device) is overwritten.
+ * SP_TC_TUNED: the triangle-counting kernels with per-vertex counts; SP_TC_PLAIN: the
+ * generated CUDA form (one thread per vertex, binary search per pair). Exact. */
+int sp_clustering_coeff(sp_graph_h g, int32_t* cf, int32_t variant);
+
+/* ---- degree and closeness centrality -----------------------------------------
+ * Replaces generated `void Degree(graph& g, int* deg)` (DSL
+ * staticDSLCodes/degree_centrality:1-6): deg[v] = out-degree of v. */
+int sp_degree_centrality(sp_graph_h g, int32_t* deg);
+/* Replaces generated `void Compute_CC(graph& g, float* CC, std::set<int>& sourceSet)`
+ * (DSL staticDSLCodes/CC:1-26): CC[src] = 1.0 / (sum of the finite shortest-path
+ * distances from src over the edge weights) for every source, CC = 0 elsewhere.
+ * weight NULL = the graph's edgeLen. Distances by sp_sssp (learned schedule); the sum
+ * is exact in 64 bits, where the DSL's int would overflow past 2^31 - 1. Sources must
+ * be distinct; CC[V] host or device. */
+int sp_closeness(sp_graph_h g, const int32_t* weight, const int32_t* sources, int32_t nsrc, float* CC);
+/* Replaces generated `void Compute_CC_Unweighted(graph& g, float* CC, std::set<int>& sourceSet)`
+ * (DSL staticDSLCodes/closeness_centrality_unwt:1-20): CC[src] = 1.0 / (sum of the BFS
+ * levels of the vertices reached from src), CC = 0 elsewhere. Levels from the batched
+ * BFS of sp_bc, 64 sources per pass. */
+int sp_closeness_unweighted(sp_graph_h g, const int32_t* sources, int32_t nsrc, float* CC);
+
 /* ---- PageRank ----------------------------------------------------------------
  * Replaces generated `void ComputePageRank(graph& g, float beta, float delta, int maxIter,
  * float* pageRank)` (DSL staticDSLCodes/PageRankDSLV3:1-25): Jacobi pull over the

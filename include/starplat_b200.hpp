@@ -21,9 +21,15 @@
 //   void Compute_SSSP(graph& g, int* dist, int* weight, int src)      sssp_dslV3
 //   void Compute_BC(graph& g, float* BC, std::set<int>& sourceSet)    bc_dslV2
 //   auto Compute_CD(graph& g, int* weight)                            community_detection
+//   void staticClusteringCoeff(graph& g, int* cf)                     clustering_coeff
+//   void Degree(graph& g, int* deg)                                   degree_centrality
+//   void Compute_CC(graph& g, float* CC, std::set<int>& sourceSet)    CC
+//   void Compute_CC_Unweighted(graph& g, float* CC, std::set<int>& sourceSet)
+//                                                                     closeness_centrality_unwt
 #ifndef STARPLAT_B200_HPP
 #define STARPLAT_B200_HPP
 
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <map>
@@ -204,6 +210,40 @@ inline auto Compute_CD(GraphT& g, int* weight) {
   double q = 0;
   starplat_b200::check(sp_louvain(starplat_b200::mirror(g), wp, 1e-4, nullptr, &q, nullptr, nullptr, SP_LV_TUNED), "Compute_CD");
   return q;
+}
+
+template <class GraphT>
+inline void staticClusteringCoeff(GraphT& g, int* cf) {
+  starplat_b200::check(sp_clustering_coeff(starplat_b200::mirror(g), cf, SP_TC_TUNED), "staticClusteringCoeff");
+}
+
+template <class GraphT>
+inline void Degree(GraphT& g, int* deg) {
+  starplat_b200::check(sp_degree_centrality(starplat_b200::mirror(g), deg), "Degree");
+}
+
+// Closeness over the graph's edgeLen; an empty source set leaves CC all zero.
+template <class GraphT>
+inline void Compute_CC(GraphT& g, float* CC, std::set<int>& sourceSet) {
+  std::vector<int32_t> src(sourceSet.begin(), sourceSet.end());
+  if (src.empty()) {
+    std::fill(CC, CC + g.num_nodes(), 0.0f);
+    return;
+  }
+  starplat_b200::check(sp_closeness(starplat_b200::mirror(g), nullptr, src.data(), (int32_t)src.size(), CC),
+                       "Compute_CC");
+}
+
+template <class GraphT>
+inline void Compute_CC_Unweighted(GraphT& g, float* CC, std::set<int>& sourceSet) {
+  std::vector<int32_t> src(sourceSet.begin(), sourceSet.end());
+  if (src.empty()) {
+    std::fill(CC, CC + g.num_nodes(), 0.0f);
+    return;
+  }
+  starplat_b200::check(
+      sp_closeness_unweighted(starplat_b200::mirror(g), src.data(), (int32_t)src.size(), CC),
+      "Compute_CC_Unweighted");
 }
 
 #endif  // STARPLAT_B200_HPP

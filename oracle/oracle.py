@@ -33,6 +33,8 @@ def lib():
         L = ctypes.CDLL(path)
         L.or_tc.restype = ctypes.c_int64
         L.or_tc.argtypes = [ctypes.c_int32, i32p, i32p, ctypes.c_int]
+        L.or_lcc.restype = None
+        L.or_lcc.argtypes = [ctypes.c_int32, i32p, i32p, i32p, ctypes.c_int]
         L.or_tc_omp.restype = ctypes.c_int64
         L.or_tc_omp.argtypes = [ctypes.c_int32, i32p, i32p, ctypes.c_int, ctypes.c_int32, ctypes.c_int32]
         L.or_pagerank.restype = ctypes.c_int32
@@ -79,6 +81,8 @@ def ref_lib() -> Optional[ctypes.CDLL]:
         L.ref_graph_sizes.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]
         L.ref_graph_copy.restype = None
         L.ref_graph_copy.argtypes = [ctypes.c_void_p, i32p, i32p, i32p, i32p, i32p, i32p]
+        L.ref_lcc.restype = None
+        L.ref_lcc.argtypes = [ctypes.c_int32, i32p, i32p, i32p]
         L.ref_tc.restype = ctypes.c_int64
         L.ref_tc.argtypes = [ctypes.c_int32, i32p, i32p, ctypes.c_int, ctypes.c_int32, ctypes.c_int32]
         _REF = L
@@ -95,6 +99,48 @@ def tc(off, adj, nthreads: int = 0) -> int:
 
 def tc_omp(off, adj, nthreads: int = 0, vfirst: int = 0, vstride: int = 1) -> int:
     return int(lib().or_tc_omp(len(off) - 1, _c(off), _c(adj), nthreads, vfirst, vstride))
+
+
+def lcc(off, adj, nthreads: int = 0) -> np.ndarray:
+    """staticClusteringCoeff (staticDSLCodes/clustering_coeff:1-14): per-vertex counts
+    of the triangles the Compute_TC loop finds (int32)."""
+    V = len(off) - 1
+    cf = np.empty(V, np.int32)
+    lib().or_lcc(V, _c(off), _c(adj), cf, nthreads)
+    return cf
+
+
+def degree(off) -> np.ndarray:
+    """Degree (staticDSLCodes/degree_centrality:1-6): count_outNbrs(v), the out-degree."""
+    return np.diff(np.asarray(off, np.int64)).astype(np.int32)
+
+
+def closeness(off, adj, w, srcs) -> np.ndarray:
+    """Compute_CC (staticDSLCodes/CC:1-26): CC[src] = 1.0 / (sum of the finite
+    shortest-path distances from src) for every source, 0 elsewhere. The sum is kept
+    in 64 bits (the DSL's int overflows past 2^31-1); 1.0 / sum is a double division
+    stored as float, as the generated C++ does."""
+    V = len(off) - 1
+    cc = np.zeros(V, np.float32)
+    for s in np.asarray(srcs, np.int64):
+        d = sssp(off, adj, w, int(s)).astype(np.int64)
+        tot = int(d[d != np.iinfo(np.int32).max].sum())
+        cc[s] = np.float32(1.0 / tot) if tot != 0 else np.float32(np.inf)
+    return cc
+
+
+def closeness_unweighted(off, adj, srcs) -> np.ndarray:
+    """Compute_CC_Unweighted (staticDSLCodes/closeness_centrality_unwt:1-20): dist starts
+    at 0 everywhere and the BFS body sets w.dist = v.dist + 1 for each next-level w (the
+    generator's bfsDist guard, backend_omp/dsl_cpp_generator.cpp:1461-1468), so dist is
+    the BFS level of reached vertices and 0 elsewhere; CC[src] = 1.0 / sum of dist."""
+    V = len(off) - 1
+    cc = np.zeros(V, np.float32)
+    for s in np.asarray(srcs, np.int64):
+        lvl, _, _ = bfs_sigma(off, adj, int(s))
+        tot = int(lvl[lvl > 0].astype(np.int64).sum())
+        cc[s] = np.float32(1.0 / tot) if tot != 0 else np.float32(np.inf)
+    return cc
 
 
 def pagerank(off, roff, radj, beta=1e-6, delta=0.85, max_iter=100, fixed_iters=0, nthreads=0):
@@ -184,6 +230,18 @@ def num_threads() -> int:
 
 
 # ---- reference-compiled harness ------------------------------------------------
+
+def ref_lcc(off, adj) -> Optional[np.ndarray]:
+    """staticClusteringCoeff's generated loop over the reference's own check_if_nbr
+    (None when the reference harness was not built)."""
+    L = ref_lib()
+    if L is None:
+        return None
+    V = len(off) - 1
+    cf = np.empty(V, np.int32)
+    L.ref_lcc(V, _c(off), _c(adj), cf)
+    return cf
+
 
 def ref_tc(off, adj, nthreads: int = 0, vfirst: int = 0, vstride: int = 1) -> int:
     L = ref_lib()

@@ -7,7 +7,9 @@
 //     returning its CSR arrays — pins the CSR layout the kernels consume;
 //   * ref_tc: the generated OpenMP triangle count loop calling the reference's
 //     own graph::check_if_nbr / getNeighbors (graph.hpp:233-287, 982-1023) on a
-//     graph object whose CSR fields are filled from given arrays.
+//     graph object whose CSR fields are filled from given arrays;
+//   * ref_lcc: the same loop with the clustering_coeff DSL body (one added to the
+//     counts of all three vertices of each triangle found), sequential.
 //
 // Shim needed to compile graph.hpp without MKL: OMP_GNN.hpp is skipped
 // (it includes <mkl.h>), the five GNN entry points graph.hpp:1244-1300 calls
@@ -124,6 +126,41 @@ int64_t ref_tc(int32_t V, const int32_t* off, const int32_t* adj, int nthreads, 
   g.edgeList = nullptr;
   g.srcList = nullptr;
   return triangle_count;
+}
+
+// Generated loop of staticClusteringCoeff (staticDSLCodes/clustering_coeff:1-14)
+// with the reference's check_if_nbr; cf[V] is overwritten.
+void ref_lcc(int32_t V, const int32_t* off, const int32_t* adj, int32_t* cf) {
+  graph g((char*)"");
+  int32_t E = off[V];
+  g.nodesTotal = V - 1;
+  g.edgesTotal = E;
+  g.indexofNodes = const_cast<int32_t*>(off);
+  g.edgeList = const_cast<int32_t*>(adj);
+  std::vector<int32_t> wts(E, 1);
+  g.edgeLen = wts.data();
+  g.srcList = nullptr;
+  g.diff_edgeList = nullptr;
+  for (int32_t v = 0; v < V; v++) cf[v] = 0;
+  for (int32_t v = 0; v < V; v++) {
+    for (int32_t edge = g.indexofNodes[v]; edge < g.indexofNodes[v + 1]; edge++) {
+      int32_t u = g.edgeList[edge];
+      if (u < v) {
+        for (int32_t edge2 = g.indexofNodes[v]; edge2 < g.indexofNodes[v + 1]; edge2++) {
+          int32_t w = g.edgeList[edge2];
+          if (w > v && g.check_if_nbr(u, w)) {
+            cf[v] += 1;
+            cf[u] += 1;
+            cf[w] += 1;
+          }
+        }
+      }
+    }
+  }
+  // detach borrowed arrays so ~graph does not free them
+  g.edgeLen = nullptr;
+  g.edgeList = nullptr;
+  g.srcList = nullptr;
 }
 
 }  // extern "C"

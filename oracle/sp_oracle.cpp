@@ -122,6 +122,34 @@ int64_t or_tc_omp(int32_t V, const int32_t* off, const int32_t* adj, int nthread
   return triangle_count;
 }
 
+// ---------------------------------------------------------------- clustering coefficient
+// DSL staticDSLCodes/clustering_coeff:1-14 (staticClusteringCoeff): the triangle loop
+// of Compute_TC, where every (v, u, w) it finds adds one to cf of all three vertices
+// (cf starts at 0). On a symmetric graph cf[x] is the number of triangles through x.
+// Exact form: binary search in the sorted N(u) instead of check_if_nbr.
+void or_lcc(int32_t V, const int32_t* off, const int32_t* adj, int32_t* cf, int nthreads) {
+  set_threads(nthreads);
+  std::fill(cf, cf + V, 0);
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int32_t v = 0; v < V; ++v) {
+    const int32_t* b = adj + off[v];
+    const int32_t* e = adj + off[v + 1];
+    const int32_t* hi = std::upper_bound(b, e, v);  // first w > v
+    for (const int32_t* pu = b; pu < e && *pu < v; ++pu) {
+      const int32_t u = *pu;
+      const int32_t* ub = adj + off[u];
+      const int32_t* ue = adj + off[u + 1];
+      for (const int32_t* pw = hi; pw < e; ++pw) {
+        if (std::binary_search(ub, ue, *pw)) {
+          __atomic_fetch_add(&cf[v], 1, __ATOMIC_RELAXED);
+          __atomic_fetch_add(&cf[u], 1, __ATOMIC_RELAXED);
+          __atomic_fetch_add(&cf[*pw], 1, __ATOMIC_RELAXED);
+        }
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------- PageRank
 // DSL staticDSLCodes/PageRankDSLV3:1-25. nodes_to(v) iterates the reverse CSR
 // (rev_indexofNodes/srcList; the CUDA emitter backend_cuda/dsl_cpp_generator.cpp:1472-1480

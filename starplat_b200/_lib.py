@@ -74,6 +74,10 @@ SIGNATURES = {
     "sp_bc": (ctypes.c_int, [vp, vp, i32, vp, i32]),
     "sp_bc_graphs": (ctypes.c_int, [vp, i32, vp, vp, vp, vp]),
     "sp_bfs_sigma": (ctypes.c_int, [vp, vp, i32, vp, vp]),
+    "sp_clustering_coeff": (ctypes.c_int, [vp, vp, i32]),
+    "sp_degree_centrality": (ctypes.c_int, [vp, vp]),
+    "sp_closeness": (ctypes.c_int, [vp, vp, vp, i32, vp]),
+    "sp_closeness_unweighted": (ctypes.c_int, [vp, vp, i32, vp]),
     "sp_louvain": (ctypes.c_int, [vp, vp, f64, vp, P(f64), P(i32), P(i32), i32]),
     "sp_mlp_forward": (ctypes.c_int, [vp, vp, i32, vp]),
     "sp_mlp_grad": (ctypes.c_int, [vp, vp, vp, i32, vp, vp]),

@@ -56,6 +56,37 @@ def Compute_BC(g: CSRGraph, BC: np.ndarray, sourceSet) -> None:
     device_graph(g).bc(src, out=BC)
 
 
+def staticClusteringCoeff(g: CSRGraph, cf: np.ndarray) -> None:
+    """staticDSLCodes/clustering_coeff: fills int cf[num_nodes()] with the number of
+    triangles of the Compute_TC loop through each vertex."""
+    device_graph(g).clustering_coeff(out=cf)
+
+
+def Degree(g: CSRGraph, deg: np.ndarray) -> None:
+    """staticDSLCodes/degree_centrality: fills int deg[num_nodes()] with out-degrees."""
+    device_graph(g).degree(out=deg)
+
+
+def Compute_CC(g: CSRGraph, CC: np.ndarray, sourceSet) -> None:
+    """staticDSLCodes/CC: fills float CC[num_nodes()]: 1 / (sum of finite shortest-path
+    distances over the graph's edgeLen) at each source, 0 elsewhere."""
+    src = np.array(sorted(set(int(s) for s in sourceSet)), np.int32)
+    if src.shape[0] == 0:
+        CC[:] = 0
+        return
+    device_graph(g).closeness(src, out=CC)
+
+
+def Compute_CC_Unweighted(g: CSRGraph, CC: np.ndarray, sourceSet) -> None:
+    """staticDSLCodes/closeness_centrality_unwt: fills float CC[num_nodes()]: 1 / (sum
+    of BFS levels) at each source, 0 elsewhere."""
+    src = np.array(sorted(set(int(s) for s in sourceSet)), np.int32)
+    if src.shape[0] == 0:
+        CC[:] = 0
+        return
+    device_graph(g).closeness_unweighted(src, out=CC)
+
+
 def Compute_CD(g: CSRGraph, weight=None) -> float:
     """staticDSLCodes/community_detection: returns the modularity of the Louvain
     partition; weight is int[E] (or float[E]) in forward-CSR order, None = unit."""

@@ -1020,6 +1020,31 @@ extern "C" int sp_bc_graphs(sp_graph_h g, int32_t ngraphs, const int32_t* vertex
   return copy_out(BC, p->fout.p, sizeof(float) * g->V, s);
 }
 
+namespace sp {
+// Levels (-1 = unreached) and path counts of up to 64 distinct sources (device ids in
+// d_srcs) into device buffers lvl_out / sig_out of nsrc * V entries, source-major:
+// the forward pass of the batched BC kernel. A pass over more than 16 sources can fill
+// its level lists (a vertex is listed once per distinct level among the sources);
+// then the outputs are cleared and the sources run again 16 at a time, which always fits.
+int bc_levels(sp_graph* g, const int32_t* d_srcs, int nsrc, int32_t* lvl_out, double* sig_out) {
+  if (!g->bc) g->bc = new BcPlan();
+  cudaStream_t s = g->stream;
+  const size_t V = (size_t)g->V;
+  auto clear = [&]() -> int {
+    SP_CHECK_CUDA(cudaMemsetAsync(lvl_out, 0xff, sizeof(int32_t) * V * nsrc, s));
+    SP_CHECK_CUDA(cudaMemsetAsync(sig_out, 0, sizeof(double) * V * nsrc, s));
+    return SP_OK;
+  };
+  SP_TRY(clear());
+  int st = bc_grid(g, d_srcs, nsrc, 64, lvl_out, sig_out);
+  if (st != SP_ERR_UNSUPPORTED || nsrc <= 16) return st;
+  SP_TRY(clear());
+  for (int k = 0; k < nsrc; k += 16)
+    SP_TRY(bc_grid(g, d_srcs + k, std::min(16, nsrc - k), 16, lvl_out + V * k, sig_out + V * k));
+  return SP_OK;
+}
+}  // namespace sp
+
 extern "C" int sp_bfs_sigma(sp_graph_h g, const int32_t* sources, int32_t nsrc, int32_t* level, double* sigma) {
   if (!g || !sources || nsrc <= 0 || nsrc > 64 || !level || !sigma) {
     set_error("sp_bfs_sigma: invalid argument (1..64 sources)");
@@ -1042,11 +1067,9 @@ extern "C" int sp_bfs_sigma(sp_graph_h g, const int32_t* sources, int32_t nsrc, 
   dbuf<double> ds;
   SP_TRY(dl.alloc(n));
   SP_TRY(ds.alloc(n));
-  SP_CHECK_CUDA(cudaMemsetAsync(dl.p, 0xff, sizeof(int32_t) * n, s));  // -1 = unreached
-  SP_CHECK_CUDA(cudaMemsetAsync(ds.p, 0, sizeof(double) * n, s));
   SP_TRY(p->srcs.alloc(nsrc));
   SP_CHECK_CUDA(cudaMemcpyAsync(p->srcs.p, hs.data(), sizeof(int32_t) * nsrc, cudaMemcpyHostToDevice, s));
-  SP_TRY(bc_grid(g, p->srcs.p, nsrc, 64, dl.p, ds.p));
+  SP_TRY(bc_levels(g, p->srcs.p, nsrc, dl.p, ds.p));
   SP_TRY(copy_out(level, dl.p, sizeof(int32_t) * n, s));
   return copy_out(sigma, ds.p, sizeof(double) * n, s);
 }

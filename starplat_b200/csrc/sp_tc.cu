@@ -22,6 +22,14 @@
 // resident warps); larger graphs use a per-warp hash table, and anchors whose S does not fit it are counted afterwards
 // by whole CTAs with binary search in the sorted global list. Anchors are visited
 // heaviest first (estimated probe work) and dealt round-robin to the warps.
+//
+// Per-vertex counts (PV = true; DSL staticDSLCodes/clustering_coeff:1-14,
+// staticClusteringCoeff): every hit of the anchor loop is one triangle (a, p, x),
+// found once, and adds one to the counts of all three vertices: x per hit, p by the
+// hits of its probe list, a by the hits of all its probe lists. On a symmetric graph
+// that is the number of triangles through each vertex, as the DSL's u < v < w loop
+// gives; on any other graph the literal-formula path visits exactly the DSL's
+// (v, u, w) triples.
 #include <cub/cub.cuh>
 
 #include "sp_internal.cuh"
@@ -88,13 +96,15 @@ __device__ __forceinline__ void probe_range(const Lists& L, int a, int p, int& l
   le = e;
 }
 
+template <bool PV>
 __global__ void __launch_bounds__(THREADS) k_tc_warp(Lists L, const int32_t* __restrict__ order,
                                                      int* __restrict__ heavy, unsigned int* __restrict__ n_heavy,
-                                                     unsigned long long* __restrict__ total) {
+                                                     unsigned long long* __restrict__ total, int* __restrict__ cf) {
   __shared__ int s_tab[WARPS][HCAP];
   __shared__ short s_slot[WARPS][SMAX];
   __shared__ int s_lb[WARPS][32];
   __shared__ int s_excl[WARPS][32];
+  __shared__ int s_p[WARPS][PV ? 32 : 1];
   const int lane = lane_id(), w = warp_id();
   int* tab = s_tab[w];
   for (int i = lane; i < HCAP; i += 32) tab[i] = EMPTY;
@@ -124,6 +134,7 @@ __global__ void __launch_bounds__(THREADS) k_tc_warp(Lists L, const int32_t* __r
       s_slot[w][i] = (short)s;
     }
     __syncwarp();
+    unsigned ha = 0;  // PV: this lane's triangles at anchor a
     // probe lists of P(a), 32 probe vertices at a time
     for (int g0 = 0; g0 < np; g0 += 32) {
       int p = g0 + lane < np ? L.adj[pb + g0 + lane] : -1;
@@ -139,6 +150,7 @@ __global__ void __launch_bounds__(THREADS) k_tc_warp(Lists L, const int32_t* __r
       int tot = __shfl_sync(0xffffffffu, incl, 31);
       s_lb[w][lane] = lb;
       s_excl[w][lane] = incl - len;
+      if (PV) s_p[w][lane] = p;
       __syncwarp();
       for (int k = lane; k < tot; k += 32) {
         // owner: last lane whose exclusive prefix <= k
@@ -153,6 +165,11 @@ __global__ void __launch_bounds__(THREADS) k_tc_warp(Lists L, const int32_t* __r
           int t = tab[s];
           if (t == x) {
             ++cnt;
+            if (PV) {
+              atomicAdd(cf + x, 1);
+              atomicAdd(cf + s_p[w][lo], 1);
+              ++ha;
+            }
             break;
           }
           if (t == EMPTY) break;
@@ -160,6 +177,10 @@ __global__ void __launch_bounds__(THREADS) k_tc_warp(Lists L, const int32_t* __r
         }
       }
       __syncwarp();
+    }
+    if (PV) {
+      ha = warp_sum(ha);
+      if (lane == 0 && ha) atomicAdd(cf + a, (int)ha);
     }
     // clear the slots S(a) used
     for (int i = lane; i < ns; i += 32) tab[s_slot[w][i]] = EMPTY;
@@ -235,9 +256,10 @@ __global__ void __launch_bounds__(BM_THREADS) k_tc_bitmap(Lists L, const int32_t
 // one anchor at a time (LPT order, dealt round-robin to CTAs); warp w takes the
 // probes w, w + NW, ... of it, 32 probe ranges per lane load, and streams each
 // list across its lanes. The bitmap is set, probed and cleared between barriers.
-template <int NW, int MINB>
+template <int NW, int MINB, bool PV>
 __global__ void __launch_bounds__(NW * 32, MINB) k_tc_bitmap_cta(Lists L, const int32_t* __restrict__ order,
-                                                                 unsigned long long* __restrict__ total) {
+                                                                 unsigned long long* __restrict__ total,
+                                                                 int* __restrict__ cf) {
   __shared__ unsigned s_bm[BM_WORDS];
   constexpr int NT = NW * 32;
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -255,6 +277,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_tc_bitmap_cta(Lists L, const 
       atomicOr(&s_bm[k >> 5], 1u << (k & 31));
     }
     __syncthreads();
+    unsigned ha = 0;  // PV: this warp's triangles at anchor a (lane 0)
     for (int g0 = 0; w + NW * g0 < np; g0 += 32) {
       const int pi = w + NW * (g0 + lane);
       const int p = pi < np ? L.adj[pb + pi] : -1;
@@ -264,6 +287,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_tc_bitmap_cta(Lists L, const 
       for (int l = 0; l < nl; ++l) {
         const int b = __shfl_sync(0xffffffffu, lb, l);
         const int e = __shfl_sync(0xffffffffu, le, l);
+        unsigned hp = 0;  // PV: this lane's hits in the probe list of lane l's vertex
         for (int k0 = b + lane; k0 < e; k0 += 32 * BM_UNROLL) {
           int x[BM_UNROLL];
 #pragma unroll
@@ -273,10 +297,24 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_tc_bitmap_cta(Lists L, const 
           }
 #pragma unroll
           for (int u = 0; u < BM_UNROLL; ++u)
-            if (x[u] >= 0) cnt += (s_bm[x[u] >> 5] >> (x[u] & 31)) & 1u;
+            if (x[u] >= 0) {
+              const unsigned hit = (s_bm[x[u] >> 5] >> (x[u] & 31)) & 1u;
+              cnt += hit;
+              if (PV && hit) {
+                atomicAdd(cf + x[u], 1);
+                ++hp;
+              }
+            }
+        }
+        if (PV) {
+          const int pl = __shfl_sync(0xffffffffu, p, l);
+          hp = warp_sum(hp);
+          if (lane == 0 && hp) atomicAdd(cf + pl, (int)hp);
+          ha += hp;
         }
       }
     }
+    if (PV && lane == 0 && ha) atomicAdd(cf + a, (int)ha);
     __syncthreads();
     for (int i = tid; i < ns; i += NT) s_bm[L.adj[sb + i] >> 5] = 0u;
     __syncthreads();
@@ -286,11 +324,13 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_tc_bitmap_cta(Lists L, const 
 }
 
 // Heavy anchors: one CTA each, lookups by binary search in the sorted S(a).
+template <bool PV>
 __global__ void __launch_bounds__(THREADS) k_tc_heavy(Lists L, const int* __restrict__ heavy,
                                                       const unsigned int* __restrict__ n_heavy,
-                                                      unsigned long long* __restrict__ total) {
+                                                      unsigned long long* __restrict__ total, int* __restrict__ cf) {
   __shared__ int s_lb[THREADS];
   __shared__ int s_excl[THREADS];
+  __shared__ int s_p[PV ? THREADS : 1];
   __shared__ int s_tot;
   __shared__ unsigned long long s_red[WARPS];
   const int nh = (int)*n_heavy;
@@ -299,6 +339,7 @@ __global__ void __launch_bounds__(THREADS) k_tc_heavy(Lists L, const int* __rest
     const int a = heavy[h];
     int sb, se, pb, pe;
     anchor_ranges(L, a, sb, se, pb, pe);
+    unsigned long long ha = 0;  // PV: this thread's triangles at anchor a
     for (int g0 = pb; g0 < pe; g0 += THREADS) {
       int p = g0 + (int)threadIdx.x < pe ? L.adj[g0 + threadIdx.x] : -1;
       int lb = 0, le = 0;
@@ -311,6 +352,7 @@ __global__ void __launch_bounds__(THREADS) k_tc_heavy(Lists L, const int* __rest
       Scan(ts).ExclusiveSum(len, excl, tot);
       s_lb[threadIdx.x] = lb;
       s_excl[threadIdx.x] = excl;
+      if (PV) s_p[threadIdx.x] = p;
       if (threadIdx.x == 0) s_tot = tot;
       __syncthreads();
       for (int k = threadIdx.x; k < s_tot; k += THREADS) {
@@ -325,9 +367,20 @@ __global__ void __launch_bounds__(THREADS) k_tc_heavy(Lists L, const int* __rest
           int m = (l + r) >> 1;
           if (L.adj[m] < x) l = m + 1; else r = m;
         }
-        if (l < se && L.adj[l] == x) ++cnt;
+        if (l < se && L.adj[l] == x) {
+          ++cnt;
+          if (PV) {
+            atomicAdd(cf + x, 1);
+            atomicAdd(cf + s_p[lo], 1);
+            ++ha;
+          }
+        }
       }
       __syncthreads();
+    }
+    if (PV) {
+      ha = block_sum<THREADS>(ha, s_red);
+      if (threadIdx.x == 0 && ha) atomicAdd(cf + a, (int)ha);
     }
   }
   cnt = block_sum<THREADS>(cnt, s_red);
@@ -361,6 +414,35 @@ __global__ void k_tc_plain(const int32_t* __restrict__ off, const int32_t* __res
     }
   }
   if (c) atomicAdd(total, c);
+}
+
+// Plain per-vertex form: the generated CUDA shape of staticClusteringCoeff (one
+// thread per vertex v, the double loop over N(v), u->w by binary search in N(u)),
+// each triangle adding one to cf of v, u and w.
+__global__ void k_lcc_plain(const int32_t* __restrict__ off, const int32_t* __restrict__ adj, int V,
+                            int* __restrict__ cf) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= V) return;
+  for (int e = off[v]; e < off[v + 1]; ++e) {
+    int u = adj[e];
+    if (u >= v) continue;
+    for (int e2 = off[v]; e2 < off[v + 1]; ++e2) {
+      int w = adj[e2];
+      if (w <= v) continue;
+      int lo = off[u], hi = off[u + 1] - 1;
+      while (lo <= hi) {
+        int mid = (lo + hi) >> 1;
+        int x = adj[mid];
+        if (x == w) {
+          atomicAdd(cf + v, 1);
+          atomicAdd(cf + u, 1);
+          atomicAdd(cf + w, 1);
+          break;
+        }
+        if (x < w) lo = mid + 1; else hi = mid - 1;
+      }
+    }
+  }
 }
 
 // Estimated work of anchor a: the probe-list lengths it streams (sum over P(a)),
@@ -550,14 +632,14 @@ extern "C" int sp_tc(sp_graph_h g, int64_t* triangle_count, int32_t variant) {
   SP_CHECK_CUDA(cudaMemsetAsync(p->total.p, 0, sizeof(unsigned long long), s));
   const int cta_warps = g->tc_cta_warps >= 0 ? g->tc_cta_warps : tc::CTA_WARPS_DEFAULT;
   if (g->V <= 65536 && cta_warps > 0) {
-    void (*k)(tc::Lists, const int32_t*, unsigned long long*) =
-        cta_warps == 2   ? tc::k_tc_bitmap_cta<2, 24>
-        : cta_warps == 4 ? tc::k_tc_bitmap_cta<4, 16>
-        : cta_warps == 8 ? tc::k_tc_bitmap_cta<8, 8>
-                         : tc::k_tc_bitmap_cta<16, 4>;
+    void (*k)(tc::Lists, const int32_t*, unsigned long long*, int*) =
+        cta_warps == 2   ? tc::k_tc_bitmap_cta<2, 24, false>
+        : cta_warps == 4 ? tc::k_tc_bitmap_cta<4, 16, false>
+        : cta_warps == 8 ? tc::k_tc_bitmap_cta<8, 8, false>
+                         : tc::k_tc_bitmap_cta<16, 4, false>;
     int per_sm = 0;
     SP_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, cta_warps * 32, 0));
-    k<<<num_sms() * std::max(1, per_sm), cta_warps * 32, 0, s>>>(L, p->order.p, p->total.p);
+    k<<<num_sms() * std::max(1, per_sm), cta_warps * 32, 0, s>>>(L, p->order.p, p->total.p, nullptr);
     SP_CHECK_LAUNCH();
   } else if (g->V <= 65536) {
     int per_sm = 0;
@@ -565,13 +647,62 @@ extern "C" int sp_tc(sp_graph_h g, int64_t* triangle_count, int32_t variant) {
     tc::k_tc_bitmap<<<num_sms() * std::max(1, per_sm), tc::BM_THREADS, 0, s>>>(L, p->order.p, p->total.p);
     SP_CHECK_LAUNCH();
   } else {
-    tc::k_tc_warp<<<num_sms() * 4, tc::THREADS, 0, s>>>(L, p->order.p, p->heavy.p, p->ctr.p + 1, p->total.p);
+    tc::k_tc_warp<false>
+        <<<num_sms() * 4, tc::THREADS, 0, s>>>(L, p->order.p, p->heavy.p, p->ctr.p + 1, p->total.p, nullptr);
     SP_CHECK_LAUNCH();
-    tc::k_tc_heavy<<<num_sms() * 2, tc::THREADS, 0, s>>>(L, p->heavy.p, p->ctr.p + 1, p->total.p);
+    tc::k_tc_heavy<false><<<num_sms() * 2, tc::THREADS, 0, s>>>(L, p->heavy.p, p->ctr.p + 1, p->total.p, nullptr);
     SP_CHECK_LAUNCH();
   }
   unsigned long long h = 0;
   SP_TRY(copy_out(&h, p->total.p, sizeof(h), s));
   *triangle_count = (int64_t)h;
   return SP_OK;
+}
+
+extern "C" int sp_clustering_coeff(sp_graph_h g, int32_t* cf, int32_t variant) {
+  using namespace sp;
+  if (!g || !cf) {
+    set_error("sp_clustering_coeff: NULL argument");
+    return SP_ERR_INVALID;
+  }
+  if (variant != SP_TC_TUNED && variant != SP_TC_PLAIN) {
+    set_error("sp_clustering_coeff: unknown variant %d", variant);
+    return SP_ERR_INVALID;
+  }
+  cudaStream_t s = g->stream;
+  dbuf<int> counts;
+  SP_TRY(counts.alloc(g->V));
+  if (g->V) SP_CHECK_CUDA(cudaMemsetAsync(counts.p, 0, sizeof(int) * g->V, s));
+  if (variant == SP_TC_PLAIN) {
+    const int tb = 512;  // backend_cuda/dsl_cpp_generator.cpp:56-77
+    if (g->V) {
+      tc::k_lcc_plain<<<(g->V + tb - 1) / tb, tb, 0, s>>>(g->off.p, g->adj.p, g->V, counts.p);
+      SP_CHECK_LAUNCH();
+    }
+    return copy_out(cf, counts.p, sizeof(int32_t) * g->V, s);
+  }
+  SP_TRY(build_tc_plan(g));
+  TcPlan* p = g->tc;
+  tc::Lists L;
+  L.V = g->V;
+  L.directed = p->oriented ? 0 : 1;
+  L.off = p->oriented ? p->ooff.p : g->off.p;
+  L.adj = p->oriented ? p->oadj.p : g->adj.p;
+  SP_CHECK_CUDA(cudaMemsetAsync(p->ctr.p, 0, sizeof(unsigned int) * 2, s));
+  SP_CHECK_CUDA(cudaMemsetAsync(p->total.p, 0, sizeof(unsigned long long), s));
+  if (g->V <= 65536) {
+    int per_sm = 0;
+    SP_CHECK_CUDA(
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tc::k_tc_bitmap_cta<4, 16, true>, 4 * 32, 0));
+    tc::k_tc_bitmap_cta<4, 16, true>
+        <<<num_sms() * std::max(1, per_sm), 4 * 32, 0, s>>>(L, p->order.p, p->total.p, counts.p);
+    SP_CHECK_LAUNCH();
+  } else {
+    tc::k_tc_warp<true>
+        <<<num_sms() * 4, tc::THREADS, 0, s>>>(L, p->order.p, p->heavy.p, p->ctr.p + 1, p->total.p, counts.p);
+    SP_CHECK_LAUNCH();
+    tc::k_tc_heavy<true><<<num_sms() * 2, tc::THREADS, 0, s>>>(L, p->heavy.p, p->ctr.p + 1, p->total.p, counts.p);
+    SP_CHECK_LAUNCH();
+  }
+  return copy_out(cf, counts.p, sizeof(int32_t) * g->V, s);
 }

@@ -212,6 +212,46 @@ class DeviceGraph:
         check("sp_bfs_sigma", lib().sp_bfs_sigma(self.handle, _ptr(sources), k, _ptr(lvl), _ptr(sig)))
         return lvl, sig
 
+    def clustering_coeff(self, out=None, variant: int = _lib.SP_TC_TUNED):
+        """Per-vertex triangle counts of the Compute_TC loop (staticClusteringCoeff): int32[V]."""
+        if out is None:
+            out = np.empty(self.V, np.int32)
+        check("sp_clustering_coeff", lib().sp_clustering_coeff(self.handle, _ptr(out), variant))
+        return out
+
+    def degree(self, out=None):
+        """Out-degree of every vertex (Degree): int32[V]."""
+        if out is None:
+            out = np.empty(self.V, np.int32)
+        check("sp_degree_centrality", lib().sp_degree_centrality(self.handle, _ptr(out)))
+        return out
+
+    def closeness(self, sources, weight=None, out=None):
+        """Compute_CC: CC[src] = 1 / (sum of finite weighted distances from src), 0
+        elsewhere; float32[V]. weight: int32[E] or None for the graph's edgeLen."""
+        _ensure_scheduler()
+        if out is None:
+            out = np.empty(self.V, np.float32)
+        if weight is not None and str(weight.dtype) not in ("int32", "torch.int32"):
+            raise TypeError("weights must be int32")
+        if isinstance(sources, (list, tuple)):
+            sources = np.asarray(sources, np.int32)
+        n = int(sources.shape[0])
+        check("sp_closeness", lib().sp_closeness(self.handle, _ptr(weight), _ptr(sources) if n else None, n,
+                                                 _ptr(out)))
+        return out
+
+    def closeness_unweighted(self, sources, out=None):
+        """Compute_CC_Unweighted: CC[src] = 1 / (sum of BFS levels from src), 0 elsewhere."""
+        if out is None:
+            out = np.empty(self.V, np.float32)
+        if isinstance(sources, (list, tuple)):
+            sources = np.asarray(sources, np.int32)
+        n = int(sources.shape[0])
+        check("sp_closeness_unweighted", lib().sp_closeness_unweighted(self.handle, _ptr(sources) if n else None,
+                                                                       n, _ptr(out)))
+        return out
+
     def louvain(self, weight=None, threshold: float = 1e-4, community=None, variant: int = _lib.SP_LV_TUNED):
         """Louvain; returns (modularity, community[V] int32, levels)."""
         if community is None:

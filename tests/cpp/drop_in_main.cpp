@@ -43,6 +43,24 @@ int main(int argc, char** argv) {
   for (int v = 0; v < V; ++v) std::printf(" %.9g", bc[v]);
   std::printf("\n");
   std::printf("CD %.12f\n", Compute_CD(g, nullptr));
+  std::vector<int> cf(V), deg(V);
+  staticClusteringCoeff(g, cf.data());
+  std::printf("LCC");
+  for (int v = 0; v < V; ++v) std::printf(" %d", cf[v]);
+  std::printf("\n");
+  Degree(g, deg.data());
+  std::printf("DEG");
+  for (int v = 0; v < V; ++v) std::printf(" %d", deg[v]);
+  std::printf("\n");
+  std::vector<float> cc(V), ccu(V);
+  Compute_CC(g, cc.data(), sources);
+  std::printf("CC");
+  for (int v = 0; v < V; ++v) std::printf(" %.9g", cc[v]);
+  std::printf("\n");
+  Compute_CC_Unweighted(g, ccu.data(), sources);
+  std::printf("CCU");
+  for (int v = 0; v < V; ++v) std::printf(" %.9g", ccu[v]);
+  std::printf("\n");
   starplat_b200::invalidate(g);
   return 0;
 }

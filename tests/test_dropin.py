@@ -62,6 +62,12 @@ def check_outputs(res, g, src):
     # order (the strict 1e-3 bar is tested on planted partitions in test_gpu_louvain)
     q, _, _ = O.louvain(g.indexofNodes, g.edgeList)
     assert float(res["CD"][0]) > q - 2e-2
+    assert np.array_equal(np.array(res["LCC"], np.int64), O.lcc(g.indexofNodes, g.edgeList))
+    assert np.array_equal(np.array(res["DEG"], np.int64), O.degree(g.indexofNodes))
+    cc = np.array(res["CC"], np.float32)
+    assert np.array_equal(cc, O.closeness(g.indexofNodes, g.edgeList, g.edgeLen, srcs))
+    ccu = np.array(res["CCU"], np.float32)
+    assert np.array_equal(ccu, O.closeness_unweighted(g.indexofNodes, g.edgeList, srcs))
 
 
 def small_graph():

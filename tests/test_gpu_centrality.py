@@ -1,0 +1,101 @@
+"""GPU parity for the algorithms built on the same kernels: per-vertex triangle counts
+(staticClusteringCoeff), out-degrees (Degree) and closeness (Compute_CC weighted,
+Compute_CC_Unweighted). Integer outputs are bit-exact against the oracle; closeness is
+1.0 / an exact integer sum, so it is bit-exact too."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from starplat_b200 import _lib
+from starplat_b200 import generators as G
+from starplat_b200.algorithms import (Compute_CC, Compute_CC_Unweighted, Degree, device_graph,
+                                      staticClusteringCoeff)
+
+from graphs import directed_zoo, from_pairs, star, undirected_zoo
+
+pytestmark = pytest.mark.gpu
+
+
+def _lcc_graphs():
+    # V <= 65536 (shared-memory bitmap) and above (hash tables, heavy anchors), directed
+    # (literal formula) and undirected (oriented), hubs
+    return (directed_zoo()[:3] + undirected_zoo()[:5] +
+            [G.rmat(17, 16, seed=4), G.rmat(14, 16, seed=6, directed=True), star(3000, directed_in=False)])
+
+
+@pytest.mark.parametrize("variant", [_lib.SP_TC_TUNED, _lib.SP_TC_PLAIN])
+def test_clustering_coeff_matches_oracle(variant):
+    for g in _lcc_graphs():
+        out = device_graph(g).clustering_coeff(variant=variant)
+        ref = O.lcc(g.indexofNodes, g.edgeList)
+        assert np.array_equal(out, ref), (g.name, int((out != ref).sum()))
+        if variant == _lib.SP_TC_TUNED and g.is_symmetric():
+            assert int(out.astype(np.int64).sum()) == 3 * device_graph(g).tc()
+
+
+def test_clustering_coeff_entry_point_twice_and_device_output():
+    import torch
+
+    g = G.rmat(12, 16, seed=2)
+    cf = np.full(g.V, -7, np.int32)  # overwritten, not accumulated
+    staticClusteringCoeff(g, cf)
+    staticClusteringCoeff(g, cf)
+    assert np.array_equal(cf, O.lcc(g.indexofNodes, g.edgeList))
+    out = torch.empty(g.V, dtype=torch.int32, device="cuda")
+    device_graph(g).clustering_coeff(out=out)
+    assert np.array_equal(out.cpu().numpy(), cf)
+
+
+def test_degree():
+    for g in directed_zoo()[:2] + undirected_zoo()[:2] + [from_pairs(5, [[0, 1], [0, 2], [3, 1]], name="tiny")]:
+        deg = np.empty(g.V, np.int32)
+        Degree(g, deg)
+        assert np.array_equal(deg, O.degree(g.indexofNodes))
+
+
+def _weighted(g, lo, hi, seed=3):
+    g.edgeLen = G.hash_weights(g, seed, lo, hi, g.is_symmetric())
+    return g
+
+
+def test_closeness_weighted_matches_oracle():
+    cases = [_weighted(directed_zoo()[0], 1, 100), _weighted(undirected_zoo()[1], 1, 1000),
+             _weighted(G.grid(30, 40), 1, 1000), _weighted(G.rmat(13, 8, seed=2, directed=True), 1, 100)]
+    for g in cases:
+        srcs = G.pick_sources(g, 9, seed=5)
+        cc = np.empty(g.V, np.float32)
+        Compute_CC(g, cc, set(int(s) for s in srcs))
+        ref = O.closeness(g.indexofNodes, g.edgeList, g.edgeLen, np.sort(srcs))
+        assert np.array_equal(cc, ref), g.name
+        assert np.count_nonzero(cc) <= len(srcs)
+
+
+def test_closeness_unweighted_matches_oracle():
+    # more than one 64-source pass, and directed / undirected graphs
+    for g in [directed_zoo()[1], undirected_zoo()[0], G.grid(20, 25), G.rmat(12, 16, seed=8)]:
+        srcs = G.pick_sources(g, min(g.V, 150), seed=7)
+        cc = np.empty(g.V, np.float32)
+        Compute_CC_Unweighted(g, cc, set(int(s) for s in srcs))
+        ref = O.closeness_unweighted(g.indexofNodes, g.edgeList, np.sort(srcs))
+        assert np.array_equal(cc, ref), g.name
+
+
+def test_closeness_edge_cases():
+    # an isolated source (sum 0 -> +inf, as 1.0 / 0 gives in the generated C++), a
+    # source set with every vertex, an empty source set, and bad sources
+    g = from_pairs(5, [[0, 1], [1, 2], [2, 0]], name="tri_iso")
+    g.edgeLen = np.array([2, 3, 4], np.int32)
+    cc = np.empty(g.V, np.float32)
+    Compute_CC(g, cc, {4})
+    assert np.isinf(cc[4]) and cc[4] > 0 and np.count_nonzero(cc[:4]) == 0
+    Compute_CC(g, cc, set(range(g.V)))
+    assert np.array_equal(cc, O.closeness(g.indexofNodes, g.edgeList, g.edgeLen, np.arange(g.V)))
+    Compute_CC_Unweighted(g, cc, set(range(g.V)))
+    assert np.array_equal(cc, O.closeness_unweighted(g.indexofNodes, g.edgeList, np.arange(g.V)))
+    Compute_CC(g, cc, set())
+    assert not cc.any()
+    dg = device_graph(g)
+    with pytest.raises(_lib.SPError):
+        dg.closeness(np.array([1, 1], np.int32))
+    with pytest.raises(_lib.SPError):
+        dg.closeness_unweighted(np.array([5], np.int32))

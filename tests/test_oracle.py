@@ -67,6 +67,37 @@ def test_tc_reference_harness():
         assert O.ref_tc(g.indexofNodes, g.edgeList) == O.tc(g.indexofNodes, g.edgeList)
 
 
+def test_lcc_reference_harness_and_identities():
+    # per-vertex counts of the clustering_coeff loop: the reference's own check_if_nbr
+    # loop agrees (when it was built here), every triple found adds three, and each
+    # vertex of a clique K_n lies in C(n-1, 2) triangles
+    for g in [G.rmat(10, 8, seed=11), clique(12), G.rmat(9, 8, seed=2, directed=True)]:
+        cf = O.lcc(g.indexofNodes, g.edgeList)
+        assert int(cf.astype(np.int64).sum()) == 3 * O.tc(g.indexofNodes, g.edgeList)
+        if O.ref_lib() is not None:
+            assert np.array_equal(O.ref_lcc(g.indexofNodes, g.edgeList), cf)
+    assert np.all(O.lcc(clique(12).indexofNodes, clique(12).edgeList) == 55)
+
+
+def test_closeness_known_answers():
+    # path 0-1-2-3 (both directions), weights 1, 2, 3: weighted sums from 0 and 3 are
+    # 1+3+6 = 10 and 3+5+6 = 14; BFS level sums 1+2+3 = 6 from either end; vertex 4 is
+    # isolated (sum 0 -> +inf); non-sources stay 0
+    from graphs import from_pairs
+
+    g = from_pairs(5, [[0, 1], [1, 2], [2, 3]], symmetrize=True, name="path")
+    w = np.zeros(g.E, np.int32)
+    for u in range(g.V):
+        for e in range(g.indexofNodes[u], g.indexofNodes[u + 1]):
+            w[e] = min(u, g.edgeList[e]) + 1
+    cc = O.closeness(g.indexofNodes, g.edgeList, w, [0, 3, 4])
+    assert cc[0] == np.float32(1.0 / 10) and cc[3] == np.float32(1.0 / 14) and np.isinf(cc[4])
+    assert cc[1] == 0 and cc[2] == 0
+    cu = O.closeness_unweighted(g.indexofNodes, g.edgeList, [0, 3])
+    assert cu[0] == np.float32(1.0 / 6) and cu[3] == np.float32(1.0 / 6) and cu[1] == 0
+    assert np.array_equal(O.degree(g.indexofNodes), [1, 2, 2, 1, 0])
+
+
 def dense_pagerank(g, beta, delta, max_iter):
     V = g.V
     A = np.zeros((V, V))
