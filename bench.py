@@ -568,16 +568,29 @@ def bench_centrality(steps, warmup, stream, hbm, cpu):
     srcs = np.sort(G.pick_sources(g, 256, seed=20)).astype(np.int32)
     lab, ce = component_edges(g)
     er = ce[lab[srcs]].astype(np.int64)
+    w16 = srcs[:16]
+    sharded = REP is not None and REP.world > 1
     with DeviceGraph.from_csr(g) as dg:
         dg.set_stream(stream)
         tuned(dg)
-        msu, resu = timed(lambda: dg.closeness_unweighted(srcs), max(1, steps // 2), 1, stream)
-        w16 = srcs[:16]
-        msw, resw = timed(lambda: dg.closeness(w16), max(1, steps // 2), 1, stream)
+        if sharded:
+            # the sources split over the GPUs, one all-reduce of CC[V] (strong scaling)
+            from starplat_b200.distributed import closeness_on_gpus
+
+            REP.barrier()
+            msu, resu = timed(lambda: closeness_on_gpus(dg, srcs, REP, weighted=False), max(1, steps // 2), 1,
+                              stream)
+            msw, resw = timed(lambda: closeness_on_gpus(dg, w16, REP), max(1, steps // 2), 1, stream)
+            msu, msw = REP.max(msu), REP.max(msw)
+        else:
+            msu, resu = timed(lambda: dg.closeness_unweighted(srcs), max(1, steps // 2), 1, stream)
+            msw, resw = timed(lambda: dg.closeness(w16), max(1, steps // 2), 1, stream)
     cu = {"workload": "closeness unweighted rmat20 ef16 undirected seed1, 256 sources",
           "value": int(er.sum()) / (msu / 1e3) / 1e9, "unit": "GTEPS", "ms": msu}
     cw = {"workload": "closeness weighted rmat20 ef16 undirected seed1, w U[1,100], 16 sources",
           "value": int(er[:16].sum()) / (msw / 1e3) / 1e9, "unit": "GTEPS", "ms": msw}
+    if sharded:
+        cu["parallelism"] = cw["parallelism"] = f"sources split over {REP.world} GPUs, one all-reduce of CC[V]"
     if cpu:
         from oracle import oracle as O
 

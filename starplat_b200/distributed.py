@@ -1,9 +1,13 @@
-"""Brandes BC over the GPUs of one node: the sources are split among the ranks, each
-rank runs its slice on its own GPU (sp_bc, all batches in one launch), and one
-all-reduce adds the per-vertex dependency sums. BC is a sum over sources
-(bc_dslV2: BC[v] += delta_s[v] for every source s), so the split is exact up to FP32
-rounding of the partial sums. The process group comes from replicas.Replicas (NCCL on
-GPUs, gloo on the host).
+"""Multi-source algorithms over the GPUs of one node: the sources are split among the
+ranks, each rank runs its slice on its own GPU, and one all-reduce adds the per-vertex
+vectors.
+  * Brandes BC (sp_bc, all batches in one launch): BC is a sum over sources
+    (bc_dslV2: BC[v] += delta_s[v] for every source s), so the split is exact up to
+    FP32 rounding of the partial sums.
+  * Closeness (sp_closeness / sp_closeness_unweighted): CC is nonzero only at the
+    sources and each source's entry comes from one rank, so the sum of the slices is
+    the whole, bit for bit.
+The process group comes from replicas.Replicas (NCCL on GPUs, gloo on the host).
 """
 from __future__ import annotations
 
@@ -23,13 +27,27 @@ def split_sources(sources, world: int, rank: int) -> np.ndarray:
     return s[lo:hi]
 
 
-def bc_sharded(V: int, sources, rep: Replicas, compute: Callable[[np.ndarray], np.ndarray]) -> np.ndarray:
-    """BC[V] over all `sources`: this rank computes its slice with `compute` (slice ->
-    float32[V]; DeviceGraph.bc on a GPU), then the partial vectors are summed over the
-    ranks. Every rank returns the full result."""
+def sum_over_sources(V: int, sources, rep: Replicas, compute: Callable[[np.ndarray], np.ndarray]) -> np.ndarray:
+    """A float32[V] that is a sum over `sources`: this rank computes its slice with
+    `compute` (slice -> float32[V]), then the partial vectors are summed over the ranks.
+    Every rank returns the full result."""
     mine = split_sources(sources, rep.world, rep.rank)
     part = compute(mine) if mine.shape[0] else np.zeros(V, np.float32)
     return rep.all_reduce_sum(np.ascontiguousarray(part, np.float32))
+
+
+def bc_sharded(V: int, sources, rep: Replicas, compute: Callable[[np.ndarray], np.ndarray]) -> np.ndarray:
+    """BC[V] over all `sources` (compute: DeviceGraph.bc on a GPU)."""
+    return sum_over_sources(V, sources, rep, compute)
+
+
+def closeness_on_gpus(dg, sources, rep: Optional[Replicas] = None, weighted: bool = True, weight=None) -> np.ndarray:
+    """Compute_CC (weighted, the graph's edgeLen or `weight`) or Compute_CC_Unweighted
+    over `sources`, split over the ranks; every rank returns CC[V]."""
+    rep = rep or Replicas()
+    if weighted:
+        return sum_over_sources(dg.V, sources, rep, lambda s: dg.closeness(s, weight=weight))
+    return sum_over_sources(dg.V, sources, rep, lambda s: dg.closeness_unweighted(s))
 
 
 def bc_on_gpus(dg, sources, rep: Optional[Replicas] = None) -> np.ndarray:

@@ -113,3 +113,45 @@ def test_bc_split_over_ranks_sums_to_the_whole(tmp_path, world):
     for r in range(world):
         out = np.load(tmp_path / f"bc{r}.npy").astype(np.float64)
         assert np.all(np.abs(out - ref) <= 1e-5 * np.abs(ref) + 1e-6)
+
+
+def _cc_rank_main(rank, world, port, out_dir):
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port), "RANK": str(rank),
+                       "WORLD_SIZE": str(world), "LOCAL_RANK": str(rank)})
+    sys.path.insert(0, ROOT)
+    import numpy as np
+
+    from oracle import oracle as O
+    from starplat_b200 import generators as G
+    from starplat_b200.distributed import sum_over_sources
+    from starplat_b200.replicas import Replicas
+
+    g = G.rmat(9, 8, seed=6)
+    g.edgeLen = G.hash_weights(g, 6, 1, 50, True)
+    srcs = np.sort(G.pick_sources(g, 23, seed=2)).astype(np.int32)
+    rep = Replicas(backend="gloo", timeout_s=60)
+    w = sum_over_sources(g.V, srcs, rep, lambda s: O.closeness(g.indexofNodes, g.edgeList, g.edgeLen, s))
+    u = sum_over_sources(g.V, srcs, rep, lambda s: O.closeness_unweighted(g.indexofNodes, g.edgeList, s))
+    rep.close()
+    np.save(os.path.join(out_dir, f"ccw{rank}.npy"), w)
+    np.save(os.path.join(out_dir, f"ccu{rank}.npy"), u)
+
+
+def test_closeness_split_over_ranks_is_exact(tmp_path):
+    # each source's entry comes from one rank: the reduced vector equals the whole bit for bit
+    import numpy as np
+
+    from oracle import oracle as O
+    from starplat_b200 import generators as G
+
+    world = 3
+    mp.start_processes(_cc_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    g = G.rmat(9, 8, seed=6)
+    g.edgeLen = G.hash_weights(g, 6, 1, 50, True)
+    srcs = np.sort(G.pick_sources(g, 23, seed=2)).astype(np.int32)
+    rw = O.closeness(g.indexofNodes, g.edgeList, g.edgeLen, srcs)
+    ru = O.closeness_unweighted(g.indexofNodes, g.edgeList, srcs)
+    for r in range(world):
+        assert np.array_equal(np.load(tmp_path / f"ccw{r}.npy"), rw)
+        assert np.array_equal(np.load(tmp_path / f"ccu{r}.npy"), ru)
