@@ -199,6 +199,11 @@ constexpr int BM_THREADS = 32 * BM_WARPS;
 constexpr int BM_WORDS = 65536 / 32;
 constexpr int BM_UNROLL = 4;
 constexpr int CTA_WARPS_DEFAULT = 4;  // k_tc_bitmap_cta warps per CTA: 0.173 ms on R-MAT 16 vs 0.209 per-warp
+// Per-vertex counts in k_tc_bitmap_cta: anchors with at most CNT_SLOTS elements in S(a)
+// count hits per element in shared memory (16-bit halves of 32-bit words; a count is at
+// most |P(a)| < 65536 since P(a) holds distinct vertex ids below 65536) and add them to
+// cf once per (anchor, element) afterwards.
+constexpr int CNT_SLOTS = 4096;
 
 __global__ void __launch_bounds__(BM_THREADS) k_tc_bitmap(Lists L, const int32_t* __restrict__ order,
                                                           unsigned long long* __restrict__ total) {
@@ -261,9 +266,15 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_tc_bitmap_cta(Lists L, const 
                                                                  unsigned long long* __restrict__ total,
                                                                  int* __restrict__ cf) {
   __shared__ unsigned s_bm[BM_WORDS];
+  __shared__ unsigned short s_pre[PV ? BM_WORDS : 1];    // PV: set bits in the words before each word
+  __shared__ unsigned s_cnt[PV ? CNT_SLOTS / 2 : 1];      // PV: hits per element of S(a), two per word
+  __shared__ unsigned s_wsum[PV ? NW : 1];
   constexpr int NT = NW * 32;
+  constexpr int WPT = BM_WORDS / NT;  // bitmap words per thread in the prefix count
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   for (int i = tid; i < BM_WORDS; i += NT) s_bm[i] = 0u;
+  if (PV)
+    for (int i = tid; i < CNT_SLOTS / 2; i += NT) s_cnt[i] = 0u;
   __syncthreads();
   unsigned long long cnt = 0;
   for (int ai = blockIdx.x; ai < L.V; ai += gridDim.x) {
@@ -277,6 +288,30 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_tc_bitmap_cta(Lists L, const 
       atomicOr(&s_bm[k >> 5], 1u << (k & 31));
     }
     __syncthreads();
+    // PV: element x of S(a) is slot s_pre[x / 32] + (set bits of its word below x) of
+    // the sorted S(a); its hits are counted in shared memory when S(a) fits
+    const bool priv = PV && ns <= CNT_SLOTS;  // the same for every thread of the CTA
+    if (priv) {
+      unsigned c = 0;
+#pragma unroll
+      for (int j = 0; j < WPT; ++j) c += __popc(s_bm[tid * WPT + j]);
+      unsigned incl = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      if (lane == 31) s_wsum[w] = incl;
+      __syncthreads();
+      unsigned base = incl - c;
+      for (int k = 0; k < w; ++k) base += s_wsum[k];
+#pragma unroll
+      for (int j = 0; j < WPT; ++j) {
+        s_pre[tid * WPT + j] = (unsigned short)base;
+        base += __popc(s_bm[tid * WPT + j]);
+      }
+      __syncthreads();
+    }
     unsigned ha = 0;  // PV: this warp's triangles at anchor a (lane 0)
     for (int g0 = 0; w + NW * g0 < np; g0 += 32) {
       const int pi = w + NW * (g0 + lane);
@@ -301,7 +336,13 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_tc_bitmap_cta(Lists L, const 
               const unsigned hit = (s_bm[x[u] >> 5] >> (x[u] & 31)) & 1u;
               cnt += hit;
               if (PV && hit) {
-                atomicAdd(cf + x[u], 1);
+                if (priv) {
+                  const int xw = x[u] >> 5;
+                  const unsigned slot = s_pre[xw] + __popc(s_bm[xw] & ((1u << (x[u] & 31)) - 1u));
+                  atomicAdd(&s_cnt[slot >> 1], 1u << ((slot & 1u) * 16u));
+                } else {
+                  atomicAdd(cf + x[u], 1);
+                }
                 ++hp;
               }
             }
@@ -316,6 +357,14 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_tc_bitmap_cta(Lists L, const 
     }
     if (PV && lane == 0 && ha) atomicAdd(cf + a, (int)ha);
     __syncthreads();
+    if (priv) {
+      for (int i = tid; i < ns; i += NT) {
+        const unsigned c = (s_cnt[i >> 1] >> ((i & 1) * 16)) & 0xffffu;
+        if (c) atomicAdd(cf + L.adj[sb + i], (int)c);
+      }
+      __syncthreads();
+      for (int i = tid; i < (ns + 1) / 2; i += NT) s_cnt[i] = 0u;
+    }
     for (int i = tid; i < ns; i += NT) s_bm[L.adj[sb + i] >> 5] = 0u;
     __syncthreads();
   }
@@ -693,8 +742,8 @@ extern "C" int sp_clustering_coeff(sp_graph_h g, int32_t* cf, int32_t variant) {
   if (g->V <= 65536) {
     int per_sm = 0;
     SP_CHECK_CUDA(
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tc::k_tc_bitmap_cta<4, 16, true>, 4 * 32, 0));
-    tc::k_tc_bitmap_cta<4, 16, true>
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tc::k_tc_bitmap_cta<4, 8, true>, 4 * 32, 0));
+    tc::k_tc_bitmap_cta<4, 8, true>
         <<<num_sms() * std::max(1, per_sm), 4 * 32, 0, s>>>(L, p->order.p, p->total.p, counts.p);
     SP_CHECK_LAUNCH();
   } else {

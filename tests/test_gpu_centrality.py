@@ -33,6 +33,21 @@ def test_clustering_coeff_matches_oracle(variant):
             assert int(out.astype(np.int64).sum()) == 3 * device_graph(g).tc()
 
 
+def test_clustering_coeff_large_anchor_set():
+    # a directed graph whose vertex 5000 has 5,500 higher neighbours (its S, above the
+    # 4,096 counted in shared memory, so its hits go straight to global counts) and
+    # 5,000 lower ones, each with edges into S; plus small anchors counted in shared memory
+    pairs = [[5000, u] for u in range(5000)] + [[5000, w] for w in range(5001, 10501)]
+    pairs += [[u, 5001 + (u * 7) % 5500] for u in range(5000)]
+    pairs += [[u, 5001 + (u * 13 + 1) % 5500] for u in range(0, 5000, 3)]
+    pairs += [[u, u + 1] for u in range(10501, 11999)] + [[u, u + 2] for u in range(10501, 11998)]
+    g = from_pairs(12000, np.array(pairs, np.int32), name="big_anchor")
+    for variant in (_lib.SP_TC_TUNED, _lib.SP_TC_PLAIN):
+        out = device_graph(g).clustering_coeff(variant=variant)
+        assert np.array_equal(out, O.lcc(g.indexofNodes, g.edgeList)), variant
+    assert O.lcc(g.indexofNodes, g.edgeList)[5000] > 0
+
+
 def test_clustering_coeff_entry_point_twice_and_device_output():
     import torch
 
