@@ -386,39 +386,90 @@ __global__ void k_relabel_rows(int V, const int32_t* __restrict__ inv, const int
 
 // Stable transpose, step 1: the (new dst, new src) pair of every edge, written in
 // ascending new source order (source k is old vertex inv[k]; its pairs start at
-// offp[k]). Sources of more than 1024 out-edges are listed for k_fwd_pairs_big, a
-// CTA per row, so one warp never walks a hub.
+// offp[k]). A warp takes 32 consecutive sources and flattens their edges over its
+// lanes (an exclusive scan of the out-degrees), 32 edges per step and four steps'
+// loads in flight together, so short rows do not leave lanes idle. Sources of more than 1024 out-edges are listed for
+// k_fwd_pairs_big instead.
 __global__ void k_fwd_pairs(int V, const int32_t* __restrict__ inv, const int32_t* __restrict__ new_id,
                             const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
                             const int32_t* __restrict__ offp, const int32_t* __restrict__ od,
                             int32_t* __restrict__ dst, int32_t* __restrict__ src, int32_t* __restrict__ big,
                             int* __restrict__ nbig) {
+  const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
-  for (int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < V; k += (gridDim.x * blockDim.x) >> 5) {
-    const int n = od[k];
-    if (n > 1024) {
-      if (lane == 0) big[atomicAdd(nbig, 1)] = k;
-      continue;
+  for (int k0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; k0 < V; k0 += ((gridDim.x * blockDim.x) >> 5) * 32) {
+    const int k = k0 + lane;
+    int n = 0, b = 0, d = 0;
+    if (k < V) {
+      n = od[k];
+      if (n > 1024) {
+        big[atomicAdd(nbig, 1)] = k;
+        n = 0;
+      } else if (n > 0) {
+        b = off[inv[k]];
+        d = offp[k];
+      }
     }
-    const int b = off[inv[k]], d = offp[k];
-    for (int j = lane; j < n; j += 32) {
-      dst[d + j] = new_id[adj[b + j]];
-      src[d + j] = k;
+    int inc = n;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(FULL, inc, o);
+      if (lane >= o) inc += t;
+    }
+    const int total = __shfl_sync(FULL, inc, 31);
+    const int excl = inc - n;
+    constexpr int U = 4;  // steps whose loads are in flight together
+    for (int t0 = 0; t0 < total; t0 += 32 * U) {
+      int pos[U], nb[U], row[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int t = t0 + 32 * u + lane;
+        int j = 0;  // the last lane whose edges start at or before t (never a lane without edges)
+#pragma unroll
+        for (int s = 16; s > 0; s >>= 1)
+          if (__shfl_sync(FULL, excl, j + s) <= t) j += s;
+        const int jb = __shfl_sync(FULL, b, j), jd = __shfl_sync(FULL, d, j), je = __shfl_sync(FULL, excl, j);
+        pos[u] = t < total ? jd + (t - je) : -1;
+        nb[u] = t < total ? adj[jb + (t - je)] : 0;
+        row[u] = k0 + j;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) nb[u] = pos[u] >= 0 ? new_id[nb[u]] : 0;
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (pos[u] >= 0) {
+          dst[pos[u]] = nb[u];
+          src[pos[u]] = row[u];
+        }
     }
   }
 }
 
+// Rows of more than 1024 out-edges: a CTA per row, four edges per thread in flight.
 __global__ void k_fwd_pairs_big(const int32_t* __restrict__ inv, const int32_t* __restrict__ new_id,
                                 const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
                                 const int32_t* __restrict__ offp, const int32_t* __restrict__ od,
                                 int32_t* __restrict__ dst, int32_t* __restrict__ src,
                                 const int32_t* __restrict__ big, const int* __restrict__ nbig) {
+  constexpr int U = 4;
   for (int i = blockIdx.x; i < *nbig; i += gridDim.x) {
     const int k = big[i];
     const int n = od[k], b = off[inv[k]], d = offp[k];
-    for (int j = threadIdx.x; j < n; j += blockDim.x) {
-      dst[d + j] = new_id[adj[b + j]];
-      src[d + j] = k;
+    for (int j0 = threadIdx.x; j0 < n; j0 += blockDim.x * U) {
+      int a[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int j = j0 + u * blockDim.x;
+        a[u] = j < n ? adj[b + j] : 0;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int j = j0 + u * blockDim.x;
+        if (j < n) {
+          dst[d + j] = new_id[a[u]];
+          src[d + j] = k;
+        }
+      }
     }
   }
 }
@@ -634,7 +685,7 @@ static int relabel(sp_graph* g, PrPlan* p) {
   pr::k_fwd_pairs<<<grid, 256, 0, s>>>(V, inv.p, p->new_id.p, g->off.p, g->adj.p, offp.p, p->od.p, dst.p, src.p,
                                        big.p, nbig.p);
   SP_CHECK_LAUNCH();
-  pr::k_fwd_pairs_big<<<num_sms() * 2, 256, 0, s>>>(inv.p, p->new_id.p, g->off.p, g->adj.p, offp.p, p->od.p, dst.p,
+  pr::k_fwd_pairs_big<<<num_sms() * 8, 256, 0, s>>>(inv.p, p->new_id.p, g->off.p, g->adj.p, offp.p, p->od.p, dst.p,
                                                      src.p, big.p, nbig.p);
   SP_CHECK_LAUNCH();
   cub::DoubleBuffer<int32_t> keys(dst.p, dst_alt.p), vals(src.p, p->radjp.p);
