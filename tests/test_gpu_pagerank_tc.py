@@ -250,6 +250,43 @@ def test_invalid_csr_rejected():
         assert dg.V == 3
 
 
+def test_csr_check_every_position():
+    # the edge check reads four entries per load: one planted fault (an id out of range,
+    # a swapped pair, a duplicate) is found at every position modulo 4, at quad
+    # boundaries and in the tail, and the untouched graph (E not a multiple of 4) passes
+    rng = np.random.default_rng(5)
+    V = 300
+    rows = [np.sort(rng.choice(V, size=int(rng.integers(0, 12)), replace=False)) for _ in range(V)]
+    off = np.zeros(V + 1, np.int32)
+    off[1:] = np.cumsum([len(r) for r in rows])
+    adj = np.concatenate(rows).astype(np.int32)
+    if adj.shape[0] % 4 == 0:
+        rows[-1] = np.array([], np.int64) if len(rows[-1]) == 0 else rows[-1][:-1]
+        off[1:] = np.cumsum([len(r) for r in rows])
+        adj = np.concatenate(rows).astype(np.int32)
+    E = adj.shape[0]
+    assert E % 4 != 0
+    with DeviceGraph(off, adj) as dg:
+        assert dg.V == V
+    starts = set(int(x) for x in off[:-1])
+    inner = [p for p in range(E - 1) if p + 1 not in starts]  # p and p + 1 in one row
+    picks = sorted(set([0, 1, 2, 3, 4, 5, E - 1, E - 2, E - 3, E - 4] + list(rng.choice(E, 40))))
+    for p in picks:
+        a = adj.copy()
+        a[p] = V
+        with pytest.raises(_lib.SPError):
+            DeviceGraph(off, a)
+    for p in sorted(set([q for q in inner if q % 4 == 3][:6] + [q for q in inner if q % 4 != 3][:6] + inner[-3:])):
+        a = adj.copy()
+        a[p], a[p + 1] = a[p + 1], a[p]
+        with pytest.raises(_lib.SPError):
+            DeviceGraph(off, a)
+        a = adj.copy()
+        a[p + 1] = a[p]
+        with pytest.raises(_lib.SPError):
+            DeviceGraph(off, a)
+
+
 def test_tc_large_graph_hash_path():
     # above 65536 vertices the anchor sets live in per-warp hash tables (+ the heavy-anchor kernel)
     g = G.rmat(17, 16, seed=3)
