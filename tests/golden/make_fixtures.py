@@ -9,7 +9,8 @@ Edge-list files (ingest/*.txt) are written by this script, except sample_graph.t
 (py-starplat/tests/inputs/input.txt without its vertex-count header line). For every
 file, ingest/<name>.npz holds the reference parseGraph arrays; files whose lines
 carry no weight (the reference leaves those uninitialised) store no edgeLen.
-known_answers.json holds the reference TC count of each file's graph.
+known_answers.json holds the reference TC count of each file's graph and its
+per-vertex counts of the clustering_coeff loop (the reference's check_if_nbr).
 """
 import json
 import os
@@ -69,6 +70,7 @@ def main(ref_root):
         np.savez(os.path.join(OUT, name.replace(".txt", ".npz")), **arrays)
         answers[name] = {"V": int(r["indexofNodes"].shape[0] - 1), "E": int(r["edgeList"].shape[0]),
                          "tc_reference": int(O.ref_tc(r["indexofNodes"], r["edgeList"], 1)),
+                         "lcc_reference": [int(x) for x in O.ref_lcc(r["indexofNodes"], r["edgeList"])],
                          "weights": has_w}
     with open(os.path.join(HERE, "known_answers.json"), "w") as f:
         json.dump(answers, f, indent=1, sort_keys=True)

@@ -27,6 +27,8 @@ def test_load_text_matches_reference_parse(name):
         for k in gold.files:
             assert np.array_equal(got[k], gold[k]), (name, k)
         assert dg.tc() == ANSWERS[name]["tc_reference"]
+        for variant in (_lib.SP_TC_TUNED, _lib.SP_TC_PLAIN):
+            assert dg.clustering_coeff(variant=variant).tolist() == ANSWERS[name]["lcc_reference"]
 
 
 def _big_file(path, seed, n=150_000, V=20_000):

@@ -22,6 +22,8 @@ def test_restatement_matches_reference_fixtures(name):
         assert np.array_equal(got[k], gold[k]), (name, k)
     assert got["indexofNodes"].shape[0] - 1 == ANSWERS[name]["V"]
     assert O.tc(got["indexofNodes"], got["edgeList"]) == ANSWERS[name]["tc_reference"]
+    # the clustering_coeff loop's per-vertex counts, as the reference's check_if_nbr gives them
+    assert O.lcc(got["indexofNodes"], got["edgeList"]).tolist() == ANSWERS[name]["lcc_reference"]
 
 
 def test_reference_known_answers():
