@@ -116,7 +116,10 @@ int sp_graph_info(sp_graph_h g, int32_t* V, int64_t* E, int32_t* symmetric);
  *   "bc.hub_deg", "bc.hub_chunk"  BC: level-list entries of vertices with more than
  *             hub_deg edges are cut into hub_chunk-edge pieces shared by all warps
  *             (defaults 64 and 64).
- *   "bc.batch"  BC: sources traversed together in one multi-source pass (1..64, default 64). */
+ *   "bc.batch"  BC: sources traversed together in one multi-source pass (1..64, default 64).
+ *   "bc.cluster"  BC of many graphs (sp_bc_graphs): CTAs per graph, 1 (default), 2, 4 or 8;
+ *             above 1 the CTAs of a thread-block cluster share a graph and synchronise with
+ *             hardware cluster barriers. */
 int sp_tune_set(sp_graph_h g, const char* key, int64_t value);
 int sp_tune_get(sp_graph_h g, const char* key, int64_t* value);
 
