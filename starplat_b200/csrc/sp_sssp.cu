@@ -111,6 +111,18 @@ struct Ring {
   int cnt;
 };
 
+// Adjacency and weights are streamed: each is read once per expansion of its vertex,
+// so their loads skip L1 and are marked first to leave L2, which keeps dist, the
+// stamps and the offsets (random accesses) resident. R-MAT 23: 9.1 -> 7.3 ms; grid
+// 4096^2: 33.3 -> 33.8 ms. Marking the dist loads evict-last on top gained nothing.
+__device__ __forceinline__ int ld_stream(const int32_t* p) {
+  unsigned long long pol;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  int v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+  return v;
+}
+
 // Warp-aggregated append of `want` lanes into buf via counter.
 __device__ __forceinline__ void warp_push(bool want, int val, int32_t* buf, int* counter) {
   const unsigned m = __ballot_sync(0xffffffffu, want);
@@ -319,8 +331,8 @@ __device__ __forceinline__ void relax_batch(const Args& a, int v, long long thr,
       nd[q] = INT_MAX;
       if (t < total) {
         const int k = jb + (t - je);
-        u[q] = a.adj[k];
-        nd[q] = jd + a.w[k];
+        u[q] = ld_stream(a.adj + k);
+        nd[q] = jd + ld_stream(a.w + k);
       }
     }
     relax_group<!LOCAL, SU>(a, u, nd, thr, round, epoch, o.fmin, res);
@@ -342,8 +354,8 @@ __device__ __forceinline__ void relax_range(const Args& a, int vb, int ve, long 
       u[q] = 0;
       nd[q] = INT_MAX;
       if (k < ve) {
-        u[q] = a.adj[k];
-        nd[q] = vd + a.w[k];
+        u[q] = ld_stream(a.adj + k);
+        nd[q] = vd + ld_stream(a.w + k);
       }
     }
     relax_group<!LOCAL, SU>(a, u, nd, thr, round, epoch, o.fmin, res);
