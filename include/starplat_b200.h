@@ -82,6 +82,19 @@ int sp_graph_load_text(const char* path, int32_t nthreads, sp_graph_h* out);
  * from sp_graph_info. */
 int sp_graph_export(sp_graph_h g, int32_t* indexofNodes, int32_t* edgeList, int32_t* edgeLen,
                     int32_t* rev_indexofNodes, int32_t* srcList, int32_t* edgeMap);
+/* Replaces graph::updateCSRDel / updateCSRAdd (graph.hpp:869-980) for one batch of n
+ * updates, the fields of the reference's `update` record (update.hpp:9-16) as host
+ * arrays: type[i] 'd' (delete) or 'a' (add), src[i] -> dst[i], weight[i] (NULL = 1).
+ * As a DSL Batch block does, the deletions apply first, then the additions. Deleting a
+ * missing edge does nothing; adding an edge that is present sums its weights (the
+ * parseGraph rule for duplicates), where the reference's diff-CSR would keep two edges.
+ * The vertex count stays V; an id outside [0, V) or another type rejects the whole
+ * batch with SP_ERR_INVALID and leaves g unchanged. The forward CSR is rebuilt on the
+ * device (one sort of the old and added edge keys); the reverse CSR, edgeMap and every
+ * algorithm's plan are rebuilt on the next call that needs them. A graph without
+ * edgeLen stays without. */
+int sp_graph_update(sp_graph_h g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
+                    const int32_t* weight);
 /* Use this CUDA stream (a cudaStream_t) for all later work on g; NULL = the library's own stream. */
 int sp_graph_set_stream(sp_graph_h g, void* cuda_stream);
 /* V, E, symmetric (1 when the forward CSR equals the reverse CSR). */

@@ -212,6 +212,27 @@ inline auto Compute_CD(GraphT& g, int* weight) {
   return q;
 }
 
+namespace starplat_b200 {
+// One batch of the reference's `update` records (update.hpp:9-16: type 'a' / 'd',
+// source, destination, weight), batch[k, k + size), applied to the device mirror of g:
+// deletions first, then additions, as a DSL Batch block runs updateCSRDel and then
+// updateCSRAdd. The host graph is not touched: call this beside the reference's own
+// update calls, or instead of them when only the device copy is used afterwards.
+template <class GraphT, class UpdateT>
+inline void apply_updates(GraphT& g, const std::vector<UpdateT>& batch, int k, int size) {
+  std::vector<char> type;
+  std::vector<int32_t> src, dst, w;
+  for (int i = k; i < k + size && i < (int)batch.size(); ++i) {
+    type.push_back(batch[i].type);
+    src.push_back(batch[i].source);
+    dst.push_back(batch[i].destination);
+    w.push_back(batch[i].weight);
+  }
+  check(sp_graph_update(mirror(g), (int64_t)type.size(), type.data(), src.data(), dst.data(), w.data()),
+        "apply_updates");
+}
+}  // namespace starplat_b200
+
 template <class GraphT>
 inline void staticClusteringCoeff(GraphT& g, int* cf) {
   starplat_b200::check(sp_clustering_coeff(starplat_b200::mirror(g), cf, SP_TC_TUNED), "staticClusteringCoeff");

@@ -149,6 +149,30 @@ __global__ void k_forward(int32_t V, int64_t E, const unsigned long long* __rest
   }
 }
 
+// Keys (src << 32 | dst) and weights (1 without edgeLen) of the current edges in CSR
+// order, which is key order. An edge whose key is in the sorted deletion set `del` gets
+// the key V << 32 instead: it sorts after every real edge and is dropped after the merge.
+__global__ void k_edge_keys(int32_t V, const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
+                            const int32_t* __restrict__ w, const unsigned long long* __restrict__ del, int ndel,
+                            unsigned long long* __restrict__ keys, int32_t* __restrict__ kw) {
+  const int lane = threadIdx.x & 31;
+  const unsigned long long gone = (unsigned long long)(uint32_t)V << 32;
+  for (int v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < V; v += (gridDim.x * blockDim.x) >> 5) {
+    const int b = off[v], e = off[v + 1];
+    for (int i = b + lane; i < e; i += 32) {
+      unsigned long long k = ((unsigned long long)(uint32_t)v << 32) | (uint32_t)adj[i];
+      int lo = 0, hi = ndel;
+      while (lo < hi) {
+        const int m = (lo + hi) >> 1;
+        if (del[m] < k) lo = m + 1; else hi = m;
+      }
+      if (lo < ndel && del[lo] == k) k = gone;
+      keys[i] = k;
+      kw[i] = w ? w[i] : 1;
+    }
+  }
+}
+
 }  // namespace ingest
 
 // The file mapped read-only (no copy of its bytes), unmapped on scope exit.
@@ -318,6 +342,145 @@ extern "C" int sp_graph_load_text(const char* path, int32_t nthreads, sp_graph_h
   }
   *out = nullptr;
   return load_text(path, nthreads, out);
+}
+
+namespace sp {
+
+// A batch of edge updates applied to the forward CSR on the device: deletions, then
+// additions (see sp_graph_update). Everything derived from the old CSR is dropped.
+static int update_graph(sp_graph* g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
+                        const int32_t* weight) {
+  const int32_t V = g->V;
+  std::vector<unsigned long long> del;
+  std::vector<int32_t> as, ad, aw;
+  for (int64_t i = 0; i < n; ++i) {
+    if (type[i] != 'a' && type[i] != 'd') {
+      set_error("sp_graph_update: update %lld has type '%c' (expected 'a' or 'd')", (long long)i, type[i]);
+      return SP_ERR_INVALID;
+    }
+    if (src[i] < 0 || src[i] >= V || dst[i] < 0 || dst[i] >= V) {
+      set_error("sp_graph_update: update %lld names an edge %d -> %d outside [0, %d)", (long long)i, src[i], dst[i],
+                V);
+      return SP_ERR_INVALID;
+    }
+    if (type[i] == 'd') {
+      del.push_back(((unsigned long long)(uint32_t)src[i] << 32) | (uint32_t)dst[i]);
+    } else {
+      as.push_back(src[i]);
+      ad.push_back(dst[i]);
+      aw.push_back(weight ? weight[i] : 1);
+    }
+  }
+  std::sort(del.begin(), del.end());
+  del.erase(std::unique(del.begin(), del.end()), del.end());
+  const int64_t E = g->E, na = (int64_t)as.size(), m = E + na;
+  if (m > INT_MAX) {
+    set_error("sp_graph_update: %lld edges after the update (int32 edge indices)", (long long)m);
+    return SP_ERR_UNSUPPORTED;
+  }
+  cudaStream_t s = g->stream;
+  int bits = 1;  // key bits above 32: ids up to V (V itself marks a deleted edge)
+  while (bits < 31 && (1 << bits) <= V) ++bits;
+  Arena T0;
+  dspan<unsigned long long> keys, keys_alt, ukeys, ddel;
+  dspan<int32_t> kw, kw_alt, uw, das, dad;
+  dspan<int> nrun;
+  dspan<unsigned char> temp;
+  size_t t_sort = 0, t_red = 0;
+  {
+    cub::DoubleBuffer<unsigned long long> kb(nullptr, nullptr);
+    cub::DoubleBuffer<int32_t> vb(nullptr, nullptr);
+    cub::DeviceRadixSort::SortPairs(nullptr, t_sort, kb, vb, (int)m, 0, 32 + bits, s);
+    cub::DeviceReduce::ReduceByKey(nullptr, t_red, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
+                                   (int32_t*)nullptr, (int32_t*)nullptr, (int*)nullptr, cub::Sum(), (int)m, s);
+  }
+  T0.want(keys, m);
+  T0.want(keys_alt, m);
+  T0.want(ukeys, m);
+  T0.want(kw, m);
+  T0.want(kw_alt, m);
+  T0.want(uw, m);
+  T0.want(ddel, del.size());
+  T0.want(das, na);
+  T0.want(dad, na);
+  T0.want(nrun, 1);
+  T0.want(temp, std::max(t_sort, t_red));
+  SP_TRY(T0.commit());
+  if (!del.empty())
+    SP_CHECK_CUDA(cudaMemcpyAsync(ddel.p, del.data(), sizeof(unsigned long long) * del.size(), cudaMemcpyHostToDevice, s));
+  if (E > 0) {
+    ingest::k_edge_keys<<<num_sms() * 8, 256, 0, s>>>(V, g->off.p, g->adj.p, g->has_w ? g->w.p : nullptr, ddel.p,
+                                                      (int)del.size(), keys.p, kw.p);
+    SP_CHECK_LAUNCH();
+  }
+  if (na > 0) {
+    SP_CHECK_CUDA(cudaMemcpyAsync(das.p, as.data(), 4 * (size_t)na, cudaMemcpyHostToDevice, s));
+    SP_CHECK_CUDA(cudaMemcpyAsync(dad.p, ad.data(), 4 * (size_t)na, cudaMemcpyHostToDevice, s));
+    SP_CHECK_CUDA(cudaMemcpyAsync(kw.p + E, aw.data(), 4 * (size_t)na, cudaMemcpyHostToDevice, s));
+    ingest::k_pack<<<num_sms() * 4, 256, 0, s>>>(na, das.p, dad.p, keys.p + E);
+    SP_CHECK_LAUNCH();
+  }
+  int runs = 0;
+  unsigned long long last = 0;
+  const unsigned long long gone = (unsigned long long)(uint32_t)V << 32;
+  if (m > 0) {
+    cub::DoubleBuffer<unsigned long long> kd(keys.p, keys_alt.p);
+    cub::DoubleBuffer<int32_t> vd(kw.p, kw_alt.p);
+    size_t t = temp.n;
+    SP_CHECK_CUDA(cub::DeviceRadixSort::SortPairs(temp.p, t, kd, vd, (int)m, 0, 32 + bits, s));
+    t = temp.n;
+    SP_CHECK_CUDA(cub::DeviceReduce::ReduceByKey(temp.p, t, kd.Current(), ukeys.p, vd.Current(), uw.p, nrun.p,
+                                                 cub::Sum(), (int)m, s));
+    g_launches += 2;
+    SP_TRY(copy_out(&runs, nrun.p, sizeof(int), s));
+    if (runs > 0) SP_TRY(copy_out(&last, ukeys.p + runs - 1, sizeof(last), s));
+  }
+  const int E2 = runs - (runs > 0 && last == gone ? 1 : 0);
+  dbuf<int32_t> off, adj, w;
+  SP_TRY(off.alloc((size_t)V + 1));
+  SP_TRY(adj.alloc(E2));
+  if (g->has_w) SP_TRY(w.alloc(E2));
+  if (E2 > 0) {
+    ingest::k_forward<<<num_sms() * 8, 256, 0, s>>>(V, E2, ukeys.p, off.p, adj.p);
+    SP_CHECK_LAUNCH();
+    if (g->has_w) SP_CHECK_CUDA(cudaMemcpyAsync(w.p, uw.p, 4 * (size_t)E2, cudaMemcpyDeviceToDevice, s));
+  } else {
+    SP_CHECK_CUDA(cudaMemsetAsync(off.p, 0, sizeof(int32_t) * ((size_t)V + 1), s));
+  }
+  SP_CHECK_CUDA(cudaStreamSynchronize(s));
+  // the new CSR replaces the old; plans, the reverse CSR and edgeMap are rebuilt on demand
+  free_pr_plan(g->pr);
+  free_tc_plan(g->tc);
+  free_sssp_plan(g->sssp);
+  free_bc_plan(g->bc);
+  free_lv_plan(g->lv);
+  g->pr = nullptr;
+  g->tc = nullptr;
+  g->sssp = nullptr;
+  g->bc = nullptr;
+  g->lv = nullptr;
+  g->off.swap(off);
+  g->adj.swap(adj);
+  if (g->has_w) g->w.swap(w);
+  g->roff.release();
+  g->radj.release();
+  g->emap.release();
+  g->has_rev = false;
+  g->symmetric = -1;
+  g->E = E2;
+  return finish_graph(g);
+}
+
+}  // namespace sp
+
+extern "C" int sp_graph_update(sp_graph_h g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
+                               const int32_t* weight) {
+  using namespace sp;
+  if (!g || n < 0 || (n > 0 && (!type || !src || !dst))) {
+    set_error("sp_graph_update: invalid argument");
+    return SP_ERR_INVALID;
+  }
+  return update_graph(g, n, type, src, dst, weight);
 }
 
 extern "C" int sp_graph_export(sp_graph_h g, int32_t* indexofNodes, int32_t* edgeList, int32_t* edgeLen,

@@ -1,6 +1,7 @@
 // Internal definitions shared by the sm_100a kernels and the C-ABI layer.
 #pragma once
 #include <cuda_runtime.h>
+#include <utility>
 
 #include <atomic>
 #include <cstdint>
@@ -78,6 +79,12 @@ struct dbuf {
     p = nullptr;
     n = 0;
     bytes = 0;
+  }
+  void swap(dbuf& o) {
+    std::swap(p, o.p);
+    std::swap(n, o.n);
+    std::swap(bytes, o.bytes);
+    std::swap(dev, o.dev);
   }
 };
 

@@ -92,6 +92,28 @@ class DeviceGraph:
         self.V, self.E = int(V.value), int(E.value)
         return self
 
+    def update(self, types, src, dst, weight=None) -> None:
+        """One batch of edge updates (graph::updateCSRDel then updateCSRAdd): types is a
+        str or bytes of 'a' / 'd' per update, src and dst int32 ids, weight int32 or None
+        (1). Deletions apply first; an added edge that exists gets its weights summed."""
+        t = np.frombuffer(types.encode() if isinstance(types, str) else bytes(types), np.uint8)
+        s = np.ascontiguousarray(src, np.int32)
+        d = np.ascontiguousarray(dst, np.int32)
+        n = t.shape[0]
+        if s.shape[0] != n or d.shape[0] != n:
+            raise ValueError("types, src and dst must have one entry per update")
+        w = None if weight is None else np.ascontiguousarray(weight, np.int32)
+        if w is not None and w.shape[0] != n:
+            raise ValueError("weight must have one entry per update")
+        t = np.ascontiguousarray(t)
+        check("sp_graph_update", lib().sp_graph_update(self.handle, n, t.ctypes.data if n else None,
+                                                       s.ctypes.data if n else None, d.ctypes.data if n else None,
+                                                       None if w is None or n == 0 else w.ctypes.data))
+        V = ctypes.c_int32()
+        E = ctypes.c_int64()
+        check("sp_graph_info", lib().sp_graph_info(self.handle, ctypes.byref(V), ctypes.byref(E), None))
+        self.V, self.E = int(V.value), int(E.value)
+
     def export(self) -> dict:
         """The mirror's CSR as host arrays named like graph.hpp's fields."""
         V, E = self.V, self.E

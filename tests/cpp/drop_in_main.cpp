@@ -61,6 +61,23 @@ int main(int argc, char** argv) {
   std::printf("CCU");
   for (int v = 0; v < V; ++v) std::printf(" %.9g", ccu[v]);
   std::printf("\n");
+  // a batch of updates shaped like the reference's update records: drop the first
+  // edge of vertex 1 (both directions) and add 0 <-> V-1
+  struct Upd {
+    char type;
+    int source, destination, weight;
+  };
+  std::vector<Upd> batch;
+  const int* off = g.indexofNodes;
+  const int* adj = g.edgeList;
+  if (off[2] > off[1]) {
+    batch.push_back({'d', 1, adj[off[1]], 0});
+    batch.push_back({'d', adj[off[1]], 1, 0});
+  }
+  batch.push_back({'a', 0, V - 1, 3});
+  batch.push_back({'a', V - 1, 0, 3});
+  starplat_b200::apply_updates(g, batch, 0, (int)batch.size());
+  std::printf("TCU %ld\n", Compute_TC(g));
   starplat_b200::invalidate(g);
   return 0;
 }

@@ -68,6 +68,20 @@ def check_outputs(res, g, src):
     assert np.array_equal(cc, O.closeness(g.indexofNodes, g.edgeList, g.edgeLen, srcs))
     ccu = np.array(res["CCU"], np.float32)
     assert np.array_equal(ccu, O.closeness_unweighted(g.indexofNodes, g.edgeList, srcs))
+    # the update batch the driver applies (apply_updates), on the host edge set
+    off, adj = g.indexofNodes, g.edgeList
+    edges = set(zip(np.repeat(np.arange(g.V), np.diff(off)).tolist(), adj.tolist()))
+    if off[2] > off[1]:
+        x = int(adj[off[1]])
+        edges -= {(1, x), (x, 1)}
+    edges |= {(0, g.V - 1), (g.V - 1, 0)}
+    keys = sorted(edges)
+    noff = np.zeros(g.V + 1, np.int64)
+    for a, _ in keys:
+        noff[a + 1] += 1
+    noff = np.cumsum(noff).astype(np.int32)
+    nadj = np.array([b for _, b in keys], np.int32)
+    assert int(res["TCU"][0]) == O.tc(noff, nadj)
 
 
 def small_graph():

@@ -1,0 +1,149 @@
+"""GPU: batches of edge updates applied to the device mirror (sp_graph_update, the
+role of graph::updateCSRDel / updateCSRAdd). The updated CSR equals the one built from
+the edge set on the host (deletions first, then additions, duplicate additions summed),
+and every algorithm then runs on it and matches the oracle."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from starplat_b200 import _lib
+from starplat_b200 import generators as G
+from starplat_b200.device import DeviceGraph
+
+from graphs import from_pairs
+
+pytestmark = pytest.mark.gpu
+
+
+def _edges(off, adj, w):
+    src = np.repeat(np.arange(len(off) - 1), np.diff(off))
+    return {(int(a), int(b)): int(c) for a, b, c in zip(src, adj, w)}
+
+
+def _apply(edges, types, src, dst, w):
+    out = dict(edges)
+    for t, a, b in zip(types, src, dst):
+        if t == "d":
+            out.pop((int(a), int(b)), None)
+    for t, a, b, c in zip(types, src, dst, w):
+        if t == "a":
+            out[(int(a), int(b))] = out.get((int(a), int(b)), 0) + int(c)
+    return out
+
+
+def _csr(V, edges):
+    keys = sorted(edges)
+    off = np.zeros(V + 1, np.int32)
+    for a, _ in keys:
+        off[a + 1] += 1
+    off = np.cumsum(off).astype(np.int32)
+    adj = np.array([b for _, b in keys], np.int32)
+    w = np.array([edges[k] for k in keys], np.int32)
+    return off, adj, w
+
+
+def _batch(rng, V, edges, n):
+    ex = list(edges)
+    types, src, dst, w = [], [], [], []
+    for _ in range(n):
+        kind = rng.integers(0, 4)
+        if kind == 0 and ex:  # delete an existing edge
+            a, b = ex[rng.integers(0, len(ex))]
+            types.append("d")
+        elif kind == 1:  # delete an edge that may not exist
+            a, b = rng.integers(0, V, 2)
+            types.append("d")
+        elif kind == 2 and ex:  # add an existing edge (weights summed)
+            a, b = ex[rng.integers(0, len(ex))]
+            types.append("a")
+        else:  # add a new edge, self-loops included
+            a, b = rng.integers(0, V, 2)
+            types.append("a")
+        src.append(int(a))
+        dst.append(int(b))
+        w.append(int(rng.integers(1, 50)))
+    return "".join(types), np.array(src, np.int32), np.array(dst, np.int32), np.array(w, np.int32)
+
+
+def test_update_batches_match_the_host_edge_set():
+    rng = np.random.default_rng(11)
+    g = G.rmat(12, 8, seed=3, directed=True)
+    g.edgeLen = G.hash_weights(g, 3, 1, 50, False)
+    edges = _edges(g.indexofNodes, g.edgeList, g.edgeLen)
+    with DeviceGraph.from_csr(g) as dg:
+        for step in range(4):
+            t, s, d, w = _batch(rng, g.V, edges, [1, 50, 700, 3000][step])
+            dg.update(t, s, d, w)
+            edges = _apply(edges, t, s, d, w)
+            off, adj, ww = _csr(g.V, edges)
+            got = dg.export()
+            assert np.array_equal(got["indexofNodes"], off) and np.array_equal(got["edgeList"], adj)
+            assert np.array_equal(got["edgeLen"], ww)
+            # the reverse CSR is rebuilt from the new forward CSR
+            rs = np.argsort(adj, kind="stable")
+            assert np.array_equal(got["srcList"], np.repeat(np.arange(g.V), np.diff(off))[rs])
+            # algorithms run on the updated graph
+            src = int(s[0])
+            dist, _ = dg.sssp(src)
+            assert np.array_equal(dist, O.sssp(off, adj, ww, src))
+            roff = np.zeros(g.V + 1, np.int32)
+            roff[1:] = np.cumsum(np.bincount(adj, minlength=g.V))
+            radj = np.repeat(np.arange(g.V), np.diff(off))[rs].astype(np.int32)
+            pr, it, _ = dg.pagerank(1e-6, 0.85, 100)
+            ref, rit, _ = O.pagerank(off, roff, radj, 1e-6, 0.85, 100)
+            assert abs(it - rit) <= 2 and np.abs(pr.astype(np.float64) - ref).sum() < 1e-5
+            assert dg.tc() == O.tc(off, adj)
+
+
+def test_update_undirected_keeps_symmetry_and_counts():
+    # adding and deleting both directions of undirected edges: triangles, BC and
+    # Louvain see the updated symmetric graph
+    g = G.rmat(11, 8, seed=5)
+    edges = _edges(g.indexofNodes, g.edgeList, np.ones(g.E, np.int32))
+    rng = np.random.default_rng(2)
+    pairs = rng.integers(0, g.V, (300, 2))
+    t = "d" * 150 + "a" * 150
+    src = np.concatenate([pairs[:150, 0], pairs[:150, 1], pairs[150:, 0], pairs[150:, 1]]).astype(np.int32)
+    dst = np.concatenate([pairs[:150, 1], pairs[:150, 0], pairs[150:, 1], pairs[150:, 0]]).astype(np.int32)
+    types = "d" * 300 + "a" * 300
+    with DeviceGraph.from_csr(g, with_weights=False) as dg:
+        assert dg.tc() == O.tc(g.indexofNodes, g.edgeList)
+        dg.update(types, src, dst)
+        w1 = np.ones(src.shape[0], np.int32)
+        edges = _apply(edges, types, src, dst, w1)
+        off, adj, _ = _csr(g.V, edges)
+        got = dg.export()
+        assert np.array_equal(got["indexofNodes"], off) and np.array_equal(got["edgeList"], adj)
+        assert "edgeLen" not in got  # a graph without weights stays without
+        assert dg.tc() == O.tc(off, adj)
+        srcs = G.pick_sources(g, 20, seed=3)
+        bc = dg.bc(srcs).astype(np.float64)
+        rbc = O.bc(off, adj, srcs)
+        assert np.all(np.abs(bc - rbc) <= 1e-5 * np.abs(rbc) + 1e-6)
+        assert np.array_equal(dg.clustering_coeff(), O.lcc(off, adj))
+    del t
+
+
+def test_update_edge_cases():
+    g = from_pairs(4, [[0, 1], [1, 2], [2, 3]], name="path4")
+    g.edgeLen = np.array([5, 6, 7], np.int32)
+    with DeviceGraph.from_csr(g) as dg:
+        dg.update("", [], [])  # an empty batch changes nothing
+        assert dg.E == 3
+        # delete every edge, then add them back in another order with new weights
+        dg.update("ddd", [0, 1, 2], [1, 2, 3])
+        assert dg.E == 0
+        assert np.array_equal(dg.export()["indexofNodes"], [0, 0, 0, 0, 0])
+        dg.update("aaaa", [2, 0, 1, 0], [3, 1, 2, 1], [1, 2, 3, 4])
+        got = dg.export()
+        assert got["edgeList"].tolist() == [1, 2, 3] and got["edgeLen"].tolist() == [6, 3, 1]
+        # a deletion and an addition of the same edge in one batch: deleted first, then added
+        dg.update("ad", [0, 0], [1, 1], [9, 0])
+        assert dg.export()["edgeLen"].tolist() == [9, 3, 1]
+        dist, _ = dg.sssp(0)
+        assert dist.tolist() == [0, 9, 12, 13]
+        # bad batches are rejected whole and leave the graph as it was
+        for t, s, d in (("a", [4], [0]), ("d", [0], [-1]), ("x", [0], [1])):
+            with pytest.raises(_lib.SPError):
+                dg.update(t, s, d)
+        assert dg.export()["edgeLen"].tolist() == [9, 3, 1]
