@@ -25,6 +25,8 @@ baseline:
   louvain_sbm1m    Louvain, planted partition 1,048,576 vertices, 256 blocks (E * sweeps / t)
   ingest_rmat20    text edge list -> device mirror (sp_graph_load_text), directed R-MAT 20
                    ef16 with weights (M edge lines / s; not a GTEPS figure)
+  update_rmat20    one batch of 2^20 edge updates (half deletions) applied to the device
+                   mirror of directed R-MAT 20 (M updates / s, host arrays to rebuilt CSR)
   centrality       per-vertex triangle counts on the TC graph (m / t), and closeness on
                    the BC graph: unweighted over its 256 sources, weighted (U[1,100])
                    over 16 of them (sum of E_r / t)
@@ -528,7 +530,7 @@ def bench_ingest(steps, warmup, cpu):
 
 
 EXTRAS = ("tc_rmat16", "sssp_rmat23", "sssp_grid4096", "bc_rmat20", "bc_er1000", "louvain_sbm1m", "ingest_rmat20",
-          "centrality")
+          "centrality", "update_rmat20")
 
 
 def bench_centrality(steps, warmup, stream, hbm, cpu):
@@ -611,6 +613,66 @@ def bench_centrality(steps, warmup, stream, hbm, cpu):
     return out
 
 
+def bench_update(steps, warmup, stream, cpu, nupd=1 << 20):
+    """One batch of nupd edge updates (sp_graph_update) on directed R-MAT 20 ef16 with
+    weights: half deletions of existing edges, half additions of random edges. Timed
+    from host arrays to the rebuilt device CSR (M updates / s)."""
+    from starplat_b200 import generators as G
+    from starplat_b200.device import DeviceGraph
+
+    g = G.rmat(20, 16, seed=7, directed=True)
+    g.edgeLen = G.hash_weights(g, 7, 1, 100, False)
+    rng = np.random.default_rng(20)
+    src_all = np.repeat(np.arange(g.V, dtype=np.int32), np.diff(g.indexofNodes))
+    pick = rng.choice(g.E, nupd // 2, replace=False)
+    ds, dd = src_all[pick], g.edgeList[pick]
+    as_, ad = rng.integers(0, g.V, (2, nupd - nupd // 2)).astype(np.int32)
+    types = "d" * (nupd // 2) + "a" * (nupd - nupd // 2)
+    src = np.concatenate([ds, as_]).astype(np.int32)
+    dst = np.concatenate([dd, ad]).astype(np.int32)
+    w = rng.integers(1, 100, nupd).astype(np.int32)
+    times = []
+    for k in range(warmup + steps):
+        with DeviceGraph.from_csr(g, with_reverse=False) as dg:
+            dg.set_stream(stream)
+            torch_sync()
+            t = time.perf_counter()
+            dg.update(types, src, dst, w)
+            torch_sync()
+            if k >= warmup:
+                times.append(time.perf_counter() - t)
+            e_after = dg.E
+    ms = 1e3 * statistics.median(times)
+    out = {"workload": f"update rmat20 ef16 directed seed7, {nupd} updates (half deletions of existing edges)",
+           "value": nupd / (ms / 1e3) / 1e6, "unit": "M updates/s", "ms": ms, "E_before": g.E, "E_after": e_after}
+    if cpu:
+        # the same batch on the host: edge keys, deletions by search, additions merged
+        t = time.perf_counter()
+        keys = (src_all.astype(np.int64) << 32) | g.edgeList.astype(np.int64)
+        dk = np.unique((ds.astype(np.int64) << 32) | dd.astype(np.int64))
+        keep = np.ones(g.E, bool)
+        pos = np.searchsorted(keys, dk)
+        hit = pos < g.E
+        hit[hit] = keys[pos[hit]] == dk[hit]
+        keep[pos[hit]] = False
+        allk = np.concatenate([keys[keep], (as_.astype(np.int64) << 32) | ad.astype(np.int64)])
+        allw = np.concatenate([g.edgeLen[keep], w[nupd // 2:]]).astype(np.int64)
+        uk, inv = np.unique(allk, return_inverse=True)
+        uw = np.zeros(uk.shape[0], np.int64)
+        np.add.at(uw, inv, allw)
+        dt = time.perf_counter() - t
+        out["same_edge_count_as_host"] = bool(uk.shape[0] == e_after)
+        out["cpu_baseline"] = {"value": nupd / dt / 1e6, "unit": "M updates/s", "cores": 1, "kind": "port",
+                               "sample": f"numpy sort-and-merge of the same batch ({dt:.2f} s)"}
+    return out
+
+
+def torch_sync():
+    import torch
+
+    torch.cuda.synchronize()
+
+
 def run_extras(want, args, stream, hbm, cpu_ok):
     from starplat_b200 import generators as G
 
@@ -651,6 +713,8 @@ def run_extras(want, args, stream, hbm, cpu_ok):
         guarded("ingest_rmat20", lambda: bench_ingest(max(1, ks // 2), 1, cpu_ok))
     if "centrality" in want:
         guarded("centrality", lambda: bench_centrality(ks, kw, stream, hbm, cpu_ok))
+    if "update_rmat20" in want:
+        guarded("update_rmat20", lambda: bench_update(ks, kw, stream, cpu_ok))
     return extras
 
 

@@ -150,7 +150,8 @@ __global__ void k_forward(int32_t V, int64_t E, const unsigned long long* __rest
 }
 
 // Keys (src << 32 | dst) and weights (1 without edgeLen) of the current edges in CSR
-// order, which is key order. An edge whose key is in the sorted deletion set `del` gets
+// order, which is key order. An edge whose key is in the sorted deletion keys `del`
+// (repeats allowed) gets
 // the key V << 32 instead: it sorts after every real edge and is dropped after the merge.
 __global__ void k_edge_keys(int32_t V, const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
                             const int32_t* __restrict__ w, const unsigned long long* __restrict__ del, int ndel,
@@ -353,6 +354,10 @@ static int update_graph(sp_graph* g, int64_t n, const char* type, const int32_t*
   const int32_t V = g->V;
   std::vector<unsigned long long> del;
   std::vector<int32_t> as, ad, aw;
+  del.reserve(n);
+  as.reserve(n);
+  ad.reserve(n);
+  aw.reserve(n);
   for (int64_t i = 0; i < n; ++i) {
     if (type[i] != 'a' && type[i] != 'd') {
       set_error("sp_graph_update: update %lld has type '%c' (expected 'a' or 'd')", (long long)i, type[i]);
@@ -371,9 +376,7 @@ static int update_graph(sp_graph* g, int64_t n, const char* type, const int32_t*
       aw.push_back(weight ? weight[i] : 1);
     }
   }
-  std::sort(del.begin(), del.end());
-  del.erase(std::unique(del.begin(), del.end()), del.end());
-  const int64_t E = g->E, na = (int64_t)as.size(), m = E + na;
+  const int64_t E = g->E, na = (int64_t)as.size(), m = E + na, nd = (int64_t)del.size();
   if (m > INT_MAX) {
     set_error("sp_graph_update: %lld edges after the update (int32 edge indices)", (long long)m);
     return SP_ERR_UNSUPPORTED;
@@ -382,15 +385,16 @@ static int update_graph(sp_graph* g, int64_t n, const char* type, const int32_t*
   int bits = 1;  // key bits above 32: ids up to V (V itself marks a deleted edge)
   while (bits < 31 && (1 << bits) <= V) ++bits;
   Arena T0;
-  dspan<unsigned long long> keys, keys_alt, ukeys, ddel;
+  dspan<unsigned long long> keys, keys_alt, ukeys, ddel, ddel_alt;
   dspan<int32_t> kw, kw_alt, uw, das, dad;
   dspan<int> nrun;
   dspan<unsigned char> temp;
-  size_t t_sort = 0, t_red = 0;
+  size_t t_sort = 0, t_red = 0, t_del = 0;
   {
     cub::DoubleBuffer<unsigned long long> kb(nullptr, nullptr);
     cub::DoubleBuffer<int32_t> vb(nullptr, nullptr);
     cub::DeviceRadixSort::SortPairs(nullptr, t_sort, kb, vb, (int)m, 0, 32 + bits, s);
+    cub::DeviceRadixSort::SortKeys(nullptr, t_del, kb, (int)nd, 0, 32 + bits, s);
     cub::DeviceReduce::ReduceByKey(nullptr, t_red, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
                                    (int32_t*)nullptr, (int32_t*)nullptr, (int*)nullptr, cub::Sum(), (int)m, s);
   }
@@ -400,17 +404,25 @@ static int update_graph(sp_graph* g, int64_t n, const char* type, const int32_t*
   T0.want(kw, m);
   T0.want(kw_alt, m);
   T0.want(uw, m);
-  T0.want(ddel, del.size());
+  T0.want(ddel, nd);
+  T0.want(ddel_alt, nd);
   T0.want(das, na);
   T0.want(dad, na);
   T0.want(nrun, 1);
-  T0.want(temp, std::max(t_sort, t_red));
+  T0.want(temp, std::max(std::max(t_sort, t_red), t_del));
   SP_TRY(T0.commit());
-  if (!del.empty())
-    SP_CHECK_CUDA(cudaMemcpyAsync(ddel.p, del.data(), sizeof(unsigned long long) * del.size(), cudaMemcpyHostToDevice, s));
+  const unsigned long long* dsorted = ddel.p;  // the deletion keys, sorted on the device
+  if (nd > 0) {
+    SP_CHECK_CUDA(cudaMemcpyAsync(ddel.p, del.data(), sizeof(unsigned long long) * nd, cudaMemcpyHostToDevice, s));
+    cub::DoubleBuffer<unsigned long long> kd(ddel.p, ddel_alt.p);
+    size_t t = temp.n;
+    SP_CHECK_CUDA(cub::DeviceRadixSort::SortKeys(temp.p, t, kd, (int)nd, 0, 32 + bits, s));
+    g_launches++;
+    dsorted = kd.Current();
+  }
   if (E > 0) {
-    ingest::k_edge_keys<<<num_sms() * 8, 256, 0, s>>>(V, g->off.p, g->adj.p, g->has_w ? g->w.p : nullptr, ddel.p,
-                                                      (int)del.size(), keys.p, kw.p);
+    ingest::k_edge_keys<<<num_sms() * 8, 256, 0, s>>>(V, g->off.p, g->adj.p, g->has_w ? g->w.p : nullptr, dsorted,
+                                                      (int)nd, keys.p, kw.p);
     SP_CHECK_LAUNCH();
   }
   if (na > 0) {
