@@ -264,6 +264,18 @@ int sp_mlp_train(float* params, const float* X, const float* T, int32_t N, int32
 /* Load (params != NULL) or unload (params == NULL) the process-wide scheduling model;
  * feat_mean/feat_scale normalise inputs: x' = (x - mean) * scale. */
 int sp_sched_load(const float* params, const float* feat_mean, const float* feat_scale);
+/* Replaces the generated Batch block of DynSSSP (DSL dynamicDSLCodes/dynamicBatchSSSP:
+ * OnDelete + updateCSRDel + Decremental, then OnAdd + updateCSRAdd + Incremental): one
+ * batch of edge updates as in sp_graph_update, then the distances from source on the
+ * updated graph over its edgeLen. dist[V] (host or device) holds the distances from
+ * source before the batch on entry (from sp_sssp or an earlier call) and after it on
+ * return. A batch of additions only resumes from those distances with the sources of
+ * the added edges queued: distances only drop, and each drop starts at an added edge.
+ * A batch with deletions solves again from source. Results are exact either way; the
+ * DSL's OnAdd test (dest.dist > src.dist + 1) ignores the edge weight, this does not.
+ * Tune key "sssp.last_incremental" (read only) says which path the last call took. */
+int sp_sssp_dynamic(sp_graph_h g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
+                    const int32_t* weight, int32_t source, int32_t* dist);
 /* The SP_MLP_IN inputs the scheduler builds for SSSP on g with a candidate schedule
  * (delta multiple of the largest weight, CTAs per SM, cascade budget as for
  * "sssp.local"); weight NULL = edgeLen. */

@@ -349,8 +349,8 @@ namespace sp {
 
 // A batch of edge updates applied to the forward CSR on the device: deletions, then
 // additions (see sp_graph_update). Everything derived from the old CSR is dropped.
-static int update_graph(sp_graph* g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
-                        const int32_t* weight) {
+int update_graph(sp_graph* g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
+                 const int32_t* weight) {
   const int32_t V = g->V;
   std::vector<unsigned long long> del;
   std::vector<int32_t> as, ad, aw;

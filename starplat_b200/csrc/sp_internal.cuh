@@ -166,6 +166,7 @@ struct sp_graph {
   int32_t sssp_last_ctas = 0;
   int32_t sssp_last_local = 0;
   int64_t sssp_last_relaxed = 0;  // edges the last delta-stepping run relaxed
+  int32_t sssp_last_incremental = 0;  // 1 if the last sp_sssp_dynamic warm-started
   int32_t sssp_hub_deg = 0;    // SSSP: vertices above this out-degree go to shared pieces (0 = default)
   int32_t sssp_hub_chunk = 0;  // SSSP: edges per piece (0 = default)
   int32_t sssp_local = -1;     // SSSP: warp cascade budget in 32-edge steps per round (-1 = default, 0 = off)
@@ -189,6 +190,9 @@ int ensure_emap(sp_graph* g);         // builds emap (edgeMap) on device if miss
 // off[v] = first index of keys (ascending, E of them) that is >= v, for v = 0..V
 int offsets_of_sorted(int32_t V, int64_t E, const int32_t* keys, int32_t* off, cudaStream_t s);
 int finish_graph(sp_graph* g);        // checks a library-built CSR, sets max_out_deg
+// one batch of edge updates on the forward CSR, deletions then additions (sp_ingest.cu)
+int update_graph(sp_graph* g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
+                 const int32_t* weight);
 int pr_order_default();               // PageRank vertex order default (sp_pagerank.cu)
 int pr_src_hint_default();
 int tc_cta_warps_default();           // TC kernel choice default (sp_tc.cu)

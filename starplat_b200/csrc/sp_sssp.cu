@@ -549,6 +549,45 @@ __global__ void k_init(int V, int src, int32_t* dist, int32_t* qstamp, int32_t* 
   }
 }
 
+// Warm start (sp_sssp_dynamic): dist keeps the caller's values; stamps and counters
+// are reset here, and k_seed then queues the seed vertices (hubs as hub entries).
+__global__ void k_reset(int V, int32_t* qstamp, int32_t* fstamp, Ctl* c) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    qstamp[v] = -1;
+    fstamp[v] = -1;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    c->bar.arrived = 0;
+    c->bar.error = 0;
+    for (int k = 0; k < 3; ++k) {
+      c->qcount[k] = 0;
+      c->hcount[k] = 0ull;
+      c->fcount[k] = 0;
+      c->fmin[k] = INT_MAX;
+    }
+    c->rounds = c->epochs = c->status = 0;
+    c->relaxed = 0ull;
+  }
+}
+
+// Queues n distinct seeds for round 0 (after k_reset, in stream order).
+__global__ void k_seed(int n, const int32_t* __restrict__ seeds, int32_t* qstamp, int32_t* q0, int32_t* hv0,
+                       int32_t* hb0, const int32_t* __restrict__ off, Ctl* c, int hub_deg, int hub_chunk) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int v = seeds[i];
+    qstamp[v] = 0;
+    const int d = off[v + 1] - off[v];
+    if (d > hub_deg) {
+      const unsigned long long old =
+          atomicAdd(&c->hcount[0], (1ull << 32) | (unsigned long long)((d + hub_chunk - 1) / hub_chunk));
+      hv0[old >> 32] = v;
+      hb0[old >> 32] = (int)(old & 0xffffffffull);
+    } else {
+      q0[atomicAdd(&c->qcount[0], 1)] = v;
+    }
+  }
+}
+
 // ---- plain form (generated CUDA code shape)
 __global__ void k_plain(int V, const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
                         const int32_t* __restrict__ w, int32_t* dist, const char* __restrict__ modified,
@@ -670,8 +709,10 @@ static int sssp_features(sp_graph* g, double mult, int ctas, int local, float* x
   return SP_OK;
 }
 
+// One delta-stepping solve from src, or (warm, nseeds > 0) from the distances already
+// in the plan's dist buffer with the given device seed vertices queued.
 static int sssp_delta(sp_graph* g, const int32_t* w, int32_t src, int32_t* dist_out, int64_t delta, int ctas,
-                      int local, int32_t* rounds_out) {
+                      int local, int32_t* rounds_out, const int32_t* d_seeds = nullptr, int nseeds = 0) {
   SsspPlan* p = g->sssp;
   cudaStream_t s = g->stream;
   const int V = g->V;
@@ -713,9 +754,17 @@ static int sssp_delta(sp_graph* g, const int32_t* w, int32_t src, int32_t* dist_
   a.hub_deg = std::min(g->sssp_hub_deg > 0 ? g->sssp_hub_deg : ss::HUB_DEG, ss::HUB_DEG_MAX);
   a.hub_chunk = g->sssp_hub_chunk > 0 ? g->sssp_hub_chunk : ss::HUB_CHUNK;
   a.local_edges = 32 * local;
-  ss::k_init<<<num_sms() * 4, 256, 0, s>>>(V, src, p->dist.p, p->qstamp.p, p->fstamp.p, p->q0.p, p->h0.p, p->hb0.p,
-                                            g->off.p, p->ctl.p, a.hub_deg, a.hub_chunk);
-  SP_CHECK_LAUNCH();
+  if (nseeds > 0) {
+    ss::k_reset<<<num_sms() * 4, 256, 0, s>>>(V, p->qstamp.p, p->fstamp.p, p->ctl.p);
+    SP_CHECK_LAUNCH();
+    ss::k_seed<<<std::max(1, std::min(num_sms() * 4, (nseeds + 255) / 256)), 256, 0, s>>>(
+        nseeds, d_seeds, p->qstamp.p, p->q0.p, p->h0.p, p->hb0.p, g->off.p, p->ctl.p, a.hub_deg, a.hub_chunk);
+    SP_CHECK_LAUNCH();
+  } else {
+    ss::k_init<<<num_sms() * 4, 256, 0, s>>>(V, src, p->dist.p, p->qstamp.p, p->fstamp.p, p->q0.p, p->h0.p,
+                                              p->hb0.p, g->off.p, p->ctl.p, a.hub_deg, a.hub_chunk);
+    SP_CHECK_LAUNCH();
+  }
   int per_sm = 0;
   SP_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ss::k_delta, ss::THREADS, 0));
   const int grid = num_sms() * std::max(1, std::min(per_sm, ctas));
@@ -774,28 +823,12 @@ static int sssp_plain(sp_graph* g, const int32_t* w, int32_t src, int32_t* dist_
   return SP_OK;
 }
 
-}  // namespace sp
-
-extern "C" int sp_sssp(sp_graph_h g, const int32_t* weight, int32_t src, int32_t* dist, int64_t delta,
-                       int32_t variant, int32_t* rounds) {
-  using namespace sp;
-  if (!g || !dist) {
-    set_error("sp_sssp: NULL argument");
-    return SP_ERR_INVALID;
-  }
-  if (src < 0 || src >= g->V) {
-    set_error("sp_sssp: source %d out of range [0, %d)", src, g->V);
-    return SP_ERR_INVALID;
-  }
-  const int32_t* w = nullptr;
-  SP_TRY(sssp_prepare(g, weight, &w));
-  if (variant == SP_SSSP_PLAIN) return sssp_plain(g, w, src, dist, rounds);
-  if (variant != SP_SSSP_DELTA) {
-    set_error("sp_sssp: unknown variant %d", variant);
-    return SP_ERR_INVALID;
-  }
-  int ctas = g->sssp_ctas_per_sm > 0 ? g->sssp_ctas_per_sm : 4;
-  int local = g->sssp_local >= 0 ? g->sssp_local : ss::LOCAL_STEPS;
+// The schedule of a delta-stepping solve: an explicit delta (argument or sssp.delta
+// knob) and the sssp.ctas_per_sm / sssp.local knobs, else the learned choice when a
+// model is loaded (cached per weight range and model), else the fixed heuristic.
+static int sssp_schedule(sp_graph* g, int64_t& delta, int& ctas, int& local) {
+  ctas = g->sssp_ctas_per_sm > 0 ? g->sssp_ctas_per_sm : 4;
+  local = g->sssp_local >= 0 ? g->sssp_local : ss::LOCAL_STEPS;
   const int64_t wmax = std::max<int64_t>(1, (int64_t)g->sssp->w_max);
   if (delta <= 0 && g->sssp_delta > 0) delta = g->sssp_delta;
   SsspPlan* sp_ = g->sssp;
@@ -849,7 +882,77 @@ extern "C" int sp_sssp(sp_graph_h g, const int32_t* weight, int32_t src, int32_t
   g->sssp_last_delta = delta;
   g->sssp_last_ctas = ctas;
   g->sssp_last_local = local;
+  return SP_OK;
+}
+
+}  // namespace sp
+
+extern "C" int sp_sssp(sp_graph_h g, const int32_t* weight, int32_t src, int32_t* dist, int64_t delta,
+                       int32_t variant, int32_t* rounds) {
+  using namespace sp;
+  if (!g || !dist) {
+    set_error("sp_sssp: NULL argument");
+    return SP_ERR_INVALID;
+  }
+  if (src < 0 || src >= g->V) {
+    set_error("sp_sssp: source %d out of range [0, %d)", src, g->V);
+    return SP_ERR_INVALID;
+  }
+  const int32_t* w = nullptr;
+  SP_TRY(sssp_prepare(g, weight, &w));
+  if (variant == SP_SSSP_PLAIN) return sssp_plain(g, w, src, dist, rounds);
+  if (variant != SP_SSSP_DELTA) {
+    set_error("sp_sssp: unknown variant %d", variant);
+    return SP_ERR_INVALID;
+  }
+  int ctas = 0, local = 0;
+  SP_TRY(sssp_schedule(g, delta, ctas, local));
   return sssp_delta(g, w, src, dist, delta, ctas, local, rounds);
+}
+
+extern "C" int sp_sssp_dynamic(sp_graph_h g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
+                               const int32_t* weight, int32_t source, int32_t* dist) {
+  using namespace sp;
+  if (!g || !dist || n < 0 || (n > 0 && (!type || !src || !dst))) {
+    set_error("sp_sssp_dynamic: invalid argument");
+    return SP_ERR_INVALID;
+  }
+  if (source < 0 || source >= g->V) {
+    set_error("sp_sssp_dynamic: source %d out of range [0, %d)", source, g->V);
+    return SP_ERR_INVALID;
+  }
+  if (!g->has_w) {
+    set_error("sp_sssp_dynamic: the graph has no edgeLen");
+    return SP_ERR_INVALID;
+  }
+  bool deletes = false;
+  std::vector<int32_t> seeds;
+  for (int64_t i = 0; i < n; ++i) {
+    if (type[i] == 'd') deletes = true;
+    if (type[i] == 'a') seeds.push_back(src[i]);
+  }
+  SP_TRY(update_graph(g, n, type, src, dst, weight));
+  g->sssp_last_incremental = 0;
+  if (n == 0) return SP_OK;  // nothing changed: the caller's distances stand
+  const int32_t* w = nullptr;
+  SP_TRY(sssp_prepare(g, nullptr, &w));
+  int64_t delta = 0;
+  int ctas = 0, local = 0;
+  SP_TRY(sssp_schedule(g, delta, ctas, local));
+  if (deletes) return sssp_delta(g, w, source, dist, delta, ctas, local, nullptr);
+  // additions only: distances can only drop, and every drop starts at an added edge,
+  // so the solve resumes from the old distances with the added edges' sources queued
+  std::sort(seeds.begin(), seeds.end());
+  seeds.erase(std::unique(seeds.begin(), seeds.end()), seeds.end());
+  SsspPlan* p = g->sssp;
+  cudaStream_t s = g->stream;
+  SP_TRY(p->dist.alloc(g->V));
+  SP_CHECK_CUDA(cudaMemcpyAsync(p->dist.p, dist, sizeof(int32_t) * g->V, cudaMemcpyDefault, s));
+  dbuf<int32_t> d_seeds;
+  SP_TRY(d_seeds.alloc(seeds.size()));
+  SP_CHECK_CUDA(cudaMemcpyAsync(d_seeds.p, seeds.data(), sizeof(int32_t) * seeds.size(), cudaMemcpyHostToDevice, s));
+  g->sssp_last_incremental = 1;
+  return sssp_delta(g, w, source, dist, delta, ctas, local, nullptr, d_seeds.p, (int)seeds.size());
 }
 
 extern "C" int sp_sssp_features(sp_graph_h g, const int32_t* weight, double delta_mult, int32_t ctas_per_sm,

@@ -92,11 +92,9 @@ class DeviceGraph:
         self.V, self.E = int(V.value), int(E.value)
         return self
 
-    def update(self, types, src, dst, weight=None) -> None:
-        """One batch of edge updates (graph::updateCSRDel then updateCSRAdd): types is a
-        str or bytes of 'a' / 'd' per update, src and dst int32 ids, weight int32 or None
-        (1). Deletions apply first; an added edge that exists gets its weights summed."""
-        t = np.frombuffer(types.encode() if isinstance(types, str) else bytes(types), np.uint8)
+    @staticmethod
+    def _batch(types, src, dst, weight):
+        t = np.ascontiguousarray(np.frombuffer(types.encode() if isinstance(types, str) else bytes(types), np.uint8))
         s = np.ascontiguousarray(src, np.int32)
         d = np.ascontiguousarray(dst, np.int32)
         n = t.shape[0]
@@ -105,14 +103,33 @@ class DeviceGraph:
         w = None if weight is None else np.ascontiguousarray(weight, np.int32)
         if w is not None and w.shape[0] != n:
             raise ValueError("weight must have one entry per update")
-        t = np.ascontiguousarray(t)
-        check("sp_graph_update", lib().sp_graph_update(self.handle, n, t.ctypes.data if n else None,
-                                                       s.ctypes.data if n else None, d.ctypes.data if n else None,
-                                                       None if w is None or n == 0 else w.ctypes.data))
+        ptrs = [a.ctypes.data if n else None for a in (t, s, d)]
+        return n, ptrs + [None if w is None or n == 0 else w.ctypes.data], (t, s, d, w)
+
+    def _refresh_size(self):
         V = ctypes.c_int32()
         E = ctypes.c_int64()
         check("sp_graph_info", lib().sp_graph_info(self.handle, ctypes.byref(V), ctypes.byref(E), None))
         self.V, self.E = int(V.value), int(E.value)
+
+    def update(self, types, src, dst, weight=None) -> None:
+        """One batch of edge updates (graph::updateCSRDel then updateCSRAdd): types is a
+        str or bytes of 'a' / 'd' per update, src and dst int32 ids, weight int32 or None
+        (1). Deletions apply first; an added edge that exists gets its weights summed."""
+        n, ptrs, _keep = self._batch(types, src, dst, weight)
+        check("sp_graph_update", lib().sp_graph_update(self.handle, n, *ptrs))
+        self._refresh_size()
+
+    def sssp_dynamic(self, types, src, dst, weight, source: int, dist):
+        """DynSSSP's Batch block: apply the updates, then bring dist (the distances from
+        source before the batch, int32[V], host or device) up to date on the new graph.
+        Additions only resume from dist; a batch with deletions solves again. Returns
+        True when the call resumed (incremental) and False when it solved again."""
+        _ensure_scheduler()
+        n, ptrs, _keep = self._batch(types, src, dst, weight)
+        check("sp_sssp_dynamic", lib().sp_sssp_dynamic(self.handle, n, *ptrs, int(source), _ptr(dist)))
+        self._refresh_size()
+        return bool(self.tune_get("sssp.last_incremental"))
 
     def export(self) -> dict:
         """The mirror's CSR as host arrays named like graph.hpp's fields."""

@@ -147,3 +147,50 @@ def test_update_edge_cases():
             with pytest.raises(_lib.SPError):
                 dg.update(t, s, d)
         assert dg.export()["edgeLen"].tolist() == [9, 3, 1]
+
+
+def test_sssp_dynamic_additions_resume_and_deletions_resolve():
+    # DynSSSP's batch: additions resume from the old distances (and relax far fewer
+    # edges than a fresh solve); a batch with deletions solves again; exact both ways
+    rng = np.random.default_rng(4)
+    g = G.rmat(14, 8, seed=9, directed=True)
+    g.edgeLen = G.hash_weights(g, 9, 1, 100, False)
+    edges = _edges(g.indexofNodes, g.edgeList, g.edgeLen)
+    source = int(G.pick_sources(g, 1, seed=4)[0])
+    with DeviceGraph.from_csr(g) as dg:
+        dist, _ = dg.sssp(source)
+        full = dg.tune_get("sssp.last_relaxed")
+        for step in range(6):
+            n = [1, 10, 200, 2000, 50, 400][step]
+            if step % 3 == 2:  # mixed batch: deletions force a new solve
+                t, s, d, w = _batch(rng, g.V, edges, n)
+            else:  # additions only
+                s = rng.integers(0, g.V, n).astype(np.int32)
+                d = rng.integers(0, g.V, n).astype(np.int32)
+                w = rng.integers(1, 100, n).astype(np.int32)
+                t = "a" * n
+            resumed = dg.sssp_dynamic(t, s, d, w, source, dist)
+            assert resumed == ("d" not in t)
+            edges = _apply(edges, t, s, d, w)
+            off, adj, ww = _csr(g.V, edges)
+            assert np.array_equal(dist, O.sssp(off, adj, ww, source)), step
+            if resumed and n <= 10:
+                assert dg.tune_get("sssp.last_relaxed") < full // 10
+    # device distances, and the errors
+    import torch
+
+    with DeviceGraph.from_csr(g) as dg:
+        dd = torch.empty(g.V, dtype=torch.int32, device="cuda")
+        dg.sssp(source, out=dd)
+        far = int(np.argmax(np.where(O.sssp(g.indexofNodes, g.edgeList, g.edgeLen, source) == 2**31 - 1, -1,
+                                     O.sssp(g.indexofNodes, g.edgeList, g.edgeLen, source))))
+        assert dg.sssp_dynamic("a", [source], [far], [1], source, dd)
+        e2 = _apply(_edges(g.indexofNodes, g.edgeList, g.edgeLen), "a", [source], [far], [1])
+        off, adj, ww = _csr(g.V, e2)
+        assert np.array_equal(dd.cpu().numpy(), O.sssp(off, adj, ww, source))
+        with pytest.raises(_lib.SPError):
+            dg.sssp_dynamic("a", [0], [g.V], [1], source, dd)
+    h = from_pairs(3, [[0, 1], [1, 2]], name="noweights")
+    with DeviceGraph.from_csr(h, with_weights=False) as dh:
+        with pytest.raises(_lib.SPError):
+            dh.sssp_dynamic("a", [0], [2], [1], 0, np.zeros(3, np.int32))
