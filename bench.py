@@ -645,6 +645,40 @@ def bench_update(steps, warmup, stream, cpu, nupd=1 << 20):
     ms = 1e3 * statistics.median(times)
     out = {"workload": f"update rmat20 ef16 directed seed7, {nupd} updates (half deletions of existing edges)",
            "value": nupd / (ms / 1e3) / 1e6, "unit": "M updates/s", "ms": ms, "E_before": g.E, "E_after": e_after}
+    # DynSSSP batches of 4096 added edges: resume from the old distances (sp_sssp_dynamic)
+    # against the same update followed by a full solve; both rebuild the CSR
+    import torch
+
+    source = int(G.pick_sources(g, 1, seed=20)[0])
+    nb = 4096
+    res_t, full_t, same = [], [], True
+    with DeviceGraph.from_csr(g, with_reverse=False) as da, DeviceGraph.from_csr(g, with_reverse=False) as db:
+        da.set_stream(stream)
+        db.set_stream(stream)
+        dist = torch.empty(g.V, dtype=torch.int32, device="cuda")
+        dfull = torch.empty(g.V, dtype=torch.int32, device="cuda")
+        da.sssp(source, out=dist)
+        for k in range(warmup + steps):
+            bs = rng.integers(0, g.V, nb).astype(np.int32)
+            bd = rng.integers(0, g.V, nb).astype(np.int32)
+            bw = rng.integers(1, 100, nb).astype(np.int32)
+            torch_sync()
+            t = time.perf_counter()
+            resumed = da.sssp_dynamic("a" * nb, bs, bd, bw, source, dist)
+            torch_sync()
+            t1 = time.perf_counter()
+            db.update("a" * nb, bs, bd, bw)
+            db.sssp(source, out=dfull)
+            torch_sync()
+            t2 = time.perf_counter()
+            if k >= warmup:
+                res_t.append(t1 - t)
+                full_t.append(t2 - t1)
+            same = same and resumed and bool(torch.equal(dist, dfull))
+    out["sssp_dynamic"] = {"workload": f"{nb} added edges per batch, source {source}",
+                           "resume_ms": 1e3 * statistics.median(res_t),
+                           "update_and_full_solve_ms": 1e3 * statistics.median(full_t),
+                           "same_distances": same}
     if cpu:
         # the same batch on the host: edge keys, deletions by search, additions merged
         t = time.perf_counter()
