@@ -26,7 +26,9 @@ baseline:
   ingest_rmat20    text edge list -> device mirror (sp_graph_load_text), directed R-MAT 20
                    ef16 with weights (M edge lines / s; not a GTEPS figure)
   update_rmat20    one batch of 2^20 edge updates (half deletions) applied to the device
-                   mirror of directed R-MAT 20 (M updates / s, host arrays to rebuilt CSR)
+                   mirror of directed R-MAT 20 (M updates / s, host arrays to rebuilt CSR);
+                   with batches of 4096 added edges, SSSP resumed from the old distances
+                   and PageRank started from the old ranks, each against a cold solve
   centrality       per-vertex triangle counts on the TC graph (m / t), and closeness on
                    the BC graph: unweighted over its 256 sources, weighted (U[1,100])
                    over 16 of them (sum of E_r / t)
@@ -679,6 +681,38 @@ def bench_update(steps, warmup, stream, cpu, nupd=1 << 20):
                            "resume_ms": 1e3 * statistics.median(res_t),
                            "update_and_full_solve_ms": 1e3 * statistics.median(full_t),
                            "same_distances": same}
+    # DynPR batches of 4096 added edges: PageRank from the previous ranks
+    # (sp_pagerank_dynamic) against the same update followed by PageRank from 1/V
+    warm_t, cold_t, warm_it, cold_it, l1 = [], [], [], [], 0.0
+    with DeviceGraph.from_csr(g, with_reverse=False) as da, DeviceGraph.from_csr(g, with_reverse=False) as db:
+        da.set_stream(stream)
+        db.set_stream(stream)
+        ranks = torch.empty(g.V, dtype=torch.float32, device="cuda")
+        cold = torch.empty(g.V, dtype=torch.float32, device="cuda")
+        da.pagerank(out=ranks)
+        for k in range(warmup + steps):
+            bs, bd = rng.integers(0, g.V, (2, nb)).astype(np.int32)
+            torch_sync()
+            t = time.perf_counter()
+            _, itw, _ = da.pagerank_dynamic("a" * nb, bs, bd, None, ranks)
+            torch_sync()
+            t1 = time.perf_counter()
+            db.update("a" * nb, bs, bd)
+            _, itc, _ = db.pagerank(out=cold)
+            torch_sync()
+            t2 = time.perf_counter()
+            if k >= warmup:
+                warm_t.append(t1 - t)
+                cold_t.append(t2 - t1)
+                warm_it.append(itw)
+                cold_it.append(itc)
+            l1 = max(l1, float((ranks.double() - cold.double()).abs().sum()))
+    out["pagerank_dynamic"] = {"workload": f"{nb} added edges per batch, beta 1e-6",
+                               "warm_ms": 1e3 * statistics.median(warm_t),
+                               "update_and_cold_ms": 1e3 * statistics.median(cold_t),
+                               "warm_iterations": statistics.median(warm_it),
+                               "cold_iterations": statistics.median(cold_it),
+                               "max_l1_warm_vs_cold": l1}
     if cpu:
         # the same batch on the host: edge keys, deletions by search, additions merged
         t = time.perf_counter()

@@ -276,6 +276,20 @@ int sp_sched_load(const float* params, const float* feat_mean, const float* feat
  * Tune key "sssp.last_incremental" (read only) says which path the last call took. */
 int sp_sssp_dynamic(sp_graph_h g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
                     const int32_t* weight, int32_t source, int32_t* dist);
+/* Replaces the generated Batch block of DynPR (DSL dynamicDSLCodes/dynamicBatchPR:
+ * OnDelete + propagateNodeFlags + updateCSRDel + Decremental, then the same for the
+ * additions): one batch of edge updates as in sp_graph_update (n = 0: none), then
+ * PageRank on the updated graph started from pageRank[V] (host or device; the ranks
+ * before the batch, from sp_pagerank or an earlier call) instead of 1/V, with
+ * sp_pagerank's iteration, stop test (L1 diff <= beta or maxIter) and outputs; the
+ * new ranks are written back to pageRank. Every vertex is iterated: graph.hpp's
+ * propagateNodeFlags (graph.hpp:444-462) marks the destination of every edge, so the
+ * DSL's modified-only sweeps cover all vertices with in-edges, and the others hold
+ * (1 - delta) / V in any PageRank output. The DSL's dynamic sweeps sum signed
+ * differences (dynamicBatchPR:56); this uses the L1 sum of the static form. */
+int sp_pagerank_dynamic(sp_graph_h g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
+                        const int32_t* weight, float beta, float delta, int32_t maxIter, float* pageRank,
+                        int32_t* iterations, double* final_diff);
 /* The SP_MLP_IN inputs the scheduler builds for SSSP on g with a candidate schedule
  * (delta multiple of the largest weight, CTAs per SM, cascade budget as for
  * "sssp.local"); weight NULL = edgeLen. */

@@ -218,18 +218,46 @@ namespace starplat_b200 {
 // deletions first, then additions, as a DSL Batch block runs updateCSRDel and then
 // updateCSRAdd. The host graph is not touched: call this beside the reference's own
 // update calls, or instead of them when only the device copy is used afterwards.
-template <class GraphT, class UpdateT>
-inline void apply_updates(GraphT& g, const std::vector<UpdateT>& batch, int k, int size) {
+// Entries k .. k + size - 1 of an update list as the C ABI's parallel arrays.
+struct UpdateArrays {
   std::vector<char> type;
   std::vector<int32_t> src, dst, w;
-  for (int i = k; i < k + size && i < (int)batch.size(); ++i) {
-    type.push_back(batch[i].type);
-    src.push_back(batch[i].source);
-    dst.push_back(batch[i].destination);
-    w.push_back(batch[i].weight);
+  template <class UpdateT>
+  UpdateArrays(const std::vector<UpdateT>& batch, int k, int size) {
+    for (int i = k; i < k + size && i < (int)batch.size(); ++i) {
+      type.push_back(batch[i].type);
+      src.push_back(batch[i].source);
+      dst.push_back(batch[i].destination);
+      w.push_back(batch[i].weight);
+    }
   }
-  check(sp_graph_update(mirror(g), (int64_t)type.size(), type.data(), src.data(), dst.data(), w.data()),
-        "apply_updates");
+  int64_t n() const { return (int64_t)type.size(); }
+};
+
+template <class GraphT, class UpdateT>
+inline void apply_updates(GraphT& g, const std::vector<UpdateT>& batch, int k, int size) {
+  UpdateArrays u(batch, k, size);
+  check(sp_graph_update(mirror(g), u.n(), u.type.data(), u.src.data(), u.dst.data(), u.w.data()), "apply_updates");
+}
+
+// DynSSSP's Batch block on the device copy: apply entries k .. k + size - 1, then bring
+// dist (the distances from src before the batch) up to date on the new graph.
+template <class GraphT, class UpdateT>
+inline void dynamic_sssp(GraphT& g, const std::vector<UpdateT>& batch, int k, int size, int* dist, int src) {
+  UpdateArrays u(batch, k, size);
+  check(sp_sssp_dynamic(mirror(g), u.n(), u.type.data(), u.src.data(), u.dst.data(), u.w.data(), src, dist),
+        "dynamic_sssp");
+}
+
+// DynPR's Batch block on the device copy: apply entries k .. k + size - 1, then run
+// PageRank on the new graph from pageRank (the ranks before the batch), in place.
+template <class GraphT, class UpdateT>
+inline void dynamic_pagerank(GraphT& g, const std::vector<UpdateT>& batch, int k, int size, float beta,
+                             float delta, int maxIter, float* pageRank) {
+  UpdateArrays u(batch, k, size);
+  check(sp_pagerank_dynamic(mirror(g), u.n(), u.type.data(), u.src.data(), u.dst.data(), u.w.data(), beta, delta,
+                            maxIter, pageRank, nullptr, nullptr),
+        "dynamic_pagerank");
 }
 }  // namespace starplat_b200
 

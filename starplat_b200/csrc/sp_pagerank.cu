@@ -596,6 +596,27 @@ __global__ void k_init(int V, const int32_t* __restrict__ odeg, float* __restric
   }
 }
 
+// Warm start (sp_pagerank_dynamic): the caller's ranks, staged in `init` in the
+// caller's vertex order, placed at their relabelled ids with their contributions.
+__global__ void k_init_from(int V, const int32_t* __restrict__ new_id, const int32_t* __restrict__ odeg,
+                            const float* __restrict__ init, float* __restrict__ pr, float* __restrict__ con,
+                            State* st) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    const int k = new_id[v];
+    const float x = init[v];
+    pr[k] = x;
+    const int od = odeg[k];
+    con[k] = od > 0 ? __fdiv_rn(x, (float)od) : 0.0f;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->iter = 0;
+    st->done = 0;
+    st->ticket = 0;
+    st->diff = 0;
+    st->extra = 0;
+  }
+}
+
 // ---- plain variant: the generated CUDA form (one thread per vertex, serial gather
 // of pr[u]/outdeg(u), atomic float diff; backend_cuda/dsl_cpp_generator.cpp:1682-1761)
 __global__ void k_plain_iter(int V, const int32_t* __restrict__ off, const int32_t* __restrict__ roff,
@@ -825,8 +846,9 @@ static int build_pr_plan(sp_graph* g, int hot, int order) {
   return SP_OK;
 }
 
+// init: starting ranks in the caller's vertex order (host or device), or null for 1/V.
 static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float* out, int32_t* iters,
-                    double* fdiff) {
+                    double* fdiff, const float* init = nullptr) {
   const int hot = std::max(0, std::min(g->pr_hot >= 0 ? g->pr_hot : pr::HOT_DEFAULT, pr::HOT_MAX));
   const int order = g->pr_order >= 0 ? g->pr_order : pr::ORDER_DEFAULT;
   SP_TRY(build_pr_plan(g, hot, order));
@@ -866,7 +888,13 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
   const PhaseFn ph1 = sh == 1 ? pr::k_phase<1, 1> : sh == 2 ? pr::k_phase<1, 2> : pr::k_phase<1, 0>;
   SP_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ph1, pr::THREADS, 0));
   const int grid = std::max(1, std::min(num_sms() * 32, num_sms() * std::max(1, per_sm)));
-  pr::k_init<<<num_sms() * 4, 256, 0, s>>>(V, p->od.p, p->prb[0].p, p->con[0].p, p->state.p);
+  if (init) {
+    SP_CHECK_CUDA(cudaMemcpyAsync(p->outbuf.p, init, sizeof(float) * V, cudaMemcpyDefault, s));
+    pr::k_init_from<<<num_sms() * 4, 256, 0, s>>>(V, p->new_id.p, p->od.p, p->outbuf.p, p->prb[0].p, p->con[0].p,
+                                                  p->state.p);
+  } else {
+    pr::k_init<<<num_sms() * 4, 256, 0, s>>>(V, p->od.p, p->prb[0].p, p->con[0].p, p->state.p);
+  }
   SP_CHECK_LAUNCH();
   if (!(p->exec && p->exec_iters == n_iter && p->exec_beta == beta && p->exec_delta == delta && p->exec_stream == s &&
         p->exec_sh == sh)) {
@@ -964,4 +992,19 @@ extern "C" int sp_pagerank(sp_graph_h g, float beta, float delta, int32_t maxIte
     return SP_ERR_INVALID;
   }
   return sp::pr_tuned(g, beta, delta, maxIter, pageRank, iterations, final_diff);
+}
+
+// DynPR's Batch block (dynamicDSLCodes/dynamicBatchPR:112-153): the batch is applied
+// (deletions, then additions), then PageRank runs from the caller's ranks instead of
+// 1/V, with the static form's iteration and stop test.
+extern "C" int sp_pagerank_dynamic(sp_graph_h g, int64_t n, const char* type, const int32_t* src,
+                                   const int32_t* dst, const int32_t* weight, float beta, float delta,
+                                   int32_t maxIter, float* pageRank, int32_t* iterations, double* final_diff) {
+  using namespace sp;
+  if (!g || !pageRank || n < 0 || (n > 0 && (!type || !src || !dst))) {
+    set_error("sp_pagerank_dynamic: invalid argument");
+    return SP_ERR_INVALID;
+  }
+  if (n > 0) SP_TRY(update_graph(g, n, type, src, dst, weight));
+  return pr_tuned(g, beta, delta, maxIter, pageRank, iterations, final_diff, pageRank);
 }

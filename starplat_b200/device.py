@@ -131,6 +131,22 @@ class DeviceGraph:
         self._refresh_size()
         return bool(self.tune_get("sssp.last_incremental"))
 
+    def pagerank_dynamic(self, types, src, dst, weight, pagerank, beta: float = 1e-6, delta: float = 0.85,
+                         max_iter: int = 100):
+        """DynPR's Batch block: apply the updates (none if types is empty), then run
+        PageRank on the new graph from `pagerank` (float32[V], host or device: the ranks
+        before the batch) instead of 1/V. The new ranks overwrite `pagerank`; returns
+        (pagerank, iterations, final L1 diff)."""
+        if str(pagerank.dtype) not in ("float32", "torch.float32") or len(pagerank) != self.V:
+            raise ValueError("pagerank must be float32 with one entry per vertex")
+        n, ptrs, _keep = self._batch(types, src, dst, weight)
+        it = ctypes.c_int32()
+        diff = ctypes.c_double()
+        check("sp_pagerank_dynamic", lib().sp_pagerank_dynamic(self.handle, n, *ptrs, beta, delta, max_iter,
+                                                               _ptr(pagerank), ctypes.byref(it), ctypes.byref(diff)))
+        self._refresh_size()
+        return pagerank, int(it.value), float(diff.value)
+
     def export(self) -> dict:
         """The mirror's CSR as host arrays named like graph.hpp's fields."""
         V, E = self.V, self.E

@@ -78,6 +78,20 @@ int main(int argc, char** argv) {
   batch.push_back({'a', V - 1, 0, 3});
   starplat_b200::apply_updates(g, batch, 0, (int)batch.size());
   std::printf("TCU %ld\n", Compute_TC(g));
+  // DynPR's batch on the updated copy: add 1 <-> V-2 and refresh the ranks from the
+  // previous ones
+  std::vector<Upd> batch2 = {{'a', 1, V - 2, 2}, {'a', V - 2, 1, 2}};
+  starplat_b200::dynamic_pagerank(g, batch2, 0, 2, 1e-9f, 0.85f, 100, pr.data());
+  std::printf("PRU");
+  for (int v = 0; v < V; ++v) std::printf(" %.9g", pr[v]);
+  std::printf("\n");
+  // a batch with a deletion solves again (on the copy's edgeLen); additions only resume
+  starplat_b200::dynamic_sssp(g, std::vector<Upd>{{'d', 0, 0, 0}}, 0, 1, dist.data(), atoi(argv[2]));
+  std::vector<Upd> batch3 = {{'a', 2, V - 3, 1}, {'a', V - 3, 2, 1}};
+  starplat_b200::dynamic_sssp(g, batch3, 0, 2, dist.data(), atoi(argv[2]));
+  std::printf("SSSPU");
+  for (int v = 0; v < V; ++v) std::printf(" %d", dist[v]);
+  std::printf("\n");
   starplat_b200::invalidate(g);
   return 0;
 }

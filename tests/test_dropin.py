@@ -68,20 +68,46 @@ def check_outputs(res, g, src):
     assert np.array_equal(cc, O.closeness(g.indexofNodes, g.edgeList, g.edgeLen, srcs))
     ccu = np.array(res["CCU"], np.float32)
     assert np.array_equal(ccu, O.closeness_unweighted(g.indexofNodes, g.edgeList, srcs))
-    # the update batch the driver applies (apply_updates), on the host edge set
+    # the update batches the driver applies (apply_updates, dynamic_pagerank, dynamic_sssp),
+    # replayed on the host edge set: deletions first, then additions with weights summed
     off, adj = g.indexofNodes, g.edgeList
-    edges = set(zip(np.repeat(np.arange(g.V), np.diff(off)).tolist(), adj.tolist()))
+    edges = {(int(a), int(b)): int(c) for a, b, c in zip(np.repeat(np.arange(g.V), np.diff(off)), adj, g.edgeLen)}
+    V = g.V
+    first = [("a", 0, V - 1, 3), ("a", V - 1, 0, 3)]
     if off[2] > off[1]:
         x = int(adj[off[1]])
-        edges -= {(1, x), (x, 1)}
-    edges |= {(0, g.V - 1), (g.V - 1, 0)}
-    keys = sorted(edges)
-    noff = np.zeros(g.V + 1, np.int64)
-    for a, _ in keys:
-        noff[a + 1] += 1
-    noff = np.cumsum(noff).astype(np.int32)
-    nadj = np.array([b for _, b in keys], np.int32)
+        first = [("d", 1, x, 0), ("d", x, 1, 0)] + first
+    edges = _apply(edges, first)
+    noff, nadj, _ = _csr(V, edges)
     assert int(res["TCU"][0]) == O.tc(noff, nadj)
+    edges = _apply(edges, [("a", 1, V - 2, 2), ("a", V - 2, 1, 2)])
+    noff, nadj, _ = _csr(V, edges)
+    rev = sorted((b, a) for a, b in edges)
+    roff = np.searchsorted(np.array([b for b, _ in rev], np.int64), np.arange(V + 1)).astype(np.int32)
+    radj = np.array([a for _, a in rev], np.int32)
+    ref, _, _ = O.pagerank(noff, roff, radj, 0.0, 0.85, 300)
+    assert np.abs(np.array(res["PRU"], np.float64) - ref).sum() < 1e-6
+    edges = _apply(edges, [("d", 0, 0, 0)])
+    edges = _apply(edges, [("a", 2, V - 3, 1), ("a", V - 3, 2, 1)])
+    noff, nadj, nw = _csr(V, edges)
+    assert np.array_equal(np.array(res["SSSPU"], np.int64), O.sssp(noff, nadj, nw, src))
+
+
+def _apply(edges, batch):
+    out = dict(edges)
+    for t, a, b, _ in batch:
+        if t == "d":
+            out.pop((a, b), None)
+    for t, a, b, c in batch:
+        if t == "a":
+            out[(a, b)] = out.get((a, b), 0) + c
+    return out
+
+
+def _csr(V, edges):
+    keys = sorted(edges)
+    off = np.searchsorted(np.array([a for a, _ in keys], np.int64), np.arange(V + 1)).astype(np.int32)
+    return off, np.array([b for _, b in keys], np.int32), np.array([edges[k] for k in keys], np.int32)
 
 
 def small_graph():
