@@ -221,7 +221,16 @@ def bench_tc(steps, warmup, stream, hbm, cpu):
     with DeviceGraph.from_csr(g, with_weights=False) as dg:
         dg.set_stream(stream)
         tuned(dg)
-        ms, res = timed(lambda: dg.tc(), steps, warmup, stream)
+        if REP is not None and REP.world > 1:
+            # anchor parts over the GPUs, one all-reduce of the int64 count (strong scaling)
+            from starplat_b200.distributed import tc_on_gpus
+
+            REP.barrier()
+            ms, res = timed(lambda: tc_on_gpus(dg, REP), steps, warmup, stream)
+            ms = REP.max(ms)
+            out["parallelism"] = f"anchor parts over {REP.world} GPUs, one all-reduce of the count"
+        else:
+            ms, res = timed(lambda: dg.tc(), steps, warmup, stream)
         msp, resp = timed(lambda: dg.tc(_lib.SP_TC_PLAIN), max(1, steps // 2), 1, stream)
     out.update({"triangles": res[0], "value": m / (ms / 1e3) / 1e9, "unit": "GTEPS", "ms": ms,
                 "plain": {"value": m / (msp / 1e3) / 1e9, "ms": msp, "triangles": resp[0]},
@@ -549,12 +558,23 @@ def bench_centrality(steps, warmup, stream, hbm, cpu):
     with DeviceGraph.from_csr(g, with_weights=False) as dg:
         dg.set_stream(stream)
         tuned(dg)
-        ms, res = timed(lambda: dg.clustering_coeff(), steps, warmup, stream)
+        lcc_sharded = REP is not None and REP.world > 1
+        if lcc_sharded:
+            # anchor parts over the GPUs, one all-reduce of the int32 counts (strong scaling)
+            from starplat_b200.distributed import clustering_coeff_on_gpus
+
+            REP.barrier()
+            ms, res = timed(lambda: clustering_coeff_on_gpus(dg, REP), steps, warmup, stream)
+            ms = REP.max(ms)
+        else:
+            ms, res = timed(lambda: dg.clustering_coeff(), steps, warmup, stream)
         msp, _ = timed(lambda: dg.clustering_coeff(variant=_lib.SP_TC_PLAIN), 1, 1, stream)
         cf = res[0]
     lcc = {"workload": "clustering_coeff rmat16 ef16 undirected seed1", "value": m / (ms / 1e3) / 1e9,
            "unit": "GTEPS", "ms": ms, "triangle_incidences": int(cf.astype(np.int64).sum()),
            "plain": {"value": m / (msp / 1e3) / 1e9, "ms": msp}}
+    if lcc_sharded:
+        lcc["parallelism"] = f"anchor parts over {REP.world} GPUs, one all-reduce of cf[V]"
     if cpu:
         from oracle import oracle as O
 

@@ -156,6 +156,19 @@ int sp_tc(sp_graph_h g, int64_t* triangle_count, int32_t variant);
  * generated CUDA form (one thread per vertex, binary search per pair). Exact. */
 int sp_clustering_coeff(sp_graph_h g, int32_t* cf, int32_t variant);
 
+/* ---- triangle counting over several GPUs --------------------------------------
+ * For one process per GPU, each holding the whole graph (the TC graphs are small:
+ * R-MAT 16 is 7 MB): part `part` of `nparts` (0 <= part < nparts) counts only the
+ * triangles anchored at every nparts-th vertex of the tuned kernels' heaviest-first
+ * anchor order, starting at position part. Every triangle falls in exactly one part,
+ * so the parts' counts sum to sp_tc's and their cf vectors to sp_clustering_coeff's
+ * (one all-reduce of an int64, or of int32[V]). Exact. nparts = 1 is the whole graph.
+ * The reference's multi-GPU generator splits every forall into contiguous vertex
+ * ranges (backend_multigpu/dsl_cpp_generator.cpp:4286-4288); the strided order keeps
+ * the parts' work even on skewed degrees. cf[V] is overwritten. */
+int sp_tc_part(sp_graph_h g, int32_t part, int32_t nparts, int64_t* triangle_count);
+int sp_clustering_coeff_part(sp_graph_h g, int32_t part, int32_t nparts, int32_t* cf);
+
 /* ---- degree and closeness centrality -----------------------------------------
  * Replaces generated `void Degree(graph& g, int* deg)` (DSL
  * staticDSLCodes/degree_centrality:1-6): deg[v] = out-degree of v. */

@@ -72,6 +72,8 @@ SIGNATURES = {
     "sp_tune_set": (ctypes.c_int, [vp, ctypes.c_char_p, i64]),
     "sp_tune_get": (ctypes.c_int, [vp, ctypes.c_char_p, P(i64)]),
     "sp_tc": (ctypes.c_int, [vp, P(i64), i32]),
+    "sp_tc_part": (ctypes.c_int, [vp, i32, i32, P(i64)]),
+    "sp_clustering_coeff_part": (ctypes.c_int, [vp, i32, i32, vp]),
     "sp_pagerank": (ctypes.c_int, [vp, f32, f32, i32, vp, P(i32), P(f64), i32]),
     "sp_sssp": (ctypes.c_int, [vp, vp, i32, vp, i64, i32, P(i32)]),
     "sp_bc": (ctypes.c_int, [vp, vp, i32, vp, i32]),

@@ -51,6 +51,7 @@ struct Lists {
   const int32_t* __restrict__ adj;
   int V;
   int directed;
+  int n;  // entries of the anchor order the counting loops visit (V, or a part's share)
 };
 
 // S and P ranges of anchor a (as index ranges into adj).
@@ -112,7 +113,7 @@ __global__ void __launch_bounds__(THREADS) k_tc_warp(Lists L, const int32_t* __r
   unsigned long long cnt = 0;
   // anchors in decreasing estimated work, dealt round-robin to the warps (no atomics)
   const int gwarp = (blockIdx.x * THREADS + threadIdx.x) >> 5, nwarps = (gridDim.x * THREADS) >> 5;
-  for (int ai = gwarp; ai < L.V; ai += nwarps) {
+  for (int ai = gwarp; ai < L.n; ai += nwarps) {
     const int a = order[ai];
     int sb, se, pb, pe;
     anchor_ranges(L, (int)a, sb, se, pb, pe);
@@ -214,7 +215,7 @@ __global__ void __launch_bounds__(BM_THREADS) k_tc_bitmap(Lists L, const int32_t
   __syncwarp();
   unsigned long long cnt = 0;
   const int gwarp = (blockIdx.x * BM_THREADS + threadIdx.x) >> 5, nwarps = (gridDim.x * BM_THREADS) >> 5;
-  for (int ai = gwarp; ai < L.V; ai += nwarps) {
+  for (int ai = gwarp; ai < L.n; ai += nwarps) {
     const int a = order[ai];
     int sb, se, pb, pe;
     anchor_ranges(L, a, sb, se, pb, pe);
@@ -277,7 +278,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_tc_bitmap_cta(Lists L, const 
     for (int i = tid; i < CNT_SLOTS / 2; i += NT) s_cnt[i] = 0u;
   __syncthreads();
   unsigned long long cnt = 0;
-  for (int ai = blockIdx.x; ai < L.V; ai += gridDim.x) {
+  for (int ai = blockIdx.x; ai < L.n; ai += gridDim.x) {
     const int a = order[ai];
     int sb, se, pb, pe;
     anchor_ranges(L, a, sb, se, pb, pe);
@@ -553,6 +554,14 @@ __global__ void k_orient_fill(const int32_t* __restrict__ off, const int32_t* __
   }
 }
 
+// Part `part` of `nparts`: every nparts-th anchor of the heaviest-first order, starting at
+// position part (n = ceil((V - part) / nparts) entries, so part + (n - 1) * nparts < V).
+__global__ void k_order_part(const int32_t* __restrict__ order, int n, int part, int nparts,
+                             int32_t* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = order[part + i * nparts];
+}
+
 }  // namespace tc
 
 struct TcPlan {
@@ -623,6 +632,7 @@ static int build_tc_plan(sp_graph* g) {
     L.directed = p->oriented ? 0 : 1;
     L.off = p->oriented ? p->ooff.p : g->off.p;
     L.adj = p->oriented ? p->oadj.p : g->adj.p;
+    L.n = g->V;
     dbuf<int32_t> key, id, skey;
     if ((st = key.alloc(g->V)) || (st = id.alloc(g->V)) || (st = skey.alloc(g->V)) || (st = p->order.alloc(g->V)))
       return fail(st);
@@ -641,6 +651,88 @@ static int build_tc_plan(sp_graph* g) {
   }
   p->built = true;
   g->tc = p;
+  return SP_OK;
+}
+
+static tc::Lists tc_lists(sp_graph* g, int n) {
+  TcPlan* p = g->tc;
+  tc::Lists L;
+  L.V = g->V;
+  L.directed = p->oriented ? 0 : 1;
+  L.off = p->oriented ? p->ooff.p : g->off.p;
+  L.adj = p->oriented ? p->oadj.p : g->adj.p;
+  L.n = n;
+  return L;
+}
+
+// Triangles anchored at order[0 .. n) (the whole count when order is the plan's and n = V).
+static int tc_count(sp_graph* g, const int32_t* order, int n, int64_t* triangle_count) {
+  TcPlan* p = g->tc;
+  cudaStream_t s = g->stream;
+  const tc::Lists L = tc_lists(g, n);
+  SP_CHECK_CUDA(cudaMemsetAsync(p->ctr.p, 0, sizeof(unsigned int) * 2, s));
+  SP_CHECK_CUDA(cudaMemsetAsync(p->total.p, 0, sizeof(unsigned long long), s));
+  const int cta_warps = g->tc_cta_warps >= 0 ? g->tc_cta_warps : tc::CTA_WARPS_DEFAULT;
+  if (g->V <= 65536 && cta_warps > 0) {
+    void (*k)(tc::Lists, const int32_t*, unsigned long long*, int*) =
+        cta_warps == 2   ? tc::k_tc_bitmap_cta<2, 24, false>
+        : cta_warps == 4 ? tc::k_tc_bitmap_cta<4, 16, false>
+        : cta_warps == 8 ? tc::k_tc_bitmap_cta<8, 8, false>
+                         : tc::k_tc_bitmap_cta<16, 4, false>;
+    int per_sm = 0;
+    SP_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, cta_warps * 32, 0));
+    k<<<num_sms() * std::max(1, per_sm), cta_warps * 32, 0, s>>>(L, order, p->total.p, nullptr);
+    SP_CHECK_LAUNCH();
+  } else if (g->V <= 65536) {
+    int per_sm = 0;
+    SP_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tc::k_tc_bitmap, tc::BM_THREADS, 0));
+    tc::k_tc_bitmap<<<num_sms() * std::max(1, per_sm), tc::BM_THREADS, 0, s>>>(L, order, p->total.p);
+    SP_CHECK_LAUNCH();
+  } else {
+    tc::k_tc_warp<false>
+        <<<num_sms() * 4, tc::THREADS, 0, s>>>(L, order, p->heavy.p, p->ctr.p + 1, p->total.p, nullptr);
+    SP_CHECK_LAUNCH();
+    tc::k_tc_heavy<false><<<num_sms() * 2, tc::THREADS, 0, s>>>(L, p->heavy.p, p->ctr.p + 1, p->total.p, nullptr);
+    SP_CHECK_LAUNCH();
+  }
+  unsigned long long h = 0;
+  SP_TRY(copy_out(&h, p->total.p, sizeof(h), s));
+  *triangle_count = (int64_t)h;
+  return SP_OK;
+}
+
+// Per-vertex triangle counts of the triangles anchored at order[0 .. n), added to counts.
+static int lcc_count(sp_graph* g, const int32_t* order, int n, int* counts) {
+  TcPlan* p = g->tc;
+  cudaStream_t s = g->stream;
+  const tc::Lists L = tc_lists(g, n);
+  SP_CHECK_CUDA(cudaMemsetAsync(p->ctr.p, 0, sizeof(unsigned int) * 2, s));
+  SP_CHECK_CUDA(cudaMemsetAsync(p->total.p, 0, sizeof(unsigned long long), s));
+  if (g->V <= 65536) {
+    int per_sm = 0;
+    SP_CHECK_CUDA(
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tc::k_tc_bitmap_cta<4, 8, true>, 4 * 32, 0));
+    tc::k_tc_bitmap_cta<4, 8, true><<<num_sms() * std::max(1, per_sm), 4 * 32, 0, s>>>(L, order, p->total.p, counts);
+    SP_CHECK_LAUNCH();
+  } else {
+    tc::k_tc_warp<true>
+        <<<num_sms() * 4, tc::THREADS, 0, s>>>(L, order, p->heavy.p, p->ctr.p + 1, p->total.p, counts);
+    SP_CHECK_LAUNCH();
+    tc::k_tc_heavy<true><<<num_sms() * 2, tc::THREADS, 0, s>>>(L, p->heavy.p, p->ctr.p + 1, p->total.p, counts);
+    SP_CHECK_LAUNCH();
+  }
+  return SP_OK;
+}
+
+// The anchors of part `part` of `nparts` (every nparts-th of the heaviest-first order) in
+// out, their number in n. The plan must be built.
+static int order_part(sp_graph* g, int part, int nparts, dbuf<int32_t>& out, int& n) {
+  n = part < g->V ? (g->V - part + nparts - 1) / nparts : 0;
+  SP_TRY(out.alloc(std::max(1, n)));
+  if (n > 0) {
+    tc::k_order_part<<<num_sms() * 4, 256, 0, g->stream>>>(g->tc->order.p, n, part, nparts, out.p);
+    SP_CHECK_LAUNCH();
+  }
   return SP_OK;
 }
 
@@ -670,42 +762,7 @@ extern "C" int sp_tc(sp_graph_h g, int64_t* triangle_count, int32_t variant) {
     return SP_ERR_INVALID;
   }
   SP_TRY(build_tc_plan(g));
-  TcPlan* p = g->tc;
-  cudaStream_t s = g->stream;
-  tc::Lists L;
-  L.V = g->V;
-  L.directed = p->oriented ? 0 : 1;
-  L.off = p->oriented ? p->ooff.p : g->off.p;
-  L.adj = p->oriented ? p->oadj.p : g->adj.p;
-  SP_CHECK_CUDA(cudaMemsetAsync(p->ctr.p, 0, sizeof(unsigned int) * 2, s));
-  SP_CHECK_CUDA(cudaMemsetAsync(p->total.p, 0, sizeof(unsigned long long), s));
-  const int cta_warps = g->tc_cta_warps >= 0 ? g->tc_cta_warps : tc::CTA_WARPS_DEFAULT;
-  if (g->V <= 65536 && cta_warps > 0) {
-    void (*k)(tc::Lists, const int32_t*, unsigned long long*, int*) =
-        cta_warps == 2   ? tc::k_tc_bitmap_cta<2, 24, false>
-        : cta_warps == 4 ? tc::k_tc_bitmap_cta<4, 16, false>
-        : cta_warps == 8 ? tc::k_tc_bitmap_cta<8, 8, false>
-                         : tc::k_tc_bitmap_cta<16, 4, false>;
-    int per_sm = 0;
-    SP_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, cta_warps * 32, 0));
-    k<<<num_sms() * std::max(1, per_sm), cta_warps * 32, 0, s>>>(L, p->order.p, p->total.p, nullptr);
-    SP_CHECK_LAUNCH();
-  } else if (g->V <= 65536) {
-    int per_sm = 0;
-    SP_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tc::k_tc_bitmap, tc::BM_THREADS, 0));
-    tc::k_tc_bitmap<<<num_sms() * std::max(1, per_sm), tc::BM_THREADS, 0, s>>>(L, p->order.p, p->total.p);
-    SP_CHECK_LAUNCH();
-  } else {
-    tc::k_tc_warp<false>
-        <<<num_sms() * 4, tc::THREADS, 0, s>>>(L, p->order.p, p->heavy.p, p->ctr.p + 1, p->total.p, nullptr);
-    SP_CHECK_LAUNCH();
-    tc::k_tc_heavy<false><<<num_sms() * 2, tc::THREADS, 0, s>>>(L, p->heavy.p, p->ctr.p + 1, p->total.p, nullptr);
-    SP_CHECK_LAUNCH();
-  }
-  unsigned long long h = 0;
-  SP_TRY(copy_out(&h, p->total.p, sizeof(h), s));
-  *triangle_count = (int64_t)h;
-  return SP_OK;
+  return tc_count(g, g->tc->order.p, g->V, triangle_count);
 }
 
 extern "C" int sp_clustering_coeff(sp_graph_h g, int32_t* cf, int32_t variant) {
@@ -731,27 +788,56 @@ extern "C" int sp_clustering_coeff(sp_graph_h g, int32_t* cf, int32_t variant) {
     return copy_out(cf, counts.p, sizeof(int32_t) * g->V, s);
   }
   SP_TRY(build_tc_plan(g));
-  TcPlan* p = g->tc;
-  tc::Lists L;
-  L.V = g->V;
-  L.directed = p->oriented ? 0 : 1;
-  L.off = p->oriented ? p->ooff.p : g->off.p;
-  L.adj = p->oriented ? p->oadj.p : g->adj.p;
-  SP_CHECK_CUDA(cudaMemsetAsync(p->ctr.p, 0, sizeof(unsigned int) * 2, s));
-  SP_CHECK_CUDA(cudaMemsetAsync(p->total.p, 0, sizeof(unsigned long long), s));
-  if (g->V <= 65536) {
-    int per_sm = 0;
-    SP_CHECK_CUDA(
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tc::k_tc_bitmap_cta<4, 8, true>, 4 * 32, 0));
-    tc::k_tc_bitmap_cta<4, 8, true>
-        <<<num_sms() * std::max(1, per_sm), 4 * 32, 0, s>>>(L, p->order.p, p->total.p, counts.p);
-    SP_CHECK_LAUNCH();
-  } else {
-    tc::k_tc_warp<true>
-        <<<num_sms() * 4, tc::THREADS, 0, s>>>(L, p->order.p, p->heavy.p, p->ctr.p + 1, p->total.p, counts.p);
-    SP_CHECK_LAUNCH();
-    tc::k_tc_heavy<true><<<num_sms() * 2, tc::THREADS, 0, s>>>(L, p->heavy.p, p->ctr.p + 1, p->total.p, counts.p);
-    SP_CHECK_LAUNCH();
+  SP_TRY(lcc_count(g, g->tc->order.p, g->V, counts.p));
+  return copy_out(cf, counts.p, sizeof(int32_t) * g->V, s);
+}
+
+// Anchor parts for several GPUs: part r of n counts the triangles anchored at every n-th
+// vertex of the heaviest-first anchor order, starting at position r, so the parts' work
+// is dealt like the single-GPU kernels deal it to warps and every triangle falls in
+// exactly one part. The parts' counts add up to sp_tc's, and their per-vertex vectors
+// to sp_clustering_coeff's. The reference's multi-GPU generator gives each device the
+// contiguous vertex range [i V / n, (i + 1) V / n) of every forall instead
+// (backend_multigpu/dsl_cpp_generator.cpp:4286-4288), which on R-MAT puts the hubs, and
+// most of the work, in the first range.
+static int check_part(const char* fn, sp_graph_h g, const void* out, int32_t part, int32_t nparts) {
+  if (!g || !out) {
+    sp::set_error("%s: NULL argument", fn);
+    return SP_ERR_INVALID;
   }
+  if (nparts < 1 || part < 0 || part >= nparts) {
+    sp::set_error("%s: part %d of %d", fn, part, nparts);
+    return SP_ERR_INVALID;
+  }
+  return SP_OK;
+}
+
+extern "C" int sp_tc_part(sp_graph_h g, int32_t part, int32_t nparts, int64_t* triangle_count) {
+  using namespace sp;
+  SP_TRY(check_part("sp_tc_part", g, triangle_count, part, nparts));
+  SP_TRY(build_tc_plan(g));
+  if (nparts == 1) return tc_count(g, g->tc->order.p, g->V, triangle_count);
+  dbuf<int32_t> mine;
+  int n = 0;
+  SP_TRY(order_part(g, part, nparts, mine, n));
+  return tc_count(g, mine.p, n, triangle_count);
+}
+
+extern "C" int sp_clustering_coeff_part(sp_graph_h g, int32_t part, int32_t nparts, int32_t* cf) {
+  using namespace sp;
+  SP_TRY(check_part("sp_clustering_coeff_part", g, cf, part, nparts));
+  cudaStream_t s = g->stream;
+  dbuf<int> counts;
+  SP_TRY(counts.alloc(g->V));
+  if (g->V) SP_CHECK_CUDA(cudaMemsetAsync(counts.p, 0, sizeof(int) * g->V, s));
+  SP_TRY(build_tc_plan(g));
+  dbuf<int32_t> mine;
+  int n = g->V;
+  const int32_t* order = g->tc->order.p;
+  if (nparts > 1) {
+    SP_TRY(order_part(g, part, nparts, mine, n));
+    order = mine.p;
+  }
+  SP_TRY(lcc_count(g, order, n, counts.p));
   return copy_out(cf, counts.p, sizeof(int32_t) * g->V, s);
 }

@@ -215,6 +215,13 @@ class DeviceGraph:
         check("sp_tc", lib().sp_tc(self.handle, ctypes.byref(out), variant))
         return int(out.value)
 
+    def tc_part(self, part: int, nparts: int) -> int:
+        """Triangles anchored in part `part` of `nparts` of the anchor order; the parts sum
+        to tc()."""
+        out = ctypes.c_int64()
+        check("sp_tc_part", lib().sp_tc_part(self.handle, int(part), int(nparts), ctypes.byref(out)))
+        return int(out.value)
+
     def pagerank(self, beta: float = 1e-6, delta: float = 0.85, max_iter: int = 100, out=None,
                  variant: int = _lib.SP_PR_TUNED):
         if out is None:
@@ -272,6 +279,15 @@ class DeviceGraph:
         if out is None:
             out = np.empty(self.V, np.int32)
         check("sp_clustering_coeff", lib().sp_clustering_coeff(self.handle, _ptr(out), variant))
+        return out
+
+    def clustering_coeff_part(self, part: int, nparts: int, out=None):
+        """Per-vertex counts of the triangles in part `part` of `nparts`; the parts' vectors
+        sum to clustering_coeff()."""
+        if out is None:
+            out = np.empty(self.V, np.int32)
+        check("sp_clustering_coeff_part",
+              lib().sp_clustering_coeff_part(self.handle, int(part), int(nparts), _ptr(out)))
         return out
 
     def degree(self, out=None):

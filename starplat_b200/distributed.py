@@ -7,6 +7,9 @@ vectors.
   * Closeness (sp_closeness / sp_closeness_unweighted): CC is nonzero only at the
     sources and each source's entry comes from one rank, so the sum of the slices is
     the whole, bit for bit.
+Triangle counting and the clustering coefficient split anchors instead: rank r counts
+the triangles of part r of the anchor order (sp_tc_part / sp_clustering_coeff_part), and
+one all-reduce adds an int64 count or an int32[V] vector, exactly.
 The process group comes from replicas.Replicas (NCCL on GPUs, gloo on the host).
 """
 from __future__ import annotations
@@ -54,3 +57,30 @@ def bc_on_gpus(dg, sources, rep: Optional[Replicas] = None) -> np.ndarray:
     """bc_sharded with this rank's DeviceGraph doing its slice."""
     rep = rep or Replicas()
     return bc_sharded(dg.V, sources, rep, lambda s: dg.bc(s))
+
+
+def tc_sharded(rep: Replicas, compute: Callable[[int, int], int]) -> int:
+    """Compute_TC over the ranks: compute(part, nparts) counts this rank's part (an exact
+    int64), and the parts are summed."""
+    mine = np.array([compute(rep.rank, rep.world)], np.int64)
+    return int(rep.all_reduce_sum(mine)[0])
+
+
+def lcc_sharded(V: int, rep: Replicas, compute: Callable[[int, int], np.ndarray]) -> np.ndarray:
+    """staticClusteringCoeff over the ranks: compute(part, nparts) gives this rank's
+    int32[V] counts, and the vectors are summed (int32, exact)."""
+    mine = np.ascontiguousarray(compute(rep.rank, rep.world), np.int32)
+    assert mine.shape == (V,)
+    return rep.all_reduce_sum(mine)
+
+
+def tc_on_gpus(dg, rep: Optional[Replicas] = None) -> int:
+    """tc_sharded with this rank's DeviceGraph (the whole graph on every GPU)."""
+    rep = rep or Replicas()
+    return tc_sharded(rep, dg.tc_part)
+
+
+def clustering_coeff_on_gpus(dg, rep: Optional[Replicas] = None) -> np.ndarray:
+    """lcc_sharded with this rank's DeviceGraph."""
+    rep = rep or Replicas()
+    return lcc_sharded(dg.V, rep, lambda r, n: dg.clustering_coeff_part(r, n))

@@ -114,3 +114,48 @@ def test_closeness_edge_cases():
         dg.closeness(np.array([1, 1], np.int32))
     with pytest.raises(_lib.SPError):
         dg.closeness_unweighted(np.array([5], np.int32))
+
+
+@pytest.mark.parametrize("nparts", [1, 2, 3, 8])
+def test_triangle_parts_sum_to_the_whole(nparts):
+    # sp_tc_part / sp_clustering_coeff_part: every triangle falls in exactly one part of
+    # the anchor order, so the parts add up to the oracle's figures exactly
+    for g in _lcc_graphs():
+        dg = device_graph(g)
+        tcs = [dg.tc_part(r, nparts) for r in range(nparts)]
+        cfs = [dg.clustering_coeff_part(r, nparts).astype(np.int64) for r in range(nparts)]
+        ref_tc = O.tc(g.indexofNodes, g.edgeList)
+        assert sum(tcs) == ref_tc, g.name
+        assert np.array_equal(np.sum(cfs, axis=0), O.lcc(g.indexofNodes, g.edgeList)), g.name
+    if nparts > 1:  # R-MAT 17: every part holds a share
+        g = G.rmat(17, 16, seed=4)
+        parts = [device_graph(g).tc_part(r, nparts) for r in range(nparts)]
+        assert all(0 < p < sum(parts) for p in parts)
+
+
+def test_triangle_parts_under_every_small_graph_kernel():
+    from starplat_b200.device import DeviceGraph
+
+    g = G.rmat(12, 16, seed=9)
+    ref_tc = O.tc(g.indexofNodes, g.edgeList)
+    ref_cf = O.lcc(g.indexofNodes, g.edgeList)
+    with DeviceGraph.from_csr(g) as dg:
+        for warps in (0, 2, 4, 8, 16):  # 0: the per-warp bitmap kernel
+            dg.tune_set("tc.cta_warps", warps)
+            assert sum(dg.tc_part(r, 3) for r in range(3)) == ref_tc, warps
+        cf = sum(dg.clustering_coeff_part(r, 3).astype(np.int64) for r in range(3))
+        assert np.array_equal(cf, ref_cf)
+
+
+def test_triangle_parts_beyond_the_vertex_count_and_bad_parts():
+    g = from_pairs(3, [[0, 1], [1, 2], [0, 2]], symmetrize=True)
+    dg = device_graph(g)
+    parts = [dg.tc_part(r, 5) for r in range(5)]
+    assert sum(parts) == 1 and parts[3] == 0 and parts[4] == 0
+    cf = sum(dg.clustering_coeff_part(r, 5).astype(np.int64) for r in range(5))
+    assert np.array_equal(cf, [1, 1, 1])
+    for part, nparts in ((2, 2), (0, 0), (-1, 3)):
+        with pytest.raises(_lib.SPError):
+            dg.tc_part(part, nparts)
+        with pytest.raises(_lib.SPError):
+            dg.clustering_coeff_part(part, nparts)

@@ -155,3 +155,61 @@ def test_closeness_split_over_ranks_is_exact(tmp_path):
     for r in range(world):
         assert np.array_equal(np.load(tmp_path / f"ccw{r}.npy"), rw)
         assert np.array_equal(np.load(tmp_path / f"ccu{r}.npy"), ru)
+
+
+def _lcc_part(off, adj, part, nparts):
+    """The Compute_TC loop over the outer vertices v = part, part + nparts, ..., each
+    triangle (v, u, w) adding one to all three (a small-graph restatement)."""
+    import numpy as np
+
+    cf = np.zeros(len(off) - 1, np.int32)
+    for v in range(part, len(off) - 1, nparts):
+        nb = adj[off[v]:off[v + 1]]
+        for u in nb[nb < v]:
+            nu = set(adj[off[u]:off[u + 1]].tolist())
+            for w in nb[nb > v]:
+                if int(w) in nu:
+                    cf[v] += 1
+                    cf[u] += 1
+                    cf[w] += 1
+    return cf
+
+
+def _tc_rank_main(rank, world, port, out_dir):
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port), "RANK": str(rank),
+                       "WORLD_SIZE": str(world), "LOCAL_RANK": str(rank)})
+    sys.path.insert(0, ROOT)
+    import numpy as np
+
+    from oracle import oracle as O
+    from starplat_b200 import generators as G
+    from starplat_b200.distributed import lcc_sharded, tc_sharded
+    from starplat_b200.replicas import Replicas
+
+    g = G.rmat(9, 8, seed=8)
+    rep = Replicas(backend="gloo", timeout_s=60)
+    tc = tc_sharded(rep, lambda r, n: O.tc_omp(g.indexofNodes, g.edgeList, 1, r, n))
+    cf = lcc_sharded(g.V, rep, lambda r, n: _lcc_part(g.indexofNodes, g.edgeList, r, n))
+    rep.close()
+    np.save(os.path.join(out_dir, f"tc{rank}.npy"), np.array([tc], np.int64))
+    np.save(os.path.join(out_dir, f"cf{rank}.npy"), cf)
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_triangle_parts_over_ranks_sum_to_the_whole(tmp_path, world):
+    # every rank counts one part of the outer vertices; one all-reduce of an int64 (and of
+    # the int32 per-vertex counts) gives every rank the whole graph's figures, exactly
+    import numpy as np
+
+    from oracle import oracle as O
+    from starplat_b200 import generators as G
+
+    mp.start_processes(_tc_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    g = G.rmat(9, 8, seed=8)
+    want_tc = O.tc(g.indexofNodes, g.edgeList)
+    want_cf = O.lcc(g.indexofNodes, g.edgeList)
+    assert want_tc > 0
+    for r in range(world):
+        assert int(np.load(tmp_path / f"tc{r}.npy")[0]) == want_tc
+        assert np.array_equal(np.load(tmp_path / f"cf{r}.npy"), want_cf)
