@@ -28,7 +28,8 @@ baseline:
   update_rmat20    one batch of 2^20 edge updates (half deletions) applied to the device
                    mirror of directed R-MAT 20 (M updates / s, host arrays to rebuilt CSR);
                    with batches of 4096 added edges, SSSP resumed from the old distances
-                   and PageRank started from the old ranks, each against a cold solve
+                   and PageRank started from the old ranks, each against a cold solve; on
+                   undirected R-MAT 20, triangles counted through the batch against a recount
   centrality       per-vertex triangle counts on the TC graph (m / t), and closeness on
                    the BC graph: unweighted over its 256 sources, weighted (U[1,100])
                    over 16 of them (sum of E_r / t)
@@ -727,6 +728,44 @@ def bench_update(steps, warmup, stream, cpu, nupd=1 << 20):
                 warm_it.append(itw)
                 cold_it.append(itc)
             l1 = max(l1, float((ranks.double() - cold.double()).abs().sum()))
+    # DynTC batches of 2048 undirected updates given in both directions (half deletions of
+    # edges of the original graph, half random additions) on undirected R-MAT 20:
+    # triangles through the batch only (sp_tc_dynamic) against the same update and a recount
+    gu = G.rmat(20, 16, seed=1)
+    src_u = np.repeat(np.arange(gu.V, dtype=np.int32), np.diff(gu.indexofNodes))
+    inc_t, upd_t, rec_t, same_tc = [], [], [], True
+    with DeviceGraph.from_csr(gu, with_weights=False) as da, DeviceGraph.from_csr(gu, with_weights=False) as db:
+        da.set_stream(stream)
+        db.set_stream(stream)
+        count = da.tc()
+        for k in range(warmup + steps):
+            pick = rng.choice(gu.E, nb // 4, replace=False)
+            xs, xd = src_u[pick], gu.edgeList[pick]
+            ys, yd = rng.integers(0, gu.V, (2, nb // 4)).astype(np.int32)
+            bs = np.concatenate([xs, xd, ys, yd]).astype(np.int32)
+            bd = np.concatenate([xd, xs, yd, ys]).astype(np.int32)
+            bt = "d" * (nb // 2) + "a" * (nb // 2)
+            torch_sync()
+            t = time.perf_counter()
+            count, inc = da.tc_dynamic(bt, bs, bd, None, count)
+            torch_sync()
+            t1 = time.perf_counter()
+            db.update(bt, bs, bd)
+            torch_sync()
+            t2 = time.perf_counter()
+            full = db.tc()
+            torch_sync()
+            t3 = time.perf_counter()
+            if k >= warmup:
+                inc_t.append(t1 - t)
+                upd_t.append(t2 - t1)
+                rec_t.append(t3 - t2)
+            same_tc = same_tc and inc and count == full
+    out["tc_dynamic"] = {"workload": f"tc rmat20 ef16 undirected seed1, {nb // 2} undirected updates per batch",
+                         "incremental_ms": 1e3 * statistics.median(inc_t),
+                         "update_ms": 1e3 * statistics.median(upd_t),
+                         "recount_ms": 1e3 * statistics.median(rec_t),
+                         "triangles": count, "same_count": same_tc}
     out["pagerank_dynamic"] = {"workload": f"{nb} added edges per batch, beta 1e-6",
                                "warm_ms": 1e3 * statistics.median(warm_t),
                                "update_and_cold_ms": 1e3 * statistics.median(cold_t),

@@ -119,6 +119,8 @@ int sp_graph_info(sp_graph_h g, int32_t* V, int64_t* E, int32_t* symmetric);
  *             out-edge of a vertex once per time the vertex was expanded).
  *   "tc.cta_warps"  TC on graphs of up to 65536 vertices: 0 = a bitmap per warp;
  *             2, 4, 8 or 16 = one bitmap per CTA of that many warps sharing each anchor.
+ *   "tc.last_incremental" (read only): 1 if the last sp_tc_dynamic counted only the
+ *             triangles through the batch's edges, 0 if it counted the graph again.
  *   "sssp.hub_deg", "sssp.hub_chunk"  SSSP: queued vertices with more out-edges than
  *             hub_deg are relaxed in hub_chunk-edge pieces shared by all warps
  *             (defaults 128 and 64).
@@ -300,6 +302,19 @@ int sp_sssp_dynamic(sp_graph_h g, int64_t n, const char* type, const int32_t* sr
  * DSL's modified-only sweeps cover all vertices with in-edges, and the others hold
  * (1 - delta) / V in any PageRank output. The DSL's dynamic sweeps sum signed
  * differences (dynamicBatchPR:56); this uses the L1 sum of the static form. */
+/* Replaces the generated Batch block of DynTC (DSL dynamicDSLCodes/dynamicBatchTCV2:
+ * OnDelete + Decremental + updateCSRDel + updateCSRAdd + OnAdd + Incremental): one batch
+ * of edge updates as in sp_graph_update, then the triangle count of the updated graph.
+ * triangle_count holds sp_tc's count before the batch on entry and after it on return.
+ * On a symmetric graph whose batch keeps it symmetric (deletions and additions each
+ * given in both directions), only triangles through the changed edges are counted:
+ * those of the old graph through edges it held and the batch deletes, and those of the
+ * new graph through edges it gains, each weighted 1 / (changed edges in it). Otherwise
+ * the updated graph is counted again. Exact either way; the DSL's form counts deletions
+ * of absent edges and repeated updates as changes, this does not. Tune key
+ * "tc.last_incremental" (read only) says which path the last call took. */
+int sp_tc_dynamic(sp_graph_h g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
+                  const int32_t* weight, int64_t* triangle_count);
 int sp_pagerank_dynamic(sp_graph_h g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
                         const int32_t* weight, float beta, float delta, int32_t maxIter, float* pageRank,
                         int32_t* iterations, double* final_diff);

@@ -249,6 +249,16 @@ inline void dynamic_sssp(GraphT& g, const std::vector<UpdateT>& batch, int k, in
         "dynamic_sssp");
 }
 
+// DynTC's Batch block on the device copy: apply entries k .. k + size - 1 and return the
+// triangle count of the new graph from `count`, the count before the batch.
+template <class GraphT, class UpdateT>
+inline long dynamic_tc(GraphT& g, const std::vector<UpdateT>& batch, int k, int size, long count) {
+  UpdateArrays u(batch, k, size);
+  int64_t c = count;
+  check(sp_tc_dynamic(mirror(g), u.n(), u.type.data(), u.src.data(), u.dst.data(), u.w.data(), &c), "dynamic_tc");
+  return (long)c;
+}
+
 // DynPR's Batch block on the device copy: apply entries k .. k + size - 1, then run
 // PageRank on the new graph from pageRank (the ranks before the batch), in place.
 template <class GraphT, class UpdateT>

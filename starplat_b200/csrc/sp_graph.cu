@@ -720,6 +720,10 @@ int sp_tune_get(sp_graph_h g, const char* key, int64_t* value) {
     *value = g->sssp_last_incremental;
     return SP_OK;
   }
+  if (!strcmp(key, "tc.last_incremental")) {
+    *value = g->tc_last_incremental;
+    return SP_OK;
+  }
   if (!strcmp(key, "sssp.hub_deg")) {
     *value = g->sssp_hub_deg > 0 ? g->sssp_hub_deg : sssp_hub_deg_default();
     return SP_OK;

@@ -32,6 +32,9 @@
 // (v, u, w) triples.
 #include <cub/cub.cuh>
 
+#include <algorithm>
+#include <vector>
+
 #include "sp_internal.cuh"
 
 namespace sp {
@@ -562,6 +565,96 @@ __global__ void k_order_part(const int32_t* __restrict__ order, int n, int part,
     out[i] = order[part + i * nparts];
 }
 
+// ---- batches of edge updates on a symmetric graph (DynTC's Batch block)
+__device__ __forceinline__ unsigned long long ukey(int a, int b) {
+  const unsigned lo = (unsigned)min(a, b), hi = (unsigned)max(a, b);
+  return ((unsigned long long)lo << 32) | hi;
+}
+
+__device__ __forceinline__ bool in_sorted(const unsigned long long* __restrict__ s, int n, unsigned long long k) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int m = (lo + hi) >> 1;
+    if (s[m] < k) lo = m + 1; else hi = m;
+  }
+  return lo < n && s[lo] == k;
+}
+
+// x in the sorted row adj[b .. e)
+__device__ __forceinline__ bool in_row(const int32_t* __restrict__ adj, int b, int e, int x) {
+  int lo = b, hi = e;
+  while (lo < hi) {
+    const int m = (lo + hi) >> 1;
+    if (adj[m] < x) lo = m + 1; else hi = m;
+  }
+  return lo < e && adj[lo] == x;
+}
+
+// Triangles of a symmetric CSR through the undirected edges keys[0 .. n) (lo << 32 | hi,
+// lo < hi, sorted, distinct), in two kernels. k_tri_work gives each edge (a, b) its work,
+// the length of the shorter of the two rows (0 when check is set and (a, b) is not an
+// edge; its two other edges, found in both rows, always are). After a scan of the work,
+// k_tri_flat gives every (edge, entry of its shorter row) pair one thread, which
+// searches the longer row for that third vertex c: an edge between two hubs is spread
+// over as many threads as its shorter row has entries. A triangle holding k of the edges
+// is found once from each of them, so cnt[k - 1] counts finds and the triangles number
+// cnt[0] + cnt[1] / 2 + cnt[2] / 3.
+__global__ void k_tri_work(const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
+                           const unsigned long long* __restrict__ keys, int n, int check,
+                           unsigned long long* __restrict__ work) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const unsigned long long k = keys[i];
+    const int a = (int)(k >> 32), b = (int)(k & 0xffffffffull);
+    const int ab = off[a], ae = off[a + 1], bb = off[b], be = off[b + 1];
+    work[i] = check && !in_row(adj, ab, ae, b) ? 0ull : (unsigned long long)min(ae - ab, be - bb);
+  }
+}
+
+__global__ void k_tri_flat(const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
+                           const unsigned long long* __restrict__ keys, int n,
+                           const unsigned long long* __restrict__ pre, unsigned long long total,
+                           unsigned long long* __restrict__ cnt) {
+  unsigned long long c1 = 0, c2 = 0, c3 = 0;
+  const unsigned long long step = (unsigned long long)gridDim.x * blockDim.x;
+  for (unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += step) {
+    // the edge i with pre[i] <= t < pre[i + 1] (pre[0] = 0, pre[n] = total)
+    int lo = 0, hi = n;
+    while (hi - lo > 1) {
+      const int m = (lo + hi) >> 1;
+      if (pre[m] <= t) lo = m; else hi = m;
+    }
+    const unsigned long long k = keys[lo];
+    const int a = (int)(k >> 32), b = (int)(k & 0xffffffffull);
+    const int ab = off[a], ae = off[a + 1], bb = off[b], be = off[b + 1];
+    const bool a_short = ae - ab <= be - bb;
+    const int c = adj[(a_short ? ab : bb) + (int)(t - pre[lo])];
+    if (c == a || c == b || !in_row(adj, a_short ? bb : ab, a_short ? be : ae, c)) continue;
+    const int m = 1 + (int)in_sorted(keys, n, ukey(a, c)) + (int)in_sorted(keys, n, ukey(b, c));
+    c1 += m == 1;
+    c2 += m == 2;
+    c3 += m == 3;
+  }
+  c1 = warp_sum(c1);
+  c2 = warp_sum(c2);
+  c3 = warp_sum(c3);
+  if ((threadIdx.x & 31) == 0 && (c1 | c2 | c3)) {
+    atomicAdd(&cnt[0], c1);
+    atomicAdd(&cnt[1], c2);
+    atomicAdd(&cnt[2], c3);
+  }
+}
+
+// Additions that add an edge: absent from the CSR before the batch, or deleted by it.
+__global__ void k_new_edges(const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
+                            const unsigned long long* __restrict__ add, int na,
+                            const unsigned long long* __restrict__ del, int nd, unsigned char* __restrict__ flag) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < na; i += gridDim.x * blockDim.x) {
+    const unsigned long long k = add[i];
+    const int a = (int)(k >> 32), b = (int)(k & 0xffffffffull);
+    flag[i] = !in_row(adj, off[a], off[a + 1], b) || in_sorted(del, nd, k);
+  }
+}
+
 }  // namespace tc
 
 struct TcPlan {
@@ -840,4 +933,131 @@ extern "C" int sp_clustering_coeff_part(sp_graph_h g, int32_t part, int32_t npar
   }
   SP_TRY(lcc_count(g, order, n, counts.p));
   return copy_out(cf, counts.p, sizeof(int32_t) * g->V, s);
+}
+
+namespace sp {
+
+// Triangles of g's CSR through the sorted undirected keys d_keys[0 .. n).
+static int tri_through(sp_graph* g, const unsigned long long* d_keys, int n, int check, int64_t* out) {
+  *out = 0;
+  if (n == 0) return SP_OK;
+  cudaStream_t s = g->stream;
+  dbuf<unsigned long long> cnt, work, pre;
+  dbuf<unsigned char> temp;
+  SP_TRY(cnt.alloc(3));
+  SP_TRY(work.alloc((size_t)n + 1));
+  SP_TRY(pre.alloc((size_t)n + 1));
+  SP_CHECK_CUDA(cudaMemsetAsync(cnt.p, 0, 3 * sizeof(unsigned long long), s));
+  SP_CHECK_CUDA(cudaMemsetAsync(work.p + n, 0, sizeof(unsigned long long), s));
+  tc::k_tri_work<<<std::min(num_sms() * 4, (n + 255) / 256), 256, 0, s>>>(g->off.p, g->adj.p, d_keys, n, check,
+                                                                          work.p);
+  SP_CHECK_LAUNCH();
+  size_t tb = 0;
+  SP_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, work.p, pre.p, n + 1, s));
+  SP_TRY(temp.alloc(std::max<size_t>(1, tb)));
+  SP_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, tb, work.p, pre.p, n + 1, s));
+  g_launches++;
+  unsigned long long total = 0;
+  SP_TRY(copy_out(&total, pre.p + n, sizeof(total), s));
+  if (total > 0) {
+    const unsigned long long want = (total + 255) / 256;
+    const int blocks = (int)std::min<unsigned long long>(want, (unsigned long long)num_sms() * 16);
+    tc::k_tri_flat<<<blocks, 256, 0, s>>>(g->off.p, g->adj.p, d_keys, n, pre.p, total, cnt.p);
+    SP_CHECK_LAUNCH();
+  }
+  unsigned long long h[3];
+  SP_TRY(copy_out(h, cnt.p, sizeof(h), s));
+  if (h[1] % 2 || h[2] % 3) {
+    set_error("sp_tc_dynamic: %llu / %llu finds of triangles with two / three batch edges", h[1], h[2]);
+    return SP_ERR_UNSUPPORTED;
+  }
+  *out = (int64_t)(h[0] + h[1] / 2 + h[2] / 3);
+  return SP_OK;
+}
+
+// Sorted distinct directed keys of one update type, and whether that set is symmetric.
+static bool symmetric_set(std::vector<unsigned long long>& k) {
+  std::sort(k.begin(), k.end());
+  k.erase(std::unique(k.begin(), k.end()), k.end());
+  std::vector<unsigned long long> t(k.size());
+  for (size_t i = 0; i < k.size(); ++i) t[i] = (k[i] << 32) | (k[i] >> 32);
+  std::sort(t.begin(), t.end());
+  return t == k;
+}
+
+}  // namespace sp
+
+// DynTC's Batch block (dynamicDSLCodes/dynamicBatchTCV2:142-199): the batch is applied
+// (deletions, then additions) and the count updated. On a symmetric graph with a batch
+// that keeps it symmetric, only triangles through changed edges are counted:
+//   T(new) = T(old) - [triangles of the old graph through deleted edges]
+//                   + [triangles of the new graph through added edges],
+// where a deleted edge is one the old graph holds and an added edge one the graph
+// lacks after the deletions; a triangle through k changed edges is weighted 1/k, as
+// the DSL's count1/2 + count2/4 + count3/6 does for updates given in both directions.
+// Otherwise the batch is applied and the whole graph counted again.
+extern "C" int sp_tc_dynamic(sp_graph_h g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
+                             const int32_t* weight, int64_t* triangle_count) {
+  using namespace sp;
+  if (!g || !triangle_count || n < 0 || (n > 0 && (!type || !src || !dst))) {
+    set_error("sp_tc_dynamic: invalid argument");
+    return SP_ERR_INVALID;
+  }
+  g->tc_last_incremental = 0;
+  if (n == 0) {  // nothing changed: the caller's count stands
+    g->tc_last_incremental = 1;
+    return SP_OK;
+  }
+  std::vector<unsigned long long> dd, ad, du, au;  // directed keys; undirected keys (lo < hi)
+  for (int64_t i = 0; i < n; ++i) {
+    const int32_t a = src[i], b = dst[i];
+    if ((type[i] != 'a' && type[i] != 'd') || a < 0 || a >= g->V || b < 0 || b >= g->V)
+      return update_graph(g, n, type, src, dst, weight);  // reports the bad update, changes nothing
+    const unsigned long long k = ((unsigned long long)(uint32_t)a << 32) | (uint32_t)b;
+    const unsigned long long u = ((unsigned long long)(uint32_t)std::min(a, b) << 32) | (uint32_t)std::max(a, b);
+    (type[i] == 'd' ? dd : ad).push_back(k);
+    if (a != b) (type[i] == 'd' ? du : au).push_back(u);
+  }
+  SP_TRY(ensure_symmetry(g));
+  const bool incremental = g->symmetric == 1 && symmetric_set(dd) && symmetric_set(ad);
+  if (!incremental) {
+    SP_TRY(update_graph(g, n, type, src, dst, weight));
+    SP_TRY(build_tc_plan(g));
+    return tc_count(g, g->tc->order.p, g->V, triangle_count);
+  }
+  for (auto* v : {&du, &au}) {
+    std::sort(v->begin(), v->end());
+    v->erase(std::unique(v->begin(), v->end()), v->end());
+  }
+  const int nd = (int)du.size(), na = (int)au.size();
+  cudaStream_t s = g->stream;
+  dbuf<unsigned long long> d_del, d_add, d_new;
+  dbuf<unsigned char> flag, temp;
+  dbuf<int> d_nnew;
+  SP_TRY(d_del.alloc(std::max(1, nd)));
+  SP_TRY(d_add.alloc(std::max(1, na)));
+  SP_TRY(d_new.alloc(std::max(1, na)));
+  SP_TRY(flag.alloc(std::max(1, na)));
+  SP_TRY(d_nnew.alloc(1));
+  if (nd) SP_CHECK_CUDA(cudaMemcpyAsync(d_del.p, du.data(), 8 * (size_t)nd, cudaMemcpyHostToDevice, s));
+  if (na) SP_CHECK_CUDA(cudaMemcpyAsync(d_add.p, au.data(), 8 * (size_t)na, cudaMemcpyHostToDevice, s));
+  int64_t lost = 0, gained = 0;
+  SP_TRY(tri_through(g, d_del.p, nd, 1, &lost));
+  int nnew = 0;
+  if (na) {
+    tc::k_new_edges<<<num_sms() * 4, 256, 0, s>>>(g->off.p, g->adj.p, d_add.p, na, d_del.p, nd, flag.p);
+    SP_CHECK_LAUNCH();
+    size_t tb = 0;
+    SP_CHECK_CUDA(cub::DeviceSelect::Flagged(nullptr, tb, d_add.p, flag.p, d_new.p, d_nnew.p, na, s));
+    SP_TRY(temp.alloc(std::max<size_t>(1, tb)));
+    SP_CHECK_CUDA(cub::DeviceSelect::Flagged(temp.p, tb, d_add.p, flag.p, d_new.p, d_nnew.p, na, s));
+    g_launches++;
+    SP_TRY(copy_out(&nnew, d_nnew.p, sizeof(int), s));
+  }
+  SP_TRY(update_graph(g, n, type, src, dst, weight));
+  g->symmetric = 1;  // a symmetric graph minus and plus symmetric edge sets
+  SP_TRY(tri_through(g, d_new.p, nnew, 0, &gained));
+  *triangle_count = *triangle_count - lost + gained;
+  g->tc_last_incremental = 1;
+  return SP_OK;
 }

@@ -131,6 +131,16 @@ class DeviceGraph:
         self._refresh_size()
         return bool(self.tune_get("sssp.last_incremental"))
 
+    def tc_dynamic(self, types, src, dst, weight, count: int):
+        """DynTC's Batch block: apply the updates, then bring `count` (the graph's
+        triangle count before the batch) up to date. Returns (new count, True when only
+        the triangles through the batch's edges were counted)."""
+        n, ptrs, _keep = self._batch(types, src, dst, weight)
+        c = ctypes.c_int64(int(count))
+        check("sp_tc_dynamic", lib().sp_tc_dynamic(self.handle, n, *ptrs, ctypes.byref(c)))
+        self._refresh_size()
+        return int(c.value), bool(self.tune_get("tc.last_incremental"))
+
     def pagerank_dynamic(self, types, src, dst, weight, pagerank, beta: float = 1e-6, delta: float = 0.85,
                          max_iter: int = 100):
         """DynPR's Batch block: apply the updates (none if types is empty), then run

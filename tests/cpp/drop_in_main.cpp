@@ -78,6 +78,9 @@ int main(int argc, char** argv) {
   batch.push_back({'a', V - 1, 0, 3});
   starplat_b200::apply_updates(g, batch, 0, (int)batch.size());
   std::printf("TCU %ld\n", Compute_TC(g));
+  // DynTC's batch: drop 0 <-> V-1 again (incremental: the graph and batch are symmetric)
+  std::vector<Upd> batch1 = {{'d', 0, V - 1, 0}, {'d', V - 1, 0, 0}};
+  std::printf("TCD %ld\n", starplat_b200::dynamic_tc(g, batch1, 0, 2, Compute_TC(g)));
   // DynPR's batch on the updated copy: add 1 <-> V-2 and refresh the ranks from the
   // previous ones
   std::vector<Upd> batch2 = {{'a', 1, V - 2, 2}, {'a', V - 2, 1, 2}};

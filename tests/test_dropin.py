@@ -80,6 +80,9 @@ def check_outputs(res, g, src):
     edges = _apply(edges, first)
     noff, nadj, _ = _csr(V, edges)
     assert int(res["TCU"][0]) == O.tc(noff, nadj)
+    edges = _apply(edges, [("d", 0, V - 1, 0), ("d", V - 1, 0, 0)])
+    noff, nadj, _ = _csr(V, edges)
+    assert int(res["TCD"][0]) == O.tc(noff, nadj)
     edges = _apply(edges, [("a", 1, V - 2, 2), ("a", V - 2, 1, 2)])
     noff, nadj, _ = _csr(V, edges)
     rev = sorted((b, a) for a, b in edges)

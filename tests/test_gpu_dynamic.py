@@ -259,3 +259,64 @@ def test_pagerank_dynamic_rejects_bad_arguments():
             dg.pagerank_dynamic("x", [0], [1], None, np.zeros(g.V, np.float32))
         with pytest.raises(_lib.SPError):
             dg.pagerank_dynamic("a", [0], [g.V], None, np.zeros(g.V, np.float32))
+
+
+def _sym_batch(rng, V, edges, n):
+    """n / 2 undirected updates, each given in both directions (kinds as in _batch)."""
+    t, s, d, w = _batch(rng, V, edges, n // 2)
+    return (t + t, np.concatenate([s, d]), np.concatenate([d, s]), np.concatenate([w, w]))
+
+
+def test_tc_dynamic_counts_only_the_batch_on_symmetric_graphs():
+    rng = np.random.default_rng(21)
+    g = G.rmat(12, 16, seed=5)  # undirected
+    g.edgeLen = G.hash_weights(g, 5, 1, 50, True)
+    edges = _edges(g.indexofNodes, g.edgeList, g.edgeLen)
+    with DeviceGraph.from_csr(g) as dg:
+        count = dg.tc()
+        for n in (2, 60, 800, 6000):
+            t, s, d, w = _sym_batch(rng, g.V, edges, n)
+            count, incremental = dg.tc_dynamic(t, s, d, w, count)
+            edges = _apply(edges, t, s, d, w)
+            off, adj, _ = _csr(g.V, edges)
+            assert incremental
+            assert count == O.tc(off, adj) == dg.tc()
+
+
+def test_tc_dynamic_edge_deleted_and_added_in_one_batch():
+    # deletions apply first: the edge is gone, then back, and so are its triangles
+    g = G.rmat(10, 16, seed=3)
+    with DeviceGraph.from_csr(g) as dg:
+        before = dg.tc()
+        a = int(np.argmax(np.diff(g.indexofNodes)))
+        b = int(g.edgeList[g.indexofNodes[a]])
+        count, incremental = dg.tc_dynamic("ddaa", [a, b, a, b], [b, a, b, a], None, before)
+        assert incremental and count == before == dg.tc()
+        # an added edge that is already there changes nothing either
+        count, incremental = dg.tc_dynamic("aa", [a, b], [b, a], None, count)
+        assert incremental and count == before
+
+
+def test_tc_dynamic_counts_again_otherwise():
+    rng = np.random.default_rng(22)
+    for g, sym in ((G.rmat(11, 8, seed=2), False), (G.rmat(11, 8, seed=2, directed=True), True)):
+        g.edgeLen = G.hash_weights(g, 2, 1, 50, g.is_symmetric())
+        edges = _edges(g.indexofNodes, g.edgeList, g.edgeLen)
+        with DeviceGraph.from_csr(g) as dg:
+            count = dg.tc()
+            t, s, d, w = (_sym_batch if sym else _batch)(rng, g.V, edges, 300)
+            count, incremental = dg.tc_dynamic(t, s, d, w, count)
+            edges = _apply(edges, t, s, d, w)
+            off, adj, _ = _csr(g.V, edges)
+            assert not incremental  # an unsymmetric batch, or a directed graph
+            assert count == O.tc(off, adj)
+
+
+def test_tc_dynamic_rejects_a_bad_batch_unchanged():
+    g = G.rmat(9, 8, seed=4)
+    with DeviceGraph.from_csr(g) as dg:
+        before, E = dg.tc(), dg.E
+        for t, s, d in (("ax", [0, 1], [1, 0]), ("aa", [0, g.V], [g.V, 0])):
+            with pytest.raises(_lib.SPError):
+                dg.tc_dynamic(t, s, d, None, before)
+        assert dg.E == E and dg.tc() == before
