@@ -315,6 +315,21 @@ int sp_sssp_dynamic(sp_graph_h g, int64_t n, const char* type, const int32_t* sr
  * "tc.last_incremental" (read only) says which path the last call took. */
 int sp_tc_dynamic(sp_graph_h g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
                   const int32_t* weight, int64_t* triangle_count);
+/* Replaces the generated Batch block of DynCF (DSL dynamicDSLCodes/dynamicBatchClustering):
+ * one batch of edge updates as in sp_graph_update, then cf[V] (host or device;
+ * sp_clustering_coeff's counts before the batch on entry) brought up to date. On a
+ * symmetric graph with a batch that keeps it symmetric, only the triangles through the
+ * changed edges are found (as in sp_tc_dynamic), each adding -1 (deleted) or +1 (added)
+ * to its three vertices once; otherwise the updated graph is counted again. Exact.
+ * "tc.last_incremental" says which path the call took. */
+int sp_clustering_coeff_dynamic(sp_graph_h g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
+                                const int32_t* weight, int32_t* cf);
+/* Replaces the generated Batch block of DynDegree (DSL dynamicDSLCodes/dynamicBatchDeg):
+ * one batch of edge updates, then deg[V] = the out-degrees of the updated graph (the
+ * DSL's per-update +1 / -1 also counts deletions of absent edges and additions of
+ * present ones; these are the exact degrees). */
+int sp_degree_dynamic(sp_graph_h g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
+                      const int32_t* weight, int32_t* deg);
 int sp_pagerank_dynamic(sp_graph_h g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
                         const int32_t* weight, float beta, float delta, int32_t maxIter, float* pageRank,
                         int32_t* iterations, double* final_diff);

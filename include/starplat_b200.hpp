@@ -259,6 +259,22 @@ inline long dynamic_tc(GraphT& g, const std::vector<UpdateT>& batch, int k, int 
   return (long)c;
 }
 
+// DynCF's and DynDegree's Batch blocks on the device copy: apply entries k .. k + size - 1,
+// then bring cf (the counts before the batch) up to date / write the new out-degrees.
+template <class GraphT, class UpdateT>
+inline void dynamic_clustering_coeff(GraphT& g, const std::vector<UpdateT>& batch, int k, int size, int* cf) {
+  UpdateArrays u(batch, k, size);
+  check(sp_clustering_coeff_dynamic(mirror(g), u.n(), u.type.data(), u.src.data(), u.dst.data(), u.w.data(), cf),
+        "dynamic_clustering_coeff");
+}
+
+template <class GraphT, class UpdateT>
+inline void dynamic_degree(GraphT& g, const std::vector<UpdateT>& batch, int k, int size, int* deg) {
+  UpdateArrays u(batch, k, size);
+  check(sp_degree_dynamic(mirror(g), u.n(), u.type.data(), u.src.data(), u.dst.data(), u.w.data(), deg),
+        "dynamic_degree");
+}
+
 // DynPR's Batch block on the device copy: apply entries k .. k + size - 1, then run
 // PageRank on the new graph from pageRank (the ranks before the batch), in place.
 template <class GraphT, class UpdateT>

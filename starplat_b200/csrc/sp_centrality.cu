@@ -94,6 +94,21 @@ extern "C" int sp_degree_centrality(sp_graph_h g, int32_t* deg) {
   return copy_out(deg, d.p, sizeof(int32_t) * g->V, g->stream);
 }
 
+// DynDegree's Batch block (dynamicDSLCodes/dynamicBatchDeg:26-37): the batch, then the
+// out-degrees of the updated graph. The DSL adjusts deg[src] by one per update, which
+// also counts deletions of absent edges and additions of present ones; the degrees here
+// are read from the updated rows, so they are exact.
+extern "C" int sp_degree_dynamic(sp_graph_h g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
+                                 const int32_t* weight, int32_t* deg) {
+  using namespace sp;
+  if (!g || !deg || n < 0 || (n > 0 && (!type || !src || !dst))) {
+    set_error("sp_degree_dynamic: invalid argument");
+    return SP_ERR_INVALID;
+  }
+  if (n > 0) SP_TRY(update_graph(g, n, type, src, dst, weight));
+  return sp_degree_centrality(g, deg);
+}
+
 extern "C" int sp_closeness(sp_graph_h g, const int32_t* weight, const int32_t* sources, int32_t nsrc, float* CC) {
   using namespace sp;
   if (!g || !sources || nsrc <= 0 || !CC) {

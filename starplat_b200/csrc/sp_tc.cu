@@ -610,10 +610,12 @@ __global__ void k_tri_work(const int32_t* __restrict__ off, const int32_t* __res
   }
 }
 
+// delta (optional): each triangle adds `sign` to its three vertices once, from the find
+// whose edge (a, b) has the smallest key among the triangle's edges in keys.
 __global__ void k_tri_flat(const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
                            const unsigned long long* __restrict__ keys, int n,
                            const unsigned long long* __restrict__ pre, unsigned long long total,
-                           unsigned long long* __restrict__ cnt) {
+                           unsigned long long* __restrict__ cnt, int* __restrict__ delta, int sign) {
   unsigned long long c1 = 0, c2 = 0, c3 = 0;
   const unsigned long long step = (unsigned long long)gridDim.x * blockDim.x;
   for (unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += step) {
@@ -629,10 +631,17 @@ __global__ void k_tri_flat(const int32_t* __restrict__ off, const int32_t* __res
     const bool a_short = ae - ab <= be - bb;
     const int c = adj[(a_short ? ab : bb) + (int)(t - pre[lo])];
     if (c == a || c == b || !in_row(adj, a_short ? bb : ab, a_short ? be : ae, c)) continue;
-    const int m = 1 + (int)in_sorted(keys, n, ukey(a, c)) + (int)in_sorted(keys, n, ukey(b, c));
+    const unsigned long long kac = ukey(a, c), kbc = ukey(b, c);
+    const bool sac = in_sorted(keys, n, kac), sbc = in_sorted(keys, n, kbc);
+    const int m = 1 + (int)sac + (int)sbc;
     c1 += m == 1;
     c2 += m == 2;
     c3 += m == 3;
+    if (delta && (!sac || k < kac) && (!sbc || k < kbc)) {
+      atomicAdd(&delta[a], sign);
+      atomicAdd(&delta[b], sign);
+      atomicAdd(&delta[c], sign);
+    }
   }
   c1 = warp_sum(c1);
   c2 = warp_sum(c2);
@@ -642,6 +651,10 @@ __global__ void k_tri_flat(const int32_t* __restrict__ off, const int32_t* __res
     atomicAdd(&cnt[1], c2);
     atomicAdd(&cnt[2], c3);
   }
+}
+
+__global__ void k_add_i32(int n, const int* __restrict__ d, int32_t* __restrict__ x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] += d[i];
 }
 
 // Additions that add an edge: absent from the CSR before the batch, or deleted by it.
@@ -938,7 +951,9 @@ extern "C" int sp_clustering_coeff_part(sp_graph_h g, int32_t part, int32_t npar
 namespace sp {
 
 // Triangles of g's CSR through the sorted undirected keys d_keys[0 .. n).
-static int tri_through(sp_graph* g, const unsigned long long* d_keys, int n, int check, int64_t* out) {
+// delta (optional, int32[V] on the device): each triangle adds sign to its vertices.
+static int tri_through(sp_graph* g, const unsigned long long* d_keys, int n, int check, int64_t* out,
+                       int* delta = nullptr, int sign = 0) {
   *out = 0;
   if (n == 0) return SP_OK;
   cudaStream_t s = g->stream;
@@ -962,7 +977,7 @@ static int tri_through(sp_graph* g, const unsigned long long* d_keys, int n, int
   if (total > 0) {
     const unsigned long long want = (total + 255) / 256;
     const int blocks = (int)std::min<unsigned long long>(want, (unsigned long long)num_sms() * 16);
-    tc::k_tri_flat<<<blocks, 256, 0, s>>>(g->off.p, g->adj.p, d_keys, n, pre.p, total, cnt.p);
+    tc::k_tri_flat<<<blocks, 256, 0, s>>>(g->off.p, g->adj.p, d_keys, n, pre.p, total, cnt.p, delta, sign);
     SP_CHECK_LAUNCH();
   }
   unsigned long long h[3];
@@ -985,29 +1000,18 @@ static bool symmetric_set(std::vector<unsigned long long>& k) {
   return t == k;
 }
 
-}  // namespace sp
-
-// DynTC's Batch block (dynamicDSLCodes/dynamicBatchTCV2:142-199): the batch is applied
-// (deletions, then additions) and the count updated. On a symmetric graph with a batch
-// that keeps it symmetric, only triangles through changed edges are counted:
+// One batch on g (deletions, then additions) with the triangles it changes. On a
+// symmetric graph whose batch keeps it symmetric (incremental = true):
 //   T(new) = T(old) - [triangles of the old graph through deleted edges]
 //                   + [triangles of the new graph through added edges],
 // where a deleted edge is one the old graph holds and an added edge one the graph
-// lacks after the deletions; a triangle through k changed edges is weighted 1/k, as
-// the DSL's count1/2 + count2/4 + count3/6 does for updates given in both directions.
-// Otherwise the batch is applied and the whole graph counted again.
-extern "C" int sp_tc_dynamic(sp_graph_h g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
-                             const int32_t* weight, int64_t* triangle_count) {
-  using namespace sp;
-  if (!g || !triangle_count || n < 0 || (n > 0 && (!type || !src || !dst))) {
-    set_error("sp_tc_dynamic: invalid argument");
-    return SP_ERR_INVALID;
-  }
-  g->tc_last_incremental = 0;
-  if (n == 0) {  // nothing changed: the caller's count stands
-    g->tc_last_incremental = 1;
-    return SP_OK;
-  }
+// lacks after the deletions; dcount gets the difference and delta (optional, int32[V]
+// on the device, zeroed) the per-vertex differences. Otherwise the batch is only
+// applied (incremental = false). A bad update is reported with g unchanged.
+static int batch_triangles(sp_graph* g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
+                           const int32_t* weight, int64_t* dcount, int* delta, bool& incremental) {
+  *dcount = 0;
+  incremental = false;
   std::vector<unsigned long long> dd, ad, du, au;  // directed keys; undirected keys (lo < hi)
   for (int64_t i = 0; i < n; ++i) {
     const int32_t a = src[i], b = dst[i];
@@ -1019,12 +1023,7 @@ extern "C" int sp_tc_dynamic(sp_graph_h g, int64_t n, const char* type, const in
     if (a != b) (type[i] == 'd' ? du : au).push_back(u);
   }
   SP_TRY(ensure_symmetry(g));
-  const bool incremental = g->symmetric == 1 && symmetric_set(dd) && symmetric_set(ad);
-  if (!incremental) {
-    SP_TRY(update_graph(g, n, type, src, dst, weight));
-    SP_TRY(build_tc_plan(g));
-    return tc_count(g, g->tc->order.p, g->V, triangle_count);
-  }
+  if (!(g->symmetric == 1 && symmetric_set(dd) && symmetric_set(ad))) return update_graph(g, n, type, src, dst, weight);
   for (auto* v : {&du, &au}) {
     std::sort(v->begin(), v->end());
     v->erase(std::unique(v->begin(), v->end()), v->end());
@@ -1042,7 +1041,7 @@ extern "C" int sp_tc_dynamic(sp_graph_h g, int64_t n, const char* type, const in
   if (nd) SP_CHECK_CUDA(cudaMemcpyAsync(d_del.p, du.data(), 8 * (size_t)nd, cudaMemcpyHostToDevice, s));
   if (na) SP_CHECK_CUDA(cudaMemcpyAsync(d_add.p, au.data(), 8 * (size_t)na, cudaMemcpyHostToDevice, s));
   int64_t lost = 0, gained = 0;
-  SP_TRY(tri_through(g, d_del.p, nd, 1, &lost));
+  SP_TRY(tri_through(g, d_del.p, nd, 1, &lost, delta, -1));
   int nnew = 0;
   if (na) {
     tc::k_new_edges<<<num_sms() * 4, 256, 0, s>>>(g->off.p, g->adj.p, d_add.p, na, d_del.p, nd, flag.p);
@@ -1056,8 +1055,73 @@ extern "C" int sp_tc_dynamic(sp_graph_h g, int64_t n, const char* type, const in
   }
   SP_TRY(update_graph(g, n, type, src, dst, weight));
   g->symmetric = 1;  // a symmetric graph minus and plus symmetric edge sets
-  SP_TRY(tri_through(g, d_new.p, nnew, 0, &gained));
-  *triangle_count = *triangle_count - lost + gained;
-  g->tc_last_incremental = 1;
+  SP_TRY(tri_through(g, d_new.p, nnew, 0, &gained, delta, 1));
+  *dcount = gained - lost;
+  incremental = true;
   return SP_OK;
+}
+
+}  // namespace sp
+
+// DynTC's Batch block (dynamicDSLCodes/dynamicBatchTCV2:142-199): the batch is applied
+// (deletions, then additions) and the count updated. On a symmetric graph with a batch
+// that keeps it symmetric, only triangles through changed edges are counted; a
+// triangle through k changed edges is found k times and weighted 1/k, as the DSL's
+// count1/2 + count2/4 + count3/6 does for updates given in both directions. Otherwise
+// the updated graph is counted again.
+extern "C" int sp_tc_dynamic(sp_graph_h g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
+                             const int32_t* weight, int64_t* triangle_count) {
+  using namespace sp;
+  if (!g || !triangle_count || n < 0 || (n > 0 && (!type || !src || !dst))) {
+    set_error("sp_tc_dynamic: invalid argument");
+    return SP_ERR_INVALID;
+  }
+  g->tc_last_incremental = 1;
+  if (n == 0) return SP_OK;  // nothing changed: the caller's count stands
+  int64_t dcount = 0;
+  bool incremental = false;
+  SP_TRY(batch_triangles(g, n, type, src, dst, weight, &dcount, nullptr, incremental));
+  g->tc_last_incremental = incremental ? 1 : 0;
+  if (incremental) {
+    *triangle_count += dcount;
+    return SP_OK;
+  }
+  SP_TRY(build_tc_plan(g));
+  return tc_count(g, g->tc->order.p, g->V, triangle_count);
+}
+
+// DynCF's Batch block (dynamicDSLCodes/dynamicBatchClustering:44-53): the batch, then
+// cf[V] (host or device; staticClusteringCoeff's counts before the batch on entry)
+// brought up to date. Incremental on a symmetric graph with a symmetric batch, as for
+// sp_tc_dynamic, each changed triangle adding -1 or +1 to its three vertices once;
+// otherwise the updated graph is counted again.
+extern "C" int sp_clustering_coeff_dynamic(sp_graph_h g, int64_t n, const char* type, const int32_t* src,
+                                           const int32_t* dst, const int32_t* weight, int32_t* cf) {
+  using namespace sp;
+  if (!g || !cf || n < 0 || (n > 0 && (!type || !src || !dst))) {
+    set_error("sp_clustering_coeff_dynamic: invalid argument");
+    return SP_ERR_INVALID;
+  }
+  g->tc_last_incremental = 1;
+  if (n == 0) return SP_OK;
+  cudaStream_t s = g->stream;
+  dbuf<int> delta;
+  SP_TRY(delta.alloc(std::max(1, g->V)));
+  if (g->V) SP_CHECK_CUDA(cudaMemsetAsync(delta.p, 0, sizeof(int) * g->V, s));
+  int64_t dcount = 0;
+  bool incremental = false;
+  SP_TRY(batch_triangles(g, n, type, src, dst, weight, &dcount, delta.p, incremental));
+  g->tc_last_incremental = incremental ? 1 : 0;
+  if (incremental) {
+    dbuf<int32_t> x;
+    SP_TRY(x.alloc(std::max(1, g->V)));
+    SP_CHECK_CUDA(cudaMemcpyAsync(x.p, cf, sizeof(int32_t) * g->V, cudaMemcpyDefault, s));
+    tc::k_add_i32<<<num_sms() * 4, 256, 0, s>>>(g->V, delta.p, x.p);
+    SP_CHECK_LAUNCH();
+    return copy_out(cf, x.p, sizeof(int32_t) * g->V, s);
+  }
+  SP_CHECK_CUDA(cudaMemsetAsync(delta.p, 0, sizeof(int) * g->V, s));
+  SP_TRY(build_tc_plan(g));
+  SP_TRY(lcc_count(g, g->tc->order.p, g->V, delta.p));
+  return copy_out(cf, delta.p, sizeof(int32_t) * g->V, s);
 }

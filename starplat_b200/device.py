@@ -141,6 +141,26 @@ class DeviceGraph:
         self._refresh_size()
         return int(c.value), bool(self.tune_get("tc.last_incremental"))
 
+    def clustering_coeff_dynamic(self, types, src, dst, weight, cf):
+        """DynCF's Batch block: apply the updates, then bring cf (int32[V], host or device:
+        the per-vertex triangle counts before the batch) up to date in place. Returns
+        True when only the triangles through the batch's edges were counted."""
+        if str(cf.dtype) not in ("int32", "torch.int32") or len(cf) != self.V:
+            raise ValueError("cf must be int32 with one entry per vertex")
+        n, ptrs, _keep = self._batch(types, src, dst, weight)
+        check("sp_clustering_coeff_dynamic", lib().sp_clustering_coeff_dynamic(self.handle, n, *ptrs, _ptr(cf)))
+        self._refresh_size()
+        return bool(self.tune_get("tc.last_incremental"))
+
+    def degree_dynamic(self, types, src, dst, weight=None, out=None):
+        """DynDegree's Batch block: apply the updates, then the out-degrees: int32[V]."""
+        if out is None:
+            out = np.empty(self.V, np.int32)
+        n, ptrs, _keep = self._batch(types, src, dst, weight)
+        check("sp_degree_dynamic", lib().sp_degree_dynamic(self.handle, n, *ptrs, _ptr(out)))
+        self._refresh_size()
+        return out
+
     def pagerank_dynamic(self, types, src, dst, weight, pagerank, beta: float = 1e-6, delta: float = 0.85,
                          max_iter: int = 100):
         """DynPR's Batch block: apply the updates (none if types is empty), then run

@@ -81,6 +81,19 @@ int main(int argc, char** argv) {
   // DynTC's batch: drop 0 <-> V-1 again (incremental: the graph and batch are symmetric)
   std::vector<Upd> batch1 = {{'d', 0, V - 1, 0}, {'d', V - 1, 0, 0}};
   std::printf("TCD %ld\n", starplat_b200::dynamic_tc(g, batch1, 0, 2, Compute_TC(g)));
+  // DynCF's batch (add 0 <-> V-1 back) from the counts of the current graph, then
+  // DynDegree's (add 3 -> V-4)
+  staticClusteringCoeff(g, cf.data());
+  std::vector<Upd> batch_cf = {{'a', 0, V - 1, 1}, {'a', V - 1, 0, 1}};
+  starplat_b200::dynamic_clustering_coeff(g, batch_cf, 0, 2, cf.data());
+  std::printf("LCCU");
+  for (int v = 0; v < V; ++v) std::printf(" %d", cf[v]);
+  std::printf("\n");
+  std::vector<Upd> batch_deg = {{'a', 3, V - 4, 1}};
+  starplat_b200::dynamic_degree(g, batch_deg, 0, 1, deg.data());
+  std::printf("DEGU");
+  for (int v = 0; v < V; ++v) std::printf(" %d", deg[v]);
+  std::printf("\n");
   // DynPR's batch on the updated copy: add 1 <-> V-2 and refresh the ranks from the
   // previous ones
   std::vector<Upd> batch2 = {{'a', 1, V - 2, 2}, {'a', V - 2, 1, 2}};

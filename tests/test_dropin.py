@@ -83,6 +83,12 @@ def check_outputs(res, g, src):
     edges = _apply(edges, [("d", 0, V - 1, 0), ("d", V - 1, 0, 0)])
     noff, nadj, _ = _csr(V, edges)
     assert int(res["TCD"][0]) == O.tc(noff, nadj)
+    edges = _apply(edges, [("a", 0, V - 1, 1), ("a", V - 1, 0, 1)])
+    noff, nadj, _ = _csr(V, edges)
+    assert np.array_equal(np.array(res["LCCU"], np.int64), O.lcc(noff, nadj))
+    edges = _apply(edges, [("a", 3, V - 4, 1)])
+    noff, nadj, _ = _csr(V, edges)
+    assert np.array_equal(np.array(res["DEGU"], np.int64), np.diff(noff))
     edges = _apply(edges, [("a", 1, V - 2, 2), ("a", V - 2, 1, 2)])
     noff, nadj, _ = _csr(V, edges)
     rev = sorted((b, a) for a, b in edges)

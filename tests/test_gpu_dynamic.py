@@ -320,3 +320,37 @@ def test_tc_dynamic_rejects_a_bad_batch_unchanged():
             with pytest.raises(_lib.SPError):
                 dg.tc_dynamic(t, s, d, None, before)
         assert dg.E == E and dg.tc() == before
+
+
+def test_clustering_coeff_dynamic_matches_the_oracle():
+    # symmetric batches: per-vertex triangle counts moved by the changed triangles only;
+    # an unsymmetric batch: counted again; host and device arrays
+    import torch
+
+    rng = np.random.default_rng(23)
+    g = G.rmat(12, 16, seed=7)
+    edges = _edges(g.indexofNodes, g.edgeList, np.ones(g.E, np.int32))
+    with DeviceGraph.from_csr(g) as dg:
+        cf = dg.clustering_coeff()
+        for step, (n, sym) in enumerate(((2, True), (50, True), (900, True), (4000, True), (100, False))):
+            t, s, d, w = (_sym_batch if sym else _batch)(rng, g.V, edges, n)
+            x = torch.from_numpy(cf).cuda() if step == 2 else cf
+            incremental = dg.clustering_coeff_dynamic(t, s, d, w, x)
+            cf = x.cpu().numpy() if step == 2 else x
+            edges = _apply(edges, t, s, d, w)
+            off, adj, _ = _csr(g.V, edges)
+            assert incremental == sym
+            assert np.array_equal(cf, O.lcc(off, adj)), step
+
+
+def test_degree_dynamic_gives_the_new_out_degrees():
+    rng = np.random.default_rng(24)
+    g = G.rmat(11, 8, seed=3, directed=True)
+    edges = _edges(g.indexofNodes, g.edgeList, np.ones(g.E, np.int32))
+    with DeviceGraph.from_csr(g, with_weights=False) as dg:
+        for n in (1, 300):
+            t, s, d, w = _batch(rng, g.V, edges, n)
+            deg = dg.degree_dynamic(t, s, d, None)
+            edges = _apply(edges, t, s, d, w)
+            off, _, _ = _csr(g.V, edges)
+            assert np.array_equal(deg, np.diff(off))
