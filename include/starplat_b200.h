@@ -330,6 +330,12 @@ int sp_clustering_coeff_dynamic(sp_graph_h g, int64_t n, const char* type, const
  * present ones; these are the exact degrees). */
 int sp_degree_dynamic(sp_graph_h g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
                       const int32_t* weight, int32_t* deg);
+/* Replaces the generated Batch block of DynBC (DSL dynamicDSLCodes/dynamicDecBC,
+ * dynamicBatchIncNorm, dynamicBatchDecNorm): one batch of edge updates, then BC over
+ * the distinct seeds (host or device ids) on the updated graph, as sp_bc computes it.
+ * Seeds are checked before the batch is applied. */
+int sp_bc_dynamic(sp_graph_h g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
+                  const int32_t* weight, const int32_t* sources, int32_t nsrc, float* BC);
 int sp_pagerank_dynamic(sp_graph_h g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
                         const int32_t* weight, float beta, float delta, int32_t maxIter, float* pageRank,
                         int32_t* iterations, double* final_diff);

@@ -275,6 +275,18 @@ inline void dynamic_degree(GraphT& g, const std::vector<UpdateT>& batch, int k, 
         "dynamic_degree");
 }
 
+// DynBC's Batch block on the device copy: apply entries k .. k + size - 1, then BC over
+// the seeds on the new graph.
+template <class GraphT, class UpdateT>
+inline void dynamic_bc(GraphT& g, const std::vector<UpdateT>& batch, int k, int size, float* BC,
+                       std::set<int>& seeds) {
+  UpdateArrays u(batch, k, size);
+  std::vector<int32_t> s(seeds.begin(), seeds.end());
+  check(sp_bc_dynamic(mirror(g), u.n(), u.type.data(), u.src.data(), u.dst.data(), u.w.data(), s.data(),
+                      (int32_t)s.size(), BC),
+        "dynamic_bc");
+}
+
 // DynPR's Batch block on the device copy: apply entries k .. k + size - 1, then run
 // PageRank on the new graph from pageRank (the ranks before the batch), in place.
 template <class GraphT, class UpdateT>

@@ -71,6 +71,7 @@ SIGNATURES = {
     "sp_tc_dynamic": (ctypes.c_int, [vp, i64, vp, vp, vp, vp, P(i64)]),
     "sp_clustering_coeff_dynamic": (ctypes.c_int, [vp, i64, vp, vp, vp, vp, vp]),
     "sp_degree_dynamic": (ctypes.c_int, [vp, i64, vp, vp, vp, vp, vp]),
+    "sp_bc_dynamic": (ctypes.c_int, [vp, i64, vp, vp, vp, vp, vp, i32, vp]),
     "sp_pagerank_dynamic": (ctypes.c_int, [vp, i64, vp, vp, vp, vp, f32, f32, i32, vp, P(i32), P(f64)]),
     "sp_tune_set": (ctypes.c_int, [vp, ctypes.c_char_p, i64]),
     "sp_tune_get": (ctypes.c_int, [vp, ctypes.c_char_p, P(i64)]),

@@ -1073,3 +1073,26 @@ extern "C" int sp_bfs_sigma(sp_graph_h g, const int32_t* sources, int32_t nsrc, 
   SP_TRY(copy_out(level, dl.p, sizeof(int32_t) * n, s));
   return copy_out(sigma, ds.p, sizeof(double) * n, s);
 }
+
+// DynBC's Batch block (dynamicDSLCodes/dynamicDecBC:271-347, dynamicBatchIncNorm:231-290,
+// dynamicBatchDecNorm:280-353): the batch, then BC over the seeds on the updated graph.
+// The DSL keeps every seed's BFS levels, path counts and dependencies and repairs those
+// the batch reaches; this runs the batched Brandes pass again, whose cost is one forward
+// and one backward sweep per 64 seeds.
+extern "C" int sp_bc_dynamic(sp_graph_h g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
+                             const int32_t* weight, const int32_t* sources, int32_t nsrc, float* BC) {
+  using namespace sp;
+  if (!g || !BC || nsrc < 0 || (nsrc > 0 && !sources) || n < 0 || (n > 0 && (!type || !src || !dst))) {
+    set_error("sp_bc_dynamic: invalid argument");
+    return SP_ERR_INVALID;
+  }
+  std::vector<int32_t> hs(nsrc);
+  if (nsrc) SP_CHECK_CUDA(cudaMemcpy(hs.data(), sources, sizeof(int32_t) * nsrc, cudaMemcpyDefault));
+  for (int32_t v : hs)
+    if (v < 0 || v >= g->V) {  // checked before the batch changes anything
+      set_error("sp_bc_dynamic: source %d out of range [0, %d)", v, g->V);
+      return SP_ERR_INVALID;
+    }
+  if (n > 0) SP_TRY(update_graph(g, n, type, src, dst, weight));
+  return sp_bc(g, hs.data(), nsrc, BC, SP_BC_BATCHED);
+}

@@ -161,6 +161,20 @@ class DeviceGraph:
         self._refresh_size()
         return out
 
+    def bc_dynamic(self, types, src, dst, weight, sources, out=None):
+        """DynBC's Batch block: apply the updates, then BC over `sources` on the new graph
+        (float32[V])."""
+        if out is None:
+            out = np.empty(self.V, np.float32)
+        if isinstance(sources, (list, tuple, np.ndarray)):
+            sources = np.ascontiguousarray(sources, np.int32)
+        ns = int(sources.shape[0])
+        n, ptrs, _keep = self._batch(types, src, dst, weight)
+        check("sp_bc_dynamic", lib().sp_bc_dynamic(self.handle, n, *ptrs, _ptr(sources) if ns else None, ns,
+                                                   _ptr(out)))
+        self._refresh_size()
+        return out
+
     def pagerank_dynamic(self, types, src, dst, weight, pagerank, beta: float = 1e-6, delta: float = 0.85,
                          max_iter: int = 100):
         """DynPR's Batch block: apply the updates (none if types is empty), then run

@@ -354,3 +354,25 @@ def test_degree_dynamic_gives_the_new_out_degrees():
             edges = _apply(edges, t, s, d, w)
             off, _, _ = _csr(g.V, edges)
             assert np.array_equal(deg, np.diff(off))
+
+
+def test_bc_dynamic_matches_the_oracle_on_the_new_graph():
+    rng = np.random.default_rng(25)
+    g = G.rmat(11, 8, seed=6)
+    edges = _edges(g.indexofNodes, g.edgeList, np.ones(g.E, np.int32))
+    srcs = G.pick_sources(g, 40, seed=3)
+    with DeviceGraph.from_csr(g, with_weights=False) as dg:
+        for n, sym in ((2, True), (400, True), (100, False)):
+            t, s, d, w = (_sym_batch if sym else _batch)(rng, g.V, edges, n)
+            bc = dg.bc_dynamic(t, s, d, None, srcs).astype(np.float64)
+            edges = _apply(edges, t, s, d, w)
+            off, adj, _ = _csr(g.V, edges)
+            ref = O.bc(off, adj, srcs)
+            assert np.all(np.abs(bc - ref) <= 1e-5 * np.abs(ref) + 1e-9 * max(1.0, ref.max()))
+        # a seed outside the graph is rejected before the batch is applied
+        E = dg.E
+        a = next(v for v in range(1, g.V) if (0, v) not in edges)
+        with pytest.raises(_lib.SPError):
+            dg.bc_dynamic("aa", [0, a], [a, 0], None, [0, g.V])
+        dg._refresh_size()
+        assert dg.E == E
