@@ -152,23 +152,17 @@ void dev_free(void* p, size_t bytes, int dev) {
 }
 
 // ---------------------------------------------------------------- reverse CSR on device
-// Row of every CSR entry: each thread takes 32 consecutive entries, finds the row of
-// the first by binary search over the offsets and walks forward (empty rows and hub
-// rows cost nothing extra).
+// Row of every CSR entry, edge-parallel in tiles of EDGE_TILE entries (coalesced writes;
+// hub rows spread over many blocks).
 __global__ void k_row_of(int32_t V, int64_t E, const int32_t* __restrict__ off, int32_t* __restrict__ row) {
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x * 32;
-  for (int64_t e0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) * 32; e0 < E; e0 += stride) {
-    int lo = 0, hi = V;  // last v with off[v] <= e0
-    while (lo < hi) {
-      const int m = (lo + hi + 1) >> 1;
-      if (off[m] <= e0) lo = m; else hi = m - 1;
-    }
-    int r = lo;
-    const int64_t e1 = e0 + 32 < E ? e0 + 32 : E;
-    for (int64_t e = e0; e < e1; ++e) {
-      while (off[r + 1] <= e) ++r;
-      row[e] = r;
-    }
+  __shared__ int s_v[2];
+  for (long long t0 = (long long)blockIdx.x * EDGE_TILE; t0 < E; t0 += (long long)gridDim.x * EDGE_TILE) {
+    const long long t1 = t0 + EDGE_TILE < E ? t0 + EDGE_TILE : E;
+    if (threadIdx.x < 2) s_v[threadIdx.x] = edge_source(off, 0, V, threadIdx.x == 0 ? t0 : t1 - 1);
+    __syncthreads();
+    const int vlo = s_v[0], vhi = s_v[1];
+    for (long long e = t0 + threadIdx.x; e < t1; e += blockDim.x) row[e] = edge_source(off, vlo, vhi + 1, e);
+    __syncthreads();
   }
 }
 

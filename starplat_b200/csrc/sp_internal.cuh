@@ -210,6 +210,21 @@ int num_sms();
 
 // ----------------------------------------------------------------- device helpers
 namespace sp {
+// The row of CSR entry x: the last vertex v in [lo, hi) with off[v] <= x, given
+// off[lo] <= x < off[hi] (empty rows are never returned).
+__device__ __forceinline__ int edge_source(const int32_t* __restrict__ off, int lo, int hi, long long x) {
+  while (hi - lo > 1) {
+    const int m = (lo + hi) >> 1;
+    if (off[m] <= x) lo = m; else hi = m;
+  }
+  return lo;
+}
+
+// Edge-parallel loops over CSR entries: a block takes EDGE_TILE consecutive entries,
+// finds the rows of the first and last by binary search over the whole offsets, and each
+// thread then searches only between those two rows. Hub rows spread over many blocks.
+constexpr int EDGE_TILE = 1024;
+
 __device__ __forceinline__ int warp_id() { return threadIdx.x >> 5; }
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 
