@@ -931,11 +931,39 @@ extern "C" int sp_sssp_dynamic(sp_graph_h g, int64_t n, const char* type, const 
     if (type[i] == 'd') deletes = true;
     if (type[i] == 'a') seeds.push_back(src[i]);
   }
+  // The learned schedule of the last solve carries over the batch when the weights'
+  // range is unchanged: scoring again would read the graph's symmetry, which the
+  // update forgets (a reverse CSR build on a directed graph).
+  struct {
+    unsigned gen = 0;
+    int wmin = 0, wmax = 0, ctas = 0, local = 0, local_knob = -1;
+    int64_t delta = 0;
+  } kept;
+  if (g->sssp) {
+    const SsspPlan* q = g->sssp;
+    kept.gen = q->sel_gen;
+    kept.wmin = q->sel_wmin;
+    kept.wmax = q->sel_wmax;
+    kept.ctas = q->sel_ctas;
+    kept.local = q->sel_local;
+    kept.local_knob = q->sel_local_knob;
+    kept.delta = q->sel_delta;
+  }
   SP_TRY(update_graph(g, n, type, src, dst, weight));
   g->sssp_last_incremental = 0;
   if (n == 0) return SP_OK;  // nothing changed: the caller's distances stand
   const int32_t* w = nullptr;
   SP_TRY(sssp_prepare(g, nullptr, &w));
+  if (kept.gen != 0) {  // sssp_schedule uses it only while model, range and knob match
+    SsspPlan* p = g->sssp;
+    p->sel_gen = kept.gen;
+    p->sel_wmin = kept.wmin;
+    p->sel_wmax = kept.wmax;
+    p->sel_delta = kept.delta;
+    p->sel_ctas = kept.ctas;
+    p->sel_local = kept.local;
+    p->sel_local_knob = kept.local_knob;
+  }
   int64_t delta = 0;
   int ctas = 0, local = 0;
   SP_TRY(sssp_schedule(g, delta, ctas, local));
