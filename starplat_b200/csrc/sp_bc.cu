@@ -1087,7 +1087,7 @@ extern "C" int sp_bc_dynamic(sp_graph_h g, int64_t n, const char* type, const in
     return SP_ERR_INVALID;
   }
   std::vector<int32_t> hs(nsrc);
-  if (nsrc) SP_CHECK_CUDA(cudaMemcpy(hs.data(), sources, sizeof(int32_t) * nsrc, cudaMemcpyDefault));
+  if (nsrc) SP_TRY(copy_out(hs.data(), sources, sizeof(int32_t) * nsrc, g->stream));  // host or device ids
   for (int32_t v : hs)
     if (v < 0 || v >= g->V) {  // checked before the batch changes anything
       set_error("sp_bc_dynamic: source %d out of range [0, %d)", v, g->V);
