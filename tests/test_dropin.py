@@ -27,6 +27,14 @@ def build_driver(outdir, library_parse=False):
     return exe
 
 
+def test_every_header_template_instantiates():
+    # the wrappers no driver calls (e.g. dynamic_bc) are type-checked only when instantiated
+    with tempfile.TemporaryDirectory() as d:
+        cmd = ["g++", "-std=c++17", "-c", "-I", os.path.join(ROOT, "tests", "cpp"), "-I", os.path.join(ROOT, "include"),
+               os.path.join(ROOT, "tests", "cpp", "instantiate_all.cpp"), "-o", os.path.join(d, "all.o")]
+        subprocess.check_call(cmd)
+
+
 def test_dropin_header_compiles():
     with tempfile.TemporaryDirectory() as d:
         assert os.path.exists(build_driver(d))
