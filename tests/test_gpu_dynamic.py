@@ -376,3 +376,51 @@ def test_bc_dynamic_matches_the_oracle_on_the_new_graph():
             dg.bc_dynamic("aa", [0, a], [a, 0], None, [0, g.V])
         dg._refresh_size()
         assert dg.E == E
+
+
+def test_dsl_dynamic_programs_run_batch_by_batch():
+    # DynTC, DynPR, DynSSSP, DynCF, DynDegree and DynBC (starplat_b200.algorithms) over 30
+    # update records in batches of 8, each undirected update given in both directions
+    # next to each other; results against the oracle on the edge set replayed batch by batch
+    from starplat_b200 import algorithms as A
+
+    def fresh():
+        g = G.rmat(10, 8, seed=8)
+        g.edgeLen = G.hash_weights(g, 8, 1, 40, True)
+        return g
+
+    rng = np.random.default_rng(26)
+    g0 = fresh()
+    edges = _edges(g0.indexofNodes, g0.edgeList, g0.edgeLen)
+    t, s, d, w = _batch(rng, g0.V, edges, 15)
+    updates = []
+    for i in range(len(t)):
+        updates += [(t[i], int(s[i]), int(d[i]), int(w[i])), (t[i], int(d[i]), int(s[i]), int(w[i]))]
+    for k in range(0, len(updates), 8):
+        chunk = updates[k:k + 8]
+        edges = _apply(edges, "".join(u[0] for u in chunk), [u[1] for u in chunk], [u[2] for u in chunk],
+                       [u[3] for u in chunk])
+    off, adj, ww = _csr(g0.V, edges)
+    V = g0.V
+
+    assert A.DynTC(fresh(), updates, 8) == O.tc(off, adj)
+    pr = np.zeros(V, np.float32)
+    A.DynPR(fresh(), 1e-9, 0.85, 100, pr, updates, 8)
+    assert np.abs(pr.astype(np.float64) - _pagerank_fixed_point(V, edges)).sum() < 1e-6
+    src = int(G.pick_sources(g0, 1, seed=1)[0])
+    dist = np.zeros(V, np.int32)
+    A.DynSSSP(fresh(), dist, None, None, updates, 8, src)
+    assert np.array_equal(dist, O.sssp(off, adj, ww, src))
+    cf = np.zeros(V, np.int32)
+    A.DynCF(fresh(), updates, cf, 8)
+    assert np.array_equal(cf, O.lcc(off, adj))
+    deg = np.zeros(V, np.int32)
+    A.DynDegree(fresh(), updates, deg, 8)
+    assert np.array_equal(deg, np.diff(off))
+    seeds = set(int(x) for x in G.pick_sources(g0, 20, seed=2))
+    bc = np.zeros(V, np.float32)
+    A.DynBC(fresh(), bc, seeds, updates, 8)
+    ref = O.bc(off, adj, np.array(sorted(seeds), np.int32))
+    assert np.all(np.abs(bc.astype(np.float64) - ref) <= 1e-5 * np.abs(ref) + 1e-9 * max(1.0, ref.max()))
+    with pytest.raises(ValueError):
+        A.DynSSSP(fresh(), dist, np.zeros(V, np.int32), None, updates, 8, src)
