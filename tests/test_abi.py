@@ -44,3 +44,21 @@ def test_errors_do_not_cross_abi():
     assert st == -1 and b"invalid" in L.sp_last_error()
     assert L.sp_graph_free(None) == 0
     assert L.sp_tc(None, None, 0) == -1
+
+
+def test_dynamic_programs_slice_update_records_into_batches():
+    # updates<g>.currentBatch(): consecutive slices of batchSize records, converted to the
+    # C ABI's parallel arrays (host logic only; no GPU call)
+    import numpy as np
+    import pytest
+
+    from starplat_b200.algorithms import _batches
+
+    recs = [("a", 0, 1, 5), ("d", 2, 3, 0), ("a", 4, 5, 7), ("d", 6, 7, 0), ("a", 8, 9, 1)]
+    got = list(_batches(recs, 2))
+    assert [b[0] for b in got] == ["ad", "ad", "a"]
+    assert np.array_equal(got[1][1], [4, 6]) and np.array_equal(got[1][2], [5, 7])
+    assert np.array_equal(got[2][3], [1]) and got[0][1].dtype == np.int32
+    assert list(_batches([], 3)) == []
+    with pytest.raises(ValueError):
+        list(_batches(recs, 0))
