@@ -356,7 +356,11 @@ int sp_sssp_features(sp_graph_h g, const int32_t* weight, double delta_mult, int
  * loads the library until exit), so V is limited to SP_NOALLOC_MAX_V; larger graphs
  * get SP_ERR_INVALID. The first call on a device looks up that array's address
  * (cudaGetSymbolAddress) with the device current; make it before any stream capture.
- * Calls share the array: calls that overlap on the GPU race and must be serialised.
+ * The address is kept until exit: a cudaDeviceReset of that device is not supported
+ * while the library is loaded. Calls share the array: calls that overlap on the GPU
+ * race and must be serialised. The CSR is checked on the device before any gather
+ * (offsets from 0 to E, never decreasing; srcList ids in [0, V)); a malformed graph
+ * returns SP_ERR_INVALID. Each call synchronises cuda_stream before it returns.
  * cuda_stream may be NULL (default stream); iterations may be NULL. */
 #define SP_NOALLOC_MAX_V (1 << 20)
 int sp_pagerank_noalloc(const int32_t* indexofNodes, const int32_t* rev_indexofNodes, const int32_t* srcList,

@@ -18,7 +18,7 @@
 // counting is pinned against the reference's own code (graph::check_if_nbr,
 // run through oracle/ref_harness.cpp) and its sample graphs; PageRank, SSSP,
 // BC and Louvain are pinned by hand-computed known answers and by networkx
-// cross-checks on small graphs (tests/golden/make_golden.py).
+// cross-checks on small graphs (tests/test_oracle.py).
 #include <algorithm>
 #include <climits>
 #include <cmath>

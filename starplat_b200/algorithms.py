@@ -97,8 +97,9 @@ def Compute_CD(g: CSRGraph, weight=None) -> float:
 
 # ---- the dynamic programs (dynamicDSLCodes): the static pass, then one Batch block per
 # batchSize updates. updateBatch is a sequence of update records (type 'a' / 'd',
-# source, destination, weight), as graph.hpp's `update` struct. The batches change the
-# cached device copy only; the host CSRGraph keeps the arrays it was built from.
+# source, destination, weight), as graph.hpp's `update` struct. Each program works on a
+# private device copy of g that it frees on return: the host CSRGraph and the mirror that
+# the static entry points cache on it keep the graph as it was before the batches.
 
 def _batches(updateBatch, batchSize: int):
     """updates<g>.currentBatch(): consecutive slices of batchSize records, as arrays."""
@@ -113,21 +114,21 @@ def _batches(updateBatch, batchSize: int):
 
 def DynTC(g: CSRGraph, updateBatch, batchSize: int) -> int:
     """dynamicBatchTCV2 DynTC: the triangle count after every batch (the last is returned)."""
-    dg = device_graph(g)
-    count = dg.tc()
-    for t, s, d, w in _batches(updateBatch, batchSize):
-        count, _ = dg.tc_dynamic(t, s, d, w, count)
-    return count
+    with DeviceGraph.from_csr(g) as dg:
+        count = dg.tc()
+        for t, s, d, w in _batches(updateBatch, batchSize):
+            count, _ = dg.tc_dynamic(t, s, d, w, count)
+        return count
 
 
 def DynPR(g: CSRGraph, beta: float, delta: float, maxIter: int, pageRank: np.ndarray, updateBatch,
           batchSize: int) -> None:
     """dynamicBatchPR DynPR: pageRank[V] of the graph after the last batch, each batch
     started from the ranks before it."""
-    dg = device_graph(g)
-    dg.pagerank(beta, delta, maxIter, out=pageRank)
-    for t, s, d, w in _batches(updateBatch, batchSize):
-        dg.pagerank_dynamic(t, s, d, w, pageRank, beta, delta, maxIter)
+    with DeviceGraph.from_csr(g) as dg:
+        dg.pagerank(beta, delta, maxIter, out=pageRank)
+        for t, s, d, w in _batches(updateBatch, batchSize):
+            dg.pagerank_dynamic(t, s, d, w, pageRank, beta, delta, maxIter)
 
 
 def DynSSSP(g: CSRGraph, dist: np.ndarray, parent, weight, updateBatch, batchSize: int, src: int) -> None:
@@ -136,33 +137,33 @@ def DynSSSP(g: CSRGraph, dist: np.ndarray, parent, weight, updateBatch, batchSiz
     be None: the device copy's edgeLen is the propEdge the batches update."""
     if parent is not None or weight is not None:
         raise ValueError("DynSSSP: parent is not computed and weight must be None (edgeLen is used)")
-    dg = device_graph(g)
-    dg.sssp(int(src), out=dist)
-    for t, s, d, w in _batches(updateBatch, batchSize):
-        dg.sssp_dynamic(t, s, d, w, int(src), dist)
+    with DeviceGraph.from_csr(g) as dg:
+        dg.sssp(int(src), out=dist)
+        for t, s, d, w in _batches(updateBatch, batchSize):
+            dg.sssp_dynamic(t, s, d, w, int(src), dist)
 
 
 def DynCF(g: CSRGraph, updateBatch, cf: np.ndarray, batchSize: int) -> None:
     """dynamicBatchClustering DynCF: cf[V] after the last batch."""
-    dg = device_graph(g)
-    dg.clustering_coeff(out=cf)
-    for t, s, d, w in _batches(updateBatch, batchSize):
-        dg.clustering_coeff_dynamic(t, s, d, w, cf)
+    with DeviceGraph.from_csr(g) as dg:
+        dg.clustering_coeff(out=cf)
+        for t, s, d, w in _batches(updateBatch, batchSize):
+            dg.clustering_coeff_dynamic(t, s, d, w, cf)
 
 
 def DynDegree(g: CSRGraph, updateBatch, deg: np.ndarray, batchSize: int) -> None:
     """dynamicBatchDeg DynDegree: deg[V] (out-degrees) after the last batch."""
-    dg = device_graph(g)
-    dg.degree(out=deg)
-    for t, s, d, w in _batches(updateBatch, batchSize):
-        dg.degree_dynamic(t, s, d, w, out=deg)
+    with DeviceGraph.from_csr(g) as dg:
+        dg.degree(out=deg)
+        for t, s, d, w in _batches(updateBatch, batchSize):
+            dg.degree_dynamic(t, s, d, w, out=deg)
 
 
 def DynBC(g: CSRGraph, BC: np.ndarray, seeds, updateBatch, batchSize: int) -> None:
     """dynamicDecBC / dynamicBatchIncNorm / dynamicBatchDecNorm DynBC: BC[V] over seeds
     after the last batch."""
-    dg = device_graph(g)
-    src = np.array(sorted(seeds), np.int32)
-    dg.bc(src, out=BC)
-    for t, s, d, w in _batches(updateBatch, batchSize):
-        dg.bc_dynamic(t, s, d, w, src, out=BC)
+    with DeviceGraph.from_csr(g) as dg:
+        src = np.array(sorted(seeds), np.int32)
+        dg.bc(src, out=BC)
+        for t, s, d, w in _batches(updateBatch, batchSize):
+            dg.bc_dynamic(t, s, d, w, src, out=BC)

@@ -202,13 +202,14 @@ __global__ void k_add_fresh(const int32_t* __restrict__ off, const int32_t* __re
 }
 
 // The current edges to their new places (tiles of EDGE_TILE entries); a held edge that
-// the batch adds again keeps its place and gains the added weight.
+// the batch adds again keeps its place and gains the added weight. A sum outside int32
+// raises *overflow (the host then rejects the batch and keeps the old CSR).
 __global__ void k_merge_edges(int32_t V, long long E, const int32_t* __restrict__ off,
                               const int32_t* __restrict__ adj, const int32_t* __restrict__ w,
                               const unsigned long long* __restrict__ udel, int nud, const int32_t* __restrict__ xrank,
                               const unsigned long long* __restrict__ uak, const int32_t* __restrict__ uaw, int nua,
                               const int32_t* __restrict__ newrank, int32_t* __restrict__ adj2,
-                              int32_t* __restrict__ w2) {
+                              int32_t* __restrict__ w2, int* __restrict__ overflow) {
   __shared__ int s_v[2];
   for (long long t0 = (long long)blockIdx.x * EDGE_TILE; t0 < E; t0 += (long long)gridDim.x * EDGE_TILE) {
     const long long t1 = t0 + EDGE_TILE < E ? t0 + EDGE_TILE : E;
@@ -224,7 +225,11 @@ __global__ void k_merge_edges(int32_t V, long long E, const int32_t* __restrict_
       const int l = lb_u64(uak, nua, k);
       const long long pos = i - xrank[j] + newrank[l];
       adj2[pos] = v;
-      if (w2) w2[pos] = w[i] + (l < nua && uak[l] == k ? uaw[l] : 0);
+      if (w2) {
+        const long long s = (long long)w[i] + (l < nua && uak[l] == k ? uaw[l] : 0);
+        if (s > INT_MAX || s < INT_MIN) *overflow = 1;
+        w2[pos] = (int32_t)s;
+      }
     }
     __syncthreads();  // s_v is rewritten for the next tile
   }
@@ -431,7 +436,7 @@ namespace sp {
 // A batch of edge updates applied to the forward CSR on the device: deletions, then
 // additions (see sp_graph_update). Everything derived from the old CSR is dropped.
 int update_graph(sp_graph* g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
-                 const int32_t* weight) {
+                 const int32_t* weight, int64_t* held_adds) {
   const int32_t V = g->V;
   std::vector<unsigned long long> del;
   std::vector<int32_t> as, ad, aw;
@@ -458,6 +463,27 @@ int update_graph(sp_graph* g, int64_t n, const char* type, const int32_t* src, c
     }
   }
   const int64_t E = g->E, na = (int64_t)as.size(), m = E + na, nd = (int64_t)del.size();
+  {  // repeated additions of one edge are summed in int32 on the device: reject a sum that wraps
+    int64_t mag = 0;
+    for (int32_t x : aw) mag += x < 0 ? -(int64_t)x : (int64_t)x;
+    if (mag > INT_MAX) {  // rare: check the per-edge sums exactly
+      std::vector<std::pair<unsigned long long, int64_t>> kw((size_t)na);
+      for (int64_t i = 0; i < na; ++i)
+        kw[i] = {((unsigned long long)(uint32_t)as[i] << 32) | (uint32_t)ad[i], (int64_t)aw[i]};
+      std::sort(kw.begin(), kw.end());
+      for (size_t i = 0; i < kw.size();) {
+        size_t j = i;
+        int64_t sum = 0;
+        for (; j < kw.size() && kw[j].first == kw[i].first; ++j) sum += kw[j].second;
+        if (sum > INT_MAX || sum < INT_MIN) {
+          set_error("sp_graph_update: the added weights of edge %d -> %d sum to %lld (outside int32)",
+                    (int)(kw[i].first >> 32), (int)(kw[i].first & 0xffffffffull), (long long)sum);
+          return SP_ERR_INVALID;
+        }
+        i = j;
+      }
+    }
+  }
   if (m > INT_MAX) {
     set_error("sp_graph_update: %lld edges after the update (int32 edge indices)", (long long)m);
     return SP_ERR_UNSUPPORTED;
@@ -503,12 +529,12 @@ int update_graph(sp_graph* g, int64_t n, const char* type, const int32_t* src, c
   T0.want(newrank, na + 1);
   T0.want(das, na);
   T0.want(dad, na);
-  T0.want(cnt, 2);
+  T0.want(cnt, 3);
   T0.want(temp, std::max<size_t>(t_need, 16));
   SP_TRY(T0.commit());
   SP_CHECK_CUDA(cudaMemsetAsync(xflag.p, 0, sizeof(int32_t) * (nd + 1), s));
   SP_CHECK_CUDA(cudaMemsetAsync(fresh.p, 0, sizeof(int32_t) * (na + 1), s));
-  SP_CHECK_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int) * 2, s));
+  SP_CHECK_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int) * 3, s));
   if (nd > 0) {  // deletion keys: sorted, unique
     SP_CHECK_CUDA(cudaMemcpyAsync(dk.p, del.data(), sizeof(unsigned long long) * nd, cudaMemcpyHostToDevice, s));
     cub::DoubleBuffer<unsigned long long> kd(dk.p, dk_alt.p);
@@ -562,7 +588,7 @@ int update_graph(sp_graph* g, int64_t n, const char* type, const int32_t* src, c
   if (E > 0) {
     ingest::k_merge_edges<<<num_sms() * 8, 256, 0, s>>>(V, E, g->off.p, g->adj.p, g->has_w ? g->w.p : nullptr,
                                                         udel.p, nud, xrank.p, uak.p, uaw.p, nua, newrank.p, adj.p,
-                                                        g->has_w ? w.p : nullptr);
+                                                        g->has_w ? w.p : nullptr, cnt.p + 2);
     SP_CHECK_LAUNCH();
   }
   if (added > 0) {
@@ -572,7 +598,13 @@ int update_graph(sp_graph* g, int64_t n, const char* type, const int32_t* src, c
   }
   ingest::k_merge_off<<<num_sms() * 4, 256, 0, s>>>(V, g->off.p, udel.p, nud, xrank.p, uak.p, nua, newrank.p, off.p);
   SP_CHECK_LAUNCH();
-  SP_CHECK_CUDA(cudaStreamSynchronize(s));
+  int overflow = 0;
+  SP_TRY(copy_out(&overflow, cnt.p + 2, sizeof(int), s));  // synchronises the stream
+  if (overflow) {
+    set_error("sp_graph_update: an added weight makes an edge's weight leave int32; the graph is unchanged");
+    return SP_ERR_INVALID;
+  }
+  if (held_adds) *held_adds = (int64_t)nua - added;
   // the new CSR replaces the old; plans, the reverse CSR and edgeMap are rebuilt on demand
   free_pr_plan(g->pr);
   free_tc_plan(g->tc);

@@ -191,9 +191,11 @@ int ensure_emap(sp_graph* g);         // builds emap (edgeMap) on device if miss
 // off[v] = first index of keys (ascending, E of them) that is >= v, for v = 0..V
 int offsets_of_sorted(int32_t V, int64_t E, const int32_t* keys, int32_t* off, cudaStream_t s);
 int finish_graph(sp_graph* g);        // checks a library-built CSR, sets max_out_deg
-// one batch of edge updates on the forward CSR, deletions then additions (sp_ingest.cu)
+// one batch of edge updates on the forward CSR, deletions then additions (sp_ingest.cu);
+// *held_adds (when given) receives the number of distinct added keys that were already
+// edges of the graph after the deletions, whose weights grew by the added weight
 int update_graph(sp_graph* g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
-                 const int32_t* weight);
+                 const int32_t* weight, int64_t* held_adds = nullptr);
 int pr_order_default();               // PageRank vertex order default (sp_pagerank.cu)
 int pr_src_hint_default();
 int tc_cta_warps_default();           // TC kernel choice default (sp_tc.cu)

@@ -13,10 +13,18 @@
 // Host code may not use the array's name as a device pointer: on the host it is
 // only a stand-in symbol. Its device address is looked up once per device with
 // cudaGetSymbolAddress, on the first call made while that device is current;
-// that first call should therefore happen before any stream capture. All calls
-// share the one array and each call clears what must start at zero, so calls
-// that overlap on the GPU (different streams or threads at the same time) race and
-// must be serialised by the caller.
+// that first call should therefore happen before any stream capture. The address
+// is kept for the life of the process, so a cudaDeviceReset of a device that has
+// made a call is not supported while the library stays loaded. All calls share the
+// one array and each call clears what must start at zero, so calls that overlap on
+// the GPU (different streams or threads at the same time) race and must be
+// serialised by the caller. Each call reads its result state back and synchronises
+// its stream before it returns.
+//
+// The caller's CSR is checked on the device before any gather (offsets start at 0,
+// never decrease and end at E; every srcList entry is a vertex id), with the verdict
+// kept in the scratch state, so a malformed graph returns SP_ERR_INVALID instead of
+// reading outside the caller's arrays.
 #include <mutex>
 
 #include "sp_internal.cuh"
@@ -32,7 +40,7 @@ struct State {
   int iter;
   int done;
   unsigned int ticket;
-  int pad;
+  int bad;  // 0, or which check failed: 1 indexofNodes, 2 rev_indexofNodes, 3 srcList
   double diff;
 };
 
@@ -59,7 +67,32 @@ __global__ void k_init(int V, const int32_t* __restrict__ off, float* __restrict
     st->iter = 0;
     st->done = 0;
     st->ticket = 0;
+    st->bad = 0;
     st->diff = 0.0;
+  }
+}
+
+// The caller's CSR, checked before the first iteration (runs after k_init on the same
+// stream): a failed check marks the state bad and done, so no iteration gathers.
+__global__ void k_check(int V, long long E, const int32_t* __restrict__ off, const int32_t* __restrict__ roff,
+                        const int32_t* __restrict__ radj, State* st) {
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  int bad = 0;
+  for (long long v = tid; v <= V; v += stride) {
+    const int a = off[v], b = roff[v];
+    if (v == 0 ? a != 0 : a < off[v - 1]) bad = 1;
+    if (v == V && a != E) bad = 1;
+    if (v == 0 ? b != 0 : b < roff[v - 1]) bad = 2;
+    if (v == V && b != E) bad = 2;
+  }
+  for (long long e = tid; e < E; e += stride) {
+    const int u = radj[e];
+    if (u < 0 || u >= V) bad = 3;
+  }
+  if (bad) {
+    atomicMax(&st->bad, bad);
+    st->done = 1;
   }
 }
 
@@ -161,6 +194,8 @@ extern "C" int sp_pagerank_noalloc(const int32_t* indexofNodes, const int32_t* r
   const int grid = std::min(na::MAX_BLOCKS, num_sms() * 8);
   na::k_init<<<num_sms() * 4, na::THREADS, 0, s>>>(V, indexofNodes, pr[0], con[0], st);
   SP_CHECK_LAUNCH();
+  na::k_check<<<num_sms() * 4, na::THREADS, 0, s>>>(V, (long long)E, indexofNodes, rev_indexofNodes, srcList, st);
+  SP_CHECK_LAUNCH();
   for (int k = 0; k < n_iter; ++k) {
     const int c = k & 1, n = c ^ 1;
     na::k_iter<<<grid, na::THREADS, 0, s>>>(V, indexofNodes, rev_indexofNodes, srcList, pr[c], con[c], pr[n], con[n],
@@ -170,6 +205,13 @@ extern "C" int sp_pagerank_noalloc(const int32_t* indexofNodes, const int32_t* r
   na::State hs;
   SP_CHECK_CUDA(cudaMemcpyAsync(&hs, st, sizeof(hs), cudaMemcpyDeviceToHost, s));
   SP_CHECK_CUDA(cudaStreamSynchronize(s));
+  if (hs.bad) {
+    static const char* what[] = {"", "indexofNodes (must start at 0, never decrease and end at E)",
+                                 "rev_indexofNodes (must start at 0, never decrease and end at E)",
+                                 "srcList (every entry must be a vertex id in [0, V))"};
+    set_error("sp_pagerank_noalloc: malformed %s; no ranks were computed", what[hs.bad & 3]);
+    return SP_ERR_INVALID;
+  }
   if (hs.iter & 1) {  // the last iteration wrote the scratch copy
     SP_CHECK_CUDA(cudaMemcpyAsync(pageRank, pr[1], sizeof(float) * V, cudaMemcpyDeviceToDevice, s));
     SP_CHECK_CUDA(cudaStreamSynchronize(s));

@@ -949,7 +949,8 @@ extern "C" int sp_sssp_dynamic(sp_graph_h g, int64_t n, const char* type, const 
     kept.local_knob = q->sel_local_knob;
     kept.delta = q->sel_delta;
   }
-  SP_TRY(update_graph(g, n, type, src, dst, weight));
+  int64_t held_adds = 0;
+  SP_TRY(update_graph(g, n, type, src, dst, weight, &held_adds));
   g->sssp_last_incremental = 0;
   if (n == 0) return SP_OK;  // nothing changed: the caller's distances stand
   const int32_t* w = nullptr;
@@ -967,9 +968,11 @@ extern "C" int sp_sssp_dynamic(sp_graph_h g, int64_t n, const char* type, const 
   int64_t delta = 0;
   int ctas = 0, local = 0;
   SP_TRY(sssp_schedule(g, delta, ctas, local));
-  if (deletes) return sssp_delta(g, w, source, dist, delta, ctas, local, nullptr);
-  // additions only: distances can only drop, and every drop starts at an added edge,
-  // so the solve resumes from the old distances with the added edges' sources queued
+  // A deletion, or an addition of an edge the graph already held (its weight grows by
+  // the added weight), can raise distances: solve again from the source.
+  if (deletes || held_adds > 0) return sssp_delta(g, w, source, dist, delta, ctas, local, nullptr);
+  // additions of new edges only: distances can only drop, and every drop starts at an
+  // added edge, so the solve resumes from the old distances with their sources queued
   std::sort(seeds.begin(), seeds.end());
   seeds.erase(std::unique(seeds.begin(), seeds.end()), seeds.end());
   SsspPlan* p = g->sssp;

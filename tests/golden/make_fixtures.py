@@ -78,4 +78,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("STARPLAT_REFERENCE")
+    if not root:
+        sys.exit("usage: make_fixtures.py <reference checkout> (or set STARPLAT_REFERENCE)")
+    main(root)

@@ -170,7 +170,8 @@ def test_sssp_dynamic_additions_resume_and_deletions_resolve():
                 w = rng.integers(1, 100, n).astype(np.int32)
                 t = "a" * n
             resumed = dg.sssp_dynamic(t, s, d, w, source, dist)
-            assert resumed == ("d" not in t)
+            held = any((int(a), int(b)) in edges for a, b in zip(s, d))
+            assert resumed == ("d" not in t and not held)
             edges = _apply(edges, t, s, d, w)
             off, adj, ww = _csr(g.V, edges)
             assert np.array_equal(dist, O.sssp(off, adj, ww, source)), step
@@ -194,6 +195,53 @@ def test_sssp_dynamic_additions_resume_and_deletions_resolve():
     with DeviceGraph.from_csr(h, with_weights=False) as dh:
         with pytest.raises(_lib.SPError):
             dh.sssp_dynamic("a", [0], [2], [1], 0, np.zeros(3, np.int32))
+
+
+def test_sssp_dynamic_readding_a_held_tree_edge_solves_again():
+    # an additions-only batch that adds an edge the graph already holds makes it longer
+    # (the weights are summed), so distances through it rise: the call must not resume
+    g = G.rmat(12, 8, seed=5, directed=True)
+    g.edgeLen = G.hash_weights(g, 5, 1, 100, False)
+    source = int(G.pick_sources(g, 1, seed=5)[0])
+    edges = _edges(g.indexofNodes, g.edgeList, g.edgeLen)
+    ref = O.sssp(g.indexofNodes, g.edgeList, g.edgeLen, source)
+    # tree edges out of the source: d(v) == w(source, v), and no other edge reaches v as short
+    tree = [(source, int(v)) for v in g.edgeList[g.indexofNodes[source]:g.indexofNodes[source + 1]]
+            if ref[v] == edges[(source, int(v))] and int(v) != source]
+    assert tree
+    with DeviceGraph.from_csr(g) as dg:
+        dist, _ = dg.sssp(source)
+        s = np.array([a for a, _ in tree], np.int32)
+        d = np.array([b for _, b in tree], np.int32)
+        w = np.full(len(tree), 1000, np.int32)
+        resumed = dg.sssp_dynamic("a" * len(tree), s, d, w, source, dist)
+        assert not resumed
+        edges = _apply(edges, "a" * len(tree), s, d, w)
+        off, adj, ww = _csr(g.V, edges)
+        new = O.sssp(off, adj, ww, source)
+        assert np.array_equal(dist, new)
+        assert (new[d] > ref[d]).any()  # some distance did rise
+        # a fresh edge in the next batch resumes again
+        far = int(np.argmax(np.where(new == 2**31 - 1, -1, new)))
+        if (source, far) not in edges:
+            assert dg.sssp_dynamic("a", [source], [far], [1], source, dist)
+            edges = _apply(edges, "a", [source], [far], [1])
+            off, adj, ww = _csr(g.V, edges)
+            assert np.array_equal(dist, O.sssp(off, adj, ww, source))
+
+
+def test_update_rejects_weight_sums_outside_int32():
+    g = from_pairs(3, [[0, 1], [1, 2]], name="w")
+    g.edgeLen = np.array([2**31 - 10, 5], np.int32)
+    with DeviceGraph.from_csr(g) as dg:
+        with pytest.raises(_lib.SPError):  # held edge + addition wraps
+            dg.update("a", [0], [1], [100])
+        with pytest.raises(_lib.SPError):  # two additions of one new edge wrap
+            dg.update("aa", [2], [0], [2**31 - 1, 2**31 - 1])
+        # rejected batches leave the graph as it was
+        assert dg.export()["edgeLen"].tolist() == [2**31 - 10, 5]
+        dg.update("a", [0], [1], [9])
+        assert dg.export()["edgeLen"].tolist() == [2**31 - 1, 5]
 
 
 def _pagerank_fixed_point(V, edges):
@@ -404,6 +452,12 @@ def test_dsl_dynamic_programs_run_batch_by_batch():
     V = g0.V
 
     assert A.DynTC(fresh(), updates, 8) == O.tc(off, adj)
+    # the programs leave g and its cached mirror as they were before the batches
+    g1 = fresh()
+    before = A.Compute_TC(g1)
+    assert A.DynTC(g1, updates, 8) == O.tc(off, adj)
+    assert A.Compute_TC(g1) == before == O.tc(g1.indexofNodes, g1.edgeList)
+    A.invalidate(g1)
     pr = np.zeros(V, np.float32)
     A.DynPR(fresh(), 1e-9, 0.85, 100, pr, updates, 8)
     assert np.abs(pr.astype(np.float64) - _pagerank_fixed_point(V, edges)).sum() < 1e-6

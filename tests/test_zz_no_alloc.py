@@ -14,6 +14,7 @@ import ctypes
 import numpy as np
 import pytest
 
+from oracle import oracle as O
 from starplat_b200 import _lib
 from starplat_b200 import generators as G
 from starplat_b200.device import DeviceGraph
@@ -38,6 +39,8 @@ def test_pagerank_noalloc_matches_allocating_entry_point():
     assert g.V <= MAX_V
     with DeviceGraph.from_csr(g) as dg:
         ref, ref_it, _ = dg.pagerank(1e-6, 0.85, 100)
+    # the FP64 oracle at the allocating path's iteration count
+    exact, _, _ = O.pagerank(g.indexofNodes, g.rev_indexofNodes, g.srcList, 0.0, 0.85, ref_it)
     off = torch.from_numpy(g.indexofNodes).cuda()
     roff = torch.from_numpy(g.rev_indexofNodes).cuda()
     radj = torch.from_numpy(g.srcList).cuda()
@@ -50,6 +53,36 @@ def test_pagerank_noalloc_matches_allocating_entry_point():
         assert it == ref_it, (call, it, ref_it)
         assert np.isfinite(got).all()
         assert np.abs(got.astype(np.float64) - ref.astype(np.float64)).sum() < 1e-6, call
+        assert np.abs(got.astype(np.float64) - exact).sum() < 1e-6, call
+
+
+def test_pagerank_noalloc_rejects_a_malformed_csr():
+    # the device check runs before any gather, so a bad srcList entry or a decreasing
+    # offset is reported instead of read through (the bad id here is V itself, and the
+    # bad offsets only shrink rows)
+    import torch
+
+    g = G.rmat(8, 4, seed=2, directed=True)
+    off = torch.from_numpy(g.indexofNodes).cuda()
+    roff = torch.from_numpy(g.rev_indexofNodes).cuda()
+    out = torch.zeros(g.V, dtype=torch.float32, device="cuda")
+    bad_src = g.srcList.copy()
+    bad_src[g.E // 2] = g.V
+    rc, _ = _noalloc(off, roff, torch.from_numpy(bad_src).cuda(), g.V, g.E, 1e-6, 0.85, 10, out)
+    assert rc == _lib.SP_ERR_INVALID_CODE
+    assert b"srcList" in _lib.lib().sp_last_error()
+    r = g.rev_indexofNodes.copy()
+    k = int(np.flatnonzero((r[:-1] > 0) & (np.diff(r) > 0))[0])  # a row with in-edges, not the first
+    r[k + 1] = r[k] - 1  # its end moves below its start
+    rc, _ = _noalloc(off, torch.from_numpy(r).cuda(), torch.from_numpy(g.srcList).cuda(), g.V, g.E, 1e-6,
+                     0.85, 10, out)
+    assert rc == _lib.SP_ERR_INVALID_CODE
+    assert b"rev_indexofNodes" in _lib.lib().sp_last_error()
+    # a good call right after the failures still matches the oracle
+    rc, it = _noalloc(off, roff, torch.from_numpy(g.srcList).cuda(), g.V, g.E, 1e-6, 0.85, 100, out)
+    assert rc == 0
+    exact, _, _ = O.pagerank(g.indexofNodes, g.rev_indexofNodes, g.srcList, 0.0, 0.85, it)
+    assert np.abs(out.cpu().numpy().astype(np.float64) - exact).sum() < 1e-6
 
 
 def test_pagerank_noalloc_rejects_graphs_above_its_scratch():
