@@ -140,6 +140,14 @@ def cpu_pagerank(g, iters: int = 3):
             "sample": f"{it} iterations of the OpenMP-form PageRank over the full graph ({dt:.2f} s)"}
 
 
+def pr_config(g, world):
+    """The headline's config, the same keys and values in both arms."""
+    return {"workload": f"pagerank rmat{PR_SCALE} ef{PR_EF} directed seed{PR_SEED}", "V": g.V, "E": g.E,
+            "beta": BETA, "delta": DELTA, "max_iter": MAX_ITER,
+            "l2": "inputs larger than L2 (srcList %.2f GB streamed per iteration)" % (4 * g.E / 1e9),
+            "parallelism": "replicas" if world > 1 else "single"}
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
@@ -151,9 +159,9 @@ def run_reference(args, rank):
     line = {"metric": METRIC, "value": v, "unit": "GTEPS", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-            "config": {"workload": f"pagerank rmat{PR_SCALE} ef{PR_EF} directed seed{PR_SEED}", "V": g.V, "E": g.E,
-                       "beta": BETA, "delta": DELTA, "max_iter": MAX_ITER},
-            "cpu_baseline": {**vals[-1], "value": v},
+            "config": pr_config(g, args.gpus),
+            "cpu_baseline": {**vals[-1], "value": v,
+                             "sample": vals[-1]["sample"] + "; sampled: 3 of the run's iterations per step"},
             "e2e": {"value": v, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -184,6 +192,19 @@ def tuned(dg):
         except Exception:
             pass
     return dg
+
+
+def bc_error(got, ref):
+    """BC against the FP64 oracle: per-vertex bar |got - ref| <= 1e-5 |ref| + 1e-9 max(1, max ref).
+    Returns the largest ratio of error to bar (<= 1 passes) and the largest relative
+    error over vertices with BC >= 1."""
+    got = np.asarray(got, np.float64)
+    ref = np.asarray(ref, np.float64)
+    err = np.abs(got - ref)
+    bar = 1e-5 * np.abs(ref) + 1e-9 * max(1.0, float(ref.max(initial=0.0)))
+    big = np.abs(ref) >= 1.0
+    rel = float((err[big] / np.abs(ref[big])).max(initial=0.0))
+    return float((err / bar).max(initial=0.0)), rel
 
 
 def roof(alg_bytes, ms, hbm):
@@ -319,16 +340,21 @@ def bench_sssp(name, g, src, steps, warmup, stream, hbm, cpu, cpu_mode):
         nt = O.num_threads()
         t = time.perf_counter()
         if cpu_mode == "omp":
-            _, rounds = O.sssp_omp(g.indexofNodes, g.edgeList, g.edgeLen, src, nthreads=nt)
+            ref, rounds = O.sssp_omp(g.indexofNodes, g.edgeList, g.edgeLen, src, nthreads=nt)
             dt = time.perf_counter() - t
             out["cpu_baseline"] = {"value": er / dt / 1e9, "unit": "GTEPS", "cores": nt, "kind": "port",
-                                   "sample": f"OpenMP fixed-point Compute_SSSP to convergence ({rounds} rounds, {dt:.2f} s)"}
+                                   "sample": f"OpenMP fixed-point Compute_SSSP to convergence ({rounds} rounds, "
+                                             f"{dt:.2f} s), full run"}
+            oracle = "the OpenMP fixed-point Compute_SSSP (correct CAS atomicMin), full graph"
         else:
-            O.sssp(g.indexofNodes, g.edgeList, g.edgeLen, src)
+            ref = O.sssp(g.indexofNodes, g.edgeList, g.edgeLen, src)
             dt = time.perf_counter() - t
             out["cpu_baseline"] = {"value": er / dt / 1e9, "unit": "GTEPS", "cores": 1, "kind": "port",
-                                   "sample": f"sequential Dijkstra ({dt:.2f} s); the OpenMP fixed-point form needs "
-                                             "thousands of full-vertex sweeps on this high-diameter grid"}
+                                   "sample": f"sequential Dijkstra ({dt:.2f} s), full run; the OpenMP fixed-point "
+                                             "form needs thousands of full-vertex sweeps on this high-diameter grid"}
+            oracle = "sequential Dijkstra, full graph"
+        out["parity"] = {"dist_equal_oracle": bool(np.array_equal(d, ref)),
+                         "mismatches": int((d != ref).sum()), "oracle": oracle, "tolerance": "bit-exact"}
     return out
 
 
@@ -353,12 +379,16 @@ def bench_bc(steps, warmup, stream, hbm, cpu, nsrc=256):
             # the sources split over the GPUs, one all-reduce of BC[V] (strong scaling)
             from starplat_b200.distributed import bc_on_gpus
 
+            import torch
+
+            bc_dev = torch.empty(g.V, dtype=torch.float32, device="cuda")  # summed in place by NCCL
             REP.barrier()
-            ms, _ = timed(lambda: bc_on_gpus(dg, srcs, REP), steps, warmup, stream)
+            ms, _ = timed(lambda: bc_on_gpus(dg, srcs, REP, out=bc_dev), steps, warmup, stream)
             ms = REP.max(ms)
             out["parallelism"] = f"sources split over {REP.world} GPUs, one all-reduce of BC[V]"
         else:
-            ms, _ = timed(lambda: dg.bc(srcs), steps, warmup, stream)
+            ms, res = timed(lambda: dg.bc(srcs), steps, warmup, stream)
+            bc_gpu = res[-1]
         few = srcs[:8]
         msp, _ = timed(lambda: dg.bc(few, variant=_lib.SP_BC_PLAIN), 1, 0, stream)
     out.update({"value": sum_er / (ms / 1e3) / 1e9, "unit": "GTEPS", "ms": ms,
@@ -373,7 +403,17 @@ def bench_bc(steps, warmup, stream, hbm, cpu, nsrc=256):
         O.bc_omp(g.indexofNodes, g.edgeList, srcs[:4], nthreads=nt)
         dt = time.perf_counter() - t
         out["cpu_baseline"] = {"value": float(er[:4].sum()) / dt / 1e9, "unit": "GTEPS", "cores": nt, "kind": "port",
-                               "sample": f"OpenMP-form Compute_BC over 4 of the 256 sources ({dt:.2f} s)"}
+                               "sample": f"OpenMP-form Compute_BC over 4 of the 256 sources ({dt:.2f} s), "
+                                         "sampled: 4 of 256 sources"}
+        if REP is None or REP.world == 1:
+            t = time.perf_counter()
+            ref = O.bc(g.indexofNodes, g.edgeList, srcs, nthreads=nt)
+            excess, rel = bc_error(bc_gpu, ref)
+            out["parity"] = {"oracle": f"FP64 Brandes with exact path counts over all {len(srcs)} sources "
+                                       f"({time.perf_counter() - t:.1f} s on {nt} threads)",
+                             "max_error_over_bar": excess, "max_rel_err_bc_ge_1": rel,
+                             "tolerance": "per vertex |bc - ref| <= 1e-5 |ref| + 1e-9 max(1, max ref)",
+                             "pass": excess <= 1.0}
     return out
 
 
@@ -411,7 +451,8 @@ def bench_bc_er(steps, warmup, stream, hbm, cpu, ngraphs=1000):
            "V": V, "E": E, "sources": int(srcs.shape[0]), "sum_E_r": er_tot, "graph_gen_s": round(gen_s, 1)}
     with DeviceGraph(off, adj, None, off, adj) as dg:
         dg.set_stream(stream)
-        ms, _ = timed(lambda: dg.bc_graphs(voff32, soff, srcs), steps, warmup, stream)
+        ms, res = timed(lambda: dg.bc_graphs(voff32, soff, srcs), steps, warmup, stream)
+        bc_all = res[-1]
     out.update({"value": er_tot / (ms / 1e3) / 1e9, "unit": "GTEPS", "ms": ms, "roofline": roof(alg, ms, hbm)})
     # plain form: one graph per call, one source at a time, on every 50th graph
     from starplat_b200 import _lib
@@ -439,7 +480,19 @@ def bench_bc_er(steps, warmup, stream, hbm, cpu, ngraphs=1000):
             er_s += er_k[k]
         dt = time.perf_counter() - t
         out["cpu_baseline"] = {"value": er_s / dt / 1e9, "unit": "GTEPS", "cores": nt, "kind": "port",
-                               "sample": f"OpenMP-form Compute_BC on 20 of the 1000 graphs, all 16 sources ({dt:.2f} s)"}
+                               "sample": f"OpenMP-form Compute_BC on 20 of the 1000 graphs, all 16 sources ({dt:.2f} s), "
+                                         "sampled: every 50th graph"}
+        worst, worst_rel = 0.0, 0.0
+        for k in range(0, len(gs), 50):
+            g = gs[k]
+            ref = O.bc(g.indexofNodes, g.edgeList, srcs[soff[k]:soff[k + 1]] - voff32[k], nthreads=nt)
+            e, r = bc_error(bc_all[voff32[k]:voff32[k + 1]], ref)
+            worst, worst_rel = max(worst, e), max(worst_rel, r)
+        out["parity"] = {"oracle": "FP64 Brandes with exact path counts on every 50th graph (20 of 1000), "
+                                   "all 16 sources, against the same graphs' slices of the batched result",
+                         "max_error_over_bar": worst, "max_rel_err_bc_ge_1": worst_rel,
+                         "tolerance": "per vertex |bc - ref| <= 1e-5 |ref| + 1e-9 max(1, max ref)",
+                         "pass": worst <= 1.0}
     return out
 
 
@@ -485,6 +538,16 @@ def bench_louvain(steps, warmup, stream, hbm, cpu):
                                "modularity": q, "sample": f"sequential restatement of the DSL, full run "
                                                           f"({sw} sweeps, {lv} levels, {dt:.2f} s)"}
         out["modularity_minus_cpu"] = res["q"] - q
+    fx = os.path.join(ROOT, "tests", "golden", "reference_gpu", "louvain.json")
+    if os.path.exists(fx):
+        ref = json.load(open(fx)).get("sbm1m")
+        if ref:
+            out["parity"] = {"oracle": "modularity (FP64) of the partition of the reference's own CUDA Louvain "
+                                       "(communitydetection_sequential_allocation.cu) on this graph, run on a B200 "
+                                       "and committed as a fixture",
+                             "reference_q": ref["reference_q"], "q_minus_reference": res["q"] - ref["reference_q"],
+                             "tolerance": "|q - reference_q| <= 1e-3",
+                             "pass": abs(res["q"] - ref["reference_q"]) <= 1e-3}
     return out
 
 
@@ -564,8 +627,12 @@ def bench_centrality(steps, warmup, stream, hbm, cpu):
             # anchor parts over the GPUs, one all-reduce of the int32 counts (strong scaling)
             from starplat_b200.distributed import clustering_coeff_on_gpus
 
+            import torch
+
+            cf_dev = torch.empty(g.V, dtype=torch.int32, device="cuda")
             REP.barrier()
-            ms, res = timed(lambda: clustering_coeff_on_gpus(dg, REP), steps, warmup, stream)
+            ms, _ = timed(lambda: clustering_coeff_on_gpus(dg, REP, out=cf_dev), steps, warmup, stream)
+            res = [cf_dev.cpu().numpy()]
             ms = REP.max(ms)
         else:
             ms, res = timed(lambda: dg.clustering_coeff(), steps, warmup, stream)
@@ -602,10 +669,15 @@ def bench_centrality(steps, warmup, stream, hbm, cpu):
             # the sources split over the GPUs, one all-reduce of CC[V] (strong scaling)
             from starplat_b200.distributed import closeness_on_gpus
 
+            import torch
+
+            cu_dev = torch.empty(g.V, dtype=torch.float32, device="cuda")
+            cw_dev = torch.empty(g.V, dtype=torch.float32, device="cuda")
             REP.barrier()
-            msu, resu = timed(lambda: closeness_on_gpus(dg, srcs, REP, weighted=False), max(1, steps // 2), 1,
-                              stream)
-            msw, resw = timed(lambda: closeness_on_gpus(dg, w16, REP), max(1, steps // 2), 1, stream)
+            msu, _ = timed(lambda: closeness_on_gpus(dg, srcs, REP, weighted=False, out=cu_dev), max(1, steps // 2),
+                           1, stream)
+            msw, _ = timed(lambda: closeness_on_gpus(dg, w16, REP, out=cw_dev), max(1, steps // 2), 1, stream)
+            resu, resw = [cu_dev.cpu().numpy()], [cw_dev.cpu().numpy()]
             msu, msw = REP.max(msu), REP.max(msw)
         else:
             msu, resu = timed(lambda: dg.closeness_unweighted(srcs), max(1, steps // 2), 1, stream)
@@ -855,6 +927,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the checks against the oracle")
     ap.add_argument("--quick", action="store_true",
                     help="PageRank device-resident timing only (no other legs): for profiler runs")
     ap.add_argument("--only", default="", help="comma list of extra workloads (default: all)")
@@ -942,6 +1015,18 @@ def main():
 
     hbm, hbm_kind = peaks()
 
+    # ---- parity of the timed result: L1 against FP64 PageRank at the same iteration count
+    parity = None
+    if rank == 0 and not args.no_parity:
+        from oracle import oracle as O
+
+        t = time.perf_counter()
+        exact, _, _ = O.pagerank(g.indexofNodes, g.rev_indexofNodes, g.srcList, 0.0, DELTA, iters,
+                                 nthreads=O.num_threads())
+        l1 = float(np.abs(out.cpu().numpy().astype(np.float64) - exact).sum())
+        parity = {"pagerank_l1_vs_fp64": l1, "tolerance": 1e-6, "pass": l1 < 1e-6, "iterations": iters,
+                  "oracle": f"FP64 Jacobi PageRank, the same {iters} iterations ({time.perf_counter() - t:.1f} s)"}
+
     # ---- kernel roofline: average iteration-kernel time from two fixed-iteration runs
     def timed_fixed(n, reps=3):
         best = None
@@ -1003,6 +1088,9 @@ def main():
 
     cpu_ok = rank == 0 and world == 1 and not args.no_cpu_baseline
     cpu = cpu_pagerank(g, 3) if cpu_ok else None
+    if cpu:
+        cpu["sample"] += "; sampled: 3 of the run's iterations"
+    cfg = pr_config(g, world)
     dg.free()
     del g
 
@@ -1016,12 +1104,9 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": f"pagerank rmat{PR_SCALE} ef{PR_EF} directed seed{PR_SEED}", "V": V, "E": E,
-                           "beta": BETA, "delta": DELTA, "max_iter": MAX_ITER, "iterations": it_total // args.steps,
-                           "l2": "inputs larger than L2 (srcList %.2f GB streamed per iteration)" % (4 * E / 1e9),
-                           "parallelism": "replicas" if world > 1 else "single", "graph_gen_s": round(gen_s, 2)},
+                "config": cfg, "iterations": it_total // args.steps, "graph_gen_s": round(gen_s, 2),
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
-                "plain": pr_plain, "algorithms": extras}
+                "parity": parity, "plain": pr_plain, "algorithms": extras}
         print(json.dumps(line), flush=True)
     rep.close()
 

@@ -110,10 +110,19 @@ int sp_graph_info(sp_graph_h g, int32_t* V, int64_t* E, int32_t* symmetric);
  *   "pr.order"  PageRank vertex order, fixed when the plan is built (a change rebuilds
  *             it): 0 = out-degree descending; 1 = in-degree class first (the row bins
  *             of the iteration kernel), out-degree descending within a class.
+ *   "pr.l1_hot"  PageRank: only gathers from the first l1_hot sources (relabelled by
+ *             out-degree, so the most-gathered ones) allocate in L1; the others bypass
+ *             it (0..2^22, default 0 = every gather allocates).
+ *   "pr.vec"  PageRank: 1 = the 32-lane bin and the long-row chunks read srcList in
+ *             16-byte loads (four entries per lane), 0 = one entry per lane per load.
  *   "sssp.delta"  SSSP bucket width used when sp_sssp gets delta <= 0 (0 = the largest
  *             edge weight).
  *   "sssp.ctas_per_sm"  SSSP: persistent CTAs per SM of the delta-stepping kernel (1..8,
  *             default 4; fewer CTAs make each grid barrier cheaper on high-diameter graphs).
+ *   "sssp.batch"  sp_sssp_batch / sp_closeness: sources per cooperative launch, each on
+ *             its own group of CTAs (1..1024, default 16; capped by the co-resident CTAs
+ *             and by 1/8 of device memory at 44 bytes per vertex per source).
+ *   "sssp.last_batch" (read only): sources per launch of the last batched run.
  *   "sssp.last_delta", "sssp.last_ctas", "sssp.last_local" (read only): the schedule the
  *             last SSSP call ran; "sssp.last_relaxed": the edges it relaxed (each
  *             out-edge of a vertex once per time the vertex was expanded).
@@ -178,9 +187,9 @@ int sp_degree_centrality(sp_graph_h g, int32_t* deg);
 /* Replaces generated `void Compute_CC(graph& g, float* CC, std::set<int>& sourceSet)`
  * (DSL staticDSLCodes/CC:1-26): CC[src] = 1.0 / (sum of the finite shortest-path
  * distances from src over the edge weights) for every source, CC = 0 elsewhere.
- * weight NULL = the graph's edgeLen. Distances by sp_sssp (learned schedule); the sum
- * is exact in 64 bits, where the DSL's int would overflow past 2^31 - 1. Sources must
- * be distinct; CC[V] host or device. */
+ * weight NULL = the graph's edgeLen. Distances by the batched solve of sp_sssp_batch
+ * (learned schedule); the sum is exact in 64 bits, where the DSL's int would overflow
+ * past 2^31 - 1. Sources must be distinct; CC[V] host or device. */
 int sp_closeness(sp_graph_h g, const int32_t* weight, const int32_t* sources, int32_t nsrc, float* CC);
 /* Replaces generated `void Compute_CC_Unweighted(graph& g, float* CC, std::set<int>& sourceSet)`
  * (DSL staticDSLCodes/closeness_centrality_unwt:1-20): CC[src] = 1.0 / (sum of the BFS
@@ -212,6 +221,14 @@ int sp_pagerank(sp_graph_h g, float beta, float delta, int32_t maxIter, float* p
 #define SP_SSSP_PLAIN 1
 int sp_sssp(sp_graph_h g, const int32_t* weight, int32_t src, int32_t* dist, int64_t delta, int32_t variant,
             int32_t* rounds);
+/* Shortest paths from many sources, for callers of the generated Compute_SSSP body in
+ * a loop over sources (the per-source fixedPoint of staticDSLCodes/CC:7-19): the
+ * sources run in batches of "sssp.batch", each batch ONE cooperative launch in which
+ * every source has its own group of CTAs (group barriers, its own queues) and the
+ * schedule is the one sp_sssp would use on this graph. dist[nsrc * V], source-major
+ * (row k = distances from sources[k]), host or device; sources in [0, V), host or
+ * device. Distances are bit-identical to sp_sssp's. */
+int sp_sssp_batch(sp_graph_h g, const int32_t* weight, const int32_t* sources, int32_t nsrc, int32_t* dist);
 
 /* ---- betweenness centrality ----------------------------------------------------
  * Replaces generated `void Compute_BC(graph& g, float* BC, std::set<int>& sourceSet)`

@@ -80,6 +80,7 @@ SIGNATURES = {
     "sp_clustering_coeff_part": (ctypes.c_int, [vp, i32, i32, vp]),
     "sp_pagerank": (ctypes.c_int, [vp, f32, f32, i32, vp, P(i32), P(f64), i32]),
     "sp_sssp": (ctypes.c_int, [vp, vp, i32, vp, i64, i32, P(i32)]),
+    "sp_sssp_batch": (ctypes.c_int, [vp, vp, vp, i32, vp]),
     "sp_bc": (ctypes.c_int, [vp, vp, i32, vp, i32]),
     "sp_bc_graphs": (ctypes.c_int, [vp, i32, vp, vp, vp, vp]),
     "sp_bfs_sigma": (ctypes.c_int, [vp, vp, i32, vp, vp]),

@@ -6,8 +6,9 @@
 //  * Compute_CC (staticDSLCodes/CC:1-26): for every source, the fixedPoint Min
 //    relaxation converges to the shortest-path distances over the edge weights;
 //    temp = the sum of the finite ones; CC[src] = 1.0 / temp, every other vertex 0.
-//    The distances come from sp_sssp's delta-stepping kernel (learned schedule) and
-//    the sum from a device reduction in 64 bits: the DSL's int temp overflows past
+//    The distances come from the batched delta-stepping kernel (sp_sssp_batch: one
+//    cooperative launch runs a batch of sources, each on its own group of CTAs, with
+//    the learned schedule) and the sum from a device reduction in 64 bits: the DSL's int temp overflows past
 //    2^31 - 1, and the exact sum is reported instead.
 //  * Compute_CC_Unweighted (staticDSLCodes/closeness_centrality_unwt:1-20): dist
 //    starts at 0 and iterateInBFS sets w.dist = v.dist + 1 for next-level neighbours
@@ -27,6 +28,10 @@ namespace sp {
 
 // Levels (-1 = unreached) and path counts of up to 64 sources, source-major (sp_bc.cu).
 int bc_levels(sp_graph* g, const int32_t* d_srcs, int nsrc, int32_t* lvl_out, double* sig_out);
+// Batched delta-stepping (sp_sssp.cu): the distance rows of every batch go to sum_rows.
+int sssp_batch_sums(sp_graph* g, const int32_t* weight, const std::vector<int32_t>& srcs,
+                    void (*sum_rows)(const int32_t*, int, int, unsigned long long*, cudaStream_t),
+                    unsigned long long* d_sums);
 
 namespace cen {
 
@@ -49,6 +54,11 @@ __global__ void k_sum_except(const int32_t* __restrict__ d, int V, int nsrc, int
     s = warp_sum(s);
     if (lane == 0 && s != 0) atomicAdd(out + k, (unsigned long long)s);
   }
+}
+
+// Sums of the finite distances of b source-major rows (the batched SSSP callback).
+void sum_finite_rows(const int32_t* rows, int V, int b, unsigned long long* out, cudaStream_t s) {
+  k_sum_except<<<num_sms() * 4, 256, 0, s>>>(rows, V, b, INT32_MAX, out);
 }
 
 }  // namespace cen
@@ -118,16 +128,12 @@ extern "C" int sp_closeness(sp_graph_h g, const int32_t* weight, const int32_t* 
   std::vector<int32_t> hs;
   SP_TRY(read_sources(g, sources, nsrc, hs, "sp_closeness"));
   cudaStream_t s = g->stream;
-  dbuf<int32_t> dist;
   dbuf<unsigned long long> sums;
-  SP_TRY(dist.alloc(g->V));
   SP_TRY(sums.alloc(nsrc));
   SP_CHECK_CUDA(cudaMemsetAsync(sums.p, 0, sizeof(unsigned long long) * nsrc, s));
-  for (int k = 0; k < nsrc; ++k) {
-    SP_TRY(sp_sssp(g, weight, hs[k], dist.p, 0, SP_SSSP_DELTA, nullptr));
-    cen::k_sum_except<<<num_sms() * 4, 256, 0, s>>>(dist.p, g->V, 1, INT32_MAX, sums.p + k);
-    SP_CHECK_LAUNCH();
-  }
+  // every source's delta-stepping solve in batched cooperative launches (one CTA group
+  // per source), the rows summed on the device
+  SP_TRY(sssp_batch_sums(g, weight, hs, cen::sum_finite_rows, sums.p));
   std::vector<long long> hsum(nsrc);
   SP_TRY(copy_out(hsum.data(), sums.p, sizeof(long long) * nsrc, s));
   return write_closeness(g, hs, hsum, CC);

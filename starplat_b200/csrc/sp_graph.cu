@@ -582,12 +582,36 @@ int sp_tune_set(sp_graph_h g, const char* key, int64_t value) {
     g->pr_src_hint = (int32_t)value;
     return SP_OK;
   }
+  if (!strcmp(key, "pr.l1_hot")) {
+    if (value < 0 || value > (1 << 22)) {
+      set_error("sp_tune_set: pr.l1_hot must be in [0, 4194304]");
+      return SP_ERR_INVALID;
+    }
+    g->pr_l1_hot = (int32_t)value;
+    return SP_OK;
+  }
+  if (!strcmp(key, "pr.vec")) {
+    if (value != 0 && value != 1) {
+      set_error("sp_tune_set: pr.vec must be 0 or 1");
+      return SP_ERR_INVALID;
+    }
+    g->pr_vec = (int32_t)value;
+    return SP_OK;
+  }
   if (!strcmp(key, "pr.order")) {
     if (value != 0 && value != 1) {
       set_error("sp_tune_set: pr.order must be 0 or 1");
       return SP_ERR_INVALID;
     }
     g->pr_order = (int32_t)value;
+    return SP_OK;
+  }
+  if (!strcmp(key, "sssp.batch")) {
+    if (value < 0 || value > 1024) {
+      set_error("sp_tune_set: sssp.batch must be in [0, 1024]");
+      return SP_ERR_INVALID;
+    }
+    g->sssp_batch = (int32_t)value;
     return SP_OK;
   }
   if (!strcmp(key, "sssp.delta")) {
@@ -686,8 +710,24 @@ int sp_tune_get(sp_graph_h g, const char* key, int64_t* value) {
     *value = g->pr_order >= 0 ? g->pr_order : pr_order_default();
     return SP_OK;
   }
+  if (!strcmp(key, "pr.l1_hot")) {
+    *value = g->pr_l1_hot >= 0 ? g->pr_l1_hot : pr_l1_hot_default();
+    return SP_OK;
+  }
+  if (!strcmp(key, "pr.vec")) {
+    *value = g->pr_vec >= 0 ? g->pr_vec : pr_vec_default();
+    return SP_OK;
+  }
   if (!strcmp(key, "sssp.delta")) {
     *value = g->sssp_delta;
+    return SP_OK;
+  }
+  if (!strcmp(key, "sssp.batch")) {
+    *value = g->sssp_batch > 0 ? g->sssp_batch : sssp_batch_default();
+    return SP_OK;
+  }
+  if (!strcmp(key, "sssp.last_batch")) {
+    *value = g->sssp_last_batch;
     return SP_OK;
   }
   if (!strcmp(key, "sssp.ctas_per_sm")) {

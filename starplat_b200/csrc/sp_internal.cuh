@@ -160,6 +160,8 @@ struct sp_graph {
   int32_t pr_hot = -1;  // PageRank: source ids of the L1 hot phase (-1 = default)
   int32_t pr_order = -1;  // PageRank: vertex order of the plan (-1 = default)
   int32_t pr_src_hint = -1;  // PageRank: L1 policy of srcList loads (-1 = default)
+  int32_t pr_l1_hot = -1;  // PageRank: sources whose gathers allocate in L1 (0 = all; -1 = default)
+  int32_t pr_vec = -1;     // PageRank: 16-byte srcList loads (-1 = default)
   int64_t sssp_delta = 0;  // SSSP bucket width (0 = max edge weight)
   int32_t sssp_ctas_per_sm = 0;  // SSSP persistent CTAs per SM (0 = learned / 4)
   int64_t sssp_last_delta = 0;   // schedule of the last SSSP call (reporting)
@@ -171,6 +173,8 @@ struct sp_graph {
   int32_t sssp_hub_deg = 0;    // SSSP: vertices above this out-degree go to shared pieces (0 = default)
   int32_t sssp_hub_chunk = 0;  // SSSP: edges per piece (0 = default)
   int32_t sssp_local = -1;     // SSSP: warp cascade budget in 32-edge steps per round (-1 = default, 0 = off)
+  int32_t sssp_batch = 0;      // batched SSSP: sources per cooperative launch (0 = default)
+  int32_t sssp_last_batch = 0;  // sources per launch of the last batched run (reporting)
   int32_t tc_cta_warps = -1;  // TC: warps per CTA of the shared-bitmap kernel (-1 = default, 0 = off)
   int32_t bc_batch = 0;
   int32_t bc_hub_deg = 0;  // BC: split level-list entries above this degree (0 = default)
@@ -198,11 +202,14 @@ int update_graph(sp_graph* g, int64_t n, const char* type, const int32_t* src, c
                  const int32_t* weight, int64_t* held_adds = nullptr);
 int pr_order_default();               // PageRank vertex order default (sp_pagerank.cu)
 int pr_src_hint_default();
+int pr_l1_hot_default();
+int pr_vec_default();
 int tc_cta_warps_default();           // TC kernel choice default (sp_tc.cu)
 int bc_hub_deg_default();             // BC entry-splitting defaults (sp_bc.cu)
 int sssp_hub_deg_default();           // SSSP hub-splitting defaults (sp_sssp.cu)
 int sssp_hub_chunk_default();
 int sssp_local_default();
+int sssp_batch_default();         // batched SSSP sources per launch (sp_sssp.cu)
 int bc_hub_chunk_default();
 int bc_cluster_default();
 int ensure_symmetry(sp_graph* g);     // fills g->symmetric

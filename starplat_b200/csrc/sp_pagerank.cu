@@ -46,6 +46,8 @@ constexpr int HOT_DEFAULT = 0;          // one phase: measured fastest on R-MAT 
 constexpr int HOT_MAX = 1 << 22;
 constexpr int SRC_HINT_DEFAULT = 2;     // srcList loads: 0 __ldg, 1 L1::no_allocate, 2 L1::evict_first
 constexpr int ORDER_DEFAULT = 0;        // vertex order: 0 out-degree, 1 in-degree class then out-degree
+constexpr int L1_HOT_DEFAULT = 0;       // gathers from every source allocate in L1
+constexpr int VEC_DEFAULT = 0;          // srcList read 4 bytes per lane per load
 // degree-bin upper bounds for 1, 4, 8 and 32 lanes per row segment
 constexpr int BIN_T1 = 4, BIN_T4 = 16, BIN_T8 = 32;
 
@@ -101,12 +103,14 @@ struct PrPlan {
   cudaGraphExec_t exec = nullptr;
   int exec_iters = 0;
   float exec_beta = -1, exec_delta = -1;
-  int exec_sh = -1;
+  int exec_sh = -1;       // srcList policy, vector loads and L1 hot count the graph was captured with
   cudaStream_t exec_stream = nullptr;
 };
 
 int pr_order_default() { return pr::ORDER_DEFAULT; }
 int pr_src_hint_default() { return pr::SRC_HINT_DEFAULT; }
+int pr_l1_hot_default() { return pr::L1_HOT_DEFAULT; }
+int pr_vec_default() { return pr::VEC_DEFAULT; }
 
 void free_pr_plan(PrPlan* p) {
   if (!p) return;
@@ -133,6 +137,7 @@ struct IterArgs {
   float delta;
   double beta;
   int max_iter;
+  int l1_hot;   // GH = 1: relabelled source ids below this allocate in L1
 };
 
 __device__ __forceinline__ double finalize_row(const IterArgs& a, int r, double sum,
@@ -166,15 +171,45 @@ __device__ __forceinline__ int ld_src(const int32_t* p) {
   return __ldg(p);
 }
 
+// srcList entries i .. i+3 in one 16-byte load (i a multiple of 4; the reverse rows
+// are 256-byte aligned and padded by 16 bytes, so a load that starts before E stays
+// inside the buffer), with the L1 policy of ld_src.
+template <int PH, int SH>
+__device__ __forceinline__ int4 ld_src4(const int32_t* p) {
+  int4 v;
+  if (PH == 0 || SH == 1) {
+    asm("ld.global.nc.L1::no_allocate.v4.b32 {%0, %1, %2, %3}, [%4];"
+        : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p));
+  } else if (SH == 2) {
+    asm("ld.global.nc.L1::evict_first.v4.b32 {%0, %1, %2, %3}, [%4];"
+        : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p));
+  } else {
+    v = __ldg(reinterpret_cast<const int4*>(p));
+  }
+  return v;
+}
+
+__device__ __forceinline__ int comp4(const int4& q, int j) { return j == 0 ? q.x : j == 1 ? q.y : j == 2 ? q.z : q.w; }
+
 // Where a gather of contrib[u] reads from. Only global memory (through L1) is used:
 // staging the hottest sources in shared memory measured 20-180% slower on R-MAT 22
 // (the carve-out shrinks L1, where those sources already hit, and large tables halve
-// the resident CTAs).
-template <int SH>
+// the resident CTAs). With GH = 1 only the `hot` most-gathered sources (the lowest
+// relabelled ids) are allocated in L1; a gather from any other source bypasses it, so
+// the stream of cold sectors does not evict the hot lines.
+template <int SH, int GH>
 struct GatherGlobal {
   static constexpr int kSrcHint = SH;
   const float* __restrict__ con;
-  __device__ __forceinline__ float operator()(int u) const { return __ldg(con + u); }
+  int hot;
+  __device__ __forceinline__ float operator()(int u) const {
+    if (GH == 1 && u >= hot) {
+      float v;
+      asm("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(con + u));
+      return v;
+    }
+    return __ldg(con + u);
+  }
 };
 // Sum of con[radj[i]] for i in [b, e) by a group of W lanes (sl = lane within the
 // group), U loads in flight per lane per round, reduced with a fixed xor tree.
@@ -200,8 +235,41 @@ __device__ __forceinline__ double group_row_sum(int b, int e, int sl, const int3
   return acc;
 }
 
-// One warp task: up to 32/W rows of one bin, W lanes per row segment.
-template <int PH, int W, int U, class G>
+// Sum of con[radj[i]] for i in [b, e) by a whole warp with 16-byte srcList loads: each
+// lane loads U4 groups of four consecutive entries per round from the 4-aligned start
+// below b (entries outside [b, e) are read but not gathered), then gathers all of them
+// before any sum; reduced with a fixed xor tree.
+template <int PH, int U4, class G>
+__device__ __forceinline__ double warp_row_sum_vec(int b, int e, int lane, const int32_t* __restrict__ radj,
+                                                   const G& gather) {
+  double acc = 0;
+  for (int base = b & ~3; base < e; base += 32 * 4 * U4) {
+    int4 q[U4];
+#pragma unroll
+    for (int k = 0; k < U4; ++k) {
+      const int i = base + 4 * lane + 128 * k;
+      q[k] = i < e ? ld_src4<PH, G::kSrcHint>(radj + i) : make_int4(0, 0, 0, 0);
+    }
+    float v[4 * U4];
+#pragma unroll
+    for (int k = 0; k < U4; ++k) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int i = base + 4 * lane + 128 * k + j;
+        v[4 * k + j] = (i >= b && i < e) ? gather(comp4(q[k], j)) : 0.0f;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 4 * U4; ++k) acc += (double)v[k];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  return acc;
+}
+
+// One warp task: up to 32/W rows of one bin, W lanes per row segment (VEC: the 32-lane
+// bin reads srcList 16 bytes at a time).
+template <int PH, int W, int U, int VEC, class G>
 __device__ __forceinline__ double warp_task(const IterArgs& a, int start, int count, int lane,
                                             const float* __restrict__ pr_old, const G& gather,
                                             float* __restrict__ pr_new, float* __restrict__ con_new) {
@@ -216,7 +284,11 @@ __device__ __forceinline__ double warp_task(const IterArgs& a, int start, int co
       b = h, e = r1, other = h - r0;  // other > 0: a hot partial is waiting
     }
   }
-  double sum = group_row_sum<PH, W, U>(b, e, sl, a.radj, gather);
+  double sum;
+  if constexpr (VEC == 1 && W == 32)
+    sum = warp_row_sum_vec<PH, U / 4>(b, e, lane, a.radj, gather);
+  else
+    sum = group_row_sum<PH, W, U>(b, e, sl, a.radj, gather);
   if (r < 0 || sl != 0) return 0.0;
   if (PH == 0) {
     if (other > 0) {
@@ -232,7 +304,7 @@ __device__ __forceinline__ double warp_task(const IterArgs& a, int start, int co
 // One phase of one iteration by persistent CTAs of NT threads: long-row chunks
 // first (a CTA each, CHUNK / NT loads per thread), then the warp tasks, heaviest
 // bins first; then the diff partials (the last CTA of the cold phase sums them).
-template <int PH, int NT, class G>
+template <int PH, int NT, int VEC, class G>
 __device__ __forceinline__ void phase_body(const IterArgs& a, const G& gather, const float* __restrict__ pr_old,
                                            float* __restrict__ pr_new, float* __restrict__ con_new, double* s_red,
                                            int& s_last) {
@@ -246,7 +318,30 @@ __device__ __forceinline__ void phase_body(const IterArgs& a, const G& gather, c
   for (int ci = blockIdx.x; ci < P.n_chunks; ci += gridDim.x) {
     const int4 c = P.chunks[ci];
     double acc = 0;
-    {
+    if constexpr (VEC == 1) {
+      // 16-byte srcList loads from the 4-aligned start below the chunk: a second round
+      // picks up the (at most three) entries past one aligned CHUNK
+      constexpr int C4 = CI / 4;
+      for (int base = c.y & ~3; base < c.z; base += 4 * NT * C4) {
+        int4 q[C4];
+#pragma unroll
+        for (int k = 0; k < C4; ++k) {
+          const int e = base + 4 * tid + 4 * NT * k;
+          q[k] = e < c.z ? ld_src4<PH, G::kSrcHint>(a.radj + e) : make_int4(0, 0, 0, 0);
+        }
+        float v[CI];
+#pragma unroll
+        for (int k = 0; k < C4; ++k) {
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int e = base + 4 * tid + 4 * NT * k + j;
+            v[4 * k + j] = (e >= c.y && e < c.z) ? gather(comp4(q[k], j)) : 0.0f;
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < CI; ++k) acc += (double)v[k];
+      }
+    } else {
       int idx[CI];
 #pragma unroll
       for (int k = 0; k < CI; ++k) {
@@ -289,10 +384,10 @@ __device__ __forceinline__ void phase_body(const IterArgs& a, const G& gather, c
     const int start = P.row_base[k] + (t - P.task_base[k]) * per;
     const int count = min(per, P.row_base[k + 1] - start);
     switch (k) {
-      case 0: my_diff += warp_task<PH, 32, 8>(a, start, count, lane, pr_old, gather, pr_new, con_new); break;
-      case 1: my_diff += warp_task<PH, 8, 4>(a, start, count, lane, pr_old, gather, pr_new, con_new); break;
-      case 2: my_diff += warp_task<PH, 4, 4>(a, start, count, lane, pr_old, gather, pr_new, con_new); break;
-      default: my_diff += warp_task<PH, 1, 4>(a, start, count, lane, pr_old, gather, pr_new, con_new); break;
+      case 0: my_diff += warp_task<PH, 32, 8, VEC>(a, start, count, lane, pr_old, gather, pr_new, con_new); break;
+      case 1: my_diff += warp_task<PH, 8, 4, VEC>(a, start, count, lane, pr_old, gather, pr_new, con_new); break;
+      case 2: my_diff += warp_task<PH, 4, 4, VEC>(a, start, count, lane, pr_old, gather, pr_new, con_new); break;
+      default: my_diff += warp_task<PH, 1, 4, VEC>(a, start, count, lane, pr_old, gather, pr_new, con_new); break;
     }
   }
 
@@ -328,14 +423,16 @@ __device__ __forceinline__ void phase_body(const IterArgs& a, const G& gather, c
 }
 
 // One phase of one iteration, every gather from global memory (256-thread CTAs).
-template <int PH, int SH>
-__global__ void __launch_bounds__(THREADS) k_phase(IterArgs a, const float* __restrict__ pr_old,
+// SH: L1 policy of srcList loads; GH: 1 = only sources below a.l1_hot allocate in L1;
+// VEC: 16-byte srcList loads in the 32-lane bin and the long-row chunks.
+template <int PH, int SH, int GH, int VEC>
+__global__ void __launch_bounds__(THREADS, 8) k_phase(IterArgs a, const float* __restrict__ pr_old,
                                                    const float* __restrict__ con_old, float* __restrict__ pr_new,
                                                    float* __restrict__ con_new) {
   __shared__ double s_red[THREADS / 32];
   __shared__ int s_last;
   if (a.st->done) return;
-  phase_body<PH, THREADS>(a, GatherGlobal<SH>{con_old}, pr_old, pr_new, con_new, s_red, s_last);
+  phase_body<PH, THREADS, VEC>(a, GatherGlobal<SH, GH>{con_old, a.l1_hot}, pr_old, pr_new, con_new, s_red, s_last);
 }
 
 // Rows without in-edges, iterations 0 and 1 only: pr' = (1-delta)/V. Their diff
@@ -884,8 +981,17 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
   a.two_phase = p->two_phase() ? 1 : 0;
   int per_sm = 0;
   const int sh = g->pr_src_hint >= 0 ? g->pr_src_hint : pr::SRC_HINT_DEFAULT;
+  const int l1_hot = g->pr_l1_hot >= 0 ? g->pr_l1_hot : pr::L1_HOT_DEFAULT;
+  const int vec = g->pr_vec >= 0 ? g->pr_vec : pr::VEC_DEFAULT;
+  a.l1_hot = l1_hot;
+  const int gh = l1_hot > 0 ? 1 : 0;
   using PhaseFn = void (*)(pr::IterArgs, const float*, const float*, float*, float*);
-  const PhaseFn ph1 = sh == 1 ? pr::k_phase<1, 1> : sh == 2 ? pr::k_phase<1, 2> : pr::k_phase<1, 0>;
+  static const PhaseFn table[3][2][2] = {
+      {{pr::k_phase<1, 0, 0, 0>, pr::k_phase<1, 0, 0, 1>}, {pr::k_phase<1, 0, 1, 0>, pr::k_phase<1, 0, 1, 1>}},
+      {{pr::k_phase<1, 1, 0, 0>, pr::k_phase<1, 1, 0, 1>}, {pr::k_phase<1, 1, 1, 0>, pr::k_phase<1, 1, 1, 1>}},
+      {{pr::k_phase<1, 2, 0, 0>, pr::k_phase<1, 2, 0, 1>}, {pr::k_phase<1, 2, 1, 0>, pr::k_phase<1, 2, 1, 1>}}};
+  const PhaseFn ph1 = table[sh][gh][vec];
+  const int exec_key = sh | (vec << 2) | (l1_hot << 3);
   SP_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ph1, pr::THREADS, 0));
   const int grid = std::max(1, std::min(num_sms() * 32, num_sms() * std::max(1, per_sm)));
   if (init) {
@@ -897,7 +1003,7 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
   }
   SP_CHECK_LAUNCH();
   if (!(p->exec && p->exec_iters == n_iter && p->exec_beta == beta && p->exec_delta == delta && p->exec_stream == s &&
-        p->exec_sh == sh)) {
+        p->exec_sh == exec_key)) {
     if (p->exec) {
       cudaGraphExecDestroy(p->exec);
       p->exec = nullptr;
@@ -909,7 +1015,7 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
       if (k < 2 && p->n_zero)
         pr::k_zero_rows<<<num_sms() * 2, 256, 0, s>>>(a, p->zrows, p->n_zero, p->prb[c].p, p->prb[n].p, p->con[n].p);
       if (a.two_phase)
-        pr::k_phase<0, 1><<<grid, pr::THREADS, 0, s>>>(a, p->prb[c].p, p->con[c].p, p->prb[n].p, p->con[n].p);
+        pr::k_phase<0, 1, 0, 0><<<grid, pr::THREADS, 0, s>>>(a, p->prb[c].p, p->con[c].p, p->prb[n].p, p->con[n].p);
       ph1<<<grid, pr::THREADS, 0, s>>>(a, p->prb[c].p, p->con[c].p, p->prb[n].p, p->con[n].p);
     }
     cudaError_t ce = cudaStreamEndCapture(s, &graph);
@@ -928,7 +1034,7 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
     p->exec_beta = beta;
     p->exec_delta = delta;
     p->exec_stream = s;
-    p->exec_sh = sh;
+    p->exec_sh = exec_key;
   }
   SP_CHECK_CUDA(cudaGraphLaunch(p->exec, s));
   g_launches.fetch_add((unsigned long long)n_iter * (p->two_phase() ? 2 : 1) +

@@ -56,6 +56,7 @@ constexpr int HUB_DEG_MAX = 1 << 25;  // 32 entries of at most this degree sum b
 constexpr int RING = 256;             // entries of a warp's cascade ring (power of two)
 constexpr int LOCAL_STEPS = 64;       // default cascade budget: 32-edge warp steps per round
 constexpr int SU = 4;                 // 32-edge steps whose loads and atomics are in flight together
+constexpr int BATCH = 16;             // sources per cooperative launch of the batched form
 constexpr unsigned FULL = 0xffffffffu;
 
 struct Ctl {
@@ -396,12 +397,13 @@ __device__ __forceinline__ void cascade(const Args& a, long long thr, int round,
   r.cnt = 0;
 }
 
-__global__ void __launch_bounds__(THREADS, 4) k_delta(Args a) {
-  __shared__ int32_t ring[(THREADS / 32) * RING];
+// One delta-stepping solve by `nblk` co-resident CTAs (this one is number `blk`):
+// the whole grid for a single source, or one group of a batched launch.
+__device__ __forceinline__ void delta_run(const Args& a, const int blk, const int nblk, int32_t* ring) {
   Ctl* c = a.ctl;
   const int lane = threadIdx.x & 31;
-  const int gw = (blockIdx.x * THREADS + threadIdx.x) >> 5;
-  const int nw = (gridDim.x * THREADS) >> 5;
+  const int gw = (blk * THREADS + threadIdx.x) >> 5;
+  const int nw = (nblk * THREADS) >> 5;
   int round = 0, epoch = 0;
   long long thr = a.delta;  // bucket 0 = [0, delta)
   while (true) {
@@ -412,7 +414,7 @@ __global__ void __launch_bounds__(THREADS, 4) k_delta(Args a) {
     const int fn = *(volatile int*)&c->fcount[epoch % 3];
     if (qv == 0 && hn == 0 && fn == 0) break;
     if ((long long)round >= a.max_rounds) {
-      if (blockIdx.x == 0 && threadIdx.x == 0) c->status = 1;
+      if (blk == 0 && threadIdx.x == 0) c->status = 1;
       break;
     }
     if (qv > 0 || hn > 0) {
@@ -455,11 +457,11 @@ __global__ void __launch_bounds__(THREADS, 4) k_delta(Args a) {
       }
       if (local) cascade(a, thr, round, epoch, o, r, work);
       if (lane == 0 && work > 0) atomicAdd(&c->relaxed, (unsigned long long)work);
-      if (blockIdx.x == 0 && threadIdx.x == 0) {
+      if (blk == 0 && threadIdx.x == 0) {
         c->qcount[(round + 2) % 3] = 0;  // read two rounds ago
         c->hcount[(round + 2) % 3] = 0ull;
       }
-      if (!grid_barrier(&c->bar)) break;
+      if (!group_barrier(&c->bar, (unsigned)nblk, blk == 0)) break;
       ++round;
     } else {
       // bucket advance: threshold to the bucket after the smallest far distance
@@ -498,22 +500,53 @@ __global__ void __launch_bounds__(THREADS, 4) k_delta(Args a) {
         queue_push(a, toq, u, Q, qcnt, HV, HB, hnext);
         warp_push(tof, u, FN, fnext);
       }
-      if (blockIdx.x == 0 && threadIdx.x == 0) {
+      if (blk == 0 && threadIdx.x == 0) {
         c->fcount[(epoch + 2) % 3] = 0;
         c->fmin[(epoch + 2) % 3] = INT_MAX;
         c->qcount[(round + 2) % 3] = 0;  // read two phases ago
         c->hcount[(round + 2) % 3] = 0ull;
       }
-      if (!grid_barrier(&c->bar)) break;
+      if (!group_barrier(&c->bar, (unsigned)nblk, blk == 0)) break;
       ++epoch;
       ++round;
     }
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (blk == 0 && threadIdx.x == 0) {
     c->rounds = round - epoch;  // relax rounds (each split also consumed a round number)
     c->epochs = epoch;
     if (c->bar.error) c->status = 1;
   }
+}
+
+__global__ void __launch_bounds__(THREADS, 4) k_delta(Args a) {
+  __shared__ int32_t ring[(THREADS / 32) * RING];
+  delta_run(a, blockIdx.x, gridDim.x, ring);
+}
+
+// Many sources in one cooperative launch: CTA group g = blockIdx.x / gsz solves the
+// g-th source of the batch over its own V-strided slice of every per-vertex buffer
+// and its own Ctl (counters, bounded group barrier). Adjacency, weights and offsets
+// are shared, so the groups' gathers share L2.
+__global__ void __launch_bounds__(THREADS, 4) k_delta_multi(Args a, int gsz) {
+  __shared__ int32_t ring[(THREADS / 32) * RING];
+  __shared__ Args b;  // this group's arguments (shared: read like the kernel parameters)
+  const int g = blockIdx.x / gsz;
+  if (threadIdx.x == 0) {
+    const size_t o = (size_t)g * (size_t)a.V;
+    b = a;
+    b.dist += o;
+    for (int k = 0; k < 2; ++k) {
+      b.q[k] += o;
+      b.f[k] += o;
+      b.hv[k] += o;
+      b.hbase[k] += o;
+    }
+    b.qstamp += o;
+    b.fstamp += o;
+    b.ctl += g;
+  }
+  __syncthreads();
+  delta_run(b, blockIdx.x % gsz, gsz, ring);
 }
 
 __global__ void k_init(int V, int src, int32_t* dist, int32_t* qstamp, int32_t* fstamp, int32_t* q0, int32_t* hv0,
@@ -543,6 +576,47 @@ __global__ void k_init(int V, int src, int32_t* dist, int32_t* qstamp, int32_t* 
     for (int k = 0; k < 3; ++k) {
       c->fcount[k] = 0;
       c->fmin[k] = INT_MAX;
+    }
+    c->rounds = c->epochs = c->status = 0;
+    c->relaxed = 0ull;
+  }
+}
+
+// Initial state of every source of a batch: blockIdx.y = position in the batch, each
+// with its V-strided slices and its own Ctl (as k_init for one source).
+__global__ void k_init_multi(int V, const int32_t* __restrict__ srcs, int32_t* dist, int32_t* qstamp, int32_t* fstamp,
+                             int32_t* q0, int32_t* hv0, int32_t* hb0, const int32_t* __restrict__ off, Ctl* ctl,
+                             int hub_deg, int hub_chunk) {
+  const int g = blockIdx.y;
+  const size_t o = (size_t)g * (size_t)V;
+  const int src = srcs[g];
+  dist += o;
+  qstamp += o;
+  fstamp += o;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    dist[v] = v == src ? 0 : INT_MAX;
+    qstamp[v] = -1;
+    fstamp[v] = -1;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    Ctl* c = ctl + g;
+    qstamp[src] = 0;
+    c->bar.arrived = 0;
+    c->bar.error = 0;
+    for (int k = 0; k < 3; ++k) {
+      c->qcount[k] = 0;
+      c->hcount[k] = 0ull;
+      c->fcount[k] = 0;
+      c->fmin[k] = INT_MAX;
+    }
+    const int d = off[src + 1] - off[src];
+    if (d > hub_deg) {
+      hv0[o] = src;
+      hb0[o] = 0;
+      c->hcount[0] = (1ull << 32) | (unsigned long long)((d + hub_chunk - 1) / hub_chunk);
+    } else {
+      q0[o] = src;
+      c->qcount[0] = 1;
     }
     c->rounds = c->epochs = c->status = 0;
     c->relaxed = 0ull;
@@ -787,6 +861,97 @@ static int sssp_delta(sp_graph* g, const int32_t* w, int32_t src, int32_t* dist_
   return SP_OK;
 }
 
+// Many sources, one cooperative launch per batch (k_delta_multi): a batch of B sources
+// gives each source a group of gsz = (co-resident CTAs) / B CTAs with its own
+// V-strided buffers and Ctl. After each batch, done(rows, b, first) receives the
+// device distance rows of its b sources (source-major, V each; `first` = the batch's
+// first position in srcs).
+int sssp_batch_default() { return ss::BATCH; }
+
+template <class F>
+static int sssp_delta_batches(sp_graph* g, const int32_t* w, const std::vector<int32_t>& srcs, int64_t delta,
+                              int ctas, int local, F done) {
+  SsspPlan* p = g->sssp;
+  cudaStream_t s = g->stream;
+  const int V = g->V, n = (int)srcs.size();
+  if (n == 0) return SP_OK;
+  const bool negative = p->w_min < 0;
+  if (negative || delta <= 0) delta = negative ? (int64_t)INT_MAX : std::max<int64_t>(1, delta);
+  int per_sm = 0;
+  SP_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ss::k_delta_multi, ss::THREADS, 0));
+  const int total = num_sms() * std::max(1, std::min(per_sm, ctas));
+  int B = g->sssp_batch > 0 ? g->sssp_batch : ss::BATCH;
+  B = std::max(1, std::min({B, n, total}));
+  {  // 11 V-sized int32 buffers per source in flight: keep a batch within 1/8 of device memory
+    size_t free_b = 0, total_b = 0;
+    SP_CHECK_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t per_src = (size_t)11 * 4 * (size_t)V + 4096;
+    B = (int)std::max<size_t>(1, std::min<size_t>(B, (total_b / 8) / per_src));
+  }
+  const int gsz = total / B;
+  const size_t BV = (size_t)B * V;
+  Arena A;
+  dspan<int32_t> dist, q0, q1, f0, f1, qs, fs, h0, h1, hb0, hb1, dsrc;
+  dspan<ss::Ctl> ctl;
+  for (dspan<int32_t>* d : {&dist, &q0, &q1, &f0, &f1, &qs, &fs, &h0, &h1, &hb0, &hb1}) A.want(*d, BV);
+  A.want(dsrc, B);
+  A.want(ctl, B);
+  SP_TRY(A.commit());
+  ss::Args a;
+  a.off = g->off.p;
+  a.adj = g->adj.p;
+  a.w = w;
+  a.dist = dist.p;
+  a.q[0] = q0.p;
+  a.q[1] = q1.p;
+  a.f[0] = f0.p;
+  a.f[1] = f1.p;
+  a.hv[0] = h0.p;
+  a.hv[1] = h1.p;
+  a.hbase[0] = hb0.p;
+  a.hbase[1] = hb1.p;
+  a.qstamp = qs.p;
+  a.fstamp = fs.p;
+  a.ctl = ctl.p;
+  a.V = V;
+  a.delta = delta;
+  a.max_rounds = (long long)V * 4 + 64;
+  a.hub_deg = std::min(g->sssp_hub_deg > 0 ? g->sssp_hub_deg : ss::HUB_DEG, ss::HUB_DEG_MAX);
+  a.hub_chunk = g->sssp_hub_chunk > 0 ? g->sssp_hub_chunk : ss::HUB_CHUNK;
+  a.local_edges = 32 * local;
+  std::vector<ss::Ctl> hc(B);
+  int64_t relaxed = 0;
+  for (int k0 = 0; k0 < n; k0 += B) {
+    const int b = std::min(B, n - k0);
+    SP_CHECK_CUDA(cudaMemcpyAsync(dsrc.p, srcs.data() + k0, sizeof(int32_t) * b, cudaMemcpyHostToDevice, s));
+    ss::k_init_multi<<<dim3(std::max(1, num_sms() * 4 / b), b), 256, 0, s>>>(
+        V, dsrc.p, dist.p, qs.p, fs.p, q0.p, h0.p, hb0.p, g->off.p, ctl.p, a.hub_deg, a.hub_chunk);
+    SP_CHECK_LAUNCH();
+    int gs = gsz;
+    void* params[] = {&a, &gs};
+    SP_CHECK_CUDA(cudaLaunchCooperativeKernel((void*)ss::k_delta_multi, b * gsz, ss::THREADS, params, 0, s));
+    g_launches++;
+    SP_TRY(copy_out(hc.data(), ctl.p, sizeof(ss::Ctl) * b, s));
+    for (int i = 0; i < b; ++i) {
+      relaxed += (int64_t)hc[i].relaxed;
+      if (hc[i].status != 0 || hc[i].bar.error) {
+        if (negative && !hc[i].bar.error) {
+          set_error("sp_sssp: no fixed point from source %d after %d rounds (negative cycle)", srcs[k0 + i],
+                    hc[i].rounds);
+          return SP_ERR_NEG_CYCLE;
+        }
+        set_error("sp_sssp: device loop gave up for source %d (status %d, barrier error %d)", srcs[k0 + i],
+                  hc[i].status, hc[i].bar.error);
+        return SP_ERR_TIMEOUT;
+      }
+    }
+    SP_TRY(done((const int32_t*)dist.p, b, k0));
+  }
+  g->sssp_last_relaxed = relaxed;
+  g->sssp_last_batch = B;
+  return SP_OK;
+}
+
 static int sssp_plain(sp_graph* g, const int32_t* w, int32_t src, int32_t* dist_out, int32_t* rounds_out) {
   SsspPlan* p = g->sssp;
   cudaStream_t s = g->stream;
@@ -985,6 +1150,50 @@ extern "C" int sp_sssp_dynamic(sp_graph_h g, int64_t n, const char* type, const 
   g->sssp_last_incremental = 1;
   return sssp_delta(g, w, source, dist, delta, ctas, local, nullptr, d_seeds.p, (int)seeds.size());
 }
+
+extern "C" int sp_sssp_batch(sp_graph_h g, const int32_t* weight, const int32_t* sources, int32_t nsrc,
+                             int32_t* dist) {
+  using namespace sp;
+  if (!g || !sources || nsrc <= 0 || !dist) {
+    set_error("sp_sssp_batch: invalid argument");
+    return SP_ERR_INVALID;
+  }
+  std::vector<int32_t> hs(nsrc);
+  SP_TRY(copy_out(hs.data(), sources, sizeof(int32_t) * nsrc, g->stream));
+  for (int32_t v : hs)
+    if (v < 0 || v >= g->V) {
+      set_error("sp_sssp_batch: source %d out of range [0, %d)", v, g->V);
+      return SP_ERR_INVALID;
+    }
+  const int32_t* w = nullptr;
+  SP_TRY(sssp_prepare(g, weight, &w));
+  int64_t delta = 0;
+  int ctas = 0, local = 0;
+  SP_TRY(sssp_schedule(g, delta, ctas, local));
+  const size_t V = (size_t)g->V;
+  return sssp_delta_batches(g, w, hs, delta, ctas, local, [&](const int32_t* rows, int b, int k0) {
+    return copy_out(dist + (size_t)k0 * V, rows, sizeof(int32_t) * V * b, g->stream);
+  });
+}
+
+namespace sp {
+// Closeness over weighted distances (sp_centrality.cu): every batch's rows are summed
+// on the device, per source, skipping INT_MAX.
+int sssp_batch_sums(sp_graph* g, const int32_t* weight, const std::vector<int32_t>& srcs,
+                    void (*sum_rows)(const int32_t*, int, int, unsigned long long*, cudaStream_t),
+                    unsigned long long* d_sums) {
+  const int32_t* w = nullptr;
+  SP_TRY(sssp_prepare(g, weight, &w));
+  int64_t delta = 0;
+  int ctas = 0, local = 0;
+  SP_TRY(sssp_schedule(g, delta, ctas, local));
+  return sssp_delta_batches(g, w, srcs, delta, ctas, local, [&](const int32_t* rows, int b, int k0) {
+    sum_rows(rows, g->V, b, d_sums + k0, g->stream);
+    SP_CHECK_LAUNCH();
+    return SP_OK;
+  });
+}
+}  // namespace sp
 
 extern "C" int sp_sssp_features(sp_graph_h g, const int32_t* weight, double delta_mult, int32_t ctas_per_sm,
                                 int32_t local_steps, float* x) {

@@ -15,12 +15,13 @@ struct GridBar {
   int error;  // nonzero once any CTA gave up waiting
 };
 
-__device__ __forceinline__ bool grid_barrier(GridBar* gb, unsigned long long limit = (1ull << 24)) {
+// The same barrier over a group of nb co-resident CTAs that share gb; `first` marks
+// exactly one CTA of the group.
+__device__ __forceinline__ bool group_barrier(GridBar* gb, unsigned int nb, bool first,
+                                              unsigned long long limit = (1ull << 24)) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    const unsigned int nb = gridDim.x * gridDim.y * gridDim.z;
-    const bool first = (blockIdx.x | blockIdx.y | blockIdx.z) == 0;
     const unsigned int inc = first ? (0x80000000u - (nb - 1u)) : 1u;
     __threadfence();
     const unsigned int old = atomicAdd(&gb->arrived, inc);
@@ -41,6 +42,10 @@ __device__ __forceinline__ bool grid_barrier(GridBar* gb, unsigned long long lim
   }
   __syncthreads();
   return s_ok != 0;
+}
+
+__device__ __forceinline__ bool grid_barrier(GridBar* gb, unsigned long long limit = (1ull << 24)) {
+  return group_barrier(gb, gridDim.x * gridDim.y * gridDim.z, (blockIdx.x | blockIdx.y | blockIdx.z) == 0, limit);
 }
 
 }  // namespace sp

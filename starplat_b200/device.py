@@ -292,6 +292,21 @@ class DeviceGraph:
                                        ctypes.byref(rounds)))
         return out, int(rounds.value)
 
+    def sssp_batch(self, sources, weight=None, out=None):
+        """Distances from every source (int32, host or device) in batched cooperative
+        launches, one CTA group per source: int32[nsrc][V], row k from sources[k]
+        (host array, or `out` of that size on the host or the device)."""
+        _ensure_scheduler()
+        if isinstance(sources, (list, tuple)):
+            sources = np.asarray(sources, np.int32)
+        n = int(sources.shape[0])
+        if out is None:
+            out = np.empty((n, self.V), np.int32)
+        if weight is not None and str(weight.dtype) not in ("int32", "torch.int32"):
+            raise TypeError("weights must be int32")
+        check("sp_sssp_batch", lib().sp_sssp_batch(self.handle, _ptr(weight), _ptr(sources), n, _ptr(out)))
+        return out
+
     def bc(self, sources, out=None, variant: int = _lib.SP_BC_BATCHED):
         """Brandes BC over distinct `sources` (int32, host or device); float32[V]."""
         if out is None:

@@ -30,32 +30,51 @@ def split_sources(sources, world: int, rank: int) -> np.ndarray:
     return s[lo:hi]
 
 
-def sum_over_sources(V: int, sources, rep: Replicas, compute: Callable[[np.ndarray], np.ndarray]) -> np.ndarray:
-    """A float32[V] that is a sum over `sources`: this rank computes its slice with
-    `compute` (slice -> float32[V]), then the partial vectors are summed over the ranks.
-    Every rank returns the full result."""
+def sum_over_sources(V: int, sources, rep: Replicas, compute: Callable, out=None):
+    """A float32[V] that is a sum over `sources`: this rank computes its slice, then the
+    partial vectors are summed over the ranks, and every rank returns the full result.
+    Without `out`, compute(slice) returns a float32[V] array and the result is numpy.
+    With `out` (a float32[V] torch tensor on the backend's device: this rank's GPU under
+    NCCL), compute(slice, out) writes the slice's vector into it and the sum is taken in
+    place, so the vector never leaves the device; `out` is returned."""
     mine = split_sources(sources, rep.world, rep.rank)
+    if out is not None:
+        if mine.shape[0]:
+            compute(mine, out)
+        else:
+            out.zero_()
+        return rep.all_reduce_sum(out)
     part = compute(mine) if mine.shape[0] else np.zeros(V, np.float32)
     return rep.all_reduce_sum(np.ascontiguousarray(part, np.float32))
 
 
-def bc_sharded(V: int, sources, rep: Replicas, compute: Callable[[np.ndarray], np.ndarray]) -> np.ndarray:
-    """BC[V] over all `sources` (compute: DeviceGraph.bc on a GPU)."""
-    return sum_over_sources(V, sources, rep, compute)
+def bc_sharded(V: int, sources, rep: Replicas, compute: Callable, out=None):
+    """BC[V] over all `sources` (compute: DeviceGraph.bc on a GPU; see sum_over_sources
+    for `out`)."""
+    return sum_over_sources(V, sources, rep, compute, out)
 
 
-def closeness_on_gpus(dg, sources, rep: Optional[Replicas] = None, weighted: bool = True, weight=None) -> np.ndarray:
+def closeness_on_gpus(dg, sources, rep: Optional[Replicas] = None, weighted: bool = True, weight=None, out=None):
     """Compute_CC (weighted, the graph's edgeLen or `weight`) or Compute_CC_Unweighted
-    over `sources`, split over the ranks; every rank returns CC[V]."""
+    over `sources`, split over the ranks; every rank returns CC[V] (in `out`, a device
+    tensor under NCCL, when given)."""
     rep = rep or Replicas()
     if weighted:
+        if out is not None:
+            return sum_over_sources(dg.V, sources, rep, lambda s, o: dg.closeness(s, weight=weight, out=o), out)
         return sum_over_sources(dg.V, sources, rep, lambda s: dg.closeness(s, weight=weight))
+    if out is not None:
+        return sum_over_sources(dg.V, sources, rep, lambda s, o: dg.closeness_unweighted(s, out=o), out)
     return sum_over_sources(dg.V, sources, rep, lambda s: dg.closeness_unweighted(s))
 
 
-def bc_on_gpus(dg, sources, rep: Optional[Replicas] = None) -> np.ndarray:
-    """bc_sharded with this rank's DeviceGraph doing its slice."""
+def bc_on_gpus(dg, sources, rep: Optional[Replicas] = None, out=None):
+    """bc_sharded with this rank's DeviceGraph doing its slice; with `out` (a float32[V]
+    tensor on this rank's GPU) the slice's BC is written there by the kernel and summed
+    over the ranks in place by NCCL."""
     rep = rep or Replicas()
+    if out is not None:
+        return bc_sharded(dg.V, sources, rep, lambda s, o: dg.bc(s, out=o), out)
     return bc_sharded(dg.V, sources, rep, lambda s: dg.bc(s))
 
 
@@ -66,9 +85,14 @@ def tc_sharded(rep: Replicas, compute: Callable[[int, int], int]) -> int:
     return int(rep.all_reduce_sum(mine)[0])
 
 
-def lcc_sharded(V: int, rep: Replicas, compute: Callable[[int, int], np.ndarray]) -> np.ndarray:
+def lcc_sharded(V: int, rep: Replicas, compute: Callable, out=None):
     """staticClusteringCoeff over the ranks: compute(part, nparts) gives this rank's
-    int32[V] counts, and the vectors are summed (int32, exact)."""
+    int32[V] counts, and the vectors are summed (int32, exact). With `out` (an int32[V]
+    tensor on the backend's device) compute(part, nparts, out) writes into it and the
+    sum is taken in place."""
+    if out is not None:
+        compute(rep.rank, rep.world, out)
+        return rep.all_reduce_sum(out)
     mine = np.ascontiguousarray(compute(rep.rank, rep.world), np.int32)
     assert mine.shape == (V,)
     return rep.all_reduce_sum(mine)
@@ -80,7 +104,9 @@ def tc_on_gpus(dg, rep: Optional[Replicas] = None) -> int:
     return tc_sharded(rep, dg.tc_part)
 
 
-def clustering_coeff_on_gpus(dg, rep: Optional[Replicas] = None) -> np.ndarray:
-    """lcc_sharded with this rank's DeviceGraph."""
+def clustering_coeff_on_gpus(dg, rep: Optional[Replicas] = None, out=None):
+    """lcc_sharded with this rank's DeviceGraph (the counts stay on the GPU in `out`)."""
     rep = rep or Replicas()
+    if out is not None:
+        return lcc_sharded(dg.V, rep, lambda r, n, o: dg.clustering_coeff_part(r, n, out=o), out)
     return lcc_sharded(dg.V, rep, lambda r, n: dg.clustering_coeff_part(r, n))

@@ -1,11 +1,14 @@
-"""Replica plumbing for runs on several GPUs of one node (one process per GPU,
+"""Process-group plumbing for runs on several GPUs of one node (one process per GPU,
 launched by torchrun, which sets RANK / WORLD_SIZE / LOCAL_RANK / MASTER_*).
 
-Every entry point of this library runs one graph on one GPU, so N GPUs run N
-independent replicas with no data-path collective. The only collectives are the
-barrier around a timed region and the reductions of its result: a whole-job rate is
-the units all ranks processed over the SLOWEST rank's time. NCCL carries them on
-GPUs; gloo does on the host (the CPU tests run two ranks that way).
+The single-graph entry points run one graph per GPU, so N GPUs run N replicas with
+no data-path collective; the timed runs need only the barrier around the timed region
+and the reductions of its result (a whole-job rate is the units all ranks processed
+over the SLOWEST rank's time). The algorithms split over the ranks (distributed.py)
+use the data-path collectives here: an in-place sum of a per-vertex vector and an
+all-gather of per-rank slices, both on device tensors when NCCL carries them, so no
+vector leaves the GPU. gloo carries them on the host (the CPU tests run 2 and 3 ranks
+that way).
 """
 from __future__ import annotations
 
@@ -59,16 +62,40 @@ class Replicas:
         return float(x) if self._dist is None else self._reduce(x, self._dist.ReduceOp.SUM)
 
     def all_reduce_sum(self, a):
-        """Element-wise sum of a float32 numpy array over all ranks (every rank gets it)."""
+        """Element-wise sum over all ranks, every rank getting the result. A torch tensor
+        is reduced in place where it lives (a CUDA tensor under NCCL, a host tensor under
+        gloo) and returned; a numpy array goes through a tensor on the backend's device
+        and comes back as numpy."""
         if self._dist is None:
             return a
-        import numpy as np
         import torch
+
+        if isinstance(a, torch.Tensor):
+            self._dist.all_reduce(a, op=self._dist.ReduceOp.SUM)
+            return a
+        import numpy as np
 
         dev = "cuda" if self.backend == "nccl" else "cpu"
         t = torch.from_numpy(np.ascontiguousarray(a)).to(dev)
         self._dist.all_reduce(t, op=self._dist.ReduceOp.SUM)
         return t.cpu().numpy()
+
+    def all_gather_into(self, full, part) -> None:
+        """full[r * n : (r + 1) * n] = rank r's `part` (n elements each) on every rank:
+        torch tensors on the backend's device, full holding world * n elements."""
+        if self._dist is None:
+            if full.data_ptr() != part.data_ptr():
+                full[: part.numel()].copy_(part)
+            return
+        self._dist.all_gather_into_tensor(full, part)
+
+    def device(self):
+        """Where this rank's collective tensors live: its GPU under NCCL, else the host."""
+        import torch
+
+        if self.backend == "nccl":
+            return torch.device("cuda", torch.cuda.current_device())
+        return torch.device("cpu")
 
     def whole_job_rate(self, units: float, seconds: float) -> float:
         """Units all ranks processed per second of the slowest rank."""

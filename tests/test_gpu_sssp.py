@@ -193,3 +193,44 @@ def test_sssp_at_scale(case):
         src = 123457
     check(g, src)
     check(g, src, variant=_lib.SP_SSSP_PLAIN)
+
+
+@pytest.mark.parametrize("batch", [1, 3, 16, 64])
+def test_sssp_batch_one_launch_per_batch_is_exact(batch):
+    # many sources, each on its own CTA group of one cooperative launch per batch:
+    # every row equals the single-source distances, for any batch size
+    graphs = [weighted(G.rmat(12, 16, seed=5, directed=True), 1, 100), weighted(G.grid(40, 50), 1, 1000),
+              weighted(G.rmat(11, 8, seed=3), 1, 50)]
+    for g in graphs:
+        srcs = G.pick_sources(g, 21, seed=batch)
+        with DeviceGraph.from_csr(g) as dg:
+            dg.tune_set("sssp.batch", batch)
+            rows = dg.sssp_batch(srcs)
+            assert dg.tune_get("sssp.last_batch") == min(batch, len(srcs))
+        for k, s in enumerate(srcs):
+            ref = O.sssp(g.indexofNodes, g.edgeList, g.edgeLen, int(s))
+            assert np.array_equal(rows[k], ref), (g.name, batch, k)
+
+
+def test_sssp_batch_device_rows_negative_weights_and_errors():
+    import torch
+
+    # negative weights without negative cycles: every group runs queue Bellman-Ford
+    g = from_pairs(5, [[0, 1], [1, 2], [0, 2], [2, 3], [3, 4], [1, 4]], name="neg")
+    g.edgeLen = np.array([4, -2, 3, 1, 2, 7], np.int32)
+    with DeviceGraph.from_csr(g) as dg:
+        rows = dg.sssp_batch(np.array([0, 1, 2, 4], np.int32))
+        for k, s in enumerate([0, 1, 2, 4]):
+            assert np.array_equal(rows[k], O.sssp(g.indexofNodes, g.edgeList, g.edgeLen, s))
+    g = weighted(G.rmat(13, 8, seed=2, directed=True), 1, 100)
+    srcs = G.pick_sources(g, 40, seed=2)
+    with DeviceGraph.from_csr(g) as dg:
+        out = torch.empty((len(srcs), g.V), dtype=torch.int32, device="cuda")
+        dg.sssp_batch(torch.from_numpy(srcs).cuda(), out=out)
+        got = out.cpu().numpy()
+        for k in (0, 17, 39):
+            assert np.array_equal(got[k], O.sssp(g.indexofNodes, g.edgeList, g.edgeLen, int(srcs[k])))
+        with pytest.raises(_lib.SPError):
+            dg.sssp_batch(np.array([0, g.V], np.int32))
+        with pytest.raises(_lib.SPError):
+            dg.tune_set("sssp.batch", 5000)

@@ -213,3 +213,61 @@ def test_triangle_parts_over_ranks_sum_to_the_whole(tmp_path, world):
     for r in range(world):
         assert int(np.load(tmp_path / f"tc{r}.npy")[0]) == want_tc
         assert np.array_equal(np.load(tmp_path / f"cf{r}.npy"), want_cf)
+
+
+def _device_sum_rank_main(rank, world, port, out_dir):
+    # the in-place path the GPUs take: each rank's slice is written into a tensor, which is
+    # summed where it lives (a host tensor under gloo, a CUDA tensor under NCCL); plus the
+    # all-gather of equal slices
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port), "RANK": str(rank),
+                       "WORLD_SIZE": str(world), "LOCAL_RANK": str(rank)})
+    sys.path.insert(0, ROOT)
+    import numpy as np
+    import torch
+
+    from oracle import oracle as O
+    from starplat_b200 import generators as G
+    from starplat_b200.distributed import bc_sharded, lcc_sharded
+    from starplat_b200.replicas import Replicas
+
+    g = G.rmat(9, 8, seed=4)
+    srcs = G.pick_sources(g, 37, seed=1)
+    rep = Replicas(backend="gloo", timeout_s=60)
+    assert rep.device().type == "cpu"
+    out = torch.full((g.V,), float("nan"), dtype=torch.float32)
+
+    def compute(s, o):
+        o.copy_(torch.from_numpy(O.bc(g.indexofNodes, g.edgeList, s).astype(np.float32)))
+
+    got = bc_sharded(g.V, srcs, rep, compute, out=out)
+    assert got is out
+    cf = torch.zeros(g.V, dtype=torch.int32)
+    lcc_sharded(g.V, rep, lambda r, n, o: o.copy_(torch.from_numpy(_lcc_part(g.indexofNodes, g.edgeList, r, n))),
+                out=cf)
+    part = torch.full((5,), float(rank), dtype=torch.float32)
+    full = torch.empty(5 * world, dtype=torch.float32)
+    rep.all_gather_into(full, part)
+    rep.close()
+    np.save(os.path.join(out_dir, f"bc{rank}.npy"), out.numpy())
+    np.save(os.path.join(out_dir, f"cf{rank}.npy"), cf.numpy())
+    np.save(os.path.join(out_dir, f"ag{rank}.npy"), full.numpy())
+
+
+def test_device_tensor_sums_over_ranks(tmp_path):
+    import numpy as np
+
+    from oracle import oracle as O
+    from starplat_b200 import generators as G
+
+    world = 3
+    mp.start_processes(_device_sum_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    g = G.rmat(9, 8, seed=4)
+    srcs = G.pick_sources(g, 37, seed=1)
+    ref = O.bc(g.indexofNodes, g.edgeList, srcs)
+    want_cf = O.lcc(g.indexofNodes, g.edgeList)
+    for r in range(world):
+        out = np.load(tmp_path / f"bc{r}.npy").astype(np.float64)
+        assert np.all(np.abs(out - ref) <= 1e-5 * np.abs(ref) + 1e-6)
+        assert np.array_equal(np.load(tmp_path / f"cf{r}.npy"), want_cf)
+        assert np.array_equal(np.load(tmp_path / f"ag{r}.npy"), np.repeat(np.arange(world, dtype=np.float32), 5))
