@@ -1086,6 +1086,41 @@ def main():
     e2e = {"value": rep.sum(E * e_it) / e_s / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h, "ms_per_step": 1e3 * e_s / e_steps}
 
+    # ---- N > 1: the same graph split over the ranks by vertices (strong scaling), one
+    # all-gather of the contrib blocks and one all-reduce of the diff per iteration
+    split = None
+    if world > 1:
+        from starplat_b200.distributed import pagerank_on_gpus
+
+        split_out = torch.empty(V, dtype=torch.float32, device="cuda")
+        for _ in range(2):
+            pagerank_on_gpus(dg, rep, BETA, DELTA, MAX_ITER, out=split_out)
+        barrier()
+        torch.cuda.synchronize()
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        sp_steps = max(1, min(args.steps, 5))
+        sp_it = 0
+        for _ in range(sp_steps):
+            _, it_s, _ = pagerank_on_gpus(dg, rep, BETA, DELTA, MAX_ITER, out=split_out)
+            sp_it += it_s
+        s1.record(stream)
+        torch.cuda.synchronize()
+        sp_ms = max_over_ranks(s0.elapsed_time(s1)) / sp_steps
+        split = {"workload": f"pagerank rmat{PR_SCALE} split over {world} GPUs by vertices",
+                 "value": E * (sp_it / sp_steps) / (sp_ms / 1e3) / 1e9, "unit": "GTEPS", "ms_per_step": sp_ms,
+                 "iterations": sp_it // sp_steps, "scaling": "strong",
+                 "parallelism": f"1-D vertex partition over {world} GPUs: NCCL all-gather of contrib blocks and "
+                                "all-reduce of the diff per iteration, stop test on the device"}
+        if rank == 0 and not args.no_parity:
+            from oracle import oracle as O
+
+            exact, _, _ = O.pagerank(g.indexofNodes, g.rev_indexofNodes, g.srcList, 0.0, DELTA, it_s,
+                                     nthreads=O.num_threads())
+            split["parity"] = {"pagerank_l1_vs_fp64": float(np.abs(split_out.cpu().numpy().astype(np.float64)
+                                                                   - exact).sum()), "tolerance": 1e-6}
+
     cpu_ok = rank == 0 and world == 1 and not args.no_cpu_baseline
     cpu = cpu_pagerank(g, 3) if cpu_ok else None
     if cpu:
@@ -1107,6 +1142,8 @@ def main():
                 "config": cfg, "iterations": it_total // args.steps, "graph_gen_s": round(gen_s, 2),
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
                 "parity": parity, "plain": pr_plain, "algorithms": extras}
+        if split:
+            line["pagerank_split"] = split
         print(json.dumps(line), flush=True)
     rep.close()
 

@@ -208,6 +208,35 @@ int sp_closeness_unweighted(sp_graph_h g, const int32_t* sources, int32_t nsrc, 
 int sp_pagerank(sp_graph_h g, float beta, float delta, int32_t maxIter, float* pageRank,
                 int32_t* iterations, double* final_diff, int32_t variant);
 
+/* PageRank split over the GPUs of a node by vertices, one part per rank; replaces the
+ * host-staged copies of the reference's multi-GPU generator
+ * (backend_multigpu/dsl_cpp_generator.cpp:604-678). Every rank holds the whole graph
+ * and owns the rows of one part; the caller's collectives run between the calls, on
+ * the same stream (sp_graph_set_stream), with device buffers:
+ *   begin    part in [0, nparts); con0 / con1: the caller's ping-pong contrib buffers,
+ *            DEVICE, nparts * S floats each; diff: one DEVICE double; *slice = S.
+ *   iterate(k), k = 0, 1, ...: the part's rows of iteration k: reads con[k % 2], writes
+ *            the part's block con[(k + 1) % 2][part * S, (part + 1) * S) and its L1 diff
+ *            into *diff. The caller then all-gathers the blocks of con[(k + 1) % 2]
+ *            (equal S-float blocks, in part order) and sums *diff over the ranks.
+ *   decide   the stop test on the summed diff (diff > beta and fewer than maxIter
+ *            iterations: go on), on the device; later iterate calls of a finished run
+ *            return at once, so a caller may queue several iterations before it reads
+ *            the state (one synchronisation per several iterations).
+ *   state    iterations run, done flag and the last summed diff (synchronises).
+ *   ranks    the part's S ranks (its block, in the split plan's order) into slice,
+ *            host or device; the caller all-gathers them into nparts * S floats.
+ *   finish   that gathered DEVICE vector to pageRank[V] in the caller's vertex order.
+ * With the same beta, delta and maxIter every rank reaches the ranks of sp_pagerank to
+ * FP32 rounding of the per-row FP64 sums. */
+int sp_pagerank_part_begin(sp_graph_h g, int32_t part, int32_t nparts, float beta, float delta, int32_t maxIter,
+                           float* con0, float* con1, double* diff, int32_t* slice);
+int sp_pagerank_part_iterate(sp_graph_h g, int32_t k);
+int sp_pagerank_part_decide(sp_graph_h g);
+int sp_pagerank_part_state(sp_graph_h g, int32_t* iterations, int32_t* done, double* diff);
+int sp_pagerank_part_ranks(sp_graph_h g, float* slice);
+int sp_pagerank_part_finish(sp_graph_h g, const float* ranks, float* pageRank);
+
 /* ---- single-source shortest paths --------------------------------------------
  * Replaces generated `void Compute_SSSP(graph& g, int* dist, int* weight, int src)`
  * (DSL staticDSLCodes/sssp_dslV3:1-26). weight[E] in forward-CSR order (the drivers
@@ -296,6 +325,21 @@ int sp_mlp_train(float* params, const float* X, const float* T, int32_t N, int32
 /* Load (params != NULL) or unload (params == NULL) the process-wide scheduling model;
  * feat_mean/feat_scale normalise inputs: x' = (x - mean) * scale. */
 int sp_sched_load(const float* params, const float* feat_mean, const float* feat_scale);
+/* No counterpart in the reference (the learned per-iteration schedule). Load or unload
+ * the process-wide SSSP epoch model: the same network shape, scoring for every bucket
+ * advance of a delta-stepping solve each width factor (1/4, 1/2, 1, 2, 4, 8 times the
+ * call's delta) from inputs the kernel computes on the device (far-pile size, rounds
+ * and relaxations of the previous epoch, progress, the previous factor, graph shape);
+ * the kernel takes the factor with the lowest predicted log cost per unit of distance.
+ * Knob "sssp.epoch": -1 (default) learned when a model is loaded, else fixed width;
+ * 0 fixed; 1 learned; 2 a seeded pseudo-random factor per epoch ("sssp.epoch_seed",
+ * exploration). Distances are exact under any width sequence. */
+int sp_sched_epoch_load(const float* params, const float* feat_mean, const float* feat_scale);
+/* With knob "sssp.trace" = 1 and a per-epoch policy, the last single-source solve's
+ * epochs: records[k][16] = the SP_MLP_IN inputs of the chosen factor, the factor, the
+ * distance the threshold advanced, padding; times[k] = device timer (ns) at advance k,
+ * times[n] at the end. *n = epochs recorded; up to cap records are copied. */
+int sp_sssp_epoch_trace(sp_graph_h g, float* records, unsigned long long* times, int32_t cap, int32_t* n);
 /* Replaces the generated Batch block of DynSSSP (DSL dynamicDSLCodes/dynamicBatchSSSP:
  * OnDelete + updateCSRDel + Decremental, then OnAdd + updateCSRAdd + Incremental): one
  * batch of edge updates as in sp_graph_update, then the distances from source on the

@@ -79,6 +79,12 @@ SIGNATURES = {
     "sp_tc_part": (ctypes.c_int, [vp, i32, i32, P(i64)]),
     "sp_clustering_coeff_part": (ctypes.c_int, [vp, i32, i32, vp]),
     "sp_pagerank": (ctypes.c_int, [vp, f32, f32, i32, vp, P(i32), P(f64), i32]),
+    "sp_pagerank_part_begin": (ctypes.c_int, [vp, i32, i32, f32, f32, i32, vp, vp, vp, P(i32)]),
+    "sp_pagerank_part_iterate": (ctypes.c_int, [vp, i32]),
+    "sp_pagerank_part_decide": (ctypes.c_int, [vp]),
+    "sp_pagerank_part_state": (ctypes.c_int, [vp, P(i32), P(i32), P(f64)]),
+    "sp_pagerank_part_ranks": (ctypes.c_int, [vp, vp]),
+    "sp_pagerank_part_finish": (ctypes.c_int, [vp, vp, vp]),
     "sp_sssp": (ctypes.c_int, [vp, vp, i32, vp, i64, i32, P(i32)]),
     "sp_sssp_batch": (ctypes.c_int, [vp, vp, vp, i32, vp]),
     "sp_bc": (ctypes.c_int, [vp, vp, i32, vp, i32]),
@@ -93,6 +99,8 @@ SIGNATURES = {
     "sp_mlp_grad": (ctypes.c_int, [vp, vp, vp, i32, vp, vp]),
     "sp_mlp_train": (ctypes.c_int, [vp, vp, vp, i32, i32, f32, vp]),
     "sp_sched_load": (ctypes.c_int, [vp, vp, vp]),
+    "sp_sched_epoch_load": (ctypes.c_int, [vp, vp, vp]),
+    "sp_sssp_epoch_trace": (ctypes.c_int, [vp, vp, vp, i32, P(i32)]),
     "sp_sssp_features": (ctypes.c_int, [vp, vp, f64, i32, i32, vp]),
     "sp_pagerank_noalloc": (ctypes.c_int, [vp, vp, vp, i32, i64, f32, f32, i32, vp, P(i32), vp]),
 }

@@ -606,6 +606,26 @@ int sp_tune_set(sp_graph_h g, const char* key, int64_t value) {
     g->pr_order = (int32_t)value;
     return SP_OK;
   }
+  if (!strcmp(key, "sssp.epoch")) {
+    if (value < -1 || value > 2) {
+      set_error("sp_tune_set: sssp.epoch must be -1, 0, 1 or 2");
+      return SP_ERR_INVALID;
+    }
+    g->sssp_epoch = (int32_t)value;
+    return SP_OK;
+  }
+  if (!strcmp(key, "sssp.epoch_seed")) {
+    g->sssp_epoch_seed = (int32_t)value;
+    return SP_OK;
+  }
+  if (!strcmp(key, "sssp.trace")) {
+    if (value != 0 && value != 1) {
+      set_error("sp_tune_set: sssp.trace must be 0 or 1");
+      return SP_ERR_INVALID;
+    }
+    g->sssp_trace = (int32_t)value;
+    return SP_OK;
+  }
   if (!strcmp(key, "sssp.batch")) {
     if (value < 0 || value > 1024) {
       set_error("sp_tune_set: sssp.batch must be in [0, 1024]");
@@ -728,6 +748,18 @@ int sp_tune_get(sp_graph_h g, const char* key, int64_t* value) {
   }
   if (!strcmp(key, "sssp.last_batch")) {
     *value = g->sssp_last_batch;
+    return SP_OK;
+  }
+  if (!strcmp(key, "sssp.epoch")) {
+    *value = g->sssp_epoch;
+    return SP_OK;
+  }
+  if (!strcmp(key, "sssp.last_epochs")) {
+    *value = g->sssp_last_epochs;
+    return SP_OK;
+  }
+  if (!strcmp(key, "sssp.last_epolicy")) {
+    *value = g->sssp_last_epolicy;
     return SP_OK;
   }
   if (!strcmp(key, "sssp.ctas_per_sm")) {

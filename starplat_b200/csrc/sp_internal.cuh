@@ -174,6 +174,11 @@ struct sp_graph {
   int32_t sssp_hub_chunk = 0;  // SSSP: edges per piece (0 = default)
   int32_t sssp_local = -1;     // SSSP: warp cascade budget in 32-edge steps per round (-1 = default, 0 = off)
   int32_t sssp_batch = 0;      // batched SSSP: sources per cooperative launch (0 = default)
+  int32_t sssp_epoch = -1;     // SSSP per-epoch width: -1 learned if an epoch model is loaded, 0 fixed, 1 learned, 2 explore
+  int32_t sssp_epoch_seed = 0;  // exploration seed
+  int32_t sssp_trace = 0;      // 1: record the per-epoch trace of single-source solves
+  int32_t sssp_last_epochs = 0;  // bucket advances of the last single-source solve
+  int32_t sssp_last_epolicy = 0;  // the width policy the last solve ran
   int32_t sssp_last_batch = 0;  // sources per launch of the last batched run (reporting)
   int32_t tc_cta_warps = -1;  // TC: warps per CTA of the shared-bitmap kernel (-1 = default, 0 = off)
   int32_t bc_batch = 0;

@@ -186,8 +186,19 @@ std::mutex g_mu;
 std::vector<float> g_params;   // empty = no model: fixed heuristic
 unsigned g_generation = 0;     // bumped by every sp_sched_load
 std::vector<float> g_mean, g_scale;
+// the per-epoch bucket-width model of SSSP (same network shape, its own inputs)
+std::vector<float> g_eparams;  // params, mean, scale packed; empty = no model
+unsigned g_egeneration = 0;
 
 }  // namespace mlp
+
+// The epoch model packed for the device (params, feature mean, feature scale) and its
+// generation (0 = none loaded).
+unsigned mlp_epoch_model(std::vector<float>& packed) {
+  std::lock_guard<std::mutex> lock(mlp::g_mu);
+  packed = mlp::g_eparams;
+  return mlp::g_eparams.empty() ? 0u : mlp::g_egeneration;
+}
 
 // Score candidate rows X[n][IN] with the loaded model (host in, host out).
 // Returns SP_ERR_UNSUPPORTED when no model is loaded.
@@ -299,5 +310,22 @@ extern "C" int sp_sched_load(const float* params, const float* feat_mean, const 
   mlp::g_params.assign(params, params + mlp::P);
   mlp::g_mean.assign(feat_mean, feat_mean + mlp::IN);
   mlp::g_scale.assign(feat_scale, feat_scale + mlp::IN);
+  return SP_OK;
+}
+
+extern "C" int sp_sched_epoch_load(const float* params, const float* feat_mean, const float* feat_scale) {
+  std::lock_guard<std::mutex> lock(mlp::g_mu);
+  ++mlp::g_egeneration;
+  if (!params) {
+    mlp::g_eparams.clear();
+    return SP_OK;
+  }
+  if (!feat_mean || !feat_scale) {
+    set_error("sp_sched_epoch_load: feature normalisation required");
+    return SP_ERR_INVALID;
+  }
+  mlp::g_eparams.assign(params, params + mlp::P);
+  mlp::g_eparams.insert(mlp::g_eparams.end(), feat_mean, feat_mean + mlp::IN);
+  mlp::g_eparams.insert(mlp::g_eparams.end(), feat_scale, feat_scale + mlp::IN);
   return SP_OK;
 }

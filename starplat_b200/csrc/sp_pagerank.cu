@@ -99,6 +99,13 @@ struct PrPlan {
   dspan<pr::State> state;
   int hot = -1;           // hot id count the plan was built for
   int order = 0;          // vertex order (k_deg_keys)
+  int nparts = 1, part_idx = 0;  // split plan: part part_idx of nparts (lay())
+  int S = 0, Vp = 0;      // ids per part and the id space (nparts * S; V when not split)
+  int lo = 0, hi = 0;     // this part's rows
+  float pbeta = 0, pdelta = 0;  // split run: stop test and damping of sp_pagerank_part_begin
+  int pmax_iter = 0;
+  float* pcon[2] = {nullptr, nullptr};  // split run: the caller's all-gathered contrib buffers
+  double* pdiff = nullptr;              // split run: the caller's diff (this part's, then the sum)
   bool two_phase() const { return task_base[0][4] > 0 || n_chunks[0] > 0; }
   cudaGraphExec_t exec = nullptr;
   int exec_iters = 0;
@@ -138,6 +145,7 @@ struct IterArgs {
   double beta;
   int max_iter;
   int l1_hot;   // GH = 1: relabelled source ids below this allocate in L1
+  double* diff_out;  // split plan: this part's L1 diff of the iteration (summed over parts by the caller)
 };
 
 __device__ __forceinline__ double finalize_row(const IterArgs& a, int r, double sum,
@@ -412,6 +420,7 @@ __device__ __forceinline__ void phase_body(const IterArgs& a, const G& gather, c
     const double total = block_sum<NT>(p, s_red);
     if (tid == 0) {
       const double all = total + *(volatile double*)&a.st->extra;
+      if (a.diff_out) *a.diff_out = all;
       const int it = a.st->iter + 1;
       a.st->iter = it;
       a.st->diff = all;
@@ -472,13 +481,26 @@ __global__ void k_deg_keys(int V, int order, const int32_t* __restrict__ off, co
   }
 }
 
-__global__ void k_relabel_rows(int V, const int32_t* __restrict__ inv, const int32_t* __restrict__ off,
+// Vertex ids of a plan split into np parts (sp_pagerank_part_*): out-degree rank k goes
+// to part k % np at position k / np, and part r's vertices are the id range
+// [r * S, r * S + count_r). Every part's slice of contrib is then one contiguous block
+// of S floats (what an all-gather of equal blocks needs), and the ranks' heavy
+// vertices are dealt round-robin, so the parts' in-edge counts stay close. np = 1 is
+// the identity.
+__device__ __forceinline__ int lay(int k, int np, int S) { return np == 1 ? k : (k % np) * S + k / np; }
+
+__global__ void k_relabel_rows(int V, int np, int S, const int32_t* __restrict__ inv, const int32_t* __restrict__ off,
                                int32_t* __restrict__ new_id, int32_t* __restrict__ od) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < V; k += gridDim.x * blockDim.x) {
     const int v = inv[k];
-    new_id[v] = k;
+    new_id[v] = lay(k, np, S);
     od[k] = off[v + 1] - off[v];
   }
+}
+
+// Out-degrees moved from rank order to the plan's ids (pads of a split plan keep 0).
+__global__ void k_od_layout(int V, int np, int S, const int32_t* __restrict__ odk, int32_t* __restrict__ od) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < V; k += gridDim.x * blockDim.x) od[lay(k, np, S)] = odk[k];
 }
 
 // Stable transpose, step 1: the (new dst, new src) pair of every edge, written in
@@ -487,7 +509,7 @@ __global__ void k_relabel_rows(int V, const int32_t* __restrict__ inv, const int
 // lanes (an exclusive scan of the out-degrees), 32 edges per step and four steps'
 // loads in flight together, so short rows do not leave lanes idle. Sources of more than 1024 out-edges are listed for
 // k_fwd_pairs_big instead.
-__global__ void k_fwd_pairs(int V, const int32_t* __restrict__ inv, const int32_t* __restrict__ new_id,
+__global__ void k_fwd_pairs(int V, int np, int S, const int32_t* __restrict__ inv, const int32_t* __restrict__ new_id,
                             const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
                             const int32_t* __restrict__ offp, const int32_t* __restrict__ od,
                             int32_t* __restrict__ dst, int32_t* __restrict__ src, int32_t* __restrict__ big,
@@ -528,7 +550,7 @@ __global__ void k_fwd_pairs(int V, const int32_t* __restrict__ inv, const int32_
         const int jb = __shfl_sync(FULL, b, j), jd = __shfl_sync(FULL, d, j), je = __shfl_sync(FULL, excl, j);
         pos[u] = t < total ? jd + (t - je) : -1;
         nb[u] = t < total ? adj[jb + (t - je)] : 0;
-        row[u] = k0 + j;
+        row[u] = lay(k0 + j, np, S);
       }
 #pragma unroll
       for (int u = 0; u < U; ++u) nb[u] = pos[u] >= 0 ? new_id[nb[u]] : 0;
@@ -543,7 +565,7 @@ __global__ void k_fwd_pairs(int V, const int32_t* __restrict__ inv, const int32_
 }
 
 // Rows of more than 1024 out-edges: a CTA per row, four edges per thread in flight.
-__global__ void k_fwd_pairs_big(const int32_t* __restrict__ inv, const int32_t* __restrict__ new_id,
+__global__ void k_fwd_pairs_big(int np, int S, const int32_t* __restrict__ inv, const int32_t* __restrict__ new_id,
                                 const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
                                 const int32_t* __restrict__ offp, const int32_t* __restrict__ od,
                                 int32_t* __restrict__ dst, int32_t* __restrict__ src,
@@ -564,7 +586,7 @@ __global__ void k_fwd_pairs_big(const int32_t* __restrict__ inv, const int32_t* 
         const int j = j0 + u * blockDim.x;
         if (j < n) {
           dst[d + j] = new_id[a[u]];
-          src[d + j] = k;
+          src[d + j] = lay(k, np, S);
         }
       }
     }
@@ -575,8 +597,11 @@ __device__ __forceinline__ int bin_of(int d) { return d > BIN_T8 ? 0 : d > BIN_T
 
 // Row class per phase (see N_CLASS) and the class sizes; iota[r] = r is the value
 // array of the stable sort that groups rows by class.
-__global__ void k_row_classes(int V, const int32_t* __restrict__ roffp, const int32_t* __restrict__ hot_end,
-                              uint8_t* __restrict__ key0, uint8_t* __restrict__ key1, int32_t* __restrict__ iota,
+// Rows outside [lo, hi) (another part's, or a split plan's pads) get class 4 in both
+// phases: no work.
+__global__ void k_row_classes(int V, int lo, int hi, const int32_t* __restrict__ roffp,
+                              const int32_t* __restrict__ hot_end, uint8_t* __restrict__ key0,
+                              uint8_t* __restrict__ key1, int32_t* __restrict__ iota,
                               int* __restrict__ counts /* [2 * N_CLASS] */) {
   int c0[N_CLASS], c1[N_CLASS];
 #pragma unroll
@@ -584,7 +609,9 @@ __global__ void k_row_classes(int V, const int32_t* __restrict__ roffp, const in
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < V; r += gridDim.x * blockDim.x) {
     const int b = roffp[r], e = roffp[r + 1], h = hot_end[r];
     int k0 = 4, k1;
-    if (e == b) {
+    if (r < lo || r >= hi) {
+      k1 = 4;
+    } else if (e == b) {
       k1 = 6;
     } else if (e - b > LONG_DEG) {
       k1 = 5;
@@ -714,6 +741,35 @@ __global__ void k_init_from(int V, const int32_t* __restrict__ new_id, const int
   }
 }
 
+// Split run (sp_pagerank_part_begin): pr = 1/V and contrib at every id of the plan (the
+// pads of the last positions have out-degree 0), so every part starts from the same
+// full contrib vector without an exchange.
+__global__ void k_init_part(int Vp, int V, const int32_t* __restrict__ odeg, float* __restrict__ pr,
+                            float* __restrict__ con, State* st) {
+  const float p0 = 1.0f / (float)V;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < Vp; v += gridDim.x * blockDim.x) {
+    pr[v] = p0;
+    const int od = odeg[v];
+    con[v] = od > 0 ? __fdiv_rn(p0, (float)od) : 0.0f;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->iter = 0;
+    st->done = 0;
+    st->ticket = 0;
+    st->diff = 0;
+    st->extra = 0;
+  }
+}
+
+// Split run: once the caller has summed every part's diff into *diff, the stop test of
+// the single-GPU run (iterate while diff > beta and fewer than max_iter iterations).
+__global__ void k_decide(State* st, const double* __restrict__ diff, double beta, int max_iter) {
+  if (st->done) return;
+  const double d = *diff;
+  st->diff = d;
+  st->done = (d > beta && st->iter < max_iter) ? 0 : 1;
+}
+
 // ---- plain variant: the generated CUDA form (one thread per vertex, serial gather
 // of pr[u]/outdeg(u), atomic float diff; backend_cuda/dsl_cpp_generator.cpp:1682-1761)
 __global__ void k_plain_iter(int V, const int32_t* __restrict__ off, const int32_t* __restrict__ roff,
@@ -747,25 +803,26 @@ __global__ void k_plain_init(int V, float* pr) {
 static int relabel(sp_graph* g, PrPlan* p) {
   const int V = g->V;
   const int E = (int)g->E;
+  const int np = p->nparts, S = p->S, Vp = p->Vp;  // ids: lay(rank) in [0, Vp)
   cudaStream_t s = g->stream;
   Arena& A = p->graph_mem;
   A.want(p->new_id, V);
-  A.want(p->od, V);
-  A.want(p->roffp, (size_t)V + 1);
+  A.want(p->od, Vp);
+  A.want(p->roffp, (size_t)Vp + 1);
   A.want(p->radjp, (size_t)E);
   A.want(p->outbuf, V);
-  A.want(p->hot_end, V);
-  A.want(p->part, V);
+  A.want(p->hot_end, Vp);
+  A.want(p->part, Vp);
   A.want(p->diff_part, 2 * (size_t)num_sms() * 32);
   A.want(p->state, 1);
   for (int i = 0; i < 2; ++i) {
-    A.want(p->prb[i], V);
-    A.want(p->con[i], V);
+    A.want(p->prb[i], Vp);
+    A.want(p->con[i], Vp);
   }
   SP_TRY(A.commit());
 
   int bits = 1;
-  while (bits < 31 && (1 << bits) < V) ++bits;
+  while (bits < 31 && (1 << bits) < Vp) ++bits;
   size_t t_vsort = 0, t_scan = 0, t_esort = 0;
   cub::DoubleBuffer<int32_t> nk(nullptr, nullptr), nv(nullptr, nullptr);
   cub::DeviceRadixSort::SortPairs(nullptr, t_vsort, (const int32_t*)nullptr, (int32_t*)nullptr,
@@ -773,9 +830,10 @@ static int relabel(sp_graph* g, PrPlan* p) {
   cub::DeviceScan::ExclusiveSum(nullptr, t_scan, (const int32_t*)nullptr, (int32_t*)nullptr, V + 1, s);
   cub::DeviceRadixSort::SortPairs(nullptr, t_esort, nk, nv, E, 0, bits, s);
   Arena T;
-  dspan<int32_t> key, id, skey, inv, offp, dst, dst_alt, src, big;
+  dspan<int32_t> key, id, skey, inv, offp, dst, dst_alt, src, big, odk;
   dspan<int> nbig;
   dspan<unsigned char> temp;
+  T.want(odk, V);  // out-degrees in rank order (the transpose's source order)
   T.want(key, V);
   T.want(id, V);
   T.want(skey, V);
@@ -795,16 +853,19 @@ static int relabel(sp_graph* g, PrPlan* p) {
   SP_CHECK_LAUNCH();
   size_t t = tb;
   SP_CHECK_CUDA(cub::DeviceRadixSort::SortPairs(temp.p, t, key.p, skey.p, id.p, inv.p, V, 0, 32, s));
-  pr::k_relabel_rows<<<grid, 256, 0, s>>>(V, inv.p, g->off.p, p->new_id.p, p->od.p);
+  pr::k_relabel_rows<<<grid, 256, 0, s>>>(V, np, S, inv.p, g->off.p, p->new_id.p, odk.p);
   SP_CHECK_LAUNCH();
   t = tb;
-  SP_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, t, p->od.p, offp.p, V, s));
+  SP_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, t, odk.p, offp.p, V, s));
   SP_CHECK_CUDA(cudaMemsetAsync(nbig.p, 0, sizeof(int), s));
-  pr::k_fwd_pairs<<<grid, 256, 0, s>>>(V, inv.p, p->new_id.p, g->off.p, g->adj.p, offp.p, p->od.p, dst.p, src.p,
-                                       big.p, nbig.p);
+  pr::k_fwd_pairs<<<grid, 256, 0, s>>>(V, np, S, inv.p, p->new_id.p, g->off.p, g->adj.p, offp.p, odk.p, dst.p,
+                                       src.p, big.p, nbig.p);
   SP_CHECK_LAUNCH();
-  pr::k_fwd_pairs_big<<<num_sms() * 8, 256, 0, s>>>(inv.p, p->new_id.p, g->off.p, g->adj.p, offp.p, p->od.p, dst.p,
-                                                     src.p, big.p, nbig.p);
+  pr::k_fwd_pairs_big<<<num_sms() * 8, 256, 0, s>>>(np, S, inv.p, p->new_id.p, g->off.p, g->adj.p, offp.p, odk.p,
+                                                     dst.p, src.p, big.p, nbig.p);
+  SP_CHECK_LAUNCH();
+  SP_CHECK_CUDA(cudaMemsetAsync(p->od.p, 0, sizeof(int32_t) * Vp, s));
+  pr::k_od_layout<<<grid, 256, 0, s>>>(V, np, S, odk.p, p->od.p);
   SP_CHECK_LAUNCH();
   cub::DoubleBuffer<int32_t> keys(dst.p, dst_alt.p), vals(src.p, p->radjp.p);
   t = tb;
@@ -813,7 +874,7 @@ static int relabel(sp_graph* g, PrPlan* p) {
     SP_CHECK_CUDA(cudaMemcpyAsync(p->radjp.p, vals.Current(), sizeof(int32_t) * E, cudaMemcpyDeviceToDevice, s));
   // row offsets of the relabelled reverse CSR straight from the sorted destinations
   // (no reverse CSR of the caller's graph is needed)
-  SP_TRY(offsets_of_sorted(V, E, keys.Current(), p->roffp.p, s));
+  SP_TRY(offsets_of_sorted(Vp, E, keys.Current(), p->roffp.p, s));
   SP_CHECK_CUDA(cudaStreamSynchronize(s));
   return SP_OK;
 }
@@ -822,18 +883,24 @@ static int relabel(sp_graph* g, PrPlan* p) {
 // 3-bit radix sort groups each phase's rows by class (ascending ids within a class),
 // and one scan over the long rows places their chunks and chunk-partial slots. The
 // host reads back only the class sizes and the chunk totals.
-static int build_pr_plan(sp_graph* g, int hot, int order) {
-  if (g->pr && g->pr->hot == hot && g->pr->order == order) return SP_OK;
+static int build_pr_plan(sp_graph* g, int hot, int order, int part = 0, int nparts = 1) {
+  if (g->pr && g->pr->hot == hot && g->pr->order == order && g->pr->part_idx == part && g->pr->nparts == nparts)
+    return SP_OK;
   if (order != 0) SP_TRY(ensure_reverse(g));  // in-degree classes read the caller's reverse offsets
-  const int V = g->V;
-  if (g->pr && g->pr->order != order) {  // a new vertex order: a new plan
-    free_pr_plan(g->pr);
+  if (g->pr && (g->pr->order != order || g->pr->part_idx != part || g->pr->nparts != nparts)) {
+    free_pr_plan(g->pr);  // a new vertex order or split: a new plan
     g->pr = nullptr;
   }
   PrPlan* p = g->pr;
   if (!p) {
     p = new PrPlan();
     p->order = order;
+    p->nparts = nparts;
+    p->part_idx = part;
+    p->S = nparts == 1 ? g->V : (g->V + nparts - 1) / nparts;
+    p->Vp = nparts == 1 ? g->V : nparts * p->S;
+    p->lo = nparts == 1 ? 0 : part * p->S;
+    p->hi = nparts == 1 ? g->V : p->lo + (g->V - part + nparts - 1) / nparts;  // ranks k = part mod nparts
     int st = relabel(g, p);
     if (st) {
       free_pr_plan(p);
@@ -847,6 +914,7 @@ static int build_pr_plan(sp_graph* g, int hot, int order) {
     p->exec = nullptr;
   }
   p->hot = -1;  // incomplete until the end
+  const int V = p->Vp;  // rows of the plan's id space
   const int32_t* hend = p->roffp.p;  // hot = 0: every row is all cold
   if (hot > 0) {
     pr::k_hot_end<<<num_sms() * 8, 256, 0, s>>>(V, p->roffp.p, p->radjp.p, hot, p->hot_end.p);
@@ -877,7 +945,8 @@ static int build_pr_plan(sp_graph* g, int hot, int order) {
   const size_t tb = temp.n;
 
   SP_CHECK_CUDA(cudaMemsetAsync(counts.p, 0, sizeof(int) * 2 * pr::N_CLASS, s));
-  pr::k_row_classes<<<num_sms() * 8, 256, 0, s>>>(V, p->roffp.p, hend, key0.p, key1.p, iota.p, counts.p);
+  pr::k_row_classes<<<num_sms() * 8, 256, 0, s>>>(V, p->lo, p->hi, p->roffp.p, hend, key0.p, key1.p, iota.p,
+                                                   counts.p);
   SP_CHECK_LAUNCH();
   int hc[2 * pr::N_CLASS];
   SP_TRY(copy_out(hc, counts.p, sizeof(hc), s));
@@ -943,16 +1012,9 @@ static int build_pr_plan(sp_graph* g, int hot, int order) {
   return SP_OK;
 }
 
-// init: starting ranks in the caller's vertex order (host or device), or null for 1/V.
-static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float* out, int32_t* iters,
-                    double* fdiff, const float* init = nullptr) {
-  const int hot = std::max(0, std::min(g->pr_hot >= 0 ? g->pr_hot : pr::HOT_DEFAULT, pr::HOT_MAX));
-  const int order = g->pr_order >= 0 ? g->pr_order : pr::ORDER_DEFAULT;
-  SP_TRY(build_pr_plan(g, hot, order));
-  PrPlan* p = g->pr;
-  cudaStream_t s = g->stream;
-  const int V = g->V;
-  const int n_iter = std::max(1, (int)maxIter);
+// The iteration kernel's arguments for plan p (V = the graph's vertices, for the base
+// term (1 - delta) / V).
+static pr::IterArgs iter_args(const PrPlan* p, float beta, float delta, int n_iter, int V) {
   pr::IterArgs a;
   a.roff = p->roffp.p;
   a.radj = p->radjp.p;
@@ -979,6 +1041,22 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
   a.beta = (double)beta;
   a.max_iter = n_iter;
   a.two_phase = p->two_phase() ? 1 : 0;
+  a.l1_hot = 0;
+  a.diff_out = nullptr;
+  return a;
+}
+
+// init: starting ranks in the caller's vertex order (host or device), or null for 1/V.
+static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float* out, int32_t* iters,
+                    double* fdiff, const float* init = nullptr) {
+  const int hot = std::max(0, std::min(g->pr_hot >= 0 ? g->pr_hot : pr::HOT_DEFAULT, pr::HOT_MAX));
+  const int order = g->pr_order >= 0 ? g->pr_order : pr::ORDER_DEFAULT;
+  SP_TRY(build_pr_plan(g, hot, order));
+  PrPlan* p = g->pr;
+  cudaStream_t s = g->stream;
+  const int V = g->V;
+  const int n_iter = std::max(1, (int)maxIter);
+  pr::IterArgs a = iter_args(p, beta, delta, n_iter, V);
   int per_sm = 0;
   const int sh = g->pr_src_hint >= 0 ? g->pr_src_hint : pr::SRC_HINT_DEFAULT;
   const int l1_hot = g->pr_l1_hot >= 0 ? g->pr_l1_hot : pr::L1_HOT_DEFAULT;
@@ -1113,4 +1191,122 @@ extern "C" int sp_pagerank_dynamic(sp_graph_h g, int64_t n, const char* type, co
   }
   if (n > 0) SP_TRY(update_graph(g, n, type, src, dst, weight));
   return pr_tuned(g, beta, delta, maxIter, pageRank, iterations, final_diff, pageRank);
+}
+
+// ---- PageRank split over GPUs by vertices (one part per rank) ----------------------
+// Replaces the host-staged exchange of the reference's multi-GPU generator
+// (backend_multigpu/dsl_cpp_generator.cpp:604-678): part r owns the rows of ids
+// [r * S, r * S + count_r) of a split plan (lay()), computes their ranks and contrib
+// each iteration, and the caller all-gathers the contrib slices (S floats per part)
+// and sums the parts' diffs with its collectives, on the device, between the calls.
+namespace sp {
+static int part_plan(sp_graph* g, const char* who, PrPlan** out) {
+  if (!g || !g->pr || g->pr->nparts < 1 || !g->pr->pcon[0]) {
+    set_error("%s: no split PageRank begun on this graph", who);
+    return SP_ERR_INVALID;
+  }
+  *out = g->pr;
+  return SP_OK;
+}
+}  // namespace sp
+
+extern "C" int sp_pagerank_part_begin(sp_graph_h g, int32_t part, int32_t nparts, float beta, float delta,
+                                      int32_t maxIter, float* con0, float* con1, double* diff, int32_t* slice) {
+  using namespace sp;
+  if (!g || nparts < 1 || part < 0 || part >= nparts || !con0 || !con1 || !diff || !slice) {
+    set_error("sp_pagerank_part_begin: invalid argument");
+    return SP_ERR_INVALID;
+  }
+  if (g->V == 0) {
+    set_error("sp_pagerank_part_begin: empty graph");
+    return SP_ERR_INVALID;
+  }
+  SP_TRY(build_pr_plan(g, 0, 0, part, nparts));
+  PrPlan* p = g->pr;
+  p->pcon[0] = con0;
+  p->pcon[1] = con1;
+  p->pdiff = diff;
+  p->pbeta = beta;
+  p->pdelta = delta;
+  p->pmax_iter = std::max(1, (int)maxIter);  // the DSL's do-while runs at least once
+  pr::k_init_part<<<num_sms() * 4, 256, 0, g->stream>>>(p->Vp, g->V, p->od.p, p->prb[0].p, con0, p->state.p);
+  SP_CHECK_LAUNCH();
+  *slice = p->S;
+  return SP_OK;
+}
+
+extern "C" int sp_pagerank_part_iterate(sp_graph_h g, int32_t k) {
+  using namespace sp;
+  PrPlan* p = nullptr;
+  SP_TRY(part_plan(g, "sp_pagerank_part_iterate", &p));
+  if (k < 0) {
+    set_error("sp_pagerank_part_iterate: iteration %d", k);
+    return SP_ERR_INVALID;
+  }
+  cudaStream_t s = g->stream;
+  // no local stop: the part's kernel only counts the iteration; k_decide applies the
+  // stop test to the summed diff
+  pr::IterArgs a = iter_args(p, -1.0f, p->pdelta, INT_MAX, g->V);
+  a.diff_out = p->pdiff;
+  const int sh = g->pr_src_hint >= 0 ? g->pr_src_hint : pr::SRC_HINT_DEFAULT;
+  using PhaseFn = void (*)(pr::IterArgs, const float*, const float*, float*, float*);
+  const PhaseFn ph1 = sh == 1 ? pr::k_phase<1, 1, 0, 0> : sh == 2 ? pr::k_phase<1, 2, 0, 0> : pr::k_phase<1, 0, 0, 0>;
+  int per_sm = 0;
+  SP_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ph1, pr::THREADS, 0));
+  const int grid = std::max(1, std::min(num_sms() * 32, num_sms() * std::max(1, per_sm)));
+  const int c = k & 1, n = c ^ 1;
+  if (k < 2 && p->n_zero) {
+    pr::k_zero_rows<<<num_sms() * 2, 256, 0, s>>>(a, p->zrows, p->n_zero, p->prb[c].p, p->prb[n].p, p->pcon[n]);
+    SP_CHECK_LAUNCH();
+  }
+  ph1<<<grid, pr::THREADS, 0, s>>>(a, p->prb[c].p, p->pcon[c], p->prb[n].p, p->pcon[n]);
+  SP_CHECK_LAUNCH();
+  return SP_OK;
+}
+
+extern "C" int sp_pagerank_part_decide(sp_graph_h g) {
+  using namespace sp;
+  PrPlan* p = nullptr;
+  SP_TRY(part_plan(g, "sp_pagerank_part_decide", &p));
+  pr::k_decide<<<1, 1, 0, g->stream>>>(p->state.p, p->pdiff, (double)p->pbeta, p->pmax_iter);
+  SP_CHECK_LAUNCH();
+  return SP_OK;
+}
+
+extern "C" int sp_pagerank_part_state(sp_graph_h g, int32_t* iterations, int32_t* done, double* diff) {
+  using namespace sp;
+  PrPlan* p = nullptr;
+  SP_TRY(part_plan(g, "sp_pagerank_part_state", &p));
+  pr::State st;
+  SP_TRY(copy_out(&st, p->state.p, sizeof(st), g->stream));
+  if (iterations) *iterations = st.iter;
+  if (done) *done = st.done;
+  if (diff) *diff = st.diff;
+  return SP_OK;
+}
+
+extern "C" int sp_pagerank_part_ranks(sp_graph_h g, float* slice) {
+  using namespace sp;
+  PrPlan* p = nullptr;
+  SP_TRY(part_plan(g, "sp_pagerank_part_ranks", &p));
+  if (!slice) {
+    set_error("sp_pagerank_part_ranks: NULL slice");
+    return SP_ERR_INVALID;
+  }
+  pr::State st;
+  SP_TRY(copy_out(&st, p->state.p, sizeof(st), g->stream));
+  return copy_out(slice, p->prb[st.iter & 1].p + p->lo, sizeof(float) * p->S, g->stream);
+}
+
+extern "C" int sp_pagerank_part_finish(sp_graph_h g, const float* ranks, float* pageRank) {
+  using namespace sp;
+  PrPlan* p = nullptr;
+  SP_TRY(part_plan(g, "sp_pagerank_part_finish", &p));
+  if (!ranks || !pageRank) {
+    set_error("sp_pagerank_part_finish: NULL argument");
+    return SP_ERR_INVALID;
+  }
+  pr::k_unpermute<<<num_sms() * 4, 256, 0, g->stream>>>(g->V, p->new_id.p, ranks, p->outbuf.p);
+  SP_CHECK_LAUNCH();
+  return copy_out(pageRank, p->outbuf.p, sizeof(float) * g->V, g->stream);
 }

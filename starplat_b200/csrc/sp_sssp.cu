@@ -90,7 +90,23 @@ struct Args {
   int hub_deg;          // vertices with more out-edges are relaxed in pieces by all warps
   int hub_chunk;        // edges per piece
   int local_edges;      // cascade budget of a warp per round, in edges (0 = no cascades)
+  // Bucket width per epoch (the learned scheduler's per-iteration decision): 0 = every
+  // bucket `delta` wide; 1 = the width factor whose predicted cost per unit of distance
+  // advanced is lowest under the epoch model; 2 = a pseudo-random factor per epoch
+  // (exploration, to collect training data).
+  int epolicy;
+  unsigned eseed;
+  const float* emodel;   // [SP_MLP_PARAMS + 2 * SP_MLP_IN]: parameters, feature mean, feature scale
+  float* etrace;         // [etrace_cap][ETRACE]: per epoch, the chosen candidate's inputs, factor, advance
+  unsigned long long* etime;  // [etrace_cap + 1]: globaltimer at each advance, then at the end
+  int etrace_cap;
+  float sfeat[4];        // log2 V, log2 E, mean out-degree, log2 largest weight
 };
+
+// Width factors of the per-epoch choice, as num / 4 of the call's delta.
+constexpr int NFAC = 6;
+__device__ __constant__ int kFacNum[NFAC] = {1, 2, 4, 8, 16, 32};
+constexpr int ETRACE = 16;  // floats per trace record: SP_MLP_IN inputs, factor, advance, pad
 
 // Where a round's relaxations go: the next round's queue and hub list, this
 // epoch's far pile.
@@ -397,6 +413,76 @@ __device__ __forceinline__ void cascade(const Args& a, long long thr, int round,
   r.cnt = 0;
 }
 
+// The inputs of the per-epoch width choice for candidate factor f (all from values
+// every CTA of the solve reads identically after a barrier).
+__device__ __forceinline__ void epoch_inputs(const Args& a, int f, float fn, float rounds_prev, float relaxed_prev,
+                                             int epoch, int f_prev, float progress, float* x) {
+  x[0] = a.sfeat[0];
+  x[1] = a.sfeat[1];
+  x[2] = a.sfeat[2];
+  x[3] = a.sfeat[3];
+  x[4] = log2f(1.0f + fn);            // far pile at this advance
+  x[5] = x[4] - a.sfeat[0];           // ... as a fraction of V (log)
+  x[6] = log2f(1.0f + rounds_prev);   // relax rounds of the previous epoch
+  x[7] = log2f(1.0f + relaxed_prev);  // edges relaxed in the previous epoch
+  x[8] = log2f(1.0f + (float)epoch);
+  x[9] = log2f((float)kFacNum[f_prev]) - 2.0f;  // previous width factor (log2)
+  x[10] = log2f((float)kFacNum[f]) - 2.0f;      // candidate width factor (log2)
+  x[11] = x[10] * x[4];
+  x[12] = progress;                   // log2(1 + smallest far distance / largest weight)
+}
+
+// The width factor the epoch model scores lowest (predicted log cost per unit of
+// distance): NFAC candidates x 32 hidden units over the CTA's threads, every CTA
+// evaluating the same inputs with the same instructions in the same order, so all
+// pick the same factor without a barrier between them. Ties go to the smaller factor.
+__device__ int epoch_choice(const Args& a, float fn, float rounds_prev, float relaxed_prev, int epoch, int f_prev,
+                            float progress) {
+  constexpr int IN = SP_MLP_IN, H = SP_MLP_HIDDEN;
+  __shared__ float s_x[NFAC][IN];
+  __shared__ float s_h1[NFAC][H];
+  __shared__ float s_y[NFAC];
+  __shared__ int s_pick;
+  const float* P = a.emodel;
+  const float* mean = P + SP_MLP_PARAMS;
+  const float* scale = mean + IN;
+  const int t = threadIdx.x;
+  if (t < NFAC) {
+    float x[IN];
+    epoch_inputs(a, t, fn, rounds_prev, relaxed_prev, epoch, f_prev, progress, x);
+#pragma unroll
+    for (int i = 0; i < IN; ++i) s_x[t][i] = (x[i] - mean[i]) * scale[i];
+  }
+  __syncthreads();
+  const int c = t >> 5, j = t & 31;
+  constexpr int W1 = 0, B1 = W1 + H * IN, W2 = B1 + H, B2 = W2 + H * H, W3 = B2 + H, B3 = W3 + H;
+  if (c < NFAC) {
+    float z = P[B1 + j];
+#pragma unroll
+    for (int i = 0; i < IN; ++i) z = fmaf(P[W1 + j * IN + i], s_x[c][i], z);
+    s_h1[c][j] = tanhf(z);
+  }
+  __syncthreads();
+  if (c < NFAC) {
+    float z = P[B2 + j];
+#pragma unroll 8
+    for (int k = 0; k < H; ++k) z = fmaf(P[W2 + j * H + k], s_h1[c][k], z);
+    float v = P[W3 + j] * tanhf(z);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (j == 0) s_y[c] = P[B3] + v;
+  }
+  __syncthreads();
+  if (t == 0) {
+    int best = 0;
+    for (int k = 1; k < NFAC; ++k)
+      if (s_y[k] < s_y[best]) best = k;
+    s_pick = best;
+  }
+  __syncthreads();
+  return s_pick;
+}
+
 // One delta-stepping solve by `nblk` co-resident CTAs (this one is number `blk`):
 // the whole grid for a single source, or one group of a batched launch.
 __device__ __forceinline__ void delta_run(const Args& a, const int blk, const int nblk, int32_t* ring) {
@@ -406,6 +492,9 @@ __device__ __forceinline__ void delta_run(const Args& a, const int blk, const in
   const int nw = (nblk * THREADS) >> 5;
   int round = 0, epoch = 0;
   long long thr = a.delta;  // bucket 0 = [0, delta)
+  // per-epoch width state (identical in every CTA of the solve)
+  int f_prev = 2, round_mark = 0;
+  unsigned long long relaxed_mark = 0;
   while (true) {
     const int qv = *(volatile int*)&c->qcount[round % 3];
     const unsigned long long hc = *(volatile unsigned long long*)&c->hcount[round % 3];
@@ -467,8 +556,40 @@ __device__ __forceinline__ void delta_run(const Args& a, const int blk, const in
       // bucket advance: threshold to the bucket after the smallest far distance
       const long long fm = *(volatile int*)&c->fmin[epoch % 3];
       const long long thr_old = thr;
-      thr = (a.delta >= (long long)INT_MAX) ? (long long)INT_MAX + 1 : (fm / a.delta + 1) * a.delta;
-      if (thr <= thr_old) thr = thr_old + a.delta;
+      long long w = a.delta;
+      if (a.epolicy != 0 && a.delta < (long long)INT_MAX) {
+        const unsigned long long rel = *(volatile unsigned long long*)&c->relaxed;
+        const float rounds_prev = (float)(round - round_mark), relaxed_prev = (float)(rel - relaxed_mark);
+        const float progress = log2f(1.0f + (float)fm / fmaxf(1.0f, exp2f(a.sfeat[3])));
+        int f;
+        if (a.epolicy == 2) {
+          unsigned h = a.eseed * 0x9e3779b9u ^ ((unsigned)epoch * 0x85ebca6bu);
+          h ^= h >> 15;
+          h *= 0x2c1b3c6du;
+          h ^= h >> 12;
+          f = (int)(h % NFAC);
+        } else {
+          f = epoch_choice(a, (float)fn, rounds_prev, relaxed_prev, epoch, f_prev, progress);
+        }
+        w = max(1ll, a.delta * kFacNum[f] / 4);
+        if (a.etrace && blk == 0 && threadIdx.x == 0 && epoch < a.etrace_cap) {
+          float x[SP_MLP_IN];
+          epoch_inputs(a, f, (float)fn, rounds_prev, relaxed_prev, epoch, f_prev, progress, x);
+          float* r = a.etrace + (size_t)epoch * ETRACE;
+          for (int i = 0; i < SP_MLP_IN; ++i) r[i] = x[i];
+          r[SP_MLP_IN] = (float)kFacNum[f] / 4.0f;
+          const long long t_new = max((fm / w + 1) * w, thr_old + w);
+          r[SP_MLP_IN + 1] = (float)(t_new - thr_old);
+          unsigned long long now;
+          asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+          a.etime[epoch] = now;
+        }
+        f_prev = f;
+        round_mark = round;
+        relaxed_mark = rel;
+      }
+      thr = (a.delta >= (long long)INT_MAX) ? (long long)INT_MAX + 1 : (fm / w + 1) * w;
+      if (thr <= thr_old) thr = thr_old + w;
       // The split fills the queue of the NEXT round (its own counter slot): every
       // phase decision reads qcount[round % 3], and no phase may write the slot its
       // own decision read while slower CTAs may still be reading it.
@@ -513,6 +634,11 @@ __device__ __forceinline__ void delta_run(const Args& a, const int blk, const in
   }
   if (blk == 0 && threadIdx.x == 0) {
     c->rounds = round - epoch;  // relax rounds (each split also consumed a round number)
+    if (a.etrace && epoch <= a.etrace_cap) {  // the end of the last traced epoch
+      unsigned long long now;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+      a.etime[min(epoch, a.etrace_cap)] = now;
+    }
     c->epochs = epoch;
     if (c->bar.error) c->status = 1;
   }
@@ -720,9 +846,60 @@ struct SsspPlan {
   unsigned sel_gen = 0;
   int sel_wmin = 0, sel_wmax = 0, sel_ctas = 0, sel_local = 0, sel_local_knob = -1;
   int64_t sel_delta = 0;
+  // the per-epoch width model on the device (uploaded when its generation changes) and
+  // the trace of the last traced solve
+  dbuf<float> emodel;
+  unsigned emodel_gen = 0;
+  dbuf<float> etrace;
+  dbuf<unsigned long long> etime;
+  int etrace_n = 0;
 };
 
 void free_sssp_plan(SsspPlan* p) { delete p; }
+
+unsigned mlp_epoch_model(std::vector<float>& packed);  // sp_mlp.cu
+constexpr int ETRACE_CAP = 1 << 16;                     // traced epochs per solve
+
+// The per-epoch width fields of a: the policy (knob sssp.epoch; by default learned when
+// an epoch model is loaded), the model on the device, the static inputs, and the trace
+// buffers when tracing a single-source solve.
+static int epoch_setup(sp_graph* g, ss::Args& a, bool trace) {
+  SsspPlan* p = g->sssp;
+  std::vector<float> packed;
+  const unsigned gen = mlp_epoch_model(packed);
+  int pol = g->sssp_epoch;
+  if (pol < 0) pol = gen ? 1 : 0;
+  if (pol == 1 && !gen) pol = 0;  // no model: the fixed width
+  a.epolicy = pol;
+  a.eseed = (unsigned)g->sssp_epoch_seed;
+  a.emodel = nullptr;
+  a.etrace = nullptr;
+  a.etime = nullptr;
+  a.etrace_cap = 0;
+  if (pol == 1) {
+    if (p->emodel_gen != gen) {
+      SP_TRY(p->emodel.alloc(packed.size()));
+      SP_CHECK_CUDA(cudaMemcpyAsync(p->emodel.p, packed.data(), sizeof(float) * packed.size(),
+                                    cudaMemcpyHostToDevice, g->stream));
+      p->emodel_gen = gen;
+    }
+    a.emodel = p->emodel.p;
+  }
+  const double V = std::max(1, g->V), E = (double)g->E;
+  a.sfeat[0] = (float)std::log2(V);
+  a.sfeat[1] = (float)std::log2(E + 1.0);
+  a.sfeat[2] = (float)(E / V);
+  a.sfeat[3] = (float)std::log2(std::max(1.0, (double)p->w_max));
+  if (trace && pol != 0) {
+    SP_TRY(p->etrace.alloc((size_t)ETRACE_CAP * ss::ETRACE));
+    SP_TRY(p->etime.alloc((size_t)ETRACE_CAP + 1));
+    a.etrace = p->etrace.p;
+    a.etime = p->etime.p;
+    a.etrace_cap = ETRACE_CAP;
+  }
+  g->sssp_last_epolicy = pol;
+  return SP_OK;
+}
 int sssp_hub_deg_default() { return ss::HUB_DEG; }
 int sssp_hub_chunk_default() { return ss::HUB_CHUNK; }
 int sssp_local_default() { return ss::LOCAL_STEPS; }
@@ -828,6 +1005,7 @@ static int sssp_delta(sp_graph* g, const int32_t* w, int32_t src, int32_t* dist_
   a.hub_deg = std::min(g->sssp_hub_deg > 0 ? g->sssp_hub_deg : ss::HUB_DEG, ss::HUB_DEG_MAX);
   a.hub_chunk = g->sssp_hub_chunk > 0 ? g->sssp_hub_chunk : ss::HUB_CHUNK;
   a.local_edges = 32 * local;
+  SP_TRY(epoch_setup(g, a, g->sssp_trace != 0));
   if (nseeds > 0) {
     ss::k_reset<<<num_sms() * 4, 256, 0, s>>>(V, p->qstamp.p, p->fstamp.p, p->ctl.p);
     SP_CHECK_LAUNCH();
@@ -849,6 +1027,8 @@ static int sssp_delta(sp_graph* g, const int32_t* w, int32_t src, int32_t* dist_
   SP_TRY(copy_out(&hc, p->ctl.p, sizeof(hc), s));
   if (rounds_out) *rounds_out = hc.rounds;
   g->sssp_last_relaxed = (int64_t)hc.relaxed;
+  g->sssp_last_epochs = hc.epochs;
+  p->etrace_n = a.etrace ? std::min(hc.epochs, ETRACE_CAP) : 0;
   if (hc.status != 0 || hc.bar.error) {
     if (negative && !hc.bar.error) {
       set_error("sp_sssp: no fixed point after %d rounds (negative cycle)", hc.rounds);
@@ -919,6 +1099,7 @@ static int sssp_delta_batches(sp_graph* g, const int32_t* w, const std::vector<i
   a.hub_deg = std::min(g->sssp_hub_deg > 0 ? g->sssp_hub_deg : ss::HUB_DEG, ss::HUB_DEG_MAX);
   a.hub_chunk = g->sssp_hub_chunk > 0 ? g->sssp_hub_chunk : ss::HUB_CHUNK;
   a.local_edges = 32 * local;
+  SP_TRY(epoch_setup(g, a, false));
   std::vector<ss::Ctl> hc(B);
   int64_t relaxed = 0;
   for (int k0 = 0; k0 < n; k0 += B) {
@@ -1194,6 +1375,21 @@ int sssp_batch_sums(sp_graph* g, const int32_t* weight, const std::vector<int32_
   });
 }
 }  // namespace sp
+
+extern "C" int sp_sssp_epoch_trace(sp_graph_h g, float* records, unsigned long long* times, int32_t cap,
+                                   int32_t* n) {
+  using namespace sp;
+  if (!g || !n || cap < 0 || (cap > 0 && (!records || !times))) {
+    set_error("sp_sssp_epoch_trace: invalid argument");
+    return SP_ERR_INVALID;
+  }
+  const int have = g->sssp ? g->sssp->etrace_n : 0;
+  *n = have;
+  const int k = std::min(have, (int)cap);
+  if (k == 0) return SP_OK;
+  SP_TRY(copy_out(records, g->sssp->etrace.p, sizeof(float) * ss::ETRACE * k, g->stream));
+  return copy_out(times, g->sssp->etime.p, sizeof(unsigned long long) * (k + 1), g->stream);
+}
 
 extern "C" int sp_sssp_features(sp_graph_h g, const int32_t* weight, double delta_mult, int32_t ctas_per_sm,
                                 int32_t local_steps, float* x) {

@@ -292,6 +292,37 @@ class DeviceGraph:
                                        ctypes.byref(rounds)))
         return out, int(rounds.value)
 
+    # ---- PageRank split over ranks by vertices (sp_pagerank_part_*; driven by
+    # distributed.pagerank_on_gpus)
+    def pagerank_part_begin(self, part: int, nparts: int, beta: float, delta: float, max_iter: int, con0, con1,
+                            diff) -> int:
+        """Starts this rank's part; con0 / con1 (nparts * S float32) and diff (one float64)
+        are device tensors the caller's collectives work on. Returns S."""
+        S = ctypes.c_int32()
+        check("sp_pagerank_part_begin", lib().sp_pagerank_part_begin(
+            self.handle, int(part), int(nparts), float(beta), float(delta), int(max_iter), _ptr(con0), _ptr(con1),
+            _ptr(diff), ctypes.byref(S)))
+        return int(S.value)
+
+    def pagerank_part_iterate(self, k: int) -> None:
+        check("sp_pagerank_part_iterate", lib().sp_pagerank_part_iterate(self.handle, int(k)))
+
+    def pagerank_part_decide(self) -> None:
+        check("sp_pagerank_part_decide", lib().sp_pagerank_part_decide(self.handle))
+
+    def pagerank_part_state(self):
+        """(iterations, done, summed diff); synchronises the stream."""
+        it, done, diff = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_double()
+        check("sp_pagerank_part_state", lib().sp_pagerank_part_state(self.handle, ctypes.byref(it), ctypes.byref(done),
+                                                                     ctypes.byref(diff)))
+        return int(it.value), bool(done.value), float(diff.value)
+
+    def pagerank_part_ranks(self, slice_out) -> None:
+        check("sp_pagerank_part_ranks", lib().sp_pagerank_part_ranks(self.handle, _ptr(slice_out)))
+
+    def pagerank_part_finish(self, ranks, out) -> None:
+        check("sp_pagerank_part_finish", lib().sp_pagerank_part_finish(self.handle, _ptr(ranks), _ptr(out)))
+
     def sssp_batch(self, sources, weight=None, out=None):
         """Distances from every source (int32, host or device) in batched cooperative
         launches, one CTA group per source: int32[nsrc][V], row k from sources[k]

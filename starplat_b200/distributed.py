@@ -10,6 +10,9 @@ vectors.
 Triangle counting and the clustering coefficient split anchors instead: rank r counts
 the triangles of part r of the anchor order (sp_tc_part / sp_clustering_coeff_part), and
 one all-reduce adds an int64 count or an int32[V] vector, exactly.
+PageRank splits vertices (pagerank_on_gpus): rank r owns the rows of part r, and every
+iteration ends with an all-gather of the parts' contrib blocks and an all-reduce of the
+L1 diff, both on device buffers; the stop test runs on the device.
 The process group comes from replicas.Replicas (NCCL on GPUs, gloo on the host).
 """
 from __future__ import annotations
@@ -110,3 +113,54 @@ def clustering_coeff_on_gpus(dg, rep: Optional[Replicas] = None, out=None):
     if out is not None:
         return lcc_sharded(dg.V, rep, lambda r, n, o: dg.clustering_coeff_part(r, n, out=o), out)
     return lcc_sharded(dg.V, rep, lambda r, n: dg.clustering_coeff_part(r, n))
+
+
+def pagerank_on_gpus(dg, rep: Optional[Replicas] = None, beta: float = 1e-6, delta: float = 0.85,
+                     max_iter: int = 100, out=None, check_every: int = 8):
+    """ComputePageRank split over the ranks by vertices (sp_pagerank_part_*): every rank
+    holds the whole graph and computes the rows of its part; per iteration, one NCCL
+    all-gather of the parts' contrib blocks (S floats each) and one all-reduce of the
+    diff, in stream order with the kernels, so nothing crosses to the host. The stop
+    test runs on the device; the host reads the state once every `check_every`
+    iterations. Replaces the host-staged exchange of the reference's multi-GPU code
+    (backend_multigpu/dsl_cpp_generator.cpp:604-678). Returns (pageRank[V] float32 in
+    the caller's vertex order, iterations, final diff); `out` (host or device) receives
+    the ranks when given."""
+    import torch
+
+    from .device import DeviceGraph
+
+    rep = rep or Replicas()
+    dev = rep.device()
+    if isinstance(dg, DeviceGraph):
+        if dev.type != "cuda":
+            raise ValueError("pagerank_on_gpus: the part buffers must be device tensors (NCCL or one GPU)")
+        dg.set_stream(torch.cuda.current_stream())  # the collectives' stream order
+    n, r = rep.world, rep.rank
+    S = -(-dg.V // n)
+    con = [torch.empty(n * S, dtype=torch.float32, device=dev) for _ in range(2)]
+    diff = torch.zeros(1, dtype=torch.float64, device=dev)
+    if dg.pagerank_part_begin(r, n, beta, delta, max_iter, con[0], con[1], diff) != S:
+        raise RuntimeError("pagerank_on_gpus: slice size mismatch")
+    k = 0
+    while True:
+        for _ in range(check_every):
+            dg.pagerank_part_iterate(k)
+            nxt = con[(k + 1) & 1]
+            rep.all_gather_into(nxt, nxt[r * S:(r + 1) * S])
+            rep.all_reduce_sum(diff)
+            dg.pagerank_part_decide()
+            k += 1
+        it, done, d = dg.pagerank_part_state()
+        if done:
+            break
+        if k > max(1, max_iter) + check_every:
+            raise RuntimeError("pagerank_on_gpus: the stop test never fired")
+    part = torch.empty(S, dtype=torch.float32, device=dev)
+    dg.pagerank_part_ranks(part)
+    full = torch.empty(n * S, dtype=torch.float32, device=dev)
+    rep.all_gather_into(full, part)
+    if out is None:
+        out = np.empty(dg.V, np.float32)
+    dg.pagerank_part_finish(full, out)
+    return out, it, d

@@ -90,10 +90,11 @@ class Replicas:
         self._dist.all_gather_into_tensor(full, part)
 
     def device(self):
-        """Where this rank's collective tensors live: its GPU under NCCL, else the host."""
+        """Where this rank's collective tensors live: the host under gloo, else this
+        rank's GPU (NCCL, or a single process with a GPU), else the host."""
         import torch
 
-        if self.backend == "nccl":
+        if self.backend != "gloo" and torch.cuda.is_available():
             return torch.device("cuda", torch.cuda.current_device())
         return torch.device("cpu")
 

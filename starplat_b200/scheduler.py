@@ -13,6 +13,16 @@ skewed ones, so they are part of the choice. Without a model the fixed heuristic
 speed only: distances are exact either way.
 
     python -m starplat_b200.scheduler train     # collect, train, write sched_model.json
+
+A second network with the same shape makes a decision per iteration inside the
+kernel: at every bucket advance of a delta-stepping solve it scores six width factors
+(1/4 .. 8 times the call's delta) from inputs the kernel reads on the device (far-pile
+size, rounds and relaxations of the previous epoch, progress, the previous factor) and
+widens or narrows the next bucket accordingly (knob sssp.epoch). Its training data are
+traces of solves that pick a seeded random factor per epoch (sssp.epoch = 2): per epoch
+the chosen factor's inputs and the measured device time per unit of distance advanced.
+
+    python -m starplat_b200.scheduler train-epoch   # collect traces, train, write sched_epoch_model.json
 """
 from __future__ import annotations
 
@@ -30,6 +40,8 @@ from ._lib import check, lib
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 MODEL_PATH = os.path.join(_HERE, "sched_model.json")
+EPOCH_MODEL_PATH = os.path.join(_HERE, "sched_epoch_model.json")
+EPOCH_FACTORS = (0.25, 0.5, 1.0, 2.0, 4.0, 8.0)  # the kernel's width candidates (kFacNum / 4)
 MULTS = (1, 2, 4, 8, 16, 32, 64)
 CTAS = (1, 2, 4)
 LOCALS = (0, 64)  # warp cascade budget per round (sssp.local), off or the default
@@ -106,9 +118,12 @@ def _settle_auto_load() -> None:
     device._SCHED_TRIED = True
 
 
-def load(path: str = MODEL_PATH) -> bool:
-    """Load the model into the library; False (fixed heuristic stays) if absent."""
+def load(path: str = MODEL_PATH, epoch_path: str = EPOCH_MODEL_PATH) -> bool:
+    """Load the model (and the per-epoch width model, when its file exists) into the
+    library; False (fixed heuristic stays) if the model file is absent."""
     _settle_auto_load()
+    if epoch_path and os.path.exists(epoch_path):
+        load_epoch(epoch_path)
     if not os.path.exists(path):
         return False
     d = json.load(open(path))
@@ -122,9 +137,132 @@ def load(path: str = MODEL_PATH) -> bool:
 
 
 def unload() -> None:
-    """Back to the fixed heuristic, also for later calls in this process."""
+    """Back to the fixed heuristic (and fixed bucket widths), also for later calls in
+    this process."""
     _settle_auto_load()
     check("sp_sched_load", lib().sp_sched_load(None, None, None))
+    check("sp_sched_epoch_load", lib().sp_sched_epoch_load(None, None, None))
+
+
+def load_epoch(path: str = EPOCH_MODEL_PATH) -> bool:
+    """Load the per-epoch width model only; False if the file is absent."""
+    if not os.path.exists(path):
+        return False
+    d = json.load(open(path))
+    p = np.asarray(d["params"], np.float32)
+    mean = np.asarray(d["feat_mean"], np.float32)
+    scale = np.asarray(d["feat_scale"], np.float32)
+    if p.shape[0] != P or mean.shape[0] != IN:
+        raise ValueError(f"{path}: model shape does not match this library")
+    check("sp_sched_epoch_load", lib().sp_sched_epoch_load(p.ctypes.data, mean.ctypes.data, scale.ctypes.data))
+    return True
+
+
+def unload_epoch() -> None:
+    """Fixed bucket widths again (the per-call model stays)."""
+    check("sp_sched_epoch_load", lib().sp_sched_epoch_load(None, None, None))
+
+
+def epoch_trace(dg):
+    """The last traced solve's epochs: (inputs[n][IN], factor[n], advance[n], ns[n]), the
+    time of each epoch from its advance to the next (the last epoch's to the end)."""
+    cap = 1 << 16
+    rec = np.empty((cap, 16), np.float32)
+    t = np.empty(cap + 1, np.uint64)
+    n = ctypes.c_int32()
+    check("sp_sssp_epoch_trace", lib().sp_sssp_epoch_trace(dg.handle, rec.ctypes.data, t.ctypes.data, cap,
+                                                           ctypes.byref(n)))
+    k = min(int(n.value), cap)
+    if int(n.value) > cap:
+        k -= 1  # the last record's end lies past the trace
+    ns = (t[1:k + 1].astype(np.int64) - t[:k].astype(np.int64)).astype(np.float64)
+    return rec[:k, :IN].copy(), rec[:k, IN].copy(), rec[:k, IN + 1].copy(), ns
+
+
+def epoch_scores(params, mean, scale, inputs):
+    """Scores of every width factor for each traced epoch's state (the kernel's argmin
+    is the chosen factor): inputs[n][IN] with the candidate columns replaced."""
+    rows = []
+    for x in inputs:
+        for f in EPOCH_FACTORS:
+            r = np.array(x, np.float32)
+            r[10] = math.log2(f)
+            r[11] = r[10] * r[4]
+            rows.append(r)
+    y = mlp_forward(params, (np.array(rows, np.float32) - mean) * scale)
+    return y.reshape(len(inputs), len(EPOCH_FACTORS))
+
+
+def collect_epochs(graphs, seeds=(1, 2, 3, 4, 5, 6), log=print):
+    """Exploration solves (a seeded random width factor per epoch) with traces: one
+    sample per epoch, target log2(ns per unit of distance advanced)."""
+    from .device import DeviceGraph
+
+    import torch
+
+    X, T, meta = [], [], []
+    for name, g, src in graphs:
+        with DeviceGraph.from_csr(g) as dg:
+            dg.set_stream(torch.cuda.current_stream())
+            out = torch.empty(g.V, dtype=torch.int32, device="cuda")
+            dg.sssp(src, out=out)  # warm-up; fixes the call's learned delta
+            dg.tune_set("sssp.trace", 1)
+            dg.tune_set("sssp.epoch", 2)
+            for sd in seeds:
+                dg.tune_set("sssp.epoch_seed", sd)
+                dg.sssp(src, out=out)
+                torch.cuda.synchronize()
+                x, f, adv, ns = epoch_trace(dg)
+                ok = (adv > 0) & (ns > 0)
+                X.append(x[ok])
+                T.append(np.log2(ns[ok] / adv[ok]).astype(np.float32))
+                meta += [(name, sd)] * int(ok.sum())
+            dg.tune_set("sssp.epoch", -1)
+            dg.tune_set("sssp.trace", 0)
+        log(f"  {name}: {sum(1 for m in meta if m[0] == name)} epochs")
+    return np.concatenate(X), np.concatenate(T), meta
+
+
+def time_policy(dg, src, policy: int, reps: int = 3) -> float:
+    """Best-of-reps device time of one solve under an epoch policy (0 fixed, 1 learned)."""
+    import torch
+
+    dg.tune_set("sssp.epoch", policy)
+    out = torch.empty(dg.V, dtype=torch.int32, device="cuda")
+    dg.sssp(src, out=out)
+    best = None
+    for _ in range(reps):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(torch.cuda.current_stream())
+        dg.sssp(src, out=out)
+        b.record(torch.cuda.current_stream())
+        torch.cuda.synchronize()
+        t = a.elapsed_time(b)
+        best = t if best is None else min(best, t)
+    dg.tune_set("sssp.epoch", -1)
+    return best
+
+
+def train_epoch(out: str = EPOCH_MODEL_PATH, log=print) -> dict:
+    """Collect exploration traces on the training graphs, fit the epoch model with the
+    fused training kernel, and write it."""
+    import torch
+
+    t0 = time.time()
+    load(MODEL_PATH, epoch_path=None)  # the per-call choice fixes each solve's base delta
+    graphs = training_graphs()
+    log(f"collecting per-epoch traces on {len(graphs)} graphs")
+    X, T, meta = collect_epochs(graphs, log=log)
+    params, mean, scale, loss = fit(X, T, steps=6000)
+    d = {"params": params.tolist(), "feat_mean": mean.tolist(), "feat_scale": scale.tolist(),
+         "factors": list(EPOCH_FACTORS), "train_loss": loss, "samples": int(X.shape[0]),
+         "target": "log2(device ns per unit of distance advanced) of one epoch",
+         "gpu": torch.cuda.get_device_name(0), "collect_and_train_s": round(time.time() - t0, 1)}
+    with open(out, "w") as f:
+        json.dump(d, f, indent=1)
+    log(f"trained on {X.shape[0]} epochs: loss {loss:.4f}; wrote {out}")
+    return d
 
 
 # ----------------------------------------------------------------------------- data collection
@@ -225,6 +363,10 @@ def main(argv=None):
     import torch
 
     argv = sys.argv[1:] if argv is None else argv
+    if argv and argv[0] == "train-epoch":
+        torch.cuda.set_device(0)
+        train_epoch(argv[1] if len(argv) > 1 else EPOCH_MODEL_PATH)
+        return 0
     if not argv or argv[0] != "train":
         print(__doc__)
         return 1

@@ -7,6 +7,7 @@ import socket
 import subprocess
 import sys
 
+import numpy as np
 import pytest
 import torch.multiprocessing as mp
 
@@ -271,3 +272,105 @@ def test_device_tensor_sums_over_ranks(tmp_path):
         assert np.all(np.abs(out - ref) <= 1e-5 * np.abs(ref) + 1e-6)
         assert np.array_equal(np.load(tmp_path / f"cf{r}.npy"), want_cf)
         assert np.array_equal(np.load(tmp_path / f"ag{r}.npy"), np.repeat(np.arange(world, dtype=np.float32), 5))
+
+
+class _HostPartGraph:
+    """A host stand-in for DeviceGraph's split-PageRank calls (test infrastructure): the
+    same contract (contiguous blocks of S ids per part, the caller's buffers, a stop test
+    on the summed diff), computed with numpy in the identity vertex order, so that the
+    collectives and the loop of distributed.pagerank_on_gpus run between real gloo ranks."""
+
+    def __init__(self, g):
+        self.g, self.V = g, g.V
+        self.od = np.diff(g.indexofNodes).astype(np.float32)
+
+    def pagerank_part_begin(self, part, nparts, beta, delta, max_iter, con0, con1, diff):
+        self.r, self.n, self.S = part, nparts, -(-self.V // nparts)
+        self.lo, self.hi = part * self.S, min(self.V, (part + 1) * self.S)
+        self.beta, self.delta, self.max_iter = beta, delta, max(1, max_iter)
+        self.con, self.diff = [con0, con1], diff
+        V = self.V
+        self.pr = [np.full(V, np.float32(1.0) / np.float32(V), np.float32), np.zeros(V, np.float32)]
+        c = np.zeros(self.n * self.S, np.float32)
+        c[:V] = np.where(self.od > 0, self.pr[0] / np.maximum(self.od, 1), 0)
+        con0.copy_(torch_from(c))
+        self.it, self.done, self.last = 0, False, 0.0
+        return self.S
+
+    def pagerank_part_iterate(self, k):
+        if self.done:
+            return
+        g, c, nx = self.g, k & 1, (k + 1) & 1
+        con = self.con[c].numpy()
+        base = np.float32((1.0 - self.delta) / self.V)
+        d = 0.0
+        for v in range(self.lo, self.hi):
+            s = float(con[g.srcList[g.rev_indexofNodes[v]:g.rev_indexofNodes[v + 1]]].astype(np.float64).sum())
+            np_ = np.float32(base + np.float32(self.delta) * np.float32(s))
+            d += abs(float(np_) - float(self.pr[c][v]))
+            self.pr[nx][v] = np_
+            self.con[nx][v] = float(np_ / self.od[v]) if self.od[v] > 0 else 0.0
+        self.diff[0] = d
+        self.it += 1
+
+    def pagerank_part_decide(self):
+        if not self.done:
+            self.last = float(self.diff[0])
+            self.done = not (self.last > self.beta and self.it < self.max_iter)
+
+    def pagerank_part_state(self):
+        return self.it, self.done, self.last
+
+    def pagerank_part_ranks(self, out):
+        block = np.zeros(self.S, np.float32)
+        block[:self.hi - self.lo] = self.pr[self.it & 1][self.lo:self.hi]
+        out.copy_(torch_from(block))
+
+    def pagerank_part_finish(self, full, out):
+        out[:] = full.numpy()[:self.V]
+
+
+def torch_from(a):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(a))
+
+
+def _pr_rank_main(rank, world, port, out_dir):
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port), "RANK": str(rank),
+                       "WORLD_SIZE": str(world), "LOCAL_RANK": str(rank)})
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from starplat_b200 import generators as G
+    from starplat_b200.distributed import pagerank_on_gpus
+    from starplat_b200.replicas import Replicas
+    from test_replicas import _HostPartGraph
+
+    g = G.rmat(9, 8, seed=11, directed=True)
+    rep = Replicas(backend="gloo", timeout_s=60)
+    pr, it, diff = pagerank_on_gpus(_HostPartGraph(g), rep, beta=1e-7, check_every=3)
+    rep.close()
+    np.save(os.path.join(out_dir, f"pr{rank}.npy"), pr)
+    np.save(os.path.join(out_dir, f"it{rank}.npy"), np.array([it, diff]))
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_pagerank_split_over_ranks_matches_the_oracle(tmp_path, world):
+    # every rank owns one block of rows; the contrib blocks are all-gathered and the diff
+    # summed by gloo each iteration; every rank ends with the whole vector at the same
+    # iteration, equal to FP64 PageRank at that iteration count
+    from oracle import oracle as O
+    from starplat_b200 import generators as G
+
+    mp.start_processes(_pr_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    g = G.rmat(9, 8, seed=11, directed=True)
+    its = [np.load(tmp_path / f"it{r}.npy") for r in range(world)]
+    assert len({int(x[0]) for x in its}) == 1
+    it = int(its[0][0])
+    exact, it64, _ = O.pagerank(g.indexofNodes, g.rev_indexofNodes, g.srcList, 1e-7, 0.85, 100)
+    assert abs(it - it64) <= 1
+    exact, _, _ = O.pagerank(g.indexofNodes, g.rev_indexofNodes, g.srcList, 0.0, 0.85, it)
+    for r in range(world):
+        pr = np.load(tmp_path / f"pr{r}.npy").astype(np.float64)
+        assert np.abs(pr - exact).sum() < 1e-6
