@@ -141,6 +141,17 @@ int sp_graph_info(sp_graph_h g, int32_t* V, int64_t* E, int32_t* symmetric);
  *             hub_deg edges are cut into hub_chunk-edge pieces shared by all warps
  *             (defaults 64 and 64).
  *   "bc.batch"  BC: sources traversed together in one multi-source pass (1..64, default 64).
+ *   "bc.dir"  BC forward direction per level (one cooperative launch, sp_bc and
+ *             sp_bfs_sigma): 0 push (expand the level's entries along out-edges);
+ *             1 pull while bc.pull_alpha * (out-edges of the level's entries) exceeds the
+ *             in-edges of the vertices some source has not reached + V / 8 (pull: every
+ *             such vertex scans its in-edges for parents in the level, no atomics except
+ *             on vertices above 1024 in-edges); 2 a seeded random direction per level
+ *             ("bc.dir_seed", exploration); 3 pull at every level. Default 0. The decision
+ *             is taken on the device from counters every CTA reads after the same barrier.
+ *   "bc.pull_alpha"  factor of the bc.dir = 1 rule, in thousandths (default 1000).
+ *   "bc.trace"  1: record per level (entries, their out-edges, unreached in-edges, pull)
+ *             and the device timer; read with sp_bc_level_trace.
  *   "bc.cluster"  BC of many graphs (sp_bc_graphs): CTAs per graph, 1 (default), 2, 4 or 8;
  *             above 1 the CTAs of a thread-block cluster share a graph and synchronise with
  *             hardware cluster barriers. */
@@ -340,6 +351,11 @@ int sp_sched_epoch_load(const float* params, const float* feat_mean, const float
  * distance the threshold advanced, padding; times[k] = device timer (ns) at advance k,
  * times[n] at the end. *n = epochs recorded; up to cap records are copied. */
 int sp_sssp_epoch_trace(sp_graph_h g, float* records, unsigned long long* times, int32_t cap, int32_t* n);
+/* With knob "bc.trace" = 1 and bc.dir != 0, the last sp_bc grid run's levels (over all
+ * batches): records[k][4] = level entries, their out-edges, in-edges of vertices not
+ * yet reached by every source, 1 if pulled; times[k] = device timer (ns) at each level
+ * start, times[n] at the end of the run. No counterpart in the reference. */
+int sp_bc_level_trace(sp_graph_h g, float* records, unsigned long long* times, int32_t cap, int32_t* n);
 /* Replaces the generated Batch block of DynSSSP (DSL dynamicDSLCodes/dynamicBatchSSSP:
  * OnDelete + updateCSRDel + Decremental, then OnAdd + updateCSRAdd + Incremental): one
  * batch of edge updates as in sp_graph_update, then the distances from source on the

@@ -101,6 +101,7 @@ SIGNATURES = {
     "sp_sched_load": (ctypes.c_int, [vp, vp, vp]),
     "sp_sched_epoch_load": (ctypes.c_int, [vp, vp, vp]),
     "sp_sssp_epoch_trace": (ctypes.c_int, [vp, vp, vp, i32, P(i32)]),
+    "sp_bc_level_trace": (ctypes.c_int, [vp, vp, vp, i32, P(i32)]),
     "sp_sssp_features": (ctypes.c_int, [vp, vp, f64, i32, i32, vp]),
     "sp_pagerank_noalloc": (ctypes.c_int, [vp, vp, vp, i32, i64, f32, f32, i32, vp, P(i32), vp]),
 }

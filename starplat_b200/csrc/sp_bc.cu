@@ -61,6 +61,11 @@ constexpr int BU = 2;
 // 32-edge chunks of one entry whose loads and atomics are in flight together in the
 // forward sweep.
 constexpr int FU = 2;
+// Forward direction per level (knob bc.dir): 0 push only; 1 pull while
+// PULL_ALPHA * (out-edges of the level) > in-edges of the vertices some source has not
+// reached + V / 8 (knob bc.pull_alpha, in thousandths).
+constexpr int DIR_DEFAULT = 0;
+constexpr float PULL_ALPHA = 1.0f;
 
 struct Work {
   const int32_t* __restrict__ off;  // CSR rows of this graph (global edge indices)
@@ -88,7 +93,27 @@ struct Work {
   int hub_deg;                      // entries of vertices with more edges are split
   int hub_chunk;                    // edges per piece
   double* dacc;                     // [V][SW] FP64 partial dependencies of hub entries
+  // Forward direction per level (grid form): push expands the level's entries along
+  // their out-edges; pull has every vertex some source of the batch has not reached scan
+  // its in-edges for parents in the level (dense masks), with no atomics except on the
+  // vertices of more than PULL_SPLIT in-edges, whose edges are pieces shared by all warps.
+  const int32_t* __restrict__ roff;  // in-edges: the reverse CSR (off/adj when symmetric)
+  const int32_t* __restrict__ radj;
+  const int32_t* __restrict__ phub;  // [n_phub] vertices of more than PULL_SPLIT in-edges
+  const int32_t* __restrict__ phub_base;  // [n_phub + 1] first piece of each (exclusive prefix)
+  int n_phub;
+  int dir_policy;                   // 0 push; 1 rule: pull while alpha * (frontier edges) > unreached edges; 2 seeded random (exploration); 3 pull whenever allowed
+  float dir_alpha;
+  unsigned dir_seed;
+  long long e_in;                   // in-edges of the graph
+  unsigned long long* ldeg;         // [maxd + 2] out-edges of each level's entries
+  unsigned long long* full_in;      // in-edges of vertices every batch source has reached
+  float* trace;                     // [trace_cap][4] per level: entries, their out-edges, unreached in-edges, pull
+  unsigned long long* ttime;        // [trace_cap + 1] device timer at each level start, then the end
+  int trace_cap;
+  int* tcount;                      // levels traced
 };
+constexpr int PULL_SPLIT = 1024;    // in-edges per piece of a pull hub
 
 struct GridSync {
   GridBar* bar;
@@ -176,7 +201,7 @@ __device__ __forceinline__ int half_pick(unsigned& em, int lane, int& from) {
 // 16 when the batch has at most 16 sources, so that the two half-warps take two
 // edges per step instead of leaving lanes 16-31 idle.
 template <int NW, int GS>
-__device__ void expand_entry(const Work& W, int i, int lane, int eb, int ee) {
+__device__ void expand_entry(const Work& W, int i, int lane, int eb, int ee, unsigned long long* dslot = nullptr) {
   static_assert(GS == 32 || (GS == 16 && NW == 1), "half-warp steps hold up to 16 sources");
   constexpr int SW = 32 * NW;
   const int v = W.flv[i];
@@ -226,6 +251,15 @@ __device__ void expand_entry(const Work& W, int i, int lane, int eb, int ee) {
         }
         base += __popc(nm[f]);
       }
+      if (dslot) {  // the appended vertices' out-edges (the next level's push cost)
+        unsigned long long ds = 0;
+#pragma unroll
+        for (int f = 0; f < FU; ++f)
+          if (isnew[f]) ds += (unsigned long long)(W.off[w[f] + 1] - W.off[w[f]]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) ds += __shfl_xor_sync(0xffffffffu, ds, o);
+        if (lane == 0 && ds) atomicAdd(dslot, ds);
+      }
     }
 #pragma unroll
     for (int f = 0; f < FU; ++f) {
@@ -253,6 +287,130 @@ __device__ void expand_entry(const Work& W, int i, int lane, int eb, int ee) {
       }
     }
   }
+}
+
+// Pull: the parents of w among in-edges [eb, ee) that sit in the level (dense masks)
+// for sources w has not reached (sw): newm gets their sources, acc[k] the sum of their
+// sigma for source bit lane + 32k, in edge order. Warp-uniform newm.
+template <int NW>
+__device__ __forceinline__ void pull_scan(const Work& W, unsigned long long sw, int eb, int ee, int lane,
+                                          unsigned long long& newm, double (&acc)[NW]) {
+  constexpr int SW = 32 * NW;
+  for (int c = eb; c < ee; c += 32) {
+    const int j = c + lane;
+    const int v = j < ee ? W.radj[j] - W.vbase : -1;
+    const unsigned long long fm = v >= 0 ? W.dense[v] & ~sw : 0ull;
+    unsigned em = __ballot_sync(0xffffffffu, fm != 0ull);
+    while (em) {
+      const int l = __ffs(em) - 1;
+      em &= em - 1;
+      const unsigned long long fl = shfl64(fm, l);
+      const int vl = __shfl_sync(0xffffffffu, v, l);
+      newm |= fl;
+#pragma unroll
+      for (int k = 0; k < NW; ++k) {
+        const int b = lane + 32 * k;
+        if ((fl >> b) & 1ull) acc[k] += W.sigma[(size_t)vl * SW + b];
+      }
+    }
+  }
+}
+
+// A warp's appends to the level list, 32 at a time (one counter atomic each); the
+// out-edges of the appended vertices go to ldeg[slot].
+struct AppendBuf {
+  int32_t* s;  // this warp's 32 slots in shared memory
+  int n;       // warp-uniform
+};
+
+__device__ __forceinline__ void append_flush(const Work& W, AppendBuf& ab, int lane, int slot) {
+  if (ab.n == 0) return;
+  __syncwarp();
+  int base = 0;
+  if (lane == 0) base = atomicAdd(W.cnt, ab.n);
+  base = __shfl_sync(0xffffffffu, base, 0);
+  unsigned long long dsum = 0;
+  if (lane < ab.n) {
+    const int w = ab.s[lane];
+    if (base + lane < W.cap)
+      W.flv[base + lane] = w;
+    else
+      atomicExch(W.err, 1);
+    dsum = (unsigned long long)(W.off[w + 1] - W.off[w]);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) dsum += __shfl_xor_sync(0xffffffffu, dsum, o);
+  if (lane == 0 && dsum) atomicAdd(W.ldeg + slot, dsum);
+  __syncwarp();
+  ab.n = 0;
+}
+
+// One pull level: the level's masks are in dense. Vertices of at most PULL_SPLIT
+// in-edges are scanned by one warp each (their sigma and next mask written directly);
+// the pieces of the larger ones are shared by all warps and merged with atomics (FP64
+// adds of integers, exact in any order; the first piece to set a next-mask bit appends
+// the vertex). `slot` = the next level's index in ldeg.
+template <int NW>
+__device__ void pull_level(const Work& W, unsigned long long full, int lane, int gw, int nw, int slot,
+                           int32_t* s_app) {
+  constexpr int SW = 32 * NW;
+  AppendBuf ab{s_app + (threadIdx.x >> 5) * 32, 0};
+  for (int w = gw; w < W.V; w += nw) {
+    const int eb = W.roff[w], ee = W.roff[w + 1];
+    if (ee - eb > PULL_SPLIT) continue;
+    const unsigned long long sw = W.seen[w];
+    if ((sw & full) == full || ee == eb) continue;
+    unsigned long long newm = 0;
+    double acc[NW];
+#pragma unroll
+    for (int k = 0; k < NW; ++k) acc[k] = 0.0;
+    pull_scan<NW>(W, sw, eb, ee, lane, newm, acc);
+    if (newm) {
+#pragma unroll
+      for (int k = 0; k < NW; ++k) {
+        const int b = lane + 32 * k;
+        if ((newm >> b) & 1ull) W.sigma[(size_t)w * SW + b] = acc[k];
+      }
+      if (lane == 0) {
+        W.nxt[w] = newm;
+        ab.s[ab.n] = w;
+      }
+      if (++ab.n == 32) append_flush(W, ab, lane, slot);
+    }
+  }
+  const int np = W.n_phub ? W.phub_base[W.n_phub] : 0;
+  for (int p = gw; p < np; p += nw) {
+    int lo = 0, hi = W.n_phub - 1;  // the last hub whose first piece <= p
+    while (lo < hi) {
+      const int m = (lo + hi + 1) >> 1;
+      if (W.phub_base[m] <= p) lo = m; else hi = m - 1;
+    }
+    const int w = W.phub[lo];
+    const unsigned long long sw = W.seen[w];
+    if ((sw & full) == full) continue;
+    const int eb = W.roff[w] + (p - W.phub_base[lo]) * PULL_SPLIT;
+    const int ee = min(eb + PULL_SPLIT, W.roff[w + 1]);
+    unsigned long long newm = 0;
+    double acc[NW];
+#pragma unroll
+    for (int k = 0; k < NW; ++k) acc[k] = 0.0;
+    pull_scan<NW>(W, sw, eb, ee, lane, newm, acc);
+    if (newm) {
+#pragma unroll
+      for (int k = 0; k < NW; ++k) {
+        const int b = lane + 32 * k;
+        if ((newm >> b) & 1ull) atomicAdd(&W.sigma[(size_t)w * SW + b], acc[k]);
+      }
+      int first = 0;
+      if (lane == 0) {
+        first = atomicOr(&W.nxt[w], newm) == 0ull;
+        if (first) ab.s[ab.n] = w;
+      }
+      first = __shfl_sync(0xffffffffu, first, 0);
+      if (first && ++ab.n == 32) append_flush(W, ab, lane, slot);
+    }
+  }
+  append_flush(W, ab, lane, slot);
 }
 
 // piece = false: the whole entry, dependencies written to delta; piece = true: an
@@ -360,19 +518,46 @@ __device__ void backward_entry(const Work& W, int i, int lane, int eb, int ee, b
 
 // One batch of nsrc (<= 32*NW) sources (local ids). Every participating thread
 // calls this with the same arguments; S provides the barrier and thread ranks.
+// The direction of level d (every thread computes the same answer from values read
+// after the same barrier): pull when the policy and the statistics say so.
+__device__ __forceinline__ bool pull_this_level(const Work& W, int d, int nent, int V) {
+  if (W.dir_policy == 0 || W.radj == nullptr) return false;
+  if (W.dir_policy == 3) return true;
+  if (W.dir_policy == 2) {
+    unsigned h = W.dir_seed * 0x9e3779b9u ^ ((unsigned)d * 0x85ebca6bu);
+    h ^= h >> 15;
+    h *= 0x2c1b3c6du;
+    h ^= h >> 13;
+    return (h & 1u) != 0u;
+  }
+  // rule: a push level walks the level's out-edges with atomics on every new vertex;
+  // a pull level scans the in-edges of every vertex not yet reached by all sources
+  const double mf = (double)*(volatile unsigned long long*)(W.ldeg + d);
+  const double mu = (double)W.e_in - (double)*(volatile unsigned long long*)W.full_in;
+  return (double)W.dir_alpha * mf > mu + 0.125 * (double)V && nent > 0;
+}
+
 template <int NW, int GS, class S>
 __device__ bool run_batch(const Work& W, const int32_t* srcs, int nsrc, S& sync, int32_t* lvl_out = nullptr,
-                          double* sig_out = nullptr) {
+                          double* sig_out = nullptr, int32_t* s_app = nullptr) {
   constexpr int SW = 32 * NW;
   const int gt = sync.tid(), nt = sync.nthreads();
   const int lane = threadIdx.x & 31;
   const int gw = gt >> 5, nw = nt >> 5;
+  const bool dirs = s_app != nullptr && W.dir_policy != 0 && W.radj != nullptr;
+  const unsigned long long full = nsrc >= 64 ? ~0ull : ((1ull << nsrc) - 1ull);
+  if (dirs) {
+    for (int k = gt; k < W.maxd + 2; k += nt) W.ldeg[k] = 0ull;
+    if (gt == 0) *W.full_in = 0ull;
+    if (!sync.sync()) return false;
+  }
   for (int k = gt; k < nsrc; k += nt) {
     const int v = srcs[k];
     W.flv[k] = v;
     W.flm[k] = 1ull << k;
     W.sigma[(size_t)v * SW + k] = 1.0;
     atomicOr(&W.seen[v], 1ull << k);
+    if (dirs) atomicAdd(W.ldeg, (unsigned long long)(W.off[v + 1] - W.off[v]));
   }
   if (gt == 0) {
     W.lo[0] = 0;
@@ -388,29 +573,54 @@ __device__ bool run_batch(const Work& W, const int32_t* srcs, int nsrc, S& sync,
       if (gt == 0) atomicExch(W.err, 2);
       return false;
     }
-    for (int i = b + gw; i < e; i += nw)
-      if (!queue_hub(W, i, lane)) expand_entry<NW, GS>(W, i, lane, W.off[W.flv[i]], W.off[W.flv[i] + 1]);
-    if (!sync.sync()) return false;
-    if (W.hub_cap) {
+    const bool pull = dirs && pull_this_level(W, d, e - b, W.V);
+    if (dirs && W.trace && gt == 0) {
+      const int t = atomicAdd(W.tcount, 1);
+      if (t < W.trace_cap) {
+        float* r = W.trace + (size_t)t * 4;
+        r[0] = (float)(e - b);
+        r[1] = (float)*(volatile unsigned long long*)(W.ldeg + d);
+        r[2] = (float)((double)W.e_in - (double)*(volatile unsigned long long*)W.full_in);
+        r[3] = pull ? 1.0f : 0.0f;
+        unsigned long long now;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+        W.ttime[t] = now;
+      }
+    }
+    if (pull) {
+      for (int i = b + gt; i < e; i += nt) W.dense[W.flv[i]] = W.flm[i];
+      if (!sync.sync()) return false;
+      pull_level<NW>(W, full, lane, gw, nw, d + 1, s_app);
+      if (!sync.sync()) return false;
+      for (int i = b + gt; i < e; i += nt) W.dense[W.flv[i]] = 0ull;
+    } else {
+      for (int i = b + gw; i < e; i += nw)
+        if (!queue_hub(W, i, lane))
+          expand_entry<NW, GS>(W, i, lane, W.off[W.flv[i]], W.off[W.flv[i] + 1], dirs ? W.ldeg + d + 1 : nullptr);
+      if (!sync.sync()) return false;
+    }
+    if (!pull && W.hub_cap) {
       const unsigned long long hc = *(volatile unsigned long long*)W.hub_cnt;
       const int nh = min((int)(hc >> 32), W.hub_cap), np = (int)(hc & 0xffffffffull);
       if (nh > 0) {
         for (int p = gw; p < np; p += nw) {
           int i, eb, ee;
           hub_piece(W, nh, p, i, eb, ee);
-          expand_entry<NW, GS>(W, i, lane, eb, ee);
+          expand_entry<NW, GS>(W, i, lane, eb, ee, dirs ? W.ldeg + d + 1 : nullptr);
         }
         if (!sync.sync()) return false;
       }
     }
     const int c = min(*(volatile int*)W.cnt, W.cap);
-    if (W.hub_cap && gt == 0) *W.hub_cnt = 0ull;  // read by every CTA before the barrier above
+    if (!pull && W.hub_cap && gt == 0) *W.hub_cnt = 0ull;  // read by every CTA before the barrier above
     for (int i = e + gt; i < c; i += nt) {
       const int w = W.flv[i];
       const unsigned long long mk = W.nxt[w];
       W.flm[i] = mk;
-      W.seen[w] |= mk;
+      const unsigned long long was = W.seen[w];
+      W.seen[w] = was | mk;
       W.nxt[w] = 0ull;
+      if (dirs && (was | mk) == full) atomicAdd(W.full_in, (unsigned long long)(W.roff[w + 1] - W.roff[w]));
     }
     if (gt == 0) W.lo[d + 2] = c;
     if (!sync.sync()) return false;
@@ -494,11 +704,11 @@ __device__ bool run_batch(const Work& W, const int32_t* srcs, int nsrc, S& sync,
 // thread of the team sees the same nsrc, so all take the same branch).
 template <int NW, class S>
 __device__ bool run_batch_any(const Work& W, const int32_t* srcs, int nsrc, S& sync, int32_t* lvl_out = nullptr,
-                              double* sig_out = nullptr) {
+                              double* sig_out = nullptr, int32_t* s_app = nullptr) {
   if constexpr (NW == 1) {
-    if (nsrc <= 16) return run_batch<1, 16>(W, srcs, nsrc, sync, lvl_out, sig_out);
+    if (nsrc <= 16) return run_batch<1, 16>(W, srcs, nsrc, sync, lvl_out, sig_out, s_app);
   }
-  return run_batch<NW, 32>(W, srcs, nsrc, sync, lvl_out, sig_out);
+  return run_batch<NW, 32>(W, srcs, nsrc, sync, lvl_out, sig_out, s_app);
 }
 
 struct GridArgs {
@@ -513,9 +723,10 @@ struct GridArgs {
 
 template <int NW>
 __global__ void __launch_bounds__(GRID_THREADS, 4) k_bc_grid(GridArgs a) {
+  __shared__ int32_t s_app[GRID_THREADS];  // pull levels: 32 append slots per warp
   GridSync gs{a.bar};
   for (int s0 = 0; s0 < a.nsrc; s0 += a.batch) {
-    if (!run_batch_any<NW>(a.W, a.srcs + s0, min(a.batch, a.nsrc - s0), gs, a.lvl_out, a.sig_out)) {
+    if (!run_batch_any<NW>(a.W, a.srcs + s0, min(a.batch, a.nsrc - s0), gs, a.lvl_out, a.sig_out, s_app)) {
       if (threadIdx.x == 0 && a.bar->error) atomicCAS(a.W.err, 0, 3);
       return;
     }
@@ -651,6 +862,12 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(CTA_THREADS) k_bc_cl
   }
 }
 
+__global__ void k_stamp_time(unsigned long long* t) {
+  unsigned long long now;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+  *t = now;
+}
+
 __global__ void k_zero(void* p, size_t words) {
   unsigned long long* q = (unsigned long long*)p;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < words; i += (size_t)gridDim.x * blockDim.x) q[i] = 0ull;
@@ -699,6 +916,16 @@ __global__ void k_plain_bwd(int V, const int32_t* __restrict__ off, const int32_
 }  // namespace bc
 
 struct BcPlan {
+  // pull levels: the vertices of more than PULL_SPLIT in-edges and their piece prefix
+  // (built once per graph), the per-level out-edge counts and the reached in-edges
+  bool phub_built = false;
+  int n_phub = 0;
+  dbuf<int32_t> phub, phub_base;
+  dbuf<unsigned long long> ldeg;
+  dbuf<float> trace;
+  dbuf<unsigned long long> ttime;
+  dbuf<int> tcount;
+  int trace_n = 0;
   dbuf<double> sigma, bc, dacc;
   dbuf<int32_t> hub_ent, hub_base;
   dbuf<unsigned long long> hub_cnt;
@@ -777,6 +1004,63 @@ static int bc_grid(sp_graph* g, const int32_t* d_srcs, int nsrc, int batch_hint,
   W.hub_deg = g->bc_hub_deg > 0 ? g->bc_hub_deg : bc::HUB_DEG;
   W.hub_chunk = g->bc_hub_chunk > 0 ? g->bc_hub_chunk : bc::HUB_CHUNK;
   W.dacc = p->dacc.p;
+  // forward direction per level
+  W.dir_policy = g->bc_dir >= 0 ? g->bc_dir : bc::DIR_DEFAULT;
+  W.dir_alpha = g->bc_pull_alpha > 0 ? (float)g->bc_pull_alpha / 1000.0f : bc::PULL_ALPHA;
+  W.dir_seed = (unsigned)g->bc_dir_seed;
+  W.roff = nullptr;
+  W.radj = nullptr;
+  W.phub = nullptr;
+  W.phub_base = nullptr;
+  W.n_phub = 0;
+  W.e_in = g->E;
+  W.trace = nullptr;
+  W.ttime = nullptr;
+  W.trace_cap = 0;
+  W.tcount = nullptr;
+  p->trace_n = 0;
+  if (W.dir_policy != 0) {
+    SP_TRY(ensure_reverse(g));
+    if (!p->phub_built) {
+      std::vector<int32_t> roff(V + 1);
+      SP_TRY(copy_out(roff.data(), g->roff.p, sizeof(int32_t) * (V + 1), s));
+      std::vector<int32_t> hubs, base{0};
+      for (int v = 0; v < V; ++v) {
+        const int d = roff[v + 1] - roff[v];
+        if (d > bc::PULL_SPLIT) {
+          hubs.push_back(v);
+          base.push_back(base.back() + (d + bc::PULL_SPLIT - 1) / bc::PULL_SPLIT);
+        }
+      }
+      p->n_phub = (int)hubs.size();
+      SP_TRY(p->phub.alloc(std::max<size_t>(1, hubs.size())));
+      SP_TRY(p->phub_base.alloc(base.size()));
+      if (!hubs.empty())
+        SP_CHECK_CUDA(cudaMemcpyAsync(p->phub.p, hubs.data(), sizeof(int32_t) * hubs.size(), cudaMemcpyHostToDevice, s));
+      SP_CHECK_CUDA(cudaMemcpyAsync(p->phub_base.p, base.data(), sizeof(int32_t) * base.size(), cudaMemcpyHostToDevice, s));
+      SP_CHECK_CUDA(cudaStreamSynchronize(s));
+      p->phub_built = true;
+    }
+    SP_TRY(p->ldeg.alloc((size_t)maxd + 3));  // per level, then the reached in-edges
+    W.roff = g->roff.p;
+    W.radj = g->radj.p;
+    W.phub = p->phub.p;
+    W.phub_base = p->phub_base.p;
+    W.n_phub = p->n_phub;
+    W.ldeg = p->ldeg.p;
+    W.full_in = p->ldeg.p + maxd + 2;
+    if (g->bc_trace) {
+      constexpr int CAP = 1 << 14;
+      SP_TRY(p->trace.alloc((size_t)CAP * 4));
+      SP_TRY(p->ttime.alloc((size_t)CAP + 1));
+      SP_TRY(p->tcount.alloc(1));
+      SP_CHECK_CUDA(cudaMemsetAsync(p->tcount.p, 0, sizeof(int), s));
+      W.trace = p->trace.p;
+      W.ttime = p->ttime.p;
+      W.trace_cap = CAP;
+      W.tcount = p->tcount.p;
+    }
+  }
   a.srcs = d_srcs;
   a.nsrc = nsrc;
   a.batch = batch;
@@ -795,6 +1079,13 @@ static int bc_grid(sp_graph* g, const int32_t* d_srcs, int nsrc, int batch_hint,
   if (herr) {
     set_error("sp_bc: device error %d (1 level lists full, 2 deeper than %d levels, 3 barrier timeout)", herr, maxd);
     return herr == 3 ? SP_ERR_TIMEOUT : SP_ERR_UNSUPPORTED;
+  }
+  if (W.trace) {  // the end of the last traced level
+    int n = 0;
+    SP_TRY(copy_out(&n, p->tcount.p, sizeof(int), s));
+    p->trace_n = std::min(n, W.trace_cap);
+    bc::k_stamp_time<<<1, 1, 0, s>>>(p->ttime.p + p->trace_n);
+    SP_CHECK_LAUNCH();
   }
   return SP_OK;
 }
@@ -1095,4 +1386,18 @@ extern "C" int sp_bc_dynamic(sp_graph_h g, int64_t n, const char* type, const in
     }
   if (n > 0) SP_TRY(update_graph(g, n, type, src, dst, weight));
   return sp_bc(g, hs.data(), nsrc, BC, SP_BC_BATCHED);
+}
+
+extern "C" int sp_bc_level_trace(sp_graph_h g, float* records, unsigned long long* times, int32_t cap, int32_t* n) {
+  using namespace sp;
+  if (!g || !n || cap < 0 || (cap > 0 && (!records || !times))) {
+    set_error("sp_bc_level_trace: invalid argument");
+    return SP_ERR_INVALID;
+  }
+  const int have = g->bc ? g->bc->trace_n : 0;
+  *n = have;
+  const int k = std::min(have, (int)cap);
+  if (k == 0) return SP_OK;
+  SP_TRY(copy_out(records, g->bc->trace.p, sizeof(float) * 4 * k, g->stream));
+  return copy_out(times, g->bc->ttime.p, sizeof(unsigned long long) * (k + 1), g->stream);
 }

@@ -606,6 +606,34 @@ int sp_tune_set(sp_graph_h g, const char* key, int64_t value) {
     g->pr_order = (int32_t)value;
     return SP_OK;
   }
+  if (!strcmp(key, "bc.dir")) {
+    if (value < -1 || value > 3) {
+      set_error("sp_tune_set: bc.dir must be -1, 0, 1, 2 or 3");
+      return SP_ERR_INVALID;
+    }
+    g->bc_dir = (int32_t)value;
+    return SP_OK;
+  }
+  if (!strcmp(key, "bc.pull_alpha")) {
+    if (value < 0 || value > 1000000000) {
+      set_error("sp_tune_set: bc.pull_alpha must be in [0, 1e9] (thousandths)");
+      return SP_ERR_INVALID;
+    }
+    g->bc_pull_alpha = (int32_t)value;
+    return SP_OK;
+  }
+  if (!strcmp(key, "bc.dir_seed")) {
+    g->bc_dir_seed = (int32_t)value;
+    return SP_OK;
+  }
+  if (!strcmp(key, "bc.trace")) {
+    if (value != 0 && value != 1) {
+      set_error("sp_tune_set: bc.trace must be 0 or 1");
+      return SP_ERR_INVALID;
+    }
+    g->bc_trace = (int32_t)value;
+    return SP_OK;
+  }
   if (!strcmp(key, "sssp.epoch")) {
     if (value < -1 || value > 2) {
       set_error("sp_tune_set: sssp.epoch must be -1, 0, 1 or 2");
@@ -752,6 +780,14 @@ int sp_tune_get(sp_graph_h g, const char* key, int64_t* value) {
   }
   if (!strcmp(key, "sssp.epoch")) {
     *value = g->sssp_epoch;
+    return SP_OK;
+  }
+  if (!strcmp(key, "bc.dir")) {
+    *value = g->bc_dir;
+    return SP_OK;
+  }
+  if (!strcmp(key, "bc.pull_alpha")) {
+    *value = g->bc_pull_alpha;
     return SP_OK;
   }
   if (!strcmp(key, "sssp.last_epochs")) {

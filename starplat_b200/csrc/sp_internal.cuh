@@ -181,6 +181,10 @@ struct sp_graph {
   int32_t sssp_last_epolicy = 0;  // the width policy the last solve ran
   int32_t sssp_last_batch = 0;  // sources per launch of the last batched run (reporting)
   int32_t tc_cta_warps = -1;  // TC: warps per CTA of the shared-bitmap kernel (-1 = default, 0 = off)
+  int32_t bc_dir = -1;        // BC forward direction policy (-1 = default)
+  int32_t bc_pull_alpha = 0;  // BC pull rule factor in thousandths (0 = default)
+  int32_t bc_dir_seed = 0;    // BC direction exploration seed
+  int32_t bc_trace = 0;       // 1: record the per-level trace of the grid form
   int32_t bc_batch = 0;
   int32_t bc_hub_deg = 0;  // BC: split level-list entries above this degree (0 = default)
   int32_t bc_hub_chunk = 0;  // BC: edges per piece of a split entry (0 = default)

@@ -15,19 +15,19 @@
 //     edges are flattened over its lanes (an exclusive scan of the degrees), 32
 //     edges per step, so a 4-neighbour grid vertex costs one step, not four; a
 //     small frontier is spread over all warps. SU steps go together: their dist
-//     loads, atomicMins and stamp exchanges are all issued before any is waited
+//     loads, atomicMins and mark updates are all issued before any is waited
 //     for, and their queue appends share one counter atomic. Vertices above hub_deg out-edges
 //     (R-MAT hubs) are queued in a hub list whose chunks all warps share in the
 //     next round; queue appends are warp-aggregated and de-duplicated with
-//     per-round / per-epoch stamps;
+//     per-round / per-epoch mark bitmaps;
 //   * warp-local cascades (rounds whose frontier is at most 32 vertices per warp):
 //     a vertex a warp improves below the bucket threshold goes to the warp's ring
 //     in shared memory instead of the next round's queue, and the warp relaxes its
 //     ring until it is empty or its edge budget (sssp.local warp steps) is spent,
 //     then moves what is left to the queue. On a high-diameter graph one round then
 //     covers many hops of the same bucket, where each hop used to cost a grid
-//     barrier. Ring entries carry no stamp: every improvement puts its vertex in
-//     the ring (or, when full, in the stamped queue), so the last improvement of a
+//     barrier. Ring entries carry no mark: every improvement puts its vertex in
+//     the ring (or, when full, in the marked queue), so the last improvement of a
 //     vertex is always relaxed after it;
 //   * when Q empties, the threshold jumps to the bucket of the smallest far
 //     distance and F is split into Q and the next far pile.
@@ -67,7 +67,7 @@ struct Ctl {
   int fmin[3];     // per epoch: smallest distance pushed to the far pile
   int rounds;      // relax rounds executed
   int epochs;
-  int status;      // 0 ok, 1 timeout / round cap, 2 negative cycle suspected
+  int status;      // 0 ok, 1 timeout / round cap, 2 negative cycle suspected, 3 a buffer overflowed
   int pad;
   unsigned long long relaxed;  // edges relaxed over the run (work inflation = relaxed / E_r)
 };
@@ -81,8 +81,13 @@ struct Args {
   int32_t* f[2];
   int32_t* hv[2];      // hub vertices per round (ping-pong)
   int32_t* hbase[2];   // first chunk index of each hub entry (increasing)
-  int32_t* qstamp;
-  int32_t* fstamp;
+  // Marks (one bit per vertex, 4 * nwords words): qbits(k) = bits + k * nwords says a
+  // vertex is queued for a round of parity k, fbits(k) = bits + (2 + k) * nwords that it
+  // is in the far pile of an epoch of parity k. Every phase clears the generation that no
+  // phase of its own touches (k_delta's phases), so each bitmap is zero before its first
+  // mark. At V = 2^23 they take 4 MB where two int32 stamp arrays took 67 MB of L2.
+  unsigned* bits;
+  int nwords;
   Ctl* ctl;
   int V;
   long long delta;      // bucket width; >= INT_MAX means a single bucket
@@ -130,7 +135,7 @@ struct Ring {
 
 // Adjacency and weights are streamed: each is read once per expansion of its vertex,
 // so their loads skip L1 and are marked first to leave L2, which keeps dist, the
-// stamps and the offsets (random accesses) resident. R-MAT 23: 9.1 -> 7.3 ms; grid
+// mark bitmaps and the offsets (random accesses) resident. R-MAT 23: 9.1 -> 7.3 ms; grid
 // 4096^2: 33.3 -> 33.8 ms. Marking the dist loads evict-last on top gained nothing.
 __device__ __forceinline__ int ld_stream(const int32_t* p) {
   unsigned long long pol;
@@ -140,8 +145,28 @@ __device__ __forceinline__ int ld_stream(const int32_t* p) {
   return v;
 }
 
+// Sets vertex u's bit in bm; true for the one caller that set it first.
+__device__ __forceinline__ bool mark(unsigned* bm, int u) {
+  const unsigned b = 1u << (u & 31);
+  return (atomicOr(bm + (u >> 5), b) & b) == 0u;
+}
+__device__ __forceinline__ unsigned* qbits(const Args& a, int round) { return a.bits + (size_t)(round & 1) * a.nwords; }
+__device__ __forceinline__ unsigned* fbits(const Args& a, int epoch) {
+  return a.bits + (size_t)(2 + (epoch & 1)) * a.nwords;
+}
+
+// A queue, hub list or far pile holds at most V entries (the marks admit each vertex
+// once per round or epoch); an append past that is dropped and flagged (status 3), so
+// a broken mark could never write outside the buffer.
+__device__ __forceinline__ void put(const Args& a, int32_t* buf, int idx, int val) {
+  if (idx < a.V)
+    buf[idx] = val;
+  else
+    atomicExch(&a.ctl->status, 3);
+}
+
 // Warp-aggregated append of `want` lanes into buf via counter.
-__device__ __forceinline__ void warp_push(bool want, int val, int32_t* buf, int* counter) {
+__device__ __forceinline__ void warp_push(const Args& a, bool want, int val, int32_t* buf, int* counter) {
   const unsigned m = __ballot_sync(0xffffffffu, want);
   if (!m) return;
   const int lane = threadIdx.x & 31;
@@ -149,7 +174,7 @@ __device__ __forceinline__ void warp_push(bool want, int val, int32_t* buf, int*
   int base = 0;
   if (lane == leader) base = atomicAdd(counter, __popc(m));
   base = __shfl_sync(0xffffffffu, base, leader);
-  if (want) buf[base + __popc(m & ((1u << lane) - 1u))] = val;
+  if (want) put(a, buf, base + __popc(m & ((1u << lane) - 1u)), val);
 }
 
 // Queue u for the next round: hubs go to the hub list (with their chunk count),
@@ -168,15 +193,15 @@ __device__ __forceinline__ void queue_push(const Args& a, bool want, int u, int3
   if (hub) {
     const unsigned long long old = atomicAdd(hcnt, (1ull << 32) | (unsigned long long)nch);
     const int idx = (int)(old >> 32);
-    HV[idx] = u;
-    HB[idx] = (int)(old & 0xffffffffull);
+    put(a, HV, idx, u);
+    put(a, HB, idx, (int)(old & 0xffffffffull));
   }
-  warp_push(want && !hub, u, QN, qnext);
+  warp_push(a, want && !hub, u, QN, qnext);
 }
 
 // Below-threshold improvements of this step (want lanes). LOCAL: into the warp's
-// ring while it has room, the rest stamped into the next round's queue. Otherwise
-// the caller's relax already stamped them: straight into the queue.
+// ring while it has room, the rest marked into the next round's queue. Otherwise
+// the caller's relax already marked them: straight into the queue.
 template <bool LOCAL>
 __device__ __forceinline__ void push_near(const Args& a, bool want, int u, int round, const Out& o, Ring& r) {
   if (LOCAL) {
@@ -188,13 +213,13 @@ __device__ __forceinline__ void push_near(const Args& a, bool want, int u, int r
     const bool mine = want && rank < room;
     if (mine) r.s[(r.head + r.cnt + rank) & (RING - 1)] = u;
     r.cnt += min(__popc(m), room);
-    want = want && !mine && atomicExch(a.qstamp + u, round + 1) != round + 1;
+    want = want && !mine && mark(qbits(a, round + 1), u);
   }
   queue_push(a, want, u, o.QN, o.qnext, o.HV, o.HB, o.hnext);
 }
 
 // Relax N edges per lane (nd = dist + weight for target u; nd >= INT_MAX: no edge):
-// every dist load is issued, then every atomicMin, then every stamp exchange, before
+// every dist load is issued, then every atomicMin, then every mark update, before
 // any result is waited for. res: 1 = improved below the bucket threshold (with
 // STAMP, only the first such improvement of u this round), 2 = improved above it
 // and first in the far pile this epoch, 0 = nothing to queue. When two edges of a
@@ -216,10 +241,10 @@ __device__ __forceinline__ void relax_group(const Args& a, const int (&u)[N], co
     const int ndi = (int)nd[q];
     if (ndi < old[q]) {
       if (nd[q] < thr) {
-        res[q] = (!STAMP || atomicExch(a.qstamp + u[q], round + 1) != round + 1) ? 1 : 0;
+        res[q] = (!STAMP || mark(qbits(a, round + 1), u[q])) ? 1 : 0;
       } else {
         atomicMin(fmin_slot, ndi);
-        res[q] = atomicExch(a.fstamp + u[q], epoch) != epoch ? 2 : 0;
+        res[q] = mark(fbits(a, epoch), u[q]) ? 2 : 0;
       }
     }
   }
@@ -227,7 +252,7 @@ __device__ __forceinline__ void relax_group(const Args& a, const int (&u)[N], co
 
 // Appends the flagged values of N steps to buf with one counter atomic per warp.
 template <int N>
-__device__ __forceinline__ void warp_push_many(const bool (&want)[N], const int (&val)[N], int32_t* buf,
+__device__ __forceinline__ void warp_push_many(const Args& a, const bool (&want)[N], const int (&val)[N], int32_t* buf,
                                                int* counter) {
   unsigned m[N];
   int n = 0;
@@ -244,7 +269,7 @@ __device__ __forceinline__ void warp_push_many(const bool (&want)[N], const int 
   const unsigned lt = (1u << lane) - 1u;
 #pragma unroll
   for (int q = 0; q < N; ++q) {
-    if (want[q]) buf[base + __popc(m[q] & lt)] = val[q];
+    if (want[q]) put(a, buf, base + __popc(m[q] & lt), val[q]);
     base += __popc(m[q]);
   }
 }
@@ -269,12 +294,12 @@ __device__ __forceinline__ void queue_push_many(const Args& a, const bool (&want
     if (nch[q]) {
       const unsigned long long old = atomicAdd(o.hnext, (1ull << 32) | (unsigned long long)nch[q]);
       const int idx = (int)(old >> 32);
-      o.HV[idx] = u[q];
-      o.HB[idx] = (int)(old & 0xffffffffull);
+      put(a, o.HV, idx, u[q]);
+      put(a, o.HB, idx, (int)(old & 0xffffffffull));
     }
     nr[q] = want[q] && nch[q] == 0;
   }
-  warp_push_many<N>(nr, u, o.QN, o.qnext);
+  warp_push_many<N>(a, nr, u, o.QN, o.qnext);
 }
 
 // Pushes of one group: below-threshold improvements to the ring (LOCAL) or the next
@@ -294,7 +319,7 @@ __device__ __forceinline__ void push_group(const Args& a, const int (&res)[N], c
   } else {
     queue_push_many<N>(a, nr, u, o);
   }
-  warp_push_many<N>(fr, u, o.F, o.fcnt);
+  warp_push_many<N>(a, fr, u, o.F, o.fcnt);
 }
 
 // Relax the out-edges of the warp's batch: lane i holds frontier vertex v (or -1).
@@ -320,8 +345,7 @@ __device__ __forceinline__ void relax_batch(const Args& a, int v, long long thr,
       dv = __ldcg(a.dist + v);
     }
   }
-  if (LOCAL) queue_push(a, hub && atomicExch(a.qstamp + v, round + 1) != round + 1, v, o.QN, o.qnext, o.HV, o.HB,
-                        o.hnext);
+  if (LOCAL) queue_push(a, hub && mark(qbits(a, round + 1), v), v, o.QN, o.qnext, o.HV, o.HB, o.hnext);
   int inc = d;
 #pragma unroll
   for (int k = 1; k < 32; k <<= 1) {
@@ -404,7 +428,7 @@ __device__ __forceinline__ void cascade(const Args& a, long long thr, int round,
     bool want = false;
     if (i < r.cnt) {
       u = r.s[(r.head + i) & (RING - 1)];
-      want = atomicExch(a.qstamp + u, round + 1) != round + 1;
+      want = mark(qbits(a, round + 1), u);
     }
     queue_push(a, want, u, o.QN, o.qnext, o.HV, o.HB, o.hnext);
   }
@@ -496,16 +520,20 @@ __device__ __forceinline__ void delta_run(const Args& a, const int blk, const in
   int f_prev = 2, round_mark = 0;
   unsigned long long relaxed_mark = 0;
   while (true) {
-    const int qv = *(volatile int*)&c->qcount[round % 3];
+    // counts clamped to the buffers (an overflow was already flagged by put())
+    const int qv = min(*(volatile int*)&c->qcount[round % 3], a.V);
     const unsigned long long hc = *(volatile unsigned long long*)&c->hcount[round % 3];
-    const int hn = (int)(hc >> 32), hchunks = (int)(hc & 0xffffffffull);
+    const int hn = min((int)(hc >> 32), a.V), hchunks = (int)(hc & 0xffffffffull);
     const int qn = qv;
-    const int fn = *(volatile int*)&c->fcount[epoch % 3];
+    const int fn = min(*(volatile int*)&c->fcount[epoch % 3], a.V);
     if (qv == 0 && hn == 0 && fn == 0) break;
     if ((long long)round >= a.max_rounds) {
       if (blk == 0 && threadIdx.x == 0) c->status = 1;
       break;
     }
+    // this phase marks round + 1 (and the current epoch); the marks of `round` are
+    // tested by no one from here on: clear them for round + 2
+    for (int i = blk * THREADS + threadIdx.x; i < a.nwords; i += nblk * THREADS) qbits(a, round)[i] = 0u;
     if (qv > 0 || hn > 0) {
       const int32_t* Q = a.q[round & 1];
       const Out o = {a.q[(round + 1) & 1], &c->qcount[(round + 1) % 3], a.hv[(round + 1) & 1],
@@ -593,6 +621,8 @@ __device__ __forceinline__ void delta_run(const Args& a, const int blk, const in
       // The split fills the queue of the NEXT round (its own counter slot): every
       // phase decision reads qcount[round % 3], and no phase may write the slot its
       // own decision read while slower CTAs may still be reading it.
+      // the split marks epoch + 1; nothing tests this epoch's far marks any more
+      for (int i = blk * THREADS + threadIdx.x; i < a.nwords; i += nblk * THREADS) fbits(a, epoch)[i] = 0u;
       const int32_t* F = a.f[epoch & 1];
       int32_t* FN = a.f[(epoch + 1) & 1];
       int* fnext = &c->fcount[(epoch + 1) % 3];
@@ -611,15 +641,15 @@ __device__ __forceinline__ void delta_run(const Args& a, const int blk, const in
           const int du = __ldcg(a.dist + u);
           if ((long long)du >= thr_old) {  // below thr_old: already settled through the queue
             if ((long long)du < thr) {
-              toq = atomicExch(a.qstamp + u, round + 1) != round + 1;
+              toq = mark(qbits(a, round + 1), u);
             } else {
-              tof = atomicExch(a.fstamp + u, epoch + 1) != epoch + 1;
+              tof = mark(fbits(a, epoch + 1), u);
               if (tof) atomicMin(fminn, du);
             }
           }
         }
         queue_push(a, toq, u, Q, qcnt, HV, HB, hnext);
-        warp_push(tof, u, FN, fnext);
+        warp_push(a, tof, u, FN, fnext);
       }
       if (blk == 0 && threadIdx.x == 0) {
         c->fcount[(epoch + 2) % 3] = 0;
@@ -667,23 +697,18 @@ __global__ void __launch_bounds__(THREADS, 4) k_delta_multi(Args a, int gsz) {
       b.hv[k] += o;
       b.hbase[k] += o;
     }
-    b.qstamp += o;
-    b.fstamp += o;
+    b.bits += (size_t)g * 4 * a.nwords;
     b.ctl += g;
   }
   __syncthreads();
   delta_run(b, blockIdx.x % gsz, gsz, ring);
 }
 
-__global__ void k_init(int V, int src, int32_t* dist, int32_t* qstamp, int32_t* fstamp, int32_t* q0, int32_t* hv0,
-                       int32_t* hb0, const int32_t* __restrict__ off, Ctl* c, int hub_deg, int hub_chunk) {
-  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
-    dist[v] = v == src ? 0 : INT_MAX;
-    qstamp[v] = -1;
-    fstamp[v] = -1;
-  }
+// Initial state of a solve from src (the mark bitmaps are zeroed by the host).
+__global__ void k_init(int V, int src, int32_t* dist, int32_t* q0, int32_t* hv0, int32_t* hb0,
+                       const int32_t* __restrict__ off, Ctl* c, int hub_deg, int hub_chunk) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) dist[v] = v == src ? 0 : INT_MAX;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    qstamp[src] = 0;
     c->bar.arrived = 0;
     c->bar.error = 0;
     for (int k = 0; k < 3; ++k) {
@@ -710,23 +735,15 @@ __global__ void k_init(int V, int src, int32_t* dist, int32_t* qstamp, int32_t* 
 
 // Initial state of every source of a batch: blockIdx.y = position in the batch, each
 // with its V-strided slices and its own Ctl (as k_init for one source).
-__global__ void k_init_multi(int V, const int32_t* __restrict__ srcs, int32_t* dist, int32_t* qstamp, int32_t* fstamp,
-                             int32_t* q0, int32_t* hv0, int32_t* hb0, const int32_t* __restrict__ off, Ctl* ctl,
-                             int hub_deg, int hub_chunk) {
+__global__ void k_init_multi(int V, const int32_t* __restrict__ srcs, int32_t* dist, int32_t* q0, int32_t* hv0,
+                             int32_t* hb0, const int32_t* __restrict__ off, Ctl* ctl, int hub_deg, int hub_chunk) {
   const int g = blockIdx.y;
   const size_t o = (size_t)g * (size_t)V;
   const int src = srcs[g];
   dist += o;
-  qstamp += o;
-  fstamp += o;
-  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
-    dist[v] = v == src ? 0 : INT_MAX;
-    qstamp[v] = -1;
-    fstamp[v] = -1;
-  }
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) dist[v] = v == src ? 0 : INT_MAX;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     Ctl* c = ctl + g;
-    qstamp[src] = 0;
     c->bar.arrived = 0;
     c->bar.error = 0;
     for (int k = 0; k < 3; ++k) {
@@ -749,13 +766,10 @@ __global__ void k_init_multi(int V, const int32_t* __restrict__ srcs, int32_t* d
   }
 }
 
-// Warm start (sp_sssp_dynamic): dist keeps the caller's values; stamps and counters
-// are reset here, and k_seed then queues the seed vertices (hubs as hub entries).
-__global__ void k_reset(int V, int32_t* qstamp, int32_t* fstamp, Ctl* c) {
-  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
-    qstamp[v] = -1;
-    fstamp[v] = -1;
-  }
+// Warm start (sp_sssp_dynamic): dist keeps the caller's values; the counters are reset
+// here (the host zeroes the mark bitmaps), and k_seed then queues the seed vertices
+// (hubs as hub entries).
+__global__ void k_reset(Ctl* c) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     c->bar.arrived = 0;
     c->bar.error = 0;
@@ -771,11 +785,10 @@ __global__ void k_reset(int V, int32_t* qstamp, int32_t* fstamp, Ctl* c) {
 }
 
 // Queues n distinct seeds for round 0 (after k_reset, in stream order).
-__global__ void k_seed(int n, const int32_t* __restrict__ seeds, int32_t* qstamp, int32_t* q0, int32_t* hv0,
+__global__ void k_seed(int n, const int32_t* __restrict__ seeds, int32_t* q0, int32_t* hv0,
                        int32_t* hb0, const int32_t* __restrict__ off, Ctl* c, int hub_deg, int hub_chunk) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int v = seeds[i];
-    qstamp[v] = 0;
     const int d = off[v + 1] - off[v];
     if (d > hub_deg) {
       const unsigned long long old =
@@ -835,7 +848,8 @@ __global__ void k_minmax_w(const int32_t* __restrict__ w, int64_t E, int* mn, in
 }  // namespace ss
 
 struct SsspPlan {
-  dbuf<int32_t> dist, q0, q1, f0, f1, qstamp, fstamp, wbuf, h0, h1, hb0, hb1;
+  dbuf<int32_t> dist, q0, q1, f0, f1, wbuf, h0, h1, hb0, hb1;
+  dbuf<unsigned> bits;  // the four mark bitmaps
   dbuf<char> m0, m1;
   dbuf<ss::Ctl> ctl;
   dbuf<int> tmp;
@@ -972,8 +986,9 @@ static int sssp_delta(sp_graph* g, const int32_t* w, int32_t src, int32_t* dist_
   SP_TRY(p->q1.alloc(V));
   SP_TRY(p->f0.alloc(V));
   SP_TRY(p->f1.alloc(V));
-  SP_TRY(p->qstamp.alloc(V));
-  SP_TRY(p->fstamp.alloc(V));
+  const int nwords = (V + 31) / 32;
+  SP_TRY(p->bits.alloc((size_t)4 * nwords));
+  SP_CHECK_CUDA(cudaMemsetAsync(p->bits.p, 0, sizeof(unsigned) * 4 * (size_t)nwords, s));
   SP_TRY(p->h0.alloc(V));
   SP_TRY(p->h1.alloc(V));
   SP_TRY(p->hb0.alloc(V));
@@ -994,8 +1009,8 @@ static int sssp_delta(sp_graph* g, const int32_t* w, int32_t src, int32_t* dist_
   a.hv[1] = p->h1.p;
   a.hbase[0] = p->hb0.p;
   a.hbase[1] = p->hb1.p;
-  a.qstamp = p->qstamp.p;
-  a.fstamp = p->fstamp.p;
+  a.bits = p->bits.p;
+  a.nwords = nwords;
   a.ctl = p->ctl.p;
   a.V = V;
   a.delta = delta;
@@ -1007,14 +1022,14 @@ static int sssp_delta(sp_graph* g, const int32_t* w, int32_t src, int32_t* dist_
   a.local_edges = 32 * local;
   SP_TRY(epoch_setup(g, a, g->sssp_trace != 0));
   if (nseeds > 0) {
-    ss::k_reset<<<num_sms() * 4, 256, 0, s>>>(V, p->qstamp.p, p->fstamp.p, p->ctl.p);
+    ss::k_reset<<<1, 32, 0, s>>>(p->ctl.p);
     SP_CHECK_LAUNCH();
     ss::k_seed<<<std::max(1, std::min(num_sms() * 4, (nseeds + 255) / 256)), 256, 0, s>>>(
-        nseeds, d_seeds, p->qstamp.p, p->q0.p, p->h0.p, p->hb0.p, g->off.p, p->ctl.p, a.hub_deg, a.hub_chunk);
+        nseeds, d_seeds, p->q0.p, p->h0.p, p->hb0.p, g->off.p, p->ctl.p, a.hub_deg, a.hub_chunk);
     SP_CHECK_LAUNCH();
   } else {
-    ss::k_init<<<num_sms() * 4, 256, 0, s>>>(V, src, p->dist.p, p->qstamp.p, p->fstamp.p, p->q0.p, p->h0.p,
-                                              p->hb0.p, g->off.p, p->ctl.p, a.hub_deg, a.hub_chunk);
+    ss::k_init<<<num_sms() * 4, 256, 0, s>>>(V, src, p->dist.p, p->q0.p, p->h0.p, p->hb0.p, g->off.p, p->ctl.p,
+                                              a.hub_deg, a.hub_chunk);
     SP_CHECK_LAUNCH();
   }
   int per_sm = 0;
@@ -1029,6 +1044,10 @@ static int sssp_delta(sp_graph* g, const int32_t* w, int32_t src, int32_t* dist_
   g->sssp_last_relaxed = (int64_t)hc.relaxed;
   g->sssp_last_epochs = hc.epochs;
   p->etrace_n = a.etrace ? std::min(hc.epochs, ETRACE_CAP) : 0;
+  if (hc.status == 3) {
+    set_error("sp_sssp: a queue overflowed its V entries (internal error; distances not valid)");
+    return SP_ERR_CUDA;
+  }
   if (hc.status != 0 || hc.bar.error) {
     if (negative && !hc.bar.error) {
       set_error("sp_sssp: no fixed point after %d rounds (negative cycle)", hc.rounds);
@@ -1062,18 +1081,22 @@ static int sssp_delta_batches(sp_graph* g, const int32_t* w, const std::vector<i
   const int total = num_sms() * std::max(1, std::min(per_sm, ctas));
   int B = g->sssp_batch > 0 ? g->sssp_batch : ss::BATCH;
   B = std::max(1, std::min({B, n, total}));
-  {  // 11 V-sized int32 buffers per source in flight: keep a batch within 1/8 of device memory
+  {  // 9 V-sized int32 buffers and 4 bitmaps per source in flight: keep a batch within
+     // 1/8 of device memory
     size_t free_b = 0, total_b = 0;
     SP_CHECK_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    const size_t per_src = (size_t)11 * 4 * (size_t)V + 4096;
+    const size_t per_src = (size_t)9 * 4 * (size_t)V + (size_t)V / 2 + 4096;
     B = (int)std::max<size_t>(1, std::min<size_t>(B, (total_b / 8) / per_src));
   }
   const int gsz = total / B;
   const size_t BV = (size_t)B * V;
   Arena A;
-  dspan<int32_t> dist, q0, q1, f0, f1, qs, fs, h0, h1, hb0, hb1, dsrc;
+  const int nwords = (V + 31) / 32;
+  dspan<int32_t> dist, q0, q1, f0, f1, h0, h1, hb0, hb1, dsrc;
+  dspan<unsigned> bits;
   dspan<ss::Ctl> ctl;
-  for (dspan<int32_t>* d : {&dist, &q0, &q1, &f0, &f1, &qs, &fs, &h0, &h1, &hb0, &hb1}) A.want(*d, BV);
+  for (dspan<int32_t>* d : {&dist, &q0, &q1, &f0, &f1, &h0, &h1, &hb0, &hb1}) A.want(*d, BV);
+  A.want(bits, (size_t)4 * nwords * B);
   A.want(dsrc, B);
   A.want(ctl, B);
   SP_TRY(A.commit());
@@ -1090,8 +1113,8 @@ static int sssp_delta_batches(sp_graph* g, const int32_t* w, const std::vector<i
   a.hv[1] = h1.p;
   a.hbase[0] = hb0.p;
   a.hbase[1] = hb1.p;
-  a.qstamp = qs.p;
-  a.fstamp = fs.p;
+  a.bits = bits.p;
+  a.nwords = nwords;
   a.ctl = ctl.p;
   a.V = V;
   a.delta = delta;
@@ -1105,8 +1128,9 @@ static int sssp_delta_batches(sp_graph* g, const int32_t* w, const std::vector<i
   for (int k0 = 0; k0 < n; k0 += B) {
     const int b = std::min(B, n - k0);
     SP_CHECK_CUDA(cudaMemcpyAsync(dsrc.p, srcs.data() + k0, sizeof(int32_t) * b, cudaMemcpyHostToDevice, s));
+    SP_CHECK_CUDA(cudaMemsetAsync(bits.p, 0, sizeof(unsigned) * 4 * (size_t)nwords * b, s));
     ss::k_init_multi<<<dim3(std::max(1, num_sms() * 4 / b), b), 256, 0, s>>>(
-        V, dsrc.p, dist.p, qs.p, fs.p, q0.p, h0.p, hb0.p, g->off.p, ctl.p, a.hub_deg, a.hub_chunk);
+        V, dsrc.p, dist.p, q0.p, h0.p, hb0.p, g->off.p, ctl.p, a.hub_deg, a.hub_chunk);
     SP_CHECK_LAUNCH();
     int gs = gsz;
     void* params[] = {&a, &gs};
@@ -1115,6 +1139,10 @@ static int sssp_delta_batches(sp_graph* g, const int32_t* w, const std::vector<i
     SP_TRY(copy_out(hc.data(), ctl.p, sizeof(ss::Ctl) * b, s));
     for (int i = 0; i < b; ++i) {
       relaxed += (int64_t)hc[i].relaxed;
+      if (hc[i].status == 3) {
+        set_error("sp_sssp_batch: a queue overflowed its V entries for source %d (internal error)", srcs[k0 + i]);
+        return SP_ERR_CUDA;
+      }
       if (hc[i].status != 0 || hc[i].bar.error) {
         if (negative && !hc[i].bar.error) {
           set_error("sp_sssp: no fixed point from source %d after %d rounds (negative cycle)", srcs[k0 + i],

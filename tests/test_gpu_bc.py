@@ -138,3 +138,50 @@ def test_bc_at_scale():
     srcs = G.pick_sources(g, 96, seed=20)
     out = device_graph(g).bc(srcs)
     assert_bc_close(out, O.bc(g.indexofNodes, g.edgeList, srcs), "rmat17")
+
+
+@pytest.mark.parametrize("policy", [1, 2, 3])
+def test_bc_forward_direction_per_level_keeps_results(policy):
+    # pull levels (bottom-up over in-edges, hubs in shared pieces) and push levels mixed by
+    # the rule, by a seeded random choice, or pull everywhere: BFS levels and path counts
+    # stay bit-exact and BC within its tolerance, on undirected and directed graphs and
+    # on a star whose hub has more in-edges than a pull piece
+    from graphs import star
+
+    graphs = [G.rmat(13, 16, seed=3), G.rmat(12, 8, seed=5, directed=True), G.grid(30, 40),
+              star(5000, directed_in=False)]
+    for g in graphs:
+        srcs = G.pick_sources(g, 40, seed=policy)
+        with DeviceGraph.from_csr(g, with_weights=False) as dg:
+            dg.tune_set("bc.dir", policy)
+            for seed in (1, 2):
+                dg.tune_set("bc.dir_seed", seed)
+                out = dg.bc(srcs)
+                assert_bc_close(out, O.bc(g.indexofNodes, g.edgeList, srcs), g.name)
+                lvl, sig = dg.bfs_sigma(srcs[:8])
+                for k, s in enumerate(srcs[:8]):
+                    rl, rs, _ = O.bfs_sigma(g.indexofNodes, g.edgeList, int(s))
+                    assert np.array_equal(lvl[k], rl) and np.array_equal(sig[k], rs), (g.name, policy, k)
+
+
+def test_bc_level_trace_records_the_directions():
+    import ctypes
+
+    from starplat_b200._lib import check, lib
+
+    g = G.rmat(14, 16, seed=2)
+    srcs = G.pick_sources(g, 64, seed=4)
+    with DeviceGraph.from_csr(g, with_weights=False) as dg:
+        dg.tune_set("bc.dir", 2)
+        dg.tune_set("bc.trace", 1)
+        dg.bc(srcs)
+        rec = np.zeros((4096, 4), np.float32)
+        t = np.zeros(4097, np.uint64)
+        n = ctypes.c_int32()
+        check("sp_bc_level_trace", lib().sp_bc_level_trace(dg.handle, rec.ctypes.data, t.ctypes.data, 4096,
+                                                           ctypes.byref(n)))
+    k = int(n.value)
+    assert k > 3
+    assert set(rec[:k, 3].tolist()) <= {0.0, 1.0} and rec[:k, 3].sum() > 0
+    assert (np.diff(t[:k + 1].astype(np.int64)) >= 0).all()
+    assert (rec[:k, 0] > 0).all()
