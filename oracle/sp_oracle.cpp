@@ -14,11 +14,17 @@
 //     the CPU baseline (float arithmetic where the DSL declares float).
 //
 // Parity status: the reference ships no golden outputs for these paths and its
-// compiler cannot be built here (flex/bison are absent), so only triangle
-// counting is pinned against the reference's own code (graph::check_if_nbr,
-// run through oracle/ref_harness.cpp) and its sample graphs; PageRank, SSSP,
-// BC and Louvain are pinned by hand-computed known answers and by networkx
-// cross-checks on small graphs (tests/test_oracle.py).
+// compiler cannot be built here (flex/bison are absent). Pinned against the
+// reference's own code: triangle counting and the per-vertex clustering counts
+// (graph::check_if_nbr through oracle/ref_harness.cpp, and its sample graphs), and
+// Brandes BC (the reference's manual CUDA BC, bcManualv5.cu, run on a GPU by
+// oracle/ref_bc_manual.cu; twice its halved values equal or_bc to 1e-12 relative on
+// the committed fixtures, tests/test_reference_gpu_fixtures.py). Louvain is compared
+// by modularity with the reference's CUDA Louvain (fixtures of
+// tests/golden/make_gpu_fixtures.py). PageRank and SSSP have unique answers (the FP64
+// fixed point at a given iteration count, exact shortest distances): they are pinned by
+// hand-computed known answers and by networkx / numpy on small graphs
+// (tests/test_oracle.py).
 #include <algorithm>
 #include <climits>
 #include <cmath>

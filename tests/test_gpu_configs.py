@@ -10,8 +10,8 @@
   1e-5 relative of FP64 Brandes (bc_dslV2:1-21); and the 1000 Erdos-Renyi graphs run
   as one batch, every 20th graph checked;
 * Louvain, the 1,048,576-vertex planted partition: the returned partition has the
-  returned modularity (the comparison with the reference's own Louvain is in
-  test_gpu_reference_fixtures.py).
+  returned modularity, at least that of the reference's own CUDA Louvain on this graph
+  (a committed fixture) minus 1e-3.
 
 Each graph is built by the same seeded generator call as bench.py."""
 import numpy as np
@@ -111,11 +111,17 @@ def test_bc_er1000_batched():
         assert ok, (k, worst)
 
 
-def test_louvain_sbm1m_partition_has_its_modularity():
+def test_louvain_sbm1m_against_the_reference_louvain():
+    # the reference's CUDA Louvain reaches the committed fixture's modularity on this
+    # graph; this library's partition must reach at least that minus 1e-3, and have the
+    # modularity it returns
+    import json
+    import os
+
     g = G.sbm(1 << 20, 256, exponent=2.0, avg_degree=32, p_in=0.8, seed=1)
     with DeviceGraph.from_csr(g, with_weights=False) as dg:
         q, comm, _ = dg.louvain(None, 1e-4)
     assert abs(O.modularity(g.indexofNodes, g.edgeList, comm) - q) < 1e-9
-    bs = g.meta["block_start"]
-    planted = (np.searchsorted(bs, np.arange(g.V), side="right") - 1).astype(np.int32)
-    assert q > O.modularity(g.indexofNodes, g.edgeList, planted) - 1e-2
+    fx = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_gpu", "louvain.json")
+    ref = json.load(open(fx))["sbm1m"]["reference_q"]
+    assert q >= ref - 1e-3, (q, ref)
