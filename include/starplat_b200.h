@@ -147,8 +147,11 @@ int sp_graph_info(sp_graph_h g, int32_t* V, int64_t* E, int32_t* symmetric);
  *             in-edges of the vertices some source has not reached + V / 8 (pull: every
  *             such vertex scans its in-edges for parents in the level, no atomics except
  *             on vertices above 1024 in-edges); 2 a seeded random direction per level
- *             ("bc.dir_seed", exploration); 3 pull at every level. Default 0. The decision
- *             is taken on the device from counters every CTA reads after the same barrier.
+ *             ("bc.dir_seed", exploration); 3 pull at every level; 4 the level model
+ *             (sp_sched_level_load) scores push and pull from the level's statistics
+ *             (rule 1 without a model). Default: 4 when a level model is loaded, else 0.
+ *             The decision is taken on the device from counters every CTA reads after the
+ *             same barrier, so every CTA takes the same direction.
  *   "bc.pull_alpha"  factor of the bc.dir = 1 rule, in thousandths (default 1000).
  *   "bc.trace"  1: record per level (entries, their out-edges, unreached in-edges, pull)
  *             and the device timer; read with sp_bc_level_trace.
@@ -346,15 +349,21 @@ int sp_sched_load(const float* params, const float* feat_mean, const float* feat
  * 0 fixed; 1 learned; 2 a seeded pseudo-random factor per epoch ("sssp.epoch_seed",
  * exploration). Distances are exact under any width sequence. */
 int sp_sched_epoch_load(const float* params, const float* feat_mean, const float* feat_scale);
+/* No counterpart in the reference. Load or unload the process-wide BC level model: the
+ * same network shape, predicting the log time of a forward level in each direction from
+ * the inputs recorded by sp_bc_level_trace; with it, bc.dir defaults to 4. */
+int sp_sched_level_load(const float* params, const float* feat_mean, const float* feat_scale);
 /* With knob "sssp.trace" = 1 and a per-epoch policy, the last single-source solve's
  * epochs: records[k][16] = the SP_MLP_IN inputs of the chosen factor, the factor, the
  * distance the threshold advanced, padding; times[k] = device timer (ns) at advance k,
  * times[n] at the end. *n = epochs recorded; up to cap records are copied. */
 int sp_sssp_epoch_trace(sp_graph_h g, float* records, unsigned long long* times, int32_t cap, int32_t* n);
 /* With knob "bc.trace" = 1 and bc.dir != 0, the last sp_bc grid run's levels (over all
- * batches): records[k][4] = level entries, their out-edges, in-edges of vertices not
- * yet reached by every source, 1 if pulled; times[k] = device timer (ns) at each level
- * start, times[n] at the end of the run. No counterpart in the reference. */
+ * batches): records[k][16] = the level model's SP_MLP_IN inputs for the direction taken
+ * (graph size, batch size, the level's entries and their out-edges, the in-edges of the
+ * vertices not yet reached by every source, the level, the direction), then 1 if pulled;
+ * times[k] = device timer (ns) at each level start, times[n] at the end of the run.
+ * No counterpart in the reference. */
 int sp_bc_level_trace(sp_graph_h g, float* records, unsigned long long* times, int32_t cap, int32_t* n);
 /* Replaces the generated Batch block of DynSSSP (DSL dynamicDSLCodes/dynamicBatchSSSP:
  * OnDelete + updateCSRDel + Decremental, then OnAdd + updateCSRAdd + Incremental): one

@@ -100,6 +100,7 @@ SIGNATURES = {
     "sp_mlp_train": (ctypes.c_int, [vp, vp, vp, i32, i32, f32, vp]),
     "sp_sched_load": (ctypes.c_int, [vp, vp, vp]),
     "sp_sched_epoch_load": (ctypes.c_int, [vp, vp, vp]),
+    "sp_sched_level_load": (ctypes.c_int, [vp, vp, vp]),
     "sp_sssp_epoch_trace": (ctypes.c_int, [vp, vp, vp, i32, P(i32)]),
     "sp_bc_level_trace": (ctypes.c_int, [vp, vp, vp, i32, P(i32)]),
     "sp_sssp_features": (ctypes.c_int, [vp, vp, f64, i32, i32, vp]),

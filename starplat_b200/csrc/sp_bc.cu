@@ -36,6 +36,7 @@
 #include <vector>
 
 #include "sp_internal.cuh"
+#include "sp_mlp_dev.cuh"
 #include "sp_sync.cuh"
 
 namespace sp {
@@ -108,12 +109,34 @@ struct Work {
   long long e_in;                   // in-edges of the graph
   unsigned long long* ldeg;         // [maxd + 2] out-edges of each level's entries
   unsigned long long* full_in;      // in-edges of vertices every batch source has reached
-  float* trace;                     // [trace_cap][4] per level: entries, their out-edges, unreached in-edges, pull
+  const float* dmodel;              // dir_policy 4: the level model (params, feature mean, scale)
+  float* trace;                     // [trace_cap][LTRACE] per level: the chosen direction's inputs, pull
   unsigned long long* ttime;        // [trace_cap + 1] device timer at each level start, then the end
   int trace_cap;
   int* tcount;                      // levels traced
 };
 constexpr int PULL_SPLIT = 1024;    // in-edges per piece of a pull hub
+constexpr int LTRACE = 16;          // floats per level trace record
+
+// The inputs of the level model for direction `pull` (0 push, 1 pull) at level d with
+// nent entries (values every CTA reads after the same barrier).
+__device__ __forceinline__ void level_inputs(const Work& W, int d, int nent, int nsrc, int pull, float* x) {
+  const float mf = (float)*(volatile unsigned long long*)(W.ldeg + d);
+  const float mu = (float)((double)W.e_in - (double)*(volatile unsigned long long*)W.full_in);
+  x[0] = log2f((float)W.V);
+  x[1] = log2f(1.0f + (float)W.e_in);
+  x[2] = (float)W.e_in / (float)W.V;
+  x[3] = log2f(1.0f + (float)nsrc);
+  x[4] = log2f(1.0f + (float)nent);       // entries of the level
+  x[5] = log2f(1.0f + mf);                // their out-edges (push cost)
+  x[6] = log2f(1.0f + fmaxf(mu, 0.0f));   // in-edges of vertices not reached by every source (pull cost)
+  x[7] = x[5] - x[6];
+  x[8] = log2f(1.0f + (float)d);
+  x[9] = x[4] - x[0];
+  x[10] = (float)pull;
+  x[11] = x[10] * x[7];
+  x[12] = x[10] * x[4];
+}
 
 struct GridSync {
   GridBar* bar;
@@ -523,6 +546,7 @@ __device__ void backward_entry(const Work& W, int i, int lane, int eb, int ee, b
 __device__ __forceinline__ bool pull_this_level(const Work& W, int d, int nent, int V) {
   if (W.dir_policy == 0 || W.radj == nullptr) return false;
   if (W.dir_policy == 3) return true;
+  // (policy 4, the level model, is decided in run_batch; without a model: the rule)
   if (W.dir_policy == 2) {
     unsigned h = W.dir_seed * 0x9e3779b9u ^ ((unsigned)d * 0x85ebca6bu);
     h ^= h >> 15;
@@ -573,15 +597,22 @@ __device__ bool run_batch(const Work& W, const int32_t* srcs, int nsrc, S& sync,
       if (gt == 0) atomicExch(W.err, 2);
       return false;
     }
-    const bool pull = dirs && pull_this_level(W, d, e - b, W.V);
+    bool pull;
+    if (dirs && W.dir_policy == 4 && W.dmodel) {
+      // the level model scores push and pull on this level's statistics; every CTA
+      // evaluates the same inputs the same way, so all take the same direction
+      __shared__ float s_rows[2][SP_MLP_IN];
+      if (threadIdx.x < 2) level_inputs(W, d, e - b, nsrc, threadIdx.x, s_rows[threadIdx.x]);
+      pull = mlp_argmin<2>(W.dmodel, s_rows) == 1;
+    } else {
+      pull = dirs && pull_this_level(W, d, e - b, W.V);
+    }
     if (dirs && W.trace && gt == 0) {
       const int t = atomicAdd(W.tcount, 1);
       if (t < W.trace_cap) {
-        float* r = W.trace + (size_t)t * 4;
-        r[0] = (float)(e - b);
-        r[1] = (float)*(volatile unsigned long long*)(W.ldeg + d);
-        r[2] = (float)((double)W.e_in - (double)*(volatile unsigned long long*)W.full_in);
-        r[3] = pull ? 1.0f : 0.0f;
+        float* r = W.trace + (size_t)t * LTRACE;
+        level_inputs(W, d, e - b, nsrc, pull ? 1 : 0, r);
+        r[SP_MLP_IN] = pull ? 1.0f : 0.0f;
         unsigned long long now;
         asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
         W.ttime[t] = now;
@@ -915,7 +946,11 @@ __global__ void k_plain_bwd(int V, const int32_t* __restrict__ off, const int32_
 
 }  // namespace bc
 
+unsigned mlp_level_model(std::vector<float>& packed);  // sp_mlp.cu
+
 struct BcPlan {
+  dbuf<float> dmodel;  // the level model on the device
+  unsigned dmodel_gen = 0;
   // pull levels: the vertices of more than PULL_SPLIT in-edges and their piece prefix
   // (built once per graph), the per-level out-edge counts and the reached in-edges
   bool phub_built = false;
@@ -1005,7 +1040,19 @@ static int bc_grid(sp_graph* g, const int32_t* d_srcs, int nsrc, int batch_hint,
   W.hub_chunk = g->bc_hub_chunk > 0 ? g->bc_hub_chunk : bc::HUB_CHUNK;
   W.dacc = p->dacc.p;
   // forward direction per level
-  W.dir_policy = g->bc_dir >= 0 ? g->bc_dir : bc::DIR_DEFAULT;
+  std::vector<float> packed;
+  const unsigned lgen = mlp_level_model(packed);
+  W.dir_policy = g->bc_dir >= 0 ? g->bc_dir : (lgen ? 4 : bc::DIR_DEFAULT);
+  W.dmodel = nullptr;
+  if (W.dir_policy == 4 && lgen) {
+    if (p->dmodel_gen != lgen) {
+      SP_TRY(p->dmodel.alloc(packed.size()));
+      SP_CHECK_CUDA(cudaMemcpyAsync(p->dmodel.p, packed.data(), sizeof(float) * packed.size(),
+                                    cudaMemcpyHostToDevice, s));
+      p->dmodel_gen = lgen;
+    }
+    W.dmodel = p->dmodel.p;
+  }
   W.dir_alpha = g->bc_pull_alpha > 0 ? (float)g->bc_pull_alpha / 1000.0f : bc::PULL_ALPHA;
   W.dir_seed = (unsigned)g->bc_dir_seed;
   W.roff = nullptr;
@@ -1051,7 +1098,7 @@ static int bc_grid(sp_graph* g, const int32_t* d_srcs, int nsrc, int batch_hint,
     W.full_in = p->ldeg.p + maxd + 2;
     if (g->bc_trace) {
       constexpr int CAP = 1 << 14;
-      SP_TRY(p->trace.alloc((size_t)CAP * 4));
+      SP_TRY(p->trace.alloc((size_t)CAP * bc::LTRACE));
       SP_TRY(p->ttime.alloc((size_t)CAP + 1));
       SP_TRY(p->tcount.alloc(1));
       SP_CHECK_CUDA(cudaMemsetAsync(p->tcount.p, 0, sizeof(int), s));
@@ -1398,6 +1445,6 @@ extern "C" int sp_bc_level_trace(sp_graph_h g, float* records, unsigned long lon
   *n = have;
   const int k = std::min(have, (int)cap);
   if (k == 0) return SP_OK;
-  SP_TRY(copy_out(records, g->bc->trace.p, sizeof(float) * 4 * k, g->stream));
+  SP_TRY(copy_out(records, g->bc->trace.p, sizeof(float) * bc::LTRACE * k, g->stream));
   return copy_out(times, g->bc->ttime.p, sizeof(unsigned long long) * (k + 1), g->stream);
 }

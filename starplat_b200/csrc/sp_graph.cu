@@ -607,8 +607,8 @@ int sp_tune_set(sp_graph_h g, const char* key, int64_t value) {
     return SP_OK;
   }
   if (!strcmp(key, "bc.dir")) {
-    if (value < -1 || value > 3) {
-      set_error("sp_tune_set: bc.dir must be -1, 0, 1, 2 or 3");
+    if (value < -1 || value > 4) {
+      set_error("sp_tune_set: bc.dir must be -1, 0, 1, 2, 3 or 4");
       return SP_ERR_INVALID;
     }
     g->bc_dir = (int32_t)value;

@@ -189,8 +189,18 @@ std::vector<float> g_mean, g_scale;
 // the per-epoch bucket-width model of SSSP (same network shape, its own inputs)
 std::vector<float> g_eparams;  // params, mean, scale packed; empty = no model
 unsigned g_egeneration = 0;
+// the per-level direction model of BC's forward sweep
+std::vector<float> g_bparams;
+unsigned g_bgeneration = 0;
 
 }  // namespace mlp
+
+// The BC level model packed for the device and its generation (0 = none loaded).
+unsigned mlp_level_model(std::vector<float>& packed) {
+  std::lock_guard<std::mutex> lock(mlp::g_mu);
+  packed = mlp::g_bparams;
+  return mlp::g_bparams.empty() ? 0u : mlp::g_bgeneration;
+}
 
 // The epoch model packed for the device (params, feature mean, feature scale) and its
 // generation (0 = none loaded).
@@ -327,5 +337,22 @@ extern "C" int sp_sched_epoch_load(const float* params, const float* feat_mean, 
   mlp::g_eparams.assign(params, params + mlp::P);
   mlp::g_eparams.insert(mlp::g_eparams.end(), feat_mean, feat_mean + mlp::IN);
   mlp::g_eparams.insert(mlp::g_eparams.end(), feat_scale, feat_scale + mlp::IN);
+  return SP_OK;
+}
+
+extern "C" int sp_sched_level_load(const float* params, const float* feat_mean, const float* feat_scale) {
+  std::lock_guard<std::mutex> lock(mlp::g_mu);
+  ++mlp::g_bgeneration;
+  if (!params) {
+    mlp::g_bparams.clear();
+    return SP_OK;
+  }
+  if (!feat_mean || !feat_scale) {
+    set_error("sp_sched_level_load: feature normalisation required");
+    return SP_ERR_INVALID;
+  }
+  mlp::g_bparams.assign(params, params + mlp::P);
+  mlp::g_bparams.insert(mlp::g_bparams.end(), feat_mean, feat_mean + mlp::IN);
+  mlp::g_bparams.insert(mlp::g_bparams.end(), feat_scale, feat_scale + mlp::IN);
   return SP_OK;
 }

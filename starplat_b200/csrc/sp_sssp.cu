@@ -40,6 +40,7 @@
 #include <vector>
 
 #include "sp_internal.cuh"
+#include "sp_mlp_dev.cuh"
 #include "sp_sync.cuh"
 
 namespace sp {
@@ -462,49 +463,10 @@ __device__ __forceinline__ void epoch_inputs(const Args& a, int f, float fn, flo
 // pick the same factor without a barrier between them. Ties go to the smaller factor.
 __device__ int epoch_choice(const Args& a, float fn, float rounds_prev, float relaxed_prev, int epoch, int f_prev,
                             float progress) {
-  constexpr int IN = SP_MLP_IN, H = SP_MLP_HIDDEN;
-  __shared__ float s_x[NFAC][IN];
-  __shared__ float s_h1[NFAC][H];
-  __shared__ float s_y[NFAC];
-  __shared__ int s_pick;
-  const float* P = a.emodel;
-  const float* mean = P + SP_MLP_PARAMS;
-  const float* scale = mean + IN;
-  const int t = threadIdx.x;
-  if (t < NFAC) {
-    float x[IN];
-    epoch_inputs(a, t, fn, rounds_prev, relaxed_prev, epoch, f_prev, progress, x);
-#pragma unroll
-    for (int i = 0; i < IN; ++i) s_x[t][i] = (x[i] - mean[i]) * scale[i];
-  }
-  __syncthreads();
-  const int c = t >> 5, j = t & 31;
-  constexpr int W1 = 0, B1 = W1 + H * IN, W2 = B1 + H, B2 = W2 + H * H, W3 = B2 + H, B3 = W3 + H;
-  if (c < NFAC) {
-    float z = P[B1 + j];
-#pragma unroll
-    for (int i = 0; i < IN; ++i) z = fmaf(P[W1 + j * IN + i], s_x[c][i], z);
-    s_h1[c][j] = tanhf(z);
-  }
-  __syncthreads();
-  if (c < NFAC) {
-    float z = P[B2 + j];
-#pragma unroll 8
-    for (int k = 0; k < H; ++k) z = fmaf(P[W2 + j * H + k], s_h1[c][k], z);
-    float v = P[W3 + j] * tanhf(z);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (j == 0) s_y[c] = P[B3] + v;
-  }
-  __syncthreads();
-  if (t == 0) {
-    int best = 0;
-    for (int k = 1; k < NFAC; ++k)
-      if (s_y[k] < s_y[best]) best = k;
-    s_pick = best;
-  }
-  __syncthreads();
-  return s_pick;
+  __shared__ float s_x[NFAC][SP_MLP_IN];
+  if (threadIdx.x < NFAC)
+    epoch_inputs(a, threadIdx.x, fn, rounds_prev, relaxed_prev, epoch, f_prev, progress, s_x[threadIdx.x]);
+  return mlp_argmin<NFAC>(a.emodel, s_x);
 }
 
 // One delta-stepping solve by `nblk` co-resident CTAs (this one is number `blk`):

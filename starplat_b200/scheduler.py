@@ -23,6 +23,14 @@ traces of solves that pick a seeded random factor per epoch (sssp.epoch = 2): pe
 the chosen factor's inputs and the measured device time per unit of distance advanced.
 
     python -m starplat_b200.scheduler train-epoch   # collect traces, train, write sched_epoch_model.json
+
+A third network of the same shape decides BC's forward direction per level inside the
+kernel (push along the level's out-edges, or pull over the in-edges of the vertices not
+yet reached by every source): it predicts the level's log time in each direction from
+the level's statistics, and every CTA takes the direction with the lower prediction.
+Its training data are traces of runs with a seeded random direction per level (bc.dir = 2).
+
+    python -m starplat_b200.scheduler train-level   # collect BC traces, train, write sched_level_model.json
 """
 from __future__ import annotations
 
@@ -42,6 +50,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 MODEL_PATH = os.path.join(_HERE, "sched_model.json")
 EPOCH_MODEL_PATH = os.path.join(_HERE, "sched_epoch_model.json")
 EPOCH_FACTORS = (0.25, 0.5, 1.0, 2.0, 4.0, 8.0)  # the kernel's width candidates (kFacNum / 4)
+LEVEL_MODEL_PATH = os.path.join(_HERE, "sched_level_model.json")
 MULTS = (1, 2, 4, 8, 16, 32, 64)
 CTAS = (1, 2, 4)
 LOCALS = (0, 64)  # warp cascade budget per round (sssp.local), off or the default
@@ -118,12 +127,15 @@ def _settle_auto_load() -> None:
     device._SCHED_TRIED = True
 
 
-def load(path: str = MODEL_PATH, epoch_path: str = EPOCH_MODEL_PATH) -> bool:
-    """Load the model (and the per-epoch width model, when its file exists) into the
-    library; False (fixed heuristic stays) if the model file is absent."""
+def load(path: str = MODEL_PATH, epoch_path: str = EPOCH_MODEL_PATH, level_path: str = LEVEL_MODEL_PATH) -> bool:
+    """Load the model (and the per-epoch width and per-level direction models, when their
+    files exist) into the library; False (fixed heuristic stays) if the model file is
+    absent."""
     _settle_auto_load()
     if epoch_path and os.path.exists(epoch_path):
         load_epoch(epoch_path)
+    if level_path and os.path.exists(level_path):
+        load_level(level_path)
     if not os.path.exists(path):
         return False
     d = json.load(open(path))
@@ -142,10 +154,10 @@ def unload() -> None:
     _settle_auto_load()
     check("sp_sched_load", lib().sp_sched_load(None, None, None))
     check("sp_sched_epoch_load", lib().sp_sched_epoch_load(None, None, None))
+    check("sp_sched_level_load", lib().sp_sched_level_load(None, None, None))
 
 
-def load_epoch(path: str = EPOCH_MODEL_PATH) -> bool:
-    """Load the per-epoch width model only; False if the file is absent."""
+def _load_packed(path, call) -> bool:
     if not os.path.exists(path):
         return False
     d = json.load(open(path))
@@ -154,8 +166,126 @@ def load_epoch(path: str = EPOCH_MODEL_PATH) -> bool:
     scale = np.asarray(d["feat_scale"], np.float32)
     if p.shape[0] != P or mean.shape[0] != IN:
         raise ValueError(f"{path}: model shape does not match this library")
-    check("sp_sched_epoch_load", lib().sp_sched_epoch_load(p.ctypes.data, mean.ctypes.data, scale.ctypes.data))
+    check(call, getattr(lib(), call)(p.ctypes.data, mean.ctypes.data, scale.ctypes.data))
     return True
+
+
+def load_epoch(path: str = EPOCH_MODEL_PATH) -> bool:
+    """Load the per-epoch width model only; False if the file is absent."""
+    return _load_packed(path, "sp_sched_epoch_load")
+
+
+def load_level(path: str = LEVEL_MODEL_PATH) -> bool:
+    """Load the BC per-level direction model only; False if the file is absent."""
+    return _load_packed(path, "sp_sched_level_load")
+
+
+def unload_level() -> None:
+    check("sp_sched_level_load", lib().sp_sched_level_load(None, None, None))
+
+
+def level_trace(dg):
+    """The last traced BC run's levels: (inputs[n][IN], pull[n], ns[n])."""
+    cap = 1 << 14
+    rec = np.empty((cap, 16), np.float32)
+    t = np.empty(cap + 1, np.uint64)
+    n = ctypes.c_int32()
+    check("sp_bc_level_trace", lib().sp_bc_level_trace(dg.handle, rec.ctypes.data, t.ctypes.data, cap,
+                                                       ctypes.byref(n)))
+    k = min(int(n.value), cap)
+    if int(n.value) > cap:
+        k -= 1
+    ns = (t[1:k + 1].astype(np.int64) - t[:k].astype(np.int64)).astype(np.float64)
+    return rec[:k, :IN].copy(), rec[:k, IN].copy(), ns
+
+
+def bc_training_graphs():
+    """(name, graph, sources) for the level model: sizes below the benchmark's R-MAT 20."""
+    from . import generators as G
+
+    out = []
+    for sc in (14, 16, 18, 19):
+        g = G.rmat(sc, 16, seed=sc + 50)
+        out.append((f"rmat{sc}u", g, G.pick_sources(g, 64, seed=sc)))
+    g = G.rmat(17, 8, seed=9, directed=True)
+    out.append(("rmat17d", g, G.pick_sources(g, 64, seed=9)))
+    for n, d in ((1 << 16, 8), (1 << 18, 16)):
+        g = G.erdos_renyi(n, d, seed=n % 97)
+        out.append((f"er{n}_d{d}", g, G.pick_sources(g, 64, seed=3)))
+    g = G.grid(512, 512)
+    out.append(("grid512", g, G.pick_sources(g, 32, seed=5)))
+    g = G.sbm(1 << 17, 64, seed=3)
+    out.append(("sbm17", g, G.pick_sources(g, 64, seed=2)))
+    return out
+
+
+def collect_levels(graphs, seeds=(1, 2, 3, 4, 5, 6), log=print):
+    """Exploration runs (a seeded random direction per level) with traces: one sample
+    per level, target log2 of its device nanoseconds."""
+    from .device import DeviceGraph
+
+    import torch
+
+    X, T = [], []
+    for name, g, srcs in graphs:
+        with DeviceGraph.from_csr(g, with_weights=False) as dg:
+            dg.set_stream(torch.cuda.current_stream())
+            dg.tune_set("bc.dir", 0)
+            dg.bc(srcs)  # warm-up
+            dg.tune_set("bc.dir", 2)
+            dg.tune_set("bc.trace", 1)
+            n0 = sum(x.shape[0] for x in X)
+            for sd in seeds:
+                dg.tune_set("bc.dir_seed", sd)
+                dg.bc(srcs)
+                torch.cuda.synchronize()
+                x, pull, ns = level_trace(dg)
+                ok = ns > 0
+                X.append(x[ok])
+                T.append(np.log2(ns[ok]).astype(np.float32))
+            dg.tune_set("bc.trace", 0)
+            dg.tune_set("bc.dir", -1)
+        log(f"  {name}: {sum(x.shape[0] for x in X) - n0} levels")
+    return np.concatenate(X), np.concatenate(T)
+
+
+def time_bc(dg, srcs, policy: int, reps: int = 3) -> float:
+    """Best-of-reps device time of sp_bc under a direction policy."""
+    import torch
+
+    dg.tune_set("bc.dir", policy)
+    dg.bc(srcs)
+    best = None
+    for _ in range(reps):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(torch.cuda.current_stream())
+        dg.bc(srcs)
+        b.record(torch.cuda.current_stream())
+        torch.cuda.synchronize()
+        t = a.elapsed_time(b)
+        best = t if best is None else min(best, t)
+    dg.tune_set("bc.dir", -1)
+    return best
+
+
+def train_level(out: str = LEVEL_MODEL_PATH, log=print) -> dict:
+    """Collect BC exploration traces, fit the level model with the fused training kernel,
+    and write it."""
+    import torch
+
+    t0 = time.time()
+    graphs = bc_training_graphs()
+    log(f"collecting BC level traces on {len(graphs)} graphs")
+    X, T = collect_levels(graphs, log=log)
+    params, mean, scale, loss = fit(X, T, steps=6000)
+    d = {"params": params.tolist(), "feat_mean": mean.tolist(), "feat_scale": scale.tolist(),
+         "train_loss": loss, "samples": int(X.shape[0]), "target": "log2(device ns) of one forward level",
+         "gpu": torch.cuda.get_device_name(0), "collect_and_train_s": round(time.time() - t0, 1)}
+    with open(out, "w") as f:
+        json.dump(d, f, indent=1)
+    log(f"trained on {X.shape[0]} levels: loss {loss:.4f}; wrote {out}")
+    return d
 
 
 def unload_epoch() -> None:
@@ -363,6 +493,10 @@ def main(argv=None):
     import torch
 
     argv = sys.argv[1:] if argv is None else argv
+    if argv and argv[0] == "train-level":
+        torch.cuda.set_device(0)
+        train_level(argv[1] if len(argv) > 1 else LEVEL_MODEL_PATH)
+        return 0
     if argv and argv[0] == "train-epoch":
         torch.cuda.set_device(0)
         train_epoch(argv[1] if len(argv) > 1 else EPOCH_MODEL_PATH)

@@ -185,3 +185,39 @@ def test_bc_level_trace_records_the_directions():
     assert set(rec[:k, 3].tolist()) <= {0.0, 1.0} and rec[:k, 3].sum() > 0
     assert (np.diff(t[:k + 1].astype(np.int64)) >= 0).all()
     assert (rec[:k, 0] > 0).all()
+
+
+def test_bc_level_model_direction_keeps_results_and_matches_the_network():
+    # a loaded level model (random weights: the device evaluation is what is checked)
+    # decides each level's direction; results stay exact, and every traced level's
+    # direction is the argmin of the network's two scores computed by the forward kernel
+    import ctypes
+
+    from starplat_b200 import scheduler as S
+    from starplat_b200._lib import check, lib
+
+    p = S.init_params(21)
+    mean = np.zeros(_lib.SP_MLP_IN, np.float32)
+    scale = np.full(_lib.SP_MLP_IN, 0.4, np.float32)
+    check("sp_sched_level_load", lib().sp_sched_level_load(p.ctypes.data, mean.ctypes.data, scale.ctypes.data))
+    try:
+        g = G.rmat(14, 16, seed=6)
+        srcs = G.pick_sources(g, 64, seed=2)
+        with DeviceGraph.from_csr(g, with_weights=False) as dg:
+            assert dg.tune_get("bc.dir") == -1  # default: the model when one is loaded
+            dg.tune_set("bc.trace", 1)
+            out = dg.bc(srcs)
+            x, pull, ns = S.level_trace(dg)
+        assert_bc_close(out, O.bc(g.indexofNodes, g.edgeList, srcs), g.name)
+        assert x.shape[0] > 3
+        rows = np.repeat(x, 2, axis=0)
+        rows[0::2, 10], rows[1::2, 10] = 0.0, 1.0
+        rows[:, 11] = rows[:, 10] * rows[:, 7]
+        rows[:, 12] = rows[:, 10] * rows[:, 4]
+        y = S.mlp_forward(p, (rows - mean) * scale).reshape(-1, 2)
+        best = np.argmin(y, axis=1)
+        taken = pull.astype(np.int64)
+        gap = y[np.arange(len(y)), taken] - y[np.arange(len(y)), best]
+        assert np.all(gap <= 1e-4 * np.maximum(1.0, np.abs(y).max(axis=1))), gap.max()
+    finally:
+        S.unload_level()
