@@ -112,7 +112,7 @@ int sp_graph_info(sp_graph_h g, int32_t* V, int64_t* E, int32_t* symmetric);
  *             of the iteration kernel), out-degree descending within a class.
  *   "pr.l1_hot"  PageRank: only gathers from the first l1_hot sources (relabelled by
  *             out-degree, so the most-gathered ones) allocate in L1; the others bypass
- *             it (0..2^22, default 0 = every gather allocates).
+ *             it (0..2^22, default 32768; 0 = every gather allocates).
  *   "pr.vec"  PageRank: 1 = the 32-lane bin and the long-row chunks read srcList in
  *             16-byte loads (four entries per lane), 0 = one entry per lane per load.
  *   "sssp.delta"  SSSP bucket width used when sp_sssp gets delta <= 0 (0 = the largest
@@ -120,7 +120,7 @@ int sp_graph_info(sp_graph_h g, int32_t* V, int64_t* E, int32_t* symmetric);
  *   "sssp.ctas_per_sm"  SSSP: persistent CTAs per SM of the delta-stepping kernel (1..8,
  *             default 4; fewer CTAs make each grid barrier cheaper on high-diameter graphs).
  *   "sssp.batch"  sp_sssp_batch / sp_closeness: sources per cooperative launch, each on
- *             its own group of CTAs (1..1024, default 16; capped by the co-resident CTAs
+ *             its own group of CTAs (1..1024, default 4; capped by the co-resident CTAs
  *             and by 1/8 of device memory at 44 bytes per vertex per source).
  *   "sssp.last_batch" (read only): sources per launch of the last batched run.
  *   "sssp.last_delta", "sssp.last_ctas", "sssp.last_local" (read only): the schedule the

@@ -46,8 +46,13 @@ constexpr int HOT_DEFAULT = 0;          // one phase: measured fastest on R-MAT 
 constexpr int HOT_MAX = 1 << 22;
 constexpr int SRC_HINT_DEFAULT = 2;     // srcList loads: 0 __ldg, 1 L1::no_allocate, 2 L1::evict_first
 constexpr int ORDER_DEFAULT = 0;        // vertex order: 0 out-degree, 1 in-degree class then out-degree
-constexpr int L1_HOT_DEFAULT = 0;       // gathers from every source allocate in L1
-constexpr int VEC_DEFAULT = 0;          // srcList read 4 bytes per lane per load
+// Gathers from sources beyond the first L1_HOT_DEFAULT ids (the most-gathered, after
+// relabelling by out-degree) bypass L1. R-MAT 22: 11.83 ms per run with every gather
+// allocating, 11.65 with 32768 or 65536, 11.78 with 131072, 12.17 with 16384, 13.31 with 8192.
+constexpr int L1_HOT_DEFAULT = 32768;
+// srcList read 4 bytes per lane per load: 16-byte loads (pr.vec = 1) measured 0.7-3.7%
+// slower on R-MAT 22 at every l1_hot setting.
+constexpr int VEC_DEFAULT = 0;
 // degree-bin upper bounds for 1, 4, 8 and 32 lanes per row segment
 constexpr int BIN_T1 = 4, BIN_T4 = 16, BIN_T8 = 32;
 

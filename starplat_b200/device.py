@@ -340,6 +340,7 @@ class DeviceGraph:
 
     def bc(self, sources, out=None, variant: int = _lib.SP_BC_BATCHED):
         """Brandes BC over distinct `sources` (int32, host or device); float32[V]."""
+        _ensure_scheduler()  # the level model, when shipped, picks each level's direction
         if out is None:
             out = np.empty(self.V, np.float32)
         if isinstance(sources, (list, tuple)):

@@ -237,7 +237,7 @@ def test_update_rejects_weight_sums_outside_int32():
         with pytest.raises(_lib.SPError):  # held edge + addition wraps
             dg.update("a", [0], [1], [100])
         with pytest.raises(_lib.SPError):  # two additions of one new edge wrap
-            dg.update("aa", [2], [0], [2**31 - 1, 2**31 - 1])
+            dg.update("aa", [2, 2], [0, 0], [2**31 - 1, 2**31 - 1])
         # rejected batches leave the graph as it was
         assert dg.export()["edgeLen"].tolist() == [2**31 - 10, 5]
         dg.update("a", [0], [1], [9])
