@@ -4,11 +4,13 @@ Each algorithm's kernels take thresholds that change only how work is split:
   tc        tc.cta_warps: a bitmap per warp (0) or per CTA of 2 / 4 / 8 warps
   pagerank  pr.order: vertex order by out-degree (0) or in-degree class first (1);
             pr.src_hint: L1 policy of the srcList loads; pr.hot: sources of the
-            L1-resident hot phase (0 = one phase)
+            L1-resident hot phase (0 = one phase); pr.l1_hot: sources whose gathers
+            allocate in L1
   sssp      sssp.hub_deg / sssp.hub_chunk: queued vertices above hub_deg out-edges are
             relaxed in hub_chunk-edge pieces shared by all warps; sssp.local: warp
             cascade budget per round (0 = off)
-  bc        bc.hub_deg / bc.hub_chunk: the same for level-list entries
+  bc        bc.hub_deg / bc.hub_chunk: the same for level-list entries; bc.dir: push
+            only (0) or the pull rule (1) per forward level
 tune() times every candidate on the caller's graph with CUDA events on the graph's
 stream (median of `reps` runs after one untimed run), keeps the fastest, leaves it set
 on the graph and returns the table. Counts, distances, levels and path counts are the
@@ -25,9 +27,9 @@ import numpy as np
 
 KNOBS: Dict[str, Dict[str, Sequence[int]]] = {
     "tc": {"tc.cta_warps": (0, 2, 4, 8)},
-    "pagerank": {"pr.order": (0, 1), "pr.src_hint": (0, 2), "pr.hot": (0, 4096)},
+    "pagerank": {"pr.order": (0, 1), "pr.src_hint": (0, 2), "pr.hot": (0, 4096), "pr.l1_hot": (0, 32768, 131072)},
     "sssp": {"sssp.hub_deg": (64, 128, 512, 2048), "sssp.hub_chunk": (32, 64, 256), "sssp.local": (0, 16, 64)},
-    "bc": {"bc.hub_deg": (32, 64, 256, 4096), "bc.hub_chunk": (64, 128, 256)},
+    "bc": {"bc.hub_deg": (32, 64, 256, 4096), "bc.hub_chunk": (64, 128, 256), "bc.dir": (0, 1)},
 }
 
 

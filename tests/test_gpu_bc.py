@@ -175,16 +175,18 @@ def test_bc_level_trace_records_the_directions():
         dg.tune_set("bc.dir", 2)
         dg.tune_set("bc.trace", 1)
         dg.bc(srcs)
-        rec = np.zeros((4096, 4), np.float32)
+        rec = np.zeros((4096, 16), np.float32)
         t = np.zeros(4097, np.uint64)
         n = ctypes.c_int32()
         check("sp_bc_level_trace", lib().sp_bc_level_trace(dg.handle, rec.ctypes.data, t.ctypes.data, 4096,
                                                            ctypes.byref(n)))
     k = int(n.value)
     assert k > 3
-    assert set(rec[:k, 3].tolist()) <= {0.0, 1.0} and rec[:k, 3].sum() > 0
+    pull = rec[:k, _lib.SP_MLP_IN]
+    assert set(pull.tolist()) <= {0.0, 1.0} and pull.sum() > 0
+    assert np.array_equal(rec[:k, 10], pull)  # the direction input of the level model
     assert (np.diff(t[:k + 1].astype(np.int64)) >= 0).all()
-    assert (rec[:k, 0] > 0).all()
+    assert (rec[:k, 4] > 0).all()  # log2(1 + entries of the level)
 
 
 def test_bc_level_model_direction_keeps_results_and_matches_the_network():
