@@ -95,7 +95,10 @@ int sp_graph_export(sp_graph_h g, int32_t* indexofNodes, int32_t* edgeList, int3
  * edgeLen stays without. */
 int sp_graph_update(sp_graph_h g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
                     const int32_t* weight);
-/* Use this CUDA stream (a cudaStream_t) for all later work on g; NULL = the library's own stream. */
+/* Use this CUDA stream (a cudaStream_t) for all later work on g; NULL = the library's own
+ * stream (the one every graph starts with: a blocking stream, so it is ordered with work on
+ * the legacy default stream). To run on the legacy default stream itself pass
+ * cudaStreamLegacy, not NULL. */
 int sp_graph_set_stream(sp_graph_h g, void* cuda_stream);
 /* V, E, symmetric (1 when the forward CSR equals the reverse CSR). */
 int sp_graph_info(sp_graph_h g, int32_t* V, int64_t* E, int32_t* symmetric);
@@ -347,7 +350,8 @@ int sp_sched_load(const float* params, const float* feat_mean, const float* feat
  * the kernel takes the factor with the lowest predicted log cost per unit of distance.
  * Knob "sssp.epoch": -1 (default) learned when a model is loaded, else fixed width;
  * 0 fixed; 1 learned; 2 a seeded pseudo-random factor per epoch ("sssp.epoch_seed",
- * exploration). Distances are exact under any width sequence. */
+ * exploration). Knob "sssp.epoch_widen" = 1 restricts the choice to factors >= 1.
+ * Distances are exact under any width sequence. */
 int sp_sched_epoch_load(const float* params, const float* feat_mean, const float* feat_scale);
 /* No counterpart in the reference. Load or unload the process-wide BC level model: the
  * same network shape, predicting the log time of a forward level in each direction from

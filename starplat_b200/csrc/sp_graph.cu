@@ -466,7 +466,9 @@ int sp_graph_create(int32_t V, int64_t E, const int32_t* indexofNodes, const int
     sp_graph_free(g);
     return st;
   };
-  if (cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  // A blocking stream: ordered with the legacy default stream in both directions, so
+  // device inputs written there (and readers of device outputs there) need no extra sync.
+  if (cudaStreamCreateWithFlags(&g->stream, cudaStreamDefault) != cudaSuccess) {
     delete g;
     set_error("sp_graph_create: cudaStreamCreate failed");
     return SP_ERR_CUDA;
@@ -555,7 +557,7 @@ int sp_graph_set_stream(sp_graph_h g, void* cuda_stream) {
   g->own_stream = false;
   g->stream = (cudaStream_t)cuda_stream;
   if (!cuda_stream) {
-    cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
+    cudaStreamCreateWithFlags(&g->stream, cudaStreamDefault);
     g->own_stream = true;
   }
   return SP_OK;
@@ -640,6 +642,14 @@ int sp_tune_set(sp_graph_h g, const char* key, int64_t value) {
       return SP_ERR_INVALID;
     }
     g->sssp_epoch = (int32_t)value;
+    return SP_OK;
+  }
+  if (!strcmp(key, "sssp.epoch_widen")) {
+    if (value != 0 && value != 1) {
+      set_error("sp_tune_set: sssp.epoch_widen must be 0 or 1");
+      return SP_ERR_INVALID;
+    }
+    g->sssp_epoch_widen = (int32_t)value;
     return SP_OK;
   }
   if (!strcmp(key, "sssp.epoch_seed")) {

@@ -334,7 +334,7 @@ static int load_text(const char* path, int nthreads, sp_graph_h* out) {
   };
   cudaGetDevice(&g->device);
   g->V = V;
-  if (cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&g->stream, cudaStreamDefault) != cudaSuccess) {
     delete g;
     set_error("sp_graph_load_text: cudaStreamCreate failed");
     return SP_ERR_CUDA;

@@ -176,6 +176,7 @@ struct sp_graph {
   int32_t sssp_batch = 0;      // batched SSSP: sources per cooperative launch (0 = default)
   int32_t sssp_epoch = -1;     // SSSP per-epoch width: -1 learned if an epoch model is loaded, 0 fixed, 1 learned, 2 explore
   int32_t sssp_epoch_seed = 0;  // exploration seed
+  int32_t sssp_epoch_widen = 0;  // 1: the epoch model may only widen buckets
   int32_t sssp_trace = 0;      // 1: record the per-epoch trace of single-source solves
   int32_t sssp_last_epochs = 0;  // bucket advances of the last single-source solve
   int32_t sssp_last_epolicy = 0;  // the width policy the last solve ran

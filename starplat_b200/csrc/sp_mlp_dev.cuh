@@ -16,9 +16,10 @@ namespace sp {
 // barrier). NC x 32 threads of the CTA evaluate the hidden units (NC * 32 <= blockDim.x);
 // every thread of the CTA must call it. Every CTA that evaluates the same rows runs the
 // same instructions in the same order, so all return the same candidate: a decision
-// taken this way needs no barrier between CTAs. Ties go to the lower index.
+// taken this way needs no barrier between CTAs. Only candidates first .. NC-1 are
+// eligible; ties go to the lower index.
 template <int NC>
-__device__ int mlp_argmin(const float* __restrict__ model, float (*rows)[SP_MLP_IN]) {
+__device__ int mlp_argmin(const float* __restrict__ model, float (*rows)[SP_MLP_IN], int first = 0) {
   constexpr int IN = SP_MLP_IN, H = SP_MLP_HIDDEN;
   constexpr int W1 = 0, B1 = W1 + H * IN, W2 = B1 + H, B2 = W2 + H * H, W3 = B2 + H, B3 = W3 + H;
   static_assert(B3 + 1 == SP_MLP_PARAMS, "parameter layout");
@@ -53,8 +54,8 @@ __device__ int mlp_argmin(const float* __restrict__ model, float (*rows)[SP_MLP_
   }
   __syncthreads();
   if (t == 0) {
-    int best = 0;
-    for (int k = 1; k < NC; ++k)
+    int best = first;
+    for (int k = first + 1; k < NC; ++k)
       if (s_y[k] < s_y[best]) best = k;
     s_pick = best;
   }

@@ -116,7 +116,9 @@ struct PrPlan {
   int exec_iters = 0;
   float exec_beta = -1, exec_delta = -1;
   int exec_sh = -1;       // srcList policy, vector loads and L1 hot count the graph was captured with
-  cudaStream_t exec_stream = nullptr;
+  // The iterations are captured on this private stream and launched on the graph's
+  // stream, which may be the legacy default stream (where capture is not allowed).
+  cudaStream_t cap = nullptr;
 };
 
 int pr_order_default() { return pr::ORDER_DEFAULT; }
@@ -127,6 +129,7 @@ int pr_vec_default() { return pr::VEC_DEFAULT; }
 void free_pr_plan(PrPlan* p) {
   if (!p) return;
   if (p->exec) cudaGraphExecDestroy(p->exec);
+  if (p->cap) cudaStreamDestroy(p->cap);
   delete p;
 }
 
@@ -1085,23 +1088,25 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
     pr::k_init<<<num_sms() * 4, 256, 0, s>>>(V, p->od.p, p->prb[0].p, p->con[0].p, p->state.p);
   }
   SP_CHECK_LAUNCH();
-  if (!(p->exec && p->exec_iters == n_iter && p->exec_beta == beta && p->exec_delta == delta && p->exec_stream == s &&
+  if (!(p->exec && p->exec_iters == n_iter && p->exec_beta == beta && p->exec_delta == delta &&
         p->exec_sh == exec_key)) {
     if (p->exec) {
       cudaGraphExecDestroy(p->exec);
       p->exec = nullptr;
     }
+    if (!p->cap) SP_CHECK_CUDA(cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking));
+    cudaStream_t cs = p->cap;  // capture only records: nothing runs on it
     cudaGraph_t graph;
-    SP_CHECK_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    SP_CHECK_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < n_iter; ++k) {
       const int c = k & 1, n = c ^ 1;
       if (k < 2 && p->n_zero)
-        pr::k_zero_rows<<<num_sms() * 2, 256, 0, s>>>(a, p->zrows, p->n_zero, p->prb[c].p, p->prb[n].p, p->con[n].p);
+        pr::k_zero_rows<<<num_sms() * 2, 256, 0, cs>>>(a, p->zrows, p->n_zero, p->prb[c].p, p->prb[n].p, p->con[n].p);
       if (a.two_phase)
-        pr::k_phase<0, 1, 0, 0><<<grid, pr::THREADS, 0, s>>>(a, p->prb[c].p, p->con[c].p, p->prb[n].p, p->con[n].p);
-      ph1<<<grid, pr::THREADS, 0, s>>>(a, p->prb[c].p, p->con[c].p, p->prb[n].p, p->con[n].p);
+        pr::k_phase<0, 1, 0, 0><<<grid, pr::THREADS, 0, cs>>>(a, p->prb[c].p, p->con[c].p, p->prb[n].p, p->con[n].p);
+      ph1<<<grid, pr::THREADS, 0, cs>>>(a, p->prb[c].p, p->con[c].p, p->prb[n].p, p->con[n].p);
     }
-    cudaError_t ce = cudaStreamEndCapture(s, &graph);
+    cudaError_t ce = cudaStreamEndCapture(cs, &graph);
     if (ce != cudaSuccess) {
       set_error("pagerank graph capture: %s", cudaGetErrorString(ce));
       return SP_ERR_CUDA;
@@ -1116,7 +1121,6 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
     p->exec_iters = n_iter;
     p->exec_beta = beta;
     p->exec_delta = delta;
-    p->exec_stream = s;
     p->exec_sh = exec_key;
   }
   SP_CHECK_CUDA(cudaGraphLaunch(p->exec, s));

@@ -103,6 +103,7 @@ struct Args {
   // advanced is lowest under the epoch model; 2 = a pseudo-random factor per epoch
   // (exploration, to collect training data).
   int epolicy;
+  int ewiden;            // 1: only factors >= 1 (never narrower than the call's delta)
   unsigned eseed;
   const float* emodel;   // [SP_MLP_PARAMS + 2 * SP_MLP_IN]: parameters, feature mean, feature scale
   float* etrace;         // [etrace_cap][ETRACE]: per epoch, the chosen candidate's inputs, factor, advance
@@ -468,7 +469,7 @@ __device__ int epoch_choice(const Args& a, float fn, float rounds_prev, float re
   __shared__ float s_x[NFAC][SP_MLP_IN];
   if (threadIdx.x < NFAC)
     epoch_inputs(a, threadIdx.x, fn, rounds_prev, relaxed_prev, epoch, f_prev, progress, s_x[threadIdx.x]);
-  return mlp_argmin<NFAC>(a.emodel, s_x);
+  return mlp_argmin<NFAC>(a.emodel, s_x, a.ewiden ? 2 : 0);
 }
 
 // One delta-stepping solve by `nblk` co-resident CTAs (this one is number `blk`):
@@ -849,6 +850,7 @@ static int epoch_setup(sp_graph* g, ss::Args& a, bool trace) {
   if (pol < 0) pol = gen ? 1 : 0;
   if (pol == 1 && !gen) pol = 0;  // no model: the fixed width
   a.epolicy = pol;
+  a.ewiden = g->sssp_epoch_widen;
   a.eseed = (unsigned)g->sssp_epoch_seed;
   a.emodel = nullptr;
   a.etrace = nullptr;

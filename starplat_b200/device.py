@@ -40,6 +40,8 @@ def _is_device(a) -> bool:
     return hasattr(a, "is_cuda") and bool(a.is_cuda)
 
 
+CUDA_STREAM_LEGACY = 1  # cudaStreamLegacy: the legacy default stream, as a stream handle
+
 _SCHED_TRIED = False
 
 
@@ -236,8 +238,14 @@ class DeviceGraph:
         self.free()
 
     def set_stream(self, stream) -> None:
-        """Run later work on this CUDA stream (torch.cuda.Stream or raw cudaStream_t int)."""
+        """Run later work on this CUDA stream (torch.cuda.Stream or raw cudaStream_t int).
+
+        Torch's default stream has the handle 0, which the C ABI reads as "the library's
+        own stream"; it is passed as cudaStreamLegacy instead, so that the library's
+        kernels and torch's (and NCCL's) work on that stream stay in stream order."""
         raw = getattr(stream, "cuda_stream", stream)
+        if hasattr(stream, "cuda_stream") and raw == 0:
+            raw = CUDA_STREAM_LEGACY
         check("sp_graph_set_stream", lib().sp_graph_set_stream(self.handle, raw))
 
     def tune_set(self, key: str, value: int) -> None:
