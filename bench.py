@@ -39,9 +39,12 @@ graph (7 MB CSR), which is small by definition of its config.
 
 --impl reference times the reference's CPU path (the OpenMP form of the generated
 PageRank, restated in oracle/) alone on the host cores, same metric and config.
-Multi-GPU: the graph algorithms here run per graph on one GPU, so --gpus N runs N
-replicas ("replicas only"); value sums the edges all ranks processed over the max
-time (weak scaling).
+Multi-GPU (--gpus N under torchrun): the headline runs N replicas of the whole
+PageRank, and value sums the edges all ranks processed over the max time (weak
+scaling). Beside it, "pagerank_split" runs the same graph split over the ranks by
+vertices (all-gather of contrib blocks and all-reduce of the diff per iteration on
+device buffers; strong scaling), and the BC, clustering-coefficient and closeness
+legs split their sources or anchor parts over the ranks with one all-reduce.
 """
 from __future__ import annotations
 
@@ -389,6 +392,17 @@ def bench_bc(steps, warmup, stream, hbm, cpu, nsrc=256):
         else:
             ms, res = timed(lambda: dg.bc(srcs), steps, warmup, stream)
             bc_gpu = res[-1]
+            # forward direction per level: the default (push at every level, or the level
+            # model's choice when one is loaded) against the on-device frontier rule
+            dflt = dg.tune_get("bc.dir")
+            dg.tune_set("bc.dir", 1)
+            ms_rule, _ = timed(lambda: dg.bc(srcs), 3, 1, stream)
+            dg.tune_set("bc.dir", dflt)
+            out["direction"] = {"default": {"bc.dir": dflt, "ms": ms},
+                                "device_rule": {"bc.dir": 1, "ms": ms_rule},
+                                "note": "bc.dir -1 = the library default (push at every level, or the level "
+                                        "model when a model file is loaded); 1 = per-level push/pull rule on "
+                                        "the device"}
         few = srcs[:8]
         msp, _ = timed(lambda: dg.bc(few, variant=_lib.SP_BC_PLAIN), 1, 0, stream)
     out.update({"value": sum_er / (ms / 1e3) / 1e9, "unit": "GTEPS", "ms": ms,
@@ -546,8 +560,12 @@ def bench_louvain(steps, warmup, stream, hbm, cpu):
                                        "(communitydetection_sequential_allocation.cu) on this graph, run on a B200 "
                                        "and committed as a fixture",
                              "reference_q": ref["reference_q"], "q_minus_reference": res["q"] - ref["reference_q"],
-                             "tolerance": "|q - reference_q| <= 1e-3",
-                             "pass": abs(res["q"] - ref["reference_q"]) <= 1e-3}
+                             "tolerance": "q >= reference_q - 1e-3; where both stop in the same optimum, also "
+                                          "q <= reference_q + 1e-3",
+                             "same_optimum": abs(res["q"] - ref["reference_q"]) <= 1e-3,
+                             "reference_communities": ref.get("reference_communities"),
+                             "note": "Louvain is order dependent; the two may stop in different optima",
+                             "pass": res["q"] >= ref["reference_q"] - 1e-3}
     return out
 
 

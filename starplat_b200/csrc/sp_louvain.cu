@@ -29,14 +29,16 @@
 //    for integer weights); Q from the total internal weight (a CTA reduction) and
 //    the tot_c;
 //  * aggregation: communities renumbered densely, external edges emitted at scan
-//    positions, sorted by (c_u, c_v) with a radix sort and merged with a reduce-by-key.
-#include <cub/cub.cuh>
+//    positions with the key c_u * C + c_v, sorted by this library's stable LSD radix
+//    sort (sp_prims.cuh), and each run of equal keys summed by one warp in a fixed
+//    order (so the next level's weights do not depend on scheduling).
 
 #include <climits>
 #include <cmath>
 #include <vector>
 
 #include "sp_internal.cuh"
+#include "sp_prims.cuh"
 
 namespace sp {
 
@@ -395,8 +397,11 @@ __global__ void k_count_ext(Level L, const int32_t* __restrict__ comm, int32_t* 
   }
 }
 
+// External edge (v, u) of the level -> key newid[comm v] * C + newid[comm u], at the
+// scan position of v's external edges (in edge order)
 __global__ void k_emit(Level L, const int32_t* __restrict__ comm, const int32_t* __restrict__ newid,
-                       const int32_t* __restrict__ pos, unsigned long long* keys, double* vals, double* sl_new) {
+                       const int32_t* __restrict__ pos, unsigned long long C, unsigned long long* keys, double* vals,
+                       double* sl_new) {
   const int lane = threadIdx.x & 31;
   for (int v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < L.n; v += (gridDim.x * blockDim.x) >> 5) {
     const int cv = comm[v];
@@ -415,7 +420,7 @@ __global__ void k_emit(Level L, const int32_t* __restrict__ comm, const int32_t*
       const unsigned m = __ballot_sync(0xffffffffu, ext);
       if (ext) {
         const int p = base + __popc(m & ((1u << lane) - 1u));
-        keys[p] = (nv << 32) | (unsigned long long)(unsigned)newid[cu];
+        keys[p] = nv * C + (unsigned long long)(unsigned)newid[cu];
         vals[p] = L.w[j];
       }
       base += __popc(m);
@@ -425,10 +430,25 @@ __global__ void k_emit(Level L, const int32_t* __restrict__ comm, const int32_t*
   }
 }
 
-__global__ void k_build_rows(int m, const unsigned long long* __restrict__ ukeys, int32_t* adj, int32_t* rowcnt) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
-    adj[i] = (int32_t)(ukeys[i] & 0xffffffffull);
-    atomicAdd(&rowcnt[(int)(ukeys[i] >> 32)], 1);
+// One warp per run r of equal sorted keys [start[r], start[r + 1]): the next level's
+// edge r (column key % C, weight = the run's sum: lane-strided partial sums, then a
+// fixed xor tree) and one more edge in row key / C.
+__global__ void k_merge_runs(int runs, const int32_t* __restrict__ start, const unsigned long long* __restrict__ keys,
+                             const double* __restrict__ vals, unsigned long long C, int32_t* __restrict__ adj,
+                             double* __restrict__ w, int32_t* __restrict__ rowcnt) {
+  const int lane = threadIdx.x & 31;
+  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < runs; r += (gridDim.x * blockDim.x) >> 5) {
+    const int b = start[r], e = start[r + 1];
+    double acc = 0.0;
+    for (int j = b + lane; j < e; j += 32) acc += vals[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) {
+      const unsigned long long k = keys[b];
+      adj[r] = (int32_t)(k % C);
+      w[r] = acc;
+      atomicAdd(&rowcnt[(int)(k / C)], 1);
+    }
   }
 }
 
@@ -461,10 +481,10 @@ struct LvPlan {
   dbuf<double> w[2], sl[2];
   dbuf<int32_t> comm, newcomm, csize, used, newid, cnt, pos, orig, lists, rowcnt;
   dbuf<double> kv, tot, scal, qpart;
-  dbuf<unsigned long long> keys, skeys, ukeys;
-  dbuf<double> vals, svals, uvals;
+  dbuf<unsigned long long> keys, skeys;
+  dbuf<double> vals, svals;
+  dbuf<int32_t> head, ridx, rstart, scr;
   dbuf<int> icnt;
-  dbuf<unsigned char> temp;
   dbuf<double> gval;
   dbuf<int32_t> gkey;
   dbuf<int64_t> goff;
@@ -474,14 +494,9 @@ void free_lv_plan(LvPlan* p) { delete p; }
 
 namespace {
 
-template <class T>
-int dev_scan(LvPlan* p, const T* in, T* out, int n, cudaStream_t s) {
-  size_t tb = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, tb, in, out, n, s);
-  SP_TRY(p->temp.alloc(tb));
-  cub::DeviceScan::ExclusiveSum(p->temp.p, tb, in, out, n, s);
-  g_launches++;
-  return SP_OK;
+int dev_scan(LvPlan* p, const int32_t* in, int32_t* out, int n, cudaStream_t s) {
+  SP_TRY(p->scr.alloc(prim::scan_scratch(n)));
+  return prim::scan_exclusive<int32_t>(in, out, n, p->scr.p, s);
 }
 
 int read_int(const int* d, int* h, cudaStream_t s) { return copy_out(h, d, sizeof(int), s); }
@@ -725,36 +740,37 @@ extern "C" int sp_louvain(sp_graph_h g, const float* weight, double threshold, i
     SP_TRY(p->vals.alloc(std::max(1, mx)));
     SP_TRY(p->skeys.alloc(std::max(1, mx)));
     SP_TRY(p->svals.alloc(std::max(1, mx)));
-    SP_TRY(p->ukeys.alloc(std::max(1, mx)));
-    SP_TRY(p->uvals.alloc(std::max(1, mx)));
     SP_TRY(p->sl[nx].alloc(C));
     SP_CHECK_CUDA(cudaMemsetAsync(p->sl[nx].p, 0, sizeof(double) * C, s));
-    lv::k_emit<<<gs, 256, 0, s>>>(L, p->comm.p, p->newid.p, p->pos.p, p->keys.p, p->vals.p, p->sl[nx].p);
+    const unsigned long long CC = (unsigned long long)C;
+    lv::k_emit<<<gs, 256, 0, s>>>(L, p->comm.p, p->newid.p, p->pos.p, CC, p->keys.p, p->vals.p, p->sl[nx].p);
     SP_CHECK_LAUNCH();
-    int bits = 1;
-    while ((1ll << bits) < C) ++bits;
-    size_t tb = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, tb, p->keys.p, p->skeys.p, p->vals.p, p->svals.p, mx, 0, 32 + bits, s);
-    SP_TRY(p->temp.alloc(tb));
-    cub::DeviceRadixSort::SortPairs(p->temp.p, tb, p->keys.p, p->skeys.p, p->vals.p, p->svals.p, mx, 0, 32 + bits, s);
-    g_launches++;
-    tb = 0;
-    cub::DeviceReduce::ReduceByKey(nullptr, tb, p->skeys.p, p->ukeys.p, p->svals.p, p->uvals.p, p->icnt.p,
-                                   cub::Sum(), mx, s);
-    SP_TRY(p->temp.alloc(tb));
-    cub::DeviceReduce::ReduceByKey(p->temp.p, tb, p->skeys.p, p->ukeys.p, p->svals.p, p->uvals.p, p->icnt.p,
-                                   cub::Sum(), mx, s);
-    g_launches++;
+    int key_bits = 1;  // keys are below C * C
+    while (key_bits < 63 && (1ull << key_bits) < CC * CC) ++key_bits;
+    SP_TRY(p->scr.alloc(std::max(prim::sort_scratch(mx), prim::scan_scratch((int64_t)mx + 1))));
+    unsigned long long* sk = nullptr;
+    double* sv = nullptr;
+    SP_TRY(prim::radix_sort_pairs(p->keys.p, p->vals.p, p->skeys.p, p->svals.p, mx, key_bits, p->scr.p, &sk, &sv, s));
+    // runs of equal keys: heads, their scan, run starts
+    SP_TRY(p->head.alloc((size_t)mx + 1));
+    SP_TRY(p->ridx.alloc((size_t)mx + 1));
+    prim::k_run_heads<<<gs, 256, 0, s>>>(sk, mx, p->head.p);
+    SP_CHECK_LAUNCH();
+    SP_TRY(prim::scan_exclusive<int32_t>(p->head.p, p->ridx.p, (int64_t)mx + 1, p->scr.p, s));
     int mu = 0;
-    if (mx) SP_TRY(read_int(p->icnt.p, &mu, s));
+    SP_TRY(read_int(p->ridx.p + mx, &mu, s));
+    SP_TRY(p->rstart.alloc((size_t)mu + 1));
+    prim::k_run_starts<<<gs, 256, 0, s>>>(p->head.p, p->ridx.p, mx, p->rstart.p);
+    SP_CHECK_LAUNCH();
+    g_launches += 2;
     SP_TRY(p->off[nx].alloc(C + 1));
     SP_TRY(p->adj[nx].alloc(std::max(1, mu)));
     SP_TRY(p->w[nx].alloc(std::max(1, mu)));
     SP_CHECK_CUDA(cudaMemsetAsync(p->rowcnt.p, 0, sizeof(int32_t) * (C + 1), s));
     if (mu) {
-      lv::k_build_rows<<<gs, 256, 0, s>>>(mu, p->ukeys.p, p->adj[nx].p, p->rowcnt.p);
+      lv::k_merge_runs<<<gs, 256, 0, s>>>(mu, p->rstart.p, sk, sv, CC, p->adj[nx].p, p->w[nx].p, p->rowcnt.p);
       SP_CHECK_LAUNCH();
-      SP_CHECK_CUDA(cudaMemcpyAsync(p->w[nx].p, p->uvals.p, sizeof(double) * mu, cudaMemcpyDeviceToDevice, s));
+      g_launches++;
     }
     SP_TRY(dev_scan(p, p->rowcnt.p, p->off[nx].p, C + 1, s));
     cur = nx;
