@@ -136,6 +136,9 @@ int sp_graph_info(sp_graph_h g, int32_t* V, int64_t* E, int32_t* symmetric);
  *   "sssp.hub_deg", "sssp.hub_chunk"  SSSP: queued vertices with more out-edges than
  *             hub_deg are relaxed in hub_chunk-edge pieces shared by all warps
  *             (defaults 128 and 64).
+ *   "sssp.filter"  SSSP: 1 = load dist[u] and send the atomicMin only when the candidate
+ *             is lower; 0 = send every atomicMin at once (one L2 round trip less per
+ *             hop, more atomics); -1 = default: 0 inside warp cascades, 1 elsewhere.
  *   "sssp.local"  SSSP: in rounds whose frontier is at most 32 vertices per warp, a warp
  *             keeps relaxing the vertices it improved below the bucket threshold, up to
  *             this many 32-edge steps per round, before the grid barrier (0 = off,

@@ -699,6 +699,14 @@ int sp_tune_set(sp_graph_h g, const char* key, int64_t value) {
       g->sssp_hub_chunk = (int32_t)value;
     return SP_OK;
   }
+  if (!strcmp(key, "sssp.filter")) {
+    if (value < -1 || value > 1) {
+      set_error("sp_tune_set: sssp.filter must be -1, 0 or 1");
+      return SP_ERR_INVALID;
+    }
+    g->sssp_filter = (int32_t)value;
+    return SP_OK;
+  }
   if (!strcmp(key, "sssp.local")) {
     if (value < 0 || value > (1 << 16)) {
       set_error("sp_tune_set: sssp.local must be in [0, 65536]");
@@ -842,6 +850,10 @@ int sp_tune_get(sp_graph_h g, const char* key, int64_t* value) {
   }
   if (!strcmp(key, "sssp.hub_chunk")) {
     *value = g->sssp_hub_chunk > 0 ? g->sssp_hub_chunk : sssp_hub_chunk_default();
+    return SP_OK;
+  }
+  if (!strcmp(key, "sssp.filter")) {
+    *value = g->sssp_filter;
     return SP_OK;
   }
   if (!strcmp(key, "sssp.local")) {

@@ -171,6 +171,7 @@ struct sp_graph {
   int32_t sssp_last_incremental = 0;  // 1 if the last sp_sssp_dynamic warm-started
   int32_t tc_last_incremental = 0;    // 1 if the last sp_tc_dynamic counted only the batch
   int32_t sssp_hub_deg = 0;    // SSSP: vertices above this out-degree go to shared pieces (0 = default)
+  int32_t sssp_filter = -1;    // SSSP: 1 = load dist before each atomicMin, 0 = atomicMin only (-1 = default)
   int32_t sssp_hub_chunk = 0;  // SSSP: edges per piece (0 = default)
   int32_t sssp_local = -1;     // SSSP: warp cascade budget in 32-edge steps per round (-1 = default, 0 = off)
   int32_t sssp_batch = 0;      // batched SSSP: sources per cooperative launch (0 = default)

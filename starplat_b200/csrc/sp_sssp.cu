@@ -98,6 +98,9 @@ struct Args {
   int hub_deg;          // vertices with more out-edges are relaxed in pieces by all warps
   int hub_chunk;        // edges per piece
   int local_edges;      // cascade budget of a warp per round, in edges (0 = no cascades)
+  int filter;           // 1: load dist[u] and send the atomicMin only when it would lower it;
+                        // 0: send the atomicMin straight away (one L2 round trip less per hop);
+                        // -1: 0 in cascades, 1 elsewhere
   // Bucket width per epoch (the learned scheduler's per-iteration decision): 0 = every
   // bucket `delta` wide; 1 = the width factor whose predicted cost per unit of distance
   // advanced is lowest under the epoch model; 2 = a pseudo-random factor per epoch
@@ -227,13 +230,21 @@ __device__ __forceinline__ void push_near(const Args& a, bool want, int u, int r
 // any result is waited for. res: 1 = improved below the bucket threshold (with
 // STAMP, only the first such improvement of u this round), 2 = improved above it
 // and first in the far pile this epoch, 0 = nothing to queue. When two edges of a
-// group hit the same vertex, the atomics decide; the loads only filter.
+// group hit the same vertex, the atomics decide; the loads only filter. The dist
+// loads are skipped (every candidate goes to atomicMin) when a.filter is 0, and by
+// default in cascades (!STAMP), where they would add a round trip to each hop: grid
+// 4096^2 33.5 -> 30.6 ms; R-MAT 23 (no cascades) keeps them, where skipping them
+// everywhere measured 6.6 against 6.4 ms. Carrying each ring entry's CSR row, loaded
+// beside the atomicMin, to save the offset load of the next hop measured slower
+// (33.6 ms on the grid).
 template <bool STAMP, int N>
 __device__ __forceinline__ void relax_group(const Args& a, const int (&u)[N], const long long (&nd)[N],
                                             long long thr, int round, int epoch, int* fmin_slot, int (&res)[N]) {
+  const bool filt = a.filter < 0 ? STAMP : a.filter != 0;
   int cur[N], old[N];
 #pragma unroll
-  for (int q = 0; q < N; ++q) cur[q] = nd[q] < (long long)INT_MAX ? __ldcg(a.dist + u[q]) : INT_MIN;
+  for (int q = 0; q < N; ++q)
+    cur[q] = nd[q] < (long long)INT_MAX ? (filt ? __ldcg(a.dist + u[q]) : INT_MAX) : INT_MIN;
 #pragma unroll
   for (int q = 0; q < N; ++q) {
     old[q] = INT_MIN;
@@ -340,13 +351,15 @@ __device__ __forceinline__ void relax_batch(const Args& a, int v, long long thr,
   long long dv = 0;
   bool hub = false;
   if (v >= 0) {
+    // dist[v] is loaded with the offsets, not after the hub test; it is first needed
+    // after the adjacency loads below are issued
     b = a.off[v];
-    d = a.off[v + 1] - b;
+    const int e = a.off[v + 1];
+    dv = __ldcg(a.dist + v);
+    d = e - b;
     if (LOCAL && d > a.hub_deg) {
       hub = true;
       d = 0;
-    } else {
-      dv = __ldcg(a.dist + v);
     }
   }
   if (LOCAL) queue_push(a, hub && mark(qbits(a, round + 1), v), v, o.QN, o.qnext, o.HV, o.HB, o.hnext);
@@ -360,7 +373,7 @@ __device__ __forceinline__ void relax_batch(const Args& a, int v, long long thr,
   const int excl = inc - d;
   work += total;
   for (int t0 = 0; t0 < total; t0 += 32 * SU) {
-    int u[SU], res[SU];
+    int u[SU], res[SU], wt[SU], jq[SU];
     long long nd[SU];
 #pragma unroll
     for (int q = 0; q < SU; ++q) {
@@ -371,14 +384,19 @@ __device__ __forceinline__ void relax_batch(const Args& a, int v, long long thr,
         if (__shfl_sync(FULL, excl, j + k) <= t) j += k;
       const int jb = __shfl_sync(FULL, b, j);
       const int je = __shfl_sync(FULL, excl, j);
-      const long long jd = __shfl_sync(FULL, dv, j);
+      jq[q] = j;
       u[q] = 0;
-      nd[q] = INT_MAX;
+      wt[q] = 0;
       if (t < total) {
         const int k = jb + (t - je);
         u[q] = ld_stream(a.adj + k);
-        nd[q] = jd + ld_stream(a.w + k);
+        wt[q] = ld_stream(a.w + k);
       }
+    }
+#pragma unroll
+    for (int q = 0; q < SU; ++q) {
+      const long long jd = __shfl_sync(FULL, dv, jq[q]);
+      nd[q] = t0 + 32 * q + lane < total ? jd + wt[q] : (long long)INT_MAX;
     }
     relax_group<!LOCAL, SU>(a, u, nd, thr, round, epoch, o.fmin, res);
     push_group<LOCAL, SU>(a, res, u, round, o, r);
@@ -986,6 +1004,7 @@ static int sssp_delta(sp_graph* g, const int32_t* w, int32_t src, int32_t* dist_
   a.hub_deg = std::min(g->sssp_hub_deg > 0 ? g->sssp_hub_deg : ss::HUB_DEG, ss::HUB_DEG_MAX);
   a.hub_chunk = g->sssp_hub_chunk > 0 ? g->sssp_hub_chunk : ss::HUB_CHUNK;
   a.local_edges = 32 * local;
+  a.filter = g->sssp_filter;
   SP_TRY(epoch_setup(g, a, g->sssp_trace != 0));
   if (nseeds > 0) {
     ss::k_reset<<<1, 32, 0, s>>>(p->ctl.p);
@@ -1088,6 +1107,7 @@ static int sssp_delta_batches(sp_graph* g, const int32_t* w, const std::vector<i
   a.hub_deg = std::min(g->sssp_hub_deg > 0 ? g->sssp_hub_deg : ss::HUB_DEG, ss::HUB_DEG_MAX);
   a.hub_chunk = g->sssp_hub_chunk > 0 ? g->sssp_hub_chunk : ss::HUB_CHUNK;
   a.local_edges = 32 * local;
+  a.filter = g->sssp_filter;
   SP_TRY(epoch_setup(g, a, false));
   std::vector<ss::Ctl> hc(B);
   int64_t relaxed = 0;

@@ -90,6 +90,36 @@ def test_sssp_warp_cascade_budget_keeps_distances_exact(local):
         dg.tune_set("sssp.local", 64)
 
 
+@pytest.mark.parametrize("flt", [0, 1])
+def test_sssp_atomic_filter_knob_keeps_distances_exact(flt):
+    # 0: every candidate goes straight to atomicMin (no dist load first); also with
+    # negative weights (Bellman-Ford mode) and in the batched multi-source form
+    from graphs import star
+
+    cases = [weighted(G.rmat(13, 16, seed=8, directed=True), 1, 100), weighted(star(5000, directed_in=False), 1, 9),
+             weighted(G.grid(64, 80), 1, 1000), weighted(undirected_zoo()[3], 1, 1000)]
+    for g in cases:
+        dg = device_graph(g)
+        dg.tune_set("sssp.filter", flt)
+        assert dg.tune_get("sssp.filter") == flt
+        for src in (0, g.V // 2):
+            check(g, src)
+        check(g, g.V - 1, delta=2**31 - 1)
+        srcs = np.array([0, g.V // 3, g.V - 1], np.int32)
+        rows = dg.sssp_batch(srcs)
+        for k, s in enumerate(srcs):
+            assert np.array_equal(rows[k], O.sssp(g.indexofNodes, g.edgeList, g.edgeLen, int(s))), (g.name, int(s))
+        dg.tune_set("sssp.filter", -1)
+    rng = np.random.default_rng(4)
+    n = 300
+    pairs = np.array([(i, j) for i in range(n) for j in rng.choice(n, 4) if i < j], np.int32)
+    gn = from_pairs(n, pairs, name="dag_filter")
+    gn.edgeLen = rng.integers(-40, 100, gn.E).astype(np.int32)
+    dn = device_graph(gn)
+    dn.tune_set("sssp.filter", flt)
+    check(gn, 0)
+
+
 def test_sssp_cascade_with_negative_weights():
     rng = np.random.default_rng(2)
     n = 400
