@@ -6,7 +6,7 @@ graph size, degree skew, symmetry, weight range, the candidate). It is trained o
 timings this method generates (``collect`` times every candidate on a set of
 training graphs with CUDA events) by the project's own fused training kernel
 (``sp_mlp_train``), and loaded with ``sp_sched_load``; from then on sp_sssp with no
-explicit delta scores all 42 candidates on the GPU and runs the best one. Warp
+explicit delta scores all 63 candidates on the GPU and runs the best one. Warp
 cascades (the sssp.local knob) pay on thin, high-diameter frontiers and cost on
 skewed ones, so they are part of the choice. Without a model the fixed heuristic
 (delta = largest weight, 4 CTAs per SM, cascades of 64 steps) runs. Schedules change
@@ -53,7 +53,7 @@ EPOCH_FACTORS = (0.25, 0.5, 1.0, 2.0, 4.0, 8.0)  # the kernel's width candidates
 LEVEL_MODEL_PATH = os.path.join(_HERE, "sched_level_model.json")
 MULTS = (1, 2, 4, 8, 16, 32, 64)
 CTAS = (1, 2, 4)
-LOCALS = (0, 64)  # warp cascade budget per round (sssp.local), off or the default
+LOCALS = (0, 64, 256)  # warp cascade budget per round (sssp.local): off, the default, long
 CANDIDATES = [(m, c, l) for m in MULTS for c in CTAS for l in LOCALS]
 IN, P = _lib.SP_MLP_IN, _lib.SP_MLP_PARAMS
 
