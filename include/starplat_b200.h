@@ -279,6 +279,37 @@ int sp_sssp(sp_graph_h g, const int32_t* weight, int32_t src, int32_t* dist, int
  * device. Distances are bit-identical to sp_sssp's. */
 int sp_sssp_batch(sp_graph_h g, const int32_t* weight, const int32_t* sources, int32_t nsrc, int32_t* dist);
 
+/* Single-source SSSP split over GPUs by vertices: the 1-D partition with a per-bucket
+ * frontier exchange, in place of the host-staged property copies of the reference's
+ * multi-GPU generator (backend_multigpu/dsl_cpp_generator.cpp:604-678, :964-1005). Every
+ * rank holds the whole graph and owns the vertices v with v % nparts == part. The caller
+ * runs the collectives between the calls, on the same stream (sp_graph_set_stream),
+ * on DEVICE buffers:
+ *   begin     weight as in sp_sssp; delta <= 0 = the schedule sp_sssp would choose;
+ *             *cap = ceil(V / nparts). send and recv hold nparts * cap pairs of int32.
+ *   loop over rounds:
+ *     relax   the part's frontier: send <- (vertex, distance) pairs for the other parts'
+ *             vertices, packed in part order, send_counts[nparts] pairs each (at most
+ *             one pair per vertex per round).
+ *             The caller all-to-alls the counts, then the pairs.
+ *     apply   the n received pairs (msgs); *frontier = this part's next frontier size.
+ *             The caller sums *frontier over the ranks; while the sum is > 0, relax again.
+ *     far_min when the sum is 0: *far_min = this part's smallest far distance (INT_MAX:
+ *             none). The caller takes the minimum over the ranks: INT_MAX ends the solve.
+ *     advance otherwise: the next bucket from the global *far_min; *frontier as in apply
+ *             (sum it, then relax again).
+ *   dist      dist[V] (host or device): the owned entries, INT_MAX elsewhere; the
+ *             minimum over the ranks is Compute_SSSP's dist.
+ * Negative weights run as one bucket; more than 4V + 64 rounds is SP_ERR_NEG_CYCLE
+ * (from apply). A message for a vertex the part does not own is SP_ERR_INVALID. */
+int sp_sssp_part_begin(sp_graph_h g, int32_t part, int32_t nparts, const int32_t* weight, int32_t src,
+                       int64_t delta, int32_t* cap);
+int sp_sssp_part_relax(sp_graph_h g, int32_t* send, int32_t* send_counts);
+int sp_sssp_part_apply(sp_graph_h g, const int32_t* msgs, int32_t n, int32_t* frontier);
+int sp_sssp_part_far_min(sp_graph_h g, int32_t* far_min);
+int sp_sssp_part_advance(sp_graph_h g, const int32_t* far_min, int32_t* frontier);
+int sp_sssp_part_dist(sp_graph_h g, int32_t* dist);
+
 /* ---- betweenness centrality ----------------------------------------------------
  * Replaces generated `void Compute_BC(graph& g, float* BC, std::set<int>& sourceSet)`
  * (DSL staticDSLCodes/bc_dslV2:1-21): Brandes over the given distinct sources,

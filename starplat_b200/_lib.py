@@ -87,6 +87,12 @@ SIGNATURES = {
     "sp_pagerank_part_finish": (ctypes.c_int, [vp, vp, vp]),
     "sp_sssp": (ctypes.c_int, [vp, vp, i32, vp, i64, i32, P(i32)]),
     "sp_sssp_batch": (ctypes.c_int, [vp, vp, vp, i32, vp]),
+    "sp_sssp_part_begin": (ctypes.c_int, [vp, i32, i32, vp, i32, i64, P(i32)]),
+    "sp_sssp_part_relax": (ctypes.c_int, [vp, vp, vp]),
+    "sp_sssp_part_apply": (ctypes.c_int, [vp, vp, i32, vp]),
+    "sp_sssp_part_far_min": (ctypes.c_int, [vp, vp]),
+    "sp_sssp_part_advance": (ctypes.c_int, [vp, vp, vp]),
+    "sp_sssp_part_dist": (ctypes.c_int, [vp, vp]),
     "sp_bc": (ctypes.c_int, [vp, vp, i32, vp, i32]),
     "sp_bc_graphs": (ctypes.c_int, [vp, i32, vp, vp, vp, vp]),
     "sp_bfs_sigma": (ctypes.c_int, [vp, vp, i32, vp, vp]),

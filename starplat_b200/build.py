@@ -20,7 +20,8 @@ ROOT = os.path.dirname(HERE)
 INCLUDE = os.path.join(ROOT, "include")
 
 CU_SOURCES = ["sp_graph.cu", "sp_pagerank.cu", "sp_tc.cu", "sp_sssp.cu", "sp_bc.cu", "sp_louvain.cu",
-              "sp_noalloc.cu", "sp_mlp.cu", "sp_ingest.cu", "sp_centrality.cu"]
+              "sp_noalloc.cu", "sp_mlp.cu", "sp_ingest.cu", "sp_centrality.cu",
+              "sp_sssp_part.cu"]
 NVCC_FLAGS = [
     "-O3", "-std=c++17", "-lineinfo",
     "-gencode", "arch=compute_100a,code=sm_100a",

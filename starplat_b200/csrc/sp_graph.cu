@@ -536,6 +536,7 @@ int sp_graph_free(sp_graph_h g) {
   free_sssp_plan(g->sssp);
   free_bc_plan(g->bc);
   free_lv_plan(g->lv);
+  free_sssp_part_plan(g->sssp_part);
   g->off.release();
   g->adj.release();
   g->w.release();

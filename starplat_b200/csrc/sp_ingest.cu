@@ -611,11 +611,13 @@ int update_graph(sp_graph* g, int64_t n, const char* type, const int32_t* src, c
   free_sssp_plan(g->sssp);
   free_bc_plan(g->bc);
   free_lv_plan(g->lv);
+  free_sssp_part_plan(g->sssp_part);
   g->pr = nullptr;
   g->tc = nullptr;
   g->sssp = nullptr;
   g->bc = nullptr;
   g->lv = nullptr;
+  g->sssp_part = nullptr;
   g->off.swap(off);
   g->adj.swap(adj);
   if (g->has_w) g->w.swap(w);

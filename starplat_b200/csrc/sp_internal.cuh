@@ -134,11 +134,13 @@ struct TcPlan;
 struct SsspPlan;
 struct BcPlan;
 struct LvPlan;
+struct SsspPartPlan;
 void free_pr_plan(PrPlan*);
 void free_tc_plan(TcPlan*);
 void free_sssp_plan(SsspPlan*);
 void free_bc_plan(BcPlan*);
 void free_lv_plan(LvPlan*);
+void free_sssp_part_plan(SsspPartPlan*);
 
 }  // namespace sp
 
@@ -198,6 +200,7 @@ struct sp_graph {
   sp::SsspPlan* sssp = nullptr;
   sp::BcPlan* bc = nullptr;
   sp::LvPlan* lv = nullptr;
+  sp::SsspPartPlan* sssp_part = nullptr;  // split single-source SSSP (sp_sssp_part_*)
 };
 
 namespace sp {
@@ -225,6 +228,12 @@ int bc_hub_chunk_default();
 int bc_cluster_default();
 int ensure_symmetry(sp_graph* g);     // fills g->symmetric
 int copy_out(void* dst, const void* src, size_t bytes, cudaStream_t s);  // host or device dst
+// SSSP helpers shared with the split solve (sp_sssp.cu): the weights on the device (the
+// caller's, host or device, or edgeLen) with their range recorded; the bucket width the
+// single-GPU solve would use; the smallest weight of the last weights prepared.
+int sssp_weights_for(sp_graph* g, const int32_t* weight, const int32_t** w);
+int sssp_width_for(sp_graph* g, int64_t& delta);
+int sssp_weight_min(sp_graph* g);
 int num_sms();
 }  // namespace sp
 

@@ -1247,6 +1247,15 @@ static int sssp_schedule(sp_graph* g, int64_t& delta, int& ctas, int& local) {
   return SP_OK;
 }
 
+int sssp_weights_for(sp_graph* g, const int32_t* weight, const int32_t** w) { return sssp_prepare(g, weight, w); }
+
+int sssp_width_for(sp_graph* g, int64_t& delta) {
+  int ctas = 0, local = 0;
+  return sssp_schedule(g, delta, ctas, local);
+}
+
+int sssp_weight_min(sp_graph* g) { return g->sssp ? g->sssp->w_min : 0; }
+
 }  // namespace sp
 
 extern "C" int sp_sssp(sp_graph_h g, const int32_t* weight, int32_t src, int32_t* dist, int64_t delta,

@@ -331,6 +331,35 @@ class DeviceGraph:
     def pagerank_part_finish(self, ranks, out) -> None:
         check("sp_pagerank_part_finish", lib().sp_pagerank_part_finish(self.handle, _ptr(ranks), _ptr(out)))
 
+    # ---- single-source SSSP split over ranks by vertices (sp_sssp_part_*; driven by
+    # distributed.sssp_on_gpus)
+    def sssp_part_begin(self, part: int, nparts: int, src: int, weight=None, delta: int = 0) -> int:
+        """Starts this rank's part of a split solve from src; returns cap (the send and
+        receive buffers hold nparts * cap int32 pairs)."""
+        _ensure_scheduler()  # delta <= 0: the width sp_sssp would choose
+        if weight is not None and str(weight.dtype) not in ("int32", "torch.int32"):
+            raise TypeError("weights must be int32")
+        cap = ctypes.c_int32()
+        check("sp_sssp_part_begin", lib().sp_sssp_part_begin(self.handle, int(part), int(nparts), _ptr(weight),
+                                                             int(src), int(delta), ctypes.byref(cap)))
+        return int(cap.value)
+
+    def sssp_part_relax(self, send, send_counts) -> None:
+        check("sp_sssp_part_relax", lib().sp_sssp_part_relax(self.handle, _ptr(send), _ptr(send_counts)))
+
+    def sssp_part_apply(self, msgs, n: int, frontier) -> None:
+        check("sp_sssp_part_apply", lib().sp_sssp_part_apply(self.handle, _ptr(msgs) if n else None, int(n),
+                                                             _ptr(frontier)))
+
+    def sssp_part_far_min(self, far_min) -> None:
+        check("sp_sssp_part_far_min", lib().sp_sssp_part_far_min(self.handle, _ptr(far_min)))
+
+    def sssp_part_advance(self, far_min, frontier) -> None:
+        check("sp_sssp_part_advance", lib().sp_sssp_part_advance(self.handle, _ptr(far_min), _ptr(frontier)))
+
+    def sssp_part_dist(self, dist) -> None:
+        check("sp_sssp_part_dist", lib().sp_sssp_part_dist(self.handle, _ptr(dist)))
+
     def sssp_batch(self, sources, weight=None, out=None):
         """Distances from every source (int32, host or device) in batched cooperative
         launches, one CTA group per source: int32[nsrc][V], row k from sources[k]

@@ -13,6 +13,9 @@ one all-reduce adds an int64 count or an int32[V] vector, exactly.
 PageRank splits vertices (pagerank_on_gpus): rank r owns the rows of part r, and every
 iteration ends with an all-gather of the parts' contrib blocks and an all-reduce of the
 L1 diff, both on device buffers; the stop test runs on the device.
+Single-source SSSP splits vertices too (sssp_on_gpus): rank r owns v % world == r, and
+every delta-stepping round ends with an all-to-all of (vertex, distance) messages for
+the other ranks' vertices and a sum of the frontier sizes.
 The process group comes from replicas.Replicas (NCCL on GPUs, gloo on the host).
 """
 from __future__ import annotations
@@ -164,3 +167,66 @@ def pagerank_on_gpus(dg, rep: Optional[Replicas] = None, beta: float = 1e-6, del
         out = np.empty(dg.V, np.float32)
     dg.pagerank_part_finish(full, out)
     return out, it, d
+
+
+INT_MAX = 2**31 - 1
+
+
+def sssp_on_gpus(dg, rep: Optional[Replicas] = None, src: int = 0, weight=None, delta: int = 0, out=None):
+    """Compute_SSSP split over the ranks by vertices (sp_sssp_part_*): every rank holds
+    the whole graph and owns the vertices v with v % world == rank. A delta-stepping
+    round relaxes each rank's frontier; candidates for other ranks' vertices travel as
+    (vertex, distance) pairs, at most one per vertex per round, in one all-to-all (its
+    counts first); the frontier sizes are summed to decide whether the bucket goes on.
+    An empty bucket everywhere moves all ranks to the bucket of the smallest far
+    distance (a minimum over the ranks), and INT_MAX there ends the solve. This is the
+    1-D partition with a per-bucket frontier exchange that replaces the host-staged
+    copies of the reference's multi-GPU code (backend_multigpu/dsl_cpp_generator.cpp:
+    604-678). Returns (dist int32[V], rounds); `out` (host or device) receives dist."""
+    import torch
+
+    from .device import DeviceGraph
+
+    rep = rep or Replicas()
+    dev = rep.device()
+    if isinstance(dg, DeviceGraph):
+        if dev.type != "cuda":
+            raise ValueError("sssp_on_gpus: the message buffers must be device tensors (NCCL or one GPU)")
+        dg.set_stream(torch.cuda.current_stream())  # the collectives' stream order
+    n, r = rep.world, rep.rank
+    cap = dg.sssp_part_begin(r, n, src, weight, delta)
+    send = torch.empty((n * cap, 2), dtype=torch.int32, device=dev)
+    recv = torch.empty((n * cap, 2), dtype=torch.int32, device=dev)
+    scount = torch.zeros(n, dtype=torch.int32, device=dev)
+    rcount = torch.zeros(n, dtype=torch.int32, device=dev)
+    frontier = torch.zeros(1, dtype=torch.int32, device=dev)
+    far = torch.zeros(1, dtype=torch.int32, device=dev)
+    rounds = 0
+    while True:
+        while True:  # the rounds of one bucket
+            dg.sssp_part_relax(send, scount)
+            rep.all_to_all(rcount, scount, [1] * n, [1] * n)
+            sc, rc = scount.tolist(), rcount.tolist()
+            ns, nr = sum(sc), sum(rc)
+            rep.all_to_all(recv[:nr], send[:ns], rc, sc)
+            dg.sssp_part_apply(recv, nr, frontier)
+            rep.all_reduce_sum(frontier)
+            rounds += 1
+            if int(frontier.item()) == 0:
+                break
+        dg.sssp_part_far_min(far)
+        rep.all_reduce_min(far)
+        if int(far.item()) == INT_MAX:
+            break
+        dg.sssp_part_advance(far, frontier)
+        rep.all_reduce_sum(frontier)
+    full = torch.empty(dg.V, dtype=torch.int32, device=dev)
+    dg.sssp_part_dist(full)
+    rep.all_reduce_min(full)
+    if out is None:
+        out = full.cpu().numpy()
+    elif isinstance(out, np.ndarray):
+        out[:] = full.cpu().numpy()
+    else:
+        out.copy_(full)
+    return out, rounds

@@ -89,6 +89,23 @@ class Replicas:
             return
         self._dist.all_gather_into_tensor(full, part)
 
+    def all_reduce_min(self, t) -> None:
+        """Element-wise minimum over all ranks, in place (a torch tensor on the backend's
+        device)."""
+        if self._dist is not None:
+            self._dist.all_reduce(t, op=self._dist.ReduceOp.MIN)
+
+    def all_to_all(self, out, inp, out_splits, in_splits) -> None:
+        """Rank q's inp[sum(in_splits[:r]) : + in_splits[r]] lands in rank r's out at
+        sum(out_splits[:q]); splits are element counts along dim 0 (host ints). One rank:
+        a copy."""
+        if self._dist is None:
+            n = int(in_splits[0])
+            if n:
+                out[:n].copy_(inp[:n])
+            return
+        self._dist.all_to_all_single(out, inp, [int(x) for x in out_splits], [int(x) for x in in_splits])
+
     def device(self):
         """Where this rank's collective tensors live: the host under gloo, else this
         rank's GPU (NCCL, or a single process with a GPU), else the host."""

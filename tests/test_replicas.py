@@ -374,3 +374,129 @@ def test_pagerank_split_over_ranks_matches_the_oracle(tmp_path, world):
     for r in range(world):
         pr = np.load(tmp_path / f"pr{r}.npy").astype(np.float64)
         assert np.abs(pr - exact).sum() < 1e-6
+
+
+INT_MAX = 2**31 - 1
+
+
+class _HostSsspPart:
+    """A host stand-in for DeviceGraph's split-SSSP calls (test infrastructure): the same
+    contract (vertices owned by v % nparts, one (vertex, distance) pair per foreign vertex
+    per round packed in part order, frontier sizes and far minima for the caller to
+    combine), computed with Python sets and numpy, so that the loop and the collectives
+    of distributed.sssp_on_gpus run between real gloo ranks."""
+
+    def __init__(self, g):
+        self.g, self.V = g, g.V
+
+    def sssp_part_begin(self, part, nparts, src, weight=None, delta=0):
+        g = self.g
+        self.r, self.n = part, nparts
+        self.w = np.asarray(g.edgeLen if weight is None else weight, np.int64)
+        if self.w.size and self.w.min() < 0:
+            self.delta = 1 << 62
+        else:
+            self.delta = int(delta) if delta > 0 else max(1, int(self.w.max()) if self.w.size else 1)
+        self.dist = np.full(self.V, INT_MAX, np.int64)
+        self.Q, self.QN, self.F = set(), set(), set()
+        if src % nparts == part:
+            self.dist[src] = 0
+            self.Q.add(src)
+        self.thr, self.rounds = self.delta, 0
+        self.cap = -(-self.V // nparts)
+        return self.cap
+
+    def _queue(self, u, d):
+        (self.QN if d < self.thr else self.F).add(u)
+
+    def sssp_part_relax(self, send, send_counts):
+        g, out = self.g, [dict() for _ in range(self.n)]
+        for v in sorted(self.Q):
+            for k in range(g.indexofNodes[v], g.indexofNodes[v + 1]):
+                u, nd = int(g.edgeList[k]), int(self.dist[v] + self.w[k])
+                if nd >= INT_MAX:
+                    continue
+                q = u % self.n
+                if q == self.r:
+                    if nd < self.dist[u]:
+                        self.dist[u] = nd
+                        self._queue(u, nd)
+                elif nd < out[q].get(u, INT_MAX):
+                    out[q][u] = nd
+        at = 0
+        for q in range(self.n):
+            pairs = sorted(out[q].items())
+            for i, (u, d) in enumerate(pairs):
+                send[at + i, 0], send[at + i, 1] = u, d
+            send_counts[q] = len(pairs)
+            at += len(pairs)
+
+    def sssp_part_apply(self, msgs, n, frontier):
+        for i in range(n):
+            u, d = int(msgs[i, 0]), int(msgs[i, 1])
+            assert u % self.n == self.r
+            if d < self.dist[u]:
+                self.dist[u] = d
+                self._queue(u, d)
+        self.Q, self.QN = self.QN, set()
+        frontier[0] = len(self.Q)
+        self.rounds += 1
+        if self.rounds > 4 * self.V + 64:
+            from starplat_b200 import _lib
+
+            raise _lib.SPError(-6, "negative cycle")
+
+    def sssp_part_far_min(self, far):
+        far[0] = min([int(self.dist[u]) for u in self.F if self.dist[u] >= self.thr], default=INT_MAX)
+
+    def sssp_part_advance(self, far, frontier):
+        fm, old = int(far[0]), self.thr
+        self.thr = (fm // self.delta + 1) * self.delta
+        self.Q = {u for u in self.F if old <= self.dist[u] < self.thr}
+        self.F = {u for u in self.F if self.dist[u] >= self.thr}
+        frontier[0] = len(self.Q)
+
+    def sssp_part_dist(self, out):
+        own = np.arange(self.V) % self.n == self.r
+        out.copy_(torch_from(np.where(own, self.dist, INT_MAX).astype(np.int32)))
+
+
+def _sssp_graphs():
+    from starplat_b200 import generators as G
+
+    g = G.rmat(9, 8, seed=13, directed=True)
+    g.edgeLen = G.hash_weights(g, 13, 1, 100, False)
+    gg = G.grid(12, 17)
+    gg.edgeLen = G.hash_weights(gg, 14, 1, 1000, True)
+    return [(g, 3), (gg, 0), (gg, 100)]
+
+
+def _sssp_rank_main(rank, world, port, out_dir):
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port), "RANK": str(rank),
+                       "WORLD_SIZE": str(world), "LOCAL_RANK": str(rank)})
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from starplat_b200.distributed import sssp_on_gpus
+    from starplat_b200.replicas import Replicas
+    from test_replicas import _HostSsspPart, _sssp_graphs
+
+    rep = Replicas(backend="gloo", timeout_s=60)
+    for k, (g, src) in enumerate(_sssp_graphs()):
+        d, rounds = sssp_on_gpus(_HostSsspPart(g), rep, src)
+        np.save(os.path.join(out_dir, f"d{k}_{rank}.npy"), d)
+    rep.close()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_sssp_split_over_ranks_matches_the_oracle(tmp_path, world):
+    # every rank owns v % world; each round's pairs for other ranks' vertices go through
+    # one gloo all-to-all, frontier sizes are summed, far minima and dist vectors reduced
+    # by minimum; every rank ends with the whole dist vector, equal to the oracle's
+    from oracle import oracle as O
+
+    mp.start_processes(_sssp_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    for k, (g, src) in enumerate(_sssp_graphs()):
+        ref = O.sssp(g.indexofNodes, g.edgeList, g.edgeLen, src)
+        for r in range(world):
+            assert np.array_equal(np.load(tmp_path / f"d{k}_{r}.npy"), ref), (k, r)
