@@ -43,8 +43,9 @@ Multi-GPU (--gpus N under torchrun): the headline runs N replicas of the whole
 PageRank, and value sums the edges all ranks processed over the max time (weak
 scaling). Beside it, "pagerank_split" runs the same graph split over the ranks by
 vertices (all-gather of contrib blocks and all-reduce of the diff per iteration on
-device buffers; strong scaling), and the BC, clustering-coefficient and closeness
-legs split their sources or anchor parts over the ranks with one all-reduce.
+device buffers; strong scaling), the BC, clustering-coefficient and closeness legs
+split their sources or anchor parts over the ranks with one all-reduce, and the SSSP
+legs add a "split" entry: the single-source solve split over the ranks by vertices.
 """
 from __future__ import annotations
 
@@ -330,6 +331,19 @@ def bench_sssp(name, g, src, steps, warmup, stream, hbm, cpu, cpu_mode):
                  "ctas_per_sm": dg.tune_get("sssp.last_ctas"), "local": dg.tune_get("sssp.last_local")}
         msp, resp = timed(lambda: dg.sssp(src, out=dist, variant=_lib.SP_SSSP_PLAIN), 1, 0, stream)
         same = bool(np.array_equal(dist.cpu().numpy(), d) and np.array_equal(d_fixed, d))
+        if REP is not None and REP.world > 1:
+            # the same solve split over the GPUs by vertices (strong scaling): an all-to-all
+            # of (vertex, distance) pairs per round, MIN reductions per bucket
+            from starplat_b200.distributed import sssp_on_gpus
+
+            dsplit = torch.empty(g.V, dtype=torch.int32, device="cuda")
+            sssp_on_gpus(dg, REP, src, out=dsplit)
+            REP.barrier()
+            mss, ress = timed(lambda: sssp_on_gpus(dg, REP, src, out=dsplit), max(1, min(steps, 3)), 0, stream)
+            mss = REP.max(mss)
+            out["split"] = {"value": er / (mss / 1e3) / 1e9, "unit": "GTEPS", "ms": mss, "rounds": ress[-1][1],
+                            "scaling": "strong", "same_distances": bool(np.array_equal(dsplit.cpu().numpy(), d)),
+                            "parallelism": f"1-D vertex partition over {REP.world} GPUs (v mod {REP.world})"}
     fixed["value"] = er / (msf / 1e3) / 1e9
     out.update({"value": er / (ms / 1e3) / 1e9, "unit": "GTEPS", "ms": ms, "E_r": er, "reached": nr,
                 "rounds": res[0][1], "relaxed_per_edge": round(relaxed / max(1, er), 3), "schedule": sched,
