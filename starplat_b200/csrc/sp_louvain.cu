@@ -352,19 +352,59 @@ __global__ void k_tot(int n, const int32_t* __restrict__ comm, const double* __r
 // Q = sum_c in_c / W - (tot_c / W)^2 needs only the total internal weight
 // sum_c in_c = sum_v (weight of v's edges inside its community + its self-loop):
 // one partial per CTA, no per-community atomics; the host adds the partials of both
-// kernels in CTA order, so Q is the same on every run.
+// kernels in CTA order, so Q is the same on every run. A warp takes 32 vertices at a
+// time and spreads their edges over its lanes (an exclusive scan of the degrees), four
+// 32-edge steps with their loads in flight together: the row walk of one vertex per
+// warp was a chain of dependent loads per vertex (SBM 1M: 318 us per call).
 __global__ void __launch_bounds__(THREADS) k_internal(Level L, const int32_t* __restrict__ comm, double W,
                                                       double* q) {
+  constexpr int U = 4;
   __shared__ double s_red[THREADS / 32];
   const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
   double acc = 0;
-  for (int v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < L.n; v += (gridDim.x * blockDim.x) >> 5) {
-    const int cv = comm[v];
-    double s = 0;
-    for (int j = L.off[v] + lane; j < L.off[v + 1]; j += 32)
-      if (comm[L.adj[j]] == cv) s += L.w[j];
-    s = warp_sum(s);
-    if (lane == 0) acc += s + L.sl[v];
+  for (int base = gw * 32; base < L.n; base += nw * 32) {
+    const int v = base + lane;
+    int b = 0, d = 0, cv = -1;
+    if (v < L.n) {
+      b = L.off[v];
+      d = L.off[v + 1] - b;
+      cv = comm[v];
+      acc += L.sl[v];
+    }
+    int inc = d;
+#pragma unroll
+    for (int k = 1; k < 32; k <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, inc, k);
+      if (lane >= k) inc += t;
+    }
+    const int total = __shfl_sync(0xffffffffu, inc, 31);
+    const int excl = inc - d;
+    for (int t0 = 0; t0 < total; t0 += 32 * U) {
+      int u[U], cq[U];
+      double wq[U];
+#pragma unroll
+      for (int q = 0; q < U; ++q) {
+        const int t = t0 + 32 * q + lane;
+        int j = 0;  // the last lane whose edges start at or before t
+#pragma unroll
+        for (int k = 16; k > 0; k >>= 1)
+          if (__shfl_sync(0xffffffffu, excl, j + k) <= t) j += k;
+        const int jb = __shfl_sync(0xffffffffu, b, j);
+        const int je = __shfl_sync(0xffffffffu, excl, j);
+        cq[q] = __shfl_sync(0xffffffffu, cv, j);
+        u[q] = -1;
+        wq[q] = 0.0;
+        if (t < total) {
+          const int k = jb + (t - je);
+          u[q] = L.adj[k];
+          wq[q] = L.w[k];
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < U; ++q)
+        if (u[q] >= 0 && comm[u[q]] == cq[q]) acc += wq[q];
+    }
   }
   acc = block_sum<THREADS>(acc, s_red);
   if (threadIdx.x == 0) q[blockIdx.x] = acc / W;
