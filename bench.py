@@ -806,6 +806,48 @@ def bench_update(steps, warmup, stream, cpu, nupd=1 << 20):
                            "resume_ms": 1e3 * statistics.median(res_t),
                            "update_and_full_solve_ms": 1e3 * statistics.median(full_t),
                            "same_distances": same}
+    # DynSSSP batches of deletions of edges the graph holds (64 or 4096 per batch): the
+    # decremental pass through parents (or a new solve when it would reset > V / 4)
+    # against the same update followed by a full solve
+    src_of = np.repeat(np.arange(g.V, dtype=np.int32), np.diff(g.indexofNodes))
+    out["sssp_dynamic_deletions"] = {}
+    gd = G.grid(1024, 1024)  # high diameter: a full solve takes hundreds of rounds
+    gd.edgeLen = G.hash_weights(gd, 1024, 1, 1000, True)
+    gd_src = np.repeat(np.arange(gd.V, dtype=np.int32), np.diff(gd.indexofNodes))
+    for key, gg, gsrc, sv, nd in (("rmat20_64", g, src_of, source, 64), ("rmat20_4096", g, src_of, source, 4096),
+                                  ("grid1024_64", gd, gd_src, 3 * gd.V // 7, 64)):
+        rep_t, full_t, same, paths, marked = [], [], True, [], []
+        with DeviceGraph.from_csr(gg, with_reverse=False) as da, DeviceGraph.from_csr(gg, with_reverse=False) as db:
+            da.set_stream(stream)
+            db.set_stream(stream)
+            dist = torch.empty(gg.V, dtype=torch.int32, device="cuda")
+            dfull = torch.empty(gg.V, dtype=torch.int32, device="cuda")
+            _, first_rounds = da.sssp(sv, out=dist)
+            da.tune_set("sssp.repair", 1)  # time the repair itself; the default picks by rounds
+            for k in range(warmup + steps):
+                pick = rng.choice(gg.E, nd, replace=False)  # edges of the original graph (some already gone)
+                bs, bd = gsrc[pick], gg.edgeList[pick].astype(np.int32)
+                torch_sync()
+                t = time.perf_counter()
+                da.sssp_dynamic("d" * nd, bs, bd, None, sv, dist)
+                torch_sync()
+                t1 = time.perf_counter()
+                paths.append(da.tune_get("sssp.last_incremental"))
+                marked.append(da.tune_get("sssp.last_marked"))
+                db.update("d" * nd, bs, bd)
+                db.sssp(sv, out=dfull)
+                torch_sync()
+                t2 = time.perf_counter()
+                if k >= warmup:
+                    rep_t.append(t1 - t)
+                    full_t.append(t2 - t1)
+                same = same and bool(torch.equal(dist, dfull))
+        out["sssp_dynamic_deletions"][key] = {
+            "workload": f"{nd} deleted edges per batch, source {sv}", "ms": 1e3 * statistics.median(rep_t),
+            "update_and_full_solve_ms": 1e3 * statistics.median(full_t), "batches_repaired": paths.count(2),
+            "vertices_reset_median": statistics.median(marked), "V": gg.V, "first_solve_rounds": first_rounds,
+            "default_policy": "repair" if first_rounds >= 32 else "solve again",
+            "batches_solved_again": paths.count(0), "same_distances": same}
     # DynPR batches of 4096 added edges: PageRank from the previous ranks
     # (sp_pagerank_dynamic) against the same update followed by PageRank from 1/V
     warm_t, cold_t, warm_it, cold_it, l1 = [], [], [], [], 0.0

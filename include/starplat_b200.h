@@ -136,6 +136,13 @@ int sp_graph_info(sp_graph_h g, int32_t* V, int64_t* E, int32_t* symmetric);
  *   "sssp.hub_deg", "sssp.hub_chunk"  SSSP: queued vertices with more out-edges than
  *             hub_deg are relaxed in hub_chunk-edge pieces shared by all warps
  *             (defaults 128 and 64).
+ *   "sssp.repair"  sp_sssp_dynamic: 1 = a batch with deletions repairs through parents
+ *             (weights >= 1), 0 = it solves again from the source, -1 (default) = repair
+ *             when the graph's last solve from a source took at least 32 rounds. The
+ *             repair pays on high-diameter graphs (grid 1024^2, 64 deletions: 1.5 ms
+ *             against 8.3 ms for update + solve) and loses where a solve takes a dozen
+ *             rounds (R-MAT 20: 3.4 against 2.2 ms). "sssp.last_marked" (read only):
+ *             vertices the last repair reset (-1: no repair ran).
  *   "sssp.filter"  SSSP: 1 = load dist[u] and send the atomicMin only when the candidate
  *             is lower; 0 = send every atomicMin at once (one L2 round trip less per
  *             hop, more atomics); -1 = default: 0 inside warp cascades, 1 elsewhere.
@@ -410,9 +417,17 @@ int sp_bc_level_trace(sp_graph_h g, float* records, unsigned long long* times, i
  * source before the batch on entry (from sp_sssp or an earlier call) and after it on
  * return. A batch of additions only resumes from those distances with the sources of
  * the added edges queued: distances only drop, and each drop starts at an added edge.
- * A batch with deletions solves again from source. Results are exact either way; the
- * DSL's OnAdd test (dest.dist > src.dist + 1) ignores the edge weight, this does not.
- * Tune key "sssp.last_incremental" (read only) says which path the last call took. */
+ * A batch with deletions on a graph whose weights are all >= 1 repairs through parents
+ * (the decremental pass): every vertex gets a parent among its tight in-edges on the old
+ * graph; a record on a vertex's parent edge (deleted, or lengthened by an added weight)
+ * unmarks its whole parent subtree, whose distances are reset, lowered from unmarked
+ * in-neighbours, and the solve resumes from them and from the sources of the additions;
+ * when the subtrees hold more than a quarter of the vertices it solves again instead.
+ * Other batches with deletions, and additions to edges the graph already holds, solve
+ * again from source. Results are exact on every path; the DSL's OnAdd test
+ * (dest.dist > src.dist + 1) ignores the edge weight, this does not. Tune key
+ * "sssp.last_incremental" (read only): 0 = solved again, 1 = resumed after additions,
+ * 2 = repaired through parents. */
 int sp_sssp_dynamic(sp_graph_h g, int64_t n, const char* type, const int32_t* src, const int32_t* dst,
                     const int32_t* weight, int32_t source, int32_t* dist);
 /* Replaces the generated Batch block of DynPR (DSL dynamicDSLCodes/dynamicBatchPR:

@@ -700,6 +700,14 @@ int sp_tune_set(sp_graph_h g, const char* key, int64_t value) {
       g->sssp_hub_chunk = (int32_t)value;
     return SP_OK;
   }
+  if (!strcmp(key, "sssp.repair")) {
+    if (value < -1 || value > 1) {
+      set_error("sp_tune_set: sssp.repair must be -1, 0 or 1");
+      return SP_ERR_INVALID;
+    }
+    g->sssp_repair = (int32_t)value;
+    return SP_OK;
+  }
   if (!strcmp(key, "sssp.filter")) {
     if (value < -1 || value > 1) {
       set_error("sp_tune_set: sssp.filter must be -1, 0 or 1");
@@ -855,6 +863,14 @@ int sp_tune_get(sp_graph_h g, const char* key, int64_t* value) {
   }
   if (!strcmp(key, "sssp.filter")) {
     *value = g->sssp_filter;
+    return SP_OK;
+  }
+  if (!strcmp(key, "sssp.repair")) {
+    *value = g->sssp_repair;
+    return SP_OK;
+  }
+  if (!strcmp(key, "sssp.last_marked")) {
+    *value = g->sssp_last_marked;
     return SP_OK;
   }
   if (!strcmp(key, "sssp.local")) {

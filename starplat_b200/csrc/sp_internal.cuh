@@ -174,6 +174,10 @@ struct sp_graph {
   int32_t tc_last_incremental = 0;    // 1 if the last sp_tc_dynamic counted only the batch
   int32_t sssp_hub_deg = 0;    // SSSP: vertices above this out-degree go to shared pieces (0 = default)
   int32_t sssp_filter = -1;    // SSSP: 1 = load dist before each atomicMin, 0 = atomicMin only (-1 = default)
+  int32_t sssp_repair = -1;    // sp_sssp_dynamic: 1 = repair batches with deletions through parents, 0 = solve
+                               // again, -1 = repair when the last solve took many rounds
+  int32_t sssp_last_rounds = 0;  // rounds of the last delta-stepping solve from a source
+  int64_t sssp_last_marked = 0;  // vertices the last repair reset (-1: no repair ran)
   int32_t sssp_hub_chunk = 0;  // SSSP: edges per piece (0 = default)
   int32_t sssp_local = -1;     // SSSP: warp cascade budget in 32-edge steps per round (-1 = default, 0 = off)
   int32_t sssp_batch = 0;      // batched SSSP: sources per cooperative launch (0 = default)

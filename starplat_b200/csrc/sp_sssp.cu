@@ -60,6 +60,10 @@ constexpr int SU = 4;                 // 32-edge steps whose loads and atomics a
 // Sources per cooperative launch of the batched form. 16 weighted closeness sources of
 // undirected R-MAT 20: 34.1 ms with 1 per launch, 34.5 with 4 or 8, 36.0 with 16.
 constexpr int BATCH = 4;
+// sp_sssp_dynamic repairs a batch with deletions by default when the graph's last solve
+// took at least this many rounds (grid 1024^2 repairs in 1.5 ms against 8.3 ms for a new
+// solve; R-MAT 20, a dozen rounds, 3.4 against 2.2 ms).
+constexpr int REPAIR_MIN_ROUNDS = 32;
 constexpr unsigned FULL = 0xffffffffu;
 
 struct Ctl {
@@ -828,6 +832,96 @@ __global__ void k_minmax_w(const int32_t* __restrict__ w, int64_t E, int* mn, in
   }
 }
 
+// ---- decremental repair of a batch with deletions (positive weights)
+__global__ void k_fill(int n, int32_t* a, int32_t val) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = val;
+}
+
+// parent[v] = the smallest u with d[u] + w(u, v) == d[v] (a tight in-edge), INT_MAX for
+// none (the source, unreachable vertices). With every weight >= 1, tight edges raise the
+// distance, so the parents form a forest.
+__global__ void k_parents(int V, const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
+                          const int32_t* __restrict__ w, const int32_t* __restrict__ d, int32_t* parent) {
+  const int lane = threadIdx.x & 31;
+  for (int u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < V; u += (gridDim.x * blockDim.x) >> 5) {
+    const int du = d[u];
+    if (du == INT_MAX) continue;
+    for (int j = off[u] + lane; j < off[u + 1]; j += 32) {
+      const int v = adj[j];
+      if ((long long)du + w[j] == (long long)d[v]) atomicMin(parent + v, u);
+    }
+  }
+}
+
+// A record (s, t) of the batch on t's parent edge (deleted, or lengthened by an added
+// weight) leaves t's distance unsupported: t is marked.
+__global__ void k_mark_parent_edges(int n, const int32_t* __restrict__ s, const int32_t* __restrict__ t,
+                                    const int32_t* __restrict__ parent, int V, uint8_t* bad, int* nbad) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int ti = t[i];
+    if (ti >= 0 && ti < V && parent[ti] == s[i] && bad[ti] == 0) {
+      bad[ti] = 1;
+      atomicAdd(nbad, 1);
+    }
+  }
+}
+
+// Ancestor links for pointer jumping: the parent, or the vertex itself at a root.
+__global__ void k_anc_init(int V, const int32_t* __restrict__ parent, int32_t* anc) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x)
+    anc[v] = parent[v] == INT_MAX ? v : parent[v];
+}
+
+// One synchronous pointer-jumping pass (inputs and outputs in separate buffers): after
+// pass k, bad[v] covers v's 2^k nearest ancestors and anc[v] is its 2^k-th ancestor (or
+// its root), so ceil(log2 V) + 1 passes cover every chain. An in-place pass is not
+// enough: a link can jump past an ancestor whose mark is set later in the same pass.
+__global__ void k_jump(int V, const int32_t* __restrict__ anc_in, const uint8_t* __restrict__ bad_in,
+                       int32_t* __restrict__ anc_out, uint8_t* __restrict__ bad_out) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    const int a = anc_in[v];
+    bad_out[v] = bad_in[v] | bad_in[a];
+    anc_out[v] = anc_in[a];
+  }
+}
+
+__global__ void k_reset_marked(int V, const uint8_t* __restrict__ bad, int32_t* dist) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x)
+    if (bad[v]) dist[v] = INT_MAX;
+}
+
+// Edges of the updated graph from unmarked vertices into marked ones lower the marked
+// ends (the unmarked distances are still achievable and are not changed here).
+__global__ void k_push_into_marked(int V, const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
+                                   const int32_t* __restrict__ w, const uint8_t* __restrict__ bad, int32_t* dist) {
+  const int lane = threadIdx.x & 31;
+  for (int y = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; y < V; y += (gridDim.x * blockDim.x) >> 5) {
+    if (bad[y]) continue;
+    const int dy = dist[y];
+    if (dy == INT_MAX) continue;
+    for (int j = off[y] + lane; j < off[y + 1]; j += 32) {
+      const int x = adj[j];
+      if (!bad[x]) continue;
+      const long long nd = (long long)dy + w[j];
+      if (nd < (long long)INT_MAX) atomicMin(dist + x, (int)nd);
+    }
+  }
+}
+
+// The marked vertices that now have a finite distance: the repair's seeds.
+__global__ void k_collect_marked(int V, const uint8_t* __restrict__ bad, const int32_t* __restrict__ dist,
+                                 int32_t* seeds, int* nseeds) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x)
+    if (bad[v] && dist[v] != INT_MAX) seeds[atomicAdd(nseeds, 1)] = v;
+}
+
+__global__ void k_count_marked(int V, const uint8_t* __restrict__ bad, int* count) {
+  int c = 0;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) c += bad[v];
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
+}
+
 }  // namespace ss
 
 struct SsspPlan {
@@ -1026,6 +1120,7 @@ static int sssp_delta(sp_graph* g, const int32_t* w, int32_t src, int32_t* dist_
   ss::Ctl hc;
   SP_TRY(copy_out(&hc, p->ctl.p, sizeof(hc), s));
   if (rounds_out) *rounds_out = hc.rounds;
+  if (nseeds == 0) g->sssp_last_rounds = hc.rounds;  // a solve from the source
   g->sssp_last_relaxed = (int64_t)hc.relaxed;
   g->sssp_last_epochs = hc.epochs;
   p->etrace_n = a.etrace ? std::min(hc.epochs, ETRACE_CAP) : 0;
@@ -1320,6 +1415,45 @@ extern "C" int sp_sssp_dynamic(sp_graph_h g, int64_t n, const char* type, const 
     kept.local_knob = q->sel_local_knob;
     kept.delta = q->sel_delta;
   }
+  // A batch with deletions: the parents of the old distances on the old graph (weights
+  // >= 1 only, so that they form a forest), and the records on parent edges marked,
+  // before the update replaces the graph.
+  const int V = g->V;
+  cudaStream_t s = g->stream;
+  dbuf<int32_t> old_dist, parent, rec;
+  dbuf<uint8_t> bad;  // [2 * V]: pointer jumping's two mark buffers
+  dbuf<int> nbad;
+  bool repair = false;
+  g->sssp_last_marked = -1;
+  // By default the repair runs on graphs whose last solve from a source took at least
+  // REPAIR_MIN_ROUNDS rounds: where a solve takes a dozen rounds (R-MAT 20: 1.3 ms) its
+  // fixed passes over the graph cost more than solving again.
+  const bool want_repair = g->sssp_repair > 0 || (g->sssp_repair < 0 && g->sssp_last_rounds >= ss::REPAIR_MIN_ROUNDS);
+  if (deletes && want_repair) {
+    const int32_t* w0 = nullptr;
+    SP_TRY(sssp_prepare(g, nullptr, &w0));
+    if (g->sssp->w_min >= 1) {
+      repair = true;
+      SP_TRY(old_dist.alloc(V));
+      SP_TRY(parent.alloc(V));
+      SP_TRY(bad.alloc(2 * (size_t)V));
+      SP_TRY(nbad.alloc(3));
+      SP_TRY(rec.alloc(2 * (size_t)std::max<int64_t>(1, n)));
+      SP_CHECK_CUDA(cudaMemcpyAsync(old_dist.p, dist, sizeof(int32_t) * V, cudaMemcpyDefault, s));
+      ss::k_fill<<<num_sms() * 4, 256, 0, s>>>(V, parent.p, INT_MAX);  // no parent yet
+      SP_CHECK_LAUNCH();
+      SP_CHECK_CUDA(cudaMemsetAsync(bad.p, 0, V, s));
+      SP_CHECK_CUDA(cudaMemsetAsync(nbad.p, 0, 3 * sizeof(int), s));
+      SP_CHECK_CUDA(cudaMemcpyAsync(rec.p, src, sizeof(int32_t) * n, cudaMemcpyDefault, s));
+      SP_CHECK_CUDA(cudaMemcpyAsync(rec.p + n, dst, sizeof(int32_t) * n, cudaMemcpyDefault, s));
+      ss::k_parents<<<num_sms() * 8, 256, 0, s>>>(V, g->off.p, g->adj.p, w0, old_dist.p, parent.p);
+      SP_CHECK_LAUNCH();
+      ss::k_mark_parent_edges<<<std::max(1, std::min(num_sms() * 4, (int)((n + 255) / 256))), 256, 0, s>>>(
+          (int)n, rec.p, rec.p + n, parent.p, V, bad.p, nbad.p);
+      SP_CHECK_LAUNCH();
+      g_launches += 3;
+    }
+  }
   int64_t held_adds = 0;
   SP_TRY(update_graph(g, n, type, src, dst, weight, &held_adds));
   g->sssp_last_incremental = 0;
@@ -1339,15 +1473,72 @@ extern "C" int sp_sssp_dynamic(sp_graph_h g, int64_t n, const char* type, const 
   int64_t delta = 0;
   int ctas = 0, local = 0;
   SP_TRY(sssp_schedule(g, delta, ctas, local));
-  // A deletion, or an addition of an edge the graph already held (its weight grows by
-  // the added weight), can raise distances: solve again from the source.
+  if (repair) {
+    // DynSSSP's decremental pass (dynamicBatchSSSP:37-60, repair through parents): a
+    // marked vertex's subtree loses its support, is reset and lowered again from the
+    // unmarked in-neighbours; the solve resumes from those vertices and from the sources
+    // of the added edges. Unmarked distances keep a path of unchanged edges, so they stay
+    // achievable; only additions can lower them, and the sources of the additions are
+    // queued.
+    int nb = 0;
+    SP_TRY(copy_out(&nb, nbad.p, sizeof(int), s));
+    g->sssp_last_marked = 0;
+    SsspPlan* p = g->sssp;
+    SP_TRY(p->dist.alloc(V));
+    SP_CHECK_CUDA(cudaMemcpyAsync(p->dist.p, old_dist.p, sizeof(int32_t) * V, cudaMemcpyDeviceToDevice, s));
+    std::vector<int32_t> add_src(seeds);
+    int nseed = 0;
+    dbuf<int32_t> d_seeds, anc;
+    SP_TRY(d_seeds.alloc((size_t)V + add_src.size() + 1));
+    if (nb > 0) {
+      int passes = 1;
+      while (passes < 32 && (1ll << (passes - 1)) < (long long)V) ++passes;
+      SP_TRY(anc.alloc(2 * (size_t)V));
+      ss::k_anc_init<<<num_sms() * 8, 256, 0, s>>>(V, parent.p, anc.p);
+      SP_CHECK_LAUNCH();
+      int cur = 0;
+      for (int k = 0; k < passes; ++k, cur ^= 1) {
+        ss::k_jump<<<num_sms() * 8, 256, 0, s>>>(V, anc.p + (size_t)cur * V, bad.p + (size_t)cur * V,
+                                                 anc.p + (size_t)(cur ^ 1) * V, bad.p + (size_t)(cur ^ 1) * V);
+        SP_CHECK_LAUNCH();
+      }
+      const uint8_t* marked = bad.p + (size_t)cur * V;
+      // a repair that resets more than a quarter of the vertices costs more than a solve
+      ss::k_count_marked<<<num_sms() * 4, 256, 0, s>>>(V, marked, nbad.p + 2);
+      SP_CHECK_LAUNCH();
+      g_launches += (unsigned long long)passes + 2;
+      int nmarked = 0;
+      SP_TRY(copy_out(&nmarked, nbad.p + 2, sizeof(int), s));
+      g->sssp_last_marked = nmarked;
+      if ((int64_t)nmarked * 4 > (int64_t)V) return sssp_delta(g, w, source, dist, delta, ctas, local, nullptr);
+      ss::k_reset_marked<<<num_sms() * 8, 256, 0, s>>>(V, marked, p->dist.p);
+      SP_CHECK_LAUNCH();
+      ss::k_push_into_marked<<<num_sms() * 8, 256, 0, s>>>(V, g->off.p, g->adj.p, w, marked, p->dist.p);
+      SP_CHECK_LAUNCH();
+      ss::k_collect_marked<<<num_sms() * 8, 256, 0, s>>>(V, marked, p->dist.p, d_seeds.p, nbad.p + 1);
+      SP_CHECK_LAUNCH();
+      g_launches += 3;
+      SP_TRY(copy_out(&nseed, nbad.p + 1, sizeof(int), s));
+    }
+    std::sort(add_src.begin(), add_src.end());
+    add_src.erase(std::unique(add_src.begin(), add_src.end()), add_src.end());
+    if (!add_src.empty())
+      SP_CHECK_CUDA(cudaMemcpyAsync(d_seeds.p + nseed, add_src.data(), sizeof(int32_t) * add_src.size(),
+                                    cudaMemcpyHostToDevice, s));
+    nseed += (int)add_src.size();
+    g->sssp_last_incremental = 2;
+    if (nseed == 0) return copy_out(dist, p->dist.p, sizeof(int32_t) * V, s);
+    return sssp_delta(g, w, source, dist, delta, ctas, local, nullptr, d_seeds.p, nseed);
+  }
+  // A deletion (with a weight below 1 somewhere) or an addition of an edge the graph
+  // already held (its weight grows by the added weight) can raise distances: solve
+  // again from the source.
   if (deletes || held_adds > 0) return sssp_delta(g, w, source, dist, delta, ctas, local, nullptr);
   // additions of new edges only: distances can only drop, and every drop starts at an
   // added edge, so the solve resumes from the old distances with their sources queued
   std::sort(seeds.begin(), seeds.end());
   seeds.erase(std::unique(seeds.begin(), seeds.end()), seeds.end());
   SsspPlan* p = g->sssp;
-  cudaStream_t s = g->stream;
   SP_TRY(p->dist.alloc(g->V));
   SP_CHECK_CUDA(cudaMemcpyAsync(p->dist.p, dist, sizeof(int32_t) * g->V, cudaMemcpyDefault, s));
   dbuf<int32_t> d_seeds;

@@ -125,10 +125,12 @@ class DeviceGraph:
     def sssp_dynamic(self, types, src, dst, weight, source: int, dist):
         """DynSSSP's Batch block: apply the updates, then bring dist (the distances from
         source before the batch, int32[V], host or device) up to date on the new graph.
-        A batch that only adds new edges resumes from dist; a batch with deletions, or
-        one that adds an edge the graph already holds (its weight grows, so distances can
-        rise), solves again. Returns True when the call resumed (incremental) and False
-        when it solved again."""
+        A batch that only adds new edges resumes from dist; a batch with deletions on a
+        graph with all weights >= 1 repairs the subtrees that lost their parent edge and
+        resumes; other batches with deletions, and additions to edges the graph already
+        holds (their weight grows, so distances can rise), solve again. Returns True when
+        the call resumed or repaired (incremental) and False when it solved again;
+        tune_get("sssp.last_incremental") tells 1 (resumed) from 2 (repaired)."""
         _ensure_scheduler()
         n, ptrs, _keep = self._batch(types, src, dst, weight)
         check("sp_sssp_dynamic", lib().sp_sssp_dynamic(self.handle, n, *ptrs, int(source), _ptr(dist)))

@@ -149,9 +149,10 @@ def test_update_edge_cases():
         assert dg.export()["edgeLen"].tolist() == [9, 3, 1]
 
 
-def test_sssp_dynamic_additions_resume_and_deletions_resolve():
+def test_sssp_dynamic_additions_resume_and_deletions_repair():
     # DynSSSP's batch: additions resume from the old distances (and relax far fewer
-    # edges than a fresh solve); a batch with deletions solves again; exact both ways
+    # edges than a fresh solve); a batch with deletions repairs through parents (weights
+    # >= 1 here); exact every way
     rng = np.random.default_rng(4)
     g = G.rmat(14, 8, seed=9, directed=True)
     g.edgeLen = G.hash_weights(g, 9, 1, 100, False)
@@ -171,7 +172,11 @@ def test_sssp_dynamic_additions_resume_and_deletions_resolve():
                 t = "a" * n
             resumed = dg.sssp_dynamic(t, s, d, w, source, dist)
             held = any((int(a), int(b)) in edges for a, b in zip(s, d))
-            assert resumed == ("d" not in t and not held)
+            path = dg.tune_get("sssp.last_incremental")
+            if "d" in t:  # repaired, or solved again when the repair would reset > V / 4
+                assert path in (0, 2) and resumed == (path == 2)
+            else:
+                assert resumed == (not held) and path == (1 if not held else 0)
             edges = _apply(edges, t, s, d, w)
             off, adj, ww = _csr(g.V, edges)
             assert np.array_equal(dist, O.sssp(off, adj, ww, source)), step
@@ -228,6 +233,153 @@ def test_sssp_dynamic_readding_a_held_tree_edge_solves_again():
             edges = _apply(edges, "a", [source], [far], [1])
             off, adj, ww = _csr(g.V, edges)
             assert np.array_equal(dist, O.sssp(off, adj, ww, source))
+
+
+def _tight(off, adj, w, dist):
+    """(u, v) edges with dist[u] + w == dist[v]: the tight edges of the distances."""
+    out = []
+    for u in range(len(off) - 1):
+        if dist[u] == 2**31 - 1:
+            continue
+        for k in range(off[u], off[u + 1]):
+            v = int(adj[k])
+            if int(dist[u]) + int(w[k]) == int(dist[v]):
+                out.append((u, v))
+    return out
+
+
+@pytest.mark.parametrize("case", ["grid", "rmat"])
+def test_sssp_dynamic_decremental_repair_through_parents(case):
+    # deletions of tight (tree) edges reset whole subtrees, which are lowered again from
+    # their unmarked in-neighbours; batches mix deletions of tree edges, other deletions,
+    # lengthened tree edges (additions to held edges) and new edges; exact every batch
+    import torch
+
+    rng = np.random.default_rng(11)
+    if case == "grid":
+        g = G.grid(60, 70)
+        g.edgeLen = G.hash_weights(g, 3, 1, 50, True)
+    else:
+        g = G.rmat(13, 8, seed=3, directed=True)
+        g.edgeLen = G.hash_weights(g, 3, 1, 100, False)
+    source = int(G.pick_sources(g, 1, seed=2)[0])
+    edges = _edges(g.indexofNodes, g.edgeList, g.edgeLen)
+    paths = []
+    with DeviceGraph.from_csr(g) as dg:
+        dg.tune_set("sssp.repair", 1)  # whatever the rounds of the first solve
+        dd = torch.empty(g.V, dtype=torch.int32, device="cuda")
+        dg.sssp(source, out=dd)
+        for step in range(5):
+            off, adj, ww = _csr(g.V, edges)
+            tight = _tight(off, adj, ww, dd.cpu().numpy())
+            pick = rng.choice(len(tight), min(len(tight), [5, 40, 200, 3, 60][step]), replace=False)
+            dels = [tight[i] for i in pick]
+            keys = list(edges)
+            others = [keys[i] for i in rng.choice(len(keys), 20, replace=False)]
+            longer = [tight[i] for i in rng.choice(len(tight), 5, replace=False)]
+            fresh = [(int(a), int(b)) for a, b in rng.integers(0, g.V, (10, 2))]
+            t = "d" * (len(dels) + len(others)) + "a" * (len(longer) + len(fresh))
+            s_ = np.array([a for a, _ in dels + others + longer + fresh], np.int32)
+            d_ = np.array([b for _, b in dels + others + longer + fresh], np.int32)
+            w_ = np.concatenate([np.ones(len(dels) + len(others), np.int32),
+                                 rng.integers(1, 30, len(longer) + len(fresh)).astype(np.int32)])
+            repaired = dg.sssp_dynamic(t, s_, d_, w_, source, dd)
+            paths.append(dg.tune_get("sssp.last_incremental"))
+            assert paths[-1] in (0, 2) and repaired == (paths[-1] == 2)
+            edges = _apply(edges, t, s_, d_, w_)
+            off, adj, ww = _csr(g.V, edges)
+            assert np.array_equal(dd.cpu().numpy(), O.sssp(off, adj, ww, source)), (case, step, paths[-1])
+    assert 2 in paths, paths  # the repair ran (larger resets solve again)
+
+
+def test_sssp_dynamic_repair_edge_cases():
+    # every out-edge of the source deleted (all else unreachable), then re-added; and a
+    # graph with a zero weight, where the parents need not form a forest: solve again
+    g = G.grid(20, 20)
+    g.edgeLen = G.hash_weights(g, 5, 1, 9, True)
+    source = 210
+    edges = _edges(g.indexofNodes, g.edgeList, g.edgeLen)
+    outs = [(source, int(v)) for v in g.edgeList[g.indexofNodes[source]:g.indexofNodes[source + 1]]]
+    with DeviceGraph.from_csr(g) as dg:
+        dist, _ = dg.sssp(source)
+        s_ = np.array([a for a, _ in outs], np.int32)
+        d_ = np.array([b for _, b in outs], np.int32)
+        ones = np.ones(len(outs), np.int32)
+        dg.sssp_dynamic("d" * len(outs), s_, d_, ones, source, dist)  # resets everything: solves again
+        assert dg.tune_get("sssp.last_incremental") == 0
+        assert dist[source] == 0 and np.all(np.delete(dist, source) == 2**31 - 1)
+        edges = _apply(edges, "d" * len(outs), s_, d_, ones)
+        w_ = np.full(len(outs), 4, np.int32)
+        assert dg.sssp_dynamic("a" * len(outs), s_, d_, w_, source, dist)
+        edges = _apply(edges, "a" * len(outs), s_, d_, w_)
+        off, adj, ww = _csr(g.V, edges)
+        assert np.array_equal(dist, O.sssp(off, adj, ww, source))
+    z = G.grid(12, 12)
+    z.edgeLen = G.hash_weights(z, 6, 0, 5, True)
+    assert (z.edgeLen == 0).any()
+    ez = _edges(z.indexofNodes, z.edgeList, z.edgeLen)
+    with DeviceGraph.from_csr(z) as dz:
+        dist, _ = dz.sssp(0)
+        k = list(ez)[:30]
+        s_ = np.array([a for a, _ in k], np.int32)
+        d_ = np.array([b for _, b in k], np.int32)
+        ones = np.ones(len(k), np.int32)
+        assert not dz.sssp_dynamic("d" * len(k), s_, d_, ones, 0, dist)
+        assert dz.tune_get("sssp.last_marked") == -1
+        ez = _apply(ez, "d" * len(k), s_, d_, ones)
+        off, adj, ww = _csr(z.V, ez)
+        assert np.array_equal(dist, O.sssp(off, adj, ww, 0))
+    # the knob: sssp.repair = 0 solves again on a batch with deletions
+    g2 = G.grid(16, 16)
+    g2.edgeLen = G.hash_weights(g2, 8, 1, 9, True)
+    e2 = _edges(g2.indexofNodes, g2.edgeList, g2.edgeLen)
+    with DeviceGraph.from_csr(g2) as d2:
+        dist, _ = d2.sssp(0)
+        d2.tune_set("sssp.repair", 0)
+        k = list(e2)[5:9]
+        s_ = np.array([a for a, _ in k], np.int32)
+        d_ = np.array([b for _, b in k], np.int32)
+        assert not d2.sssp_dynamic("dddd", s_, d_, np.ones(4, np.int32), 0, dist)
+        e2 = _apply(e2, "dddd", s_, d_, np.ones(4, np.int32))
+        off, adj, ww = _csr(g2.V, e2)
+        assert np.array_equal(dist, O.sssp(off, adj, ww, 0))
+        d2.tune_set("sssp.repair", -1)
+        with pytest.raises(_lib.SPError):
+            d2.tune_set("sssp.repair", 2)
+
+
+def test_sssp_dynamic_repair_policy_follows_the_rounds_of_the_last_solve():
+    # by default (sssp.repair = -1) a batch with deletions repairs when the last solve
+    # took at least 32 rounds, and solves again otherwise; exact either way
+    chain = np.array([[i, i + 1] for i in range(399)] + [[i + 1, i] for i in range(399)], np.int32)
+    p = from_pairs(400, chain, name="path400")
+    p.edgeLen = G.hash_weights(p, 2, 1, 9, True)
+    ep = _edges(p.indexofNodes, p.edgeList, p.edgeLen)
+    with DeviceGraph.from_csr(p) as dp:
+        assert dp.tune_get("sssp.repair") == -1
+        dp.tune_set("sssp.delta", 1)  # one distance per bucket: hundreds of rounds
+        dist, rounds = dp.sssp(0)
+        assert rounds >= 32
+        s_, d_ = np.array([300], np.int32), np.array([301], np.int32)
+        assert dp.sssp_dynamic("d", s_, d_, np.ones(1, np.int32), 0, dist)
+        assert dp.tune_get("sssp.last_incremental") == 2 and dp.tune_get("sssp.last_marked") > 0
+        ep = _apply(ep, "d", s_, d_, np.ones(1, np.int32))
+        off, adj, ww = _csr(p.V, ep)
+        assert np.array_equal(dist, O.sssp(off, adj, ww, 0))
+    g = G.rmat(12, 8, seed=7, directed=True)
+    g.edgeLen = G.hash_weights(g, 7, 1, 100, False)
+    eg = _edges(g.indexofNodes, g.edgeList, g.edgeLen)
+    source = int(G.pick_sources(g, 1, seed=7)[0])
+    with DeviceGraph.from_csr(g) as dg:
+        dist, rounds = dg.sssp(source)
+        k = list(eg)[:20]
+        s_ = np.array([a for a, _ in k], np.int32)
+        d_ = np.array([b for _, b in k], np.int32)
+        dg.sssp_dynamic("d" * 20, s_, d_, np.ones(20, np.int32), source, dist)
+        assert dg.tune_get("sssp.last_incremental") == (2 if rounds >= 32 else 0)
+        eg = _apply(eg, "d" * 20, s_, d_, np.ones(20, np.int32))
+        off, adj, ww = _csr(g.V, eg)
+        assert np.array_equal(dist, O.sssp(off, adj, ww, source))
 
 
 def test_update_rejects_weight_sums_outside_int32():
