@@ -45,6 +45,7 @@ constexpr int WARPS = THREADS / 32;
 constexpr int HCAP = 1024;          // hash slots per warp (load factor <= 1/2)
 constexpr int SMAX = HCAP / 2;      // largest S(a) handled by the warp path
 constexpr int EMPTY = -1;
+constexpr int WU = 4;               // k_tc_warp: probe-list elements per lane per pass
 
 __device__ __forceinline__ unsigned hslot(int k) { return ((unsigned)k * 2654435761u) >> 22; }  // 10 bits
 
@@ -156,28 +157,45 @@ __global__ void __launch_bounds__(THREADS) k_tc_warp(Lists L, const int32_t* __r
       s_excl[w][lane] = incl - len;
       if (PV) s_p[w][lane] = p;
       __syncwarp();
-      for (int k = lane; k < tot; k += 32) {
-        // owner: last lane whose exclusive prefix <= k
-        int lo = 0, hi = 31;
-        while (lo < hi) {
-          int m = (lo + hi + 1) >> 1;
-          if (s_excl[w][m] <= k) lo = m; else hi = m - 1;
-        }
-        int x = L.adj[s_lb[w][lo] + (k - s_excl[w][lo])];
-        unsigned s = hslot(x);
-        for (int probe = 0; probe < HCAP; ++probe) {
-          int t = tab[s];
-          if (t == x) {
-            ++cnt;
-            if (PV) {
-              atomicAdd(cf + x, 1);
-              atomicAdd(cf + s_p[w][lo], 1);
-              ++ha;
+      // WU elements per lane per pass: their owners are found and their list entries
+      // loaded before any lookup, so the global loads of a pass overlap
+      for (int k0 = lane; k0 < tot; k0 += 32 * WU) {
+        int xs[WU], own[WU];
+#pragma unroll
+        for (int q = 0; q < WU; ++q) {
+          const int k = k0 + 32 * q;
+          xs[q] = -1;
+          own[q] = 0;
+          if (k < tot) {
+            // owner: last lane whose exclusive prefix <= k
+            int lo = 0, hi = 31;
+            while (lo < hi) {
+              int m = (lo + hi + 1) >> 1;
+              if (s_excl[w][m] <= k) lo = m; else hi = m - 1;
             }
-            break;
+            own[q] = lo;
+            xs[q] = L.adj[s_lb[w][lo] + (k - s_excl[w][lo])];
           }
-          if (t == EMPTY) break;
-          s = (s + 1) & (HCAP - 1);
+        }
+#pragma unroll
+        for (int q = 0; q < WU; ++q) {
+          const int x = xs[q];
+          if (x < 0) continue;
+          unsigned s = hslot(x);
+          for (int probe = 0; probe < HCAP; ++probe) {
+            int t = tab[s];
+            if (t == x) {
+              ++cnt;
+              if (PV) {
+                atomicAdd(cf + x, 1);
+                atomicAdd(cf + s_p[w][own[q]], 1);
+                ++ha;
+              }
+              break;
+            }
+            if (t == EMPTY) break;
+            s = (s + 1) & (HCAP - 1);
+          }
         }
       }
       __syncwarp();
