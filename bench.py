@@ -198,6 +198,34 @@ def tuned(dg):
     return dg
 
 
+def learned_vs_fixed(dg, algo, run, stream, reps=3):
+    """The algorithm's kernel-variant choice: fixed defaults (knob -2) against the trained
+    network (-1), each timed over `reps` calls after one warm-up. A model not marked
+    shipped is loaded for this comparison only."""
+    from starplat_b200 import variants
+
+    path = variants.model_path(algo)
+    if not os.path.exists(path):
+        return {"model": "none"}
+    d = json.load(open(path))
+    key = variants.KNOB[algo] + ".variant"
+    variants.load([algo], shipped_only=False)
+    try:
+        dg.tune_set(key, -2)
+        ms_f, _ = timed(run, reps, 1, stream)
+        dg.tune_set(key, -1)
+        ms_l, _ = timed(run, reps, 1, stream)
+        cand = dg.tune_get(variants.KNOB[algo] + ".last_variant")
+    finally:
+        dg.tune_set(key, -1)
+        if not d.get("shipped", False):
+            variants.unload([algo])
+    lo = d.get("leave_one_graph_out", {})
+    return {"fixed_ms": ms_f, "learned_ms": ms_l, "learned_over_fixed": ms_f / ms_l, "learned_candidate": cand,
+            "shipped": bool(d.get("shipped", False)), "decision": d.get("ship_decision"),
+            "held_out_regret": {"learned": lo.get("learned_regret"), "fixed": lo.get("fixed_regret")}}
+
+
 def bc_error(got, ref):
     """BC against the FP64 oracle: per-vertex bar |got - ref| <= 1e-5 |ref| + 1e-9 max(1, max ref).
     Returns the largest ratio of error to bar (<= 1 passes) and the largest relative
@@ -258,6 +286,8 @@ def bench_tc(steps, warmup, stream, hbm, cpu):
         else:
             ms, res = timed(lambda: dg.tc(), steps, warmup, stream)
         msp, resp = timed(lambda: dg.tc(_lib.SP_TC_PLAIN), max(1, steps // 2), 1, stream)
+        if REP is None or REP.world == 1:
+            out["learned_vs_fixed"] = learned_vs_fixed(dg, "tc", lambda: dg.tc(), stream)
     out.update({"triangles": res[0], "value": m / (ms / 1e3) / 1e9, "unit": "GTEPS", "ms": ms,
                 "plain": {"value": m / (msp / 1e3) / 1e9, "ms": msp, "triangles": resp[0]},
                 "roofline": roof(alg, ms, hbm)})
@@ -417,6 +447,7 @@ def bench_bc(steps, warmup, stream, hbm, cpu, nsrc=256):
                                 "note": "bc.dir -1 = the library default (push at every level, or the level "
                                         "model when a model file is loaded); 1 = per-level push/pull rule on "
                                         "the device"}
+            out["learned_vs_fixed"] = learned_vs_fixed(dg, "bc", lambda: dg.bc(srcs), stream)
         few = srcs[:8]
         msp, _ = timed(lambda: dg.bc(few, variant=_lib.SP_BC_PLAIN), 1, 0, stream)
     out.update({"value": sum_er / (ms / 1e3) / 1e9, "unit": "GTEPS", "ms": ms,
@@ -541,6 +572,9 @@ def bench_louvain(steps, warmup, stream, hbm, cpu):
             return q
 
         ms, _ = timed(run, steps, warmup, stream)
+        out["variant"] = {"last_level_candidate": dg.tune_get("lv.last_variant"),
+                          "note": "-1 = the fixed CTA-bin table; the shipped per-level model loads on first use"}
+        out["learned_vs_fixed"] = learned_vs_fixed(dg, "louvain", lambda: dg.louvain(None, 1e-4), stream)
 
         def run_plain():
             from starplat_b200 import _lib
@@ -1130,6 +1164,11 @@ def main():
         except Exception:
             pass
 
+    # kernel-variant choice of the iteration: fixed defaults against the trained network
+    pr_variants = None
+    if rank == 0 and world == 1:
+        pr_variants = learned_vs_fixed(dg, "pagerank", lambda: dg.pagerank(BETA, DELTA, MAX_ITER, out=out), stream)
+
     # plain (generated-code form) PageRank for comparison
     msp, resp = timed(lambda: dg.pagerank(BETA, DELTA, MAX_ITER, out=out, variant=_lib.SP_PR_PLAIN), 1, 1, stream)
     pr_plain = {"value": E * resp[0][1] / (msp / 1e3) / 1e9, "ms_per_step": msp, "iterations": resp[0][1]}
@@ -1215,7 +1254,7 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": cfg, "iterations": it_total // args.steps, "graph_gen_s": round(gen_s, 2),
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
-                "parity": parity, "plain": pr_plain, "algorithms": extras}
+                "parity": parity, "plain": pr_plain, "learned_vs_fixed": pr_variants, "algorithms": extras}
         if split:
             line["pagerank_split"] = split
         print(json.dumps(line), flush=True)

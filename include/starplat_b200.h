@@ -410,6 +410,43 @@ int sp_sssp_epoch_trace(sp_graph_h g, float* records, unsigned long long* times,
  * times[k] = device timer (ns) at each level start, times[n] at the end of the run.
  * No counterpart in the reference. */
 int sp_bc_level_trace(sp_graph_h g, float* records, unsigned long long* times, int32_t cap, int32_t* n);
+
+/* ---- learned kernel variants ---------------------------------------------------
+ * No counterpart in the reference, whose kernels have one fixed shape each. PageRank,
+ * TC, BC and Louvain each have a table of kernel variants that change only how work is
+ * split or cached (PageRank: gathers that allocate in L1, srcList policy and load width;
+ * TC: the bitmap kernel's CTA width below 65537 vertices, else the hash kernel's
+ * probe-list elements per lane; BC: the degree above which a level-list entry is cut
+ * into shared pieces, and the piece size; Louvain: the shared-memory table size of the
+ * CTA degree bin). A network of the scheduler's shape, loaded per algorithm, predicts
+ * the log run time of every applicable candidate from degree statistics computed on
+ * the device (PageRank, TC, BC: once per graph and model; Louvain: at every level, from
+ * the level graph) and the call runs the lowest. Knob "<a>.variant" (a = pr, tc, bc,
+ * lv): -1 (default) learned when a model is loaded and none of the algorithm's own
+ * variant knobs is set (pr.l1_hot / pr.src_hint / pr.vec, tc.cta_warps / tc.unroll,
+ * bc.hub_deg / bc.hub_chunk, lv.cta_slots), else those knobs and the defaults; -2 the
+ * knobs and defaults even with a model; k >= 0 candidate k (to time the table).
+ * "<a>.last_variant" (read only): the candidate the last call ran (Louvain: its last
+ * level), -1 for knobs and defaults. Counts, distances, levels and path counts are the
+ * same under every candidate; floating-point sums may change grouping. */
+#define SP_VARIANT_PAGERANK 0
+#define SP_VARIANT_TC 1
+#define SP_VARIANT_BC 2
+#define SP_VARIANT_LOUVAIN 3
+/* Load (params != NULL) or unload (params == NULL) algo's variant model. A call leaves
+ * the fixed defaults' candidate only when the best predicted log time is lower than the
+ * defaults' by more than margin (>= 0; log(1.05) = a predicted gain above 5%). */
+int sp_sched_variant_load(int32_t algo, const float* params, const float* feat_mean, const float* feat_scale,
+                          float margin);
+/* *n = the candidates in algo's table. */
+int sp_variant_count(int32_t algo, int32_t* n);
+/* x[SP_MLP_IN] = the inputs of candidate cand on g (BC: for a run of nsrc sources;
+ * Louvain: its first level); *applicable = 0 when the candidate is not one g can run. */
+int sp_variant_features(sp_graph_h g, int32_t algo, int32_t cand, int32_t nsrc, float* x, int32_t* applicable);
+/* With knob "lv.trace" = 1, the last tuned sp_louvain run's levels: records[k][16] = the
+ * SP_MLP_IN inputs of the candidate the level ran, its index, the level's bins, tables
+ * and sweeps in device milliseconds, padding. *n = levels; up to cap records copied. */
+int sp_louvain_level_trace(sp_graph_h g, float* records, int32_t cap, int32_t* n);
 /* Replaces the generated Batch block of DynSSSP (DSL dynamicDSLCodes/dynamicBatchSSSP:
  * OnDelete + updateCSRDel + Decremental, then OnAdd + updateCSRAdd + Incremental): one
  * batch of edge updates as in sp_graph_update, then the distances from source on the

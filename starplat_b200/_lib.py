@@ -36,6 +36,10 @@ SP_LV_PLAIN = 1
 SP_MLP_IN = 13
 SP_MLP_HIDDEN = 32
 SP_MLP_PARAMS = SP_MLP_HIDDEN * SP_MLP_IN + SP_MLP_HIDDEN * SP_MLP_HIDDEN + 3 * SP_MLP_HIDDEN + 1
+SP_VARIANT_PAGERANK = 0
+SP_VARIANT_TC = 1
+SP_VARIANT_BC = 2
+SP_VARIANT_LOUVAIN = 3
 
 _L = None
 
@@ -110,6 +114,10 @@ SIGNATURES = {
     "sp_sssp_epoch_trace": (ctypes.c_int, [vp, vp, vp, i32, P(i32)]),
     "sp_bc_level_trace": (ctypes.c_int, [vp, vp, vp, i32, P(i32)]),
     "sp_sssp_features": (ctypes.c_int, [vp, vp, f64, i32, i32, vp]),
+    "sp_sched_variant_load": (ctypes.c_int, [i32, vp, vp, vp, f32]),
+    "sp_variant_count": (ctypes.c_int, [i32, P(i32)]),
+    "sp_variant_features": (ctypes.c_int, [vp, i32, i32, i32, vp, P(i32)]),
+    "sp_louvain_level_trace": (ctypes.c_int, [vp, vp, i32, P(i32)]),
     "sp_pagerank_noalloc": (ctypes.c_int, [vp, vp, vp, i32, i64, f32, f32, i32, vp, P(i32), vp]),
 }
 

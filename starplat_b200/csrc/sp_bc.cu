@@ -969,6 +969,11 @@ struct BcPlan {
   dbuf<int32_t> flv, lo, cnt, srcs, level, aux;
   dbuf<GridBar> bar;
   dbuf<int> err;
+  // learned variant inputs (vstat < 0: not yet) and the choice for var_nsrc sources
+  int vstat = -1;
+  int64_t vmax = 0, vsq = 0, vrows[4] = {}, vedges[4] = {};
+  int var_choice = -1, var_nsrc = 0;
+  unsigned var_gen = 0;
 };
 
 int bc_hub_deg_default() { return bc::HUB_DEG; }
@@ -976,6 +981,92 @@ int bc_cluster_default() { return bc::CLUSTER_DEFAULT; }
 int bc_hub_chunk_default() { return bc::HUB_CHUNK; }
 
 void free_bc_plan(BcPlan* p) { delete p; }
+
+// ---- learned kernel variant -------------------------------------------------------
+// The degree above which a level-list entry is cut into pieces that all warps share, and
+// the piece size. Entry 3 is the fixed default (64, 64).
+namespace bc {
+struct Variant {
+  int hub_deg, hub_chunk;
+};
+constexpr int VHUB[4] = {32, 64, 256, 4096};
+constexpr Variant VARIANTS[] = {{32, 64},   {32, 128},  {32, 256},  {64, 64},    {64, 128},   {64, 256},
+                                {256, 64},  {256, 128}, {256, 256}, {4096, 64}, {4096, 128}, {4096, 256}};
+constexpr int N_VARIANTS = (int)(sizeof(VARIANTS) / sizeof(VARIANTS[0]));
+constexpr int DEFAULT_VARIANT = 3;
+}  // namespace bc
+
+int bc_variant_count() { return bc::N_VARIANTS; }
+
+// Inputs: graph shape, symmetry, the batch's source count, the share of entries in rows
+// above 4096, then the candidate: its threshold and piece size, the share of entries and
+// the rows that the threshold splits.
+int bc_variant_features(sp_graph* g, int cand, int nsrc, float* x, int* applicable) {
+  if (cand < 0 || cand >= bc::N_VARIANTS) return SP_ERR_INVALID;
+  if (!g->bc) g->bc = new BcPlan();
+  BcPlan* p = g->bc;
+  if (p->vstat < 0) {
+    SP_TRY(ensure_symmetry(g));
+    DegStats ds;
+    SP_TRY(degree_stats(g->off.p, g->V, bc::VHUB, 4, g->stream, &ds));
+    p->vmax = ds.max_deg;
+    p->vsq = ds.sum_sq;
+    for (int i = 0; i < 4; ++i) {
+      p->vrows[i] = ds.rows_above[i];
+      p->vedges[i] = ds.edges_above[i];
+    }
+    p->vstat = 1;
+  }
+  const bc::Variant& c = bc::VARIANTS[cand];
+  int t = 0;
+  while (bc::VHUB[t] != c.hub_deg) ++t;
+  const double V = g->V, E = std::max<double>(1.0, (double)g->E), avg = E / std::max(1.0, V);
+  x[0] = (float)std::log2(std::max(1.0, V));
+  x[1] = (float)std::log2(E + 1.0);
+  x[2] = (float)avg;
+  x[3] = (float)std::log2((double)p->vmax + 1.0);
+  x[4] = (float)std::log2((double)p->vsq / E + 1.0);
+  x[5] = (float)(g->symmetric > 0);
+  x[6] = (float)std::log2((double)std::max(1, nsrc));
+  x[7] = (float)((double)p->vedges[3] / E);
+  x[8] = (float)std::log2((double)c.hub_deg);
+  x[9] = (float)std::log2((double)c.hub_chunk);
+  x[10] = (float)((double)p->vedges[t] / E);
+  x[11] = (float)std::log2((double)p->vrows[t] + 1.0);
+  x[12] = (float)std::log2((double)c.hub_deg / c.hub_chunk);
+  *applicable = 1;
+  return SP_OK;
+}
+
+static int bc_variant_pick(sp_graph* g, int nsrc, int* cand) {
+  *cand = -1;
+  const int mode = g->variant[VAR_BC];
+  if (mode >= 0) {
+    *cand = mode;
+    return SP_OK;
+  }
+  if (mode != -1 || g->bc_hub_deg > 0 || g->bc_hub_chunk > 0) return SP_OK;
+  const unsigned gen = variant_generation(VAR_BC);
+  if (!gen) return SP_OK;
+  BcPlan* p = g->bc;
+  if (p->var_gen == gen && p->var_nsrc == nsrc && p->var_choice >= 0) {
+    *cand = p->var_choice;
+    return SP_OK;
+  }
+  std::vector<float> X((size_t)bc::N_VARIANTS * SP_MLP_IN);
+  std::vector<int> ok(bc::N_VARIANTS);
+  for (int k = 0; k < bc::N_VARIANTS; ++k)
+    SP_TRY(bc_variant_features(g, k, nsrc, X.data() + (size_t)k * SP_MLP_IN, &ok[k]));
+  int best = -1;
+  const int st = variant_choose(VAR_BC, X, ok, bc::DEFAULT_VARIANT, g->stream, &best);
+  if (st == SP_ERR_UNSUPPORTED) return SP_OK;
+  SP_TRY(st);
+  p->var_choice = best;
+  p->var_gen = gen;
+  p->var_nsrc = nsrc;
+  *cand = best;
+  return SP_OK;
+}
 
 static int bc_grid(sp_graph* g, const int32_t* d_srcs, int nsrc, int batch_hint, int32_t* lvl_out = nullptr,
                    double* sig_out = nullptr) {
@@ -1038,6 +1129,15 @@ static int bc_grid(sp_graph* g, const int32_t* d_srcs, int nsrc, int batch_hint,
   W.hub_cap = hub_cap;
   W.hub_deg = g->bc_hub_deg > 0 ? g->bc_hub_deg : bc::HUB_DEG;
   W.hub_chunk = g->bc_hub_chunk > 0 ? g->bc_hub_chunk : bc::HUB_CHUNK;
+  {
+    int cand = -1;
+    SP_TRY(bc_variant_pick(g, nsrc, &cand));
+    if (cand >= 0) {
+      W.hub_deg = bc::VARIANTS[cand].hub_deg;
+      W.hub_chunk = bc::VARIANTS[cand].hub_chunk;
+    }
+    g->last_variant[VAR_BC] = cand;
+  }
   W.dacc = p->dacc.p;
   // forward direction per level
   std::vector<float> packed;

@@ -764,6 +764,44 @@ int sp_tune_set(sp_graph_h g, const char* key, int64_t value) {
     g->bc_batch = (int32_t)value;
     return SP_OK;
   }
+  if (!strcmp(key, "tc.unroll")) {
+    if (value != 1 && value != 2 && value != 4) {
+      set_error("sp_tune_set: tc.unroll must be 1, 2 or 4");
+      return SP_ERR_INVALID;
+    }
+    g->tc_unroll = (int32_t)value;
+    return SP_OK;
+  }
+  if (!strcmp(key, "lv.cta_slots")) {
+    if (value != 1024 && value != 2048 && value != 4096 && value != 8192 && value != 16384) {
+      set_error("sp_tune_set: lv.cta_slots must be 1024, 2048, 4096, 8192 or 16384");
+      return SP_ERR_INVALID;
+    }
+    g->lv_cta_slots = (int32_t)value;
+    return SP_OK;
+  }
+  if (!strcmp(key, "lv.trace")) {
+    if (value != 0 && value != 1) {
+      set_error("sp_tune_set: lv.trace must be 0 or 1");
+      return SP_ERR_INVALID;
+    }
+    g->lv_trace = (int32_t)value;
+    return SP_OK;
+  }
+  {
+    static const char* const vkeys[VAR_ALGOS] = {"pr.variant", "tc.variant", "bc.variant", "lv.variant"};
+    for (int a = 0; a < VAR_ALGOS; ++a)
+      if (!strcmp(key, vkeys[a])) {
+        int32_t n = 0;
+        sp_variant_count(a, &n);
+        if (value < -2 || value >= n) {
+          set_error("sp_tune_set: %s must be -2 (defaults), -1 (learned) or a candidate in [0, %d)", key, n);
+          return SP_ERR_INVALID;
+        }
+        g->variant[a] = (int32_t)value;
+        return SP_OK;
+      }
+  }
   set_error("sp_tune_set: unknown key '%s'", key);
   return SP_ERR_INVALID;
 }
@@ -896,6 +934,32 @@ int sp_tune_get(sp_graph_h g, const char* key, int64_t* value) {
   if (!strcmp(key, "bc.batch")) {
     *value = g->bc_batch > 0 ? g->bc_batch : 64;
     return SP_OK;
+  }
+  if (!strcmp(key, "tc.unroll")) {
+    *value = g->tc_unroll > 0 ? g->tc_unroll : 4;
+    return SP_OK;
+  }
+  if (!strcmp(key, "lv.cta_slots")) {
+    *value = g->lv_cta_slots > 0 ? g->lv_cta_slots : 16384;
+    return SP_OK;
+  }
+  if (!strcmp(key, "lv.trace")) {
+    *value = g->lv_trace;
+    return SP_OK;
+  }
+  {
+    static const char* const vkeys[VAR_ALGOS] = {"pr.", "tc.", "bc.", "lv."};
+    for (int a = 0; a < VAR_ALGOS; ++a)
+      if (!strncmp(key, vkeys[a], 3)) {
+        if (!strcmp(key + 3, "variant")) {
+          *value = g->variant[a];
+          return SP_OK;
+        }
+        if (!strcmp(key + 3, "last_variant")) {
+          *value = g->last_variant[a];
+          return SP_OK;
+        }
+      }
   }
   set_error("sp_tune_get: unknown key '%s'", key);
   return SP_ERR_INVALID;

@@ -197,6 +197,14 @@ struct sp_graph {
   int32_t bc_hub_deg = 0;  // BC: split level-list entries above this degree (0 = default)
   int32_t bc_hub_chunk = 0;  // BC: edges per piece of a split entry (0 = default)
   int32_t bc_cluster = 0;    // BC many-graphs form: CTAs per graph (0 = default)    // BC sources per multi-source batch (0 = 64)
+  int32_t tc_unroll = -1;    // TC hash path: probe-list elements per lane per pass (-1 = default)
+  int32_t lv_cta_slots = -1;  // Louvain: shared table slots of the CTA bin (-1 = default)
+  int32_t lv_trace = 0;       // 1: record the per-level trace of sp_louvain
+  // learned kernel variants, per algorithm (pr, tc, bc, lv): -1 learned when a variant
+  // model is loaded and no variant knob is set, -2 the defaults, k >= 0 candidate k
+  int32_t variant[4] = {-1, -1, -1, -1};
+  int32_t last_variant[4] = {-1, -1, -1, -1};  // candidate the last call ran (-1 = knobs/defaults)
+  std::vector<float> lv_trace_rec;  // per level: SP_MLP_IN inputs, candidate, ms, pad (16 floats)
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   sp::PrPlan* pr = nullptr;
@@ -239,6 +247,41 @@ int sssp_weights_for(sp_graph* g, const int32_t* weight, const int32_t** w);
 int sssp_width_for(sp_graph* g, int64_t& delta);
 int sssp_weight_min(sp_graph* g);
 int num_sms();
+
+// Degree statistics of a CSR (off[n+1], device), on the device: the largest row, the
+// sum of squared row lengths, and for each threshold t[i] the rows longer than t[i] and
+// the entries in those rows.
+constexpr int DEG_THR_MAX = 6;
+struct DegStats {
+  int64_t max_deg = 0, sum_sq = 0;
+  int64_t rows_above[DEG_THR_MAX] = {}, edges_above[DEG_THR_MAX] = {};
+};
+int degree_stats(const int32_t* off, int n, const int* thr, int nthr, cudaStream_t s, DegStats* out);
+// The same statistics left on the device: acc[0] = largest row, acc[1] = sum of squares,
+// acc[2 + 2i] / acc[3 + 2i] = rows above thr[i] / their entries (acc: 2 + 2 * DEG_THR_MAX).
+int degree_stats_launch(const int32_t* off, int n, const int* thr, int nthr, unsigned long long* acc,
+                        cudaStream_t s);
+
+// Learned kernel variants (sp_mlp.cu). Algorithms index sp_graph::variant.
+enum { VAR_PR = 0, VAR_TC = 1, VAR_BC = 2, VAR_LV = 3, VAR_ALGOS = 4 };
+unsigned variant_generation(int algo);  // 0 = no model loaded for algo
+// algo's model packed for the device (params, feature mean, scale, margin) and its
+// generation (0 = none loaded, packed empty)
+unsigned variant_model(int algo, std::vector<float>& packed);
+// Score the rows X[k][SP_MLP_IN] with algo's model on the device; *best = the row with
+// the lowest predicted log time among those with ok[k] != 0, or dflt (the fixed
+// defaults' row, -1 for none) unless the best beats it by more than the model's margin.
+int variant_choose(int algo, const std::vector<float>& X, const std::vector<int>& ok, int dflt, cudaStream_t s,
+                   int* best);
+// Per-algorithm variant tables and their inputs (in the algorithms' files).
+int pr_variant_count();
+int pr_variant_features(sp_graph* g, int cand, float* x, int* applicable);
+int tc_variant_count();
+int tc_variant_features(sp_graph* g, int cand, float* x, int* applicable);
+int bc_variant_count();
+int bc_variant_features(sp_graph* g, int cand, int nsrc, float* x, int* applicable);
+int lv_variant_count();
+int lv_variant_features(sp_graph* g, int cand, float* x, int* applicable);
 }  // namespace sp
 
 // ----------------------------------------------------------------- device helpers

@@ -20,9 +20,10 @@
 //    smaller) keep neighbours from swapping back and forth;
 //  * per-vertex neighbour-community weights by degree bin: up to 64 edges, one warp
 //    with no table (lanes holding one community found by __match_any_sync and summed
-//    by shuffles); up to 8192, one CTA with a hash table of up to 16384 slots in
-//    dynamic shared memory; above that, one CTA with a table in global scratch; FP64
-//    values, shared-memory atomics in the tables;
+//    by shuffles); up to slots / 2, one CTA with a hash table of up to `slots` entries
+//    in dynamic shared memory (16384 by default; per level, the learned variant may
+//    take 1024, 2048 or 4096, which fit more CTAs per SM); above that, one CTA with a
+//    table in global scratch; FP64 values, shared-memory atomics in the tables;
 //  * vertices binned by degree class and by sub-sweep parity, so a sub-sweep's
 //    kernels read only the vertices that may move in it;
 //  * tot_c with FP64 atomics aggregated per warp over lanes of one community (exact
@@ -34,10 +35,12 @@
 //    order (so the next level's weights do not depend on scheduling).
 
 #include <climits>
+#include <cstring>
 #include <cmath>
 #include <vector>
 
 #include "sp_internal.cuh"
+#include "sp_mlp_dev.cuh"
 #include "sp_prims.cuh"
 
 namespace sp {
@@ -45,7 +48,6 @@ namespace sp {
 namespace lv {
 constexpr int THREADS = 256;
 constexpr int WARP_DEG = 64;
-constexpr int CTA_DEG = 8192;
 constexpr int CTA_SLOTS_MAX = 16384;
 constexpr int EMPTY = -1;
 
@@ -513,10 +515,13 @@ __global__ void k_f2d(const float* __restrict__ a, double* b, int64_t n) {
 
 // Vertex lists per (degree class, sub-sweep parity): list 2 * b + parity, b = 0 warp,
 // 1 CTA, 2 CTA with a global table; each list holds at most cap entries.
-__global__ void k_bins(int n, const int32_t* __restrict__ off, int32_t* lists, int* counts, int cap) {
+// cta_deg: the CTA bin's bound, or sel[0] / 2 when the level's variant was chosen on the device
+__global__ void k_bins(int n, const int32_t* __restrict__ off, int32_t* lists, int* counts, int cap, int cta_deg,
+                       const int* __restrict__ sel) {
+  if (sel) cta_deg = sel[0] / 2;
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
     const int d = off[v + 1] - off[v];
-    const int b = d <= WARP_DEG ? 0 : (d <= CTA_DEG ? 1 : 2);
+    const int b = d <= WARP_DEG ? 0 : (d <= cta_deg ? 1 : 2);
     const int k = 2 * b + (int)(hmix((unsigned)v) & 1u);
     const int p = atomicAdd(&counts[k], 1);
     lists[(size_t)k * cap + p] = v;
@@ -534,7 +539,10 @@ struct LvPlan {
   dbuf<unsigned long long> keys, skeys;
   dbuf<double> vals, svals;
   dbuf<int32_t> head, ridx, rstart, scr;
-  dbuf<int> icnt;
+  dbuf<int> icnt;  // [0, 6) bin sizes, [6] moves applied, [8 ..) the level's variant (lv::SEL)
+  dbuf<unsigned long long> vacc;  // the level's degree statistics
+  dbuf<float> vmodel;             // the variant model on the device, generation vmodel_gen
+  unsigned vmodel_gen = 0;
   dbuf<double> gval;
   dbuf<int32_t> gkey;
   dbuf<int64_t> goff;
@@ -582,7 +590,7 @@ static int lv_recount(LvPlan* p, int n, cudaStream_t s) {
 // = entries of list (b, parity); the global tables of parity 1's big list follow
 // parity 0's in gtab_off.
 static int lv_subsweep(LvPlan* p, lv::MoveArgs a, const int counts[6], int cap, int parity, bool plain,
-                       cudaStream_t s) {
+                       int slots, cudaStream_t s) {
   a.parity = parity;
   if (plain) {
     const int tb = 512;  // the generated code's launch shape (backend_cuda/dsl_cpp_generator.cpp:56-77)
@@ -601,10 +609,13 @@ static int lv_subsweep(LvPlan* p, lv::MoveArgs a, const int counts[6], int cap, 
   if (counts[2 + parity]) {
     a.list = list(1);
     a.nlist = counts[2 + parity];
-    const int slots = lv::CTA_SLOTS_MAX;  // degree <= 8192 fits at load factor <= 1/2
+    // degree <= slots / 2 fits at load factor <= 1/2; smaller tables fit more CTAs per SM
     const size_t dyn = (size_t)slots * (sizeof(double) + sizeof(int32_t));
-    SP_CHECK_CUDA(cudaFuncSetAttribute(lv::k_move_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-    lv::k_move_cta<false><<<num_sms(), lv::THREADS, dyn, s>>>(a, slots);
+    SP_CHECK_CUDA(cudaFuncSetAttribute(lv::k_move_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(lv::CTA_SLOTS_MAX * (sizeof(double) + sizeof(int32_t)))));
+    int per_sm = 1;
+    SP_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lv::k_move_cta<false>, lv::THREADS, dyn));
+    lv::k_move_cta<false><<<num_sms() * std::max(1, per_sm), lv::THREADS, dyn, s>>>(a, slots);
     SP_CHECK_LAUNCH();
   }
   if (counts[4 + parity]) {
@@ -614,6 +625,94 @@ static int lv_subsweep(LvPlan* p, lv::MoveArgs a, const int counts[6], int cap, 
     lv::k_move_cta<true><<<num_sms() * 2, lv::THREADS, 0, s>>>(a, 0);
     SP_CHECK_LAUNCH();
   }
+  return SP_OK;
+}
+
+// ---- learned kernel variant, per level ---------------------------------------------
+// The shared-memory table of the CTA bin: vertices above WARP_DEG and up to slots / 2
+// edges get a CTA with a table of slots entries in shared memory (smaller tables fit more
+// CTAs per SM); longer rows use tables in global memory. The last entry is the fixed
+// default. The choice is made on the device: the level's degree statistics, the inputs
+// of every candidate and the network's scores never leave it, and the degree bins read
+// the chosen bound there.
+namespace lv {
+constexpr int VSLOTS[] = {1024, 2048, 4096, 8192, CTA_SLOTS_MAX};
+constexpr int N_VARIANTS = (int)(sizeof(VSLOTS) / sizeof(VSLOTS[0]));
+constexpr int DEFAULT_VARIANT = N_VARIANTS - 1;
+// degree thresholds of the level statistics: WARP_DEG, then slots / 2 of each candidate
+constexpr int VTHR[6] = {WARP_DEG, 512, 1024, 2048, 4096, CTA_SLOTS_MAX / 2};
+static_assert(N_VARIANTS + 1 == 6, "one threshold per candidate after WARP_DEG");
+constexpr int SEL = 8;  // icnt[SEL]: chosen slots, [SEL + 1] candidate, [SEL + 2 ..] its inputs (float bits)
+
+__host__ __device__ inline int vslots(int cand) { return 1024 << cand; }  // = VSLOTS[cand]
+
+// Inputs of candidate cand on a level graph of n vertices and m entries, from its degree
+// statistics acc (thresholds VTHR, layout of degree_stats_launch): the level's shape, the
+// level index, the share of entries and the rows above WARP_DEG, then the candidate's
+// table size, the entries in its shared-table and global-table bins, and the rows of each.
+__host__ __device__ inline void level_features(int n, double m, int level, const unsigned long long* acc, int cand,
+                                               float* x) {
+  const int t = cand + 1;  // VTHR[t] = slots / 2
+  const double N = n > 1 ? (double)n : 1.0, M = m > 1.0 ? m : 1.0;
+  const double r0 = (double)acc[2], e0 = (double)acc[3], rt = (double)acc[2 + 2 * t], et = (double)acc[3 + 2 * t];
+  x[0] = (float)log2(N);
+  x[1] = (float)log2(M + 1.0);
+  x[2] = (float)(M / N);
+  x[3] = (float)log2((double)acc[0] + 1.0);
+  x[4] = (float)log2((double)acc[1] / M + 1.0);
+  x[5] = (float)level;
+  x[6] = (float)(e0 / M);
+  x[7] = (float)log2(r0 + 1.0);
+  x[8] = (float)log2((double)vslots(cand));
+  x[9] = (float)((e0 - et) / M);
+  x[10] = (float)(et / M);
+  x[11] = (float)log2(rt + 1.0);
+  x[12] = (float)log2((r0 - rt) + 1.0);
+}
+
+// One CTA of N_VARIANTS * 32 threads: the inputs of every candidate, then the candidate
+// (forced >= 0; else the network's lowest score with the margin rule toward dflt when a
+// model is given; else dflt), its slots and its inputs into sel.
+__global__ void __launch_bounds__(N_VARIANTS * 32) k_choose(const unsigned long long* __restrict__ acc,
+                                                            const int32_t* __restrict__ off, int n, int level,
+                                                            const float* __restrict__ model, int forced, int dflt,
+                                                            int* sel) {
+  __shared__ float rows[N_VARIANTS][SP_MLP_IN];
+  __shared__ float raw[N_VARIANTS][SP_MLP_IN];
+  const int t = threadIdx.x;
+  if (t < N_VARIANTS) {
+    level_features(n, (double)off[n], level, acc, t, raw[t]);
+    for (int i = 0; i < SP_MLP_IN; ++i) rows[t][i] = raw[t][i];
+  }
+  int cand = forced >= 0 ? forced : dflt;
+  if (model && forced < 0) {
+    cand = mlp_argmin<N_VARIANTS>(model, rows, 0, dflt, model[SP_MLP_PARAMS + 2 * SP_MLP_IN]);
+  } else {
+    __syncthreads();
+  }
+  if (t == 0) {
+    sel[0] = vslots(cand);
+    sel[1] = cand;
+  }
+  if (t < SP_MLP_IN) sel[2 + t] = __float_as_int(raw[cand][t]);
+}
+}  // namespace lv
+
+int lv_variant_count() { return lv::N_VARIANTS; }
+
+int lv_variant_features(sp_graph* g, int cand, float* x, int* applicable) {
+  if (cand < 0 || cand >= lv::N_VARIANTS) return SP_ERR_INVALID;
+  DegStats ds;
+  SP_TRY(degree_stats(g->off.p, g->V, lv::VTHR, 6, g->stream, &ds));
+  unsigned long long acc[2 + 2 * DEG_THR_MAX] = {};
+  acc[0] = (unsigned long long)ds.max_deg;
+  acc[1] = (unsigned long long)ds.sum_sq;
+  for (int i = 0; i < 6; ++i) {
+    acc[2 + 2 * i] = (unsigned long long)ds.rows_above[i];
+    acc[3 + 2 * i] = (unsigned long long)ds.edges_above[i];
+  }
+  lv::level_features(g->V, (double)g->E, 0, acc, cand, x);
+  *applicable = 1;
   return SP_OK;
 }
 
@@ -633,6 +732,7 @@ extern "C" int sp_louvain(sp_graph_h g, const float* weight, double threshold, i
     return SP_ERR_INVALID;
   }
   const bool plain = variant == SP_LV_PLAIN;
+  if (!plain) g->lv_trace_rec.clear();
   if (!g->lv) g->lv = new LvPlan();
   LvPlan* p = g->lv;
   cudaStream_t s = g->stream;
@@ -669,7 +769,7 @@ extern "C" int sp_louvain(sp_graph_h g, const float* weight, double threshold, i
   SP_TRY(p->kv.alloc(n0));
   SP_TRY(p->tot.alloc(n0));
   SP_TRY(p->scal.alloc(2));
-  SP_TRY(p->icnt.alloc(8));
+  SP_TRY(p->icnt.alloc(32));
   lv::k_init_comm<<<gs, 256, 0, s>>>(n0, p->orig.p, p->newcomm.p);  // orig[v] = v
   SP_CHECK_LAUNCH();
 
@@ -710,12 +810,50 @@ extern "C" int sp_louvain(sp_graph_h g, const float* weight, double threshold, i
     SP_TRY(lv_modularity(p, L, W, s, &qlev0));
     if (first) qcur = qlev0;
     first = false;
-    // degree bins
+    // kernel variant of this level, chosen on the device (forced, learned, or the
+    // defaults' inputs for the trace), then the degree bins
+    const int mode = g->variant[VAR_LV];
+    const int fixed_slots = g->lv_cta_slots > 0 ? g->lv_cta_slots : lv::CTA_SLOTS_MAX;
+    unsigned gen = 0;
+    if (!plain && mode == -1 && g->lv_cta_slots < 0) {
+      std::vector<float> packed;
+      gen = variant_model(VAR_LV, packed);
+      if (gen && p->vmodel_gen != gen) {
+        SP_TRY(p->vmodel.alloc(packed.size()));
+        SP_CHECK_CUDA(cudaMemcpyAsync(p->vmodel.p, packed.data(), sizeof(float) * packed.size(),
+                                      cudaMemcpyHostToDevice, s));
+        p->vmodel_gen = gen;
+      }
+    }
+    const bool dev_sel = !plain && (mode >= 0 || gen || g->lv_trace);
+    // trace: the level's choice, bins, tables and sweeps on the device clock
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    if (g->lv_trace && !plain) {
+      SP_CHECK_CUDA(cudaEventCreate(&ev0));
+      SP_CHECK_CUDA(cudaEventCreate(&ev1));
+      SP_CHECK_CUDA(cudaEventRecord(ev0, s));
+    }
+    int* sel = p->icnt.p + lv::SEL;
+    if (dev_sel) {
+      int dflt = lv::DEFAULT_VARIANT;
+      for (int k = 0; k < lv::N_VARIANTS; ++k)
+        if (lv::VSLOTS[k] == fixed_slots) dflt = k;
+      SP_TRY(p->vacc.alloc(2 + 2 * DEG_THR_MAX));
+      SP_TRY(degree_stats_launch(L.off, n, lv::VTHR, 6, p->vacc.p, s));
+      lv::k_choose<<<1, lv::N_VARIANTS * 32, 0, s>>>(p->vacc.p, L.off, n, levels, gen ? p->vmodel.p : nullptr,
+                                                      mode >= 0 ? mode : -1, dflt, sel);
+      SP_CHECK_LAUNCH();
+    }
     SP_CHECK_CUDA(cudaMemsetAsync(p->icnt.p, 0, sizeof(int) * 6, s));
-    lv::k_bins<<<gs, 256, 0, s>>>(n, L.off, p->lists.p, p->icnt.p, n0);
+    lv::k_bins<<<gs, 256, 0, s>>>(n, L.off, p->lists.p, p->icnt.p, n0, fixed_slots / 2, dev_sel ? sel : nullptr);
     SP_CHECK_LAUNCH();
+    int hsel[lv::SEL + 2 + SP_MLP_IN];
+    SP_TRY(copy_out(hsel, p->icnt.p, sizeof(int) * (dev_sel ? lv::SEL + 2 + SP_MLP_IN : 6), s));
     int counts[6];
-    SP_TRY(copy_out(counts, p->icnt.p, sizeof(int) * 6, s));
+    for (int k = 0; k < 6; ++k) counts[k] = hsel[k];
+    const int slots = dev_sel ? hsel[lv::SEL] : fixed_slots;
+    const int lcand = dev_sel && (mode >= 0 || gen) ? hsel[lv::SEL + 1] : -1;
+    g->last_variant[VAR_LV] = lcand;
     const int nbig = counts[4] + counts[5];
     if (nbig && !plain) {
       // global tables for the highest-degree vertices (both parities' lists, in that
@@ -751,7 +889,7 @@ extern "C" int sp_louvain(sp_graph_h g, const float* weight, double threshold, i
     double qold = qlev0, qnew = qlev0;
     for (int sweep = 0; sweep < max_sweeps; ++sweep) {
       for (int parity = 0; parity < 2; ++parity) {
-        SP_TRY(lv_subsweep(p, a, counts, n0, parity, plain, s));
+        SP_TRY(lv_subsweep(p, a, counts, n0, parity, plain, slots, s));
         SP_CHECK_CUDA(cudaMemsetAsync(p->icnt.p + 6, 0, sizeof(int), s));
         lv::k_apply<<<gs, 256, 0, s>>>(n, parity, p->comm.p, p->newcomm.p, p->icnt.p + 6);
         SP_CHECK_LAUNCH();
@@ -761,6 +899,23 @@ extern "C" int sp_louvain(sp_graph_h g, const float* weight, double threshold, i
       ++total_sweeps;
       SP_TRY(lv_modularity(p, L, W, s, &qnew));
       if (!(qnew - qold > threshold)) break;
+    }
+    if (ev0) {
+      // trace record: the inputs of the variant that ran, its index, the level's sweep
+      // loop in device milliseconds
+      float ms = 0;
+      SP_CHECK_CUDA(cudaEventRecord(ev1, s));
+      SP_CHECK_CUDA(cudaEventSynchronize(ev1));
+      SP_CHECK_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+      cudaEventDestroy(ev0);
+      cudaEventDestroy(ev1);
+      std::vector<float>& tr = g->lv_trace_rec;
+      float lx[SP_MLP_IN];
+      memcpy(lx, hsel + lv::SEL + 2, sizeof(lx));
+      tr.insert(tr.end(), lx, lx + SP_MLP_IN);
+      tr.push_back((float)hsel[lv::SEL + 1]);
+      tr.push_back(ms);
+      tr.push_back(0.0f);
     }
     ++levels;
     // renumber communities
@@ -830,5 +985,17 @@ extern "C" int sp_louvain(sp_graph_h g, const float* weight, double threshold, i
   if (levels_out) *levels_out = levels;
   if (sweeps_out) *sweeps_out = total_sweeps;
   if (community) SP_TRY(copy_out(community, p->orig.p, sizeof(int32_t) * n0, s));
+  return SP_OK;
+}
+
+extern "C" int sp_louvain_level_trace(sp_graph_h g, float* records, int32_t cap, int32_t* n) {
+  if (!g || !n || cap < 0 || (cap > 0 && !records)) {
+    set_error("sp_louvain_level_trace: invalid argument");
+    return SP_ERR_INVALID;
+  }
+  const int k = (int)(g->lv_trace_rec.size() / 16);
+  *n = k;
+  const int c = std::min(k, (int)cap);
+  if (c) memcpy(records, g->lv_trace_rec.data(), sizeof(float) * 16 * (size_t)c);
   return SP_OK;
 }

@@ -192,8 +192,145 @@ unsigned g_egeneration = 0;
 // the per-level direction model of BC's forward sweep
 std::vector<float> g_bparams;
 unsigned g_bgeneration = 0;
+// the kernel-variant models, one per algorithm (params, mean, scale packed)
+std::vector<float> g_vparams[VAR_ALGOS];
+unsigned g_vgeneration[VAR_ALGOS] = {};
+unsigned g_vcounter = 0;  // generations are unique across algorithms and loads
+
+// Degree statistics: per-block partials in shared memory, then one atomic per counter
+// per block. out[0] = max row, out[1] = sum of squares, out[2 + 2i] / out[3 + 2i] = rows
+// longer than thr[i] / entries in them.
+struct Thr {
+  int t[DEG_THR_MAX];
+  int n;
+};
+__global__ void __launch_bounds__(256) k_deg_stats(const int32_t* __restrict__ off, int n, Thr thr,
+                                                   unsigned long long* out) {
+  __shared__ unsigned long long s_acc[2 + 2 * DEG_THR_MAX];
+  for (int i = threadIdx.x; i < 2 + 2 * DEG_THR_MAX; i += blockDim.x) s_acc[i] = 0;
+  __syncthreads();
+  unsigned long long mx = 0, sq = 0, ra[DEG_THR_MAX] = {}, ea[DEG_THR_MAX] = {};
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const unsigned long long d = (unsigned long long)(off[v + 1] - off[v]);
+    mx = d > mx ? d : mx;
+    sq += d * d;
+#pragma unroll
+    for (int i = 0; i < DEG_THR_MAX; ++i)
+      if (i < thr.n && d > (unsigned long long)thr.t[i]) {
+        ra[i] += 1;
+        ea[i] += d;
+      }
+  }
+  atomicMax(&s_acc[0], mx);
+  atomicAdd(&s_acc[1], sq);
+#pragma unroll
+  for (int i = 0; i < DEG_THR_MAX; ++i)
+    if (i < thr.n) {
+      if (ra[i]) atomicAdd(&s_acc[2 + 2 * i], ra[i]);
+      if (ea[i]) atomicAdd(&s_acc[3 + 2 * i], ea[i]);
+    }
+  __syncthreads();
+  if (threadIdx.x == 0) atomicMax(&out[0], s_acc[0]);
+  if (threadIdx.x >= 1 && threadIdx.x < 2 + 2 * thr.n && s_acc[threadIdx.x])
+    atomicAdd(&out[threadIdx.x], s_acc[threadIdx.x]);
+}
 
 }  // namespace mlp
+
+int degree_stats(const int32_t* off, int n, const int* thr, int nthr, cudaStream_t s, DegStats* st) {
+  if (nthr < 0 || nthr > DEG_THR_MAX) {
+    set_error("degree_stats: %d thresholds (at most %d)", nthr, DEG_THR_MAX);
+    return SP_ERR_INVALID;
+  }
+  *st = DegStats();
+  if (n <= 0) return SP_OK;
+  mlp::Thr t;
+  t.n = nthr;
+  for (int i = 0; i < DEG_THR_MAX; ++i) t.t[i] = i < nthr ? thr[i] : 0;
+  dbuf<unsigned long long> acc;
+  SP_TRY(acc.alloc(2 + 2 * DEG_THR_MAX));
+  SP_CHECK_CUDA(cudaMemsetAsync(acc.p, 0, sizeof(unsigned long long) * (2 + 2 * DEG_THR_MAX), s));
+  const int grid = std::max(1, std::min(num_sms() * 4, (n + 255) / 256));
+  mlp::k_deg_stats<<<grid, 256, 0, s>>>(off, n, t, acc.p);
+  SP_CHECK_LAUNCH();
+  unsigned long long h[2 + 2 * DEG_THR_MAX];
+  SP_TRY(copy_out(h, acc.p, sizeof(h), s));
+  st->max_deg = (int64_t)h[0];
+  st->sum_sq = (int64_t)h[1];
+  for (int i = 0; i < nthr; ++i) {
+    st->rows_above[i] = (int64_t)h[2 + 2 * i];
+    st->edges_above[i] = (int64_t)h[3 + 2 * i];
+  }
+  return SP_OK;
+}
+
+int degree_stats_launch(const int32_t* off, int n, const int* thr, int nthr, unsigned long long* acc,
+                        cudaStream_t s) {
+  if (nthr < 0 || nthr > DEG_THR_MAX) {
+    set_error("degree_stats: %d thresholds (at most %d)", nthr, DEG_THR_MAX);
+    return SP_ERR_INVALID;
+  }
+  mlp::Thr t;
+  t.n = nthr;
+  for (int i = 0; i < DEG_THR_MAX; ++i) t.t[i] = i < nthr ? thr[i] : 0;
+  SP_CHECK_CUDA(cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * (2 + 2 * DEG_THR_MAX), s));
+  if (n <= 0) return SP_OK;
+  const int grid = std::max(1, std::min(num_sms() * 4, (n + 255) / 256));
+  mlp::k_deg_stats<<<grid, 256, 0, s>>>(off, n, t, acc);
+  SP_CHECK_LAUNCH();
+  return SP_OK;
+}
+
+unsigned variant_model(int algo, std::vector<float>& packed) {
+  std::lock_guard<std::mutex> lock(mlp::g_mu);
+  if (algo < 0 || algo >= VAR_ALGOS || mlp::g_vparams[algo].empty()) {
+    packed.clear();
+    return 0u;
+  }
+  packed = mlp::g_vparams[algo];
+  return mlp::g_vgeneration[algo];
+}
+
+unsigned variant_generation(int algo) {
+  if (algo < 0 || algo >= VAR_ALGOS) return 0;
+  std::lock_guard<std::mutex> lock(mlp::g_mu);
+  return mlp::g_vparams[algo].empty() ? 0u : mlp::g_vgeneration[algo];
+}
+
+int variant_choose(int algo, const std::vector<float>& X, const std::vector<int>& ok, int dflt, cudaStream_t s,
+                   int* best) {
+  std::vector<float> packed;
+  {
+    std::lock_guard<std::mutex> lock(mlp::g_mu);
+    if (algo < 0 || algo >= VAR_ALGOS || mlp::g_vparams[algo].empty()) return SP_ERR_UNSUPPORTED;
+    packed = mlp::g_vparams[algo];
+  }
+  const int N = (int)(X.size() / mlp::IN);
+  const float* mean = packed.data() + mlp::P;
+  const float* scale = mean + mlp::IN;
+  const float margin = scale[mlp::IN];
+  std::vector<float> Xn(X.size());
+  for (int k = 0; k < N; ++k)
+    for (int i = 0; i < mlp::IN; ++i) Xn[(size_t)k * mlp::IN + i] = (X[(size_t)k * mlp::IN + i] - mean[i]) * scale[i];
+  dbuf<float> dp, dx, dy;
+  SP_TRY(dp.alloc(mlp::P));
+  SP_TRY(dx.alloc(Xn.size()));
+  SP_TRY(dy.alloc(N));
+  SP_CHECK_CUDA(cudaMemcpyAsync(dp.p, packed.data(), sizeof(float) * mlp::P, cudaMemcpyHostToDevice, s));
+  SP_CHECK_CUDA(cudaMemcpyAsync(dx.p, Xn.data(), sizeof(float) * Xn.size(), cudaMemcpyHostToDevice, s));
+  mlp::k_forward<<<std::max(1, (N + 127) / 128), 128, 0, s>>>(dp.p, dx.p, N, dy.p);
+  SP_CHECK_LAUNCH();
+  std::vector<float> y(N);
+  SP_TRY(copy_out(y.data(), dy.p, sizeof(float) * N, s));
+  int b = -1;
+  for (int k = 0; k < N; ++k)
+    if (ok[k] && (b < 0 || y[k] < y[b])) b = k;
+  if (b < 0) return SP_ERR_UNSUPPORTED;
+  // leave the default only for a predicted gain above the model's margin (log units)
+  if (dflt >= 0 && dflt < N && ok[dflt] && !(y[dflt] - y[b] > margin)) b = dflt;
+  *best = b;
+  return SP_OK;
+}
 
 // The BC level model packed for the device and its generation (0 = none loaded).
 unsigned mlp_level_model(std::vector<float>& packed) {
@@ -355,4 +492,56 @@ extern "C" int sp_sched_level_load(const float* params, const float* feat_mean, 
   mlp::g_bparams.insert(mlp::g_bparams.end(), feat_mean, feat_mean + mlp::IN);
   mlp::g_bparams.insert(mlp::g_bparams.end(), feat_scale, feat_scale + mlp::IN);
   return SP_OK;
+}
+
+extern "C" int sp_sched_variant_load(int32_t algo, const float* params, const float* feat_mean,
+                                     const float* feat_scale, float margin) {
+  if (algo < 0 || algo >= VAR_ALGOS) {
+    set_error("sp_sched_variant_load: unknown algorithm %d", algo);
+    return SP_ERR_INVALID;
+  }
+  std::lock_guard<std::mutex> lock(mlp::g_mu);
+  mlp::g_vgeneration[algo] = ++mlp::g_vcounter;
+  if (!params) {
+    mlp::g_vparams[algo].clear();
+    return SP_OK;
+  }
+  if (!feat_mean || !feat_scale || !(margin >= 0.0f)) {
+    set_error("sp_sched_variant_load: feature normalisation and a margin >= 0 required");
+    return SP_ERR_INVALID;
+  }
+  std::vector<float>& v = mlp::g_vparams[algo];
+  v.assign(params, params + mlp::P);
+  v.insert(v.end(), feat_mean, feat_mean + mlp::IN);
+  v.insert(v.end(), feat_scale, feat_scale + mlp::IN);
+  v.push_back(margin);
+  return SP_OK;
+}
+
+extern "C" int sp_variant_count(int32_t algo, int32_t* n) {
+  if (!n || algo < 0 || algo >= VAR_ALGOS) {
+    set_error("sp_variant_count: invalid argument");
+    return SP_ERR_INVALID;
+  }
+  *n = algo == VAR_PR ? pr_variant_count()
+       : algo == VAR_TC ? tc_variant_count()
+       : algo == VAR_BC ? bc_variant_count()
+                        : lv_variant_count();
+  return SP_OK;
+}
+
+extern "C" int sp_variant_features(sp_graph_h g, int32_t algo, int32_t cand, int32_t nsrc, float* x,
+                                   int32_t* applicable) {
+  int32_t n = 0;
+  if (!g || !x || !applicable || sp_variant_count(algo, &n) != SP_OK || cand < 0 || cand >= n) {
+    set_error("sp_variant_features: invalid argument");
+    return SP_ERR_INVALID;
+  }
+  int ok = 0;
+  int st = algo == VAR_PR ? pr_variant_features(g, cand, x, &ok)
+           : algo == VAR_TC ? tc_variant_features(g, cand, x, &ok)
+           : algo == VAR_BC ? bc_variant_features(g, cand, std::max(1, (int)nsrc), x, &ok)
+                            : lv_variant_features(g, cand, x, &ok);
+  *applicable = ok;
+  return st;
 }

@@ -17,9 +17,11 @@ namespace sp {
 // every thread of the CTA must call it. Every CTA that evaluates the same rows runs the
 // same instructions in the same order, so all return the same candidate: a decision
 // taken this way needs no barrier between CTAs. Only candidates first .. NC-1 are
-// eligible; ties go to the lower index.
+// eligible; ties go to the lower index. With dflt >= 0, the result is dflt unless the
+// best score is lower than dflt's by more than margin.
 template <int NC>
-__device__ int mlp_argmin(const float* __restrict__ model, float (*rows)[SP_MLP_IN], int first = 0) {
+__device__ int mlp_argmin(const float* __restrict__ model, float (*rows)[SP_MLP_IN], int first = 0, int dflt = -1,
+                          float margin = 0.0f) {
   constexpr int IN = SP_MLP_IN, H = SP_MLP_HIDDEN;
   constexpr int W1 = 0, B1 = W1 + H * IN, W2 = B1 + H, B2 = W2 + H * H, W3 = B2 + H, B3 = W3 + H;
   static_assert(B3 + 1 == SP_MLP_PARAMS, "parameter layout");
@@ -57,6 +59,7 @@ __device__ int mlp_argmin(const float* __restrict__ model, float (*rows)[SP_MLP_
     int best = first;
     for (int k = first + 1; k < NC; ++k)
       if (s_y[k] < s_y[best]) best = k;
+    if (dflt >= first && dflt < NC && !(s_y[dflt] - s_y[best] > margin)) best = dflt;
     s_pick = best;
   }
   __syncthreads();

@@ -119,6 +119,13 @@ struct PrPlan {
   // The iterations are captured on this private stream and launched on the graph's
   // stream, which may be the legacy default stream (where capture is not allowed).
   cudaStream_t cap = nullptr;
+  // learned variant inputs: the share of in-edges whose source is among the 8192 / 32768
+  // / 131072 highest out-degree sources, and in-degree statistics (vorder = -1: not yet)
+  int vorder = -1;
+  double vshare[3] = {0, 0, 0};
+  int64_t vin_max = 0, vin_sq = 0;
+  int var_choice = -1;     // the learned candidate for this plan, under model var_gen
+  unsigned var_gen = 0;
 };
 
 int pr_order_default() { return pr::ORDER_DEFAULT; }
@@ -1054,6 +1061,143 @@ static pr::IterArgs iter_args(const PrPlan* p, float beta, float delta, int n_it
   return a;
 }
 
+// ---- learned kernel variant -------------------------------------------------------
+// The table the variant model scores: how many of the most-gathered sources allocate
+// their contrib gathers in L1 (0 = all), the srcList L1 policy, and 16-byte srcList loads.
+// Entry 10 is the fixed default (32768, evict-first, 4-byte loads).
+namespace pr {
+struct Variant {
+  int l1_hot, src_hint, vec;
+};
+constexpr Variant VARIANTS[] = {{0, 0, 0},      {0, 2, 0},      {0, 2, 1},      {8192, 0, 0},
+                                {8192, 2, 0},   {8192, 2, 1},   {16384, 2, 0},  {32768, 0, 0},
+                                {32768, 0, 1},  {32768, 2, 1},  {32768, 2, 0},  {65536, 2, 0},
+                                {131072, 0, 0}, {131072, 2, 0}, {131072, 2, 1}, {524288, 2, 0}};
+constexpr int N_VARIANTS = (int)(sizeof(VARIANTS) / sizeof(VARIANTS[0]));
+constexpr int DEFAULT_VARIANT = 10;
+constexpr int SHARE_K[3] = {8192, 32768, 131072};
+
+// sums of od[0 .. SHARE_K[j]) (od is the out-degree in relabelled order, descending);
+// the kernel spells out SHARE_K's three values
+__global__ void k_top_share(int V, const int32_t* __restrict__ od, unsigned long long* out) {
+  __shared__ unsigned long long s[3];
+  if (threadIdx.x < 3) s[threadIdx.x] = 0;
+  __syncthreads();
+  unsigned long long a[3] = {0, 0, 0};
+  const int lim = min(V, 131072);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < lim; i += gridDim.x * blockDim.x) {
+    const unsigned long long d = (unsigned long long)od[i];
+    if (i < 8192) a[0] += d;
+    if (i < 32768) a[1] += d;
+    a[2] += d;
+  }
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const unsigned long long w = warp_sum(a[j]);
+    if ((threadIdx.x & 31) == 0 && w) atomicAdd(&s[j], w);
+  }
+  __syncthreads();
+  if (threadIdx.x < 3 && s[threadIdx.x]) atomicAdd(&out[threadIdx.x], s[threadIdx.x]);
+}
+}  // namespace pr
+
+int pr_variant_count() { return pr::N_VARIANTS; }
+
+static int pr_plan_for_call(sp_graph* g) {
+  const int hot = std::max(0, std::min(g->pr_hot >= 0 ? g->pr_hot : pr::HOT_DEFAULT, pr::HOT_MAX));
+  const int order = g->pr_order >= 0 ? g->pr_order : pr::ORDER_DEFAULT;
+  return build_pr_plan(g, hot, order);
+}
+
+static int pr_variant_stats(sp_graph* g) {
+  PrPlan* p = g->pr;
+  if (p->vorder == p->order) return SP_OK;
+  cudaStream_t s = g->stream;
+  dbuf<unsigned long long> acc;
+  SP_TRY(acc.alloc(3));
+  SP_CHECK_CUDA(cudaMemsetAsync(acc.p, 0, sizeof(unsigned long long) * 3, s));
+  pr::k_top_share<<<std::max(1, std::min(num_sms(), (g->V + 255) / 256)), 256, 0, s>>>(g->V, p->od.p, acc.p);
+  SP_CHECK_LAUNCH();
+  unsigned long long h[3];
+  SP_TRY(copy_out(h, acc.p, sizeof(h), s));
+  DegStats ds;
+  SP_TRY(degree_stats(p->roffp.p, g->V, nullptr, 0, s, &ds));
+  const double E = std::max<double>(1.0, (double)g->E);
+  for (int j = 0; j < 3; ++j) p->vshare[j] = (double)h[j] / E;
+  p->vin_max = ds.max_deg;
+  p->vin_sq = ds.sum_sq;
+  p->vorder = p->order;
+  return SP_OK;
+}
+
+// Inputs: graph shape over in-degrees (the pull's rows), the hot shares, then the
+// candidate: log of the sources that allocate in L1, that count as a fraction of V,
+// srcList policy, vector loads, and the share of gathers that hit those sources.
+int pr_variant_features(sp_graph* g, int cand, float* x, int* applicable) {
+  if (cand < 0 || cand >= pr::N_VARIANTS) return SP_ERR_INVALID;
+  SP_TRY(pr_plan_for_call(g));
+  SP_TRY(pr_variant_stats(g));
+  const PrPlan* p = g->pr;
+  const pr::Variant& c = pr::VARIANTS[cand];
+  const double V = g->V, E = (double)g->E, avg = E / std::max(1.0, V), mx = (double)p->vin_max;
+  const double eff = c.l1_hot == 0 ? V : std::min<double>(c.l1_hot, V);
+  double share = 1.0;  // share of gathers from the first eff sources
+  if (eff < V) {
+    share = eff <= pr::SHARE_K[0] ? p->vshare[0] * eff / pr::SHARE_K[0]
+            : eff <= pr::SHARE_K[1]
+                ? p->vshare[0] + (p->vshare[1] - p->vshare[0]) * (eff - pr::SHARE_K[0]) / (pr::SHARE_K[1] - pr::SHARE_K[0])
+            : eff <= pr::SHARE_K[2]
+                ? p->vshare[1] + (p->vshare[2] - p->vshare[1]) * (eff - pr::SHARE_K[1]) / (pr::SHARE_K[2] - pr::SHARE_K[1])
+                : p->vshare[2] + (1.0 - p->vshare[2]) * (eff - pr::SHARE_K[2]) / std::max(1.0, V - pr::SHARE_K[2]);
+    share = std::min(1.0, share);
+  }
+  x[0] = (float)std::log2(std::max(1.0, V));
+  x[1] = (float)std::log2(E + 1.0);
+  x[2] = (float)avg;
+  x[3] = (float)std::log2(mx + 1.0);
+  x[4] = (float)std::log2(((double)p->vin_sq / std::max(1.0, E)) + 1.0);  // in-degree second moment
+  x[5] = (float)p->vshare[0];
+  x[6] = (float)p->vshare[1];
+  x[7] = (float)p->vshare[2];
+  x[8] = (float)std::log2(eff + 1.0);
+  x[9] = (float)(eff / std::max(1.0, V));
+  x[10] = (float)c.src_hint * 0.5f;
+  x[11] = (float)c.vec;
+  x[12] = (float)share;
+  *applicable = 1;
+  return SP_OK;
+}
+
+// The candidate this call runs: forced by "pr.variant", else learned when a model is
+// loaded and no variant knob is set; -1 = the knobs and defaults.
+static int pr_variant_pick(sp_graph* g, int* cand) {
+  *cand = -1;
+  const int mode = g->variant[VAR_PR];
+  if (mode >= 0) {
+    *cand = mode;
+    return SP_OK;
+  }
+  if (mode != -1 || g->pr_l1_hot >= 0 || g->pr_src_hint >= 0 || g->pr_vec >= 0) return SP_OK;
+  const unsigned gen = variant_generation(VAR_PR);
+  if (!gen) return SP_OK;
+  PrPlan* p = g->pr;
+  if (p->var_gen == gen && p->var_choice >= 0) {
+    *cand = p->var_choice;
+    return SP_OK;
+  }
+  std::vector<float> X((size_t)pr::N_VARIANTS * SP_MLP_IN);
+  std::vector<int> ok(pr::N_VARIANTS);
+  for (int k = 0; k < pr::N_VARIANTS; ++k) SP_TRY(pr_variant_features(g, k, X.data() + (size_t)k * SP_MLP_IN, &ok[k]));
+  int best = -1;
+  const int st = variant_choose(VAR_PR, X, ok, pr::DEFAULT_VARIANT, g->stream, &best);
+  if (st == SP_ERR_UNSUPPORTED) return SP_OK;  // unloaded meanwhile
+  SP_TRY(st);
+  p->var_choice = best;
+  p->var_gen = gen;
+  *cand = best;
+  return SP_OK;
+}
+
 // init: starting ranks in the caller's vertex order (host or device), or null for 1/V.
 static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float* out, int32_t* iters,
                     double* fdiff, const float* init = nullptr) {
@@ -1066,9 +1210,17 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
   const int n_iter = std::max(1, (int)maxIter);
   pr::IterArgs a = iter_args(p, beta, delta, n_iter, V);
   int per_sm = 0;
-  const int sh = g->pr_src_hint >= 0 ? g->pr_src_hint : pr::SRC_HINT_DEFAULT;
-  const int l1_hot = g->pr_l1_hot >= 0 ? g->pr_l1_hot : pr::L1_HOT_DEFAULT;
-  const int vec = g->pr_vec >= 0 ? g->pr_vec : pr::VEC_DEFAULT;
+  int sh = g->pr_src_hint >= 0 ? g->pr_src_hint : pr::SRC_HINT_DEFAULT;
+  int l1_hot = g->pr_l1_hot >= 0 ? g->pr_l1_hot : pr::L1_HOT_DEFAULT;
+  int vec = g->pr_vec >= 0 ? g->pr_vec : pr::VEC_DEFAULT;
+  int cand = -1;
+  SP_TRY(pr_variant_pick(g, &cand));
+  if (cand >= 0) {
+    sh = pr::VARIANTS[cand].src_hint;
+    l1_hot = pr::VARIANTS[cand].l1_hot;
+    vec = pr::VARIANTS[cand].vec;
+  }
+  g->last_variant[VAR_PR] = cand;
   a.l1_hot = l1_hot;
   const int gh = l1_hot > 0 ? 1 : 0;
   using PhaseFn = void (*)(pr::IterArgs, const float*, const float*, float*, float*);

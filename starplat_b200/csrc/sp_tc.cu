@@ -45,7 +45,7 @@ constexpr int WARPS = THREADS / 32;
 constexpr int HCAP = 1024;          // hash slots per warp (load factor <= 1/2)
 constexpr int SMAX = HCAP / 2;      // largest S(a) handled by the warp path
 constexpr int EMPTY = -1;
-constexpr int WU = 4;               // k_tc_warp: probe-list elements per lane per pass
+constexpr int WU_DEFAULT = 4;       // k_tc_warp: probe-list elements per lane per pass
 
 __device__ __forceinline__ unsigned hslot(int k) { return ((unsigned)k * 2654435761u) >> 22; }  // 10 bits
 
@@ -101,7 +101,7 @@ __device__ __forceinline__ void probe_range(const Lists& L, int a, int p, int& l
   le = e;
 }
 
-template <bool PV>
+template <bool PV, int WU>
 __global__ void __launch_bounds__(THREADS) k_tc_warp(Lists L, const int32_t* __restrict__ order,
                                                      int* __restrict__ heavy, unsigned int* __restrict__ n_heavy,
                                                      unsigned long long* __restrict__ total, int* __restrict__ cf) {
@@ -692,6 +692,11 @@ struct TcPlan {
   dbuf<unsigned long long> total;
   bool oriented = false;
   bool built = false;
+  // learned variant inputs (vstat < 0: not yet) and the learned choice under model var_gen
+  int vstat = -1;
+  int64_t vmax = 0, vsq = 0, vheavy = 0;
+  int var_choice = -1;
+  unsigned var_gen = 0;
 };
 
 int tc_cta_warps_default() { return tc::CTA_WARPS_DEFAULT; }
@@ -792,6 +797,90 @@ static tc::Lists tc_lists(sp_graph* g, int n) {
   return L;
 }
 
+// ---- learned kernel variant -------------------------------------------------------
+// Graphs up to 65536 vertices choose the shared-bitmap kernel's CTA width (0 = a bitmap
+// per warp); larger graphs choose the hash kernel's probe-list elements per lane per
+// pass. Entries 2 and 7 are the fixed defaults.
+namespace tc {
+struct Variant {
+  int bitmap, cta_warps, wu;
+};
+constexpr Variant VARIANTS[] = {{1, 0, 0}, {1, 2, 0}, {1, 4, 0}, {1, 8, 0},
+                                {1, 16, 0}, {0, 0, 1}, {0, 0, 2}, {0, 0, 4}};
+constexpr int N_VARIANTS = (int)(sizeof(VARIANTS) / sizeof(VARIANTS[0]));
+constexpr int DEFAULT_BITMAP = 2, DEFAULT_HASH = 7;
+}  // namespace tc
+
+int tc_variant_count() { return tc::N_VARIANTS; }
+
+// Inputs: graph shape, symmetry, the path (bitmap below 65537 vertices), the share of
+// entries in rows above the hash path's set size, then the candidate.
+int tc_variant_features(sp_graph* g, int cand, float* x, int* applicable) {
+  if (cand < 0 || cand >= tc::N_VARIANTS) return SP_ERR_INVALID;
+  SP_TRY(build_tc_plan(g));
+  TcPlan* p = g->tc;
+  if (p->vstat < 0) {
+    const int thr[1] = {tc::SMAX};
+    DegStats ds;
+    SP_TRY(degree_stats(g->off.p, g->V, thr, 1, g->stream, &ds));
+    p->vmax = ds.max_deg;
+    p->vsq = ds.sum_sq;
+    p->vheavy = ds.edges_above[0];
+    p->vstat = 1;
+  }
+  const tc::Variant& c = tc::VARIANTS[cand];
+  const bool bitmap_path = g->V <= 65536;
+  const double V = g->V, E = std::max<double>(1.0, (double)g->E), avg = E / std::max(1.0, V);
+  const double lcw = std::log2(1.0 + c.cta_warps);
+  x[0] = (float)std::log2(std::max(1.0, V));
+  x[1] = (float)std::log2(E + 1.0);
+  x[2] = (float)avg;
+  x[3] = (float)std::log2((double)p->vmax + 1.0);
+  x[4] = (float)std::log2((double)p->vsq / E + 1.0);
+  x[5] = (float)(g->symmetric > 0);
+  x[6] = bitmap_path ? 1.0f : 0.0f;
+  x[7] = (float)((double)p->vheavy / E);
+  x[8] = (float)c.bitmap;
+  x[9] = (float)lcw;
+  x[10] = (c.bitmap && c.cta_warps == 0) ? 1.0f : 0.0f;
+  x[11] = c.wu ? (float)std::log2((double)c.wu) : 0.0f;
+  x[12] = (float)(lcw * avg / 16.0);
+  *applicable = (c.bitmap != 0) == bitmap_path;
+  return SP_OK;
+}
+
+static int tc_variant_pick(sp_graph* g, int* cand) {
+  *cand = -1;
+  const int mode = g->variant[VAR_TC];
+  if (mode >= 0) {
+    if ((tc::VARIANTS[mode].bitmap != 0) != (g->V <= 65536)) {
+      set_error("tc.variant %d does not apply to a graph of %d vertices", mode, g->V);
+      return SP_ERR_INVALID;
+    }
+    *cand = mode;
+    return SP_OK;
+  }
+  if (mode != -1 || g->tc_cta_warps >= 0 || g->tc_unroll > 0) return SP_OK;
+  const unsigned gen = variant_generation(VAR_TC);
+  if (!gen) return SP_OK;
+  TcPlan* p = g->tc;
+  if (p->var_gen == gen && p->var_choice >= 0) {
+    *cand = p->var_choice;
+    return SP_OK;
+  }
+  std::vector<float> X((size_t)tc::N_VARIANTS * SP_MLP_IN);
+  std::vector<int> ok(tc::N_VARIANTS);
+  for (int k = 0; k < tc::N_VARIANTS; ++k) SP_TRY(tc_variant_features(g, k, X.data() + (size_t)k * SP_MLP_IN, &ok[k]));
+  int best = -1;
+  const int st = variant_choose(VAR_TC, X, ok, g->V <= 65536 ? tc::DEFAULT_BITMAP : tc::DEFAULT_HASH, g->stream, &best);
+  if (st == SP_ERR_UNSUPPORTED) return SP_OK;
+  SP_TRY(st);
+  p->var_choice = best;
+  p->var_gen = gen;
+  *cand = best;
+  return SP_OK;
+}
+
 // Triangles anchored at order[0 .. n) (the whole count when order is the plan's and n = V).
 static int tc_count(sp_graph* g, const int32_t* order, int n, int64_t* triangle_count) {
   TcPlan* p = g->tc;
@@ -799,7 +888,15 @@ static int tc_count(sp_graph* g, const int32_t* order, int n, int64_t* triangle_
   const tc::Lists L = tc_lists(g, n);
   SP_CHECK_CUDA(cudaMemsetAsync(p->ctr.p, 0, sizeof(unsigned int) * 2, s));
   SP_CHECK_CUDA(cudaMemsetAsync(p->total.p, 0, sizeof(unsigned long long), s));
-  const int cta_warps = g->tc_cta_warps >= 0 ? g->tc_cta_warps : tc::CTA_WARPS_DEFAULT;
+  int cta_warps = g->tc_cta_warps >= 0 ? g->tc_cta_warps : tc::CTA_WARPS_DEFAULT;
+  int wu = g->tc_unroll > 0 ? g->tc_unroll : tc::WU_DEFAULT;
+  int cand = -1;
+  SP_TRY(tc_variant_pick(g, &cand));
+  if (cand >= 0) {
+    if (tc::VARIANTS[cand].bitmap) cta_warps = tc::VARIANTS[cand].cta_warps;
+    else wu = tc::VARIANTS[cand].wu;
+  }
+  g->last_variant[VAR_TC] = cand;
   if (g->V <= 65536 && cta_warps > 0) {
     void (*k)(tc::Lists, const int32_t*, unsigned long long*, int*) =
         cta_warps == 2   ? tc::k_tc_bitmap_cta<2, 24, false>
@@ -816,8 +913,9 @@ static int tc_count(sp_graph* g, const int32_t* order, int n, int64_t* triangle_
     tc::k_tc_bitmap<<<num_sms() * std::max(1, per_sm), tc::BM_THREADS, 0, s>>>(L, order, p->total.p);
     SP_CHECK_LAUNCH();
   } else {
-    tc::k_tc_warp<false>
-        <<<num_sms() * 4, tc::THREADS, 0, s>>>(L, order, p->heavy.p, p->ctr.p + 1, p->total.p, nullptr);
+    void (*k)(tc::Lists, const int32_t*, int*, unsigned int*, unsigned long long*, int*) =
+        wu == 1 ? tc::k_tc_warp<false, 1> : wu == 2 ? tc::k_tc_warp<false, 2> : tc::k_tc_warp<false, 4>;
+    k<<<num_sms() * 4, tc::THREADS, 0, s>>>(L, order, p->heavy.p, p->ctr.p + 1, p->total.p, nullptr);
     SP_CHECK_LAUNCH();
     tc::k_tc_heavy<false><<<num_sms() * 2, tc::THREADS, 0, s>>>(L, p->heavy.p, p->ctr.p + 1, p->total.p, nullptr);
     SP_CHECK_LAUNCH();
@@ -842,7 +940,7 @@ static int lcc_count(sp_graph* g, const int32_t* order, int n, int* counts) {
     tc::k_tc_bitmap_cta<4, 8, true><<<num_sms() * std::max(1, per_sm), 4 * 32, 0, s>>>(L, order, p->total.p, counts);
     SP_CHECK_LAUNCH();
   } else {
-    tc::k_tc_warp<true>
+    tc::k_tc_warp<true, tc::WU_DEFAULT>
         <<<num_sms() * 4, tc::THREADS, 0, s>>>(L, order, p->heavy.p, p->ctr.p + 1, p->total.p, counts);
     SP_CHECK_LAUNCH();
     tc::k_tc_heavy<true><<<num_sms() * 2, tc::THREADS, 0, s>>>(L, p->heavy.p, p->ctr.p + 1, p->total.p, counts);

@@ -456,7 +456,9 @@ class DeviceGraph:
         return out
 
     def louvain(self, weight=None, threshold: float = 1e-4, community=None, variant: int = _lib.SP_LV_TUNED):
-        """Louvain; returns (modularity, community[V] int32, levels)."""
+        """Louvain; returns (modularity, community[V] int32, levels). The shipped variant
+        model, loaded on first use, picks each level's CTA-bin table size."""
+        _ensure_scheduler()
         if community is None:
             community = np.empty(self.V, np.int32)
         if weight is not None and str(weight.dtype) not in ("float32", "torch.float32"):

@@ -129,13 +129,16 @@ def _settle_auto_load() -> None:
 
 def load(path: str = MODEL_PATH, epoch_path: str = EPOCH_MODEL_PATH, level_path: str = LEVEL_MODEL_PATH) -> bool:
     """Load the model (and the per-epoch width and per-level direction models, when their
-    files exist) into the library; False (fixed heuristic stays) if the model file is
-    absent."""
+    files exist, and the shipped kernel-variant models of variants.py) into the library;
+    False (fixed heuristic stays) if the SSSP model file is absent."""
     _settle_auto_load()
     if epoch_path and os.path.exists(epoch_path):
         load_epoch(epoch_path)
     if level_path and os.path.exists(level_path):
         load_level(level_path)
+    from . import variants
+
+    variants.load()  # the kernel-variant models marked shipped
     if not os.path.exists(path):
         return False
     d = json.load(open(path))
@@ -149,12 +152,15 @@ def load(path: str = MODEL_PATH, epoch_path: str = EPOCH_MODEL_PATH, level_path:
 
 
 def unload() -> None:
-    """Back to the fixed heuristic (and fixed bucket widths), also for later calls in
-    this process."""
+    """Back to the fixed heuristic (and fixed bucket widths and kernel variants), also for
+    later calls in this process."""
     _settle_auto_load()
     check("sp_sched_load", lib().sp_sched_load(None, None, None))
     check("sp_sched_epoch_load", lib().sp_sched_epoch_load(None, None, None))
     check("sp_sched_level_load", lib().sp_sched_level_load(None, None, None))
+    from . import variants
+
+    variants.unload()
 
 
 def _load_packed(path, call) -> bool:
