@@ -20,9 +20,11 @@
 //    marker appends w to the level list, then lanes (one per source bit) add
 //    sigma with FP64 atomics (integer-valued, so the sum is exact in any order);
 //  * backward level d: the masks of level d+1 are scattered into a dense array; for
-//    each (v, mask) of level d the lanes pull sigma/delta of the successors in edge
-//    order, the loads of BU successors in flight together — no atomics,
-//    deterministic;
+//    each (v, mask) of level d the lanes pull q[w][b] = (1 + delta[w][b]) / sigma[w][b]
+//    of the successors in edge order (stored in FP64 when w's dependency became final),
+//    the loads of BU successors in flight together, and delta[v][b] = sigma[v][b] *
+//    sum q — one 8-byte load and one add per successor instead of two loads and an FP64
+//    division; no atomics, deterministic;
 //  * level-list entries of vertices with more than hub_deg edges (default 64) are cut
 //    into hub_chunk-edge pieces (default 64) that all warps share (one extra barrier
 //    per level); their backward partials meet in an FP64 scratch through atomics;
@@ -53,12 +55,17 @@ constexpr int CTA_THREADS = 512;
 constexpr int HUB_DEG = 64;
 constexpr int HUB_CHUNK = 64;
 constexpr int CLUSTER_DEFAULT = 1;  // CTAs per graph in the many-graphs form (bc.cluster)
-// Successors whose sigma / delta loads are in flight together in the backward sweep,
+// Successors whose loads are in flight together in the backward sweep (measured when
+// each successor cost a sigma and a delta load),
 // with the grid kernel held to 64 registers (4 CTAs per SM). R-MAT 20, 256 sources:
 // 110 ms with one at a time, 87 ms with 2 at 64 registers, 97 ms with 2 at 78
 // registers (3 CTAs per SM), 121 ms with 4 at 128 registers; 1000 ER graphs: 135 ->
 // 104 ms.
 constexpr int BU = 2;
+// The same for the many-graphs kernels: with one q load per successor, 1000 ER graphs
+// take 92.8 ms at 4 in flight, 126.6 ms at 2 (which spills in k_bc_graphs<1>) and
+// 103.4 ms before q; R-MAT 20 (grid kernel, BU) 74.1 ms at 2, 76.7 at 4.
+constexpr int BU_GRAPHS = 4;
 // 32-edge chunks of one entry whose loads and atomics are in flight together in the
 // forward sweep.
 constexpr int FU = 2;
@@ -75,6 +82,8 @@ struct Work {
   int V;                            // vertices of this graph
   double* sigma;                    // [V][SW]
   float* delta;                     // [V][SW]
+  double* q;                        // [V][SW] (1 + delta) / sigma once delta is final: what a
+                                    // predecessor's dependency sum reads of a successor
   unsigned long long* seen;         // [V]
   unsigned long long* nxt;          // [V]
   unsigned long long* dense;        // [V]
@@ -438,7 +447,7 @@ __device__ void pull_level(const Work& W, unsigned long long full, int lane, int
 
 // piece = false: the whole entry, dependencies written to delta; piece = true: an
 // edge range of a hub entry, partial dependencies added to dacc (FP64 atomics).
-template <int NW, int GS>
+template <int NW, int GS, int B>
 __device__ void backward_entry(const Work& W, int i, int lane, int eb, int ee, bool piece) {
   static_assert(GS == 32 || (GS == 16 && NW == 1), "half-warp steps hold up to 16 sources");
   constexpr int SW = 32 * NW;
@@ -451,7 +460,6 @@ __device__ void backward_entry(const Work& W, int i, int lane, int eb, int ee, b
     sv[k] = ((m >> b) & 1ull) ? W.sigma[(size_t)v * SW + b] : 0.0;
     acc[k] = 0.0;
   }
-  const double svg = GS == 16 ? __shfl_sync(0xffffffffu, sv[0], lane & 15) : 0.0;
   double accg = 0.0;  // GS = 16: this half-warp's share for source bit (lane & 15)
   for (int c = eb; c < ee; c += 32) {
     const int j = c + lane;
@@ -461,17 +469,19 @@ __device__ void backward_entry(const Work& W, int i, int lane, int eb, int ee, b
       w = W.adj[j] - W.vbase;
       s = m & W.dense[w];
     }
-    // Successors are taken BU at a time: all their sigma / delta loads are issued
-    // before any is summed (one memory latency per BU successors instead of per
-    // successor), and the sums still run in edge order.
+    // Successors are taken BU at a time: all their q loads are issued before any is
+    // summed (one memory latency per BU successors instead of per successor), and the
+    // sums run in edge order. q[w] = (1 + delta[w]) / sigma[w] was stored when w's
+    // dependency became final, so a successor costs one 8-byte load and one add; the
+    // product with sigma[v] is taken once per entry.
     unsigned em = __ballot_sync(0xffffffffu, s != 0ull);
     while (em) {
       if (GS == 16) {
         const int b = lane & 15;
-        int wm[BU];
-        bool on[BU];
+        int wm[B];
+        bool on[B];
 #pragma unroll
-        for (int u = 0; u < BU; ++u) {
+        for (int u = 0; u < B; ++u) {
           int from;
           const int ml = half_pick(em, lane, from);  // -1 once em is empty
           from = max(from, 0);
@@ -479,25 +489,19 @@ __device__ void backward_entry(const Work& W, int i, int lane, int eb, int ee, b
           wm[u] = __shfl_sync(0xffffffffu, w, from);
           on[u] = ml >= 0 && ((sm >> b) & 1ull);
         }
-        double sg[BU];
-        float dl[BU];
+        double qs[B];
 #pragma unroll
-        for (int u = 0; u < BU; ++u) {
-          if (on[u]) {
-            const size_t x = (size_t)wm[u] * SW + b;
-            sg[u] = W.sigma[x];
-            dl[u] = W.delta[x];
-          }
-        }
+        for (int u = 0; u < B; ++u)
+          if (on[u]) qs[u] = W.q[(size_t)wm[u] * SW + b];
 #pragma unroll
-        for (int u = 0; u < BU; ++u)
-          if (on[u]) accg += svg / sg[u] * (1.0 + (double)dl[u]);
+        for (int u = 0; u < B; ++u)
+          if (on[u]) accg += qs[u];
         continue;
       }
-      int wl[BU];
+      int wl[B];
       unsigned pm = 0;  // bit u * NW + k: successor u has source bit lane + 32 k
 #pragma unroll
-      for (int u = 0; u < BU; ++u) {
+      for (int u = 0; u < B; ++u) {
         const bool have = em != 0u;
         const int l = have ? __ffs(em) - 1 : 0;
         em &= em - 1;
@@ -507,22 +511,17 @@ __device__ void backward_entry(const Work& W, int i, int lane, int eb, int ee, b
         for (int k = 0; k < NW; ++k)
           if (have && ((sl >> (lane + 32 * k)) & 1ull)) pm |= 1u << (u * NW + k);
       }
-      double sg[BU][NW];
-      float dl[BU][NW];
+      double qs[B][NW];
 #pragma unroll
-      for (int u = 0; u < BU; ++u)
-#pragma unroll
-        for (int k = 0; k < NW; ++k)
-          if ((pm >> (u * NW + k)) & 1u) {
-            const size_t x = (size_t)wl[u] * SW + lane + 32 * k;
-            sg[u][k] = W.sigma[x];
-            dl[u][k] = W.delta[x];
-          }
-#pragma unroll
-      for (int u = 0; u < BU; ++u)
+      for (int u = 0; u < B; ++u)
 #pragma unroll
         for (int k = 0; k < NW; ++k)
-          if ((pm >> (u * NW + k)) & 1u) acc[k] += sv[k] / sg[u][k] * (1.0 + (double)dl[u][k]);
+          if ((pm >> (u * NW + k)) & 1u) qs[u][k] = W.q[(size_t)wl[u] * SW + lane + 32 * k];
+#pragma unroll
+      for (int u = 0; u < B; ++u)
+#pragma unroll
+        for (int k = 0; k < NW; ++k)
+          if ((pm >> (u * NW + k)) & 1u) acc[k] += qs[u][k];
     }
   }
   if (GS == 16) acc[0] = accg + __shfl_down_sync(0xffffffffu, accg, 16);  // first half, then second
@@ -531,9 +530,11 @@ __device__ void backward_entry(const Work& W, int i, int lane, int eb, int ee, b
     const int b = lane + 32 * k;
     if ((m >> b) & 1ull) {
       if (piece) {
-        if (acc[k] != 0.0) atomicAdd(&W.dacc[(size_t)v * SW + b], acc[k]);
+        if (acc[k] != 0.0) atomicAdd(&W.dacc[(size_t)v * SW + b], acc[k]);  // partial sum of q
       } else {
-        W.delta[(size_t)v * SW + b] = (float)acc[k];
+        const float dv = (float)(sv[k] * acc[k]);
+        W.delta[(size_t)v * SW + b] = dv;
+        W.q[(size_t)v * SW + b] = (1.0 + (double)dv) / sv[k];
       }
     }
   }
@@ -561,7 +562,7 @@ __device__ __forceinline__ bool pull_this_level(const Work& W, int d, int nent, 
   return (double)W.dir_alpha * mf > mu + 0.125 * (double)V && nent > 0;
 }
 
-template <int NW, int GS, class S>
+template <int NW, int GS, int B, class S>
 __device__ bool run_batch(const Work& W, const int32_t* srcs, int nsrc, S& sync, int32_t* lvl_out = nullptr,
                           double* sig_out = nullptr, int32_t* s_app = nullptr) {
   constexpr int SW = 32 * NW;
@@ -679,7 +680,7 @@ __device__ bool run_batch(const Work& W, const int32_t* srcs, int nsrc, S& sync,
     if (!sync.sync()) return false;
     const int b0 = W.lo[d], e0 = W.lo[d + 1];
     for (int i = b0 + gw; i < e0; i += nw)
-      if (!queue_hub(W, i, lane)) backward_entry<NW, GS>(W, i, lane, W.off[W.flv[i]], W.off[W.flv[i] + 1], false);
+      if (!queue_hub(W, i, lane)) backward_entry<NW, GS, B>(W, i, lane, W.off[W.flv[i]], W.off[W.flv[i] + 1], false);
     if (!sync.sync()) return false;
     if (W.hub_cap) {
       const unsigned long long hc = *(volatile unsigned long long*)W.hub_cnt;
@@ -688,7 +689,7 @@ __device__ bool run_batch(const Work& W, const int32_t* srcs, int nsrc, S& sync,
         for (int p = gw; p < np; p += nw) {
           int i, eb, ee;
           hub_piece(W, nh, p, i, eb, ee);
-          backward_entry<NW, GS>(W, i, lane, eb, ee, true);
+          backward_entry<NW, GS, B>(W, i, lane, eb, ee, true);
         }
         if (!sync.sync()) return false;
         // hub dependencies: FP64 partials -> delta, scratch back to zero
@@ -701,7 +702,10 @@ __device__ bool run_batch(const Work& W, const int32_t* srcs, int nsrc, S& sync,
             const int bb = lane + 32 * q;
             if ((m >> bb) & 1ull) {
               const size_t x = (size_t)v * SW + bb;
-              W.delta[x] = (float)W.dacc[x];
+              const double sg = W.sigma[x];
+              const float dv = (float)(sg * W.dacc[x]);
+              W.delta[x] = dv;
+              W.q[x] = (1.0 + (double)dv) / sg;
               W.dacc[x] = 0.0;
             }
           }
@@ -733,13 +737,13 @@ __device__ bool run_batch(const Work& W, const int32_t* srcs, int nsrc, S& sync,
 
 // run_batch with the half-warp step when the batch has at most 16 sources (every
 // thread of the team sees the same nsrc, so all take the same branch).
-template <int NW, class S>
+template <int NW, int B, class S>
 __device__ bool run_batch_any(const Work& W, const int32_t* srcs, int nsrc, S& sync, int32_t* lvl_out = nullptr,
                               double* sig_out = nullptr, int32_t* s_app = nullptr) {
   if constexpr (NW == 1) {
-    if (nsrc <= 16) return run_batch<1, 16>(W, srcs, nsrc, sync, lvl_out, sig_out, s_app);
+    if (nsrc <= 16) return run_batch<1, 16, B>(W, srcs, nsrc, sync, lvl_out, sig_out, s_app);
   }
-  return run_batch<NW, 32>(W, srcs, nsrc, sync, lvl_out, sig_out, s_app);
+  return run_batch<NW, 32, B>(W, srcs, nsrc, sync, lvl_out, sig_out, s_app);
 }
 
 struct GridArgs {
@@ -757,7 +761,7 @@ __global__ void __launch_bounds__(GRID_THREADS, 4) k_bc_grid(GridArgs a) {
   __shared__ int32_t s_app[GRID_THREADS];  // pull levels: 32 append slots per warp
   GridSync gs{a.bar};
   for (int s0 = 0; s0 < a.nsrc; s0 += a.batch) {
-    if (!run_batch_any<NW>(a.W, a.srcs + s0, min(a.batch, a.nsrc - s0), gs, a.lvl_out, a.sig_out, s_app)) {
+    if (!run_batch_any<NW, BU>(a.W, a.srcs + s0, min(a.batch, a.nsrc - s0), gs, a.lvl_out, a.sig_out, s_app)) {
       if (threadIdx.x == 0 && a.bar->error) atomicCAS(a.W.err, 0, 3);
       return;
     }
@@ -777,6 +781,7 @@ struct GraphsArgs {
   // per-CTA scratch (sized for the largest graph)
   double* sigma;
   float* delta;
+  double* q;
   unsigned long long* masks;  // 3 * vmax per CTA
   int32_t* flv;
   unsigned long long* flm;
@@ -797,6 +802,7 @@ __global__ void __launch_bounds__(CTA_THREADS) k_bc_graphs(GraphsArgs a) {
   Work W;
   W.sigma = a.sigma + (size_t)slot * a.vmax * SW;
   W.delta = a.delta + (size_t)slot * a.vmax * SW;
+  W.q = a.q + (size_t)slot * a.vmax * SW;
   W.seen = a.masks + (size_t)slot * a.vmax * 3;
   W.nxt = W.seen + a.vmax;
   W.dense = W.nxt + a.vmax;
@@ -832,7 +838,7 @@ __global__ void __launch_bounds__(CTA_THREADS) k_bc_graphs(GraphsArgs a) {
       const int nb = min(SW, ns - s0);
       for (int t = threadIdx.x; t < nb; t += blockDim.x) s_src[t] = a.srcs[sb + s0 + t] - vb;
       __syncthreads();
-      if (!run_batch_any<NW>(W, s_src, nb, bs)) return;
+      if (!run_batch_any<NW, BU_GRAPHS>(W, s_src, nb, bs)) return;
     }
   }
 }
@@ -852,6 +858,7 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(CTA_THREADS) k_bc_cl
   Work W;
   W.sigma = a.sigma + (size_t)slot * a.vmax * SW;
   W.delta = a.delta + (size_t)slot * a.vmax * SW;
+  W.q = a.q + (size_t)slot * a.vmax * SW;
   W.seen = a.masks + (size_t)slot * a.vmax * 3;
   W.nxt = W.seen + a.vmax;
   W.dense = W.nxt + a.vmax;
@@ -888,7 +895,7 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(CTA_THREADS) k_bc_cl
       // every CTA keeps its own copy: run_batch reads srcs from the caller's CTA
       for (int t = threadIdx.x; t < nb; t += blockDim.x) s_src[t] = a.srcs[sb + s0 + t] - vb;
       __syncthreads();
-      if (!run_batch_any<NW>(W, s_src, nb, cs)) return;
+      if (!run_batch_any<NW, BU_GRAPHS>(W, s_src, nb, cs)) return;
     }
   }
 }
@@ -961,7 +968,7 @@ struct BcPlan {
   dbuf<unsigned long long> ttime;
   dbuf<int> tcount;
   int trace_n = 0;
-  dbuf<double> sigma, bc, dacc;
+  dbuf<double> sigma, bc, dacc, q;
   dbuf<int32_t> hub_ent, hub_base;
   dbuf<unsigned long long> hub_cnt;
   dbuf<float> delta, fout;
@@ -1080,6 +1087,7 @@ static int bc_grid(sp_graph* g, const int32_t* d_srcs, int nsrc, int batch_hint,
   const size_t cap = (size_t)V * std::min(batch, 16) + 1024;  // level-list entries (vertex, mask)
   SP_TRY(p->sigma.alloc((size_t)V * SW));
   SP_TRY(p->delta.alloc((size_t)V * SW));
+  SP_TRY(p->q.alloc((size_t)V * SW));
   SP_TRY(p->masks.alloc((size_t)V * 3));
   SP_TRY(p->flv.alloc(cap));
   SP_TRY(p->flm.alloc(cap));
@@ -1112,6 +1120,7 @@ static int bc_grid(sp_graph* g, const int32_t* d_srcs, int nsrc, int batch_hint,
   W.V = V;
   W.sigma = p->sigma.p;
   W.delta = p->delta.p;
+  W.q = p->q.p;
   W.seen = p->masks.p;
   W.nxt = p->masks.p + V;
   W.dense = p->masks.p + 2 * (size_t)V;
@@ -1379,6 +1388,7 @@ extern "C" int sp_bc_graphs(sp_graph_h g, int32_t ngraphs, const int32_t* vertex
   const int ctas = teams;
   SP_TRY(p->sigma.alloc((size_t)ctas * vmax * SW));
   SP_TRY(p->delta.alloc((size_t)ctas * vmax * SW));
+  SP_TRY(p->q.alloc((size_t)ctas * vmax * SW));
   SP_TRY(p->masks.alloc((size_t)ctas * vmax * 3));
   SP_TRY(p->flv.alloc((size_t)ctas * cap));
   SP_TRY(p->flm.alloc((size_t)ctas * cap));
@@ -1415,6 +1425,7 @@ extern "C" int sp_bc_graphs(sp_graph_h g, int32_t ngraphs, const int32_t* vertex
   a.next = p->cnt.p + ctas;
   a.sigma = p->sigma.p;
   a.delta = p->delta.p;
+  a.q = p->q.p;
   a.masks = p->masks.p;
   a.flv = p->flv.p;
   a.flm = p->flm.p;
