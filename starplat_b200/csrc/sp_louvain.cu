@@ -66,6 +66,7 @@ struct Level {
   const int32_t* __restrict__ adj;
   const double* __restrict__ w;
   const double* __restrict__ sl;  // self-loop weight per vertex
+  int unit;                       // 1: every w is 1.0 (the input graph without weights), not read
 };
 
 struct MoveArgs {
@@ -124,6 +125,10 @@ __device__ __forceinline__ double group_sum(unsigned grp, double w) {
   return s;
 }
 
+// A weight w for which 32 * w and every partial sum of up to 32 copies are exact in FP64
+// (an integer of magnitude below 2^40), so a group of k lanes sums to k * w in any order.
+__device__ __forceinline__ bool uniform_ok(double w) { return w == rint(w) && fabs(w) < 1099511627776.0; }
+
 // One warp per vertex of degree <= 64 (= WARP_DEG), no tables: a lane holds one
 // neighbour per 32-edge round; __match_any_sync groups the lanes holding the same
 // community and the group sums its weights in lane order; a round-1 group adds into
@@ -148,18 +153,25 @@ __global__ void __launch_bounds__(THREADS) k_move_warp(MoveArgs a) {
     const int j0 = b + lane, j1 = b + 32 + lane;
     const bool on0 = j0 < e, on1 = j1 < e;
     const int c0 = on0 ? a.comm[a.L.adj[j0]] : -1 - lane;  // idle lanes: keys no community has
-    const double w0 = on0 ? a.L.w[j0] : 0.0;
+    const double w0 = on0 ? (a.L.unit ? 1.0 : a.L.w[j0]) : 0.0;
     const unsigned g0 = __match_any_sync(0xffffffffu, c0);
-    double s0 = group_sum(g0, w0);
+    // When every edge of the round carries the same integer weight (unit weights, the
+    // usual case), a group's lane-order sum is its size times that weight, exactly: the
+    // product gives the same value without a shuffle per group member.
+    const double wr0 = __shfl_sync(0xffffffffu, w0, 0);
+    const bool uni0 = a.L.unit || (__all_sync(0xffffffffu, !on0 || w0 == wr0) && uniform_ok(wr0));
+    double s0 = uni0 ? (double)__popc(g0) * wr0 : group_sum(g0, w0);
     const bool lead0 = on0 && lane == __ffs(g0) - 1;
     bool cand1 = false;
     int c1 = -1;
     double s1 = 0.0;
     if (e - b > 32) {  // the same for the whole warp
       c1 = on1 ? a.comm[a.L.adj[j1]] : -33 - lane;
-      const double w1 = on1 ? a.L.w[j1] : 0.0;
+      const double w1 = on1 ? (a.L.unit ? 1.0 : a.L.w[j1]) : 0.0;
       const unsigned g1 = __match_any_sync(0xffffffffu, c1);
-      s1 = group_sum(g1, w1);
+      const double wr1 = __shfl_sync(0xffffffffu, w1, 0);
+      const bool uni1 = a.L.unit || (__all_sync(0xffffffffu, !on1 || w1 == wr1) && uniform_ok(wr1));
+      s1 = uni1 ? (double)__popc(g1) * wr1 : group_sum(g1, w1);
       cand1 = on1 && lane == __ffs(g1) - 1;
       unsigned leads = __ballot_sync(0xffffffffu, cand1);
       while (leads) {
@@ -267,7 +279,7 @@ __global__ void __launch_bounds__(THREADS) k_move_cta(MoveArgs a, int slots) {
     const int cv = a.comm[v];
     const double kv = a.kv[v];
     for (int j = b + threadIdx.x; j < e; j += THREADS)
-      tab_add(keys, vals, (unsigned)nslots - 1u, a.comm[a.L.adj[j]], a.L.w[j]);
+      tab_add(keys, vals, (unsigned)nslots - 1u, a.comm[a.L.adj[j]], a.L.unit ? 1.0 : a.L.w[j]);
     __syncthreads();
     double bg = -INFINITY;
     int bc = -1;
@@ -313,7 +325,7 @@ __global__ void k_kv(Level L, double* kv, double* W) {
   double acc = 0;
   for (int v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < L.n; v += (gridDim.x * blockDim.x) >> 5) {
     double s = 0;
-    for (int j = L.off[v] + lane; j < L.off[v + 1]; j += 32) s += L.w[j];
+    for (int j = L.off[v] + lane; j < L.off[v + 1]; j += 32) s += L.unit ? 1.0 : L.w[j];
     s = warp_sum(s);
     if (lane == 0) {
       kv[v] = s + L.sl[v];
@@ -410,7 +422,7 @@ __global__ void __launch_bounds__(THREADS) k_internal(Level L, const int32_t* __
         if (t < total) {
           const int k = jb + (t - je);
           u[q] = L.adj[k];
-          wq[q] = L.w[k];
+          wq[q] = L.unit ? 1.0 : L.w[k];
         }
       }
 #pragma unroll
@@ -774,7 +786,8 @@ extern "C" int sp_louvain(sp_graph_h g, const float* weight, double threshold, i
   SP_CHECK_LAUNCH();
 
   // total weight W (constant over levels)
-  lv::Level L{n0, p->off[0].p, p->adj[0].p, p->w[0].p, p->sl[0].p};
+  // unweighted input: level 0's weights are all 1.0 and the kernels do not read them
+  lv::Level L{n0, p->off[0].p, p->adj[0].p, p->w[0].p, p->sl[0].p, weight ? 0 : 1};
   SP_CHECK_CUDA(cudaMemsetAsync(p->scal.p + 1, 0, sizeof(double), s));
   lv::k_kv<<<gs, 256, 0, s>>>(L, p->kv.p, p->scal.p + 1);
   SP_CHECK_LAUNCH();
@@ -979,7 +992,7 @@ extern "C" int sp_louvain(sp_graph_h g, const float* weight, double threshold, i
     }
     SP_TRY(dev_scan(p, p->rowcnt.p, p->off[nx].p, C + 1, s));
     cur = nx;
-    L = lv::Level{C, p->off[cur].p, p->adj[cur].p, p->w[cur].p, p->sl[cur].p};
+    L = lv::Level{C, p->off[cur].p, p->adj[cur].p, p->w[cur].p, p->sl[cur].p, 0};
   }
   *modularity = qcur;
   if (levels_out) *levels_out = levels;
