@@ -22,7 +22,7 @@
 // its stream before it returns.
 //
 // The caller's CSR is checked on the device before any gather (offsets start at 0,
-// never decrease and end at E; every srcList entry is a vertex id), with the verdict
+// never decrease and end at E; every srcList entry is a vertex id), with the outcome
 // kept in the scratch state, so a malformed graph returns SP_ERR_INVALID instead of
 // reading outside the caller's arrays.
 #include <mutex>
