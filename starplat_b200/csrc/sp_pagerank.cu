@@ -116,6 +116,10 @@ struct PrPlan {
   int exec_iters = 0;
   float exec_beta = -1, exec_delta = -1;
   int exec_sh = -1;       // srcList policy, vector loads and L1 hot count the graph was captured with
+  // the settings of the last call that launched its iterations directly: the graph is
+  // captured only when a call repeats them, so a handle used once pays no capture
+  int pend_iters = 0, pend_sh = -1;
+  float pend_beta = -1, pend_delta = -1;
   // The iterations are captured on this private stream and launched on the graph's
   // stream, which may be the legacy default stream (where capture is not allowed).
   cudaStream_t cap = nullptr;
@@ -924,6 +928,7 @@ static int build_pr_plan(sp_graph* g, int hot, int order, int part = 0, int npar
     g->pr = p;
   }
   cudaStream_t s = g->stream;
+  p->pend_iters = 0;
   if (p->exec) {  // it refers to the buffers rebuilt below
     cudaGraphExecDestroy(p->exec);
     p->exec = nullptr;
@@ -1240,16 +1245,8 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
     pr::k_init<<<num_sms() * 4, 256, 0, s>>>(V, p->od.p, p->prb[0].p, p->con[0].p, p->state.p);
   }
   SP_CHECK_LAUNCH();
-  if (!(p->exec && p->exec_iters == n_iter && p->exec_beta == beta && p->exec_delta == delta &&
-        p->exec_sh == exec_key)) {
-    if (p->exec) {
-      cudaGraphExecDestroy(p->exec);
-      p->exec = nullptr;
-    }
-    if (!p->cap) SP_CHECK_CUDA(cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking));
-    cudaStream_t cs = p->cap;  // capture only records: nothing runs on it
-    cudaGraph_t graph;
-    SP_CHECK_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+  // the iterations: every kernel returns at once after the stop test has ended the run
+  auto enqueue = [&](cudaStream_t cs) {
     for (int k = 0; k < n_iter; ++k) {
       const int c = k & 1, n = c ^ 1;
       if (k < 2 && p->n_zero)
@@ -1258,6 +1255,30 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
         pr::k_phase<0, 1, 0, 0><<<grid, pr::THREADS, 0, cs>>>(a, p->prb[c].p, p->con[c].p, p->prb[n].p, p->con[n].p);
       ph1<<<grid, pr::THREADS, 0, cs>>>(a, p->prb[c].p, p->con[c].p, p->prb[n].p, p->con[n].p);
     }
+  };
+  const bool cached = p->exec && p->exec_iters == n_iter && p->exec_beta == beta && p->exec_delta == delta &&
+                      p->exec_sh == exec_key;
+  const bool repeat = p->pend_iters == n_iter && p->pend_beta == beta && p->pend_delta == delta &&
+                      p->pend_sh == exec_key;
+  if (!cached && !repeat) {
+    // first call with these settings: launch directly (no capture and instantiation
+    // before the first kernel runs); a call that repeats them captures the graph
+    enqueue(s);
+    SP_CHECK_LAUNCH();
+    p->pend_iters = n_iter;
+    p->pend_beta = beta;
+    p->pend_delta = delta;
+    p->pend_sh = exec_key;
+  } else if (!cached) {
+    if (p->exec) {
+      cudaGraphExecDestroy(p->exec);
+      p->exec = nullptr;
+    }
+    if (!p->cap) SP_CHECK_CUDA(cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking));
+    cudaStream_t cs = p->cap;  // capture only records: nothing runs on it
+    cudaGraph_t graph;
+    SP_CHECK_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    enqueue(cs);
     cudaError_t ce = cudaStreamEndCapture(cs, &graph);
     if (ce != cudaSuccess) {
       set_error("pagerank graph capture: %s", cudaGetErrorString(ce));
@@ -1275,7 +1296,7 @@ static int pr_tuned(sp_graph* g, float beta, float delta, int32_t maxIter, float
     p->exec_delta = delta;
     p->exec_sh = exec_key;
   }
-  SP_CHECK_CUDA(cudaGraphLaunch(p->exec, s));
+  if (cached || repeat) SP_CHECK_CUDA(cudaGraphLaunch(p->exec, s));
   g_launches.fetch_add((unsigned long long)n_iter * (p->two_phase() ? 2 : 1) +
                        (p->n_zero ? std::min(2, n_iter) : 0));
   pr::State st;
